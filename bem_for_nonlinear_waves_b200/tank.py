@@ -1,0 +1,166 @@
+"""Synthetic rectangular wave tanks: closed surface meshes of linear triangles
+plus the linear Stokes standing-wave potential used for boundary data.
+
+The reference builds its BVP from a `Network` surface mesh whose faces carry
+Dirichlet (free surface) or Neumann (walls, bottom) flags
+(bem/BEM_setBoundaryTypes.hpp:447-586).  This module produces the same kind of
+input as flat arrays: point coordinates, triangle connectivity with outward
+normals, and a per-face Dirichlet flag.  Values are seeded and deterministic.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Tank:
+    X: np.ndarray               # (n_points, 3) float64, physical coordinates
+    tri: np.ndarray             # (n_faces, 3) int32, outward-oriented
+    face_dirichlet: np.ndarray  # (n_faces,) uint8: 1 free surface (Dirichlet), 0 wall/bottom
+    length: float
+    width: float
+    depth: float
+    amplitude: float
+    wavenumber: float
+    g: float = 9.81
+
+    @property
+    def omega(self) -> float:
+        k, h = self.wavenumber, self.depth
+        return math.sqrt(self.g * k * math.tanh(k * h))
+
+    def phi(self, X: np.ndarray) -> np.ndarray:
+        """Linear Stokes potential (gA/w) cosh(k(z+h))/cosh(kh) sin(kx)."""
+        k, h, A = self.wavenumber, self.depth, self.amplitude
+        c = self.g * A / self.omega / math.cosh(k * h)
+        return c * np.cosh(k * (X[..., 2] + h)) * np.sin(k * X[..., 0])
+
+    def grad_phi(self, X: np.ndarray) -> np.ndarray:
+        k, h, A = self.wavenumber, self.depth, self.amplitude
+        c = self.g * A / self.omega / math.cosh(k * h)
+        gx = c * k * np.cosh(k * (X[..., 2] + h)) * np.cos(k * X[..., 0])
+        gz = c * k * np.sinh(k * (X[..., 2] + h)) * np.sin(k * X[..., 0])
+        return np.stack([gx, np.zeros_like(gx), gz], axis=-1)
+
+    @property
+    def n_points(self) -> int:
+        return int(self.X.shape[0])
+
+    @property
+    def n_faces(self) -> int:
+        return int(self.tri.shape[0])
+
+
+def make_tank(length: float = 2.0, width: float = 1.0, depth: float = 0.5, h: float = 0.05,
+              amplitude: float = 0.01, wavelength: float = 1.0, noise_sigma: float = 0.0,
+              seed: int = 0) -> Tank:
+    """Closed box [0,L]x[0,W]x[-D,0] meshed as structured right-triangle grids.
+
+    `noise_sigma` perturbs the z of every free-surface node with seeded Gaussian
+    noise (the points stay on the vertical wall planes)."""
+    nx = max(1, int(round(length / h)))
+    ny = max(1, int(round(width / h)))
+    nz = max(1, int(round(depth / h)))
+    xs = np.linspace(0.0, length, nx + 1)
+    ys = np.linspace(0.0, width, ny + 1)
+    zs = np.linspace(-depth, 0.0, nz + 1)
+
+    pid = -np.ones((nx + 1, ny + 1, nz + 1), dtype=np.int64)
+    coords = []
+
+    def point(i, j, k):
+        if pid[i, j, k] < 0:
+            pid[i, j, k] = len(coords)
+            coords.append((xs[i], ys[j], zs[k]))
+        return pid[i, j, k]
+
+    tris = []
+    fdir = []
+
+    def quad_grid(fixed_axis, fixed_index, outward_sign, dirichlet):
+        axes = [a for a in range(3) if a != fixed_axis]
+        n = [nx, ny, nz]
+        for u in range(n[axes[0]]):
+            for v in range(n[axes[1]]):
+                def ijk(du, dv):
+                    idx = [0, 0, 0]
+                    idx[fixed_axis] = fixed_index
+                    idx[axes[0]] = u + du
+                    idx[axes[1]] = v + dv
+                    return point(*idx)
+                a, b, c, d = ijk(0, 0), ijk(1, 0), ijk(1, 1), ijk(0, 1)
+                for t in ((a, b, c), (a, c, d)):
+                    tris.append(t)
+                    fdir.append(dirichlet)
+
+    quad_grid(2, nz, +1, 1)   # free surface z = 0
+    quad_grid(2, 0, -1, 0)    # bottom
+    quad_grid(0, 0, -1, 0)    # x = 0
+    quad_grid(0, nx, +1, 0)   # x = L
+    quad_grid(1, 0, -1, 0)    # y = 0
+    quad_grid(1, ny, +1, 0)   # y = W
+
+    X = np.asarray(coords, dtype=np.float64)
+    tri = np.asarray(tris, dtype=np.int32)
+    fdir = np.asarray(fdir, dtype=np.uint8)
+
+    # orient every triangle outward: normal . (centroid - box centre) > 0 on a box
+    centre = np.array([length / 2, width / 2, -depth / 2])
+    n = np.cross(X[tri[:, 1]] - X[tri[:, 0]], X[tri[:, 2]] - X[tri[:, 0]])
+    cen = X[tri].mean(axis=1)
+    flip = np.einsum("ij,ij->i", n, cen - centre) < 0
+    tri[flip] = tri[flip][:, [0, 2, 1]]
+
+    if noise_sigma > 0.0:
+        rng = np.random.default_rng(seed)
+        top = np.isclose(X[:, 2], 0.0)
+        X[top, 2] += rng.normal(0.0, noise_sigma, size=int(top.sum()))
+
+    return Tank(X=X, tri=tri, face_dirichlet=fdir, length=length, width=width, depth=depth,
+                amplitude=amplitude, wavenumber=2.0 * math.pi / wavelength)
+
+
+# Named workloads (tank sizes, spacing, expansion order).
+CONFIGS = {
+    # ~2,800 nodes / 5,600 triangles, p=8 (the reference's CPU-runnable case)
+    "tank_2800": dict(length=2.0, width=1.0, depth=0.5, h=0.05, p=8, tol=1e-10),
+    # ~60,000 nodes / 120,000 triangles, free surface z-noise 0.2h, p=10
+    "tank_60k": dict(length=2.0, width=1.0, depth=0.5, h=2.0 / 185, p=10, tol=1e-8, noise=0.2),
+}
+
+
+def known_values(tank: Tank, dof_point: np.ndarray, dof_face: np.ndarray, dof_kind: np.ndarray,
+                 point_normal: np.ndarray) -> np.ndarray:
+    """Known boundary data per DOF in physical units: phi for Dirichlet DOFs, the
+    analytic normal derivative grad(phi).n for Neumann DOFs (face normal for
+    per-face DOFs, point normal otherwise)."""
+    X = tank.X
+    kv = np.zeros(dof_point.shape[0], dtype=np.float64)
+    d = dof_kind == 0
+    kv[d] = tank.phi(X[dof_point[d]])
+    nd = ~d
+    g = tank.grad_phi(X[dof_point[nd]])
+    fn = face_normals(tank)
+    f = dof_face[nd]
+    nrm = np.where((f >= 0)[:, None], fn[np.maximum(f, 0)], point_normal[dof_point[nd]])
+    kv[nd] = np.einsum("ij,ij->i", g, nrm)
+    return kv
+
+
+def face_normals(tank: Tank) -> np.ndarray:
+    X, t = tank.X, tank.tri
+    n = np.cross(X[t[:, 1]] - X[t[:, 0]], X[t[:, 2]] - X[t[:, 0]])
+    return n / np.linalg.norm(n, axis=1)[:, None]
+
+
+def point_normals(tank: Tank) -> np.ndarray:
+    """Area-weighted point normals (networkPoint::getNormalAreaAveraged)."""
+    X, t = tank.X, tank.tri
+    n = np.cross(X[t[:, 1]] - X[t[:, 0]], X[t[:, 2]] - X[t[:, 0]]) * 0.5
+    pn = np.zeros_like(X)
+    for a in range(3):
+        np.add.at(pn, t[:, a], n)
+    return pn / np.maximum(np.linalg.norm(pn, axis=1), 1e-300)[:, None]

@@ -1,0 +1,155 @@
+/*
+ * bem_b200.h — C ABI of the B200 (sm_100a) GMRES + FMM Laplace boundary-value solver.
+ *
+ * Drop-in for the reference's GMRES-FMM branch of BEM_BVP::solve()
+ * (bem/BEM_solveBVP.hpp:565-630 -> solveGMRES, bem/BEM_solveBVP_GMRES_FMM.hpp:3056-3506):
+ * mesh, boundary types and known phi/phin in; phi/phin per DOF out.
+ * Conventions follow the reference's Metal plugins (bem/metal_m2l/metal_m2l.h:23-130):
+ * opaque context, create() returns NULL on failure, int status (0 = success), no C++
+ * exceptions cross this boundary, plain pointers and sizes only.
+ *
+ * All arrays are HOST memory unless a function name ends in _device.
+ * Units: coordinates and known values are physical; the solver applies the reference's
+ * coordinate scaling internally (x' = x/L, L = bounding-box diagonal) and returns
+ * physical values.
+ */
+#ifndef BEM_B200_H
+#define BEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define BEM_OK 0
+#define BEM_ERR_INVALID_ARGUMENT -1
+#define BEM_ERR_OUT_OF_MEMORY -2
+#define BEM_ERR_NOT_CONVERGED -3
+#define BEM_ERR_NAN -4
+#define BEM_ERR_DEVICE -5
+#define BEM_ERR_NOT_READY -6
+#define BEM_ERR_UNSUPPORTED -7
+
+/* DOF kinds (bem/BEM_setBoundaryTypes.hpp:29-100):
+ *   0: Dirichlet key (p, null): phi known, phin unknown
+ *   1: Neumann key  (p, null) or (p, f): phin known, phi unknown
+ *   2: Neumann key (p, f) of a CORNER point: phi unknown and constrained to the point's
+ *      Dirichlet phi (constraint row A v = phi, BEM_solveBVP_GMRES_FMM.hpp:100-108, 2031-2047) */
+#define BEM_DOF_DIRICHLET 0
+#define BEM_DOF_NEUMANN 1
+#define BEM_DOF_CORNER_NEUMANN 2
+
+typedef struct bem_gpu_ctx bem_gpu_ctx;
+
+/* Solver options.  Replaces the reference's globals fmm_max_level, fmm_bucket_max_points,
+ * g_mac_theta, solver_tol, solver_max_iter (bem/main_time_domain.cpp:52-62) and the
+ * compile-time expansion order of B_poles (bem/BEM_solveBVP.hpp:563). */
+typedef struct {
+  int32_t expansion_order;   /* p, 1..12 (reference default 10) */
+  double mac_theta;          /* MAC parameter theta (0.25) */
+  int32_t leaf_max_elements; /* a bucket splits while it holds more elements than this */
+  int32_t max_level;         /* deepest octree level (7) */
+  double tol;                /* absolute GMRES tolerance on the scaled system (solver_tol) */
+  int32_t max_iter;          /* GMRES iteration cap (solver_max_iter) */
+  int32_t device;            /* CUDA device ordinal */
+  int32_t reserved[5];
+} bem_gpu_opts;
+
+/* One boundary-value problem.  The DOF table is what the reference's setNodeFaceIndices()
+ * produces (one DOF per (point, face-or-null) key); bem_gpu_build_dofs() derives it from
+ * the face flags with the reference's rules. */
+typedef struct {
+  int32_t n_points;
+  const double* X;               /* [3*n_points] */
+  int32_t n_faces;
+  const int32_t* tri;            /* [3*n_faces], outward orientation */
+  const uint8_t* face_dirichlet; /* [n_faces] 1 = Dirichlet (free surface), 0 = Neumann */
+  int32_t n_dof;
+  const int32_t* dof_point;      /* [n_dof] */
+  const int32_t* dof_face;       /* [n_dof] face id or -1 */
+  const int32_t* dof_kind;       /* [n_dof] BEM_DOF_* */
+  const int32_t* face_dof;       /* [3*n_faces] DOF used by each face vertex (pf2Index) */
+} bem_bvp_desc;
+
+typedef struct {
+  int32_t iterations;     /* GMRES iterations (Arnoldi steps) */
+  int32_t converged;      /* 1 if the true residual reached tol */
+  double residual;        /* last true residual |A x - b| (scaled system) */
+  double residual_est;    /* last Givens estimate */
+  double time_setup_s;    /* wall time of setup (tree, lists, near weights, diagonal) */
+  double time_solve_s;    /* wall time of the GMRES solve */
+  int64_t nnz_near;       /* cached near-field weights */
+  int64_t m2l_pairs;      /* box pairs in the M2L lists */
+  int32_t n_nodes;        /* non-empty octree nodes */
+  int32_t n_leaves;
+  int32_t matvecs;        /* operator applications in this solve */
+  int32_t reserved[5];
+} bem_gpu_stats;
+
+/* 1 if a CUDA device of compute capability 10.x is visible. */
+int bem_gpu_is_available(void);
+
+/* Default options: p=10, theta=0.25, 30 elements per leaf, 7 levels, tol 1e-9, 500 iterations. */
+void bem_gpu_default_opts(bem_gpu_opts* opts);
+
+/* Create a solver context on opts->device; NULL on failure. */
+bem_gpu_ctx* bem_gpu_create(const bem_gpu_opts* opts);
+void bem_gpu_destroy(bem_gpu_ctx* ctx);
+const char* bem_gpu_last_error(const bem_gpu_ctx* ctx);
+
+/* DOF table from face flags (setNodeFaceIndices + setIsMultipleNode,
+ * bem/BEM_setBoundaryTypes.hpp:134-254, 434-441, 555-562).  Output arrays hold up to
+ * n_points + 3*n_faces entries (face_dof: 3*n_faces; point_flags: n_points, bits
+ * 1=Neumann 2=Dirichlet 4=CORNER 8=multiple node, may be NULL).  Returns n_dof (>= 0) or
+ * a negative status.  Host-only; needs no GPU. */
+int bem_gpu_build_dofs(int32_t n_points, const double* X, int32_t n_faces, const int32_t* tri, const uint8_t* face_dirichlet,
+                       int32_t* dof_point, int32_t* dof_face, int32_t* dof_kind, int32_t* face_dof, uint8_t* point_flags);
+
+/* Geometry set-up for one BVP: scaling, element sources, octree, interaction lists,
+ * L2P targets, near-field weights and the rigid-mode diagonal.  Replaces the part of
+ * solveGMRES() before solveSystemGMRES (BEM_solveBVP_GMRES_FMM.hpp:3056-3447). */
+int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* desc);
+
+/* Solve with known boundary values (physical units; phi for Dirichlet DOFs, phin for
+ * Neumann and corner-Neumann DOFs).  x0 may be NULL (zero initial guess).  out_phi and
+ * out_phin get every DOF's phi and phin (known values copied through).  Replaces
+ * solveSystemGMRES + the unscaling in solveGMRES (BEM_solveBVP_GMRES_FMM.hpp:2007-2649,
+ * 3462-3486).  Returns BEM_OK, or BEM_ERR_NOT_CONVERGED with the outputs still written. */
+int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, double* out_phi, double* out_phin, bem_gpu_stats* stats);
+
+/* setup + solve. */
+int bem_gpu_solve_bvp(bem_gpu_ctx* ctx, const bem_bvp_desc* desc, const double* known, const double* x0, double* out_phi,
+                      double* out_phin, bem_gpu_stats* stats);
+
+/* Operator rows for per-DOF phi/phin in scaled units (compute_Ax_minus_b,
+ * BEM_solveBVP_GMRES_FMM.hpp:34-158): Av[i] = GPhin - (GnPhi + diag_i phi_i), or phi_i on
+ * corner-Neumann rows. */
+int bem_gpu_apply(bem_gpu_ctx* ctx, const double* phi, const double* phin, double* Av);
+
+/* Near + far integrals per point, GPhin = int G phin, GnPhi = int dG/dn phi
+ * (target4FMM::integrateNearField + integrateFarField, lib_multipole_expansion.hpp:1143-1150,
+ * 1273-1302).  Arrays of n_points. */
+int bem_gpu_point_integrals(bem_gpu_ctx* ctx, const double* phi, const double* phin, double* GPhin, double* GnPhi);
+
+/* Unknown-space mat-vec on device buffers: y = A x (x, y: n_dof doubles on the device),
+ * on the context's stream (return_A_dot_v, BEM_solveBVP_GMRES_FMM.hpp:2124-2155). */
+int bem_gpu_matvec_device(bem_gpu_ctx* ctx, const double* d_x, double* d_y);
+
+/* Introspection for parity tests. */
+int bem_gpu_get_diag(bem_gpu_ctx* ctx, double* diag);                 /* [n_dof] */
+double bem_gpu_scale_factor(const bem_gpu_ctx* ctx);                  /* L */
+int bem_gpu_near_row(bem_gpu_ctx* ctx, int32_t point, int32_t cap, int32_t* dof, double* wG, double* wGn);
+int bem_gpu_face_leaf(bem_gpu_ctx* ctx, int32_t* level, double* corner); /* [n_faces], [3*n_faces] */
+int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out /*[8]: nodes, leaves, depth, added, m2l, near, nnz, targets*/);
+
+/* Kernel timing of the last mat-vec executed through bem_gpu_profile_matvec: per stage
+ * milliseconds [p2m, m2m, m2l, l2l, near+l2p, total] measured with CUDA events. */
+int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[6]*/);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BEM_B200_H */
