@@ -1,0 +1,210 @@
+"""Host-side mirror of the reference's BEM_BVP for the GMRES + FMM path.
+
+`BEM_BVP.solve()` keeps the reference's contract (bem/BEM_solveBVP.hpp:565-630): it
+indexes the unknowns (setNodeFaceIndices), runs the GMRES-FMM solve and returns
+`(time_setup, time_solve, unknowns)`; the per-DOF solution lands in `ans`, `phi`, `phin`
+and the diagnostics in `last_gmres_*` (BEM_solveBVP.hpp:376-410).  Every operator
+application runs in the sm_100a kernels of lib/libbem_b200.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+
+DOF_DIRICHLET, DOF_NEUMANN, DOF_CORNER_NEUMANN = 0, 1, 2
+
+
+def build_dofs(X, tri, face_dirichlet):
+    """DOF keys (point, face or -1), kinds and per-face-vertex DOF (pf2Index) from face flags,
+    with the reference's rules (bem/BEM_setBoundaryTypes.hpp:29-254, 434-441)."""
+    lib = L.load()
+    X = np.ascontiguousarray(X, np.float64)
+    tri = np.ascontiguousarray(tri, np.int32)
+    fd = np.ascontiguousarray(face_dirichlet, np.uint8)
+    npts, nf = X.shape[0], tri.shape[0]
+    cap = npts + 3 * nf
+    dp = np.zeros(cap, np.int32)
+    df = np.zeros(cap, np.int32)
+    dk = np.zeros(cap, np.int32)
+    fdof = np.zeros(3 * nf, np.int32)
+    pfl = np.zeros(npts, np.uint8)
+    n = lib.bem_gpu_build_dofs(npts, L.ptr(X, L.P_dbl), nf, L.ptr(tri, L.P_int), L.ptr(fd, L.P_u8), L.ptr(dp, L.P_int),
+                               L.ptr(df, L.P_int), L.ptr(dk, L.P_int), L.ptr(fdof, L.P_int), L.ptr(pfl, L.P_u8))
+    if n < 0:
+        raise ValueError("invalid mesh for DOF indexing: " + L.STATUS.get(n, str(n)))
+    return dict(dof_point=dp[:n].copy(), dof_face=df[:n].copy(), dof_kind=dk[:n].copy(), face_dof=fdof.reshape(nf, 3),
+                point_flags=pfl)
+
+
+class BEM_BVP:
+    """GMRES-FMM Laplace BVP on one B200."""
+
+    def __init__(self, X, tri, face_dirichlet, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30,
+                 fmm_max_level=7, solver_tol=1e-9, solver_max_iter=500, device=0, dofs=None, tol_relative=False):
+        self.lib = L.load()
+        if not self.lib.bem_gpu_is_available():
+            raise RuntimeError("no sm_100 CUDA device visible: the GMRES-FMM solver runs only on the GPU")
+        self.X = np.ascontiguousarray(X, np.float64)
+        self.tri = np.ascontiguousarray(tri, np.int32)
+        self.face_dirichlet = np.ascontiguousarray(face_dirichlet, np.uint8)
+        o = L.Opts()
+        self.lib.bem_gpu_default_opts(ctypes.byref(o))
+        o.expansion_order = int(expansion_order)
+        o.mac_theta = float(mac_theta)
+        o.leaf_max_elements = int(fmm_bucket_max_points)
+        o.max_level = int(fmm_max_level)
+        o.tol = float(solver_tol)
+        o.max_iter = int(solver_max_iter)
+        o.device = int(device)
+        o.tol_relative = 1 if tol_relative else 0
+        self.opts = o
+        self.ctx = self.lib.bem_gpu_create(ctypes.byref(o))
+        if not self.ctx:
+            raise RuntimeError("bem_gpu_create failed")
+        self.dofs = dofs
+        self.matrix_size = 0
+        self._setup_done = False
+        self.ans = None
+        self.phi = None
+        self.phin = None
+        self.last_gmres_total_iter = 0
+        self.last_gmres_residual_norm = 0.0
+        self.last_gmres_converged = False
+        self.stats = None
+
+    def __del__(self):
+        ctx = getattr(self, "ctx", None)
+        if ctx:
+            self.lib.bem_gpu_destroy(ctx)
+            self.ctx = None
+
+    def _check(self, rc, what):
+        if rc not in (L.BEM_OK,):
+            msg = self.lib.bem_gpu_last_error(self.ctx)
+            raise RuntimeError(f"{what}: {L.STATUS.get(rc, rc)}: {msg.decode() if msg else ''}")
+
+    # setNodeFaceIndices (bem/BEM_setBoundaryTypes.hpp:134-254)
+    def setNodeFaceIndices(self):
+        if self.dofs is None:
+            self.dofs = build_dofs(self.X, self.tri, self.face_dirichlet)
+        self.matrix_size = int(self.dofs["dof_point"].shape[0])
+        return self.matrix_size
+
+    def setup(self):
+        """Geometry part of solveGMRES (scaling, sources, tree, lists, near weights, diagonal)."""
+        self.setNodeFaceIndices()
+        d = self.dofs
+        self._keep = [np.ascontiguousarray(d[k], np.int32).reshape(-1) for k in ("dof_point", "dof_face", "dof_kind", "face_dof")]
+        desc = L.Desc(self.X.shape[0], L.ptr(self.X, L.P_dbl), self.tri.shape[0], L.ptr(self.tri, L.P_int),
+                      L.ptr(self.face_dirichlet, L.P_u8), self.matrix_size, L.ptr(self._keep[0], L.P_int),
+                      L.ptr(self._keep[1], L.P_int), L.ptr(self._keep[2], L.P_int), L.ptr(self._keep[3], L.P_int))
+        self._check(self.lib.bem_gpu_setup(self.ctx, ctypes.byref(desc)), "setup")
+        self._setup_done = True
+
+    def solve(self, known, x0=None):
+        """known: per-DOF phi (Dirichlet DOFs) or phin (Neumann DOFs), physical units.
+        Returns (time_setup, time_solve, unknowns) like BEM_BVP::solve()."""
+        if not self._setup_done:
+            self.setup()
+        known = np.ascontiguousarray(known, np.float64)
+        if known.shape[0] != self.matrix_size:
+            raise ValueError("known values must have one entry per DOF")
+        phi = np.zeros(self.matrix_size)
+        phin = np.zeros(self.matrix_size)
+        st = L.Stats()
+        x0p = None if x0 is None else L.ptr(np.ascontiguousarray(x0, np.float64), L.P_dbl)
+        rc = self.lib.bem_gpu_solve(self.ctx, L.ptr(known, L.P_dbl), x0p, L.ptr(phi, L.P_dbl), L.ptr(phin, L.P_dbl), ctypes.byref(st))
+        if rc not in (L.BEM_OK, L.BEM_ERR_NOT_CONVERGED):
+            self._check(rc, "solve")
+        self.phi, self.phin = phi, phin
+        kind = self.dofs["dof_kind"]
+        self.ans = np.where(kind == DOF_DIRICHLET, phin, phi)
+        self.stats = st
+        self.last_gmres_total_iter = st.iterations
+        self.last_gmres_residual_norm = st.residual
+        self.last_gmres_converged = bool(st.converged)
+        return (st.time_setup_s, st.time_solve_s, float(self.matrix_size))
+
+    # ---- operator access (scaled units) ----
+    def apply(self, phi, phin):
+        phi = np.ascontiguousarray(phi, np.float64)
+        phin = np.ascontiguousarray(phin, np.float64)
+        out = np.zeros(self.matrix_size)
+        self._check(self.lib.bem_gpu_apply(self.ctx, L.ptr(phi, L.P_dbl), L.ptr(phin, L.P_dbl), L.ptr(out, L.P_dbl)), "apply")
+        return out
+
+    def point_integrals(self, phi, phin):
+        phi = np.ascontiguousarray(phi, np.float64)
+        phin = np.ascontiguousarray(phin, np.float64)
+        a = np.zeros(self.X.shape[0])
+        b = np.zeros(self.X.shape[0])
+        self._check(self.lib.bem_gpu_point_integrals(self.ctx, L.ptr(phi, L.P_dbl), L.ptr(phin, L.P_dbl), L.ptr(a, L.P_dbl),
+                                                     L.ptr(b, L.P_dbl)), "point_integrals")
+        return a, b
+
+    def diag(self):
+        out = np.zeros(self.matrix_size)
+        self._check(self.lib.bem_gpu_get_diag(self.ctx, L.ptr(out, L.P_dbl)), "diag")
+        return out
+
+    @property
+    def scale_factor(self):
+        return self.lib.bem_gpu_scale_factor(self.ctx)
+
+    def near_row(self, point):
+        n = self.lib.bem_gpu_near_row(self.ctx, int(point), 0, None, None, None)
+        if n < 0:
+            self._check(n, "near_row")
+        idx = np.zeros(max(n, 1), np.int32)
+        g = np.zeros(max(n, 1))
+        gn = np.zeros(max(n, 1))
+        self.lib.bem_gpu_near_row(self.ctx, int(point), n, L.ptr(idx, L.P_int), L.ptr(g, L.P_dbl), L.ptr(gn, L.P_dbl))
+        return idx[:n].copy(), g[:n].copy(), gn[:n].copy()
+
+    def face_leaf(self):
+        nf = self.tri.shape[0]
+        lv = np.zeros(nf, np.int32)
+        c = np.zeros(3 * nf)
+        self._check(self.lib.bem_gpu_face_leaf(self.ctx, L.ptr(lv, L.P_int), L.ptr(c, L.P_dbl)), "face_leaf")
+        return lv, c.reshape(-1, 3)
+
+    def tree_stats(self):
+        out = np.zeros(8, np.int64)
+        self._check(self.lib.bem_gpu_tree_stats(self.ctx, L.ptr(out, L.P_i64)), "tree_stats")
+        keys = ["nodes", "leaves", "depth", "n_added", "m2l_pairs", "near_pairs", "nnz", "near_blocks"]
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def matvec_time_ms(self, repeats=10):
+        st = np.zeros(6)
+        self._check(self.lib.bem_gpu_profile_matvec(self.ctx, int(repeats), L.ptr(st, L.P_dbl)), "profile")
+        return float(st[5])
+
+
+def inspect_plan(X, tri, face_dirichlet, dofs=None, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30,
+                 fmm_max_level=7):
+    """Builds the host set-up plan without a GPU and returns (face_level, face_corner, stats):
+    the leaf bucket of every element and the tree / list / near-field sizes."""
+    lib = L.load()
+    X = np.ascontiguousarray(X, np.float64)
+    tri = np.ascontiguousarray(tri, np.int32)
+    fd = np.ascontiguousarray(face_dirichlet, np.uint8)
+    if dofs is None:
+        dofs = build_dofs(X, tri, fd)
+    keep = [np.ascontiguousarray(dofs[k], np.int32).reshape(-1) for k in ("dof_point", "dof_face", "dof_kind", "face_dof")]
+    o = L.Opts()
+    lib.bem_gpu_default_opts(ctypes.byref(o))
+    o.expansion_order, o.mac_theta = int(expansion_order), float(mac_theta)
+    o.leaf_max_elements, o.max_level = int(fmm_bucket_max_points), int(fmm_max_level)
+    desc = L.Desc(X.shape[0], L.ptr(X, L.P_dbl), tri.shape[0], L.ptr(tri, L.P_int), L.ptr(fd, L.P_u8), keep[0].shape[0],
+                  L.ptr(keep[0], L.P_int), L.ptr(keep[1], L.P_int), L.ptr(keep[2], L.P_int), L.ptr(keep[3], L.P_int))
+    lv = np.zeros(tri.shape[0], np.int32)
+    corner = np.zeros(3 * tri.shape[0])
+    st = np.zeros(8, np.int64)
+    rc = lib.bem_plan_inspect(ctypes.byref(o), ctypes.byref(desc), L.ptr(lv, L.P_int), L.ptr(corner, L.P_dbl), L.ptr(st, L.P_i64))
+    if rc != 0:
+        raise ValueError("plan construction failed: " + L.STATUS.get(rc, str(rc)))
+    keys = ["nodes", "leaves", "depth", "n_added", "m2l_pairs", "near_pairs", "nnz", "near_blocks"]
+    return lv, corner.reshape(-1, 3), {k: int(v) for k, v in zip(keys, st)}

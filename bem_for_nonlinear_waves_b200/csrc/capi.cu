@@ -1,0 +1,811 @@
+// C ABI (include/bem_b200.h): solver context, device upload, mat-vec orchestration
+// (CUDA-graph captured) and the device-resident GMRES driver.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/bem_b200.h"
+#include "fmm_math.cuh"
+#include "kernels.cuh"
+#include "plan.hpp"
+
+using namespace bemb200;
+
+namespace {
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    release();
+    n = count;
+    if (count == 0) return cudaSuccess;
+    return cudaMalloc((void**)&p, sizeof(T) * count);
+  }
+  cudaError_t upload(const std::vector<T>& v, cudaStream_t s) {
+    cudaError_t e = alloc(v.size());
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s);
+  }
+};
+
+double now_s() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+
+}  // namespace
+
+struct bem_gpu_ctx {
+  bem_gpu_opts opts{};
+  cudaStream_t stream = nullptr;
+  std::string err;
+  Plan plan;
+  bool ready = false;
+  double time_setup = 0.0;
+
+  // geometry / tree
+  DBuf<double> Xs, e_q, e_W, e_n, e_near, node_X, WG, WGn, diag;
+  DBuf<int> e_dof, e_vtx, node_fb, node_fe, leaves, level_parents, child_begin, child_end, node_children;
+  DBuf<int> m2l_targets, m2l_off, m2l_src, nb_dofs, nb_targets, nb_ranges, dof_inc_off, dof_inc;
+  DBuf<int> point_dof_off, point_dof, dof_kind, dof_point;
+  DBuf<NearBlockDev> blocks;
+  DBuf<double2> M, L;
+  std::vector<int> level_parent_off;
+  int n_m2l_targets = 0, max_ntgt = 0, chunk = 0;
+  // state
+  DBuf<double> phi, phin, known_s, rows, GPhin, GnPhi;
+  // graph-captured A.x : mv_in -> mv_out
+  DBuf<double> mv_in, mv_out;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  // Krylov
+  DBuf<double> V, w, hdev, partial, xdev, bdev, rdev, ydev;
+  int V_cols = 0;
+
+  ~bem_gpu_ctx() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  MatvecArgs args(const double* d_phi, const double* d_phin, double* d_rows, double* d_gphin, double* d_gnphi) const {
+    MatvecArgs a;
+    a.n_nodes = (int)plan.nodes.size();
+    a.n_levels = (int)level_parent_off.size() - 1;
+    a.n_leaves = (int)plan.leaves.size();
+    a.leaves = leaves.p;
+    a.node_fb = node_fb.p;
+    a.node_fe = node_fe.p;
+    a.node_X = node_X.p;
+    a.e_q = e_q.p;
+    a.e_W = e_W.p;
+    a.e_n = e_n.p;
+    a.e_dof = e_dof.p;
+    a.level_parent_off = level_parent_off.data();
+    a.level_parents = level_parents.p;
+    a.child_begin = child_begin.p;
+    a.child_end = child_end.p;
+    a.node_children = node_children.p;
+    a.n_m2l_targets = n_m2l_targets;
+    a.m2l_targets = m2l_targets.p;
+    a.m2l_off = m2l_off.p;
+    a.m2l_src = m2l_src.p;
+    a.M = M.p;
+    a.L = L.p;
+    a.n_blocks = (int)plan.blocks.size();
+    a.chunk = chunk;
+    a.max_ntgt = max_ntgt;
+    a.blocks = blocks.p;
+    a.nb_dofs = nb_dofs.p;
+    a.nb_targets = nb_targets.p;
+    a.WG = WG.p;
+    a.WGn = WGn.p;
+    a.Xs = Xs.p;
+    a.point_dof_off = point_dof_off.p;
+    a.point_dof = point_dof.p;
+    a.dof_kind = dof_kind.p;
+    a.diag = diag.p;
+    a.phi = d_phi;
+    a.phin = d_phin;
+    a.rows = d_rows;
+    a.GPhin = d_gphin;
+    a.GnPhi = d_gnphi;
+    return a;
+  }
+};
+
+#define CK(call)                                                               \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);            \
+      return e_ == cudaErrorMemoryAllocation ? BEM_ERR_OUT_OF_MEMORY : BEM_ERR_DEVICE; \
+    }                                                                          \
+  } while (0)
+
+namespace {
+
+int fill_quadrature(bem_gpu_ctx* ctx) {
+  const double dv[6][4] = {{0.816847572980459, 0.091576213509771, 0.091576213509771, 0.054975871827661},
+                           {0.091576213509771, 0.816847572980459, 0.091576213509771, 0.054975871827661},
+                           {0.091576213509771, 0.091576213509771, 0.816847572980459, 0.054975871827661},
+                           {0.108103018168070, 0.445948490915965, 0.445948490915965, 0.111690794839006},
+                           {0.445948490915965, 0.108103018168070, 0.445948490915965, 0.111690794839006},
+                           {0.445948490915965, 0.445948490915965, 0.108103018168070, 0.111690794839006}};
+  // 5-point Gauss-Legendre nodes/weights on [-1,1], mapped to [0,1]^2 (__array_GW5xGW5__)
+  const double xs[5] = {-0.9061798459386640, -0.5384693101056831, 0.0, 0.5384693101056831, 0.9061798459386640};
+  const double ws[5] = {0.2369268850561891, 0.4786286704993665, 0.5688888888888889, 0.4786286704993665, 0.2369268850561891};
+  double gw[25][3];
+  for (int a = 0; a < 5; ++a)
+    for (int b = 0; b < 5; ++b) {
+      gw[5 * a + b][0] = 0.5 * (xs[a] + 1.0);
+      gw[5 * a + b][1] = 0.5 * (xs[b] + 1.0);
+      gw[5 * a + b][2] = 0.25 * ws[a] * ws[b];
+    }
+  upload_quadrature(dv, gw, ctx->stream);
+  CK(cudaGetLastError());
+  return BEM_OK;
+}
+
+// one operator application on device state: densities already in ctx->phi/phin
+void run_fmm(bem_gpu_ctx* ctx, double* rows, double* gphin, double* gnphi) {
+  launch_matvec(ctx->plan.opt.p, ctx->args(ctx->phi.p, ctx->phin.p, rows, gphin, gnphi), ctx->stream);
+}
+
+int build_graph(bem_gpu_ctx* ctx) {
+  if (ctx->graph_exec) {
+    cudaGraphExecDestroy(ctx->graph_exec);
+    ctx->graph_exec = nullptr;
+  }
+  if (ctx->graph) {
+    cudaGraphDestroy(ctx->graph);
+    ctx->graph = nullptr;
+  }
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  launch_densities(ctx->plan.ndof, 0, ctx->mv_in.p, nullptr, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, ctx->stream);
+  run_fmm(ctx, ctx->mv_out.p, nullptr, nullptr);
+  CK(cudaStreamEndCapture(ctx->stream, &ctx->graph));
+  CK(cudaGraphInstantiate(&ctx->graph_exec, ctx->graph, 0));
+  return BEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bem_gpu_is_available(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return 0;
+  for (int d = 0; d < n; ++d) {
+    cudaDeviceProp pr{};
+    if (cudaGetDeviceProperties(&pr, d) == cudaSuccess && pr.major == 10) return 1;
+  }
+  return 0;
+}
+
+void bem_gpu_default_opts(bem_gpu_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->expansion_order = 10;
+  o->mac_theta = 0.25;
+  o->leaf_max_elements = 30;
+  o->max_level = 7;
+  o->tol = 1e-9;
+  o->max_iter = 500;
+  o->device = 0;
+}
+
+bem_gpu_ctx* bem_gpu_create(const bem_gpu_opts* opts) {
+  if (!opts || opts->expansion_order < 1 || opts->expansion_order > 12 || !(opts->mac_theta > 0) || opts->leaf_max_elements < 1 ||
+      opts->max_level < 1 || opts->max_level > 20 || opts->max_iter < 1)
+    return nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || opts->device < 0 || opts->device >= ndev) return nullptr;
+  if (cudaSetDevice(opts->device) != cudaSuccess) return nullptr;
+  auto* ctx = new (std::nothrow) bem_gpu_ctx();
+  if (!ctx) return nullptr;
+  ctx->opts = *opts;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return nullptr;
+  }
+  if (fill_quadrature(ctx) != BEM_OK) {
+    delete ctx;
+    return nullptr;
+  }
+  return ctx;
+}
+
+void bem_gpu_destroy(bem_gpu_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->opts.device);
+  delete ctx;
+}
+
+const char* bem_gpu_last_error(const bem_gpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int bem_gpu_build_dofs(int32_t n_points, const double* X, int32_t n_faces, const int32_t* tri, const uint8_t* face_dirichlet,
+                       int32_t* dof_point, int32_t* dof_face, int32_t* dof_kind, int32_t* face_dof, uint8_t* point_flags) {
+  if (!dof_point || !dof_face || !dof_kind || !face_dof) return BEM_ERR_INVALID_ARGUMENT;
+  const int n = build_dofs(n_points, X, n_faces, tri, face_dirichlet, dof_point, dof_face, dof_kind, face_dof, point_flags);
+  return n < 0 ? BEM_ERR_INVALID_ARGUMENT : n;
+}
+
+int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
+  if (!ctx || !d) return BEM_ERR_INVALID_ARGUMENT;
+  CK(cudaSetDevice(ctx->opts.device));
+  ctx->ready = false;
+  const double t0 = now_s();
+  PlanOptions po;
+  po.p = ctx->opts.expansion_order;
+  po.theta = ctx->opts.mac_theta;
+  po.leaf_max = ctx->opts.leaf_max_elements;
+  po.max_level = ctx->opts.max_level;
+  if (!build_plan(ctx->plan, po, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face,
+                  d->dof_kind, d->face_dof)) {
+    ctx->err = ctx->plan.error;
+    return BEM_ERR_INVALID_ARGUMENT;
+  }
+  Plan& P = ctx->plan;
+  cudaStream_t s = ctx->stream;
+  const int NC = ncoef(P.opt.p);
+  const int nb = (int)P.nodes.size();
+  // node arrays
+  std::vector<double> nX(3 * nb);
+  std::vector<int> nfb(nb), nfe(nb), cb(nb), ce(nb);
+  for (int i = 0; i < nb; ++i) {
+    for (int a = 0; a < 3; ++a) nX[3 * i + a] = P.nodes[i].X[a];
+    nfb[i] = P.nodes[i].fb;
+    nfe[i] = P.nodes[i].fe;
+    cb[i] = P.nodes[i].child_begin;
+    ce[i] = P.nodes[i].child_end;
+  }
+  // parents per level (non-empty nodes with children)
+  std::vector<int> lp;
+  ctx->level_parent_off.assign(1, 0);
+  for (int l = 0; l < (int)P.level_nodes.size(); ++l) {
+    for (int i : P.level_nodes[l])
+      if (P.nodes[i].child_end > P.nodes[i].child_begin) lp.push_back(i);
+    ctx->level_parent_off.push_back((int)lp.size());
+  }
+  std::vector<int> mt;
+  for (int i = 0; i < nb; ++i)
+    if (!P.nodes[i].empty() && P.m2l_off[i + 1] > P.m2l_off[i]) mt.push_back(i);
+  ctx->n_m2l_targets = (int)mt.size();
+  std::vector<NearBlockDev> bd(P.blocks.size());
+  ctx->max_ntgt = 1;
+  int max_ndof = 1;
+  for (size_t i = 0; i < P.blocks.size(); ++i) {
+    const auto& b = P.blocks[i];
+    bd[i].w_off = b.w_off;
+    bd[i].node = b.node;
+    bd[i].dof_off = b.dof_off;
+    bd[i].ndof = b.ndof;
+    bd[i].tgt_off = b.tgt_off;
+    bd[i].ntgt = b.ntgt;
+    bd[i].rng_off = b.rng_off;
+    bd[i].nrng = b.nrng;
+    ctx->max_ntgt = std::max(ctx->max_ntgt, b.ntgt);
+    max_ndof = std::max(max_ndof, b.ndof);
+  }
+  // shared memory budget of k_targets: chunk of (phi, phin) + per-target sums
+  const int smem_cap = 160 * 1024;
+  if (ctx->max_ntgt * 16 > smem_cap / 2) {
+    ctx->err = "too many targets in one bucket";
+    return BEM_ERR_UNSUPPORTED;
+  }
+  ctx->chunk = std::min(max_ndof, (smem_cap - ctx->max_ntgt * 16) / 16);
+  configure_targets_smem(P.opt.p, (ctx->chunk + ctx->max_ntgt) * 16);
+
+  CK(ctx->Xs.upload(P.Xs, s));
+  CK(ctx->e_q.upload(P.e_q, s));
+  CK(ctx->e_W.upload(P.e_W, s));
+  CK(ctx->e_n.upload(P.e_n, s));
+  CK(ctx->e_near.upload(P.e_near, s));
+  CK(ctx->e_dof.upload(P.e_dof, s));
+  CK(ctx->e_vtx.upload(P.e_vtx, s));
+  CK(ctx->node_X.upload(nX, s));
+  CK(ctx->node_fb.upload(nfb, s));
+  CK(ctx->node_fe.upload(nfe, s));
+  CK(ctx->child_begin.upload(cb, s));
+  CK(ctx->child_end.upload(ce, s));
+  CK(ctx->node_children.upload(P.node_children, s));
+  CK(ctx->leaves.upload(P.leaves, s));
+  CK(ctx->level_parents.upload(lp, s));
+  CK(ctx->m2l_targets.upload(mt, s));
+  CK(ctx->m2l_off.upload(P.m2l_off, s));
+  CK(ctx->m2l_src.upload(P.m2l_src, s));
+  CK(ctx->nb_dofs.upload(P.nb_dofs, s));
+  CK(ctx->nb_targets.upload(P.nb_targets, s));
+  CK(ctx->nb_ranges.upload(P.nb_ranges, s));
+  CK(ctx->dof_inc_off.upload(P.dof_inc_off, s));
+  CK(ctx->dof_inc.upload(P.dof_inc, s));
+  CK(ctx->point_dof_off.upload(P.point_dof_off, s));
+  CK(ctx->point_dof.upload(P.point_dof, s));
+  CK(ctx->dof_kind.upload(P.dof_kind, s));
+  CK(ctx->dof_point.upload(P.dof_point, s));
+  CK(ctx->blocks.upload(bd, s));
+  CK(ctx->M.alloc((size_t)nb * 2 * NC));
+  CK(ctx->L.alloc((size_t)nb * 2 * NC));
+  CK(cudaMemsetAsync(ctx->M.p, 0, sizeof(double2) * ctx->M.n, s));
+  CK(ctx->WG.alloc(std::max<int64_t>(P.nnz, 1)));
+  CK(ctx->WGn.alloc(std::max<int64_t>(P.nnz, 1)));
+  const int N = P.ndof;
+  CK(ctx->phi.alloc(N));
+  CK(ctx->phin.alloc(N));
+  CK(ctx->known_s.alloc(N));
+  CK(ctx->rows.alloc(N));
+  CK(ctx->diag.alloc(N));
+  CK(ctx->GPhin.alloc(P.np));
+  CK(ctx->GnPhi.alloc(P.np));
+  CK(ctx->mv_in.alloc(N));
+  CK(ctx->mv_out.alloc(N));
+  CK(cudaMemsetAsync(ctx->GPhin.p, 0, sizeof(double) * P.np, s));
+  CK(cudaMemsetAsync(ctx->GnPhi.p, 0, sizeof(double) * P.np, s));
+
+  // near-field weights
+  NearArgs na;
+  na.n_blocks = (int)P.blocks.size();
+  na.blocks = ctx->blocks.p;
+  na.nb_dofs = ctx->nb_dofs.p;
+  na.nb_targets = ctx->nb_targets.p;
+  na.nb_ranges = ctx->nb_ranges.p;
+  na.dof_inc_off = ctx->dof_inc_off.p;
+  na.dof_inc = ctx->dof_inc.p;
+  na.Xs = ctx->Xs.p;
+  na.e_vtx = ctx->e_vtx.p;
+  na.e_near = ctx->e_near.p;
+  na.near_region = P.near_region;
+  na.WG = ctx->WG.p;
+  na.WGn = ctx->WGn.p;
+  launch_near_weights(na, s);
+  CK(cudaGetLastError());
+  // rigid-mode diagonal (BEM_solveBVP_GMRES_FMM.hpp:2661-2716)
+  launch_densities(N, 2, nullptr, nullptr, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, s);
+  run_fmm(ctx, nullptr, ctx->GPhin.p, ctx->GnPhi.p);
+  launch_diag(N, ctx->dof_point.p, ctx->GnPhi.p, ctx->diag.p, s);
+  CK(cudaGetLastError());
+  int rc = build_graph(ctx);
+  if (rc != BEM_OK) return rc;
+  CK(cudaStreamSynchronize(s));
+  ctx->time_setup = now_s() - t0;
+  ctx->ready = true;
+  return BEM_OK;
+}
+
+int bem_gpu_apply(bem_gpu_ctx* ctx, const double* phi, const double* phin, double* Av) {
+  if (!ctx || !phi || !phin || !Av) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  CK(cudaSetDevice(ctx->opts.device));
+  const int N = ctx->plan.ndof;
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->phi.p, phi, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->phin.p, phin, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  run_fmm(ctx, ctx->rows.p, nullptr, nullptr);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(Av, ctx->rows.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return BEM_OK;
+}
+
+int bem_gpu_point_integrals(bem_gpu_ctx* ctx, const double* phi, const double* phin, double* GPhin, double* GnPhi) {
+  if (!ctx || !phi || !phin || !GPhin || !GnPhi) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  CK(cudaSetDevice(ctx->opts.device));
+  const int N = ctx->plan.ndof;
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->phi.p, phi, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->phin.p, phin, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(ctx->GPhin.p, 0, sizeof(double) * ctx->plan.np, s));
+  CK(cudaMemsetAsync(ctx->GnPhi.p, 0, sizeof(double) * ctx->plan.np, s));
+  run_fmm(ctx, nullptr, ctx->GPhin.p, ctx->GnPhi.p);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(GPhin, ctx->GPhin.p, sizeof(double) * ctx->plan.np, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(GnPhi, ctx->GnPhi.p, sizeof(double) * ctx->plan.np, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return BEM_OK;
+}
+
+int bem_gpu_matvec_device(bem_gpu_ctx* ctx, const double* d_x, double* d_y) {
+  if (!ctx || !d_x || !d_y) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  const int N = ctx->plan.ndof;
+  cudaStream_t s = ctx->stream;
+  if (d_x != ctx->mv_in.p) CK(cudaMemcpyAsync(ctx->mv_in.p, d_x, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+  CK(cudaGraphLaunch(ctx->graph_exec, s));
+  if (d_y != ctx->mv_out.p) CK(cudaMemcpyAsync(d_y, ctx->mv_out.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+  return BEM_OK;
+}
+
+int bem_gpu_get_diag(bem_gpu_ctx* ctx, double* diag) {
+  if (!ctx || !diag) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  CK(cudaMemcpyAsync(diag, ctx->diag.p, sizeof(double) * ctx->plan.ndof, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return BEM_OK;
+}
+
+double bem_gpu_scale_factor(const bem_gpu_ctx* ctx) { return ctx ? ctx->plan.L : 0.0; }
+
+int bem_gpu_near_row(bem_gpu_ctx* ctx, int32_t point, int32_t cap, int32_t* dof, double* wG, double* wGn) {
+  if (!ctx || point < 0 || point >= ctx->plan.np || cap < 0) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  const Plan& P = ctx->plan;
+  const int bi = P.block_of_point[point];
+  if (bi < 0) return 0;
+  const auto& b = P.blocks[bi];
+  const int n = std::min(cap, b.ndof);
+  if (n > 0) {
+    if (!dof || !wG || !wGn) return BEM_ERR_INVALID_ARGUMENT;
+    std::memcpy(dof, &P.nb_dofs[b.dof_off], sizeof(int32_t) * n);
+    const int64_t off = b.w_off + (int64_t)P.row_of_point[point] * b.ndof;
+    CK(cudaMemcpyAsync(wG, ctx->WG.p + off, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(wGn, ctx->WGn.p + off, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  return b.ndof;
+}
+
+int bem_gpu_face_leaf(bem_gpu_ctx* ctx, int32_t* level, double* corner) {
+  if (!ctx || !level || !corner) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  const Plan& P = ctx->plan;
+  for (int f = 0; f < P.nf; ++f) {
+    level[f] = -1;
+    corner[3 * f] = corner[3 * f + 1] = corner[3 * f + 2] = 0.0;
+    const int s = P.pos_of_face[f];
+    if (s < 0) continue;
+    const int o = P.owner_of_pos[s];
+    if (o < 0 || P.nodes[o].child_end > P.nodes[o].child_begin) continue;
+    level[f] = P.nodes[o].level;
+    for (int a = 0; a < 3; ++a) corner[3 * f + a] = P.nodes[o].lo[a];
+  }
+  return BEM_OK;
+}
+
+int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out) {
+  if (!ctx || !out) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  const Plan& P = ctx->plan;
+  int64_t nodes = 0;
+  int depth = 0;
+  for (size_t l = 0; l < P.level_nodes.size(); ++l) {
+    nodes += (int64_t)P.level_nodes[l].size();
+    if (!P.level_nodes[l].empty()) depth = (int)l;
+  }
+  out[0] = nodes;
+  out[1] = (int64_t)P.leaves.size();
+  out[2] = depth;
+  out[3] = P.n_added;
+  out[4] = P.m2l_pairs;
+  out[5] = P.near_pairs;
+  out[6] = P.nnz;
+  out[7] = (int64_t)P.blocks.size();
+  return BEM_OK;
+}
+
+int bem_plan_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* d, int32_t* face_level, double* face_corner, int64_t* stats) {
+  if (!opts || !d) return BEM_ERR_INVALID_ARGUMENT;
+  PlanOptions po;
+  po.p = opts->expansion_order;
+  po.theta = opts->mac_theta;
+  po.leaf_max = opts->leaf_max_elements;
+  po.max_level = opts->max_level;
+  Plan P;
+  if (!build_plan(P, po, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face, d->dof_kind,
+                  d->face_dof))
+    return BEM_ERR_INVALID_ARGUMENT;
+  if (face_level && face_corner)
+    for (int f = 0; f < P.nf; ++f) {
+      face_level[f] = -1;
+      face_corner[3 * f] = face_corner[3 * f + 1] = face_corner[3 * f + 2] = 0.0;
+      const int s = P.pos_of_face[f];
+      if (s < 0) continue;
+      const int o = P.owner_of_pos[s];
+      if (o < 0 || P.nodes[o].child_end > P.nodes[o].child_begin) continue;
+      face_level[f] = P.nodes[o].level;
+      for (int a = 0; a < 3; ++a) face_corner[3 * f + a] = P.nodes[o].lo[a];
+    }
+  if (stats) {
+    int64_t nodes = 0;
+    int depth = 0;
+    for (size_t l = 0; l < P.level_nodes.size(); ++l) {
+      nodes += (int64_t)P.level_nodes[l].size();
+      if (!P.level_nodes[l].empty()) depth = (int)l;
+    }
+    stats[0] = nodes;
+    stats[1] = (int64_t)P.leaves.size();
+    stats[2] = depth;
+    stats[3] = P.n_added;
+    stats[4] = P.m2l_pairs;
+    stats[5] = P.near_pairs;
+    stats[6] = P.nnz;
+    stats[7] = (int64_t)P.blocks.size();
+  }
+  return BEM_OK;
+}
+
+// GMRES with the reference's driver logic (run_gmres, BEM_solveBVP_GMRES_FMM.hpp:2275-2355):
+// single Arnoldi cycle with incremental Givens QR; once the estimate is within 10*tol the
+// true residual is checked every step; six failed checks end the cycle and GMRES restarts
+// from the current iterate.  Orthogonalisation is classical Gram-Schmidt applied twice
+// (the reference uses one pass of modified Gram-Schmidt; both are FP64-stable here).
+int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, double* out_phi, double* out_phin, bem_gpu_stats* stats) {
+  if (!ctx || !known || !out_phi || !out_phin) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  CK(cudaSetDevice(ctx->opts.device));
+  const double t0 = now_s();
+  const Plan& P = ctx->plan;
+  const int N = P.ndof;
+  cudaStream_t s = ctx->stream;
+  double tol = ctx->opts.tol;
+  const int max_iter = ctx->opts.max_iter;
+  for (int i = 0; i < N; ++i)
+    if (!std::isfinite(known[i])) {
+      ctx->err = "non-finite boundary value";
+      return BEM_ERR_NAN;
+    }
+  // known values in scaled units (copyToFMM: Neumann phin x L)
+  std::vector<double> ks(N);
+  for (int i = 0; i < N; ++i) ks[i] = (P.dof_kind[i] == 0) ? known[i] : known[i] * P.L;
+  CK(cudaMemcpyAsync(ctx->known_s.p, ks.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  const int cols = max_iter + 2;
+  if (ctx->V_cols < cols || ctx->V.n < (size_t)cols * N) {
+    CK(ctx->V.alloc((size_t)cols * N));
+    ctx->V_cols = cols;
+  }
+  if (ctx->w.n < (size_t)N) {
+    CK(ctx->w.alloc(N));
+    CK(ctx->xdev.alloc(N));
+    CK(ctx->bdev.alloc(N));
+    CK(ctx->rdev.alloc(N));
+  }
+  CK(ctx->hdev.alloc((size_t)3 * cols + 8));
+  CK(ctx->ydev.alloc(cols));
+  CK(ctx->partial.alloc((size_t)mdot_blocks(N) * cols));
+  int matvecs = 0;
+  // b = -(A*0 - b) with corner rows replaced by the point's phi (:2025-2047)
+  launch_densities(N, 1, nullptr, ctx->known_s.p, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, s);
+  run_fmm(ctx, ctx->rows.p, nullptr, nullptr);
+  ++matvecs;
+  std::vector<double> b(N);
+  CK(cudaMemcpyAsync(b.data(), ctx->rows.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int i = 0; i < N; ++i) {
+    b[i] = -b[i];
+    if (P.dof_kind[i] == 2) b[i] = (P.corner_src_dof[i] >= 0) ? known[P.corner_src_dof[i]] : 0.0;
+  }
+  CK(cudaMemcpyAsync(ctx->bdev.p, b.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  if (ctx->opts.tol_relative) {
+    double bn = 0.0;
+    for (int i = 0; i < N; ++i) bn = std::fma(b[i], b[i], bn);
+    tol *= std::sqrt(bn);
+  }
+  if (x0)
+    CK(cudaMemcpyAsync(ctx->xdev.p, x0, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  else
+    CK(cudaMemsetAsync(ctx->xdev.p, 0, sizeof(double) * N, s));
+
+  auto matvec = [&](const double* din, double* dout) -> int {
+    ++matvecs;
+    return bem_gpu_matvec_device(ctx, din, dout);
+  };
+  auto norm_of = [&](const double* v, double* out) -> int {
+    launch_mdot(v, N, 1, v, N, ctx->partial.p, ctx->hdev.p, s);
+    CK(cudaMemcpyAsync(out, ctx->hdev.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    *out = std::sqrt(*out);
+    return BEM_OK;
+  };
+  int iters = 0, rc = BEM_OK;
+  double r_true = 1e300, err = 1e300;
+  std::vector<double> hh(2 * cols + 2);
+  while (iters < max_iter && r_true > tol) {
+    const int k_cycle_max = std::min(100, max_iter - iters);
+    // r0 = b - A x
+    if ((rc = matvec(ctx->xdev.p, ctx->rdev.p)) != BEM_OK) return rc;
+    launch_axpby(N, 1.0, ctx->bdev.p, -1.0, ctx->rdev.p, s);  // r = b - r
+    double beta = 0.0;
+    if ((rc = norm_of(ctx->rdev.p, &beta)) != BEM_OK) return rc;
+    if (!std::isfinite(beta)) {
+      ctx->err = "non-finite residual";
+      return BEM_ERR_NAN;
+    }
+    if (beta == 0.0) {
+      r_true = 0.0;
+      err = 0.0;
+      break;
+    }
+    launch_axpby(N, 1.0 / beta, ctx->rdev.p, 0.0, ctx->V.p, s);
+    std::vector<double> cs, sn, g{beta};
+    std::vector<std::vector<double>> Rc;
+    int n = 0;  // basis vectors beyond V[0] added in this cycle
+    auto add_basis = [&]() -> int {
+      double* vk = ctx->V.p + (size_t)n * N;
+      double* vn = ctx->V.p + (size_t)(n + 1) * N;
+      int r;
+      if ((r = matvec(vk, ctx->w.p)) != BEM_OK) return r;
+      const int k = n + 1;
+      double* h1 = ctx->hdev.p;
+      double* h2 = ctx->hdev.p + cols;
+      double* hn = ctx->hdev.p + 2 * cols;
+      launch_mdot(ctx->V.p, N, k, ctx->w.p, N, ctx->partial.p, h1, s);
+      launch_maxpy(ctx->V.p, N, k, h1, ctx->w.p, N, s);
+      launch_mdot(ctx->V.p, N, k, ctx->w.p, N, ctx->partial.p, h2, s);
+      launch_maxpy(ctx->V.p, N, k, h2, ctx->w.p, N, s);
+      launch_mdot(ctx->w.p, N, 1, ctx->w.p, N, ctx->partial.p, hn, s);
+      CK(cudaMemcpyAsync(hh.data(), h1, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(hh.data() + cols, h2, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+      double hn2 = 0.0;
+      CK(cudaMemcpyAsync(&hn2, hn, sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      std::vector<double> hcol(k + 1);
+      for (int i = 0; i < k; ++i) hcol[i] = hh[i] + hh[cols + i];
+      hcol[k] = std::sqrt(hn2);
+      if (!std::isfinite(hcol[k])) {
+        ctx->err = "non-finite Arnoldi vector";
+        return BEM_ERR_NAN;
+      }
+      launch_axpby(N, hcol[k] > 0 ? 1.0 / hcol[k] : 0.0, ctx->w.p, 0.0, vn, s);
+      for (int i = 0; i < k - 1; ++i) {
+        const double t = std::fma(cs[i], hcol[i], sn[i] * hcol[i + 1]);
+        hcol[i + 1] = std::fma(cs[i], hcol[i + 1], -sn[i] * hcol[i]);
+        hcol[i] = t;
+      }
+      const double a = hcol[k - 1], bb = hcol[k];
+      const double rr = std::hypot(a, bb);
+      double c = 1.0, sv = 0.0;
+      if (rr != 0.0) {
+        c = a / rr;
+        sv = bb / rr;
+      }
+      cs.push_back(c);
+      sn.push_back(sv);
+      {
+        const double t = std::fma(c, hcol[k - 1], sv * hcol[k]);
+        hcol[k] = std::fma(c, hcol[k], -sv * hcol[k - 1]);
+        hcol[k - 1] = t;
+      }
+      g.push_back(0.0);
+      {
+        const double t = std::fma(c, g[k - 1], sv * g[k]);
+        g[k] = std::fma(c, g[k], -sv * g[k - 1]);
+        g[k - 1] = t;
+      }
+      Rc.push_back(hcol);
+      err = std::abs(g.back());
+      ++n;
+      return BEM_OK;
+    };
+    auto update_x = [&]() -> int {
+      const int k = (int)Rc.size();
+      std::vector<double> y(k, 0.0);
+      for (int i = k - 1; i >= 0; --i) {
+        double sum = g[i];
+        for (int j = i + 1; j < k; ++j) sum -= Rc[j][i] * y[j];
+        y[i] = sum / Rc[i][i];
+      }
+      for (auto& v : y) v = -v;  // maxpy subtracts
+      CK(cudaMemcpyAsync(ctx->ydev.p, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
+      launch_maxpy(ctx->V.p, N, k, ctx->ydev.p, ctx->xdev.p, N, s);
+      return BEM_OK;
+    };
+    auto true_res = [&](double* out) -> int {
+      int r;
+      if ((r = matvec(ctx->xdev.p, ctx->rdev.p)) != BEM_OK) return r;
+      launch_axpby(N, -1.0, ctx->bdev.p, 1.0, ctx->rdev.p, s);
+      return norm_of(ctx->rdev.p, out);
+    };
+    // x_base is committed into xdev only when the solution is updated; keep a copy
+    DBuf<double> xb;
+    CK(xb.alloc(N));
+    CK(cudaMemcpyAsync(xb.p, ctx->xdev.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    auto update_from_base = [&]() -> int {
+      CK(cudaMemcpyAsync(ctx->xdev.p, xb.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+      return update_x();
+    };
+    if ((rc = add_basis()) != BEM_OK) return rc;
+    iters += 1;
+    int sat = 0;
+    while (true) {
+      if ((rc = add_basis()) != BEM_OK) return rc;
+      ++iters;
+      if (err <= tol * 10.) {
+        if ((rc = update_from_base()) != BEM_OK) return rc;
+        if ((rc = true_res(&r_true)) != BEM_OK) return rc;
+        if (r_true <= tol) break;
+        if (sat++ >= 5) break;
+      }
+      if (iters >= max_iter && (int)Rc.size() >= k_cycle_max) {
+        if ((rc = update_from_base()) != BEM_OK) return rc;
+        if (err <= tol * 10.) {
+          if ((rc = true_res(&r_true)) != BEM_OK) return rc;
+        } else
+          r_true = err;
+        break;
+      }
+      if (n + 2 > ctx->V_cols) {  // basis full: restart from the current iterate
+        if ((rc = update_from_base()) != BEM_OK) return rc;
+        break;
+      }
+    }
+  }
+  std::vector<double> x(N);
+  CK(cudaMemcpyAsync(x.data(), ctx->xdev.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  bool finite = true;
+  for (int i = 0; i < N; ++i) {
+    finite = finite && std::isfinite(x[i]);
+    if (P.dof_kind[i] == 0) {  // unscale phin (BEM_solveBVP_GMRES_FMM.hpp:3462-3486)
+      out_phi[i] = known[i];
+      out_phin[i] = x[i] / P.L;
+    } else {
+      out_phi[i] = x[i];
+      out_phin[i] = known[i];
+    }
+  }
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->iterations = iters;
+    stats->converged = r_true <= tol;
+    stats->residual = r_true;
+    stats->residual_est = err;
+    stats->time_setup_s = ctx->time_setup;
+    stats->time_solve_s = now_s() - t0;
+    stats->nnz_near = P.nnz;
+    stats->m2l_pairs = P.m2l_pairs;
+    int64_t nodes = 0;
+    for (auto& lv : P.level_nodes) nodes += (int64_t)lv.size();
+    stats->n_nodes = (int)nodes;
+    stats->n_leaves = (int)P.leaves.size();
+    stats->matvecs = matvecs;
+  }
+  if (!finite) {
+    ctx->err = "non-finite solution";
+    return BEM_ERR_NAN;
+  }
+  return (r_true <= tol) ? BEM_OK : BEM_ERR_NOT_CONVERGED;
+}
+
+int bem_gpu_solve_bvp(bem_gpu_ctx* ctx, const bem_bvp_desc* desc, const double* known, const double* x0, double* out_phi, double* out_phin,
+                      bem_gpu_stats* stats) {
+  int rc = bem_gpu_setup(ctx, desc);
+  if (rc != BEM_OK) return rc;
+  return bem_gpu_solve(ctx, known, x0, out_phi, out_phin, stats);
+}
+
+int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms) {
+  if (!ctx || !stage_ms || repeats < 1) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  cudaStream_t s = ctx->stream;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, s));
+  for (int r = 0; r < repeats; ++r) CK(cudaGraphLaunch(ctx->graph_exec, s));
+  CK(cudaEventRecord(e1, s));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (int i = 0; i < 6; ++i) stage_ms[i] = 0.0;
+  stage_ms[5] = ms / repeats;
+  return BEM_OK;
+}
+
+}  // extern "C"

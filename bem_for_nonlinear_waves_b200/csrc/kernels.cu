@@ -1,0 +1,725 @@
+// FP64 FMM mat-vec and near-field kernels for sm_100a.
+//
+// Per mat-vec (return_A_dot_v, bem/BEM_solveBVP_GMRES_FMM.hpp:2124-2155):
+//   k_densities   per-DOF phi/phin from the unknown vector (setUnknowns/setKnowns, :1142-1176)
+//   k_p2m         leaf multipoles from the 6 Dunavant points of every element (moments.hpp:307-368)
+//   k_m2m         one launch per level, bottom-up (moments.hpp:419-436, 912-915)
+//   k_m2l         every M2L pair of every level in one launch (moments.hpp:732-764)
+//   k_l2l         one launch per level, top-down (moments.hpp:869-884, 925-929)
+//   k_targets     near-field block SpMV + L2P + BIE rows (compute_Ax_minus_b, :34-158)
+// Set-up:
+//   k_near_weights  near-field quadrature into per-block dense rows (target4FMM::setDirectIntegration,
+//                   lib_multipole_expansion.hpp:1180-1271 with fill_direct_linear / fill_nonadj_linear,
+//                   BEM_solveBVP_GMRES_FMM.hpp:1824-1891)
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fmm_math.cuh"
+#include "kernels.cuh"
+
+namespace bemb200 {
+
+__constant__ double c_dv[6][4];   // Dunavant 6-point rule: b0, b1, b2, w
+__constant__ double c_gw[25][3];  // 5x5 Gauss-Legendre on [0,1]^2: t0, t1, w
+
+void upload_quadrature(const double dv[6][4], const double gw[25][3], cudaStream_t s) {
+  cudaMemcpyToSymbolAsync(c_dv, dv, sizeof(double) * 24, 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(c_gw, gw, sizeof(double) * 75, 0, cudaMemcpyHostToDevice, s);
+}
+
+// ---------------------------------------------------------------------------
+// per-DOF phi / phin.  mode 0: unknowns = x, knowns = 0 (A.x);  mode 1: unknowns = 0,
+// knowns = known (right-hand side);  mode 2: phi = 1, phin = 0 (rigid mode);  mode 3:
+// phi/phin given directly (x = phi, known = phin).
+__global__ void k_densities(int n, int mode, const double* __restrict__ x, const double* __restrict__ known, const int* __restrict__ kind,
+                            double* __restrict__ phi, double* __restrict__ phin) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const bool dir = kind[i] == 0;
+    double a, b;
+    if (mode == 0) {
+      a = dir ? 0.0 : x[i];
+      b = dir ? x[i] : 0.0;
+    } else if (mode == 1) {
+      a = dir ? known[i] : 0.0;
+      b = dir ? 0.0 : known[i];
+    } else if (mode == 2) {
+      a = 1.0;
+      b = 0.0;
+    } else {
+      a = x[i];
+      b = known[i];
+    }
+    phi[i] = a;
+    phin[i] = b;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// P2M: one block (4 warps) per leaf; each half-warp carries one P2M point, lane m its
+// column m of F_n^m, advanced degree by degree in lock-step so that the gradient
+// terms F_{n-1}^{m-1}, F_{n-1}^{m+1} come from the neighbouring lanes by shuffles.
+template <int P>
+__global__ void __launch_bounds__(128) k_p2m(const int* __restrict__ leaves, const int* __restrict__ node_fb, const int* __restrict__ node_fe,
+                                             const double* __restrict__ node_X, const double* __restrict__ e_q,
+                                             const double* __restrict__ e_W, const double* __restrict__ e_n,
+                                             const int* __restrict__ e_dof, const double* __restrict__ phi,
+                                             const double* __restrict__ phin, double2* __restrict__ M) {
+  constexpr int NC = ncoef(P);
+  static_assert(P <= 14, "column lanes live in a half warp");
+  __shared__ double2 red[4][2][NC];
+  const int leaf = leaves[blockIdx.x];
+  const int fb = node_fb[leaf], fe = node_fe[leaf];
+  const double cx = node_X[3 * leaf], cy = node_X[3 * leaf + 1], cz = node_X[3 * leaf + 2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int half = lane >> 4, m = lane & 15;
+  double2 accM[P + 1], accD[P + 1];
+#pragma unroll
+  for (int n = 0; n <= P; ++n) {
+    accM[n] = make_double2(0.0, 0.0);
+    accD[n] = make_double2(0.0, 0.0);
+  }
+  const int npts = (fe - fb) * 6;
+  for (int base = 0; base < npts; base += 8) {
+    const int pt = base + warp * 2 + half;
+    double x = 0, y = 0, z = 0, wphi = 0, wphin = 0, nx = 0, ny = 0, nz = 0;
+    if (pt < npts) {
+      const int s = fb + pt / 6, k = pt % 6;
+      x = e_q[s * 18 + 3 * k] - cx;
+      y = e_q[s * 18 + 3 * k + 1] - cy;
+      z = e_q[s * 18 + 3 * k + 2] - cz;
+      const int d0 = e_dof[3 * s], d1 = e_dof[3 * s + 1], d2 = e_dof[3 * s + 2];
+      const double W = e_W[s * 6 + k];
+      // closure get_weighted_source_densities (BEM_solveBVP_GMRES_FMM.hpp:1915-1922)
+      wphi = W * (c_dv[k][0] * phi[d0] + c_dv[k][1] * phi[d1] + c_dv[k][2] * phi[d2]);
+      wphin = W * (c_dv[k][0] * phin[d0] + c_dv[k][1] * phin[d1] + c_dv[k][2] * phin[d2]);
+      nx = e_n[3 * s];
+      ny = e_n[3 * s + 1];
+      nz = e_n[3 * s + 2];
+    }
+    const double r2 = x * x + y * y + z * z;
+    double2 diag = make_double2(1.0, 0.0);
+    for (int k = 1; k <= m && k <= P; ++k) diag = cscale(cmul(diag, make_double2(x, y)), 1.0 / (2.0 * k));
+    double2 prev = make_double2(0.0, 0.0), prev2 = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int n = 0; n <= P; ++n) {
+      double2 cur;
+      if (n < m)
+        cur = make_double2(0.0, 0.0);
+      else if (n == m)
+        cur = diag;
+      else {
+        const double inv = 1.0 / double(n * n - m * m);
+        cur = make_double2(((2 * n - 1) * z * prev.x - r2 * prev2.x) * inv, ((2 * n - 1) * z * prev.y - r2 * prev2.y) * inv);
+      }
+      double2 up = shfl_up2(prev, 1, 16);    // F_{n-1}^{m-1}
+      double2 dn = shfl_down2(prev, 1, 16);  // F_{n-1}^{m+1}
+      if (m == 0) up = make_double2(-dn.x, dn.y);  // F^{-1} = -conj(F^{1})
+      if (m == 15) dn = make_double2(0.0, 0.0);
+      // g = nu_z F^m + 1/2 (nu_x + i nu_y) F^{m-1} - 1/2 (nu_x - i nu_y) F^{m+1}
+      double2 g = cscale(prev, nz);
+      g = cadd(g, cscale(cmul(make_double2(nx, ny), up), 0.5));
+      g = csub(g, cscale(cmul(make_double2(nx, -ny), dn), 0.5));
+      if (n >= m) {
+        accM[n].x += wphin * cur.x;
+        accM[n].y -= wphin * cur.y;
+        accD[n].x += wphi * g.x;
+        accD[n].y -= wphi * g.y;
+      }
+      prev2 = prev;
+      prev = cur;
+    }
+  }
+#pragma unroll
+  for (int n = 0; n <= P; ++n) {
+    accM[n] = cadd(accM[n], shfl_down2(accM[n], 16, 32));
+    accD[n] = cadd(accD[n], shfl_down2(accD[n], 16, 32));
+  }
+  if (half == 0 && m <= P) {
+#pragma unroll
+    for (int n = 0; n <= P; ++n)
+      if (n >= m) {
+        red[warp][0][cidx(n, m)] = accM[n];
+        red[warp][1][cidx(n, m)] = accD[n];
+      }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 2 * NC; t += blockDim.x) {
+    const int d = t / NC, c = t % NC;
+    double2 s = red[0][d][c];
+    s = cadd(s, red[1][d][c]);
+    s = cadd(s, red[2][d][c]);
+    s = cadd(s, red[3][d][c]);
+    M[(size_t)leaf * 2 * NC + t] = s;
+  }
+}
+
+// full (negative-order) table fill from one lane per column
+template <int Q>
+__device__ __forceinline__ void F_full_column(int m, double x, double y, double z, double2* T /*(Q+1)^2*/) {
+  if (m > Q) return;
+  const double r2 = x * x + y * y + z * z;
+  double2 f = make_double2(1.0, 0.0);
+  for (int k = 1; k <= m; ++k) f = cscale(cmul(f, make_double2(x, y)), 1.0 / (2.0 * k));
+  double2 prev = make_double2(0.0, 0.0), cur = f;
+  for (int n = m; n <= Q; ++n) {
+    if (n > m) {
+      const double inv = 1.0 / double(n * n - m * m);
+      double2 nx = make_double2(((2 * n - 1) * z * cur.x - r2 * prev.x) * inv, ((2 * n - 1) * z * cur.y - r2 * prev.y) * inv);
+      prev = cur;
+      cur = nx;
+    }
+    T[n * (n + 1) + m] = cur;
+    if (m > 0) T[n * (n + 1) - m] = (m & 1) ? make_double2(-cur.x, cur.y) : make_double2(cur.x, -cur.y);
+  }
+}
+
+template <int Q>
+__device__ __forceinline__ void S_full_column(int q, double x, double y, double z, double2* T /*(Q+1)^2*/) {
+  if (q > Q) return;
+  const double r2 = x * x + y * y + z * z;
+  const double inv_r2 = 1.0 / r2;
+  double2 s = make_double2(1.0 / sqrt(r2), 0.0);
+  for (int k = 1; k <= q; ++k) s = cscale(cmul(s, make_double2(x, y)), (2.0 * k - 1.0) * inv_r2);
+  double2 prev = make_double2(0.0, 0.0), cur = s;
+  for (int l = q; l <= Q; ++l) {
+    if (l > q) {
+      const double a = (2 * l - 1) * z;
+      const double b = double((l - 1 + q) * (l - 1 - q));
+      double2 nx = make_double2((a * cur.x - b * prev.x) * inv_r2, (a * cur.y - b * prev.y) * inv_r2);
+      prev = cur;
+      cur = nx;
+    }
+    T[l * (l + 1) + q] = cur;
+    if (q > 0) T[l * (l + 1) - q] = (q & 1) ? make_double2(-cur.x, cur.y) : make_double2(cur.x, -cur.y);
+  }
+}
+
+// expand half-stored coefficients [2][NC] into full [2][(P+1)^2]
+template <int P>
+__device__ __forceinline__ void expand_full(const double2* __restrict__ src, double2* dst) {
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
+  for (int t = threadIdx.x; t < 2 * NF; t += blockDim.x) {
+    const int d = t / NF, i = t % NF;
+    int n = 0;
+    while ((n + 1) * (n + 1) <= i) ++n;
+    const int m = i - n * (n + 1);
+    double2 v = src[d * NC + cidx(n, m < 0 ? -m : m)];
+    if (m < 0) v = ((-m) & 1) ? make_double2(-v.x, v.y) : make_double2(v.x, -v.y);
+    dst[t] = v;
+  }
+}
+
+__device__ __forceinline__ void decode_nm(int t, int& n, int& m) {
+  n = 0;
+  while ((n + 1) * (n + 2) / 2 <= t) ++n;
+  m = t - n * (n + 1) / 2;
+}
+
+// ---------------------------------------------------------------------------
+// M2M: one block per parent, children in turn; thread per output coefficient.
+template <int P>
+__global__ void k_m2m(const int* __restrict__ parents, const int* __restrict__ child_begin, const int* __restrict__ child_end,
+                      const int* __restrict__ node_children, const double* __restrict__ node_X, double2* __restrict__ M) {
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
+  __shared__ double2 sF[NF];
+  __shared__ double2 sM[2 * NF];
+  const int par = parents[blockIdx.x];
+  const int t = threadIdx.x;
+  int n = 0, m = 0;
+  if (t < NC) decode_nm(t, n, m);
+  double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
+  for (int ci = child_begin[par]; ci < child_end[par]; ++ci) {
+    const int c = node_children[ci];
+    __syncthreads();
+    if (t < 32)
+      F_full_column<P>(t, node_X[3 * c] - node_X[3 * par], node_X[3 * c + 1] - node_X[3 * par + 1],
+                       node_X[3 * c + 2] - node_X[3 * par + 2], sF);
+    expand_full<P>(M + (size_t)c * 2 * NC, sM);
+    __syncthreads();
+    if (t < NC) {
+      for (int n1 = 0; n1 <= n; ++n1) {
+        const int n2 = n - n1;
+        const int lo = max(-n1, m - n2), hi = min(n1, m + n2);
+        for (int m1 = lo; m1 <= hi; ++m1) {
+          const double2 f = sF[n1 * (n1 + 1) + m1];
+          const int i2 = n2 * (n2 + 1) + (m - m1);
+          const double2 x0 = sM[i2], x1 = sM[NF + i2];
+          // conj(f) * x
+          a0.x += f.x * x0.x + f.y * x0.y;
+          a0.y += f.x * x0.y - f.y * x0.x;
+          a1.x += f.x * x1.x + f.y * x1.y;
+          a1.y += f.x * x1.y - f.y * x1.x;
+        }
+      }
+    }
+  }
+  if (t < NC) {
+    M[(size_t)par * 2 * NC + t] = a0;
+    M[(size_t)par * 2 * NC + NC + t] = a1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// M2L: one block per target bucket, its whole source list; thread per output (n, m>=0).
+template <int P>
+__global__ void k_m2l(const int* __restrict__ targets, const int* __restrict__ m2l_off, const int* __restrict__ m2l_src,
+                      const double* __restrict__ node_X, const double2* __restrict__ M, double2* __restrict__ L) {
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), Q = 2 * P, NS = (Q + 1) * (Q + 1);
+  __shared__ double2 sS[NS];
+  __shared__ double2 sM[2 * NF];
+  const int tgt = targets[blockIdx.x];
+  const int t = threadIdx.x;
+  int n = 0, m = 0;
+  if (t < NC) decode_nm(t, n, m);
+  double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
+  const double tx = node_X[3 * tgt], ty = node_X[3 * tgt + 1], tz = node_X[3 * tgt + 2];
+  for (int k = m2l_off[tgt]; k < m2l_off[tgt + 1]; ++k) {
+    const int src = m2l_src[k];
+    __syncthreads();
+    if (t < 32) S_full_column<Q>(t, tx - node_X[3 * src], ty - node_X[3 * src + 1], tz - node_X[3 * src + 2], sS);
+    expand_full<P>(M + (size_t)src * 2 * NC, sM);
+    __syncthreads();
+    if (t < NC) {
+      for (int n1 = 0; n1 <= P; ++n1) {
+        const int l = n + n1;
+        const double2* Srow = sS + l * (l + 1) + m;
+        const double2* M0 = sM + n1 * (n1 + 1);
+        const double2* M1 = sM + NF + n1 * (n1 + 1);
+        for (int m1 = -n1; m1 <= n1; ++m1) {
+          const double2 s = Srow[m1];
+          cfma(a0, s, M0[m1]);
+          cfma(a1, s, M1[m1]);
+        }
+      }
+    }
+  }
+  if (t < NC) {
+    const double sg = (n & 1) ? -1.0 : 1.0;
+    L[(size_t)tgt * 2 * NC + t] = make_double2(sg * a0.x, sg * a0.y);
+    L[(size_t)tgt * 2 * NC + NC + t] = make_double2(sg * a1.x, sg * a1.y);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// L2L: one block per parent; each child gets L'_k^j += sum_{n>=k} L_n^m conj(F_{n-k}^{m-j}).
+template <int P>
+__global__ void k_l2l(const int* __restrict__ parents, const int* __restrict__ child_begin, const int* __restrict__ child_end,
+                      const int* __restrict__ node_children, const double* __restrict__ node_X, double2* __restrict__ L) {
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
+  __shared__ double2 sF[NF];
+  __shared__ double2 sL[2 * NF];
+  const int par = parents[blockIdx.x];
+  const int t = threadIdx.x;
+  int k = 0, j = 0;
+  if (t < NC) decode_nm(t, k, j);
+  expand_full<P>(L + (size_t)par * 2 * NC, sL);
+  for (int ci = child_begin[par]; ci < child_end[par]; ++ci) {
+    const int c = node_children[ci];
+    __syncthreads();
+    if (t < 32)
+      F_full_column<P>(t, node_X[3 * c] - node_X[3 * par], node_X[3 * c + 1] - node_X[3 * par + 1],
+                       node_X[3 * c + 2] - node_X[3 * par + 2], sF);
+    __syncthreads();
+    if (t < NC) {
+      double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
+      for (int n = k; n <= P; ++n) {
+        const int dn = n - k;
+        const int lo = max(-n, j - dn), hi = min(n, j + dn);
+        for (int m = lo; m <= hi; ++m) {
+          const double2 f = sF[dn * (dn + 1) + (m - j)];
+          const double2 x0 = sL[n * (n + 1) + m], x1 = sL[NF + n * (n + 1) + m];
+          // x * conj(f)
+          a0.x += x0.x * f.x + x0.y * f.y;
+          a0.y += x0.y * f.x - x0.x * f.y;
+          a1.x += x1.x * f.x + x1.y * f.y;
+          a1.y += x1.y * f.x - x1.x * f.y;
+        }
+      }
+      double2* dst = L + (size_t)c * 2 * NC;
+      dst[t] = cadd(dst[t], a0);
+      dst[NC + t] = cadd(dst[NC + t], a1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Targets: one block per near block (targets sharing a deepest bucket).  The block
+// stages (phi, phin) of its DOF set in shared memory chunk by chunk, each warp reduces
+// the cached weight rows of its targets, then evaluates L2P and writes the BIE rows.
+template <int P>
+__global__ void __launch_bounds__(128) k_targets(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs,
+                                                 const int* __restrict__ nb_targets, const double* __restrict__ WG,
+                                                 const double* __restrict__ WGn, const double* __restrict__ Xs,
+                                                 const double* __restrict__ node_X, const double2* __restrict__ L,
+                                                 const double* __restrict__ phi, const double* __restrict__ phin,
+                                                 const int* __restrict__ point_dof_off, const int* __restrict__ point_dof,
+                                                 const int* __restrict__ dof_kind, const double* __restrict__ diag,
+                                                 double* __restrict__ rows, double* __restrict__ GPhin_out,
+                                                 double* __restrict__ GnPhi_out, int chunk) {
+  constexpr int NC = ncoef(P);
+  extern __shared__ double2 smem[];
+  double2* xs = smem;                   // [chunk] (phi, phin)
+  double2* accs = smem + chunk;         // [ntgt] near sums (G.phin, Gn.phi)
+  __shared__ double2 sL[2 * NC];
+  const NearBlockDev B = blocks[blockIdx.x];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarp = blockDim.x >> 5;
+  for (int i = threadIdx.x; i < 2 * NC; i += blockDim.x) sL[i] = L[(size_t)B.node * 2 * NC + i];
+  for (int i = threadIdx.x; i < B.ntgt; i += blockDim.x) accs[i] = make_double2(0, 0);
+  for (int c0 = 0; c0 < B.ndof; c0 += chunk) {
+    const int cn = min(chunk, B.ndof - c0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < cn; i += blockDim.x) {
+      const int d = nb_dofs[B.dof_off + c0 + i];
+      xs[i] = make_double2(phi[d], phin[d]);
+    }
+    __syncthreads();
+    for (int tl = warp; tl < B.ntgt; tl += nwarp) {
+      const double* wg = WG + B.w_off + (int64_t)tl * B.ndof + c0;
+      const double* wgn = WGn + B.w_off + (int64_t)tl * B.ndof + c0;
+      double s0 = 0.0, s1 = 0.0;
+      for (int i = lane; i < cn; i += 32) {
+        const double2 v = xs[i];
+        s0 = fma(wg[i], v.y, s0);
+        s1 = fma(wgn[i], v.x, s1);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      }
+      if (lane == 0) {
+        accs[tl].x += s0;
+        accs[tl].y += s1;
+      }
+    }
+  }
+  __syncthreads();
+  const double cx = node_X[3 * B.node], cy = node_X[3 * B.node + 1], cz = node_X[3 * B.node + 2];
+  for (int tl = warp; tl < B.ntgt; tl += nwarp) {
+    const int p = nb_targets[B.tgt_off + tl];
+    const double x = Xs[3 * p] - cx, y = Xs[3 * p + 1] - cy, z = Xs[3 * p + 2] - cz;
+    // L2P: lane m owns column m of F_n^m(x - c)
+    double f0 = 0.0, f1 = 0.0;
+    const int m = lane;
+    if (m <= P) {
+      const double r2 = x * x + y * y + z * z;
+      double2 cur = make_double2(1.0, 0.0);
+      for (int k = 1; k <= m; ++k) cur = cscale(cmul(cur, make_double2(x, y)), 1.0 / (2.0 * k));
+      double2 prev = make_double2(0.0, 0.0);
+      const double w = (m == 0) ? 1.0 : 2.0;
+      for (int n = m; n <= P; ++n) {
+        if (n > m) {
+          const double inv = 1.0 / double(n * n - m * m);
+          double2 nx = make_double2(((2 * n - 1) * z * cur.x - r2 * prev.x) * inv, ((2 * n - 1) * z * cur.y - r2 * prev.y) * inv);
+          prev = cur;
+          cur = nx;
+        }
+        // Re(L conj(F))
+        const double2 l0 = sL[cidx(n, m)], l1 = sL[NC + cidx(n, m)];
+        f0 += w * (l0.x * cur.x + l0.y * cur.y);
+        f1 += w * (l1.x * cur.x + l1.y * cur.y);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      f0 += __shfl_xor_sync(0xffffffffu, f0, o);
+      f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+    }
+    const double GPhin = accs[tl].x + f0, GnPhi = accs[tl].y + f1;
+    if (GPhin_out && lane == 0) {
+      GPhin_out[p] = GPhin;
+      GnPhi_out[p] = GnPhi;
+    }
+    if (rows) {
+      for (int k = point_dof_off[p] + lane; k < point_dof_off[p + 1]; k += 32) {
+        const int i = point_dof[k];
+        rows[i] = (dof_kind[i] == 2) ? phi[i] : GPhin - (GnPhi + diag[i] * phi[i]);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Near-field quadrature (set-up).  One block per near block; one thread per
+// (target, DOF) weight, summing every incident element vertex whose element lies in the
+// block's near element ranges.
+__device__ __forceinline__ double dnorm3(double x, double y, double z) { return sqrt(x * x + y * y + z * z); }
+
+__device__ void elem_vertex_weight(int s, int a, int t, const double* __restrict__ Xs, const int* __restrict__ e_vtx,
+                                   const double* __restrict__ e_near, double near_region, double& wG, double& wGn) {
+  const int v[3] = {e_vtx[3 * s], e_vtx[3 * s + 1], e_vtx[3 * s + 2]};
+  const double J = e_near[8 * s];
+  const double crx = e_near[8 * s + 1], cry = e_near[8 * s + 2], crz = e_near[8 * s + 3];
+  const double xt = Xs[3 * t], yt = Xs[3 * t + 1], zt = Xs[3 * t + 2];
+  double G = 0.0, Gn = 0.0;
+  if (v[0] == t || v[1] == t || v[2] == t) {
+    // fill_direct_linear: rotate so the target is vertex 0; Duffy-collapsed 5x5 rule;
+    // the Gn weight of the element's first vertex is dropped (rigid-mode diagonal)
+    int o = (v[0] == t) ? 0 : (v[1] == t ? 1 : 2);
+    const int r0 = v[o], r1 = v[(o + 1) % 3], r2 = v[(o + 2) % 3];
+    const int ia = (a - o + 3) % 3;  // rotated position of original vertex a
+    const double X0[3] = {Xs[3 * r0], Xs[3 * r0 + 1], Xs[3 * r0 + 2]};
+    const double X1[3] = {Xs[3 * r1], Xs[3 * r1 + 1], Xs[3 * r1 + 2]};
+    const double X2[3] = {Xs[3 * r2], Xs[3 * r2 + 1], Xs[3 * r2 + 2]};
+    for (int g = 0; g < 25; ++g) {
+      const double t0 = c_gw[g][0], t1 = c_gw[g][1], ww = c_gw[g][2];
+      const double N[3] = {t0, t1 * (1. - t0), (t0 - 1.) * (t1 - 1.)};
+      const double Rx = N[0] * X0[0] + N[1] * X1[0] + N[2] * X2[0] - xt;
+      const double Ry = N[0] * X0[1] + N[1] * X1[1] + N[2] * X2[1] - yt;
+      const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
+      const double nr_inv = 1. / dnorm3(Rx, Ry, Rz);
+      const double tmp = ww * (1. - t0) * nr_inv * N[ia];
+      G += J * tmp;
+      Gn += -((Rx * crx + Ry * cry + Rz * crz) * nr_inv) * tmp * nr_inv;
+    }
+    wG = G;
+    wGn = (a == 0) ? 0.0 : Gn;
+    return;
+  }
+  const double X0[3] = {Xs[3 * v[0]], Xs[3 * v[0] + 1], Xs[3 * v[0] + 2]};
+  const double X1[3] = {Xs[3 * v[1]], Xs[3 * v[1] + 1], Xs[3 * v[1] + 2]};
+  const double X2[3] = {Xs[3 * v[2]], Xs[3 * v[2] + 1], Xs[3 * v[2] + 2]};
+  const double dcx = e_near[8 * s + 4] - xt, dcy = e_near[8 * s + 5] - yt, dcz = e_near[8 * s + 6] - zt;
+  if (dnorm3(dcx, dcy, dcz) < near_region) {  // fill_nonadj_linear, near element: 5x5 rule
+    for (int g = 0; g < 25; ++g) {
+      const double t0 = c_gw[g][0], t1 = c_gw[g][1], ww = c_gw[g][2];
+      const double N[3] = {t0, t1 * (1. - t0), (t0 - 1.) * (t1 - 1.)};
+      const double Rx = N[0] * X0[0] + N[1] * X1[0] + N[2] * X2[0] - xt;
+      const double Ry = N[0] * X0[1] + N[1] * X1[1] + N[2] * X2[1] - yt;
+      const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
+      const double nr_inv = 1. / dnorm3(Rx, Ry, Rz);
+      const double tmp = ww * (1. - t0) * N[a] * nr_inv;
+      G += J * tmp;
+      Gn -= ((Rx * crx + Ry * cry + Rz * crz) * nr_inv) * (tmp * nr_inv);
+    }
+  } else {  // Dunavant 6-point rule
+    for (int q = 0; q < 6; ++q) {
+      const double N[3] = {c_dv[q][0], c_dv[q][1], c_dv[q][2]};
+      const double Rx = N[0] * X0[0] + N[1] * X1[0] + N[2] * X2[0] - xt;
+      const double Ry = N[0] * X0[1] + N[1] * X1[1] + N[2] * X2[1] - yt;
+      const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
+      const double nr_inv = 1. / dnorm3(Rx, Ry, Rz);
+      const double tmp = c_dv[q][3] * N[a] * nr_inv;
+      G += J * tmp;
+      Gn -= ((Rx * crx + Ry * cry + Rz * crz) * nr_inv) * (tmp * nr_inv);
+    }
+  }
+  wG = G;
+  wGn = Gn;
+}
+
+__global__ void k_near_weights(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs, const int* __restrict__ nb_targets,
+                               const int* __restrict__ nb_ranges, const int* __restrict__ dof_inc_off, const int* __restrict__ dof_inc,
+                               const double* __restrict__ Xs, const int* __restrict__ e_vtx, const double* __restrict__ e_near,
+                               double near_region, double* __restrict__ WG, double* __restrict__ WGn) {
+  const NearBlockDev B = blocks[blockIdx.x];
+  const int64_t total = (int64_t)B.ntgt * B.ndof;
+  const int* rng = nb_ranges + 2 * B.rng_off;
+  for (int64_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const int tl = (int)(idx / B.ndof), j = (int)(idx % B.ndof);
+    const int dof = nb_dofs[B.dof_off + j];
+    const int t = nb_targets[B.tgt_off + tl];
+    double G = 0.0, Gn = 0.0;
+    for (int k = dof_inc_off[dof]; k < dof_inc_off[dof + 1]; ++k) {
+      const int s = dof_inc[k] / 3, a = dof_inc[k] % 3;
+      // s in one of the sorted half-open ranges?
+      int lo = 0, hi = B.nrng - 1, hit = 0;
+      while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        if (s < rng[2 * mid])
+          hi = mid - 1;
+        else if (s >= rng[2 * mid + 1])
+          lo = mid + 1;
+        else {
+          hit = 1;
+          break;
+        }
+      }
+      if (!hit) continue;
+      double g, gn;
+      elem_vertex_weight(s, a, t, Xs, e_vtx, e_near, near_region, g, gn);
+      G += g;
+      Gn += gn;
+    }
+    WG[B.w_off + idx] = G;
+    WGn[B.w_off + idx] = Gn;
+  }
+}
+
+// rigid-mode diagonal: diag_i = -GnPhi(point of i), 1 if |.| < 1e-15
+__global__ void k_diag(int n, const int* __restrict__ dof_point, const double* __restrict__ GnPhi, double* __restrict__ diag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double d = -GnPhi[dof_point[i]];
+    if (fabs(d) < 1e-15) d = 1.0;
+    diag[i] = d;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Krylov helpers (FP64).  Dot products of w with columns V[0..k) in two deterministic
+// stages: per-block partials, then one block per column.
+__global__ void k_mdot_partial(const double* __restrict__ V, int ldv, int k, const double* __restrict__ w, int n,
+                               double* __restrict__ partial /*[gridDim.x][k]*/) {
+  extern __shared__ double red[];
+  const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c = 0; c < k; ++c) {
+    const double* v = V + (size_t)c * ldv;
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s = fma(v[i], w[i], s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int i = 0; i < nw; ++i) t += red[i];
+      partial[(size_t)blockIdx.x * k + c] = t;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_mdot_final(const double* __restrict__ partial, int nblk, int k, double* __restrict__ out) {
+  const int c = blockIdx.x;
+  __shared__ double red[32];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += partial[(size_t)b * k + c];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    out[c] = t;
+  }
+}
+
+// w -= V[:, 0:k] h   (h on device)
+__global__ void k_maxpy(const double* __restrict__ V, int ldv, int k, const double* __restrict__ h, double* __restrict__ w, int n) {
+  extern __shared__ double sh[];
+  for (int c = threadIdx.x; c < k; c += blockDim.x) sh[c] = h[c];
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = w[i];
+    for (int c = 0; c < k; ++c) s = fma(-sh[c], V[(size_t)c * ldv + i], s);
+    w[i] = s;
+  }
+}
+
+// y = a*x (+ y if accumulate)
+__global__ void k_axpby(int n, double a, const double* __restrict__ x, double b, double* __restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a * x[i] + (b == 0.0 ? 0.0 : b * y[i]);
+}
+
+// y = x * (1/s), s read from device memory
+__global__ void k_scale_inv(int n, const double* __restrict__ x, const double* __restrict__ s, double* __restrict__ y) {
+  const double inv = 1.0 / s[0];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = x[i] * inv;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+template <int P>
+void launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st) {
+  constexpr int NC = ncoef(P);
+  const int tpb_coef = ((NC + 31) / 32) * 32;
+  if (a.n_leaves > 0)
+    k_p2m<P><<<a.n_leaves, 128, 0, st>>>(a.leaves, a.node_fb, a.node_fe, a.node_X, a.e_q, a.e_W, a.e_n, a.e_dof, a.phi, a.phin, a.M);
+  for (int l = a.n_levels - 1; l >= 0; --l) {
+    const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
+    if (cnt > 0)
+      k_m2m<P><<<cnt, tpb_coef, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.M);
+  }
+  cudaMemsetAsync(a.L, 0, sizeof(double2) * 2 * NC * (size_t)a.n_nodes, st);
+  if (a.n_m2l_targets > 0)
+    k_m2l<P><<<a.n_m2l_targets, tpb_coef, 0, st>>>(a.m2l_targets, a.m2l_off, a.m2l_src, a.node_X, a.M, a.L);
+  for (int l = 0; l < a.n_levels; ++l) {
+    const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
+    if (cnt > 0)
+      k_l2l<P><<<cnt, tpb_coef, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.L);
+  }
+  if (a.n_blocks > 0) {
+    const size_t shm = sizeof(double2) * (size_t)(a.chunk + a.max_ntgt);
+    k_targets<P><<<a.n_blocks, 128, shm, st>>>(a.blocks, a.nb_dofs, a.nb_targets, a.WG, a.WGn, a.Xs, a.node_X, a.L, a.phi, a.phin,
+                                               a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.GPhin, a.GnPhi, a.chunk);
+  }
+}
+
+template <int P>
+void set_target_smem(int bytes) {
+  cudaFuncSetAttribute(k_targets<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+void launch_matvec(int p, const MatvecArgs& a, cudaStream_t st) {
+  switch (p) {
+#define BEMB200_CASE(PP) \
+  case PP:               \
+    launch_matvec_fmm<PP>(a, st); break;
+    BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5) BEMB200_CASE(6)
+    BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10) BEMB200_CASE(11) BEMB200_CASE(12)
+#undef BEMB200_CASE
+    default: break;
+  }
+}
+
+void configure_targets_smem(int p, int bytes) {
+  switch (p) {
+#define BEMB200_CASE(PP) \
+  case PP:               \
+    set_target_smem<PP>(bytes); break;
+    BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5) BEMB200_CASE(6)
+    BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10) BEMB200_CASE(11) BEMB200_CASE(12)
+#undef BEMB200_CASE
+    default: break;
+  }
+}
+
+void launch_densities(int n, int mode, const double* x, const double* known, const int* kind, double* phi, double* phin, cudaStream_t st) {
+  const int g = (n + 255) / 256;
+  k_densities<<<g > 0 ? g : 1, 256, 0, st>>>(n, mode, x, known, kind, phi, phin);
+}
+
+void launch_near_weights(const NearArgs& a, cudaStream_t st) {
+  if (a.n_blocks > 0)
+    k_near_weights<<<a.n_blocks, 256, 0, st>>>(a.blocks, a.nb_dofs, a.nb_targets, a.nb_ranges, a.dof_inc_off, a.dof_inc, a.Xs, a.e_vtx,
+                                                a.e_near, a.near_region, a.WG, a.WGn);
+}
+
+void launch_diag(int n, const int* dof_point, const double* GnPhi, double* diag, cudaStream_t st) {
+  const int g = (n + 255) / 256;
+  k_diag<<<g > 0 ? g : 1, 256, 0, st>>>(n, dof_point, GnPhi, diag);
+}
+
+int mdot_blocks(int n) {
+  int b = (n + 1023) / 1024;
+  return b < 1 ? 1 : (b > 296 ? 296 : b);
+}
+
+void launch_mdot(const double* V, int ldv, int k, const double* w, int n, double* partial, double* out, cudaStream_t st) {
+  const int nb = mdot_blocks(n);
+  k_mdot_partial<<<nb, 256, 8 * sizeof(double), st>>>(V, ldv, k, w, n, partial);
+  k_mdot_final<<<k, 256, 0, st>>>(partial, nb, k, out);
+}
+
+void launch_maxpy(const double* V, int ldv, int k, const double* h, double* w, int n, cudaStream_t st) {
+  int g = (n + 255) / 256;
+  if (g > 1184) g = 1184;
+  k_maxpy<<<g > 0 ? g : 1, 256, sizeof(double) * (k > 0 ? k : 1), st>>>(V, ldv, k, h, w, n);
+}
+
+void launch_axpby(int n, double a, const double* x, double b, double* y, cudaStream_t st) {
+  int g = (n + 255) / 256;
+  if (g > 1184) g = 1184;
+  k_axpby<<<g > 0 ? g : 1, 256, 0, st>>>(n, a, x, b, y);
+}
+
+void launch_scale_inv(int n, const double* x, const double* s, double* y, cudaStream_t st) {
+  int g = (n + 255) / 256;
+  if (g > 1184) g = 1184;
+  k_scale_inv<<<g > 0 ? g : 1, 256, 0, st>>>(n, x, s, y);
+}
+
+}  // namespace bemb200

@@ -1,0 +1,89 @@
+// Launch interface of the FMM / near-field / Krylov kernels (kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace bemb200 {
+
+struct NearBlockDev {
+  int64_t w_off;  // first weight of this block's rows
+  int node;       // deepest bucket shared by the block's targets
+  int dof_off, ndof;
+  int tgt_off, ntgt;
+  int rng_off, nrng;
+};
+
+struct MatvecArgs {
+  int n_nodes = 0, n_levels = 0;
+  // P2M
+  int n_leaves = 0;
+  const int* leaves = nullptr;
+  const int* node_fb = nullptr;
+  const int* node_fe = nullptr;
+  const double* node_X = nullptr;
+  const double* e_q = nullptr;
+  const double* e_W = nullptr;
+  const double* e_n = nullptr;
+  const int* e_dof = nullptr;
+  // tree passes
+  const int* level_parent_off = nullptr;  // host array [n_levels+1]
+  const int* level_parents = nullptr;     // device
+  const int* child_begin = nullptr;
+  const int* child_end = nullptr;
+  const int* node_children = nullptr;
+  int n_m2l_targets = 0;
+  const int* m2l_targets = nullptr;
+  const int* m2l_off = nullptr;
+  const int* m2l_src = nullptr;
+  double2* M = nullptr;
+  double2* L = nullptr;
+  // targets
+  int n_blocks = 0, chunk = 0, max_ntgt = 0;
+  const NearBlockDev* blocks = nullptr;
+  const int* nb_dofs = nullptr;
+  const int* nb_targets = nullptr;
+  const double* WG = nullptr;
+  const double* WGn = nullptr;
+  const double* Xs = nullptr;
+  const int* point_dof_off = nullptr;
+  const int* point_dof = nullptr;
+  const int* dof_kind = nullptr;
+  const double* diag = nullptr;
+  // state
+  const double* phi = nullptr;
+  const double* phin = nullptr;
+  double* rows = nullptr;   // may be null
+  double* GPhin = nullptr;  // may be null
+  double* GnPhi = nullptr;
+};
+
+struct NearArgs {
+  int n_blocks = 0;
+  const NearBlockDev* blocks = nullptr;
+  const int* nb_dofs = nullptr;
+  const int* nb_targets = nullptr;
+  const int* nb_ranges = nullptr;
+  const int* dof_inc_off = nullptr;
+  const int* dof_inc = nullptr;
+  const double* Xs = nullptr;
+  const int* e_vtx = nullptr;
+  const double* e_near = nullptr;
+  double near_region = 0.0;
+  double* WG = nullptr;
+  double* WGn = nullptr;
+};
+
+void upload_quadrature(const double dv[6][4], const double gw[25][3], cudaStream_t s);
+void configure_targets_smem(int p, int bytes);
+void launch_matvec(int p, const MatvecArgs& a, cudaStream_t st);
+void launch_densities(int n, int mode, const double* x, const double* known, const int* kind, double* phi, double* phin, cudaStream_t st);
+void launch_near_weights(const NearArgs& a, cudaStream_t st);
+void launch_diag(int n, const int* dof_point, const double* GnPhi, double* diag, cudaStream_t st);
+int mdot_blocks(int n);
+void launch_mdot(const double* V, int ldv, int k, const double* w, int n, double* partial, double* out, cudaStream_t st);
+void launch_maxpy(const double* V, int ldv, int k, const double* h, double* w, int n, cudaStream_t st);
+void launch_axpby(int n, double a, const double* x, double b, double* y, cudaStream_t st);
+void launch_scale_inv(int n, const double* x, const double* s, double* y, cudaStream_t st);
+
+}  // namespace bemb200

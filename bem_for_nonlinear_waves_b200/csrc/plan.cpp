@@ -1,0 +1,611 @@
+// Host-side set-up plan (see plan.hpp).  Compiled with g++ -O2 -march=x86-64-v3,
+// no fast-math: the element positions and bucket bounds must round like the
+// reference's so that the octree is the same tree.
+#include "plan.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <numeric>
+
+namespace bemb200 {
+namespace {
+
+using V3 = std::array<double, 3>;
+
+// std::hypot(x, y, z) as libstdc++ implements it (Norm(Tddd),
+// lib/include/basic_arithmetic_array_operations.hpp:860).
+inline double hypot3(double x, double y, double z) {
+  x = std::abs(x);
+  y = std::abs(y);
+  z = std::abs(z);
+  if (double a = x < y ? y < z ? z : y : x < z ? z : x)
+    return a * std::sqrt((x / a) * (x / a) + (y / a) * (y / a) + (z / a) * (z / a));
+  return 0.0;
+}
+inline V3 sub(const V3& a, const V3& b) { return {a[0] - b[0], a[1] - b[1], a[2] - b[2]}; }
+inline double nrm(const V3& a) { return hypot3(a[0], a[1], a[2]); }
+// Dot(weights[3], X[3]): fma into a zero accumulator per component (basic_arithmetic_array_operations.hpp:639-657)
+inline V3 bary(const double w0, const double w1, const double w2, const V3& a, const V3& b, const V3& c) {
+  V3 r{0, 0, 0};
+  for (int j = 0; j < 3; ++j) r[j] = std::fma(w0, a[j], r[j]);
+  for (int j = 0; j < 3; ++j) r[j] = std::fma(w1, b[j], r[j]);
+  for (int j = 0; j < 3; ++j) r[j] = std::fma(w2, c[j], r[j]);
+  return r;
+}
+// Cross() in binary128, rounded once (basic_arithmetic_array_operations.hpp:906-920)
+inline V3 cross128(const V3& A, const V3& B) {
+  __float128 ax = A[0], ay = A[1], az = A[2], bx = B[0], by = B[1], bz = B[2];
+  return {(double)(ay * bz - az * by), (double)(az * bx - ax * bz), (double)(ax * by - ay * bx)};
+}
+inline V3 unit(V3 a) {  // Normalize (basic_arithmetic_array_operations.hpp:837-850)
+  double n = 0.;
+  for (double v : a) n = std::fma(v, v, n);
+  if (n == 0.) return a;
+  n = std::sqrt(n);
+  for (auto& v : a) v /= n;
+  return a;
+}
+inline V3 normal128(const V3& a, const V3& b, const V3& c) {  // TriangleNormalHP (…:961-986)
+  __float128 ax = a[0], ay = a[1], az = a[2];
+  __float128 bax = (__float128)b[0] - ax, bay = (__float128)b[1] - ay, baz = (__float128)b[2] - az;
+  __float128 cax = (__float128)c[0] - ax, cay = (__float128)c[1] - ay, caz = (__float128)c[2] - az;
+  __float128 nx = bay * caz - baz * cay, ny = baz * cax - bax * caz, nz = bax * cay - bay * cax;
+  __float128 n2 = nx * nx + ny * ny + nz * nz;
+  if (n2 == 0) return {0, 0, 0};
+  __float128 inv = (__float128)1 / (__float128)std::sqrt((double)n2);
+  return {(double)(nx * inv), (double)(ny * inv), (double)(nz * inv)};
+}
+inline double dotfma(const V3& a, const V3& b) { return std::fma(a[0], b[0], std::fma(a[1], b[1], a[2] * b[2])); }
+
+// Dunavant degree-4 rule (lib/include/dunavant_rules.hpp:36-42): barycentrics + weight
+const double kDv[6][4] = {{0.816847572980459, 0.091576213509771, 0.091576213509771, 0.054975871827661},
+                          {0.091576213509771, 0.816847572980459, 0.091576213509771, 0.054975871827661},
+                          {0.091576213509771, 0.091576213509771, 0.816847572980459, 0.054975871827661},
+                          {0.108103018168070, 0.445948490915965, 0.445948490915965, 0.111690794839006},
+                          {0.445948490915965, 0.108103018168070, 0.445948490915965, 0.111690794839006},
+                          {0.445948490915965, 0.445948490915965, 0.108103018168070, 0.111690794839006}};
+
+struct Bucket {
+  double lo[3], hi[3], X[3];
+  double dL, inv_dL, xmin[3];
+  int size[3];
+  int level = 0, parent = -1;
+  std::vector<int> kids;                  // created children, cell order
+  std::vector<std::vector<int>> cell;     // elements per cell
+  std::vector<int> data;                  // data1D
+  std::vector<int> kid_of_cell;
+  double off = 0.0;
+  std::vector<int> near, m2l, l2m;
+};
+
+void bucket_init(Bucket& b, const double lo[3], const double hi[3], double dL) {
+  for (int a = 0; a < 3; ++a) {
+    b.lo[a] = lo[a];
+    b.hi[a] = hi[a];
+    b.X[a] = (lo[a] + hi[a]) / 2.;  // Mean(Transpose(bounds))
+    b.xmin[a] = lo[a];
+  }
+  b.dL = dL;
+  b.inv_dL = 1.0 / dL;
+  for (int a = 0; a < 3; ++a) {
+    double s = std::ceil((b.hi[a] - b.lo[a]) / dL);  // calculate_size
+    if (s <= 0.) s = 1.;
+    b.size[a] = (int)s;
+  }
+  b.cell.assign(b.size[0] * b.size[1] * b.size[2], {});
+  b.kid_of_cell.assign(b.size[0] * b.size[1] * b.size[2], -1);
+}
+
+inline void cell_index(const Bucket& b, const double* x, int ijk[3]) {
+  for (int a = 0; a < 3; ++a) ijk[a] = (int)std::floor((x[a] - b.xmin[a]) * b.inv_dL);
+}
+inline bool inside(const Bucket& b, const double* x) {
+  int ijk[3];
+  cell_index(b, x, ijk);
+  for (int a = 0; a < 3; ++a)
+    if (ijk[a] < 0 || ijk[a] >= b.size[a]) return false;
+  return true;
+}
+inline int cell_of(const Bucket& b, const double* x) {
+  int ijk[3];
+  cell_index(b, x, ijk);
+  for (int a = 0; a < 3; ++a) ijk[a] = std::clamp(ijk[a], 0, b.size[a] - 1);
+  return (ijk[0] * b.size[1] + ijk[1]) * b.size[2] + ijk[2];
+}
+
+struct TreeBuilder {
+  const PlanOptions& opt;
+  const std::vector<V3>& pole;
+  std::vector<Bucket> B;
+  int drops = 0;
+  explicit TreeBuilder(const PlanOptions& o, const std::vector<V3>& p) : opt(o), pole(p) {}
+
+  bool add(int bi, int e) {  // Buckets::add: InsideQ without clamp, then the clamped cell
+    Bucket& b = B[bi];
+    if (!inside(b, pole[e].data())) return false;
+    b.cell[cell_of(b, pole[e].data())].push_back(e);
+    b.data.push_back(e);
+    return true;
+  }
+  // Buckets::generateTree with newChild (lib_spatial_partitioning.hpp:1078-1111)
+  void grow(int bi) {
+    const bool cond = !B[bi].data.empty() && (int)B[bi].data.size() > opt.leaf_max && B[bi].level < opt.max_level;
+    if (!cond) return;
+    const int nc = B[bi].size[0] * B[bi].size[1] * B[bi].size[2];
+    for (int c = 0; c < nc; ++c) {
+      if (B[bi].cell[c].empty()) continue;
+      const int i = c / (B[bi].size[1] * B[bi].size[2]);
+      const int j = (c / B[bi].size[2]) % B[bi].size[1];
+      const int k = c % B[bi].size[2];
+      double lo[3], hi[3];
+      const int ijk[3] = {i, j, k};
+      for (int a = 0; a < 3; ++a) {  // getBounds({i,j,k})
+        lo[a] = B[bi].dL * ijk[a] + B[bi].xmin[a];
+        hi[a] = B[bi].dL * (ijk[a] + 1) + B[bi].xmin[a];
+      }
+      const double dLc = B[bi].dL * (0.5 + 1e-13);
+      Bucket child;
+      bucket_init(child, lo, hi, dLc);
+      child.level = B[bi].level + 1;
+      child.parent = bi;
+      B.push_back(std::move(child));
+      const int ci = (int)B.size() - 1;
+      B[bi].kids.push_back(ci);
+      B[bi].kid_of_cell[c] = ci;
+      for (int e : B[bi].cell[c])
+        if (!add(ci, e)) ++drops;
+      grow(ci);
+    }
+  }
+};
+
+bool is_far(const PlanOptions& o, const Bucket& A, const Bucket& Bk) {  // moments.hpp:950-956
+  const double eff = std::max(A.dL + 2.0 * A.off, Bk.dL + 2.0 * Bk.off);
+  const V3 d{Bk.X[0] - A.X[0], Bk.X[1] - A.X[1], Bk.X[2] - A.X[2]};
+  return o.theta > std::sqrt(3.0) * eff / nrm(d);
+}
+
+void lists(const PlanOptions& o, std::vector<Bucket>& B, int a, int b) {  // moments.hpp:967-979
+  if (is_far(o, B[a], B[b])) return;
+  if (a != b) B[a].near.push_back(b);
+  for (int ac : B[a].kids)
+    for (int bc : B[b].kids) {
+      if (ac != bc && is_far(o, B[ac], B[bc]))
+        B[ac].m2l.push_back(bc);
+      else
+        lists(o, B, ac, bc);
+    }
+}
+
+}  // namespace
+
+int build_dofs(int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int32_t* dof_point, int32_t* dof_face,
+               int32_t* dof_kind, int32_t* face_dof, uint8_t* point_flags) {
+  if (np <= 0 || nf <= 0 || !X || !tri || !fdir) return -1;
+  std::vector<int> cnt(np + 1, 0);
+  for (int f = 0; f < nf; ++f)
+    for (int a = 0; a < 3; ++a) {
+      int p = tri[3 * f + a];
+      if (p < 0 || p >= np) return -1;
+      ++cnt[p + 1];
+    }
+  for (int p = 0; p < np; ++p) cnt[p + 1] += cnt[p];
+  std::vector<int> pf(cnt[np]);
+  {
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+    for (int f = 0; f < nf; ++f)
+      for (int a = 0; a < 3; ++a) pf[fill[tri[3 * f + a]]++] = f;  // ascending face order per point
+  }
+  std::vector<V3> fn(nf);
+  std::vector<double> fa(nf);
+  auto P = [&](int i) { return V3{X[3 * i], X[3 * i + 1], X[3 * i + 2]}; };
+  for (int f = 0; f < nf; ++f) {
+    V3 a = P(tri[3 * f]), b = P(tri[3 * f + 1]), c = P(tri[3 * f + 2]);
+    fn[f] = normal128(a, b, c);
+    fa[f] = 0.5 * nrm(cross128(sub(b, a), sub(c, a)));
+  }
+  std::vector<uint8_t> neu(np, 0), dir(np, 0), cor(np, 0), mult(np, 0);
+  const double lim = 20. * M_PI / 180.;  // setIsMultipleNode (BEM_setBoundaryTypes.hpp:434-441)
+  for (int p = 0; p < np; ++p) {
+    if (cnt[p] == cnt[p + 1]) continue;
+    bool alln = true, alld = true;
+    for (int k = cnt[p]; k < cnt[p + 1]; ++k) {
+      alln = alln && !fdir[pf[k]];
+      alld = alld && fdir[pf[k]];
+    }
+    neu[p] = alln;
+    dir[p] = alld;
+    cor[p] = !alln && !alld;
+    if (cor[p]) {
+      mult[p] = 1;
+      continue;
+    }
+    V3 n{0, 0, 0};
+    for (int k = cnt[p]; k < cnt[p + 1]; ++k)
+      for (int a = 0; a < 3; ++a) n[a] += fa[pf[k]] * fn[pf[k]][a];
+    n = unit(n);
+    for (int k = cnt[p]; k < cnt[p + 1]; ++k) {
+      const V3& m = fn[pf[k]];
+      if (!(dotfma(n, m) > std::cos(lim) * std::sqrt(dotfma(n, n)) * std::sqrt(dotfma(m, m)))) mult[p] = 1;
+    }
+  }
+  auto isNeu = [&](int p, int f) {  // isNeumannID_BEM (BEM_setBoundaryTypes.hpp:29-37)
+    if (neu[p] || cor[p]) return mult[p] ? (f >= 0 && !fdir[f]) : (f < 0);
+    return false;
+  };
+  auto isDir = [&](int p, int f) { return (dir[p] || cor[p]) && f < 0; };
+  int n = 0;
+  std::vector<int> null_dof(np, -1);
+  std::vector<std::vector<std::pair<int, int>>> fkeys(np);
+  for (int p = 0; p < np; ++p) {
+    if (cnt[p] == cnt[p + 1]) continue;
+    if (isNeu(p, -1) || isDir(p, -1)) {
+      dof_point[n] = p;
+      dof_face[n] = -1;
+      dof_kind[n] = isDir(p, -1) ? 0 : 1;
+      null_dof[p] = n++;
+    }
+    for (int k = cnt[p]; k < cnt[p + 1]; ++k) {
+      const int f = pf[k];
+      if (isNeu(p, f) || isDir(p, f)) {
+        dof_point[n] = p;
+        dof_face[n] = f;
+        dof_kind[n] = cor[p] ? 2 : 1;
+        fkeys[p].push_back({f, n});
+        ++n;
+      }
+    }
+  }
+  for (int f = 0; f < nf; ++f)
+    for (int a = 0; a < 3; ++a) {  // pf2Index (BEM_setBoundaryTypes.hpp:83-95)
+      const int p = tri[3 * f + a];
+      int d = -1;
+      if (!mult[p] || fdir[f])
+        d = null_dof[p];
+      else
+        for (auto& kv : fkeys[p])
+          if (kv.first == f) d = kv.second;
+      if (d < 0) return -1;
+      face_dof[3 * f + a] = d;
+    }
+  if (point_flags)
+    for (int p = 0; p < np; ++p) point_flags[p] = (neu[p] ? 1 : 0) | (dir[p] ? 2 : 0) | (cor[p] ? 4 : 0) | (mult[p] ? 8 : 0);
+  return n;
+}
+
+bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int ndof,
+                const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof) {
+  P = Plan();
+  P.opt = opt;
+  if (np <= 0 || nf <= 0 || ndof <= 0 || !X || !tri || !fdir || !dof_point || !dof_face || !dof_kind || !face_dof) {
+    P.error = "invalid BVP description";
+    return false;
+  }
+  if (opt.p < 1 || opt.p > 12 || opt.max_level < 1 || opt.max_level > 20 || opt.leaf_max < 1 || !(opt.theta > 0)) {
+    P.error = "invalid options";
+    return false;
+  }
+  P.np = np;
+  P.nf = nf;
+  P.ndof = ndof;
+  P.dof_point.assign(dof_point, dof_point + ndof);
+  P.dof_face.assign(dof_face, dof_face + ndof);
+  P.dof_kind.assign(dof_kind, dof_kind + ndof);
+  P.face_dof.assign(face_dof, face_dof + 3 * nf);
+  for (int i = 0; i < ndof; ++i)
+    if (dof_point[i] < 0 || dof_point[i] >= np || dof_kind[i] < 0 || dof_kind[i] > 2) {
+      P.error = "invalid DOF table";
+      return false;
+    }
+  for (int i = 0; i < 3 * nf; ++i)
+    if (tri[i] < 0 || tri[i] >= np || face_dof[i] < 0 || face_dof[i] >= ndof) {
+      P.error = "invalid connectivity";
+      return false;
+    }
+  for (int i = 0; i < 3 * np; ++i)
+    if (!std::isfinite(X[i])) {
+      P.error = "non-finite coordinates";
+      return false;
+    }
+  // point -> DOFs
+  P.point_dof_off.assign(np + 1, 0);
+  for (int i = 0; i < ndof; ++i) ++P.point_dof_off[dof_point[i] + 1];
+  for (int p = 0; p < np; ++p) P.point_dof_off[p + 1] += P.point_dof_off[p];
+  P.point_dof.resize(ndof);
+  {
+    std::vector<int> fill(P.point_dof_off.begin(), P.point_dof_off.end() - 1);
+    for (int i = 0; i < ndof; ++i) P.point_dof[fill[dof_point[i]]++] = i;
+  }
+  P.corner_src_dof.assign(ndof, -1);
+  for (int i = 0; i < ndof; ++i)
+    if (dof_kind[i] == 2) {
+      const int p = dof_point[i];
+      for (int k = P.point_dof_off[p]; k < P.point_dof_off[p + 1]; ++k)
+        if (dof_kind[P.point_dof[k]] == 0) P.corner_src_dof[i] = P.point_dof[k];
+    }
+
+  // coordinate scaling (Network.hpp:3215-3245, BEM_solveBVP_GMRES_FMM.hpp:3076-3091)
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+  for (int i = 0; i < np; ++i)
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = std::min(mn[a], X[3 * i + a]);
+      mx[a] = std::max(mx[a], X[3 * i + a]);
+    }
+  const double Lx = std::abs(mx[0] - mn[0]), Ly = std::abs(mx[1] - mn[1]), Lz = std::abs(mx[2] - mn[2]);
+  P.L = std::sqrt(Lx * Lx + Ly * Ly + Lz * Lz);
+  if (!(P.L > 1e-10)) P.L = 1.0;
+  P.Xs.resize(3 * np);
+  for (int i = 0; i < 3 * np; ++i) P.Xs[i] = X[i] / P.L;
+  for (int a = 0; a < 3; ++a) {
+    mn[a] = 1e300;
+    mx[a] = -1e300;
+  }
+  for (int i = 0; i < np; ++i)
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = std::min(mn[a], P.Xs[3 * i + a]);
+      mx[a] = std::max(mx[a], P.Xs[3 * i + a]);
+    }
+  P.scale = hypot3(mx[0] - mn[0], mx[1] - mn[1], mx[2] - mn[2]);
+  const double C[3] = {(mn[0] + mx[0]) / 2., (mn[1] + mx[1]) / 2., (mn[2] + mx[2]) / 2.};
+  P.near_region = P.scale / 25.;
+
+  // element sources (BEM_solveBVP_GMRES_FMM.hpp:1799-1937)
+  auto XP = [&](int i) { return V3{P.Xs[3 * i], P.Xs[3 * i + 1], P.Xs[3 * i + 2]}; };
+  std::vector<V3> pole(nf);
+  std::vector<double> q(nf * 18), W(nf * 6), en(nf * 3), enear(nf * 8), offs(nf);
+  for (int f = 0; f < nf; ++f) {
+    const V3 a = XP(tri[3 * f]), b = XP(tri[3 * f + 1]), c = XP(tri[3 * f + 2]);
+    const V3 cr = cross128(sub(b, a), sub(c, a));
+    const V3 n = unit(cr);
+    const double J = nrm(cr);
+    pole[f] = bary(1. / 3., 1. / 3., 1. / 3., a, b, c);
+    double off = 0.0;
+    for (int k = 0; k < 6; ++k) {
+      const V3 x = bary(kDv[k][0], kDv[k][1], kDv[k][2], a, b, c);
+      for (int d = 0; d < 3; ++d) q[f * 18 + 3 * k + d] = x[d];
+      W[f * 6 + k] = J * kDv[k][3];
+      off = std::max(off, nrm(sub(x, pole[f])));
+    }
+    offs[f] = off;
+    for (int d = 0; d < 3; ++d) en[3 * f + d] = n[d];
+    const double area = 0.5 * nrm(cr);
+    const V3 nh = normal128(a, b, c);
+    enear[8 * f + 0] = 2. * area;
+    for (int d = 0; d < 3; ++d) {
+      enear[8 * f + 1 + d] = 2. * area * nh[d];
+      enear[8 * f + 4 + d] = (a[d] + b[d] + c[d]) / 3.;
+    }
+    enear[8 * f + 7] = 0.0;
+  }
+
+  // octree (BEM_solveBVP_GMRES_FMM.hpp:1178-1201; lib_spatial_partitioning.hpp)
+  TreeBuilder T(opt, pole);
+  {
+    const double dLr = 1.05 * P.scale / 2.;
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = C[a] - dLr;
+      hi[a] = C[a] + dLr;
+    }
+    Bucket root;
+    bucket_init(root, lo, hi, dLr);
+    T.B.push_back(std::move(root));
+  }
+  for (int f = 0; f < nf; ++f) P.n_added += T.add(0, f);
+  T.grow(0);
+  P.n_child_drops = T.drops;
+  std::vector<Bucket>& B = T.B;
+  const int nb = (int)B.size();
+
+  // offsets (moments.hpp:1336-1349): leaves from their elements, parents from children
+  std::vector<std::vector<int>> lvl(opt.max_level + 1);
+  for (int i = 0; i < nb; ++i)
+    if (!B[i].data.empty()) lvl[B[i].level].push_back(i);
+  for (int i = 0; i < nb; ++i)
+    if (!B[i].data.empty() && B[i].kids.empty()) {
+      B[i].off = 0.0;
+      for (int e : B[i].data) B[i].off = std::max(B[i].off, offs[e]);
+    }
+  for (int l = opt.max_level - 1; l >= 0; --l)
+    for (int i : lvl[l]) {
+      if (B[i].kids.empty()) continue;
+      B[i].off = 0.0;
+      for (int c : B[i].kids) B[i].off = std::max(B[i].off, B[c].off);
+    }
+  // lists (moments.hpp:983-997)
+  for (int a : B[0].kids)
+    for (int b : B[0].kids) lists(opt, B, a, b);
+  for (auto& lv : lvl)
+    for (int a : lv)
+      for (int b : B[a].m2l) B[b].l2m.push_back(a);
+
+  // element order: DFS pre-order of the deepest bucket holding each element
+  std::vector<int> owner(nf, -1);
+  for (int i = 0; i < nb; ++i)
+    for (int e : B[i].data) owner[e] = i;  // children come after parents in creation order
+  std::vector<std::vector<int>> owned(nb);
+  for (int i = 0; i < nb; ++i)
+    for (int e : B[i].data)
+      if (owner[e] == i) owned[i].push_back(e);
+  std::vector<int> subtree_end(nb);
+  for (int i = nb - 1; i >= 0; --i) {
+    subtree_end[i] = i + 1;
+    for (int c : B[i].kids) subtree_end[i] = std::max(subtree_end[i], subtree_end[c]);
+  }
+  P.face_of_pos.clear();
+  std::vector<int> start(nb + 1);
+  for (int i = 0; i < nb; ++i) {
+    start[i] = (int)P.face_of_pos.size();
+    for (int e : owned[i]) P.face_of_pos.push_back(e);
+  }
+  start[nb] = (int)P.face_of_pos.size();
+  P.owner_of_pos.assign(P.face_of_pos.size(), -1);
+  for (int i = 0; i < nb; ++i)
+    for (int s = start[i]; s < start[i] + (int)owned[i].size(); ++s) P.owner_of_pos[s] = i;
+  const int ne = (int)P.face_of_pos.size();
+  P.pos_of_face.assign(nf, -1);
+  for (int s = 0; s < ne; ++s) P.pos_of_face[P.face_of_pos[s]] = s;
+  P.e_q.resize(ne * 18);
+  P.e_W.resize(ne * 6);
+  P.e_n.resize(ne * 3);
+  P.e_dof.resize(ne * 3);
+  P.e_vtx.resize(ne * 3);
+  P.e_near.resize(ne * 8);
+  for (int s = 0; s < ne; ++s) {
+    const int f = P.face_of_pos[s];
+    std::memcpy(&P.e_q[s * 18], &q[f * 18], 18 * sizeof(double));
+    std::memcpy(&P.e_W[s * 6], &W[f * 6], 6 * sizeof(double));
+    std::memcpy(&P.e_n[s * 3], &en[f * 3], 3 * sizeof(double));
+    std::memcpy(&P.e_near[s * 8], &enear[f * 8], 8 * sizeof(double));
+    for (int a = 0; a < 3; ++a) {
+      P.e_dof[s * 3 + a] = face_dof[3 * f + a];
+      P.e_vtx[s * 3 + a] = tri[3 * f + a];
+    }
+  }
+  P.nodes.resize(nb);
+  P.node_children.clear();
+  for (int i = 0; i < nb; ++i) {
+    Plan::Node& N = P.nodes[i];
+    for (int a = 0; a < 3; ++a) {
+      N.lo[a] = B[i].lo[a];
+      N.hi[a] = B[i].hi[a];
+      N.X[a] = B[i].X[a];
+    }
+    N.dL = B[i].dL;
+    N.inv_dL = B[i].inv_dL;
+    for (int a = 0; a < 3; ++a) N.size[a] = B[i].size[a];
+    N.level = B[i].level;
+    N.parent = B[i].parent;
+    N.child_begin = (int)P.node_children.size();
+    for (int c : B[i].kids) P.node_children.push_back(c);
+    N.child_end = (int)P.node_children.size();
+    N.fb = start[i];
+    N.fe = start[subtree_end[i]];
+    N.n_data = (int)B[i].data.size();
+    N.max_internal_offset = B[i].off;
+  }
+  P.level_nodes = lvl;
+  P.leaves.clear();
+  for (auto& lv : lvl)
+    for (int i : lv)
+      if (B[i].kids.empty()) P.leaves.push_back(i);
+  // M2L sources per target node (non-empty targets only), near lists
+  P.m2l_off.assign(nb + 1, 0);
+  P.near_off.assign(nb + 1, 0);
+  for (int i = 0; i < nb; ++i) {
+    P.m2l_off[i + 1] = P.m2l_off[i] + (B[i].data.empty() ? 0 : (int)B[i].l2m.size());
+    P.near_off[i + 1] = P.near_off[i] + (int)B[i].near.size();
+  }
+  P.m2l_src.resize(P.m2l_off[nb]);
+  P.near_nodes.resize(P.near_off[nb]);
+  for (int i = 0; i < nb; ++i) {
+    if (!B[i].data.empty()) std::copy(B[i].l2m.begin(), B[i].l2m.end(), P.m2l_src.begin() + P.m2l_off[i]);
+    std::copy(B[i].near.begin(), B[i].near.end(), P.near_nodes.begin() + P.near_off[i]);
+  }
+  P.m2l_pairs = P.m2l_off[nb];
+  P.near_pairs = P.near_off[nb];
+  for (int i = 0; i < nb; ++i)
+    if (B[i].data.empty()) P.near_pairs -= (int)B[i].near.size();
+
+  // targets (target4FMM::setL2P / setDirectIntegration: getBucketAtDeepest)
+  P.target_box.assign(np, -1);
+  for (int p = 0; p < np; ++p) {
+    if (P.point_dof_off[p] == P.point_dof_off[p + 1]) continue;
+    const double* x = &P.Xs[3 * p];
+    int cur = 0;
+    while (!B[cur].kids.empty()) {
+      const int nx = B[cur].kid_of_cell[cell_of(B[cur], x)];
+      if (nx < 0) break;
+      cur = nx;
+    }
+    P.target_box[p] = cur;
+  }
+  // near blocks (lib_multipole_expansion.hpp:1180-1213)
+  std::vector<int> block_of_node(nb, -1);
+  P.blocks.clear();
+  P.block_of_point.assign(np, -1);
+  P.row_of_point.assign(np, -1);
+  std::vector<std::vector<int>> btargets;
+  for (int p = 0; p < np; ++p) {
+    const int t = P.target_box[p];
+    if (t < 0) continue;
+    if (block_of_node[t] < 0) {
+      block_of_node[t] = (int)P.blocks.size();
+      Plan::NearBlock nbk{};
+      nbk.node = t;
+      P.blocks.push_back(nbk);
+      btargets.emplace_back();
+    }
+    const int bi = block_of_node[t];
+    P.block_of_point[p] = bi;
+    P.row_of_point[p] = (int)btargets[bi].size();
+    btargets[bi].push_back(p);
+  }
+  P.nb_dofs.clear();
+  P.nb_targets.clear();
+  P.nb_ranges.clear();
+  int64_t woff = 0;
+  std::vector<int> mark(ndof, -1);
+  for (size_t bi = 0; bi < P.blocks.size(); ++bi) {
+    Plan::NearBlock& nbk = P.blocks[bi];
+    const int t = nbk.node;
+    std::vector<std::pair<int, int>> rng;
+    auto addr = [&](int n) {
+      if (P.nodes[n].fe > P.nodes[n].fb) rng.push_back({P.nodes[n].fb, P.nodes[n].fe});
+    };
+    addr(t);
+    for (int n : B[t].near) addr(n);
+    for (int a = B[t].parent; a >= 0; a = B[a].parent)
+      for (int n : B[a].near)
+        if (B[n].kids.empty()) addr(n);
+    std::sort(rng.begin(), rng.end());
+    std::vector<std::pair<int, int>> merged;
+    for (auto& r : rng) {
+      if (!merged.empty() && r.first <= merged.back().second)
+        merged.back().second = std::max(merged.back().second, r.second);
+      else
+        merged.push_back(r);
+    }
+    nbk.rng_off = (int)P.nb_ranges.size() / 2;
+    nbk.nrng = (int)merged.size();
+    std::vector<int> dl;
+    for (auto& r : merged) {
+      P.nb_ranges.push_back(r.first);
+      P.nb_ranges.push_back(r.second);
+      for (int s = r.first; s < r.second; ++s)
+        for (int a = 0; a < 3; ++a) {
+          const int d = P.e_dof[s * 3 + a];
+          if (mark[d] != (int)bi) {
+            mark[d] = (int)bi;
+            dl.push_back(d);
+          }
+        }
+    }
+    std::sort(dl.begin(), dl.end());
+    nbk.dof_off = (int)P.nb_dofs.size();
+    nbk.ndof = (int)dl.size();
+    P.nb_dofs.insert(P.nb_dofs.end(), dl.begin(), dl.end());
+    nbk.tgt_off = (int)P.nb_targets.size();
+    nbk.ntgt = (int)btargets[bi].size();
+    P.nb_targets.insert(P.nb_targets.end(), btargets[bi].begin(), btargets[bi].end());
+    nbk.w_off = woff;
+    woff += (int64_t)nbk.ntgt * nbk.ndof;
+  }
+  P.nnz = woff;
+  // DOF -> incident element vertices
+  P.dof_inc_off.assign(ndof + 1, 0);
+  for (int s = 0; s < ne; ++s)
+    for (int a = 0; a < 3; ++a) ++P.dof_inc_off[P.e_dof[s * 3 + a] + 1];
+  for (int i = 0; i < ndof; ++i) P.dof_inc_off[i + 1] += P.dof_inc_off[i];
+  P.dof_inc.resize(P.dof_inc_off[ndof]);
+  {
+    std::vector<int> fill(P.dof_inc_off.begin(), P.dof_inc_off.end() - 1);
+    for (int s = 0; s < ne; ++s)
+      for (int a = 0; a < 3; ++a) P.dof_inc[fill[P.e_dof[s * 3 + a]]++] = s * 3 + a;
+  }
+  return true;
+}
+
+}  // namespace bemb200

@@ -1,0 +1,103 @@
+// Host-side set-up plan of one boundary-value problem: coordinate scaling, element
+// sources, the bucket octree, MAC interaction lists, L2P targets and the near-field
+// sparsity.  Everything the device kernels need is flattened into index arrays here.
+//
+// The octree must reproduce the reference's Buckets tree exactly (same leaves for
+// every element), so the floating-point expressions that place an element or size a
+// bucket are the reference's own (lib/include/lib_spatial_partitioning.hpp:295-400,
+// 1078-1111) and this file is compiled without fast-math.
+#pragma once
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace bemb200 {
+
+struct PlanOptions {
+  int p = 10;
+  double theta = 0.25;
+  int leaf_max = 30;
+  int max_level = 7;
+};
+
+struct Plan {
+  PlanOptions opt;
+  int np = 0, nf = 0, ndof = 0;
+  double L = 1.0;      // coordinate scale factor (bounding-box diagonal)
+  double scale = 1.0;  // diagonal of the scaled bounding box
+  double near_region = 0.0;
+  std::vector<double> Xs;  // [3*np] scaled coordinates
+
+  // DOF table
+  std::vector<int32_t> dof_point, dof_face, dof_kind, face_dof;  // face_dof [3*nf] by face id
+  std::vector<int32_t> point_dof_off, point_dof;                  // CSR point -> DOFs
+  std::vector<int32_t> corner_src_dof;  // [ndof] for kind-2 rows: the point's Dirichlet DOF (or -1)
+
+  // elements in tree order (position s = 0..nf-1)
+  std::vector<int32_t> face_of_pos;   // [nf] face id at position s
+  std::vector<int32_t> pos_of_face;   // [nf]
+  std::vector<int32_t> owner_of_pos;  // [ne] deepest bucket holding the element
+  std::vector<double> e_q;            // [nf*18] P2M points (6 x xyz), scaled
+  std::vector<double> e_W;            // [nf*6] J * w_q
+  std::vector<double> e_n;            // [nf*3] unit normal of the P2M points
+  std::vector<int32_t> e_dof;         // [nf*3] face-vertex DOFs
+  std::vector<int32_t> e_vtx;         // [nf*3] face vertices (point ids)
+  std::vector<double> e_near;         // [nf*8]: J_near, cross_near xyz, centroid xyz, unused
+
+  // octree nodes (every created bucket, DFS pre-order)
+  struct Node {
+    double lo[3], hi[3];
+    double X[3];
+    double dL, inv_dL;
+    int size[3];
+    int level;
+    int parent;
+    int child_begin, child_end;  // into node_children
+    int fb, fe;                  // element range [fb, fe) in tree order (subtree, incl. orphans)
+    int n_data;                  // elements held (data1D size)
+    bool empty() const { return n_data == 0; }
+    double max_internal_offset;
+  };
+  std::vector<Node> nodes;
+  std::vector<int32_t> node_children;
+  std::vector<std::vector<int32_t>> level_nodes;  // non-empty nodes per level (reference order)
+  std::vector<int32_t> leaves;                    // non-empty childless nodes
+  int n_added = 0;
+  int n_child_drops = 0;  // elements a child bucket refused (reference edge case, counted)
+
+  // lists
+  std::vector<int32_t> m2l_off, m2l_src;  // CSR over nodes: sources of each target's M2L
+  std::vector<int32_t> near_off, near_nodes;  // CSR over nodes: same-level near buckets
+  int64_t m2l_pairs = 0, near_pairs = 0;
+
+  // L2P / near targets: one target per point with DOFs
+  std::vector<int32_t> target_box;     // [np] node of the point, -1 if the point has no DOF
+  // near-field blocks: one per distinct target node
+  struct NearBlock {
+    int node;
+    int64_t w_off;      // offset of this block's rows in the weight arrays
+    int dof_off, ndof;  // into nb_dofs
+    int tgt_off, ntgt;  // into nb_targets
+    int rng_off, nrng;  // into nb_ranges (element ranges [a,b) in tree order, sorted)
+  };
+  std::vector<NearBlock> blocks;
+  std::vector<int32_t> nb_dofs, nb_targets, nb_ranges;
+  std::vector<int32_t> block_of_point, row_of_point;  // [np]
+  int64_t nnz = 0;
+
+  // DOF -> incident (element position, vertex slot)
+  std::vector<int32_t> dof_inc_off, dof_inc;  // dof_inc = pos*3 + slot
+
+  std::string error;
+};
+
+// Fills dof tables from face flags with the reference's key rules; returns n_dof or -1.
+int build_dofs(int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int32_t* dof_point, int32_t* dof_face,
+               int32_t* dof_kind, int32_t* face_dof, uint8_t* point_flags);
+
+// Builds the plan; returns false and sets plan.error on invalid input.
+bool build_plan(Plan& plan, const PlanOptions& opt, int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int ndof,
+                const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof);
+
+}  // namespace bemb200

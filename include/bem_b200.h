@@ -55,7 +55,8 @@ typedef struct {
   double tol;                /* absolute GMRES tolerance on the scaled system (solver_tol) */
   int32_t max_iter;          /* GMRES iteration cap (solver_max_iter) */
   int32_t device;            /* CUDA device ordinal */
-  int32_t reserved[5];
+  int32_t tol_relative;      /* 0: stop at |A x - b| <= tol (reference semantics); 1: at <= tol*|b| */
+  int32_t reserved[4];
 } bem_gpu_opts;
 
 /* One boundary-value problem.  The DOF table is what the reference's setNodeFaceIndices()
@@ -144,6 +145,11 @@ double bem_gpu_scale_factor(const bem_gpu_ctx* ctx);                  /* L */
 int bem_gpu_near_row(bem_gpu_ctx* ctx, int32_t point, int32_t cap, int32_t* dof, double* wG, double* wGn);
 int bem_gpu_face_leaf(bem_gpu_ctx* ctx, int32_t* level, double* corner); /* [n_faces], [3*n_faces] */
 int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out /*[8]: nodes, leaves, depth, added, m2l, near, nnz, targets*/);
+
+/* Host-only inspection of the set-up plan (no GPU needed): builds the octree, lists and
+ * near-field sparsity for desc with opts and reports, per face, the level and lower corner
+ * of the leaf bucket holding it (-1 if none), plus stats[8] as bem_gpu_tree_stats. */
+int bem_plan_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* desc, int32_t* face_level, double* face_corner, int64_t* stats);
 
 /* Kernel timing of the last mat-vec executed through bem_gpu_profile_matvec: per stage
  * milliseconds [p2m, m2m, m2l, l2l, near+l2p, total] measured with CUDA events. */

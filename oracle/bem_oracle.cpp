@@ -1128,20 +1128,26 @@ int oracle_solve(void* h, const double* known, const double* x0_in, double tol, 
     return s;
   };
   auto nrm = [&](const std::vector<double>& a) { return std::sqrt(dot(a, a)); };
-  std::vector<double> x0(N, 0.0);
-  if (x0_in) x0.assign(x0_in, x0_in + N);
-  // gmres(return_A_dot_v, b, x0, 1)
-  std::vector<std::vector<double>> V, H;  // H[i][j] rows (n+1) x n
-  std::vector<double> r0 = Aop(x0);
-  for (int i = 0; i < N; ++i) r0[i] = b[i] - r0[i];
-  double beta = nrm(r0);
+  std::vector<double> x(N, 0.0);
+  if (x0_in) x.assign(x0_in, x0_in + N);
+  // run_gmres: restart from the current x after a saturation break
+  // (BEM_solveBVP_GMRES_FMM.hpp:2275-2355, gmres ctor basic_linear_systems.hpp:3339)
   int iters = 0;
   double r_true = 1e300, err = 1e300;
-  std::vector<double> x = x0;
-  if (beta == 0.0) {
-    r_true = 0;
-    err = 0;
-  } else {
+  const int restart_max = 100;  // solver_restart default (main_time_domain.cpp:51)
+  while (iters < max_iter && r_true > tol) {
+    const int remaining = max_iter - iters;
+    const int k_cycle_max = std::min(restart_max, remaining);
+    std::vector<double> xb = x;
+    std::vector<double> r0 = Aop(xb);
+    for (int i = 0; i < N; ++i) r0[i] = b[i] - r0[i];
+    double beta = nrm(r0);
+    if (beta == 0.0) {
+      r_true = 0.0;
+      err = 0.0;
+      break;
+    }
+    std::vector<std::vector<double>> V;
     std::vector<double> v0(N);
     for (int i = 0; i < N; ++i) v0[i] = r0[i] / beta;
     V.push_back(v0);
@@ -1159,7 +1165,6 @@ int oracle_solve(void* h, const double* known, const double* x0_in, double tol, 
       hcol[n] = nrm(w);
       for (int k = 0; k < N; ++k) w[k] /= hcol[n];
       V.push_back(w);
-      // Givens update
       for (int i = 0; i < n - 1; ++i) {
         double t = std::fma(cs[i], hcol[i], sn[i] * hcol[i + 1]);
         hcol[i + 1] = std::fma(cs[i], hcol[i + 1], -sn[i] * hcol[i]);
@@ -1195,32 +1200,30 @@ int oracle_solve(void* h, const double* known, const double* x0_in, double tol, 
         for (int j = i + 1; j < n; ++j) s -= Rm[j][i] * y[j];
         y[i] = s / Rm[i][i];
       }
-      x = x0;
+      x = xb;
       for (int i = 0; i < n; ++i)
         for (int k = 0; k < N; ++k) x[k] = std::fma(y[i], V[i][k], x[k]);
     };
+    auto true_residual = [&]() {
+      std::vector<double> ax = Aop(x);
+      for (int i = 0; i < N; ++i) ax[i] -= b[i];
+      return nrm(ax);
+    };
     add_basis();
-    iters = 1;
+    iters += 1;
     int sat = 0;
     while (true) {
       add_basis();
       ++iters;
       if (err <= tol * 10.) {
         update_solution();
-        std::vector<double> ax = Aop(x);
-        for (int i = 0; i < N; ++i) ax[i] -= b[i];
-        r_true = nrm(ax);
+        r_true = true_residual();
         if (r_true <= tol) break;
         if (sat++ >= 5) break;
       }
-      if (iters >= max_iter) {
+      if (iters >= max_iter && (int)Rm.size() >= k_cycle_max) {
         update_solution();
-        if (err <= tol * 10.) {
-          std::vector<double> ax = Aop(x);
-          for (int i = 0; i < N; ++i) ax[i] -= b[i];
-          r_true = nrm(ax);
-        } else
-          r_true = err;
+        r_true = (err <= tol * 10.) ? true_residual() : err;
         break;
       }
     }

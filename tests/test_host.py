@@ -1,0 +1,70 @@
+"""Host-side logic of the product library (no GPU): C-ABI exports, DOF keys and the
+set-up plan (octree, lists, near-field sparsity) against the oracle."""
+import re
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from bem_for_nonlinear_waves_b200 import build_dofs, make_tank
+from bem_for_nonlinear_waves_b200.bvp import inspect_plan
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "bem_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(bem_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_header_symbol(product_lib):
+    names = header_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(product_lib, n), n
+
+
+TANKS = [dict(h=0.1), dict(h=0.1, noise_sigma=0.02, seed=3), dict(h=0.05), dict(length=1.3, width=0.7, depth=0.4, h=0.1)]
+
+
+@pytest.mark.parametrize("spec", TANKS)
+def test_dofs_match_oracle(product_lib, oracle_mod, spec):
+    t = make_tank(**spec)
+    a = build_dofs(t.X, t.tri, t.face_dirichlet)
+    b = oracle_mod.build_dofs(t.X, t.tri, t.face_dirichlet)
+    for k in ("dof_point", "dof_face", "dof_kind", "face_dof", "point_flags"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    # corner points carry one Dirichlet key plus one constrained key per Neumann face
+    kinds = np.bincount(a["dof_kind"], minlength=3)
+    assert kinds[0] > 0 and kinds[1] > 0 and kinds[2] > 0
+
+
+@pytest.mark.parametrize("spec,p", [(TANKS[0], 8), (TANKS[1], 10), (TANKS[2], 8), (TANKS[3], 6)])
+def test_plan_tree_and_lists_match_oracle(product_lib, oracle_mod, spec, p):
+    t = make_tank(**spec)
+    d = build_dofs(t.X, t.tri, t.face_dirichlet)
+    lv, corner, st = inspect_plan(t.X, t.tri, t.face_dirichlet, d, expansion_order=p)
+    o = oracle_mod.Oracle(t.X, t.tri, t.face_dirichlet, d, p=p)
+    ost = o.stats()
+    olv, oc = o.face_leaf()
+    np.testing.assert_array_equal(lv, olv)
+    np.testing.assert_array_equal(corner, oc)  # bit-exact bucket bounds
+    for k in ("nodes", "leaves", "depth", "n_added", "m2l_pairs", "near_pairs", "nnz"):
+        assert st[k] == ost[k], k
+
+
+def test_build_dofs_rejects_bad_connectivity(product_lib):
+    t = make_tank(h=0.25)
+    tri = t.tri.copy()
+    tri[0, 0] = t.X.shape[0] + 5
+    with pytest.raises(ValueError):
+        build_dofs(t.X, tri, t.face_dirichlet)
+
+
+def test_plan_rejects_nonfinite_coordinates(product_lib):
+    t = make_tank(h=0.25)
+    d = build_dofs(t.X, t.tri, t.face_dirichlet)
+    X = t.X.copy()
+    X[3, 1] = np.nan
+    with pytest.raises(ValueError):
+        inspect_plan(X, t.tri, t.face_dirichlet, d)
