@@ -43,7 +43,7 @@ class BEM_BVP:
     """GMRES-FMM Laplace BVP on one B200."""
 
     def __init__(self, X, tri, face_dirichlet, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30,
-                 fmm_max_level=7, solver_tol=1e-9, solver_max_iter=500, device=0, dofs=None, tol_relative=False):
+                 fmm_max_level=7, solver_tol=1e-9, solver_max_iter=500, device=0, dofs=None, tol_relative=False, preconditioner="none"):
         self.lib = L.load()
         if not self.lib.bem_gpu_is_available():
             raise RuntimeError("no sm_100 CUDA device visible: the GMRES-FMM solver runs only on the GPU")
@@ -60,6 +60,7 @@ class BEM_BVP:
         o.max_iter = int(solver_max_iter)
         o.device = int(device)
         o.tol_relative = 1 if tol_relative else 0
+        o.preconditioner = {"none": 0, "jacobi": 1}[preconditioner]
         self.opts = o
         self.ctx = self.lib.bem_gpu_create(ctypes.byref(o))
         if not self.ctx:
@@ -178,9 +179,13 @@ class BEM_BVP:
         return {k: int(v) for k, v in zip(keys, out)}
 
     def matvec_time_ms(self, repeats=10):
+        return self.profile_matvec(repeats)["total"]
+
+    def profile_matvec(self, repeats=10):
+        """Per-stage mat-vec time in ms (CUDA events on the solver stream)."""
         st = np.zeros(6)
         self._check(self.lib.bem_gpu_profile_matvec(self.ctx, int(repeats), L.ptr(st, L.P_dbl)), "profile")
-        return float(st[5])
+        return dict(zip(["p2m", "m2m", "m2l", "l2l", "targets", "total"], map(float, st)))
 
 
 def inspect_plan(X, tri, face_dirichlet, dofs=None, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30,

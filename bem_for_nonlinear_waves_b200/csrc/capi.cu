@@ -74,10 +74,18 @@ struct bem_gpu_ctx {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   // Krylov
-  DBuf<double> V, w, hdev, partial, xdev, bdev, rdev, ydev;
+  DBuf<double> V, w, hdev, partial, xdev, bdev, rdev, ydev, tmp, dinv;
   int V_cols = 0;
+  int graph_kernels = 0;
+  // accounting of the current setup + solve
+  int64_t h2d = 0, d2h = 0, launches = 0;
+  int64_t setup_h2d = 0, setup_launches = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // setup device start/end, solve start/end
+  float setup_dev_ms = 0.f;
 
   ~bem_gpu_ctx() {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
     if (stream) cudaStreamDestroy(stream);
@@ -163,7 +171,13 @@ int fill_quadrature(bem_gpu_ctx* ctx) {
 
 // one operator application on device state: densities already in ctx->phi/phin
 void run_fmm(bem_gpu_ctx* ctx, double* rows, double* gphin, double* gnphi) {
-  launch_matvec(ctx->plan.opt.p, ctx->args(ctx->phi.p, ctx->phin.p, rows, gphin, gnphi), ctx->stream);
+  ctx->launches += launch_matvec(ctx->plan.opt.p, ctx->args(ctx->phi.p, ctx->phin.p, rows, gphin, gnphi), ctx->stream);
+}
+
+template <typename T>
+cudaError_t up(bem_gpu_ctx* ctx, DBuf<T>& b, const std::vector<T>& v) {
+  ctx->h2d += (int64_t)(sizeof(T) * v.size());
+  return b.upload(v, ctx->stream);
 }
 
 int build_graph(bem_gpu_ctx* ctx) {
@@ -180,6 +194,16 @@ int build_graph(bem_gpu_ctx* ctx) {
   run_fmm(ctx, ctx->mv_out.p, nullptr, nullptr);
   CK(cudaStreamEndCapture(ctx->stream, &ctx->graph));
   CK(cudaGraphInstantiate(&ctx->graph_exec, ctx->graph, 0));
+  size_t nn = 0;
+  CK(cudaGraphGetNodes(ctx->graph, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (nn) CK(cudaGraphGetNodes(ctx->graph, nodes.data(), &nn));
+  ctx->graph_kernels = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType ty;
+    CK(cudaGraphNodeGetType(nd, &ty));
+    if (ty == cudaGraphNodeTypeKernel) ++ctx->graph_kernels;
+  }
   return BEM_OK;
 }
 
@@ -227,6 +251,11 @@ bem_gpu_ctx* bem_gpu_create(const bem_gpu_opts* opts) {
     delete ctx;
     return nullptr;
   }
+  for (auto& e : ctx->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      delete ctx;
+      return nullptr;
+    }
   return ctx;
 }
 
@@ -249,6 +278,7 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   if (!ctx || !d) return BEM_ERR_INVALID_ARGUMENT;
   CK(cudaSetDevice(ctx->opts.device));
   ctx->ready = false;
+  ctx->h2d = ctx->d2h = ctx->launches = 0;
   const double t0 = now_s();
   PlanOptions po;
   po.p = ctx->opts.expansion_order;
@@ -311,34 +341,34 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   ctx->chunk = std::min(max_ndof, (smem_cap - ctx->max_ntgt * 16) / 16);
   configure_targets_smem(P.opt.p, (ctx->chunk + ctx->max_ntgt) * 16);
 
-  CK(ctx->Xs.upload(P.Xs, s));
-  CK(ctx->e_q.upload(P.e_q, s));
-  CK(ctx->e_W.upload(P.e_W, s));
-  CK(ctx->e_n.upload(P.e_n, s));
-  CK(ctx->e_near.upload(P.e_near, s));
-  CK(ctx->e_dof.upload(P.e_dof, s));
-  CK(ctx->e_vtx.upload(P.e_vtx, s));
-  CK(ctx->node_X.upload(nX, s));
-  CK(ctx->node_fb.upload(nfb, s));
-  CK(ctx->node_fe.upload(nfe, s));
-  CK(ctx->child_begin.upload(cb, s));
-  CK(ctx->child_end.upload(ce, s));
-  CK(ctx->node_children.upload(P.node_children, s));
-  CK(ctx->leaves.upload(P.leaves, s));
-  CK(ctx->level_parents.upload(lp, s));
-  CK(ctx->m2l_targets.upload(mt, s));
-  CK(ctx->m2l_off.upload(P.m2l_off, s));
-  CK(ctx->m2l_src.upload(P.m2l_src, s));
-  CK(ctx->nb_dofs.upload(P.nb_dofs, s));
-  CK(ctx->nb_targets.upload(P.nb_targets, s));
-  CK(ctx->nb_ranges.upload(P.nb_ranges, s));
-  CK(ctx->dof_inc_off.upload(P.dof_inc_off, s));
-  CK(ctx->dof_inc.upload(P.dof_inc, s));
-  CK(ctx->point_dof_off.upload(P.point_dof_off, s));
-  CK(ctx->point_dof.upload(P.point_dof, s));
-  CK(ctx->dof_kind.upload(P.dof_kind, s));
-  CK(ctx->dof_point.upload(P.dof_point, s));
-  CK(ctx->blocks.upload(bd, s));
+  CK(up(ctx, ctx->Xs, P.Xs));
+  CK(up(ctx, ctx->e_q, P.e_q));
+  CK(up(ctx, ctx->e_W, P.e_W));
+  CK(up(ctx, ctx->e_n, P.e_n));
+  CK(up(ctx, ctx->e_near, P.e_near));
+  CK(up(ctx, ctx->e_dof, P.e_dof));
+  CK(up(ctx, ctx->e_vtx, P.e_vtx));
+  CK(up(ctx, ctx->node_X, nX));
+  CK(up(ctx, ctx->node_fb, nfb));
+  CK(up(ctx, ctx->node_fe, nfe));
+  CK(up(ctx, ctx->child_begin, cb));
+  CK(up(ctx, ctx->child_end, ce));
+  CK(up(ctx, ctx->node_children, P.node_children));
+  CK(up(ctx, ctx->leaves, P.leaves));
+  CK(up(ctx, ctx->level_parents, lp));
+  CK(up(ctx, ctx->m2l_targets, mt));
+  CK(up(ctx, ctx->m2l_off, P.m2l_off));
+  CK(up(ctx, ctx->m2l_src, P.m2l_src));
+  CK(up(ctx, ctx->nb_dofs, P.nb_dofs));
+  CK(up(ctx, ctx->nb_targets, P.nb_targets));
+  CK(up(ctx, ctx->nb_ranges, P.nb_ranges));
+  CK(up(ctx, ctx->dof_inc_off, P.dof_inc_off));
+  CK(up(ctx, ctx->dof_inc, P.dof_inc));
+  CK(up(ctx, ctx->point_dof_off, P.point_dof_off));
+  CK(up(ctx, ctx->point_dof, P.point_dof));
+  CK(up(ctx, ctx->dof_kind, P.dof_kind));
+  CK(up(ctx, ctx->dof_point, P.dof_point));
+  CK(up(ctx, ctx->blocks, bd));
   CK(ctx->M.alloc((size_t)nb * 2 * NC));
   CK(ctx->L.alloc((size_t)nb * 2 * NC));
   CK(cudaMemsetAsync(ctx->M.p, 0, sizeof(double2) * ctx->M.n, s));
@@ -357,6 +387,8 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   CK(cudaMemsetAsync(ctx->GPhin.p, 0, sizeof(double) * P.np, s));
   CK(cudaMemsetAsync(ctx->GnPhi.p, 0, sizeof(double) * P.np, s));
 
+  // device part of the set-up starts here (inputs resident)
+  CK(cudaEventRecord(ctx->ev[0], s));
   // near-field weights
   NearArgs na;
   na.n_blocks = (int)P.blocks.size();
@@ -378,10 +410,32 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   launch_densities(N, 2, nullptr, nullptr, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, s);
   run_fmm(ctx, nullptr, ctx->GPhin.p, ctx->GnPhi.p);
   launch_diag(N, ctx->dof_point.p, ctx->GnPhi.p, ctx->diag.p, s);
+  ctx->launches += 3;
   CK(cudaGetLastError());
+  // right-Jacobi scaling from the near-field diagonal entries
+  {
+    std::vector<int> bop(P.np), rop(P.np);
+    for (int p = 0; p < P.np; ++p) {
+      bop[p] = std::max(P.block_of_point[p], 0);
+      rop[p] = std::max(P.row_of_point[p], 0);
+    }
+    DBuf<int> d_bop, d_rop;
+    CK(up(ctx, d_bop, bop));
+    CK(up(ctx, d_rop, rop));
+    CK(ctx->dinv.alloc(N));
+    launch_jacobi(N, ctx->dof_point.p, ctx->dof_kind.p, ctx->diag.p, d_bop.p, d_rop.p, ctx->blocks.p, ctx->nb_dofs.p, ctx->WG.p, ctx->WGn.p,
+                  ctx->dinv.p, s);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+  }
+  CK(cudaEventRecord(ctx->ev[1], s));
   int rc = build_graph(ctx);
   if (rc != BEM_OK) return rc;
   CK(cudaStreamSynchronize(s));
+  CK(cudaEventElapsedTime(&ctx->setup_dev_ms, ctx->ev[0], ctx->ev[1]));
+  ctx->setup_h2d = ctx->h2d;
+  ctx->setup_launches = ctx->launches;
   ctx->time_setup = now_s() - t0;
   ctx->ready = true;
   return BEM_OK;
@@ -552,6 +606,10 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   const Plan& P = ctx->plan;
   const int N = P.ndof;
   cudaStream_t s = ctx->stream;
+  ctx->h2d = ctx->setup_h2d;
+  ctx->d2h = 0;
+  ctx->launches = ctx->setup_launches;
+  const bool jacobi = ctx->opts.preconditioner == 1;
   double tol = ctx->opts.tol;
   const int max_iter = ctx->opts.max_iter;
   for (int i = 0; i < N; ++i)
@@ -563,6 +621,8 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   std::vector<double> ks(N);
   for (int i = 0; i < N; ++i) ks[i] = (P.dof_kind[i] == 0) ? known[i] : known[i] * P.L;
   CK(cudaMemcpyAsync(ctx->known_s.p, ks.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  ctx->h2d += 8LL * N;
+  CK(cudaEventRecord(ctx->ev[2], s));
   const int cols = max_iter + 2;
   if (ctx->V_cols < cols || ctx->V.n < (size_t)cols * N) {
     CK(ctx->V.alloc((size_t)cols * N));
@@ -573,6 +633,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     CK(ctx->xdev.alloc(N));
     CK(ctx->bdev.alloc(N));
     CK(ctx->rdev.alloc(N));
+    CK(ctx->tmp.alloc(N));
   }
   CK(ctx->hdev.alloc((size_t)3 * cols + 8));
   CK(ctx->ydev.alloc(cols));
@@ -581,31 +642,45 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   // b = -(A*0 - b) with corner rows replaced by the point's phi (:2025-2047)
   launch_densities(N, 1, nullptr, ctx->known_s.p, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, s);
   run_fmm(ctx, ctx->rows.p, nullptr, nullptr);
+  ctx->launches += 1;
   ++matvecs;
   std::vector<double> b(N);
   CK(cudaMemcpyAsync(b.data(), ctx->rows.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+  ctx->d2h += 8LL * N;
   CK(cudaStreamSynchronize(s));
   for (int i = 0; i < N; ++i) {
     b[i] = -b[i];
     if (P.dof_kind[i] == 2) b[i] = (P.corner_src_dof[i] >= 0) ? known[P.corner_src_dof[i]] : 0.0;
   }
   CK(cudaMemcpyAsync(ctx->bdev.p, b.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  ctx->h2d += 8LL * N;
   if (ctx->opts.tol_relative) {
     double bn = 0.0;
     for (int i = 0; i < N; ++i) bn = std::fma(b[i], b[i], bn);
     tol *= std::sqrt(bn);
   }
-  if (x0)
+  if (x0) {
     CK(cudaMemcpyAsync(ctx->xdev.p, x0, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-  else
+    ctx->h2d += 8LL * N;
+  } else
     CK(cudaMemsetAsync(ctx->xdev.p, 0, sizeof(double) * N, s));
 
   auto matvec = [&](const double* din, double* dout) -> int {
     ++matvecs;
+    ctx->launches += ctx->graph_kernels;
     return bem_gpu_matvec_device(ctx, din, dout);
+  };
+  // operator seen by GMRES: A D^{-1} with right Jacobi scaling, else A
+  auto opmatvec = [&](const double* din, double* dout) -> int {
+    if (!jacobi) return matvec(din, dout);
+    launch_mul(N, ctx->dinv.p, din, ctx->tmp.p, s);
+    ctx->launches += 1;
+    return matvec(ctx->tmp.p, dout);
   };
   auto norm_of = [&](const double* v, double* out) -> int {
     launch_mdot(v, N, 1, v, N, ctx->partial.p, ctx->hdev.p, s);
+    ctx->launches += 2;
+    ctx->d2h += 8;
     CK(cudaMemcpyAsync(out, ctx->hdev.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     *out = std::sqrt(*out);
@@ -619,6 +694,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     // r0 = b - A x
     if ((rc = matvec(ctx->xdev.p, ctx->rdev.p)) != BEM_OK) return rc;
     launch_axpby(N, 1.0, ctx->bdev.p, -1.0, ctx->rdev.p, s);  // r = b - r
+    ctx->launches += 1;
     double beta = 0.0;
     if ((rc = norm_of(ctx->rdev.p, &beta)) != BEM_OK) return rc;
     if (!std::isfinite(beta)) {
@@ -631,6 +707,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
       break;
     }
     launch_axpby(N, 1.0 / beta, ctx->rdev.p, 0.0, ctx->V.p, s);
+    ctx->launches += 1;
     std::vector<double> cs, sn, g{beta};
     std::vector<std::vector<double>> Rc;
     int n = 0;  // basis vectors beyond V[0] added in this cycle
@@ -638,7 +715,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
       double* vk = ctx->V.p + (size_t)n * N;
       double* vn = ctx->V.p + (size_t)(n + 1) * N;
       int r;
-      if ((r = matvec(vk, ctx->w.p)) != BEM_OK) return r;
+      if ((r = opmatvec(vk, ctx->w.p)) != BEM_OK) return r;
       const int k = n + 1;
       double* h1 = ctx->hdev.p;
       double* h2 = ctx->hdev.p + cols;
@@ -653,6 +730,8 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
       double hn2 = 0.0;
       CK(cudaMemcpyAsync(&hn2, hn, sizeof(double), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
+      ctx->launches += 8;
+      ctx->d2h += 8LL * (2 * k + 1);
       std::vector<double> hcol(k + 1);
       for (int i = 0; i < k; ++i) hcol[i] = hh[i] + hh[cols + i];
       hcol[k] = std::sqrt(hn2);
@@ -661,6 +740,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
         return BEM_ERR_NAN;
       }
       launch_axpby(N, hcol[k] > 0 ? 1.0 / hcol[k] : 0.0, ctx->w.p, 0.0, vn, s);
+      ctx->launches += 1;
       for (int i = 0; i < k - 1; ++i) {
         const double t = std::fma(cs[i], hcol[i], sn[i] * hcol[i + 1]);
         hcol[i + 1] = std::fma(cs[i], hcol[i + 1], -sn[i] * hcol[i]);
@@ -701,13 +781,23 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
       }
       for (auto& v : y) v = -v;  // maxpy subtracts
       CK(cudaMemcpyAsync(ctx->ydev.p, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
-      launch_maxpy(ctx->V.p, N, k, ctx->ydev.p, ctx->xdev.p, N, s);
+      ctx->h2d += 8LL * k;
+      if (!jacobi) {
+        launch_maxpy(ctx->V.p, N, k, ctx->ydev.p, ctx->xdev.p, N, s);
+        ctx->launches += 1;
+      } else {  // x = x_base + D^{-1} (V y)
+        CK(cudaMemsetAsync(ctx->tmp.p, 0, sizeof(double) * N, s));
+        launch_maxpy(ctx->V.p, N, k, ctx->ydev.p, ctx->tmp.p, N, s);
+        launch_add_mul(N, ctx->xdev.p, ctx->dinv.p, ctx->tmp.p, ctx->xdev.p, s);
+        ctx->launches += 2;
+      }
       return BEM_OK;
     };
     auto true_res = [&](double* out) -> int {
       int r;
       if ((r = matvec(ctx->xdev.p, ctx->rdev.p)) != BEM_OK) return r;
       launch_axpby(N, -1.0, ctx->bdev.p, 1.0, ctx->rdev.p, s);
+      ctx->launches += 1;
       return norm_of(ctx->rdev.p, out);
     };
     // x_base is committed into xdev only when the solution is updated; keep a copy
@@ -744,9 +834,13 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
       }
     }
   }
+  CK(cudaEventRecord(ctx->ev[3], s));
   std::vector<double> x(N);
   CK(cudaMemcpyAsync(x.data(), ctx->xdev.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+  ctx->d2h += 8LL * N;
   CK(cudaStreamSynchronize(s));
+  float solve_dev_ms = 0.f;
+  CK(cudaEventElapsedTime(&solve_dev_ms, ctx->ev[2], ctx->ev[3]));
   bool finite = true;
   for (int i = 0; i < N; ++i) {
     finite = finite && std::isfinite(x[i]);
@@ -773,6 +867,10 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     stats->n_nodes = (int)nodes;
     stats->n_leaves = (int)P.leaves.size();
     stats->matvecs = matvecs;
+    stats->time_device_s = 1e-3 * ((double)ctx->setup_dev_ms + (double)solve_dev_ms);
+    stats->h2d_bytes = ctx->h2d;
+    stats->d2h_bytes = ctx->d2h;
+    stats->kernel_launches = ctx->launches;
   }
   if (!finite) {
     ctx->err = "non-finite solution";
@@ -791,21 +889,48 @@ int bem_gpu_solve_bvp(bem_gpu_ctx* ctx, const bem_bvp_desc* desc, const double* 
 int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms) {
   if (!ctx || !stage_ms || repeats < 1) return BEM_ERR_INVALID_ARGUMENT;
   if (!ctx->ready) return BEM_ERR_NOT_READY;
+  CK(cudaSetDevice(ctx->opts.device));
   cudaStream_t s = ctx->stream;
+  const int N = ctx->plan.ndof;
+  // representative input: unit unknowns
+  std::vector<double> one(N, 1.0);
+  CK(cudaMemcpyAsync(ctx->mv_in.p, one.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  launch_densities(N, 0, ctx->mv_in.p, nullptr, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, s);
+  run_fmm(ctx, ctx->mv_out.p, nullptr, nullptr);
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  CK(cudaEventRecord(e0, s));
-  for (int r = 0; r < repeats; ++r) CK(cudaGraphLaunch(ctx->graph_exec, s));
-  CK(cudaEventRecord(e1, s));
-  CK(cudaEventSynchronize(e1));
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, e0, e1);
+  const int stages[5] = {STAGE_P2M, STAGE_M2M, STAGE_M2L, STAGE_L2L, STAGE_TARGETS};
+  for (int k = 0; k < 6; ++k) {
+    CK(cudaEventRecord(e0, s));
+    for (int r = 0; r < repeats; ++r) {
+      if (k < 5)
+        launch_matvec(ctx->plan.opt.p, ctx->args(ctx->phi.p, ctx->phin.p, ctx->mv_out.p, nullptr, nullptr), s, stages[k]);
+      else
+        CK(cudaGraphLaunch(ctx->graph_exec, s));
+    }
+    CK(cudaEventRecord(e1, s));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    stage_ms[k] = ms / repeats;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  for (int i = 0; i < 6; ++i) stage_ms[i] = 0.0;
-  stage_ms[5] = ms / repeats;
   return BEM_OK;
+}
+
+double bem_gpu_fp64_peak_tflops(int32_t device) {
+  if (cudaSetDevice(device) != cudaSuccess) return 0.0;
+  cudaStream_t s;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return 0.0;
+  double* sink = nullptr;
+  if (cudaMalloc(&sink, sizeof(double)) != cudaSuccess) return 0.0;
+  const double tf = fp64_probe_tflops(s, sink);
+  cudaStreamSynchronize(s);
+  cudaFree(sink);
+  cudaStreamDestroy(s);
+  return tf;
 }
 
 }  // extern "C"

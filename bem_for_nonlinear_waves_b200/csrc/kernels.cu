@@ -620,32 +620,109 @@ __global__ void k_scale_inv(int n, const double* __restrict__ x, const double* _
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = x[i] * inv;
 }
 
+// y = a .* x
+__global__ void k_mul(int n, const double* __restrict__ a, const double* __restrict__ x, double* __restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a[i] * x[i];
+}
+
+// y = xb + a .* u
+__global__ void k_add_mul(int n, const double* __restrict__ xb, const double* __restrict__ a, const double* __restrict__ u,
+                          double* __restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = xb[i] + a[i] * u[i];
+}
+
+// Inverse of the operator's diagonal entries A_ii, read from the cached near-field row of
+// the DOF's own point: Dirichlet rows (unknown phin) w_G(i,i); Neumann rows (unknown phi)
+// -(w_Gn(i,i) + diag_i); constraint rows 1.
+__global__ void k_jacobi(int n, const int* __restrict__ dof_point, const int* __restrict__ dof_kind, const double* __restrict__ diag,
+                         const int* __restrict__ block_of_point, const int* __restrict__ row_of_point, const NearBlockDev* __restrict__ blocks,
+                         const int* __restrict__ nb_dofs, const double* __restrict__ WG, const double* __restrict__ WGn,
+                         double* __restrict__ dinv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int k = dof_kind[i];
+    double a = 1.0;
+    if (k != 2) {
+      const int t = dof_point[i];
+      const NearBlockDev B = blocks[block_of_point[t]];
+      int lo = 0, hi = B.ndof - 1, j = -1;
+      while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int v = nb_dofs[B.dof_off + mid];
+        if (v < i)
+          lo = mid + 1;
+        else if (v > i)
+          hi = mid - 1;
+        else {
+          j = mid;
+          break;
+        }
+      }
+      const int64_t w = B.w_off + (int64_t)row_of_point[t] * B.ndof + j;
+      if (j >= 0) a = (k == 0) ? WG[w] : -(WGn[w] + diag[i]);
+    }
+    dinv[i] = (fabs(a) > 1e-300) ? 1.0 / a : 1.0;
+  }
+}
+
+// FP64 FMA throughput probe: 8 independent FMA chains per thread.
+__global__ void k_fp64_probe(int iters, double seed, double* __restrict__ sink) {
+  double a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6, a7 = a0 + 7;
+  const double m = 0.999999, c = 1e-7;
+  for (int i = 0; i < iters; ++i) {
+    a0 = fma(a0, m, c);
+    a1 = fma(a1, m, c);
+    a2 = fma(a2, m, c);
+    a3 = fma(a3, m, c);
+    a4 = fma(a4, m, c);
+    a5 = fma(a5, m, c);
+    a6 = fma(a6, m, c);
+    a7 = fma(a7, m, c);
+  }
+  const double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == 12345.678) sink[0] = s;
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 template <int P>
-void launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st) {
+int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
   constexpr int NC = ncoef(P);
   const int tpb_coef = ((NC + 31) / 32) * 32;
-  if (a.n_leaves > 0)
+  int launches = 0;
+  if ((stages & STAGE_P2M) && a.n_leaves > 0) {
     k_p2m<P><<<a.n_leaves, 128, 0, st>>>(a.leaves, a.node_fb, a.node_fe, a.node_X, a.e_q, a.e_W, a.e_n, a.e_dof, a.phi, a.phin, a.M);
-  for (int l = a.n_levels - 1; l >= 0; --l) {
-    const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
-    if (cnt > 0)
-      k_m2m<P><<<cnt, tpb_coef, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.M);
+    ++launches;
   }
-  cudaMemsetAsync(a.L, 0, sizeof(double2) * 2 * NC * (size_t)a.n_nodes, st);
-  if (a.n_m2l_targets > 0)
-    k_m2l<P><<<a.n_m2l_targets, tpb_coef, 0, st>>>(a.m2l_targets, a.m2l_off, a.m2l_src, a.node_X, a.M, a.L);
-  for (int l = 0; l < a.n_levels; ++l) {
-    const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
-    if (cnt > 0)
-      k_l2l<P><<<cnt, tpb_coef, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.L);
+  if (stages & STAGE_M2M)
+    for (int l = a.n_levels - 1; l >= 0; --l) {
+      const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
+      if (cnt > 0) {
+        k_m2m<P><<<cnt, tpb_coef, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.M);
+        ++launches;
+      }
+    }
+  if (stages & STAGE_M2L) {
+    cudaMemsetAsync(a.L, 0, sizeof(double2) * 2 * NC * (size_t)a.n_nodes, st);
+    if (a.n_m2l_targets > 0) {
+      k_m2l<P><<<a.n_m2l_targets, tpb_coef, 0, st>>>(a.m2l_targets, a.m2l_off, a.m2l_src, a.node_X, a.M, a.L);
+      ++launches;
+    }
   }
-  if (a.n_blocks > 0) {
+  if (stages & STAGE_L2L)
+    for (int l = 0; l < a.n_levels; ++l) {
+      const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
+      if (cnt > 0) {
+        k_l2l<P><<<cnt, tpb_coef, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.L);
+        ++launches;
+      }
+    }
+  if ((stages & STAGE_TARGETS) && a.n_blocks > 0) {
     const size_t shm = sizeof(double2) * (size_t)(a.chunk + a.max_ntgt);
     k_targets<P><<<a.n_blocks, 128, shm, st>>>(a.blocks, a.nb_dofs, a.nb_targets, a.WG, a.WGn, a.Xs, a.node_X, a.L, a.phi, a.phin,
                                                a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.GPhin, a.GnPhi, a.chunk);
+    ++launches;
   }
+  return launches;
 }
 
 template <int P>
@@ -653,16 +730,17 @@ void set_target_smem(int bytes) {
   cudaFuncSetAttribute(k_targets<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-void launch_matvec(int p, const MatvecArgs& a, cudaStream_t st) {
+int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages) {
   switch (p) {
 #define BEMB200_CASE(PP) \
   case PP:               \
-    launch_matvec_fmm<PP>(a, st); break;
+    return launch_matvec_fmm<PP>(a, st, stages);
     BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5) BEMB200_CASE(6)
     BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10) BEMB200_CASE(11) BEMB200_CASE(12)
 #undef BEMB200_CASE
     default: break;
   }
+  return 0;
 }
 
 void configure_targets_smem(int p, int bytes) {
@@ -714,6 +792,45 @@ void launch_axpby(int n, double a, const double* x, double b, double* y, cudaStr
   int g = (n + 255) / 256;
   if (g > 1184) g = 1184;
   k_axpby<<<g > 0 ? g : 1, 256, 0, st>>>(n, a, x, b, y);
+}
+
+void launch_mul(int n, const double* a, const double* x, double* y, cudaStream_t st) {
+  int g = (n + 255) / 256;
+  if (g > 1184) g = 1184;
+  k_mul<<<g > 0 ? g : 1, 256, 0, st>>>(n, a, x, y);
+}
+
+void launch_add_mul(int n, const double* xb, const double* a, const double* u, double* y, cudaStream_t st) {
+  int g = (n + 255) / 256;
+  if (g > 1184) g = 1184;
+  k_add_mul<<<g > 0 ? g : 1, 256, 0, st>>>(n, xb, a, u, y);
+}
+
+void launch_jacobi(int n, const int* dof_point, const int* dof_kind, const double* diag, const int* block_of_point, const int* row_of_point,
+                   const NearBlockDev* blocks, const int* nb_dofs, const double* WG, const double* WGn, double* dinv, cudaStream_t st) {
+  int g = (n + 255) / 256;
+  k_jacobi<<<g > 0 ? g : 1, 256, 0, st>>>(n, dof_point, dof_kind, diag, block_of_point, row_of_point, blocks, nb_dofs, WG, WGn, dinv);
+}
+
+double fp64_probe_tflops(cudaStream_t st, double* sink) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int iters = 1 << 14, blocks = sms * 8, threads = 256;
+  k_fp64_probe<<<blocks, threads, 0, st>>>(iters, 1.0, sink);  // warm-up
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  k_fp64_probe<<<blocks, threads, 0, st>>>(iters, 2.0, sink);
+  cudaEventRecord(e1, st);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
+  return flops / (ms * 1e-3) / 1e12;
 }
 
 void launch_scale_inv(int n, const double* x, const double* s, double* y, cudaStream_t st) {

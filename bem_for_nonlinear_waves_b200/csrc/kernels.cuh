@@ -76,7 +76,9 @@ struct NearArgs {
 
 void upload_quadrature(const double dv[6][4], const double gw[25][3], cudaStream_t s);
 void configure_targets_smem(int p, int bytes);
-void launch_matvec(int p, const MatvecArgs& a, cudaStream_t st);
+enum { STAGE_P2M = 1, STAGE_M2M = 2, STAGE_M2L = 4, STAGE_L2L = 8, STAGE_TARGETS = 16, STAGE_ALL = 31 };
+// returns the number of kernels launched
+int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages = STAGE_ALL);
 void launch_densities(int n, int mode, const double* x, const double* known, const int* kind, double* phi, double* phin, cudaStream_t st);
 void launch_near_weights(const NearArgs& a, cudaStream_t st);
 void launch_diag(int n, const int* dof_point, const double* GnPhi, double* diag, cudaStream_t st);
@@ -85,5 +87,10 @@ void launch_mdot(const double* V, int ldv, int k, const double* w, int n, double
 void launch_maxpy(const double* V, int ldv, int k, const double* h, double* w, int n, cudaStream_t st);
 void launch_axpby(int n, double a, const double* x, double b, double* y, cudaStream_t st);
 void launch_scale_inv(int n, const double* x, const double* s, double* y, cudaStream_t st);
+void launch_mul(int n, const double* a, const double* x, double* y, cudaStream_t st);
+void launch_add_mul(int n, const double* xb, const double* a, const double* u, double* y, cudaStream_t st);
+void launch_jacobi(int n, const int* dof_point, const int* dof_kind, const double* diag, const int* block_of_point, const int* row_of_point,
+                   const NearBlockDev* blocks, const int* nb_dofs, const double* WG, const double* WGn, double* dinv, cudaStream_t st);
+double fp64_probe_tflops(cudaStream_t st, double* sink);
 
 }  // namespace bemb200

@@ -1,0 +1,276 @@
+#!/usr/bin/env python
+"""Benchmark of the GMRES + FMM Laplace BVP solve (BEM-MEL boundary-value problem).
+
+Metric: BVP solves/s (one step = one complete BVP solve: set-up of geometry, octree,
+interaction lists, near-field quadrature and rigid-mode diagonal, then GMRES to a relative
+residual of 1e-8) on the 60k-node synthetic tank (2.0 x 1.0 x 0.5 m, h = 2/185 m,
+free-surface z-noise sigma = 0.2 h, p = 10, theta = 0.25, <= 30 elements per leaf).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: independent BVPs per rank (replicas, weak scaling, no collective on the data
+path); time is the max over ranks.  `--impl reference` times the reference algorithm on
+the host cores (the oracle's CPU restatement of the reference path, sampled; the compiled
+reference cannot hold this workload's per-pair M2L term cache, ~400 GB).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+CONFIGS = {
+    "tank_60k": dict(tank=dict(length=2.0, width=1.0, depth=0.5, h=2.0 / 185, noise=0.2, seed=1), p=10, rel_tol=1e-8),
+    "tank_2800": dict(tank=dict(length=2.0, width=1.0, depth=0.5, h=0.05, noise=0.0, seed=1), p=8, rel_tol=1e-10),
+}
+# GMRES iterations of the unpreconditioned reference algorithm on each workload (the same
+# Krylov iteration on the same operator), measured by the CUDA path; used to turn the
+# sampled CPU mat-vec time into solves/s.
+REFERENCE_ITERATIONS = {"tank_60k": None, "tank_2800": 384}
+
+
+def make_problem(cfg, rank):
+    from bem_for_nonlinear_waves_b200 import build_dofs, known_values, make_tank, point_normals
+    tk = dict(cfg["tank"])
+    noise = tk.pop("noise")
+    seed = tk.pop("seed") + rank
+    t = make_tank(noise_sigma=noise * tk["h"], seed=seed, **tk)
+    d = build_dofs(t.X, t.tri, t.face_dirichlet)
+    kv = known_values(t, d["dof_point"], d["dof_face"], d["dof_kind"], point_normals(t))
+    return t, d, kv
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def allreduce_max(vals, world):
+    if world == 1:
+        return list(vals)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_sample(cfg, t, d, iters):
+    """Bounded CPU sample of the same workload with the oracle (CPU restatement of the
+    reference algorithm, all host threads): near-field quadrature for every 200th point and
+    the M2L of every 100th target bucket, scaled to the whole; solves/s = 1 / (set-up +
+    (iters + 3) mat-vecs)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    o = O.Oracle(t.X, t.tri, t.face_dirichlet, d, p=cfg["p"], near_stride=200)
+    ts = o.time_sample(m2l_stride=100)
+    matvec = ts["p2m"] + ts["m2m"] + ts["m2l"] + ts["l2l"] + ts["near"] + ts["l2p"]
+    setup = ts["tree_lists"] + ts["near_setup"] + matvec
+    solve = setup + (iters + 3) * matvec
+    return dict(value=1.0 / solve, matvec_s=matvec, setup_s=setup, threads=int(ts["threads"]), iters=iters)
+
+
+def run_reference(args, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from bem_for_nonlinear_waves_b200.tank import make_tank  # mesh generator only
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    tk = dict(cfg["tank"])
+    noise = tk.pop("noise")
+    seed = tk.pop("seed")
+    t = make_tank(noise_sigma=noise * tk["h"], seed=seed, **tk)
+    d = O.build_dofs(t.X, t.tri, t.face_dirichlet)
+    iters = REFERENCE_ITERATIONS.get(args.config) or args.ref_iters
+    res = []
+    for k in range(args.warmup + args.steps):
+        r = cpu_sample(cfg, t, d, iters)
+        if k >= args.warmup:
+            res.append(r)
+    value = statistics.median([r["value"] for r in res])
+    line = {"impl": "reference", "metric": "bvp_solves_per_s", "value": value, "unit": "solves/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.config, "p": cfg["p"], "rel_tol": cfg["rel_tol"], "n_points": int(t.n_points),
+                       "n_faces": int(t.n_faces)},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": res[-1]["threads"], "kind": "port",
+                             "sample": f"oracle CPU restatement, per step: near quadrature of every 200th point and M2L of every "
+                                       f"100th target bucket scaled to the whole; {iters} GMRES iterations of the reference "
+                                       f"algorithm; matvec {res[-1]['matvec_s']:.2f} s, setup {res[-1]['setup_s']:.2f} s"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def load_traffic(kernel, workload):
+    """dram bytes per launch of a kernel from a committed ncu summary (profiles/), else None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="tank_60k", choices=list(CONFIGS))
+    ap.add_argument("--precond", default="jacobi", choices=["jacobi", "none"])
+    ap.add_argument("--max-iter", type=int, default=1500)
+    ap.add_argument("--ref-iters", type=int, default=1000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        return run_reference(args, cfg)
+
+    rank, world, local = dist_init()
+    from bem_for_nonlinear_waves_b200 import BEM_BVP
+    from bem_for_nonlinear_waves_b200 import _lib
+    t, d, kv = make_problem(cfg, rank)
+    bvp = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=cfg["p"], solver_tol=cfg["rel_tol"], tol_relative=True,
+                  solver_max_iter=args.max_iter, preconditioner=args.precond, dofs=d, device=local)
+    for _ in range(args.warmup):
+        bvp.setup()
+        bvp.solve(kv)
+    prof = bvp.profile_matvec(repeats=5)
+    tree = bvp.tree_stats()
+    fp64_peak = _lib.load().bem_gpu_fp64_peak_tflops(local)
+
+    barrier(world)
+    dev_s = e2e_s = 0.0
+    launches = h2d = d2h = iters = 0
+    converged = True
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            w0 = time.perf_counter()
+            bvp.setup()
+            bvp.solve(kv)
+            e2e_s += time.perf_counter() - w0
+            st = bvp.stats
+            dev_s += st.time_device_s
+            launches += st.kernel_launches
+            h2d += st.h2d_bytes
+            d2h += st.d2h_bytes
+            iters += st.iterations
+            converged = converged and bool(st.converged)
+    barrier(world)
+    dev_max, e2e_max = allreduce_max([dev_s, e2e_s], world)
+
+    p = cfg["p"]
+    nc = (p + 1) * (p + 2) // 2
+    m2l_flops = tree["m2l_pairs"] * 2 * nc * (p + 1) ** 2 * 8.0  # complex MACs, both densities
+    m2l_s = prof["m2l"] * 1e-3
+    achieved = m2l_flops / m2l_s / 1e12
+    traffic = load_traffic("m2l", args.config)
+    line = {
+        "metric": "bvp_solves_per_s", "value": world * args.steps / dev_max, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.config, "n_points": int(t.n_points), "n_faces": int(t.n_faces), "n_dof": int(bvp.matrix_size),
+                   "p": p, "theta": 0.25, "leaf_max": 30, "rel_tol": cfg["rel_tol"], "preconditioner": args.precond,
+                   "gmres_iterations": iters / args.steps, "converged": converged, "parallelism": f"replicas{world}",
+                   "l2": "working set > L2 (near-field weights %.1f GB)" % (tree["nnz"] * 16 / 1e9)},
+        "matvecs_per_s": world * 1e3 / prof["total"],
+        "matvec_stage_ms": prof,
+        "e2e": {"value": world * args.steps / e2e_max, "unit": "solves/s", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "gpu_launches": launches,
+        "roofline": {"kernel": "k_m2l", "bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp64_peak if fp64_peak > 0 else None, "traffic": traffic,
+                     "peak_source": "measured FP64 FMA probe on this GPU (MEASURED_PEAKS.json has no FP64 figure)",
+                     "algorithmic_flops_per_launch": m2l_flops},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ref_iters = REFERENCE_ITERATIONS.get(args.config) or args.ref_iters
+        cb = cpu_sample(cfg, t, d, ref_iters)
+        line["cpu_baseline"] = {"value": cb["value"], "unit": "solves/s", "cores": cb["threads"], "kind": "port",
+                                "sample": f"oracle CPU restatement on the same tank: near quadrature of every 200th point, M2L "
+                                          f"of every 100th target bucket, scaled; {ref_iters} unpreconditioned GMRES iterations; "
+                                          f"matvec {cb['matvec_s']:.2f} s, setup {cb['setup_s']:.2f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

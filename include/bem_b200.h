@@ -56,7 +56,8 @@ typedef struct {
   int32_t max_iter;          /* GMRES iteration cap (solver_max_iter) */
   int32_t device;            /* CUDA device ordinal */
   int32_t tol_relative;      /* 0: stop at |A x - b| <= tol (reference semantics); 1: at <= tol*|b| */
-  int32_t reserved[4];
+  int32_t preconditioner;    /* 0: none (reference default); 1: right Jacobi from the near-field diagonal */
+  int32_t reserved[3];
 } bem_gpu_opts;
 
 /* One boundary-value problem.  The DOF table is what the reference's setNodeFaceIndices()
@@ -87,7 +88,12 @@ typedef struct {
   int32_t n_nodes;        /* non-empty octree nodes */
   int32_t n_leaves;
   int32_t matvecs;        /* operator applications in this solve */
-  int32_t reserved[5];
+  int32_t reserved0;
+  double time_device_s;   /* CUDA-event time of the device work of setup + solve */
+  int64_t h2d_bytes;      /* host->device bytes of setup + solve */
+  int64_t d2h_bytes;      /* device->host bytes of setup + solve */
+  int64_t kernel_launches;/* kernels launched by setup + solve (graph nodes counted) */
+  int32_t reserved[4];
 } bem_gpu_stats;
 
 /* 1 if a CUDA device of compute capability 10.x is visible. */
@@ -151,9 +157,12 @@ int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out /*[8]: nodes, leaves, dept
  * of the leaf bucket holding it (-1 if none), plus stats[8] as bem_gpu_tree_stats. */
 int bem_plan_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* desc, int32_t* face_level, double* face_corner, int64_t* stats);
 
-/* Kernel timing of the last mat-vec executed through bem_gpu_profile_matvec: per stage
- * milliseconds [p2m, m2m, m2l, l2l, near+l2p, total] measured with CUDA events. */
+/* Mat-vec stage timing with CUDA events on the context stream, averaged over repeats:
+ * stage_ms = [p2m, m2m, m2l, l2l, near+l2p+rows, whole graph-launched mat-vec]. */
 int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[6]*/);
+
+/* FP64 FMA throughput of the device (TFLOP/s), measured by a short probe kernel. */
+double bem_gpu_fp64_peak_tflops(int32_t device);
 
 #ifdef __cplusplus
 }

@@ -239,6 +239,8 @@ struct Source {  // one linear element (lib_multipole_expansion.hpp:675-775)
 }  // namespace
 
 struct OracleCtx {
+  int near_stride = 1;  // near-field rows computed for every near_stride-th point only (timing samples)
+  double t_tree = 0.0, t_near = 0.0;
   int p = 8;
   double theta = 0.25;
   int max_points = 30;
@@ -519,10 +521,13 @@ extern "C" {
 
 // Set-up: scaling, sources, tree, lists, L2P targets, near-field weights, diagonal.
 // desc arrays: X[np*3] physical, tri[nf*3], face_dirichlet[nf], DOF table.
-void* oracle_create(int np, const double* X, int nf, const int* tri, const uint8_t* face_dirichlet, int ndof, const int* dof_point,
-                    const int* dof_face, const int* dof_kind, const int* face_dof, int p, double theta, int max_points, int max_level) {
+void* oracle_create_sampled(int np, const double* X, int nf, const int* tri, const uint8_t* face_dirichlet, int ndof, const int* dof_point,
+                            const int* dof_face, const int* dof_kind, const int* face_dof, int p, double theta, int max_points, int max_level,
+                            int near_stride) {
   auto* Cp = new OracleCtx();
   OracleCtx& C = *Cp;
+  C.near_stride = near_stride < 1 ? 1 : near_stride;
+  const double wt0 = omp_get_wtime();
   C.p = p;
   C.theta = theta;
   C.max_points = max_points;
@@ -656,6 +661,8 @@ void* oracle_create(int np, const double* X, int nf, const int* tri, const uint8
           C.aaa_l2l[C.aidx(j, k, n, m)] = bem_oracle_aaa::l2l(j, k, n, m);
         }
 
+  C.t_tree = omp_get_wtime() - wt0;
+  const double wt1 = omp_get_wtime();
   // targets: leaf + near-field weights (lib_multipole_expansion.hpp:1130-1271)
   C.tgt_leaf.assign(np, nullptr);
   C.near_idx.assign(np, {});
@@ -668,6 +675,7 @@ void* oracle_create(int np, const double* X, int nf, const int* tri, const uint8
     const V3 xt = C.Xs[t];
     Node* bd = bucket_at_deepest(R, xt);
     C.tgt_leaf[t] = bd;
+    if (t % C.near_stride != 0) continue;
     std::vector<double> accG(ndof, 0.0), accGn(ndof, 0.0);
     std::vector<uint8_t> touched(ndof, 0);
     std::vector<int> tl;
@@ -759,6 +767,7 @@ void* oracle_create(int np, const double* X, int nf, const int* tri, const uint8
     }
   }
 
+  C.t_near = omp_get_wtime() - wt1;
   int nc = C.ncoef();
   for (auto& up : C.pool) {
     up->MM.assign(nc, {0., 0.});
@@ -767,6 +776,12 @@ void* oracle_create(int np, const double* X, int nf, const int* tri, const uint8
   R->MM.assign(nc, {0., 0.});
   R->LL.assign(nc, {0., 0.});
   return Cp;
+}
+
+void* oracle_create(int np, const double* X, int nf, const int* tri, const uint8_t* face_dirichlet, int ndof, const int* dof_point,
+                    const int* dof_face, const int* dof_kind, const int* face_dof, int p, double theta, int max_points, int max_level) {
+  return oracle_create_sampled(np, X, nf, tri, face_dirichlet, ndof, dof_point, dof_face, dof_kind, face_dof, p, theta, max_points,
+                               max_level, 1);
 }
 
 void oracle_destroy(void* h) { delete (OracleCtx*)h; }
@@ -784,8 +799,15 @@ std::vector<Node*> all_nodes(OracleCtx& C) {
 
 // One FMM update + per-point (near + far) integrals for given per-DOF phi/phin
 // (moments.hpp:1547-1574; lib_multipole_expansion.hpp:1143-1150,1273-1302).
-void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, std::vector<double>& GPhin, std::vector<double>& GnPhi) {
+void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, std::vector<double>& GPhin, std::vector<double>& GnPhi,
+                         int m2l_stride = 1, double* tstage = nullptr) {
   const int p = C.p;
+  double tw = omp_get_wtime();
+  auto lap = [&](int k) {
+    const double n = omp_get_wtime();
+    if (tstage) tstage[k] += n - tw;
+    tw = n;
+  };
   const int nc = C.ncoef();
   auto nodes = all_nodes(C);
   for (auto* b : nodes) {
@@ -806,6 +828,7 @@ void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, st
     }
     conj_fill(p, b->MM);
   }
+  lap(0);
   // M2M bottom-up (moments.hpp:401-436, 912-915)
   for (int level = C.max_level - 1; level >= 0; --level) {
 #pragma omp parallel for schedule(dynamic, 1)
@@ -832,12 +855,14 @@ void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, st
       conj_fill(p, b->MM);
     }
   }
+  lap(1);
   // M2L (moments.hpp:492-598, 732-764)
   for (auto& lv : C.level_nodes) {
 #pragma omp parallel for schedule(dynamic, 1)
     for (size_t ai = 0; ai < lv.size(); ++ai) {
       Node* A = lv[ai];
       if (A->l2m.empty()) continue;
+      if (m2l_stride > 1 && (ai % m2l_stride) != 0) continue;
       std::vector<std::array<cd, 2>> acc(nc, {0., 0.});
       std::vector<cd> Ys((2 * p + 1) * (2 * p + 1));
       for (auto* B : A->l2m) {
@@ -867,6 +892,7 @@ void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, st
       conj_fill(p, A->LL);
     }
   }
+  lap(2);
   // L2L top-down (moments.hpp:862-884, 925-929)
   for (auto& lv : C.level_nodes) {
 #pragma omp parallel for schedule(dynamic, 1)
@@ -889,17 +915,24 @@ void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, st
       }
     }
   }
+  lap(3);
   // per point near + far
   GPhin.assign(C.np, 0.0);
   GnPhi.assign(C.np, 0.0);
 #pragma omp parallel for schedule(dynamic, 32)
   for (int t = 0; t < C.np; ++t) {
-    if (!C.tgt_leaf[t]) continue;
     double r0 = 0, r1 = 0;
     for (size_t i = 0; i < C.near_idx[t].size(); ++i) {
       r0 += phin[C.near_idx[t][i]] * C.near_wG[t][i];
       r1 += phi[C.near_idx[t][i]] * C.near_wGn[t][i];
     }
+    GPhin[t] = r0;
+    GnPhi[t] = r1;
+  }
+  lap(4);
+#pragma omp parallel for schedule(dynamic, 32)
+  for (int t = 0; t < C.np; ++t) {
+    if (!C.tgt_leaf[t]) continue;
     Node* b = C.tgt_leaf[t];
     Sph S(sub(C.Xs[t], b->X));
     cd f0 = 0., f1 = 0.;
@@ -909,9 +942,10 @@ void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, st
         f0 += y * b->LL[n * (n + 1) + m][0];
         f1 += y * b->LL[n * (n + 1) + m][1];
       }
-    GPhin[t] = r0 + f0.real();
-    GnPhi[t] = r1 + f1.real();
+    GPhin[t] += f0.real();
+    GnPhi[t] += f1.real();
   }
+  lap(5);
 }
 
 void apply_rows(OracleCtx& C, const double* phi, const double* phin, double* Av) {
@@ -1072,6 +1106,28 @@ int oracle_near_row(void* h, int t, int cap, int* idx, double* wG, double* wGn) 
 }
 
 double oracle_scale_factor(void* h) { return ((OracleCtx*)h)->L; }
+
+// Timing sample for the CPU baseline: set-up parts and one FMM mat-vec with M2L run for
+// every m2l_stride-th target bucket (times scaled by the pair counts).  t[0..5]: P2M, M2M,
+// M2L (scaled), L2L, near sums (scaled by near_stride), L2P; t[6]: tree+lists set-up,
+// t[7]: near-field quadrature (scaled by near_stride); t[8]: OpenMP threads.
+void oracle_time_sample(void* h, int m2l_stride, double* t) {
+  OracleCtx& C = *(OracleCtx*)h;
+  std::vector<double> phi(C.ndof, 1.0), phin(C.ndof, 0.5), a, b;
+  for (int k = 0; k < 9; ++k) t[k] = 0.0;
+  fmm_point_integrals(C, phi.data(), phin.data(), a, b, m2l_stride, t);
+  long long all = 0, sampled = 0;
+  for (auto& lv : C.level_nodes)
+    for (size_t ai = 0; ai < lv.size(); ++ai) {
+      all += lv[ai]->l2m.size();
+      if (m2l_stride <= 1 || ai % m2l_stride == 0) sampled += lv[ai]->l2m.size();
+    }
+  if (sampled > 0) t[2] *= (double)all / (double)sampled;
+  t[4] *= C.near_stride;
+  t[6] = C.t_tree;
+  t[7] = C.t_near * C.near_stride;
+  t[8] = omp_get_max_threads();
+}
 
 // GMRES solve (BEM_solveBVP_GMRES_FMM.hpp:2007-2400; basic_linear_systems.hpp:3137-3451).
 // known[i]: phi (Dirichlet DOF) or phin (Neumann DOFs) in physical units;

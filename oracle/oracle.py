@@ -39,6 +39,9 @@ def lib():
         L.oracle_create.restype = P
         L.oracle_create.argtypes = [i32, dp, i32, ip, u8p, i32, ip, ip, ip, ip, i32, ctypes.c_double, i32, i32]
         L.oracle_destroy.argtypes = [P]
+        L.oracle_create_sampled.restype = P
+        L.oracle_create_sampled.argtypes = [i32, dp, i32, ip, u8p, i32, ip, ip, ip, ip, i32, ctypes.c_double, i32, i32, i32]
+        L.oracle_time_sample.argtypes = [P, i32, dp]
         L.oracle_compute_diag.argtypes = [P]
         L.oracle_get_diag.argtypes = [P, dp]
         L.oracle_point_integrals.argtypes = [P, dp, dp, dp, dp]
@@ -79,7 +82,7 @@ def build_dofs(X, tri, face_dirichlet):
 
 
 class Oracle:
-    def __init__(self, X, tri, face_dirichlet, dofs, p=8, theta=0.25, max_points=30, max_level=7):
+    def __init__(self, X, tri, face_dirichlet, dofs, p=8, theta=0.25, max_points=30, max_level=7, near_stride=1):
         self.X = np.ascontiguousarray(X, dtype=np.float64)
         self.tri = np.ascontiguousarray(tri, dtype=np.int32)
         self.fd = np.ascontiguousarray(face_dirichlet, dtype=np.uint8)
@@ -91,10 +94,10 @@ class Oracle:
         self.np = int(self.X.shape[0])
         self.nf = int(self.tri.shape[0])
         self.p = p
-        self.h = lib().oracle_create(self.np, _p(self.X, ctypes.c_double), self.nf, _p(self.tri, ctypes.c_int),
-                                     _p(self.fd, ctypes.c_uint8), self.ndof, _p(self.dof_point, ctypes.c_int),
-                                     _p(self.dof_face, ctypes.c_int), _p(self.dof_kind, ctypes.c_int),
-                                     _p(self.face_dof, ctypes.c_int), p, theta, max_points, max_level)
+        self.h = lib().oracle_create_sampled(self.np, _p(self.X, ctypes.c_double), self.nf, _p(self.tri, ctypes.c_int),
+                                             _p(self.fd, ctypes.c_uint8), self.ndof, _p(self.dof_point, ctypes.c_int),
+                                             _p(self.dof_face, ctypes.c_int), _p(self.dof_kind, ctypes.c_int),
+                                             _p(self.face_dof, ctypes.c_int), p, theta, max_points, max_level, int(near_stride))
         self._diag = False
 
     def __del__(self):
@@ -131,6 +134,14 @@ class Oracle:
         out = np.zeros(self.ndof)
         lib().oracle_apply(self.h, _p(phi, ctypes.c_double), _p(phin, ctypes.c_double), _p(out, ctypes.c_double))
         return out
+
+    def time_sample(self, m2l_stride=1):
+        """Seconds: p2m, m2m, m2l, l2l, near sums, l2p (one mat-vec), tree+lists, near
+        quadrature; threads."""
+        t = np.zeros(9)
+        lib().oracle_time_sample(self.h, int(m2l_stride), _p(t, ctypes.c_double))
+        keys = ["p2m", "m2m", "m2l", "l2l", "near", "l2p", "tree_lists", "near_setup", "threads"]
+        return dict(zip(keys, t.tolist()))
 
     def stats(self, max_level=7):
         out = np.zeros(8, np.int64)
