@@ -19,7 +19,7 @@ BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
-CXXFLAGS = ["-O2", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-Wall"]
+CXXFLAGS = ["-O2", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-Wall", "-fopenmp"]
 
 CU_SOURCES = ["kernels.cu", "capi.cu"]
 CXX_SOURCES = ["plan.cpp"]
@@ -62,7 +62,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         if _stale(o, [s] + headers):
             _run(["g++"] + CXXFLAGS + ["-c", "-o", o, s])
     if _stale(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-cudart=static", "-o", LIB] + objs + ["-lstdc++"])
+        _run([NVCC] + ARCH + ["-shared", "-cudart=static", "-o", LIB] + objs + ["-lstdc++", "-lgomp"])
     return LIB
 
 

@@ -173,9 +173,9 @@ class BEM_BVP:
         return lv, c.reshape(-1, 3)
 
     def tree_stats(self):
-        out = np.zeros(8, np.int64)
+        out = np.zeros(10, np.int64)
         self._check(self.lib.bem_gpu_tree_stats(self.ctx, L.ptr(out, L.P_i64)), "tree_stats")
-        keys = ["nodes", "leaves", "depth", "n_added", "m2l_pairs", "near_pairs", "nnz", "near_blocks"]
+        keys = ["nodes", "leaves", "depth", "n_added", "m2l_pairs", "near_pairs", "nnz", "near_blocks", "m2l_chunks", "m2l_groups"]
         return {k: int(v) for k, v in zip(keys, out)}
 
     def matvec_time_ms(self, repeats=10):
@@ -207,9 +207,9 @@ def inspect_plan(X, tri, face_dirichlet, dofs=None, *, expansion_order=10, mac_t
                   L.ptr(keep[0], L.P_int), L.ptr(keep[1], L.P_int), L.ptr(keep[2], L.P_int), L.ptr(keep[3], L.P_int))
     lv = np.zeros(tri.shape[0], np.int32)
     corner = np.zeros(3 * tri.shape[0])
-    st = np.zeros(8, np.int64)
+    st = np.zeros(10, np.int64)
     rc = lib.bem_plan_inspect(ctypes.byref(o), ctypes.byref(desc), L.ptr(lv, L.P_int), L.ptr(corner, L.P_dbl), L.ptr(st, L.P_i64))
     if rc != 0:
         raise ValueError("plan construction failed: " + L.STATUS.get(rc, str(rc)))
-    keys = ["nodes", "leaves", "depth", "n_added", "m2l_pairs", "near_pairs", "nnz", "near_blocks"]
+    keys = ["nodes", "leaves", "depth", "n_added", "m2l_pairs", "near_pairs", "nnz", "near_blocks", "m2l_chunks", "m2l_groups"]
     return lv, corner.reshape(-1, 3), {k: int(v) for k, v in zip(keys, st)}

@@ -64,6 +64,9 @@ struct bem_gpu_ctx {
   DBuf<int> m2l_targets, m2l_off, m2l_src, nb_dofs, nb_targets, nb_ranges, dof_inc_off, dof_inc;
   DBuf<int> point_dof_off, point_dof, dof_kind, dof_point;
   DBuf<NearBlockDev> blocks;
+  DBuf<int> chunk_grp, chunk_begin, chunk_cnt, grp_pair;
+  DBuf<double> grp_vec;
+  DBuf<double2> Sg, Mf, Y;
   DBuf<double2> M, L;
   std::vector<int> level_parent_off;
   int n_m2l_targets = 0, max_ntgt = 0, chunk = 0;
@@ -112,6 +115,14 @@ struct bem_gpu_ctx {
     a.m2l_targets = m2l_targets.p;
     a.m2l_off = m2l_off.p;
     a.m2l_src = m2l_src.p;
+    a.n_chunks = (int)plan.chunk_grp.size();
+    a.chunk_grp = chunk_grp.p;
+    a.chunk_begin = chunk_begin.p;
+    a.chunk_cnt = chunk_cnt.p;
+    a.grp_pair = grp_pair.p;
+    a.Sg = Sg.p;
+    a.Mf = Mf.p;
+    a.Y = Y.p;
     a.M = M.p;
     a.L = L.p;
     a.n_blocks = (int)plan.blocks.size();
@@ -312,9 +323,7 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
       if (P.nodes[i].child_end > P.nodes[i].child_begin) lp.push_back(i);
     ctx->level_parent_off.push_back((int)lp.size());
   }
-  std::vector<int> mt;
-  for (int i = 0; i < nb; ++i)
-    if (!P.nodes[i].empty() && P.m2l_off[i + 1] > P.m2l_off[i]) mt.push_back(i);
+  const std::vector<int>& mt = P.m2l_targets;
   ctx->n_m2l_targets = (int)mt.size();
   std::vector<NearBlockDev> bd(P.blocks.size());
   ctx->max_ntgt = 1;
@@ -340,6 +349,8 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   }
   ctx->chunk = std::min(max_ndof, (smem_cap - ctx->max_ntgt * 16) / 16);
   configure_targets_smem(P.opt.p, (ctx->chunk + ctx->max_ntgt) * 16);
+  configure_m2l_smem(P.opt.p);
+
 
   CK(up(ctx, ctx->Xs, P.Xs));
   CK(up(ctx, ctx->e_q, P.e_q));
@@ -369,6 +380,20 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   CK(up(ctx, ctx->dof_kind, P.dof_kind));
   CK(up(ctx, ctx->dof_point, P.dof_point));
   CK(up(ctx, ctx->blocks, bd));
+  CK(up(ctx, ctx->chunk_grp, P.chunk_grp));
+  CK(up(ctx, ctx->chunk_begin, P.chunk_begin));
+  CK(up(ctx, ctx->chunk_cnt, P.chunk_cnt));
+  CK(up(ctx, ctx->grp_pair, P.grp_pair));
+  CK(up(ctx, ctx->grp_vec, P.grp_vec));
+  {
+    const int ngroups = (int)P.grp_off.size() - 1;
+    const int Q = 2 * P.opt.p;
+    CK(ctx->Sg.alloc((size_t)std::max(ngroups, 1) * (Q + 1) * (Q + 1)));
+    CK(ctx->Mf.alloc((size_t)nb * 2 * (P.opt.p + 1) * (P.opt.p + 1)));
+    CK(ctx->Y.alloc((size_t)std::max<int64_t>(P.m2l_pairs, 1) * 2 * NC));
+    launch_s_tables(P.opt.p, ngroups, ctx->grp_vec.p, ctx->Sg.p, s);
+    ctx->launches += 1;
+  }
   CK(ctx->M.alloc((size_t)nb * 2 * NC));
   CK(ctx->L.alloc((size_t)nb * 2 * NC));
   CK(cudaMemsetAsync(ctx->M.p, 0, sizeof(double2) * ctx->M.n, s));
@@ -549,6 +574,8 @@ int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out) {
   out[5] = P.near_pairs;
   out[6] = P.nnz;
   out[7] = (int64_t)P.blocks.size();
+  out[8] = (int64_t)P.chunk_grp.size();
+  out[9] = (int64_t)P.grp_off.size() - 1;
   return BEM_OK;
 }
 
@@ -589,6 +616,8 @@ int bem_plan_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* d, int32_t* f
     stats[5] = P.near_pairs;
     stats[6] = P.nnz;
     stats[7] = (int64_t)P.blocks.size();
+    stats[8] = (int64_t)P.chunk_grp.size();
+    stats[9] = (int64_t)P.grp_off.size() - 1;
   }
   return BEM_OK;
 }

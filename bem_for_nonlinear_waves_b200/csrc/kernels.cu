@@ -13,6 +13,7 @@
 //                   BEM_solveBVP_GMRES_FMM.hpp:1824-1891)
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "fmm_math.cuh"
@@ -261,43 +262,115 @@ __global__ void k_m2m(const int* __restrict__ parents, const int* __restrict__ c
 }
 
 // ---------------------------------------------------------------------------
-// M2L: one block per target bucket, its whole source list; thread per output (n, m>=0).
+// M2L grouped by translation vector.
+//   k_s_tables    (set-up) one irregular-harmonic table S(d_g) per group, all orders
+//   k_expand_full multipoles of every bucket expanded to negative orders
+//   k_m2l_grp     block per chunk of <= 8 pairs of one group: the group's table in shared
+//                 memory is applied to the 8 source multipoles (one S load feeds 8 complex
+//                 multiply-adds per density); partial locals to slot k of each pair
+//   k_m2l_reduce  per target bucket: L = sum of its slots (CSR order, deterministic)
 template <int P>
-__global__ void k_m2l(const int* __restrict__ targets, const int* __restrict__ m2l_off, const int* __restrict__ m2l_src,
-                      const double* __restrict__ node_X, const double2* __restrict__ M, double2* __restrict__ L) {
+__global__ void k_s_tables(int ngroups, const double* __restrict__ gvec, double2* __restrict__ Sg) {
+  constexpr int Q = 2 * P, NS = (Q + 1) * (Q + 1);
+  const int g = blockIdx.x;
+  if (g < ngroups && threadIdx.x < 32) S_full_column<Q>(threadIdx.x, gvec[3 * g], gvec[3 * g + 1], gvec[3 * g + 2], Sg + (size_t)g * NS);
+}
+
+template <int P>
+__global__ void k_expand_full(int nnodes, const double2* __restrict__ M, double2* __restrict__ Mf) {
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
+  const int64_t total = (int64_t)nnodes * 2 * NF;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t node = e / (2 * NF);
+    const int r = (int)(e - node * 2 * NF);
+    const int d = r / NF, i = r - d * NF;
+    int n = (int)sqrtf((float)i);
+    while (n * n > i) --n;
+    while ((n + 1) * (n + 1) <= i) ++n;
+    const int m = i - n * (n + 1);
+    double2 v = M[node * 2 * NC + d * NC + cidx(n, m < 0 ? -m : m)];
+    if (m < 0) v = ((-m) & 1) ? make_double2(-v.x, v.y) : make_double2(v.x, -v.y);
+    Mf[e] = v;
+  }
+}
+
+template <int P>
+constexpr int m2l_grp_smem_bytes() {
+  return (int)sizeof(double2) * ((2 * P + 1) * (2 * P + 1) + 8 * 2 * (P + 1) * (P + 1));
+}
+
+template <int P>
+__global__ void __launch_bounds__(((2 * ncoef(P) + 31) / 32) * 32) k_m2l_grp(const int* __restrict__ chunk_grp, const int* __restrict__ chunk_begin,
+                                                                             const int* __restrict__ chunk_cnt, const int* __restrict__ grp_pair,
+                                                                             const int* __restrict__ m2l_src, const double2* __restrict__ Sg,
+                                                                             const double2* __restrict__ Mf, double2* __restrict__ Y) {
   constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), Q = 2 * P, NS = (Q + 1) * (Q + 1);
-  __shared__ double2 sS[NS];
-  __shared__ double2 sM[2 * NF];
-  const int tgt = targets[blockIdx.x];
+  extern __shared__ double2 smem_grp[];
+  double2* sS = smem_grp;        // [NS]
+  double2* sM = smem_grp + NS;   // [8][2][NF]
+  const int c = blockIdx.x;
+  const int g = chunk_grp[c], b0 = chunk_begin[c], cnt = chunk_cnt[c];
   const int t = threadIdx.x;
+  {
+    const double2* src = Sg + (size_t)g * NS;
+    for (int i = t; i < NS; i += blockDim.x) sS[i] = src[i];
+    for (int j = 0; j < cnt; ++j) {
+      const double2* m = Mf + (size_t)m2l_src[grp_pair[b0 + j]] * 2 * NF;
+      for (int i = t; i < 2 * NF; i += blockDim.x) sM[j * 2 * NF + i] = m[i];
+    }
+  }
+  __syncthreads();
+  if (t >= 2 * NC) return;
+  const int dd = (t < NC) ? 0 : 1;
+  const int o = t - dd * NC;
   int n = 0, m = 0;
-  if (t < NC) decode_nm(t, n, m);
-  double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
-  const double tx = node_X[3 * tgt], ty = node_X[3 * tgt + 1], tz = node_X[3 * tgt + 2];
-  for (int k = m2l_off[tgt]; k < m2l_off[tgt + 1]; ++k) {
-    const int src = m2l_src[k];
-    __syncthreads();
-    if (t < 32) S_full_column<Q>(t, tx - node_X[3 * src], ty - node_X[3 * src + 1], tz - node_X[3 * src + 2], sS);
-    expand_full<P>(M + (size_t)src * 2 * NC, sM);
-    __syncthreads();
-    if (t < NC) {
-      for (int n1 = 0; n1 <= P; ++n1) {
-        const int l = n + n1;
-        const double2* Srow = sS + l * (l + 1) + m;
-        const double2* M0 = sM + n1 * (n1 + 1);
-        const double2* M1 = sM + NF + n1 * (n1 + 1);
-        for (int m1 = -n1; m1 <= n1; ++m1) {
-          const double2 s = Srow[m1];
-          cfma(a0, s, M0[m1]);
-          cfma(a1, s, M1[m1]);
-        }
+  decode_nm(o, n, m);
+  double2 acc[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j] = make_double2(0.0, 0.0);
+  const double2* sMd = sM + dd * NF;
+  if (cnt == 8) {
+    for (int n1 = 0; n1 <= P; ++n1) {
+      const int l = n + n1;
+      const double2* Srow = sS + l * (l + 1) + m;
+      const int mb = n1 * (n1 + 1);
+      for (int m1 = -n1; m1 <= n1; ++m1) {
+        const double2 s = Srow[m1];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) cfma(acc[j], s, sMd[j * 2 * NF + mb + m1]);
+      }
+    }
+  } else {
+    for (int n1 = 0; n1 <= P; ++n1) {
+      const int l = n + n1;
+      const double2* Srow = sS + l * (l + 1) + m;
+      const int mb = n1 * (n1 + 1);
+      for (int m1 = -n1; m1 <= n1; ++m1) {
+        const double2 s = Srow[m1];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (j < cnt) cfma(acc[j], s, sMd[j * 2 * NF + mb + m1]);
       }
     }
   }
-  if (t < NC) {
-    const double sg = (n & 1) ? -1.0 : 1.0;
-    L[(size_t)tgt * 2 * NC + t] = make_double2(sg * a0.x, sg * a0.y);
-    L[(size_t)tgt * 2 * NC + NC + t] = make_double2(sg * a1.x, sg * a1.y);
+  const double sg = (n & 1) ? -1.0 : 1.0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    if (j < cnt) Y[(size_t)grp_pair[b0 + j] * 2 * NC + t] = make_double2(sg * acc[j].x, sg * acc[j].y);
+}
+
+template <int P>
+__global__ void k_m2l_reduce(int ntargets, const int* __restrict__ targets, const int* __restrict__ m2l_off, const double2* __restrict__ Y,
+                             double2* __restrict__ L) {
+  constexpr int NC = ncoef(P);
+  const int64_t total = (int64_t)ntargets * 2 * NC;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int ti = (int)(e / (2 * NC));
+    const int r = (int)(e - (int64_t)ti * 2 * NC);
+    const int tgt = targets[ti];
+    double2 s = make_double2(0.0, 0.0);
+    for (int k = m2l_off[tgt]; k < m2l_off[tgt + 1]; ++k) s = cadd(s, Y[(size_t)k * 2 * NC + r]);
+    L[(size_t)tgt * 2 * NC + r] = s;
   }
 }
 
@@ -469,7 +542,7 @@ __device__ void elem_vertex_weight(int s, int a, int t, const double* __restrict
       const double Rx = N[0] * X0[0] + N[1] * X1[0] + N[2] * X2[0] - xt;
       const double Ry = N[0] * X0[1] + N[1] * X1[1] + N[2] * X2[1] - yt;
       const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
-      const double nr_inv = 1. / dnorm3(Rx, Ry, Rz);
+      const double nr_inv = rsqrt(Rx * Rx + Ry * Ry + Rz * Rz);
       const double tmp = ww * (1. - t0) * nr_inv * N[ia];
       G += J * tmp;
       Gn += -((Rx * crx + Ry * cry + Rz * crz) * nr_inv) * tmp * nr_inv;
@@ -489,7 +562,7 @@ __device__ void elem_vertex_weight(int s, int a, int t, const double* __restrict
       const double Rx = N[0] * X0[0] + N[1] * X1[0] + N[2] * X2[0] - xt;
       const double Ry = N[0] * X0[1] + N[1] * X1[1] + N[2] * X2[1] - yt;
       const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
-      const double nr_inv = 1. / dnorm3(Rx, Ry, Rz);
+      const double nr_inv = rsqrt(Rx * Rx + Ry * Ry + Rz * Rz);
       const double tmp = ww * (1. - t0) * N[a] * nr_inv;
       G += J * tmp;
       Gn -= ((Rx * crx + Ry * cry + Rz * crz) * nr_inv) * (tmp * nr_inv);
@@ -500,7 +573,7 @@ __device__ void elem_vertex_weight(int s, int a, int t, const double* __restrict
       const double Rx = N[0] * X0[0] + N[1] * X1[0] + N[2] * X2[0] - xt;
       const double Ry = N[0] * X0[1] + N[1] * X1[1] + N[2] * X2[1] - yt;
       const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
-      const double nr_inv = 1. / dnorm3(Rx, Ry, Rz);
+      const double nr_inv = rsqrt(Rx * Rx + Ry * Ry + Rz * Rz);
       const double tmp = c_dv[q][3] * N[a] * nr_inv;
       G += J * tmp;
       Gn -= ((Rx * crx + Ry * cry + Rz * crz) * nr_inv) * (tmp * nr_inv);
@@ -703,9 +776,18 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     }
   if (stages & STAGE_M2L) {
     cudaMemsetAsync(a.L, 0, sizeof(double2) * 2 * NC * (size_t)a.n_nodes, st);
-    if (a.n_m2l_targets > 0) {
-      k_m2l<P><<<a.n_m2l_targets, tpb_coef, 0, st>>>(a.m2l_targets, a.m2l_off, a.m2l_src, a.node_X, a.M, a.L);
-      ++launches;
+    if (a.n_chunks > 0) {
+      constexpr int NF = (P + 1) * (P + 1);
+      const int64_t tot = (int64_t)a.n_nodes * 2 * NF;
+      int ge = (int)std::min<int64_t>((tot + 255) / 256, 148 * 16);
+      k_expand_full<P><<<ge, 256, 0, st>>>(a.n_nodes, a.M, a.Mf);
+      const int tpb2 = ((2 * NC + 31) / 32) * 32;
+      k_m2l_grp<P><<<a.n_chunks, tpb2, m2l_grp_smem_bytes<P>(), st>>>(a.chunk_grp, a.chunk_begin, a.chunk_cnt, a.grp_pair, a.m2l_src, a.Sg,
+                                                                    a.Mf, a.Y);
+      const int64_t tr = (int64_t)a.n_m2l_targets * 2 * NC;
+      int gr = (int)std::min<int64_t>((tr + 255) / 256, 148 * 16);
+      k_m2l_reduce<P><<<gr, 256, 0, st>>>(a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.Y, a.L);
+      launches += 3;
     }
   }
   if (stages & STAGE_L2L)
@@ -741,6 +823,40 @@ int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages) {
     default: break;
   }
   return 0;
+}
+
+template <int P>
+void set_m2l_smem() {
+  cudaFuncSetAttribute(k_m2l_grp<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, m2l_grp_smem_bytes<P>());
+}
+
+template <int P>
+void s_tables(int ngroups, const double* gvec, double2* Sg, cudaStream_t st) {
+  if (ngroups > 0) k_s_tables<P><<<ngroups, 32, 0, st>>>(ngroups, gvec, Sg);
+}
+
+void launch_s_tables(int p, int ngroups, const double* gvec, double2* Sg, cudaStream_t st) {
+  switch (p) {
+#define BEMB200_CASE(PP) \
+  case PP:               \
+    s_tables<PP>(ngroups, gvec, Sg, st); break;
+    BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5) BEMB200_CASE(6)
+    BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10) BEMB200_CASE(11) BEMB200_CASE(12)
+#undef BEMB200_CASE
+    default: break;
+  }
+}
+
+void configure_m2l_smem(int p) {
+  switch (p) {
+#define BEMB200_CASE(PP) \
+  case PP:               \
+    set_m2l_smem<PP>(); break;
+    BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5) BEMB200_CASE(6)
+    BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10) BEMB200_CASE(11) BEMB200_CASE(12)
+#undef BEMB200_CASE
+    default: break;
+  }
 }
 
 void configure_targets_smem(int p, int bytes) {

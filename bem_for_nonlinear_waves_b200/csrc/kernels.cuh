@@ -36,6 +36,14 @@ struct MatvecArgs {
   const int* m2l_targets = nullptr;
   const int* m2l_off = nullptr;
   const int* m2l_src = nullptr;
+  int n_chunks = 0;
+  const int* chunk_grp = nullptr;
+  const int* chunk_begin = nullptr;
+  const int* chunk_cnt = nullptr;
+  const int* grp_pair = nullptr;
+  const double2* Sg = nullptr;  // per-group S tables
+  double2* Mf = nullptr;        // expanded multipoles
+  double2* Y = nullptr;         // per-pair partial locals
   double2* M = nullptr;
   double2* L = nullptr;
   // targets
@@ -76,6 +84,8 @@ struct NearArgs {
 
 void upload_quadrature(const double dv[6][4], const double gw[25][3], cudaStream_t s);
 void configure_targets_smem(int p, int bytes);
+void configure_m2l_smem(int p);
+void launch_s_tables(int p, int ngroups, const double* gvec, double2* Sg, cudaStream_t st);
 enum { STAGE_P2M = 1, STAGE_M2M = 2, STAGE_M2L = 4, STAGE_L2L = 8, STAGE_TARGETS = 16, STAGE_ALL = 31 };
 // returns the number of kernels launched
 int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages = STAGE_ALL);

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <chrono>
 #include <numeric>
 
 namespace bemb200 {
@@ -164,6 +165,12 @@ struct TreeBuilder {
 bool is_far(const PlanOptions& o, const Bucket& A, const Bucket& Bk) {  // moments.hpp:950-956
   const double eff = std::max(A.dL + 2.0 * A.off, Bk.dL + 2.0 * Bk.off);
   const V3 d{Bk.X[0] - A.X[0], Bk.X[1] - A.X[1], Bk.X[2] - A.X[2]};
+  // clear-cut cases by squared distance; only pairs within 1e-9 of the threshold go
+  // through the reference's exact expression (identical decisions, fewer hypot calls)
+  const double thr = std::sqrt(3.0) * eff / o.theta;
+  const double d2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  if (d2 > thr * thr * (1.0 + 1e-9)) return true;
+  if (d2 < thr * thr * (1.0 - 1e-9)) return false;
   return o.theta > std::sqrt(3.0) * eff / nrm(d);
 }
 
@@ -279,6 +286,12 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
                 const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof) {
   P = Plan();
   P.opt = opt;
+  auto clk = std::chrono::steady_clock::now();
+  auto lap = [&](int k) {
+    const auto n = std::chrono::steady_clock::now();
+    P.phase_s[k] += std::chrono::duration<double>(n - clk).count();
+    clk = n;
+  };
   if (np <= 0 || nf <= 0 || ndof <= 0 || !X || !tri || !fdir || !dof_point || !dof_face || !dof_kind || !face_dof) {
     P.error = "invalid BVP description";
     return false;
@@ -355,6 +368,7 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   auto XP = [&](int i) { return V3{P.Xs[3 * i], P.Xs[3 * i + 1], P.Xs[3 * i + 2]}; };
   std::vector<V3> pole(nf);
   std::vector<double> q(nf * 18), W(nf * 6), en(nf * 3), enear(nf * 8), offs(nf);
+#pragma omp parallel for schedule(static)
   for (int f = 0; f < nf; ++f) {
     const V3 a = XP(tri[3 * f]), b = XP(tri[3 * f + 1]), c = XP(tri[3 * f + 2]);
     const V3 cr = cross128(sub(b, a), sub(c, a));
@@ -380,6 +394,7 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     enear[8 * f + 7] = 0.0;
   }
 
+  lap(0);
   // octree (BEM_solveBVP_GMRES_FMM.hpp:1178-1201; lib_spatial_partitioning.hpp)
   TreeBuilder T(opt, pole);
   {
@@ -399,6 +414,7 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   std::vector<Bucket>& B = T.B;
   const int nb = (int)B.size();
 
+  lap(1);
   // offsets (moments.hpp:1336-1349): leaves from their elements, parents from children
   std::vector<std::vector<int>> lvl(opt.max_level + 1);
   for (int i = 0; i < nb; ++i)
@@ -421,6 +437,7 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     for (int a : lv)
       for (int b : B[a].m2l) B[b].l2m.push_back(a);
 
+  lap(2);
   // element order: DFS pre-order of the deepest bucket holding each element
   std::vector<int> owner(nf, -1);
   for (int i = 0; i < nb; ++i)
@@ -505,10 +522,62 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     std::copy(B[i].near.begin(), B[i].near.end(), P.near_nodes.begin() + P.near_off[i]);
   }
   P.m2l_pairs = P.m2l_off[nb];
+  lap(3);
+  // M2L grouped by (level, lattice offset); groups sorted by key, pairs in slot order
+  {
+    const int64_t npair = P.m2l_pairs;
+    std::vector<std::pair<long long, int>> keyed(npair);
+    std::vector<char> lattice_ok(npair, 1);
+#pragma omp parallel for schedule(static)
+    for (int t = 0; t < nb; ++t)
+      for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) {
+        const int s = P.m2l_src[k];
+        long long r[3];
+        for (int a = 0; a < 3; ++a) {
+          const double q = (B[t].X[a] - B[s].X[a]) / B[t].dL;
+          r[a] = std::llround(q);
+          if (std::abs(q - (double)r[a]) > 1e-9 || std::abs(r[a]) > 500) lattice_ok[k] = 0;
+        }
+        const long long key = ((long long)B[t].level << 30) | ((r[0] + 512) << 20) | ((r[1] + 512) << 10) | (r[2] + 512);
+        keyed[k] = {lattice_ok[k] ? key : ((1LL << 50) + k), k};
+      }
+    std::stable_sort(keyed.begin(), keyed.end());
+    P.grp_vec.clear();
+    P.grp_off.assign(1, 0);
+    P.grp_pair.resize(npair);
+    std::vector<int> pair_tgt(npair);
+    for (int t = 0; t < nb; ++t)
+      for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) pair_tgt[k] = t;
+    for (int64_t i = 0; i < npair;) {
+      int64_t j = i;
+      const int k0 = keyed[i].second;
+      const int t0 = pair_tgt[k0], s0 = P.m2l_src[k0];
+      for (int a = 0; a < 3; ++a) P.grp_vec.push_back(B[t0].X[a] - B[s0].X[a]);
+      while (j < npair && keyed[j].first == keyed[i].first) {
+        P.grp_pair[j] = keyed[j].second;
+        ++j;
+      }
+      P.grp_off.push_back((int)j);
+      i = j;
+    }
+    P.chunk_grp.clear();
+    P.chunk_begin.clear();
+    P.chunk_cnt.clear();
+    const int ng = (int)P.grp_off.size() - 1;
+    for (int g = 0; g < ng; ++g)
+      for (int b = P.grp_off[g]; b < P.grp_off[g + 1]; b += 8) {
+        P.chunk_grp.push_back(g);
+        P.chunk_begin.push_back(b);
+        P.chunk_cnt.push_back(std::min(8, P.grp_off[g + 1] - b));
+      }
+    P.m2l_targets.clear();
+    for (int t = 0; t < nb; ++t)
+      if (P.m2l_off[t + 1] > P.m2l_off[t]) P.m2l_targets.push_back(t);
+  }
   P.near_pairs = P.near_off[nb];
   for (int i = 0; i < nb; ++i)
     if (B[i].data.empty()) P.near_pairs -= (int)B[i].near.size();
-
+  lap(4);
   // targets (target4FMM::setL2P / setDirectIntegration: getBucketAtDeepest)
   P.target_box.assign(np, -1);
   for (int p = 0; p < np; ++p) {
@@ -546,47 +615,56 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   P.nb_dofs.clear();
   P.nb_targets.clear();
   P.nb_ranges.clear();
-  int64_t woff = 0;
-  std::vector<int> mark(ndof, -1);
-  for (size_t bi = 0; bi < P.blocks.size(); ++bi) {
-    Plan::NearBlock& nbk = P.blocks[bi];
-    const int t = nbk.node;
-    std::vector<std::pair<int, int>> rng;
-    auto addr = [&](int n) {
-      if (P.nodes[n].fe > P.nodes[n].fb) rng.push_back({P.nodes[n].fb, P.nodes[n].fe});
-    };
-    addr(t);
-    for (int n : B[t].near) addr(n);
-    for (int a = B[t].parent; a >= 0; a = B[a].parent)
-      for (int n : B[a].near)
-        if (B[n].kids.empty()) addr(n);
-    std::sort(rng.begin(), rng.end());
-    std::vector<std::pair<int, int>> merged;
-    for (auto& r : rng) {
-      if (!merged.empty() && r.first <= merged.back().second)
-        merged.back().second = std::max(merged.back().second, r.second);
-      else
-        merged.push_back(r);
-    }
-    nbk.rng_off = (int)P.nb_ranges.size() / 2;
-    nbk.nrng = (int)merged.size();
-    std::vector<int> dl;
-    for (auto& r : merged) {
-      P.nb_ranges.push_back(r.first);
-      P.nb_ranges.push_back(r.second);
-      for (int s = r.first; s < r.second; ++s)
-        for (int a = 0; a < 3; ++a) {
-          const int d = P.e_dof[s * 3 + a];
-          if (mark[d] != (int)bi) {
-            mark[d] = (int)bi;
-            dl.push_back(d);
+  const int nblk = (int)P.blocks.size();
+  std::vector<std::vector<int>> blk_rng(nblk), blk_dofs(nblk);
+#pragma omp parallel
+  {
+    std::vector<int> mark(ndof, -1);
+#pragma omp for schedule(dynamic, 8)
+    for (int bi = 0; bi < nblk; ++bi) {
+      const int t = P.blocks[bi].node;
+      std::vector<std::pair<int, int>> rng;
+      auto addr = [&](int n) {
+        if (P.nodes[n].fe > P.nodes[n].fb) rng.push_back({P.nodes[n].fb, P.nodes[n].fe});
+      };
+      addr(t);
+      for (int n : B[t].near) addr(n);
+      for (int a = B[t].parent; a >= 0; a = B[a].parent)
+        for (int n : B[a].near)
+          if (B[n].kids.empty()) addr(n);
+      std::sort(rng.begin(), rng.end());
+      std::vector<std::pair<int, int>> merged;
+      for (auto& r : rng) {
+        if (!merged.empty() && r.first <= merged.back().second)
+          merged.back().second = std::max(merged.back().second, r.second);
+        else
+          merged.push_back(r);
+      }
+      std::vector<int>& dl = blk_dofs[bi];
+      for (auto& r : merged) {
+        blk_rng[bi].push_back(r.first);
+        blk_rng[bi].push_back(r.second);
+        for (int s = r.first; s < r.second; ++s)
+          for (int a = 0; a < 3; ++a) {
+            const int d = P.e_dof[s * 3 + a];
+            if (mark[d] != bi) {
+              mark[d] = bi;
+              dl.push_back(d);
+            }
           }
-        }
+      }
+      std::sort(dl.begin(), dl.end());
     }
-    std::sort(dl.begin(), dl.end());
+  }
+  int64_t woff = 0;
+  for (int bi = 0; bi < nblk; ++bi) {
+    Plan::NearBlock& nbk = P.blocks[bi];
+    nbk.rng_off = (int)P.nb_ranges.size() / 2;
+    nbk.nrng = (int)blk_rng[bi].size() / 2;
+    P.nb_ranges.insert(P.nb_ranges.end(), blk_rng[bi].begin(), blk_rng[bi].end());
     nbk.dof_off = (int)P.nb_dofs.size();
-    nbk.ndof = (int)dl.size();
-    P.nb_dofs.insert(P.nb_dofs.end(), dl.begin(), dl.end());
+    nbk.ndof = (int)blk_dofs[bi].size();
+    P.nb_dofs.insert(P.nb_dofs.end(), blk_dofs[bi].begin(), blk_dofs[bi].end());
     nbk.tgt_off = (int)P.nb_targets.size();
     nbk.ntgt = (int)btargets[bi].size();
     P.nb_targets.insert(P.nb_targets.end(), btargets[bi].begin(), btargets[bi].end());
@@ -594,6 +672,7 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     woff += (int64_t)nbk.ntgt * nbk.ndof;
   }
   P.nnz = woff;
+  lap(5);
   // DOF -> incident element vertices
   P.dof_inc_off.assign(ndof + 1, 0);
   for (int s = 0; s < ne; ++s)
@@ -605,6 +684,7 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     for (int s = 0; s < ne; ++s)
       for (int a = 0; a < 3; ++a) P.dof_inc[fill[P.e_dof[s * 3 + a]]++] = s * 3 + a;
   }
+  lap(6);
   return true;
 }
 

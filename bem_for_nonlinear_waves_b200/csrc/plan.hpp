@@ -70,6 +70,16 @@ struct Plan {
   std::vector<int32_t> m2l_off, m2l_src;  // CSR over nodes: sources of each target's M2L
   std::vector<int32_t> near_off, near_nodes;  // CSR over nodes: same-level near buckets
   int64_t m2l_pairs = 0, near_pairs = 0;
+  // M2L grouped by translation vector: pairs of one level whose target - source offset is
+  // the same lattice vector share one irregular-harmonic table.  Pair k is the k-th entry of
+  // the target-major CSR (m2l_off / m2l_src); its partial local goes to slot k.
+  std::vector<double> grp_vec;       // [groups*3] translation (target - source) of each group
+  std::vector<int32_t> grp_off;      // [groups+1] CSR into grp_pair
+  std::vector<int32_t> grp_pair;     // pair slots k, grouped
+  std::vector<int32_t> chunk_grp;    // work chunks of <= 8 pairs: group
+  std::vector<int32_t> chunk_begin;  // first index into grp_pair
+  std::vector<int32_t> chunk_cnt;    // pairs in the chunk
+  std::vector<int32_t> m2l_targets;  // targets with at least one pair
 
   // L2P / near targets: one target per point with DOFs
   std::vector<int32_t> target_box;     // [np] node of the point, -1 if the point has no DOF
@@ -88,6 +98,8 @@ struct Plan {
 
   // DOF -> incident (element position, vertex slot)
   std::vector<int32_t> dof_inc_off, dof_inc;  // dof_inc = pos*3 + slot
+
+  double phase_s[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // host set-up phase timings
 
   std::string error;
 };

@@ -150,11 +150,11 @@ int bem_gpu_get_diag(bem_gpu_ctx* ctx, double* diag);                 /* [n_dof]
 double bem_gpu_scale_factor(const bem_gpu_ctx* ctx);                  /* L */
 int bem_gpu_near_row(bem_gpu_ctx* ctx, int32_t point, int32_t cap, int32_t* dof, double* wG, double* wGn);
 int bem_gpu_face_leaf(bem_gpu_ctx* ctx, int32_t* level, double* corner); /* [n_faces], [3*n_faces] */
-int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out /*[8]: nodes, leaves, depth, added, m2l, near, nnz, targets*/);
+int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out /*[10]: nodes, leaves, depth, added, m2l pairs, near pairs, nnz, near blocks, M2L chunks, M2L translation groups*/);
 
 /* Host-only inspection of the set-up plan (no GPU needed): builds the octree, lists and
  * near-field sparsity for desc with opts and reports, per face, the level and lower corner
- * of the leaf bucket holding it (-1 if none), plus stats[8] as bem_gpu_tree_stats. */
+ * of the leaf bucket holding it (-1 if none), plus stats[10] as bem_gpu_tree_stats. */
 int bem_plan_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* desc, int32_t* face_level, double* face_corner, int64_t* stats);
 
 /* Mat-vec stage timing with CUDA events on the context stream, averaged over repeats:

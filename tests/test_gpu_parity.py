@@ -131,7 +131,8 @@ def test_gpu_full_size_properties(product_lib):
     """60k-node tank (p=10): rigid-mode rows vanish, the operator is linear, GMRES converges."""
     t = make_tank(h=2.0 / 185, noise_sigma=0.2 * 2.0 / 185, seed=1)
     d = build_dofs(t.X, t.tri, t.face_dirichlet)
-    bvp = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=10, dofs=d, solver_tol=1e-8, tol_relative=True)
+    bvp = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=10, dofs=d, solver_tol=1e-8, tol_relative=True,
+                  preconditioner="jacobi")
     bvp.setup()
     n = bvp.matrix_size
     kind = d["dof_kind"]
