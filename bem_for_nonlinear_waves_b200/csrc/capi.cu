@@ -85,6 +85,7 @@ struct bem_gpu_ctx {
   int64_t setup_h2d = 0, setup_launches = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // setup device start/end, solve start/end
   float setup_dev_ms = 0.f;
+  double time_plan = 0.0, time_upload = 0.0;
 
   ~bem_gpu_ctx() {
     for (auto& e : ev)
@@ -301,6 +302,7 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     ctx->err = ctx->plan.error;
     return BEM_ERR_INVALID_ARGUMENT;
   }
+  ctx->time_plan = now_s() - t0;
   Plan& P = ctx->plan;
   cudaStream_t s = ctx->stream;
   const int NC = ncoef(P.opt.p);
@@ -412,6 +414,8 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   CK(cudaMemsetAsync(ctx->GPhin.p, 0, sizeof(double) * P.np, s));
   CK(cudaMemsetAsync(ctx->GnPhi.p, 0, sizeof(double) * P.np, s));
 
+  CK(cudaStreamSynchronize(s));
+  ctx->time_upload = now_s() - t0 - ctx->time_plan;
   // device part of the set-up starts here (inputs resident)
   CK(cudaEventRecord(ctx->ev[0], s));
   // near-field weights
@@ -900,6 +904,8 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     stats->h2d_bytes = ctx->h2d;
     stats->d2h_bytes = ctx->d2h;
     stats->kernel_launches = ctx->launches;
+    stats->time_plan_s = ctx->time_plan;
+    stats->time_upload_s = ctx->time_upload;
   }
   if (!finite) {
     ctx->err = "non-finite solution";

@@ -219,7 +219,7 @@ def main():
     fp64_peak = _lib.load().bem_gpu_fp64_peak_tflops(local)
 
     barrier(world)
-    dev_s = e2e_s = 0.0
+    dev_s = e2e_s = plan_s = upload_s = 0.0
     launches = h2d = d2h = iters = 0
     converged = True
     with ClockSampler(local) as clk:
@@ -230,6 +230,8 @@ def main():
             e2e_s += time.perf_counter() - w0
             st = bvp.stats
             dev_s += st.time_device_s
+            plan_s += st.time_plan_s
+            upload_s += st.time_upload_s
             launches += st.kernel_launches
             h2d += st.h2d_bytes
             d2h += st.d2h_bytes
@@ -253,6 +255,7 @@ def main():
                    "gmres_iterations": iters / args.steps, "converged": converged, "parallelism": f"replicas{world}",
                    "l2": "working set > L2 (near-field weights %.1f GB)" % (tree["nnz"] * 16 / 1e9)},
         "matvecs_per_s": world * 1e3 / prof["total"],
+        "host_setup_s_per_step": {"plan": plan_s / args.steps, "upload": upload_s / args.steps},
         "matvec_stage_ms": prof,
         "e2e": {"value": world * args.steps / e2e_max, "unit": "solves/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},

@@ -93,7 +93,8 @@ typedef struct {
   int64_t h2d_bytes;      /* host->device bytes of setup + solve */
   int64_t d2h_bytes;      /* device->host bytes of setup + solve */
   int64_t kernel_launches;/* kernels launched by setup + solve (graph nodes counted) */
-  int32_t reserved[4];
+  double time_plan_s;     /* host part of the set-up: tree, lists, near-field sparsity */
+  double time_upload_s;   /* host->device copies of the set-up */
 } bem_gpu_stats;
 
 /* 1 if a CUDA device of compute capability 10.x is visible. */
