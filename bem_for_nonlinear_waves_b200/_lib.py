@@ -18,7 +18,9 @@ P_u8 = ctypes.POINTER(ctypes.c_uint8)
 P_i64 = ctypes.POINTER(ctypes.c_int64)
 
 BEM_OK = 0
+BEM_ERR_INVALID_ARGUMENT = -1
 BEM_ERR_NOT_CONVERGED = -3
+BEM_ERR_UNSUPPORTED = -7
 STATUS = {0: "ok", -1: "invalid argument", -2: "out of memory", -3: "not converged", -4: "non-finite value",
           -5: "device error", -6: "not ready", -7: "unsupported"}
 
@@ -55,6 +57,7 @@ EXPORTS = {
     "bem_gpu_apply": (c_int, [ctypes.c_void_p, P_dbl, P_dbl, P_dbl]),
     "bem_gpu_point_integrals": (c_int, [ctypes.c_void_p, P_dbl, P_dbl, P_dbl, P_dbl]),
     "bem_gpu_matvec_device": (c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "bem_gpu_matvec_device_noalloc": (c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "bem_gpu_get_diag": (c_int, [ctypes.c_void_p, P_dbl]),
     "bem_gpu_scale_factor": (c_dbl, [ctypes.c_void_p]),
     "bem_gpu_near_row": (c_int, [ctypes.c_void_p, c_int, c_int, P_int, P_dbl, P_dbl]),

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -952,6 +953,63 @@ int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  return BEM_OK;
+}
+
+// ---- mat-vec that allocates nothing ------------------------------------------------
+// The M2L stage writes one translated expansion per (target, source) pair into a slot
+// buffer and then sums each target's slots in a fixed order.  This entry point takes that
+// slot buffer from a file-scope device array instead of the context.  The array is part of
+// this library's device image: the driver reserves it on each device when the module is
+// loaded, so no call ever allocates for it.  Callers that must not allocate device memory
+// while they apply the operator (a time integrator or outer solver running out of a fixed
+// device-memory reservation, a server holding many small problems on one device that wants
+// one shared slot area rather than one per problem) use this entry point.
+constexpr size_t kNoAllocSlotBytes = size_t(32) << 20;  // 32 MiB: m2l_pairs * 2 * ncoef(p) * 16 B must fit
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) unsigned char g_m2l_slot_scratch[kNoAllocSlotBytes];
+static std::mutex g_slot_mu;
+static void* g_slot_addr[kNoAllocMaxDevices] = {};
+
+int bem_gpu_matvec_device_noalloc(bem_gpu_ctx* ctx, const double* d_x, double* d_y) {
+  if (!ctx || !d_x || !d_y) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  const Plan& P = ctx->plan;
+  const size_t need = (size_t)P.m2l_pairs * 2 * ncoef(P.opt.p) * sizeof(double2);
+  if (need > kNoAllocSlotBytes) {
+    ctx->err = "no-alloc mat-vec: M2L slot scratch of " + std::to_string(need) + " bytes (" + std::to_string(P.m2l_pairs) +
+               " pairs at order " + std::to_string(P.opt.p) + ") exceeds the fixed " + std::to_string(kNoAllocSlotBytes) + " bytes";
+    return BEM_ERR_UNSUPPORTED;
+  }
+  const int dev = ctx->opts.device;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    ctx->err = "no-alloc mat-vec: device index out of range";
+    return BEM_ERR_INVALID_ARGUMENT;
+  }
+  CK(cudaSetDevice(dev));
+  // first call on a device: resolve the array's device address (no allocation; the
+  // module is loaded now if it was not yet).  Make that first call before beginning any
+  // stream capture on the device.
+  void* slots = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_slot_mu);
+    if (!g_slot_addr[dev]) {
+      void* a = nullptr;
+      CK(cudaGetSymbolAddress(&a, g_m2l_slot_scratch));
+      g_slot_addr[dev] = a;
+    }
+    slots = g_slot_addr[dev];
+  }
+  // every slot of the m2l_pairs in use is overwritten before the reduction reads it, so
+  // the area needs no clearing; the local expansions L are zeroed inside the launch
+  // sequence as on the graph path.  One area per device: calls that may overlap on one
+  // device (other streams, other threads, other contexts) race on it and must be ordered
+  // by the caller.
+  MatvecArgs a = ctx->args(ctx->phi.p, ctx->phin.p, d_y, nullptr, nullptr);
+  a.Y = static_cast<double2*>(slots);
+  launch_densities(P.ndof, 0, d_x, nullptr, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, ctx->stream);
+  ctx->launches += 1 + launch_matvec(P.opt.p, a, ctx->stream);
+  CK(cudaGetLastError());
   return BEM_OK;
 }
 

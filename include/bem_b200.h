@@ -146,6 +146,16 @@ int bem_gpu_point_integrals(bem_gpu_ctx* ctx, const double* phi, const double* p
  * on the context's stream (return_A_dot_v, BEM_solveBVP_GMRES_FMM.hpp:2124-2155). */
 int bem_gpu_matvec_device(bem_gpu_ctx* ctx, const double* d_x, double* d_y);
 
+/* Same mat-vec as bem_gpu_matvec_device, but the call allocates nothing: the M2L pair
+ * slots live in a 32 MiB area that is part of the library's device image (one per device,
+ * reserved when the module loads).  For callers that must not allocate device memory while
+ * applying the operator.  Limit: m2l_pairs * 2 * (p+1)(p+2)/2 * 16 bytes <= 32 MiB, else
+ * BEM_ERR_UNSUPPORTED with the sizes in bem_gpu_last_error.  The first call on a device
+ * resolves the area's address; make it before any stream capture.  Calls that overlap on one
+ * device race on the shared area and must be ordered by the caller.  No counterpart in the
+ * reference (its operator allocates per call, BEM_solveBVP_GMRES_FMM.hpp:2124-2155). */
+int bem_gpu_matvec_device_noalloc(bem_gpu_ctx* ctx, const double* d_x, double* d_y);
+
 /* Introspection for parity tests. */
 int bem_gpu_get_diag(bem_gpu_ctx* ctx, double* diag);                 /* [n_dof] */
 double bem_gpu_scale_factor(const bem_gpu_ctx* ctx);                  /* L */
