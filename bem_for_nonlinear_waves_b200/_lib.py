@@ -28,7 +28,7 @@ STATUS = {0: "ok", -1: "invalid argument", -2: "out of memory", -3: "not converg
 class Opts(ctypes.Structure):
     _fields_ = [("expansion_order", c_int), ("mac_theta", c_dbl), ("leaf_max_elements", c_int), ("max_level", c_int),
                 ("tol", c_dbl), ("max_iter", c_int), ("device", c_int), ("tol_relative", c_int), ("preconditioner", c_int),
-                ("reserved", c_int * 3)]
+                ("precision", c_int), ("reserved", c_int * 2)]
 
 
 class Desc(ctypes.Structure):
@@ -39,7 +39,7 @@ class Desc(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("iterations", c_int), ("converged", c_int), ("residual", c_dbl), ("residual_est", c_dbl),
                 ("time_setup_s", c_dbl), ("time_solve_s", c_dbl), ("nnz_near", ctypes.c_int64), ("m2l_pairs", ctypes.c_int64),
-                ("n_nodes", c_int), ("n_leaves", c_int), ("matvecs", c_int), ("reserved0", c_int), ("time_device_s", c_dbl),
+                ("n_nodes", c_int), ("n_leaves", c_int), ("matvecs", c_int), ("matvecs_lo", c_int), ("time_device_s", c_dbl),
                 ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
                 ("time_plan_s", c_dbl), ("time_upload_s", c_dbl)]
 
@@ -64,6 +64,9 @@ EXPORTS = {
     "bem_gpu_face_leaf": (c_int, [ctypes.c_void_p, P_int, P_dbl]),
     "bem_gpu_tree_stats": (c_int, [ctypes.c_void_p, P_i64]),
     "bem_gpu_profile_matvec": (c_int, [ctypes.c_void_p, c_int, P_dbl]),
+    "bem_gpu_matvec_device_mixed": (c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "bem_gpu_profile_matvec_mixed": (c_int, [ctypes.c_void_p, c_int, P_dbl]),
+    "bem_gpu_check_device_status": (c_int, [ctypes.c_void_p]),
     "bem_gpu_fp64_peak_tflops": (c_dbl, [c_int]),
     "bem_plan_inspect": (c_int, [ctypes.POINTER(Opts), ctypes.POINTER(Desc), P_int, P_dbl, P_i64]),
 }

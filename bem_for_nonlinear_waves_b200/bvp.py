@@ -43,7 +43,8 @@ class BEM_BVP:
     """GMRES-FMM Laplace BVP on one B200."""
 
     def __init__(self, X, tri, face_dirichlet, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30,
-                 fmm_max_level=7, solver_tol=1e-9, solver_max_iter=500, device=0, dofs=None, tol_relative=False, preconditioner="none"):
+                 fmm_max_level=7, solver_tol=1e-9, solver_max_iter=500, device=0, dofs=None, tol_relative=False, preconditioner="none",
+                 precision="fp64"):
         self.lib = L.load()
         if not self.lib.bem_gpu_is_available():
             raise RuntimeError("no sm_100 CUDA device visible: the GMRES-FMM solver runs only on the GPU")
@@ -61,6 +62,7 @@ class BEM_BVP:
         o.device = int(device)
         o.tol_relative = 1 if tol_relative else 0
         o.preconditioner = {"none": 0, "jacobi": 1}[preconditioner]
+        o.precision = {"fp64": 0, "mixed": 1}[precision]
         self.opts = o
         self.ctx = self.lib.bem_gpu_create(ctypes.byref(o))
         if not self.ctx:
@@ -181,11 +183,20 @@ class BEM_BVP:
     def matvec_time_ms(self, repeats=10):
         return self.profile_matvec(repeats)["total"]
 
-    def profile_matvec(self, repeats=10):
-        """Per-stage mat-vec time in ms (CUDA events on the solver stream)."""
+    def profile_matvec(self, repeats=10, mixed=False):
+        """Per-stage mat-vec time in ms (CUDA events on the solver stream); mixed=True profiles
+        the tensor-core operator of a precision="mixed" context."""
         st = np.zeros(6)
-        self._check(self.lib.bem_gpu_profile_matvec(self.ctx, int(repeats), L.ptr(st, L.P_dbl)), "profile")
+        fn = self.lib.bem_gpu_profile_matvec_mixed if mixed else self.lib.bem_gpu_profile_matvec
+        self._check(fn(self.ctx, int(repeats), L.ptr(st, L.P_dbl)), "profile")
         return dict(zip(["p2m", "m2m", "m2l", "l2l", "targets", "total"], map(float, st)))
+
+    def matvec_device(self, d_x, d_y, mixed=False):
+        """y = A x on device buffers given as integer pointers (n_dof doubles each), on the
+        solver's stream; mixed=True uses the tensor-core operator."""
+        fn = self.lib.bem_gpu_matvec_device_mixed if mixed else self.lib.bem_gpu_matvec_device
+        self._check(fn(self.ctx, int(d_x), int(d_y)), "matvec_device")
+        self._check(self.lib.bem_gpu_check_device_status(self.ctx), "device status")
 
 
 def inspect_plan(X, tri, face_dirichlet, dofs=None, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30,

@@ -81,6 +81,17 @@ struct bem_gpu_ctx {
   DBuf<double> V, w, hdev, partial, xdev, bdev, rdev, ydev, tmp, dinv;
   int V_cols = 0;
   int graph_kernels = 0;
+  // mixed precision: tensor-core M2L tables and buffers; graph of the low-precision A.x
+  bool mixed = false;
+  DBuf<int> tc_item_tab, tc_item_begin, tc_item_cnt, tc_pair, tc_err;
+  DBuf<double> tc_tabvec, tc_alpha, node_dL;
+  DBuf<uint16_t> tc_T, tc_Mt;
+  DBuf<float> tc_escale;
+  DBuf<unsigned int> tc_max;
+  int tc_grid = 148;
+  cudaGraph_t graph_lo = nullptr;
+  cudaGraphExec_t graph_exec_lo = nullptr;
+  int graph_kernels_lo = 0;
   // accounting of the current setup + solve
   int64_t h2d = 0, d2h = 0, launches = 0;
   int64_t setup_h2d = 0, setup_launches = 0;
@@ -93,6 +104,8 @@ struct bem_gpu_ctx {
       if (e) cudaEventDestroy(e);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
+    if (graph_exec_lo) cudaGraphExecDestroy(graph_exec_lo);
+    if (graph_lo) cudaGraphDestroy(graph_lo);
     if (stream) cudaStreamDestroy(stream);
   }
   MatvecArgs args(const double* d_phi, const double* d_phin, double* d_rows, double* d_gphin, double* d_gnphi) const {
@@ -147,6 +160,23 @@ struct bem_gpu_ctx {
     a.GnPhi = d_gnphi;
     return a;
   }
+  // switches an argument set to the tensor-core M2L
+  void set_tc(MatvecArgs& a) const {
+    a.use_tc = 1;
+    a.n_tc_items = (int)plan.tc_item_tab.size();
+    a.tc_grid = tc_grid;
+    a.tc_item_tab = tc_item_tab.p;
+    a.tc_item_begin = tc_item_begin.p;
+    a.tc_item_cnt = tc_item_cnt.p;
+    a.tc_pair = tc_pair.p;
+    a.tc_tab = tc_T.p;
+    a.tc_Mt = tc_Mt.p;
+    a.tc_escale = tc_escale.p;
+    a.tc_Y = reinterpret_cast<float*>(Y.p);
+    a.tc_err = tc_err.p;
+    a.node_dL = node_dL.p;
+    a.tc_alpha = tc_alpha.p;
+  }
 };
 
 #define CK(call)                                                               \
@@ -193,30 +223,49 @@ cudaError_t up(bem_gpu_ctx* ctx, DBuf<T>& b, const std::vector<T>& v) {
   return b.upload(v, ctx->stream);
 }
 
-int build_graph(bem_gpu_ctx* ctx) {
-  if (ctx->graph_exec) {
-    cudaGraphExecDestroy(ctx->graph_exec);
-    ctx->graph_exec = nullptr;
+// Captures A.x (mv_in -> mv_out) as a graph; tc selects the tensor-core M2L.
+int capture_matvec(bem_gpu_ctx* ctx, bool tc, cudaGraph_t& graph, cudaGraphExec_t& exec, int& kernels) {
+  if (exec) {
+    cudaGraphExecDestroy(exec);
+    exec = nullptr;
   }
-  if (ctx->graph) {
-    cudaGraphDestroy(ctx->graph);
-    ctx->graph = nullptr;
+  if (graph) {
+    cudaGraphDestroy(graph);
+    graph = nullptr;
   }
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   launch_densities(ctx->plan.ndof, 0, ctx->mv_in.p, nullptr, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, ctx->stream);
-  run_fmm(ctx, ctx->mv_out.p, nullptr, nullptr);
-  CK(cudaStreamEndCapture(ctx->stream, &ctx->graph));
-  CK(cudaGraphInstantiate(&ctx->graph_exec, ctx->graph, 0));
+  MatvecArgs a = ctx->args(ctx->phi.p, ctx->phin.p, ctx->mv_out.p, nullptr, nullptr);
+  if (tc) ctx->set_tc(a);
+  launch_matvec(ctx->plan.opt.p, a, ctx->stream);
+  CK(cudaStreamEndCapture(ctx->stream, &graph));
+  CK(cudaGraphInstantiate(&exec, graph, 0));
   size_t nn = 0;
-  CK(cudaGraphGetNodes(ctx->graph, nullptr, &nn));
+  CK(cudaGraphGetNodes(graph, nullptr, &nn));
   std::vector<cudaGraphNode_t> nodes(nn);
-  if (nn) CK(cudaGraphGetNodes(ctx->graph, nodes.data(), &nn));
-  ctx->graph_kernels = 0;
+  if (nn) CK(cudaGraphGetNodes(graph, nodes.data(), &nn));
+  kernels = 0;
   for (auto nd : nodes) {
     cudaGraphNodeType ty;
     CK(cudaGraphNodeGetType(nd, &ty));
-    if (ty == cudaGraphNodeTypeKernel) ++ctx->graph_kernels;
+    if (ty == cudaGraphNodeTypeKernel) ++kernels;
   }
+  return BEM_OK;
+}
+
+int build_graph(bem_gpu_ctx* ctx) {
+  int rc = capture_matvec(ctx, false, ctx->graph, ctx->graph_exec, ctx->graph_kernels);
+  if (rc != BEM_OK || !ctx->mixed) return rc;
+  return capture_matvec(ctx, true, ctx->graph_lo, ctx->graph_exec_lo, ctx->graph_kernels_lo);
+}
+
+// y = A_lo x on device buffers (tensor-core M2L), on the context's stream
+int matvec_lo(bem_gpu_ctx* ctx, const double* d_x, double* d_y) {
+  const int N = ctx->plan.ndof;
+  cudaStream_t s = ctx->stream;
+  if (d_x != ctx->mv_in.p) CK(cudaMemcpyAsync(ctx->mv_in.p, d_x, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+  CK(cudaGraphLaunch(ctx->graph_exec_lo, s));
+  if (d_y != ctx->mv_out.p) CK(cudaMemcpyAsync(d_y, ctx->mv_out.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
   return BEM_OK;
 }
 
@@ -293,6 +342,14 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   ctx->ready = false;
   ctx->h2d = ctx->d2h = ctx->launches = 0;
   const double t0 = now_s();
+  if (ctx->opts.precision == 1 && !tc_supported(ctx->opts.expansion_order)) {
+    ctx->err = "mixed precision needs (expansion_order+1)^2 <= 128 (p <= 10)";
+    return BEM_ERR_UNSUPPORTED;
+  }
+  if (ctx->opts.precision != 0 && ctx->opts.precision != 1) {
+    ctx->err = "precision must be 0 (fp64) or 1 (mixed)";
+    return BEM_ERR_INVALID_ARGUMENT;
+  }
   PlanOptions po;
   po.p = ctx->opts.expansion_order;
   po.theta = ctx->opts.mac_theta;
@@ -393,8 +450,40 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     const int Q = 2 * P.opt.p;
     CK(ctx->Sg.alloc((size_t)std::max(ngroups, 1) * (Q + 1) * (Q + 1)));
     CK(ctx->Mf.alloc((size_t)nb * 2 * (P.opt.p + 1) * (P.opt.p + 1)));
-    CK(ctx->Y.alloc((size_t)std::max<int64_t>(P.m2l_pairs, 1) * 2 * NC));
+    // per-pair slots; the tensor-core path stores [2][tc_kp] floats per pair in the same buffer
+    const size_t y64 = (size_t)std::max<int64_t>(P.m2l_pairs, 1) * 2 * NC;
+    const size_t ytc = ((size_t)std::max<int64_t>(P.m2l_pairs, 1) * 2 * tc_kp(P.opt.p) * sizeof(float) + sizeof(double2) - 1) / sizeof(double2);
+    CK(ctx->Y.alloc(ctx->opts.precision == 1 ? std::max(y64, ytc) : y64));
     launch_s_tables(P.opt.p, ngroups, ctx->grp_vec.p, ctx->Sg.p, s);
+    ctx->launches += 1;
+  }
+  ctx->mixed = ctx->opts.precision == 1;
+  if (ctx->mixed) {  // tensor-core M2L: translation tables, multipole rows, work items
+    const int p = P.opt.p, kp = tc_kp(p);
+    build_tc_groups(P, tc_max_pairs());
+    const int ntab = (int)(P.tc_tab.size() / 4);
+    std::vector<double> dl(nb), al(kp);
+    for (int i = 0; i < nb; ++i) dl[i] = P.nodes[i].dL;
+    tc_alpha_host(p, al.data());
+    CK(up(ctx, ctx->tc_item_tab, P.tc_item_tab));
+    CK(up(ctx, ctx->tc_item_begin, P.tc_item_begin));
+    CK(up(ctx, ctx->tc_item_cnt, P.tc_item_cnt));
+    CK(up(ctx, ctx->tc_pair, P.tc_pair));
+    CK(up(ctx, ctx->tc_tabvec, P.tc_tab));
+    CK(up(ctx, ctx->tc_alpha, al));
+    CK(up(ctx, ctx->node_dL, dl));
+    CK(ctx->tc_T.alloc((size_t)std::max(ntab, 1) * tc_table_bytes(p) / 2));
+    CK(ctx->tc_Mt.alloc((size_t)(2 * nb + 1) * 2 * kp));
+    CK(cudaMemsetAsync(ctx->tc_Mt.p, 0, sizeof(uint16_t) * ctx->tc_Mt.n, s));
+    CK(ctx->tc_escale.alloc((size_t)2 * nb));
+    CK(ctx->tc_err.alloc(1));
+    CK(cudaMemsetAsync(ctx->tc_err.p, 0, sizeof(int), s));
+    CK(ctx->tc_max.alloc(1));
+    CK(cudaMemsetAsync(ctx->tc_max.p, 0, sizeof(unsigned int), s));
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->opts.device));
+    ctx->tc_grid = sms;
+    launch_tc_tables(p, ntab, ctx->tc_tabvec.p, ctx->tc_alpha.p, ctx->tc_T.p, ctx->tc_max.p, s);
     ctx->launches += 1;
   }
   CK(ctx->M.alloc((size_t)nb * 2 * NC));
@@ -460,6 +549,17 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     CK(cudaStreamSynchronize(s));
   }
   CK(cudaEventRecord(ctx->ev[1], s));
+  if (ctx->mixed) {  // FP16 tables must stay far from the FP16 range limit (65504)
+    unsigned int bits = 0;
+    CK(cudaMemcpyAsync(&bits, ctx->tc_max.p, sizeof(bits), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    float mx;
+    std::memcpy(&mx, &bits, sizeof(mx));
+    if (!(mx < 1024.f)) {
+      ctx->err = "mixed precision: translation table entry " + std::to_string(mx) + " too large for FP16 operands";
+      return BEM_ERR_UNSUPPORTED;
+    }
+  }
   int rc = build_graph(ctx);
   if (rc != BEM_OK) return rc;
   CK(cudaStreamSynchronize(s));
@@ -704,13 +804,27 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     ctx->launches += ctx->graph_kernels;
     return bem_gpu_matvec_device(ctx, din, dout);
   };
+  // the Krylov operator: FP64, or the tensor-core M2L one in mixed precision
+  const bool mixed = ctx->mixed;
+  int matvecs_lo = 0;
+  auto kmatvec = [&](const double* din, double* dout) -> int {
+    if (!mixed) return matvec(din, dout);
+    ++matvecs_lo;
+    ctx->launches += ctx->graph_kernels_lo;
+    return matvec_lo(ctx, din, dout);
+  };
   // operator seen by GMRES: A D^{-1} with right Jacobi scaling, else A
   auto opmatvec = [&](const double* din, double* dout) -> int {
-    if (!jacobi) return matvec(din, dout);
+    if (!jacobi) return kmatvec(din, dout);
     launch_mul(N, ctx->dinv.p, din, ctx->tmp.p, s);
     ctx->launches += 1;
-    return matvec(ctx->tmp.p, dout);
+    return kmatvec(ctx->tmp.p, dout);
   };
+  // Mixed precision is iterative refinement: each GMRES cycle solves A_lo d = r to
+  // max(tol, kInnerRtol |r|) and the cycle ends with the FP64 true residual, from which the
+  // next cycle starts (that residual is reused, not recomputed).
+  constexpr double kInnerRtol = 1e-5;
+  bool have_res = false;
   auto norm_of = [&](const double* v, double* out) -> int {
     launch_mdot(v, N, 1, v, N, ctx->partial.p, ctx->hdev.p, s);
     ctx->launches += 2;
@@ -725,12 +839,19 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   std::vector<double> hh(2 * cols + 2);
   while (iters < max_iter && r_true > tol) {
     const int k_cycle_max = std::min(100, max_iter - iters);
-    // r0 = b - A x
-    if ((rc = matvec(ctx->xdev.p, ctx->rdev.p)) != BEM_OK) return rc;
-    launch_axpby(N, 1.0, ctx->bdev.p, -1.0, ctx->rdev.p, s);  // r = b - r
-    ctx->launches += 1;
     double beta = 0.0;
-    if ((rc = norm_of(ctx->rdev.p, &beta)) != BEM_OK) return rc;
+    if (have_res) {  // rdev = A x - b from the true-residual check that ended the last cycle
+      launch_axpby(N, 0.0, ctx->bdev.p, -1.0, ctx->rdev.p, s);
+      ctx->launches += 1;
+      beta = r_true;
+      have_res = false;
+    } else {
+      // r0 = b - A x
+      if ((rc = matvec(ctx->xdev.p, ctx->rdev.p)) != BEM_OK) return rc;
+      launch_axpby(N, 1.0, ctx->bdev.p, -1.0, ctx->rdev.p, s);  // r = b - r
+      ctx->launches += 1;
+      if ((rc = norm_of(ctx->rdev.p, &beta)) != BEM_OK) return rc;
+    }
     if (!std::isfinite(beta)) {
       ctx->err = "non-finite residual";
       return BEM_ERR_NAN;
@@ -845,13 +966,18 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     if ((rc = add_basis()) != BEM_OK) return rc;
     iters += 1;
     int sat = 0;
+    const double check_at = mixed ? std::max(tol, kInnerRtol * beta) : tol * 10.;
     while (true) {
       if ((rc = add_basis()) != BEM_OK) return rc;
       ++iters;
-      if (err <= tol * 10.) {
+      if (err <= check_at) {
         if ((rc = update_from_base()) != BEM_OK) return rc;
         if ((rc = true_res(&r_true)) != BEM_OK) return rc;
         if (r_true <= tol) break;
+        if (mixed) {  // refine: next cycle from this residual
+          have_res = true;
+          break;
+        }
         if (sat++ >= 5) break;
       }
       if (iters >= max_iter && (int)Rc.size() >= k_cycle_max) {
@@ -869,6 +995,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     }
   }
   CK(cudaEventRecord(ctx->ev[3], s));
+  if (mixed && (rc = bem_gpu_check_device_status(ctx)) != BEM_OK) return rc;
   std::vector<double> x(N);
   CK(cudaMemcpyAsync(x.data(), ctx->xdev.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
   ctx->d2h += 8LL * N;
@@ -901,6 +1028,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     stats->n_nodes = (int)nodes;
     stats->n_leaves = (int)P.leaves.size();
     stats->matvecs = matvecs;
+    stats->matvecs_lo = matvecs_lo;
     stats->time_device_s = 1e-3 * ((double)ctx->setup_dev_ms + (double)solve_dev_ms);
     stats->h2d_bytes = ctx->h2d;
     stats->d2h_bytes = ctx->d2h;
@@ -922,9 +1050,8 @@ int bem_gpu_solve_bvp(bem_gpu_ctx* ctx, const bem_bvp_desc* desc, const double* 
   return bem_gpu_solve(ctx, known, x0, out_phi, out_phin, stats);
 }
 
-int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms) {
-  if (!ctx || !stage_ms || repeats < 1) return BEM_ERR_INVALID_ARGUMENT;
-  if (!ctx->ready) return BEM_ERR_NOT_READY;
+namespace {
+int profile_matvec(bem_gpu_ctx* ctx, int repeats, bool tc, double* stage_ms) {
   CK(cudaSetDevice(ctx->opts.device));
   cudaStream_t s = ctx->stream;
   const int N = ctx->plan.ndof;
@@ -937,13 +1064,15 @@ int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms) {
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   const int stages[5] = {STAGE_P2M, STAGE_M2M, STAGE_M2L, STAGE_L2L, STAGE_TARGETS};
+  MatvecArgs a = ctx->args(ctx->phi.p, ctx->phin.p, ctx->mv_out.p, nullptr, nullptr);
+  if (tc) ctx->set_tc(a);
   for (int k = 0; k < 6; ++k) {
     CK(cudaEventRecord(e0, s));
     for (int r = 0; r < repeats; ++r) {
       if (k < 5)
-        launch_matvec(ctx->plan.opt.p, ctx->args(ctx->phi.p, ctx->phin.p, ctx->mv_out.p, nullptr, nullptr), s, stages[k]);
+        launch_matvec(ctx->plan.opt.p, a, s, stages[k]);
       else
-        CK(cudaGraphLaunch(ctx->graph_exec, s));
+        CK(cudaGraphLaunch(tc ? ctx->graph_exec_lo : ctx->graph_exec, s));
     }
     CK(cudaEventRecord(e1, s));
     CK(cudaEventSynchronize(e1));
@@ -953,6 +1082,46 @@ int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  return BEM_OK;
+}
+}  // namespace
+
+int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms) {
+  if (!ctx || !stage_ms || repeats < 1) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  return profile_matvec(ctx, repeats, false, stage_ms);
+}
+
+int bem_gpu_profile_matvec_mixed(bem_gpu_ctx* ctx, int repeats, double* stage_ms) {
+  if (!ctx || !stage_ms || repeats < 1) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  if (!ctx->mixed) {
+    ctx->err = "context was not set up with precision = 1";
+    return BEM_ERR_UNSUPPORTED;
+  }
+  return profile_matvec(ctx, repeats, true, stage_ms);
+}
+
+int bem_gpu_matvec_device_mixed(bem_gpu_ctx* ctx, const double* d_x, double* d_y) {
+  if (!ctx || !d_x || !d_y) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  if (!ctx->mixed) {
+    ctx->err = "context was not set up with precision = 1";
+    return BEM_ERR_UNSUPPORTED;
+  }
+  return matvec_lo(ctx, d_x, d_y);
+}
+
+int bem_gpu_check_device_status(bem_gpu_ctx* ctx) {
+  if (!ctx) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->mixed) return BEM_OK;
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, ctx->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (flag) {
+    ctx->err = "tensor-core M2L: a bounded wait on the MMA completion gave up";
+    return BEM_ERR_DEVICE;
+  }
   return BEM_OK;
 }
 

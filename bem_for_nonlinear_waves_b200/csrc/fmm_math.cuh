@@ -90,4 +90,45 @@ __device__ __forceinline__ void S_column(int q, double x, double y, double z, do
   }
 }
 
+// full (negative-order) table fill from one lane per column
+template <int Q>
+__device__ __forceinline__ void F_full_column(int m, double x, double y, double z, double2* T /*(Q+1)^2*/) {
+  if (m > Q) return;
+  const double r2 = x * x + y * y + z * z;
+  double2 f = make_double2(1.0, 0.0);
+  for (int k = 1; k <= m; ++k) f = cscale(cmul(f, make_double2(x, y)), 1.0 / (2.0 * k));
+  double2 prev = make_double2(0.0, 0.0), cur = f;
+  for (int n = m; n <= Q; ++n) {
+    if (n > m) {
+      const double inv = 1.0 / double(n * n - m * m);
+      double2 nx = make_double2(((2 * n - 1) * z * cur.x - r2 * prev.x) * inv, ((2 * n - 1) * z * cur.y - r2 * prev.y) * inv);
+      prev = cur;
+      cur = nx;
+    }
+    T[n * (n + 1) + m] = cur;
+    if (m > 0) T[n * (n + 1) - m] = (m & 1) ? make_double2(-cur.x, cur.y) : make_double2(cur.x, -cur.y);
+  }
+}
+
+template <int Q>
+__device__ __forceinline__ void S_full_column(int q, double x, double y, double z, double2* T /*(Q+1)^2*/) {
+  if (q > Q) return;
+  const double r2 = x * x + y * y + z * z;
+  const double inv_r2 = 1.0 / r2;
+  double2 s = make_double2(1.0 / sqrt(r2), 0.0);
+  for (int k = 1; k <= q; ++k) s = cscale(cmul(s, make_double2(x, y)), (2.0 * k - 1.0) * inv_r2);
+  double2 prev = make_double2(0.0, 0.0), cur = s;
+  for (int l = q; l <= Q; ++l) {
+    if (l > q) {
+      const double a = (2 * l - 1) * z;
+      const double b = double((l - 1 + q) * (l - 1 - q));
+      double2 nx = make_double2((a * cur.x - b * prev.x) * inv_r2, (a * cur.y - b * prev.y) * inv_r2);
+      prev = cur;
+      cur = nx;
+    }
+    T[l * (l + 1) + q] = cur;
+    if (q > 0) T[l * (l + 1) - q] = (q & 1) ? make_double2(-cur.x, cur.y) : make_double2(cur.x, -cur.y);
+  }
+}
+
 }  // namespace bemb200

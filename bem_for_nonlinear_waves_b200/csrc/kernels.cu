@@ -155,47 +155,6 @@ __global__ void __launch_bounds__(128) k_p2m(const int* __restrict__ leaves, con
   }
 }
 
-// full (negative-order) table fill from one lane per column
-template <int Q>
-__device__ __forceinline__ void F_full_column(int m, double x, double y, double z, double2* T /*(Q+1)^2*/) {
-  if (m > Q) return;
-  const double r2 = x * x + y * y + z * z;
-  double2 f = make_double2(1.0, 0.0);
-  for (int k = 1; k <= m; ++k) f = cscale(cmul(f, make_double2(x, y)), 1.0 / (2.0 * k));
-  double2 prev = make_double2(0.0, 0.0), cur = f;
-  for (int n = m; n <= Q; ++n) {
-    if (n > m) {
-      const double inv = 1.0 / double(n * n - m * m);
-      double2 nx = make_double2(((2 * n - 1) * z * cur.x - r2 * prev.x) * inv, ((2 * n - 1) * z * cur.y - r2 * prev.y) * inv);
-      prev = cur;
-      cur = nx;
-    }
-    T[n * (n + 1) + m] = cur;
-    if (m > 0) T[n * (n + 1) - m] = (m & 1) ? make_double2(-cur.x, cur.y) : make_double2(cur.x, -cur.y);
-  }
-}
-
-template <int Q>
-__device__ __forceinline__ void S_full_column(int q, double x, double y, double z, double2* T /*(Q+1)^2*/) {
-  if (q > Q) return;
-  const double r2 = x * x + y * y + z * z;
-  const double inv_r2 = 1.0 / r2;
-  double2 s = make_double2(1.0 / sqrt(r2), 0.0);
-  for (int k = 1; k <= q; ++k) s = cscale(cmul(s, make_double2(x, y)), (2.0 * k - 1.0) * inv_r2);
-  double2 prev = make_double2(0.0, 0.0), cur = s;
-  for (int l = q; l <= Q; ++l) {
-    if (l > q) {
-      const double a = (2 * l - 1) * z;
-      const double b = double((l - 1 + q) * (l - 1 - q));
-      double2 nx = make_double2((a * cur.x - b * prev.x) * inv_r2, (a * cur.y - b * prev.y) * inv_r2);
-      prev = cur;
-      cur = nx;
-    }
-    T[l * (l + 1) + q] = cur;
-    if (q > 0) T[l * (l + 1) - q] = (q & 1) ? make_double2(-cur.x, cur.y) : make_double2(cur.x, -cur.y);
-  }
-}
-
 // expand half-stored coefficients [2][NC] into full [2][(P+1)^2]
 template <int P>
 __device__ __forceinline__ void expand_full(const double2* __restrict__ src, double2* dst) {
@@ -776,7 +735,9 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     }
   if (stages & STAGE_M2L) {
     cudaMemsetAsync(a.L, 0, sizeof(double2) * 2 * NC * (size_t)a.n_nodes, st);
-    if (a.n_chunks > 0) {
+    if (a.use_tc) {
+      launches += launch_m2l_tc(P, a, st);
+    } else if (a.n_chunks > 0) {
       constexpr int NF = (P + 1) * (P + 1);
       const int64_t tot = (int64_t)a.n_nodes * 2 * NF;
       int ge = (int)std::min<int64_t>((tot + 255) / 256, 148 * 16);

@@ -46,6 +46,20 @@ struct MatvecArgs {
   double2* Y = nullptr;         // per-pair partial locals
   double2* M = nullptr;
   double2* L = nullptr;
+  // tensor-core M2L (mixed precision); used instead of the FP64 M2L when use_tc != 0
+  int use_tc = 0;
+  int n_tc_items = 0, tc_grid = 0;
+  const int* tc_item_tab = nullptr;
+  const int* tc_item_begin = nullptr;
+  const int* tc_item_cnt = nullptr;
+  const int* tc_pair = nullptr;
+  const void* tc_tab = nullptr;  // FP16 hi/lo table images
+  void* tc_Mt = nullptr;         // FP16 hi/lo multipole rows [2*n_nodes+1][2][KP]
+  float* tc_escale = nullptr;    // [2*n_nodes] power-of-two column scales
+  float* tc_Y = nullptr;         // per-pair partial locals [pairs][2][KP]
+  int* tc_err = nullptr;         // set when a bounded wait gave up
+  const double* node_dL = nullptr;
+  const double* tc_alpha = nullptr;  // [KP] sqrt((n+m)!(n-m)!) per real coefficient
   // targets
   int n_blocks = 0, chunk = 0, max_ntgt = 0;
   const NearBlockDev* blocks = nullptr;
@@ -89,6 +103,15 @@ void launch_s_tables(int p, int ngroups, const double* gvec, double2* Sg, cudaSt
 enum { STAGE_P2M = 1, STAGE_M2M = 2, STAGE_M2L = 4, STAGE_L2L = 8, STAGE_TARGETS = 16, STAGE_ALL = 31 };
 // returns the number of kernels launched
 int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages = STAGE_ALL);
+
+// tensor-core M2L (m2l_tc.cu)
+int tc_supported(int p);            // 1 if (p+1)^2 <= 128
+int tc_kp(int p);                   // real coefficients per row, padded to 16
+size_t tc_table_bytes(int p);       // bytes of one table (hi + lo images)
+int tc_max_pairs();                 // pairs per work item
+void tc_alpha_host(int p, double* alpha /*[tc_kp(p)]*/);
+void launch_tc_tables(int p, int ntab, const double* tab, const double* alpha, void* T, unsigned int* maxbits, cudaStream_t st);
+int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st);
 void launch_densities(int n, int mode, const double* x, const double* known, const int* kind, double* phi, double* phin, cudaStream_t st);
 void launch_near_weights(const NearArgs& a, cudaStream_t st);
 void launch_diag(int n, const int* dof_point, const double* GnPhi, double* diag, cudaStream_t st);

@@ -688,4 +688,57 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   return true;
 }
 
+void build_tc_groups(Plan& P, int max_pairs) {
+  const int nb = (int)P.nodes.size();
+  const int64_t npair = P.m2l_pairs;
+  std::vector<int> pair_tgt(npair);
+  for (int t = 0; t < nb; ++t)
+    for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) pair_tgt[k] = t;
+  // key: lattice offset r = (X_t - X_s)/dL_t of equal-size buckets (any level), else unique
+  std::vector<std::pair<long long, int>> keyed(npair);
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < npair; ++k) {
+    const auto& T = P.nodes[pair_tgt[k]];
+    const auto& S = P.nodes[P.m2l_src[k]];
+    bool lattice = std::abs(S.dL - T.dL) <= 1e-12 * T.dL;
+    long long r[3];
+    for (int a = 0; a < 3; ++a) {
+      const double q = (T.X[a] - S.X[a]) / T.dL;
+      r[a] = std::llround(q);
+      if (std::abs(q - (double)r[a]) > 1e-9 || std::abs(r[a]) > 500) lattice = false;
+    }
+    const long long key = ((r[0] + 512) << 20) | ((r[1] + 512) << 10) | (r[2] + 512);
+    keyed[k] = {lattice ? key : ((1LL << 40) + k), (int)k};
+  }
+  std::stable_sort(keyed.begin(), keyed.end());
+  P.tc_tab.clear();
+  P.tc_pair.resize(npair);
+  P.tc_item_tab.clear();
+  P.tc_item_begin.clear();
+  P.tc_item_cnt.clear();
+  for (int64_t i = 0; i < npair;) {
+    const int k0 = keyed[i].second;
+    const auto& T = P.nodes[pair_tgt[k0]];
+    const auto& S = P.nodes[P.m2l_src[k0]];
+    const bool lattice = keyed[i].first < (1LL << 40);
+    for (int a = 0; a < 3; ++a) {
+      const double q = (T.X[a] - S.X[a]) / T.dL;
+      P.tc_tab.push_back(lattice ? (double)std::llround(q) : q);
+    }
+    P.tc_tab.push_back(lattice ? 1.0 : S.dL / T.dL);
+    const int tab = (int)(P.tc_tab.size() / 4) - 1;
+    int64_t j = i;
+    while (j < npair && keyed[j].first == keyed[i].first) {
+      P.tc_pair[j] = keyed[j].second;
+      ++j;
+    }
+    for (int64_t b = i; b < j; b += max_pairs) {
+      P.tc_item_tab.push_back(tab);
+      P.tc_item_begin.push_back((int)b);
+      P.tc_item_cnt.push_back((int)std::min<int64_t>(max_pairs, j - b));
+    }
+    i = j;
+  }
+}
+
 }  // namespace bemb200

@@ -80,6 +80,14 @@ struct Plan {
   std::vector<int32_t> chunk_begin;  // first index into grp_pair
   std::vector<int32_t> chunk_cnt;    // pairs in the chunk
   std::vector<int32_t> m2l_targets;  // targets with at least one pair
+  // tensor-core M2L (mixed precision): pairs grouped by their translation measured in
+  // target-bucket sizes, so one table serves a lattice offset on every level; work items of
+  // at most tc_item_max pairs of one table.  Filled by build_tc_groups().
+  std::vector<double> tc_tab;        // [ntab*4]: (X_t - X_s) / dL_t, dL_s / dL_t
+  std::vector<int32_t> tc_pair;      // pair slots k ordered by table
+  std::vector<int32_t> tc_item_tab;  // table of each work item
+  std::vector<int32_t> tc_item_begin;
+  std::vector<int32_t> tc_item_cnt;
 
   // L2P / near targets: one target per point with DOFs
   std::vector<int32_t> target_box;     // [np] node of the point, -1 if the point has no DOF
@@ -111,5 +119,8 @@ int build_dofs(int np, const double* X, int nf, const int32_t* tri, const uint8_
 // Builds the plan; returns false and sets plan.error on invalid input.
 bool build_plan(Plan& plan, const PlanOptions& opt, int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int ndof,
                 const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof);
+
+// Groups the M2L pairs for the tensor-core path (tc_* fields); items hold <= max_pairs pairs.
+void build_tc_groups(Plan& plan, int max_pairs);
 
 }  // namespace bemb200

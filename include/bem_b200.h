@@ -57,7 +57,10 @@ typedef struct {
   int32_t device;            /* CUDA device ordinal */
   int32_t tol_relative;      /* 0: stop at |A x - b| <= tol (reference semantics); 1: at <= tol*|b| */
   int32_t preconditioner;    /* 0: none (reference default); 1: right Jacobi from the near-field diagonal */
-  int32_t reserved[3];
+  int32_t precision;         /* 0: FP64 throughout; 1: mixed -- GMRES corrections use the tensor-core
+                                M2L (FP16 split operands, FP32 accumulate), FP64 outer refinement on the
+                                true residual, same stopping test; needs p <= 10 */
+  int32_t reserved[2];
 } bem_gpu_opts;
 
 /* One boundary-value problem.  The DOF table is what the reference's setNodeFaceIndices()
@@ -87,8 +90,8 @@ typedef struct {
   int64_t m2l_pairs;      /* box pairs in the M2L lists */
   int32_t n_nodes;        /* non-empty octree nodes */
   int32_t n_leaves;
-  int32_t matvecs;        /* operator applications in this solve */
-  int32_t reserved0;
+  int32_t matvecs;        /* FP64 operator applications in this solve */
+  int32_t matvecs_lo;     /* tensor-core (mixed precision) operator applications */
   double time_device_s;   /* CUDA-event time of the device work of setup + solve */
   int64_t h2d_bytes;      /* host->device bytes of setup + solve */
   int64_t d2h_bytes;      /* device->host bytes of setup + solve */
@@ -171,6 +174,17 @@ int bem_plan_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* desc, int32_t
 /* Mat-vec stage timing with CUDA events on the context stream, averaged over repeats:
  * stage_ms = [p2m, m2m, m2l, l2l, near+l2p+rows, whole graph-launched mat-vec]. */
 int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[6]*/);
+
+/* Mixed precision (context set up with opts.precision = 1).  No reference counterpart: the
+ * reference's M2L is FP64 only (lib/include/moments.hpp:732-764).
+ * bem_gpu_matvec_device_mixed: y = A_lo x on device buffers (tensor-core M2L, everything
+ *   else FP64), on the context's stream — the correction operator of the mixed solve.
+ * bem_gpu_profile_matvec_mixed: stage times of that operator, same layout as above.
+ * bem_gpu_check_device_status: BEM_ERR_DEVICE if a bounded device-side wait of the
+ *   tensor-core M2L gave up since set-up (the results of that launch are invalid). */
+int bem_gpu_matvec_device_mixed(bem_gpu_ctx* ctx, const double* d_x, double* d_y);
+int bem_gpu_profile_matvec_mixed(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[6]*/);
+int bem_gpu_check_device_status(bem_gpu_ctx* ctx);
 
 /* FP64 FMA throughput of the device (TFLOP/s), measured by a short probe kernel. */
 double bem_gpu_fp64_peak_tflops(int32_t device);
