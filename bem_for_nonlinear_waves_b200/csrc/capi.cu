@@ -89,6 +89,7 @@ struct bem_gpu_ctx {
   DBuf<float> tc_escale;
   DBuf<unsigned int> tc_max;
   int tc_grid = 148;
+  std::vector<unsigned char> tc_map;  // TMA tensor map over tc_Mt (host copy, passed by value)
   cudaGraph_t graph_lo = nullptr;
   cudaGraphExec_t graph_exec_lo = nullptr;
   int graph_kernels_lo = 0;
@@ -176,6 +177,7 @@ struct bem_gpu_ctx {
     a.tc_err = tc_err.p;
     a.node_dL = node_dL.p;
     a.tc_alpha = tc_alpha.p;
+    a.tc_rows_map = tc_map.data();
   }
 };
 
@@ -450,9 +452,9 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     const int Q = 2 * P.opt.p;
     CK(ctx->Sg.alloc((size_t)std::max(ngroups, 1) * (Q + 1) * (Q + 1)));
     CK(ctx->Mf.alloc((size_t)nb * 2 * (P.opt.p + 1) * (P.opt.p + 1)));
-    // per-pair slots; the tensor-core path stores [2][tc_kp] floats per pair in the same buffer
+    // per-pair slots; the tensor-core path stores tc_kp floats per pair in the same buffer
     const size_t y64 = (size_t)std::max<int64_t>(P.m2l_pairs, 1) * 2 * NC;
-    const size_t ytc = ((size_t)std::max<int64_t>(P.m2l_pairs, 1) * 2 * tc_kp(P.opt.p) * sizeof(float) + sizeof(double2) - 1) / sizeof(double2);
+    const size_t ytc = ((size_t)std::max<int64_t>(P.m2l_pairs, 1) * tc_kp(P.opt.p) * sizeof(float) + sizeof(double2) - 1) / sizeof(double2);
     CK(ctx->Y.alloc(ctx->opts.precision == 1 ? std::max(y64, ytc) : y64));
     launch_s_tables(P.opt.p, ngroups, ctx->grp_vec.p, ctx->Sg.p, s);
     ctx->launches += 1;
@@ -473,9 +475,14 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     CK(up(ctx, ctx->tc_alpha, al));
     CK(up(ctx, ctx->node_dL, dl));
     CK(ctx->tc_T.alloc((size_t)std::max(ntab, 1) * tc_table_bytes(p) / 2));
-    CK(ctx->tc_Mt.alloc((size_t)(2 * nb + 1) * 2 * kp));
+    CK(ctx->tc_Mt.alloc((size_t)(nb + 1) * 2 * kp));
     CK(cudaMemsetAsync(ctx->tc_Mt.p, 0, sizeof(uint16_t) * ctx->tc_Mt.n, s));
-    CK(ctx->tc_escale.alloc((size_t)2 * nb));
+    ctx->tc_map.assign(tc_rows_map_bytes(), 0);
+    if (tc_make_rows_map(ctx->tc_map.data(), ctx->tc_Mt.p, 2 * (nb + 1), p) != 0) {
+      ctx->err = "mixed precision: could not encode the TMA tensor map of the multipole rows";
+      return BEM_ERR_DEVICE;
+    }
+    CK(ctx->tc_escale.alloc((size_t)nb + 1));
     CK(ctx->tc_err.alloc(1));
     CK(cudaMemsetAsync(ctx->tc_err.p, 0, sizeof(int), s));
     CK(ctx->tc_max.alloc(1));

@@ -54,12 +54,13 @@ struct MatvecArgs {
   const int* tc_item_cnt = nullptr;
   const int* tc_pair = nullptr;
   const void* tc_tab = nullptr;  // FP16 hi/lo table images
-  void* tc_Mt = nullptr;         // FP16 hi/lo multipole rows [2*n_nodes+1][2][KP]
-  float* tc_escale = nullptr;    // [2*n_nodes] power-of-two column scales
-  float* tc_Y = nullptr;         // per-pair partial locals [pairs][2][KP]
+  void* tc_Mt = nullptr;         // FP16 hi/lo rows of M[0] - M[1] [n_nodes+1][2][KP]
+  float* tc_escale = nullptr;    // [n_nodes] power-of-two column scales
+  float* tc_Y = nullptr;         // per-pair partial locals [pairs][KP]
   int* tc_err = nullptr;         // set when a bounded wait gave up
   const double* node_dL = nullptr;
   const double* tc_alpha = nullptr;  // [KP] sqrt((n+m)!(n-m)!) per real coefficient
+  const void* tc_rows_map = nullptr; // host copy of the TMA tensor map over tc_Mt
   // targets
   int n_blocks = 0, chunk = 0, max_ntgt = 0;
   const NearBlockDev* blocks = nullptr;
@@ -106,7 +107,9 @@ int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages = STAG
 
 // tensor-core M2L (m2l_tc.cu)
 int tc_supported(int p);            // 1 if (p+1)^2 <= 128
-int tc_kp(int p);                   // real coefficients per row, padded to 16
+int tc_kp(int p);                   // real coefficients per row, padded to 64
+size_t tc_rows_map_bytes();         // size of the TMA tensor map over the multipole rows
+int tc_make_rows_map(void* map_out, void* Mt, int nrows, int p);
 size_t tc_table_bytes(int p);       // bytes of one table (hi + lo images)
 int tc_max_pairs();                 // pairs per work item
 void tc_alpha_host(int p, double* alpha /*[tc_kp(p)]*/);

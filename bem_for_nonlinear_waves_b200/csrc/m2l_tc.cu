@@ -24,16 +24,22 @@
 // accumulated in FP32, so each translated coefficient carries an error of about 2^-22 of
 // the largest term of its column.
 //
-// GEMM shape per work item: D[128 rows (output coefficients) x N (2 x pairs: both
-// densities)] = T~[128 x KP] * B[N x KP]^T, A = the table (one per item), B = gathered
-// multipole rows; K-major, no swizzle, operands staged in shared memory by cp.async,
-// D in tensor memory, one thread issues the MMAs and commits to an mbarrier.
+// Densities.  A mat-vec row needs only GPhin - GnPhi, and the far field of both comes from
+// the same L2P, so the M2L here translates the combined multipole M[0] - M[1] into L[0] and
+// leaves L[1] = 0: one column per pair instead of two.
+//
+// GEMM shape per work item (<= 256 pairs of one table): D[pairs x 128 coefficients] =
+// B[pairs x KP] * T~[128 x KP]^T, B = gathered multipole rows, T~ = the table; both K-major,
+// staged in shared memory by the TMA unit, D in tensor memory, one thread issues the MMAs
+// and commits to mbarriers.
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 
 #include "fmm_math.cuh"
 #include "kernels.cuh"
@@ -42,21 +48,25 @@
 namespace bemb200 {
 namespace {
 
-constexpr int kRows = 128;          // MMA M: output coefficients (NR <= 128, p <= 10)
-constexpr int kMaxPairs = 128;      // pairs per work item
-constexpr int kMaxCols = 2 * kMaxPairs;  // MMA N (two densities per pair)
+constexpr int kRows = 128;          // table rows = MMA N: output coefficients (NR <= 128, p <= 10)
+constexpr int kMaxPairs = 256;      // pairs per work item = gathered rows (one per pair)
+constexpr int kMaxCols = kMaxPairs;
 constexpr uint32_t kWaitTries = 1u << 22;
 
 template <int P>
 struct TcDims {
   static constexpr int NR = (P + 1) * (P + 1);
-  static constexpr int KP = (NR + 15) / 16 * 16;  // K padded to the MMA K step (16)
-  static constexpr int KC = KP / 8;               // 16-byte chunks per operand row
+  static constexpr int KP = (NR + 63) / 64 * 64;  // K padded to whole 128-byte swizzle atoms
+  static constexpr int KA = KP / 64;              // K atoms (64 halves) per operand row
   static constexpr int TAB_BYTES = 2 * kRows * KP * 2;    // hi + lo images of one table
-  static constexpr int B_BYTES = 2 * kMaxCols * KP * 2;   // hi + lo gathered rows
-  // at least half the SM's shared memory, so one CTA (and one TMEM allocation) per SM
-  static constexpr int SMEM = (TAB_BYTES + B_BYTES) > 116 * 1024 ? (TAB_BYTES + B_BYTES) : 116 * 1024;
+  static constexpr int REGION = kMaxCols * 128;           // one (part, atom) region of gathered rows
+  static constexpr int B_BYTES = 2 * KA * REGION;         // hi + lo gathered rows
+  // plus 1 KB to align the gathered rows to the 1024-byte swizzle atom; at least half the
+  // SM's shared memory, so one CTA (and one TMEM allocation) per SM
+  static constexpr int NEED = TAB_BYTES + B_BYTES + 1024;
+  static constexpr int SMEM = NEED > 116 * 1024 ? NEED : 116 * 1024;
   static_assert(NR <= kRows, "tensor-core M2L needs (p+1)^2 <= 128");
+  static_assert(TAB_BYTES % 1024 == 0, "gathered rows must start on a swizzle atom");
 };
 
 // real index i -> (n, m, part) with part 0 = Re, 1 = Im
@@ -69,10 +79,6 @@ __device__ __forceinline__ void decode_real(int i, int& n, int& m, int& part) {
   part = (o > 0 && (o & 1) == 0) ? 1 : 0;
 }
 
-__device__ __forceinline__ void cp_async16(void* s, const void* g) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(s)), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
 // Set-up: one normalised table per translation, as hi/lo FP16 images in the shared-memory
@@ -133,8 +139,8 @@ __global__ void __launch_bounds__(128) k_tc_tables(int ntab, const double* __res
 }
 
 // ---------------------------------------------------------------------------
-// Per mat-vec: FP64 multipoles -> normalised, power-of-two scaled FP16 hi/lo rows.
-// One warp per (bucket, density); row layout [hi KP][lo KP] halves.
+// Per mat-vec: FP64 multipoles -> combined M[0] - M[1], normalised, power-of-two scaled FP16
+// hi/lo rows.  One warp per bucket; row layout [hi KP][lo KP] halves.
 template <int P>
 __global__ void k_tc_expand(int nnodes, const double2* __restrict__ M, const double* __restrict__ node_dL,
                             const double* __restrict__ alpha, __half* __restrict__ Mt, float* __restrict__ escale) {
@@ -142,10 +148,9 @@ __global__ void k_tc_expand(int nnodes, const double2* __restrict__ M, const dou
   constexpr int NC = ncoef(P), PER = (D::KP + 31) / 32;
   const int lane = threadIdx.x & 31;
   const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  for (int nd = w0; nd < 2 * nnodes; nd += nw) {
-    const int node = nd >> 1;
+  for (int node = w0; node < nnodes; node += nw) {
     const double inv_a = 1.0 / node_dL[node];
-    const double2* Mc = M + (size_t)nd * NC;  // [node][d][NC] with nd = 2 node + d
+    const double2* M0 = M + (size_t)node * 2 * NC;
     double v[PER];
     double mx = 0.0;
 #pragma unroll
@@ -155,10 +160,10 @@ __global__ void k_tc_expand(int nnodes, const double2* __restrict__ M, const dou
       if (k < D::NR) {
         int n1, m1, part;
         decode_real(k, n1, m1, part);
-        const double2 c = Mc[cidx(n1, m1)];
+        const double2 c0 = M0[cidx(n1, m1)], c1 = M0[NC + cidx(n1, m1)];
         double ip = 1.0;
         for (int t = 0; t < n1; ++t) ip *= inv_a;
-        x = (part ? c.y : c.x) * alpha[k] * ip;
+        x = (part ? (c0.y - c1.y) : (c0.x - c1.x)) * alpha[k] * ip;
       }
       v[q] = x;
       mx = fmax(mx, fabs(x));
@@ -166,148 +171,224 @@ __global__ void k_tc_expand(int nnodes, const double2* __restrict__ M, const dou
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     int E = 0;
     if (mx > 0.0 && mx < 1e300) frexp(mx, &E);  // mx = f 2^E, f in [0.5, 1)
-    const double s = ldexp(1.0, -E);
-    __half* row = Mt + (size_t)nd * 2 * D::KP;
+    const double sc = ldexp(1.0, -E);
+    __half* row = Mt + (size_t)node * 2 * D::KP;
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
       const int k = lane + 32 * q;
       if (k < D::KP) {
-        const double x = v[q] * s;
+        const double x = v[q] * sc;
         const __half h = __double2half(x);
         row[k] = h;
         row[D::KP + k] = __double2half(x - (double)__half2float(h));
       }
     }
-    if (lane == 0) escale[nd] = ldexpf(1.f, E);
+    if (lane == 0) escale[node] = ldexpf(1.f, E);
   }
 }
 
 // ---------------------------------------------------------------------------
-// The contraction.  Persistent CTAs of 4 warps walk the work items; per item:
-//   1. pair metadata to shared memory, 2. cp.async the table image and gather the
-//   multipole rows of the item's sources (both densities, zero rows as padding),
-//   3. thread 0 issues 3 x KP/16 MMAs (hi*hi, hi*lo, lo*hi) into one TMEM accumulator
-//   and commits to an mbarrier, 4. each warp reads its 32 TMEM lanes (= 32 output
-//   coefficients) and writes the partial locals of every pair to its slot, scaled back.
-// Every wait is bounded; a timeout sets *err, skips the remaining items and frees TMEM.
+// The contraction: persistent, warp-specialised CTAs, each over a contiguous range of work
+// items (consecutive items mostly share a table, which then stays in shared memory).
+//   warps 0-3  epilogue: TMEM lane = gathered row (= pair); read the translated coefficients
+//              of the row, undo the column scale, store the row to the pair's slot
+//   warps 4-7  producers: item metadata (loaded before the waits, so its latency overlaps
+//              them); TMA: one bulk copy of the table image when the table changes, and
+//              tile::gather4 loads of the multipole rows of the item's sources into 128-byte
+//              swizzled K-major tiles; producer thread 0 also issues the MMAs
+// MMA per item and row block u (128 gathered rows): D[rows x 128 coefficients] = A * T~^T with
+// A = gathered rows (SW128 K-major), T~ the table (no swizzle, K-major), three passes
+// hi*hi + hi*lo + lo*hi.  Shared memory holds one item, TMEM two (buffer b = item parity,
+// 2 row blocks x 128 columns each), so the epilogue of an item overlaps the loads and MMAs
+// of the next.  Barriers:
+//   full         all TMA bytes of the item landed                 -> MMA issuer
+//   smem_free    MMAs of the item finished reading shared memory  -> producers
+//   acc_full[b]  accumulator buffer b written                      -> epilogue
+//   acc_empty[b] epilogue drained buffer b                         -> producers / MMA issuer
+//   meta[b]      metadata of buffer b published                    -> epilogue
+// Every wait is bounded; a timeout records *err and ends the waiting role's loop, and the
+// roles waiting on it then time out as well rather than wait forever.
+constexpr int kProducers = 128;
+constexpr int kColsPerProducer = kMaxCols / kProducers;
+
 template <int P>
-__global__ void __launch_bounds__(128, 1)
-    k_m2l_tc(int nitems, const int* __restrict__ item_tab, const int* __restrict__ item_begin, const int* __restrict__ item_cnt,
-             const int* __restrict__ tc_pair, const int* __restrict__ m2l_src, const __half* __restrict__ Ttab,
-             const __half* __restrict__ Mt, const float* __restrict__ escale, int zero_row, float* __restrict__ Y, int* __restrict__ err) {
+__global__ void __launch_bounds__(256, 1)
+    k_m2l_tc(const __grid_constant__ CUtensorMap rows_map, int nitems, const int* __restrict__ item_tab, const int* __restrict__ item_begin,
+             const int* __restrict__ item_cnt, const int* __restrict__ tc_pair, const int* __restrict__ m2l_src,
+             const __half* __restrict__ Ttab, const float* __restrict__ escale, float* __restrict__ Y, int* __restrict__ err) {
   using D = TcDims<P>;
-  extern __shared__ __align__(128) unsigned char sm_tc[];
-  unsigned char* sT = sm_tc;                 // [hi | lo] table images
-  unsigned char* sB = sm_tc + D::TAB_BYTES;  // [hi | lo] gathered rows, kMaxCols each
+  extern __shared__ __align__(128) unsigned char sm_raw[];
+  unsigned char* sm_tc = sm_raw + ((1024u - (smem_u32(sm_raw) & 1023u)) & 1023u);
+  unsigned char* sT = sm_tc;                 // [hi | lo] table images, kRows rows each
+  unsigned char* sB = sm_tc + D::TAB_BYTES;  // regions (part, atom): kMaxCols rows x 128 B
   __shared__ int s_row[kMaxCols];
-  __shared__ float s_sc[kMaxCols];
-  __shared__ int s_slot[kMaxPairs];
-  __shared__ uint64_t bar;
+  __shared__ float s_sc[2][kMaxCols];
+  __shared__ int s_slot[2][kMaxCols];
+  __shared__ int s_ncol[2];
+  __shared__ uint64_t bar_full, bar_free, bar_accf[2], bar_acce[2], bar_meta[2];
   __shared__ uint32_t tslot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (warp == 0) tmem_alloc(&tslot, 256);
-  if (tid == 0) mbar_init(&bar, 1);
+  const int i0 = (int)((int64_t)nitems * blockIdx.x / gridDim.x);
+  const int i1 = (int)((int64_t)nitems * (blockIdx.x + 1) / gridDim.x);
+  if (warp == 0) tmem_alloc(&tslot, 512);
+  if (tid == 0) {
+    mbar_init(&bar_full, 1);
+    mbar_init(&bar_free, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&bar_accf[b], 1);
+      mbar_init(&bar_acce[b], 128);
+      mbar_init(&bar_meta[b], 1);
+    }
+  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = tslot;
-  uint32_t phase = 0;
-  bool failed = false;
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-    const int tab = item_tab[item], b0 = item_begin[item], cnt = item_cnt[item];
-    const int ncol = 2 * cnt, npad = (ncol + 15) & ~15;
-    for (int c = tid; c < npad; c += blockDim.x) {
-      if (c < ncol) {
-        const int j = c >> 1, d = c & 1;
-        const int slot = tc_pair[b0 + j];
-        const int src = m2l_src[slot];
-        s_row[c] = 2 * src + d;
-        s_sc[c] = escale[2 * src + d];
-        if (d == 0) s_slot[j] = slot;
-      } else {
-        s_row[c] = zero_row;
-        s_sc[c] = 0.f;
-      }
-    }
-    __syncthreads();
-    {
-      const unsigned char* gT = reinterpret_cast<const unsigned char*>(Ttab) + (size_t)tab * D::TAB_BYTES;
-      for (int q = tid; q < D::TAB_BYTES / 16; q += blockDim.x) cp_async16(sT + 16 * q, gT + 16 * q);
-      const int per_part = npad * D::KC;
-      for (int q = tid; q < 2 * per_part; q += blockDim.x) {
-        const int part = q >= per_part ? 1 : 0;
-        const int qq = q - part * per_part;
-        const int rg = qq / (8 * D::KC), kc = (qq >> 3) % D::KC, r8 = qq & 7;
-        const int c = rg * 8 + r8;
-        const __half* src = Mt + ((size_t)s_row[c] * 2 + part) * D::KP + kc * 8;
-        cp_async16(sB + part * (kMaxCols * D::KP * 2) + kmajor_offset(c, kc * 8, D::KP), src);
-      }
-      cp_async_wait_all();
-      fence_proxy_async_smem();
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (tid == 0) {
-      const uint32_t idesc = make_idesc_f16_f32(kRows, npad);
-      const uint32_t aH = smem_u32(sT), aL = aH + kRows * D::KP * 2;
-      const uint32_t bH = smem_u32(sB), bL = bH + kMaxCols * D::KP * 2;
-      constexpr uint32_t SBO = D::KP * 16;
-#pragma unroll 1
-      for (int k = 0; k < D::KP / 16; ++k)
-        tc_mma_f16(tbase, make_smem_desc(aH + 256 * k, 128, SBO), make_smem_desc(bH + 256 * k, 128, SBO), idesc, k > 0 ? 1u : 0u);
-#pragma unroll 1
-      for (int k = 0; k < D::KP / 16; ++k)
-        tc_mma_f16(tbase, make_smem_desc(aH + 256 * k, 128, SBO), make_smem_desc(bL + 256 * k, 128, SBO), idesc, 1u);
-#pragma unroll 1
-      for (int k = 0; k < D::KP / 16; ++k)
-        tc_mma_f16(tbase, make_smem_desc(aL + 256 * k, 128, SBO), make_smem_desc(bH + 256 * k, 128, SBO), idesc, 1u);
-      tc_commit(&bar);
-    }
-    const bool ok = mbar_wait(&bar, phase, kWaitTries);
-    phase ^= 1u;
-    if (__syncthreads_or(ok ? 0 : 1)) {
-      failed = true;
-      break;
-    }
-    tc_fence_after();
-    const int i = warp * 32 + lane;  // output coefficient of this thread's TMEM lane
-    for (int c0 = 0; c0 < npad; c0 += 8) {
-      float v[8];
-      tmem_ld8(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-      if (i < D::KP) {
+  if (warp >= 4) {
+    const int pt = tid - 128;  // producer thread
+    int last_tab = -1, issued = 0;
+    bool ok = true;
+    for (int it = i0; it < i1; ++it) {
+      const int li = it - i0, b = li & 1;
+      // metadata into registers first: independent of shared memory, overlaps the waits
+      const int tab = item_tab[it], b0 = item_begin[it], ncol = item_cnt[it];
+      int r_slot[kColsPerProducer], r_src[kColsPerProducer];
+      float r_sc[kColsPerProducer];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int c = c0 + q;
-          if (c < ncol) Y[((size_t)s_slot[c >> 1] * 2 + (c & 1)) * D::KP + i] = v[q] * s_sc[c];
+      for (int e = 0; e < kColsPerProducer; ++e) {
+        const int c = pt + e * kProducers;
+        r_slot[e] = c < ncol ? tc_pair[b0 + c] : 0;
+      }
+#pragma unroll
+      for (int e = 0; e < kColsPerProducer; ++e) r_src[e] = (pt + e * kProducers) < ncol ? m2l_src[r_slot[e]] : 0;
+#pragma unroll
+      for (int e = 0; e < kColsPerProducer; ++e) r_sc[e] = (pt + e * kProducers) < ncol ? escale[r_src[e]] : 0.f;
+      if (ok && li > 0) ok = mbar_wait(&bar_free, (li - 1) & 1, kWaitTries);
+      if (ok && li > 1) ok = mbar_wait(&bar_acce[b], ((li >> 1) - 1) & 1, kWaitTries);
+      if (named_bar_or(1, kProducers, ok ? 0 : 1)) {
+        ok = false;
+        break;
+      }
+#pragma unroll
+      for (int e = 0; e < kColsPerProducer; ++e) {
+        const int c = pt + e * kProducers;
+        if (c < ncol) {
+          s_row[c] = r_src[e];
+          s_sc[b][c] = r_sc[e];
+          s_slot[b][c] = r_slot[e];
+        }
+      }
+      const int nquad = (ncol + 3) >> 2;
+      const bool load_tab = tab != last_tab;
+      last_tab = tab;
+      if (pt == 0) {
+        s_ncol[b] = ncol;
+        const uint32_t bytes = (load_tab ? (uint32_t)D::TAB_BYTES : 0u) + (uint32_t)nquad * 4u * 128u * 2u * D::KA;
+        mbar_arrive_expect_tx(&bar_full, bytes);
+      }
+      named_bar_sync(1, kProducers);
+      if (pt == 0) {
+        mbar_arrive(&bar_meta[b]);
+        if (load_tab) bulk_copy_g2s(sT, reinterpret_cast<const unsigned char*>(Ttab) + (size_t)tab * D::TAB_BYTES, D::TAB_BYTES, &bar_full);
+      }
+      // gather4: quad q of rows, part (hi/lo), atom a -> region (part, a), rows 4q..4q+3
+      for (int g = pt; g < nquad * 2 * D::KA; g += kProducers) {
+        const int q = g / (2 * D::KA), pa = g - q * (2 * D::KA);
+        const int part = pa / D::KA, a = pa - part * D::KA;
+        int y[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int c = min(4 * q + i, ncol - 1);
+          y[i] = s_row[c] * 2 + part;
+        }
+        tma_gather4(sB + (part * D::KA + a) * D::REGION + q * 4 * 128, &rows_map, a * 64, y[0], y[1], y[2], y[3], &bar_full);
+      }
+      if (pt == 0) {
+        if (mbar_wait(&bar_full, li & 1, kWaitTries)) {
+          tc_fence_after();
+          constexpr uint32_t idesc = make_idesc_f16_f32(128, kRows);
+          constexpr uint32_t SBO_T = D::KP * 16;
+          const uint32_t aBase = smem_u32(sB);
+          const uint32_t bH = smem_u32(sT), bL = bH + kRows * D::KP * 2;
+          for (int u = 0; u * 128 < ncol; ++u) {
+            const uint32_t dt = tbase + (uint32_t)(b * 256 + u * 128);
+            const uint32_t ro = (uint32_t)(u * 128 * 128);  // row block offset inside a region
+#pragma unroll 1
+            for (int pass = 0; pass < 3; ++pass) {
+              const int apart = pass == 2 ? 1 : 0;      // A: hi, hi, lo
+              const uint32_t bT = pass == 1 ? bL : bH;  // T: hi, lo, hi
+#pragma unroll 1
+              for (int k = 0; k < D::KP / 16; ++k) {
+                const uint32_t aaddr = aBase + (uint32_t)((apart * D::KA + (k >> 2)) * D::REGION) + ro + (uint32_t)((k & 3) * 32);
+                tc_mma_f16(dt, make_smem_desc_sw128(aaddr, 1024), make_smem_desc(bT + 256 * k, 128, SBO_T), idesc,
+                           (pass > 0 || k > 0) ? 1u : 0u);
+              }
+            }
+          }
+          tc_commit(&bar_free);
+          tc_commit(&bar_accf[b]);
+          ++issued;
+        } else {
+          ok = false;  // the other producers learn of it at the next vote
         }
       }
     }
-    tc_fence_before();
-    __syncthreads();
+    if (!ok) atomicExch(err, 1);
+    // on an early exit, let copies and MMAs already issued finish before the CTA leaves
+    if (pt == 0 && !ok && issued > 0) mbar_wait(&bar_free, (issued - 1) & 1, kWaitTries);
+  } else {
+    for (int it = i0; it < i1; ++it) {
+      const int li = it - i0, b = li & 1;
+      bool ok = mbar_wait(&bar_meta[b], (li >> 1) & 1, kWaitTries);
+      if (ok) ok = mbar_wait(&bar_accf[b], (li >> 1) & 1, kWaitTries);
+      if (!__all_sync(0xffffffffu, ok ? 1 : 0)) {
+        if (lane == 0) atomicExch(err, 1);
+        break;
+      }
+      tc_fence_after();
+      const int ncol = s_ncol[b];
+      for (int u = 0; u * 128 < ncol; ++u) {
+        const int c = u * 128 + warp * 32 + lane;
+        const bool valid = c < ncol;
+        const int slot = valid ? s_slot[b][c] : 0;
+        const float sc = valid ? s_sc[b][c] : 0.f;
+        float* yrow = Y + (size_t)slot * D::KP;
+#pragma unroll 1
+        for (int q = 0; q * 32 < D::KP; ++q) {
+          float v[32];
+          tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * 256 + u * 128 + q * 32), v);
+          if (valid) {
+#pragma unroll
+            for (int e = 0; e < 32; e += 4)
+              *reinterpret_cast<float4*>(yrow + q * 32 + e) = make_float4(v[e] * sc, v[e + 1] * sc, v[e + 2] * sc, v[e + 3] * sc);
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&bar_acce[b]);
+    }
   }
-  if (failed && tid == 0) atomicExch(err, 1);
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    tmem_dealloc(tbase, 256);
+    tmem_dealloc(tbase, 512);
   }
 }
 
-// Per target bucket: L = sum of its slots (target-major CSR order, deterministic), back to
-// the FP64 complex layout [node][density][NC] with the normalisation and a_t^{n+1} undone.
+// Per target bucket: L[0] = sum of its slots (target-major CSR order, deterministic), back to
+// the FP64 complex layout [node][density][NC] with the normalisation and a_t^{n+1} undone;
+// L[1] stays zero (the combined density carries both).
 template <int P>
 __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, const int* __restrict__ m2l_off,
                                 const double* __restrict__ node_dL, const double* __restrict__ alpha, const float* __restrict__ Y,
                                 double2* __restrict__ L) {
   using D = TcDims<P>;
   constexpr int NC = ncoef(P);
-  const int64_t total = (int64_t)ntargets * 2 * NC;
+  const int64_t total = (int64_t)ntargets * NC;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int ti = (int)(e / (2 * NC));
-    const int r = (int)(e - (int64_t)ti * 2 * NC);
-    const int d = r / NC, o = r - d * NC;
+    const int ti = (int)(e / NC);
+    const int o = (int)(e - (int64_t)ti * NC);
     int n = 0;
     while ((n + 1) * (n + 2) / 2 <= o) ++n;
     const int m = o - n * (n + 1) / 2;
@@ -315,7 +396,7 @@ __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, c
     const int tgt = targets[ti];
     double sr = 0.0, si = 0.0;
     for (int k = m2l_off[tgt]; k < m2l_off[tgt + 1]; ++k) {
-      const float* y = Y + ((size_t)k * 2 + d) * D::KP;
+      const float* y = Y + (size_t)k * D::KP;
       sr += (double)y[ire];
       if (m > 0) si += (double)y[ire + 1];
     }
@@ -323,7 +404,7 @@ __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, c
     double ap = a;
     for (int t = 0; t < n; ++t) ap *= a;
     const double f = alpha[ire] / ap;
-    L[((size_t)tgt * 2 + d) * NC + o] = make_double2(sr * f, si * f);
+    L[(size_t)tgt * 2 * NC + o] = make_double2(sr * f, si * f);
   }
 }
 
@@ -331,14 +412,15 @@ template <int P>
 int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st) {
   using D = TcDims<P>;
   if (a.n_tc_items <= 0) return 0;
-  const int nd = 2 * a.n_nodes;
-  const int ge = (int)std::min<int64_t>(((int64_t)nd * 32 + 255) / 256, 148 * 8);
+  const int ge = (int)std::min<int64_t>(((int64_t)a.n_nodes * 32 + 255) / 256, 148 * 8);
   __half* Mt = static_cast<__half*>(a.tc_Mt);
   k_tc_expand<P><<<ge, 256, 0, st>>>(a.n_nodes, a.M, a.node_dL, a.tc_alpha, Mt, a.tc_escale);
   const int grid = a.n_tc_items < a.tc_grid ? a.n_tc_items : a.tc_grid;
-  k_m2l_tc<P><<<grid, 128, D::SMEM, st>>>(a.n_tc_items, a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt, a.tc_pair, a.m2l_src,
-                                           static_cast<const __half*>(a.tc_tab), Mt, a.tc_escale, nd, a.tc_Y, a.tc_err);
-  const int64_t tr = (int64_t)a.n_m2l_targets * 2 * ncoef(P);
+  CUtensorMap map;
+  std::memcpy(&map, a.tc_rows_map, sizeof(map));
+  k_m2l_tc<P><<<grid, 256, D::SMEM, st>>>(map, a.n_tc_items, a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt, a.tc_pair, a.m2l_src,
+                                           static_cast<const __half*>(a.tc_tab), a.tc_escale, a.tc_Y, a.tc_err);
+  const int64_t tr = (int64_t)a.n_m2l_targets * ncoef(P);
   const int gr = (int)std::min<int64_t>((tr + 255) / 256, 148 * 16);
   k_m2l_tc_reduce<P><<<gr, 256, 0, st>>>(a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.node_dL, a.tc_alpha, a.tc_Y, a.L);
   return 3;
@@ -353,7 +435,34 @@ void tc_tables_launch(int ntab, const double* tab, const double* alpha, __half* 
 }  // namespace
 
 int tc_supported(int p) { return p >= 1 && (p + 1) * (p + 1) <= kRows; }
-int tc_kp(int p) { return ((p + 1) * (p + 1) + 15) / 16 * 16; }
+int tc_kp(int p) { return ((p + 1) * (p + 1) + 63) / 64 * 64; }
+
+size_t tc_rows_map_bytes() { return sizeof(CUtensorMap); }
+
+// Tensor map over the multipole rows Mt viewed as [rows = 2 (n_nodes + 1)][tc_kp halves]:
+// boxes of 64 halves x 1 row, 128-byte swizzle, for tile::gather4.
+int tc_make_rows_map(void* map_out, void* Mt, int nrows, int p) {
+  using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                                const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeFn encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+      return -1;
+    encode = reinterpret_cast<EncodeFn>(fn);
+  }
+  const int kp = tc_kp(p);
+  const cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)nrows};
+  const cuuint64_t strides[1] = {(cuuint64_t)kp * 2};
+  const cuuint32_t box[2] = {64, 1};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode(static_cast<CUtensorMap*>(map_out), CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, Mt, dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : -1;
+}
 size_t tc_table_bytes(int p) { return (size_t)2 * kRows * tc_kp(p) * 2; }
 int tc_max_pairs() { return kMaxPairs; }
 
