@@ -186,10 +186,11 @@ class BEM_BVP:
     def profile_matvec(self, repeats=10, mixed=False):
         """Per-stage mat-vec time in ms (CUDA events on the solver stream); mixed=True profiles
         the tensor-core operator of a precision="mixed" context."""
-        st = np.zeros(6)
+        st = np.zeros(9)
         fn = self.lib.bem_gpu_profile_matvec_mixed if mixed else self.lib.bem_gpu_profile_matvec
         self._check(fn(self.ctx, int(repeats), L.ptr(st, L.P_dbl)), "profile")
-        return dict(zip(["p2m", "m2m", "m2l", "l2l", "targets", "total"], map(float, st)))
+        keys = ["p2m", "m2m", "m2l", "l2l", "targets", "total"] + (["m2l_expand", "m2l_contract", "m2l_reduce"] if mixed else [])
+        return dict(zip(keys, map(float, st)))
 
     def matvec_device(self, d_x, d_y, mixed=False):
         """y = A x on device buffers given as integer pointers (n_dof doubles each), on the

@@ -1087,6 +1087,18 @@ int profile_matvec(bem_gpu_ctx* ctx, int repeats, bool tc, double* stage_ms) {
     CK(cudaEventElapsedTime(&ms, e0, e1));
     stage_ms[k] = ms / repeats;
   }
+  if (tc) {  // the three kernels of the tensor-core M2L on their own
+    const int parts[3] = {TC_EXPAND, TC_CONTRACT, TC_REDUCE};
+    for (int k = 0; k < 3; ++k) {
+      CK(cudaEventRecord(e0, s));
+      for (int r = 0; r < repeats; ++r) launch_m2l_tc(ctx->plan.opt.p, a, s, parts[k]);
+      CK(cudaEventRecord(e1, s));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      stage_ms[6 + k] = ms / repeats;
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return BEM_OK;

@@ -114,7 +114,8 @@ size_t tc_table_bytes(int p);       // bytes of one table (hi + lo images)
 int tc_max_pairs();                 // pairs per work item
 void tc_alpha_host(int p, double* alpha /*[tc_kp(p)]*/);
 void launch_tc_tables(int p, int ntab, const double* tab, const double* alpha, void* T, unsigned int* maxbits, cudaStream_t st);
-int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st);
+constexpr int TC_EXPAND = 1, TC_CONTRACT = 2, TC_REDUCE = 4, TC_ALL = 7;
+int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st, int parts = TC_ALL);
 void launch_densities(int n, int mode, const double* x, const double* known, const int* kind, double* phi, double* phin, cudaStream_t st);
 void launch_near_weights(const NearArgs& a, cudaStream_t st);
 void launch_diag(int n, const int* dof_point, const double* GnPhi, double* diag, cudaStream_t st);

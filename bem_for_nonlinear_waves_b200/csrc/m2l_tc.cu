@@ -409,21 +409,31 @@ __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, c
 }
 
 template <int P>
-int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st) {
+int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts) {
   using D = TcDims<P>;
   if (a.n_tc_items <= 0) return 0;
-  const int ge = (int)std::min<int64_t>(((int64_t)a.n_nodes * 32 + 255) / 256, 148 * 8);
+  int launches = 0;
   __half* Mt = static_cast<__half*>(a.tc_Mt);
-  k_tc_expand<P><<<ge, 256, 0, st>>>(a.n_nodes, a.M, a.node_dL, a.tc_alpha, Mt, a.tc_escale);
-  const int grid = a.n_tc_items < a.tc_grid ? a.n_tc_items : a.tc_grid;
-  CUtensorMap map;
-  std::memcpy(&map, a.tc_rows_map, sizeof(map));
-  k_m2l_tc<P><<<grid, 256, D::SMEM, st>>>(map, a.n_tc_items, a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt, a.tc_pair, a.m2l_src,
-                                           static_cast<const __half*>(a.tc_tab), a.tc_escale, a.tc_Y, a.tc_err);
-  const int64_t tr = (int64_t)a.n_m2l_targets * ncoef(P);
-  const int gr = (int)std::min<int64_t>((tr + 255) / 256, 148 * 16);
-  k_m2l_tc_reduce<P><<<gr, 256, 0, st>>>(a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.node_dL, a.tc_alpha, a.tc_Y, a.L);
-  return 3;
+  if (parts & TC_EXPAND) {
+    const int ge = (int)std::min<int64_t>(((int64_t)a.n_nodes * 32 + 255) / 256, 148 * 8);
+    k_tc_expand<P><<<ge, 256, 0, st>>>(a.n_nodes, a.M, a.node_dL, a.tc_alpha, Mt, a.tc_escale);
+    ++launches;
+  }
+  if (parts & TC_CONTRACT) {
+    const int grid = a.n_tc_items < a.tc_grid ? a.n_tc_items : a.tc_grid;
+    CUtensorMap map;
+    std::memcpy(&map, a.tc_rows_map, sizeof(map));
+    k_m2l_tc<P><<<grid, 256, D::SMEM, st>>>(map, a.n_tc_items, a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt, a.tc_pair, a.m2l_src,
+                                             static_cast<const __half*>(a.tc_tab), a.tc_escale, a.tc_Y, a.tc_err);
+    ++launches;
+  }
+  if (parts & TC_REDUCE) {
+    const int64_t tr = (int64_t)a.n_m2l_targets * ncoef(P);
+    const int gr = (int)std::min<int64_t>((tr + 255) / 256, 148 * 16);
+    k_m2l_tc_reduce<P><<<gr, 256, 0, st>>>(a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.node_dL, a.tc_alpha, a.tc_Y, a.L);
+    ++launches;
+  }
+  return launches;
 }
 
 template <int P>
@@ -495,11 +505,11 @@ void launch_tc_tables(int p, int ntab, const double* tab, const double* alpha, v
   }
 }
 
-int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st) {
+int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st, int parts) {
   switch (p) {
 #define BEMB200_CASE(PP) \
   case PP:               \
-    return m2l_tc_launch<PP>(a, st);
+    return m2l_tc_launch<PP>(a, st, parts);
     BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5)
     BEMB200_CASE(6) BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10)
 #undef BEMB200_CASE

@@ -5,6 +5,9 @@ Metric: BVP solves/s (one step = one complete BVP solve: set-up of geometry, oct
 interaction lists, near-field quadrature and rigid-mode diagonal, then GMRES to a relative
 residual of 1e-8) on the 60k-node synthetic tank (2.0 x 1.0 x 0.5 m, h = 2/185 m,
 free-surface z-noise sigma = 0.2 h, p = 10, theta = 0.25, <= 30 elements per leaf).
+Default precision "mixed": GMRES corrections with the tensor-core M2L, FP64 refinement on
+the true residual; after the timed steps the FP64 GPU path solves the same tank once and
+the line reports the mixed result's error against it (fp64_gpu).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -33,6 +36,8 @@ import numpy as np  # noqa: E402
 CONFIGS = {
     "tank_60k": dict(tank=dict(length=2.0, width=1.0, depth=0.5, h=2.0 / 185, noise=0.2, seed=1), p=10, rel_tol=1e-8),
     "tank_2800": dict(tank=dict(length=2.0, width=1.0, depth=0.5, h=0.05, noise=0.0, seed=1), p=8, rel_tol=1e-10),
+    # a quarter of tank_60k (same tank, h doubled): small enough for full ncu captures
+    "tank_15k": dict(tank=dict(length=2.0, width=1.0, depth=0.5, h=2.0 / 92, noise=0.2, seed=1), p=10, rel_tol=1e-8),
 }
 # GMRES iterations of the unpreconditioned reference algorithm on each workload (the same
 # Krylov iteration on the same operator), measured by the CUDA path; used to turn the
@@ -189,6 +194,16 @@ def load_traffic(kernel, workload):
     return None
 
 
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        try:
+            return json.load(open(path)), "measured"
+        except ValueError:
+            pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -196,10 +211,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="tank_60k", choices=list(CONFIGS))
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "none"])
     ap.add_argument("--max-iter", type=int, default=1500)
     ap.add_argument("--ref-iters", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-check", action="store_true")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
@@ -209,18 +226,24 @@ def main():
     from bem_for_nonlinear_waves_b200 import BEM_BVP
     from bem_for_nonlinear_waves_b200 import _lib
     t, d, kv = make_problem(cfg, rank)
-    bvp = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=cfg["p"], solver_tol=cfg["rel_tol"], tol_relative=True,
-                  solver_max_iter=args.max_iter, preconditioner=args.precond, dofs=d, device=local)
+    mixed = args.precision == "mixed"
+
+    def make(prec):
+        return BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=cfg["p"], solver_tol=cfg["rel_tol"], tol_relative=True,
+                       solver_max_iter=args.max_iter, preconditioner=args.precond, dofs=d, device=local, precision=prec)
+
+    bvp = make(args.precision)
     for _ in range(args.warmup):
         bvp.setup()
         bvp.solve(kv)
-    prof = bvp.profile_matvec(repeats=5)
+    prof = bvp.profile_matvec(repeats=5, mixed=mixed)
+    prof64 = bvp.profile_matvec(repeats=5) if mixed else prof
     tree = bvp.tree_stats()
     fp64_peak = _lib.load().bem_gpu_fp64_peak_tflops(local)
 
     barrier(world)
     dev_s = e2e_s = plan_s = upload_s = 0.0
-    launches = h2d = d2h = iters = 0
+    launches = h2d = d2h = iters = mv = mv_lo = 0
     converged = True
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
@@ -236,23 +259,58 @@ def main():
             h2d += st.h2d_bytes
             d2h += st.d2h_bytes
             iters += st.iterations
+            mv += st.matvecs
+            mv_lo += st.matvecs_lo
             converged = converged and bool(st.converged)
     barrier(world)
     dev_max, e2e_max = allreduce_max([dev_s, e2e_s], world)
+    ans = bvp.ans.copy()
 
+    # the FP64 GPU path on the same tank: the oracle of the mixed result, and its own speed
+    fp64 = None
+    if mixed and not args.no_fp64_check:
+        b64 = make("fp64")
+        b64.setup()
+        b64.solve(kv)
+        w0 = time.perf_counter()
+        b64.setup()
+        b64.solve(kv)
+        w64 = time.perf_counter() - w0
+        ref = b64.ans
+        fp64 = {"solves_per_s": 1.0 / b64.stats.time_device_s, "e2e_solves_per_s": 1.0 / w64, "gmres_iterations": b64.stats.iterations,
+                "matvec_ms": prof64["total"], "mixed_rel_err_max": float(np.abs(ans - ref).max() / np.abs(ref).max()),
+                "mixed_rel_err_l2": float(np.linalg.norm(ans - ref) / np.linalg.norm(ref))}
+        del b64
+
+    peaks, peaks_kind = load_peaks()
     p = cfg["p"]
     nc = (p + 1) * (p + 2) // 2
-    m2l_flops = tree["m2l_pairs"] * 2 * nc * (p + 1) ** 2 * 8.0  # complex MACs, both densities
-    m2l_s = prof["m2l"] * 1e-3
-    achieved = m2l_flops / m2l_s / 1e12
-    traffic = load_traffic("m2l", args.config)
+    m2l_flops = tree["m2l_pairs"] * 2 * nc * (p + 1) ** 2 * 8.0  # the reference's M2L: complex MACs, both densities
+    if mixed:
+        kp = ((p + 1) ** 2 + 63) // 64 * 64
+        t_k = prof["m2l_contract"] * 1e-3
+        achieved = m2l_flops / t_k / 1e12
+        roof = {"kernel": "k_m2l_tc", "bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                "frac": achieved / peaks["bf16_tflops"], "traffic": load_traffic("k_m2l_tc", args.config),
+                "peak_source": f"{peaks_kind} bf16 dense burst (MEASURED_PEAKS.json bf16_tflops); kernel timed alone",
+                "algorithmic_flops_per_launch": m2l_flops,
+                "tensor_flops_issued_per_launch": tree["m2l_pairs"] * 128.0 * kp * 2 * 3,
+                "kernel_ms": prof["m2l_contract"]}
+    else:
+        t_k = prof["m2l"] * 1e-3
+        achieved = m2l_flops / t_k / 1e12
+        roof = {"kernel": "k_m2l_grp", "bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak if fp64_peak > 0 else None, "traffic": load_traffic("k_m2l_grp", args.config),
+                "peak_source": "measured FP64 FMA probe on this GPU (MEASURED_PEAKS.json has no FP64 figure)",
+                "algorithmic_flops_per_launch": m2l_flops, "kernel_ms": prof["m2l"]}
     line = {
         "metric": "bvp_solves_per_s", "value": world * args.steps / dev_max, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64/f16x3-tc" if mixed else "f64", "data": "synthetic",
         "config": {"workload": args.config, "n_points": int(t.n_points), "n_faces": int(t.n_faces), "n_dof": int(bvp.matrix_size),
-                   "p": p, "theta": 0.25, "leaf_max": 30, "rel_tol": cfg["rel_tol"], "preconditioner": args.precond,
-                   "gmres_iterations": iters / args.steps, "converged": converged, "parallelism": f"replicas{world}",
+                   "p": p, "theta": 0.25, "leaf_max": 30, "rel_tol": cfg["rel_tol"], "precision": args.precision,
+                   "preconditioner": args.precond, "gmres_iterations": iters / args.steps, "matvecs_fp64": mv / args.steps,
+                   "matvecs_lowp": mv_lo / args.steps, "converged": converged, "parallelism": f"replicas{world}",
                    "l2": "working set > L2 (near-field weights %.1f GB)" % (tree["nnz"] * 16 / 1e9)},
         "matvecs_per_s": world * 1e3 / prof["total"],
         "host_setup_s_per_step": {"plan": plan_s / args.steps, "upload": upload_s / args.steps},
@@ -260,12 +318,11 @@ def main():
         "e2e": {"value": world * args.steps / e2e_max, "unit": "solves/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "gpu_launches": launches,
-        "roofline": {"kernel": "k_m2l", "bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                     "frac": achieved / fp64_peak if fp64_peak > 0 else None, "traffic": traffic,
-                     "peak_source": "measured FP64 FMA probe on this GPU (MEASURED_PEAKS.json has no FP64 figure)",
-                     "algorithmic_flops_per_launch": m2l_flops},
+        "roofline": roof,
         "clocks": clk.summary(),
     }
+    if fp64 is not None:
+        line["fp64_gpu"] = fp64
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ref_iters = REFERENCE_ITERATIONS.get(args.config) or args.ref_iters
         cb = cpu_sample(cfg, t, d, ref_iters)

@@ -179,11 +179,12 @@ int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[6]
  * reference's M2L is FP64 only (lib/include/moments.hpp:732-764).
  * bem_gpu_matvec_device_mixed: y = A_lo x on device buffers (tensor-core M2L, everything
  *   else FP64), on the context's stream — the correction operator of the mixed solve.
- * bem_gpu_profile_matvec_mixed: stage times of that operator, same layout as above.
+ * bem_gpu_profile_matvec_mixed: stage times of that operator, the layout above followed by
+ *   the three kernels of its M2L alone: [6] expand, [7] tensor-core contraction, [8] reduce.
  * bem_gpu_check_device_status: BEM_ERR_DEVICE if a bounded device-side wait of the
  *   tensor-core M2L gave up since set-up (the results of that launch are invalid). */
 int bem_gpu_matvec_device_mixed(bem_gpu_ctx* ctx, const double* d_x, double* d_y);
-int bem_gpu_profile_matvec_mixed(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[6]*/);
+int bem_gpu_profile_matvec_mixed(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[9]*/);
 int bem_gpu_check_device_status(bem_gpu_ctx* ctx);
 
 /* FP64 FMA throughput of the device (TFLOP/s), measured by a short probe kernel. */
