@@ -21,10 +21,13 @@ using namespace bemb200;
 
 namespace {
 
+// Device buffer that keeps its allocation across set-ups: alloc() only reallocates when the
+// new size exceeds the capacity (a repeated set-up of the same or a smaller problem, e.g. the
+// time steps of one simulation, allocates nothing).
 template <typename T>
 struct DBuf {
   T* p = nullptr;
-  size_t n = 0;
+  size_t n = 0, cap = 0;
   DBuf() = default;
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
@@ -32,18 +35,47 @@ struct DBuf {
   void release() {
     if (p) cudaFree(p);
     p = nullptr;
-    n = 0;
+    n = cap = 0;
   }
   cudaError_t alloc(size_t count) {
+    n = count;
+    if (count <= cap) return cudaSuccess;
     release();
     n = count;
-    if (count == 0) return cudaSuccess;
-    return cudaMalloc((void**)&p, sizeof(T) * count);
+    const cudaError_t e = cudaMalloc((void**)&p, sizeof(T) * count);
+    if (e == cudaSuccess) cap = count;
+    return e;
   }
-  cudaError_t upload(const std::vector<T>& v, cudaStream_t s) {
-    cudaError_t e = alloc(v.size());
-    if (e != cudaSuccess || v.empty()) return e;
-    return cudaMemcpyAsync(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s);
+};
+
+// Pinned host staging area for the set-up uploads: host arrays are copied into it and sent
+// with asynchronous copies, so the upload runs at pinned-memory bandwidth instead of through
+// the driver's pageable bounce buffer.  Grown on demand (after draining the stream).
+struct PinnedStage {
+  unsigned char* p = nullptr;
+  size_t cap = 0, off = 0;
+  ~PinnedStage() {
+    if (p) cudaFreeHost(p);
+  }
+  // space for `bytes`, synchronising `s` when the area must be reused or grown
+  cudaError_t reserve(size_t bytes, cudaStream_t s, unsigned char** out) {
+    if (off + bytes > cap) {
+      cudaError_t e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return e;
+      off = 0;
+      if (bytes > cap) {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        const size_t want = std::max<size_t>(bytes, size_t(64) << 20);
+        e = cudaHostAlloc((void**)&p, want, cudaHostAllocDefault);
+        if (e != cudaSuccess) return e;
+        cap = want;
+      }
+    }
+    *out = p + off;
+    off += (bytes + 255) & ~size_t(255);
+    return cudaSuccess;
   }
 };
 
@@ -100,7 +132,9 @@ struct bem_gpu_ctx {
   float setup_dev_ms = 0.f;
   double time_plan = 0.0, time_upload = 0.0;
 
+  PinnedStage stage;  // set-up uploads
   ~bem_gpu_ctx() {
+    if (stream) cudaStreamSynchronize(stream);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -221,8 +255,14 @@ void run_fmm(bem_gpu_ctx* ctx, double* rows, double* gphin, double* gnphi) {
 
 template <typename T>
 cudaError_t up(bem_gpu_ctx* ctx, DBuf<T>& b, const std::vector<T>& v) {
-  ctx->h2d += (int64_t)(sizeof(T) * v.size());
-  return b.upload(v, ctx->stream);
+  const size_t bytes = sizeof(T) * v.size();
+  ctx->h2d += (int64_t)bytes;
+  cudaError_t e = b.alloc(v.size());
+  if (e != cudaSuccess || v.empty()) return e;
+  unsigned char* h = nullptr;
+  if ((e = ctx->stage.reserve(bytes, ctx->stream, &h)) != cudaSuccess) return e;
+  std::memcpy(h, v.data(), bytes);
+  return cudaMemcpyAsync(b.p, h, bytes, cudaMemcpyHostToDevice, ctx->stream);
 }
 
 // Captures A.x (mv_in -> mv_out) as a graph; tc selects the tensor-core M2L.

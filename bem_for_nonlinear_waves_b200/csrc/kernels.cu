@@ -177,46 +177,93 @@ __device__ __forceinline__ void decode_nm(int t, int& n, int& m) {
 }
 
 // ---------------------------------------------------------------------------
-// M2M: one block per parent, children in turn; thread per output coefficient.
+// warp-level expansion of half-stored coefficients [2][NC] into full [2][(P+1)^2]
 template <int P>
-__global__ void k_m2m(const int* __restrict__ parents, const int* __restrict__ child_begin, const int* __restrict__ child_end,
-                      const int* __restrict__ node_children, const double* __restrict__ node_X, double2* __restrict__ M) {
+__device__ __forceinline__ void expand_full_warp(const double2* __restrict__ src, double2* dst, int lane) {
   constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
-  __shared__ double2 sF[NF];
-  __shared__ double2 sM[2 * NF];
+  for (int t = lane; t < 2 * NF; t += 32) {
+    const int d = t / NF, i = t % NF;
+    int n = 0;
+    while ((n + 1) * (n + 1) <= i) ++n;
+    const int m = i - n * (n + 1);
+    double2 v = src[d * NC + cidx(n, m < 0 ? -m : m)];
+    if (m < 0) v = ((-m) & 1) ? make_double2(-v.x, v.y) : make_double2(v.x, -v.y);
+    dst[t] = v;
+  }
+}
+
+// M2M: one block of 8 warps per parent, warp w translating child w (lane per output
+// coefficient); the children's partial multipoles are summed in child order.  The upward
+// pass is level by level, so the time of one block is the time of a level: splitting the
+// children over warps shortens it eightfold against one thread per coefficient looping over
+// the children.
+constexpr int kTreeWarps = 8;
+// warps of the M2M block: 8 while the per-warp tables fit the 48 KB of static shared memory
+template <int P>
+constexpr int m2m_warps() { return kTreeWarps * 3 * (P + 1) * (P + 1) * 16 <= 48 * 1024 ? kTreeWarps : kTreeWarps / 2; }
+
+template <int P>
+__global__ void __launch_bounds__(32 * m2m_warps<P>()) k_m2m(const int* __restrict__ parents, const int* __restrict__ child_begin,
+                                                       const int* __restrict__ child_end, const int* __restrict__ node_children,
+                                                       const double* __restrict__ node_X, double2* __restrict__ M) {
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), R = (NC + 31) / 32, W = m2m_warps<P>();
+  __shared__ double2 sbuf[W * 3 * NF];  // per warp: F [NF], child multipole [2][NF]
   const int par = parents[blockIdx.x];
-  const int t = threadIdx.x;
-  int n = 0, m = 0;
-  if (t < NC) decode_nm(t, n, m);
-  double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
-  for (int ci = child_begin[par]; ci < child_end[par]; ++ci) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2* sF = sbuf + warp * 3 * NF;
+  double2* sM = sF + NF;
+  double2 acc[R][2];
+#pragma unroll
+  for (int r = 0; r < R; ++r) acc[r][0] = acc[r][1] = make_double2(0.0, 0.0);
+  const int cb = child_begin[par], ce = child_end[par];
+  for (int ci = cb + warp; ci < ce; ci += W) {
     const int c = node_children[ci];
-    __syncthreads();
-    if (t < 32)
-      F_full_column<P>(t, node_X[3 * c] - node_X[3 * par], node_X[3 * c + 1] - node_X[3 * par + 1],
-                       node_X[3 * c + 2] - node_X[3 * par + 2], sF);
-    expand_full<P>(M + (size_t)c * 2 * NC, sM);
-    __syncthreads();
-    if (t < NC) {
-      for (int n1 = 0; n1 <= n; ++n1) {
-        const int n2 = n - n1;
-        const int lo = max(-n1, m - n2), hi = min(n1, m + n2);
-        for (int m1 = lo; m1 <= hi; ++m1) {
-          const double2 f = sF[n1 * (n1 + 1) + m1];
-          const int i2 = n2 * (n2 + 1) + (m - m1);
-          const double2 x0 = sM[i2], x1 = sM[NF + i2];
-          // conj(f) * x
-          a0.x += f.x * x0.x + f.y * x0.y;
-          a0.y += f.x * x0.y - f.y * x0.x;
-          a1.x += f.x * x1.x + f.y * x1.y;
-          a1.y += f.x * x1.y - f.y * x1.x;
+    F_full_column<P>(lane, node_X[3 * c] - node_X[3 * par], node_X[3 * c + 1] - node_X[3 * par + 1],
+                     node_X[3 * c + 2] - node_X[3 * par + 2], sF);
+    expand_full_warp<P>(M + (size_t)c * 2 * NC, sM, lane);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int t = lane + 32 * r;
+      if (t < NC) {
+        int n, m;
+        decode_nm(t, n, m);
+        double2 a0 = acc[r][0], a1 = acc[r][1];
+        for (int n1 = 0; n1 <= n; ++n1) {
+          const int n2 = n - n1;
+          const int lo = max(-n1, m - n2), hi = min(n1, m + n2);
+          for (int m1 = lo; m1 <= hi; ++m1) {
+            const double2 f = sF[n1 * (n1 + 1) + m1];
+            const int i2 = n2 * (n2 + 1) + (m - m1);
+            const double2 x0 = sM[i2], x1 = sM[NF + i2];
+            // conj(f) * x
+            a0.x += f.x * x0.x + f.y * x0.y;
+            a0.y += f.x * x0.y - f.y * x0.x;
+            a1.x += f.x * x1.x + f.y * x1.y;
+            a1.y += f.x * x1.y - f.y * x1.x;
+          }
         }
+        acc[r][0] = a0;
+        acc[r][1] = a1;
       }
     }
+    __syncwarp();
   }
-  if (t < NC) {
-    M[(size_t)par * 2 * NC + t] = a0;
-    M[(size_t)par * 2 * NC + NC + t] = a1;
+  __syncthreads();
+  double2* part = sbuf;  // [warp][2][NC] partial multipoles
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int t = lane + 32 * r;
+    if (t < NC) {
+      part[warp * 2 * NC + t] = acc[r][0];
+      part[warp * 2 * NC + NC + t] = acc[r][1];
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 2 * NC; t += blockDim.x) {
+    double2 s = part[t];
+    for (int w = 1; w < W; ++w) s = cadd(s, part[w * 2 * NC + t]);
+    M[(size_t)par * 2 * NC + t] = s;
   }
 }
 
@@ -334,44 +381,52 @@ __global__ void k_m2l_reduce(int ntargets, const int* __restrict__ targets, cons
 }
 
 // ---------------------------------------------------------------------------
-// L2L: one block per parent; each child gets L'_k^j += sum_{n>=k} L_n^m conj(F_{n-k}^{m-j}).
+// L2L: one block of 8 warps per parent, warp w shifting the parent's local expansion to
+// child w (lane per output coefficient): L'_k^j += sum_{n>=k} L_n^m conj(F_{n-k}^{m-j}).
 template <int P>
-__global__ void k_l2l(const int* __restrict__ parents, const int* __restrict__ child_begin, const int* __restrict__ child_end,
-                      const int* __restrict__ node_children, const double* __restrict__ node_X, double2* __restrict__ L) {
-  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
-  __shared__ double2 sF[NF];
+__global__ void __launch_bounds__(32 * kTreeWarps) k_l2l(const int* __restrict__ parents, const int* __restrict__ child_begin,
+                                                       const int* __restrict__ child_end, const int* __restrict__ node_children,
+                                                       const double* __restrict__ node_X, double2* __restrict__ L) {
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), R = (NC + 31) / 32;
   __shared__ double2 sL[2 * NF];
+  __shared__ double2 sFw[kTreeWarps * NF];
   const int par = parents[blockIdx.x];
-  const int t = threadIdx.x;
-  int k = 0, j = 0;
-  if (t < NC) decode_nm(t, k, j);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   expand_full<P>(L + (size_t)par * 2 * NC, sL);
-  for (int ci = child_begin[par]; ci < child_end[par]; ++ci) {
+  __syncthreads();
+  double2* sF = sFw + warp * NF;
+  const int cb = child_begin[par], ce = child_end[par];
+  for (int ci = cb + warp; ci < ce; ci += kTreeWarps) {
     const int c = node_children[ci];
-    __syncthreads();
-    if (t < 32)
-      F_full_column<P>(t, node_X[3 * c] - node_X[3 * par], node_X[3 * c + 1] - node_X[3 * par + 1],
-                       node_X[3 * c + 2] - node_X[3 * par + 2], sF);
-    __syncthreads();
-    if (t < NC) {
-      double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
-      for (int n = k; n <= P; ++n) {
-        const int dn = n - k;
-        const int lo = max(-n, j - dn), hi = min(n, j + dn);
-        for (int m = lo; m <= hi; ++m) {
-          const double2 f = sF[dn * (dn + 1) + (m - j)];
-          const double2 x0 = sL[n * (n + 1) + m], x1 = sL[NF + n * (n + 1) + m];
-          // x * conj(f)
-          a0.x += x0.x * f.x + x0.y * f.y;
-          a0.y += x0.y * f.x - x0.x * f.y;
-          a1.x += x1.x * f.x + x1.y * f.y;
-          a1.y += x1.y * f.x - x1.x * f.y;
+    F_full_column<P>(lane, node_X[3 * c] - node_X[3 * par], node_X[3 * c + 1] - node_X[3 * par + 1],
+                     node_X[3 * c + 2] - node_X[3 * par + 2], sF);
+    __syncwarp();
+    double2* dst = L + (size_t)c * 2 * NC;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int t = lane + 32 * r;
+      if (t < NC) {
+        int k, j;
+        decode_nm(t, k, j);
+        double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
+        for (int n = k; n <= P; ++n) {
+          const int dn = n - k;
+          const int lo = max(-n, j - dn), hi = min(n, j + dn);
+          for (int m = lo; m <= hi; ++m) {
+            const double2 f = sF[dn * (dn + 1) + (m - j)];
+            const double2 x0 = sL[n * (n + 1) + m], x1 = sL[NF + n * (n + 1) + m];
+            // x * conj(f)
+            a0.x += x0.x * f.x + x0.y * f.y;
+            a0.y += x0.y * f.x - x0.x * f.y;
+            a1.x += x1.x * f.x + x1.y * f.y;
+            a1.y += x1.y * f.x - x1.x * f.y;
+          }
         }
+        dst[t] = cadd(dst[t], a0);
+        dst[NC + t] = cadd(dst[NC + t], a1);
       }
-      double2* dst = L + (size_t)c * 2 * NC;
-      dst[t] = cadd(dst[t], a0);
-      dst[NC + t] = cadd(dst[NC + t], a1);
     }
+    __syncwarp();
   }
 }
 
@@ -729,7 +784,7 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     for (int l = a.n_levels - 1; l >= 0; --l) {
       const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
       if (cnt > 0) {
-        k_m2m<P><<<cnt, tpb_coef, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.M);
+        k_m2m<P><<<cnt, 32 * m2m_warps<P>(), 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.M);
         ++launches;
       }
     }
@@ -755,7 +810,7 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     for (int l = 0; l < a.n_levels; ++l) {
       const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
       if (cnt > 0) {
-        k_l2l<P><<<cnt, tpb_coef, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.L);
+        k_l2l<P><<<cnt, 32 * kTreeWarps, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.L);
         ++launches;
       }
     }

@@ -378,33 +378,63 @@ __global__ void __launch_bounds__(256, 1)
 
 // Per target bucket: L[0] = sum of its slots (target-major CSR order, deterministic), back to
 // the FP64 complex layout [node][density][NC] with the normalisation and a_t^{n+1} undone;
-// L[1] stays zero (the combined density carries both).
+// L[1] stays zero (the combined density carries both; L is cleared before the M2L).
+// One warp per target: lane l sums real coefficients [l*V, l*V+V) of every slot with vector
+// loads (a warp reads one whole slot row per instruction), four slots in flight.
 template <int P>
 __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, const int* __restrict__ m2l_off,
                                 const double* __restrict__ node_dL, const double* __restrict__ alpha, const float* __restrict__ Y,
                                 double2* __restrict__ L) {
   using D = TcDims<P>;
-  constexpr int NC = ncoef(P);
-  const int64_t total = (int64_t)ntargets * NC;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int ti = (int)(e / NC);
-    const int o = (int)(e - (int64_t)ti * NC);
-    int n = 0;
-    while ((n + 1) * (n + 2) / 2 <= o) ++n;
-    const int m = o - n * (n + 1) / 2;
-    const int ire = n * n + (m == 0 ? 0 : 2 * m - 1);
+  constexpr int NC = ncoef(P), V = D::KP / 32;
+  static_assert(V == 2 || V == 4, "slot rows of 64 or 128 floats");
+  const int lane = threadIdx.x & 31;
+  const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int ti = w0; ti < ntargets; ti += nw) {
     const int tgt = targets[ti];
-    double sr = 0.0, si = 0.0;
-    for (int k = m2l_off[tgt]; k < m2l_off[tgt + 1]; ++k) {
-      const float* y = Y + (size_t)k * D::KP;
-      sr += (double)y[ire];
-      if (m > 0) si += (double)y[ire + 1];
+    const int k0 = m2l_off[tgt], k1 = m2l_off[tgt + 1];
+    double acc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = 0.0;
+    auto load = [&](int k, float out[V]) {
+      const float* row = Y + (size_t)k * D::KP + lane * V;
+      if constexpr (V == 4) {
+        const float4 q = __ldcs(reinterpret_cast<const float4*>(row));
+        out[0] = q.x; out[1] = q.y; out[2] = q.z; out[3] = q.w;
+      } else {
+        const float2 q = __ldcs(reinterpret_cast<const float2*>(row));
+        out[0] = q.x; out[1] = q.y;
+      }
+    };
+    int k = k0;
+    for (; k + 4 <= k1; k += 4) {
+      float a0[V], a1[V], a2[V], a3[V];
+      load(k, a0);
+      load(k + 1, a1);
+      load(k + 2, a2);
+      load(k + 3, a3);
+#pragma unroll
+      for (int v = 0; v < V; ++v) acc[v] += ((double)a0[v] + (double)a1[v]) + ((double)a2[v] + (double)a3[v]);
+    }
+    for (; k < k1; ++k) {
+      float a0[V];
+      load(k, a0);
+#pragma unroll
+      for (int v = 0; v < V; ++v) acc[v] += (double)a0[v];
     }
     const double a = node_dL[tgt];
-    double ap = a;
-    for (int t = 0; t < n; ++t) ap *= a;
-    const double f = alpha[ire] / ap;
-    L[(size_t)tgt * 2 * NC + o] = make_double2(sr * f, si * f);
+    double* Lr = reinterpret_cast<double*>(L + (size_t)tgt * 2 * NC);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const int i = lane * V + v;
+      if (i < D::NR) {
+        int n, m, part;
+        decode_real(i, n, m, part);
+        double ap = a;
+        for (int t = 0; t < n; ++t) ap *= a;
+        Lr[2 * cidx(n, m) + part] = acc[v] * alpha[i] / ap;
+      }
+    }
   }
 }
 
@@ -428,8 +458,7 @@ int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts) {
     ++launches;
   }
   if (parts & TC_REDUCE) {
-    const int64_t tr = (int64_t)a.n_m2l_targets * ncoef(P);
-    const int gr = (int)std::min<int64_t>((tr + 255) / 256, 148 * 16);
+    const int gr = (int)std::min<int64_t>(((int64_t)a.n_m2l_targets * 32 + 255) / 256, 148 * 16);
     k_m2l_tc_reduce<P><<<gr, 256, 0, st>>>(a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.node_dL, a.tc_alpha, a.tc_Y, a.L);
     ++launches;
   }
