@@ -115,7 +115,7 @@ struct bem_gpu_ctx {
   int graph_kernels = 0;
   // mixed precision: tensor-core M2L tables and buffers; graph of the low-precision A.x
   bool mixed = false;
-  DBuf<int> tc_item_tab, tc_item_begin, tc_item_cnt, tc_pair, tc_err;
+  DBuf<int> tc_item_tab, tc_item_begin, tc_item_cnt, tc_pair, tc_src, tc_err;
   DBuf<double> tc_tabvec, tc_alpha, node_dL;
   DBuf<uint16_t> tc_T, tc_Mt;
   DBuf<float> tc_escale;
@@ -204,6 +204,7 @@ struct bem_gpu_ctx {
     a.tc_item_begin = tc_item_begin.p;
     a.tc_item_cnt = tc_item_cnt.p;
     a.tc_pair = tc_pair.p;
+    a.tc_src = tc_src.p;
     a.tc_tab = tc_T.p;
     a.tc_Mt = tc_Mt.p;
     a.tc_escale = tc_escale.p;
@@ -511,6 +512,11 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     CK(up(ctx, ctx->tc_item_begin, P.tc_item_begin));
     CK(up(ctx, ctx->tc_item_cnt, P.tc_item_cnt));
     CK(up(ctx, ctx->tc_pair, P.tc_pair));
+    {
+      std::vector<int> src(P.tc_pair.size());
+      for (size_t j = 0; j < src.size(); ++j) src[j] = P.m2l_src[P.tc_pair[j]];
+      CK(up(ctx, ctx->tc_src, src));
+    }
     CK(up(ctx, ctx->tc_tabvec, P.tc_tab));
     CK(up(ctx, ctx->tc_alpha, al));
     CK(up(ctx, ctx->node_dL, dl));

@@ -53,6 +53,7 @@ struct MatvecArgs {
   const int* tc_item_begin = nullptr;
   const int* tc_item_cnt = nullptr;
   const int* tc_pair = nullptr;
+  const int* tc_src = nullptr;   // source bucket of each tc_pair entry
   const void* tc_tab = nullptr;  // FP16 hi/lo table images
   void* tc_Mt = nullptr;         // FP16 hi/lo rows of M[0] - M[1] [n_nodes+1][2][KP]
   float* tc_escale = nullptr;    // [n_nodes] power-of-two column scales

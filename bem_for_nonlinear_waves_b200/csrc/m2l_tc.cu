@@ -28,8 +28,8 @@
 // the same L2P, so the M2L here translates the combined multipole M[0] - M[1] into L[0] and
 // leaves L[1] = 0: one column per pair instead of two.
 //
-// GEMM shape per work item (<= 256 pairs of one table): D[pairs x 128 coefficients] =
-// B[pairs x KP] * T~[128 x KP]^T, B = gathered multipole rows, T~ = the table; both K-major,
+// GEMM shape per work item (<= 256 pairs of one table): D[128 coefficients x pairs] =
+// T~[128 x KP] * B[pairs x KP]^T, B = gathered multipole rows, T~ = the table; both K-major,
 // staged in shared memory by the TMA unit, D in tensor memory, one thread issues the MMAs
 // and commits to mbarriers.
 #include <cuda.h>
@@ -190,17 +190,20 @@ __global__ void k_tc_expand(int nnodes, const double2* __restrict__ M, const dou
 // ---------------------------------------------------------------------------
 // The contraction: persistent, warp-specialised CTAs, each over a contiguous range of work
 // items (consecutive items mostly share a table, which then stays in shared memory).
-//   warps 0-3  epilogue: TMEM lane = gathered row (= pair); read the translated coefficients
-//              of the row, undo the column scale, store the row to the pair's slot
-//   warps 4-7  producers: item metadata (loaded before the waits, so its latency overlaps
-//              them); TMA: one bulk copy of the table image when the table changes, and
+//   warps 0-7  epilogue: TMEM lane = output coefficient, column = pair; warp w reads lane
+//              quadrant w % 4 and every other 32-column chunk (w / 4 picks which); for each
+//              pair it stores 32 consecutive coefficients (one 128-byte line) of the pair's
+//              slot with the pair's column scale undone.  The next chunk's TMEM load is in
+//              flight while the current chunk is stored.
+//   warps 8-11 producers: the next item's metadata is loaded while the current one runs;
+//              TMA: one bulk copy of the table image when the table changes, and
 //              tile::gather4 loads of the multipole rows of the item's sources into 128-byte
 //              swizzled K-major tiles; producer thread 0 also issues the MMAs
-// MMA per item and row block u (128 gathered rows): D[rows x 128 coefficients] = A * T~^T with
-// A = gathered rows (SW128 K-major), T~ the table (no swizzle, K-major), three passes
+// MMA per item: D[128 coefficients x N pairs] = T~ * B^T with A = T~ (no swizzle, K-major)
+// and B = gathered rows (SW128 K-major), N = pairs rounded up to 16, three passes
 // hi*hi + hi*lo + lo*hi.  Shared memory holds one item, TMEM two (buffer b = item parity,
-// 2 row blocks x 128 columns each), so the epilogue of an item overlaps the loads and MMAs
-// of the next.  Barriers:
+// 256 columns each), so the epilogue of an item overlaps the loads and MMAs of the next.
+// Barriers:
 //   full         all TMA bytes of the item landed                 -> MMA issuer
 //   smem_free    MMAs of the item finished reading shared memory  -> producers
 //   acc_full[b]  accumulator buffer b written                      -> epilogue
@@ -209,12 +212,13 @@ __global__ void k_tc_expand(int nnodes, const double2* __restrict__ M, const dou
 // Every wait is bounded; a timeout records *err and ends the waiting role's loop, and the
 // roles waiting on it then time out as well rather than wait forever.
 constexpr int kProducers = 128;
+constexpr int kEpilogue = 256;
 constexpr int kColsPerProducer = kMaxCols / kProducers;
 
 template <int P>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(kEpilogue + kProducers, 1)
     k_m2l_tc(const __grid_constant__ CUtensorMap rows_map, int nitems, const int* __restrict__ item_tab, const int* __restrict__ item_begin,
-             const int* __restrict__ item_cnt, const int* __restrict__ tc_pair, const int* __restrict__ m2l_src,
+             const int* __restrict__ item_cnt, const int* __restrict__ tc_pair, const int* __restrict__ tc_src,
              const __half* __restrict__ Ttab, const float* __restrict__ escale, float* __restrict__ Y, int* __restrict__ err) {
   using D = TcDims<P>;
   extern __shared__ __align__(128) unsigned char sm_raw[];
@@ -236,7 +240,7 @@ __global__ void __launch_bounds__(256, 1)
     mbar_init(&bar_free, 1);
     for (int b = 0; b < 2; ++b) {
       mbar_init(&bar_accf[b], 1);
-      mbar_init(&bar_acce[b], 128);
+      mbar_init(&bar_acce[b], kEpilogue);
       mbar_init(&bar_meta[b], 1);
     }
   }
@@ -244,25 +248,30 @@ __global__ void __launch_bounds__(256, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = tslot;
-  if (warp >= 4) {
-    const int pt = tid - 128;  // producer thread
+  if (tid >= kEpilogue) {
+    const int pt = tid - kEpilogue;  // producer thread
     int last_tab = -1, issued = 0;
     bool ok = true;
-    for (int it = i0; it < i1; ++it) {
-      const int li = it - i0, b = li & 1;
-      // metadata into registers first: independent of shared memory, overlaps the waits
-      const int tab = item_tab[it], b0 = item_begin[it], ncol = item_cnt[it];
-      int r_slot[kColsPerProducer], r_src[kColsPerProducer];
-      float r_sc[kColsPerProducer];
+    // metadata of item `it` in registers (loaded one item ahead)
+    int tab = 0, ncol = 0;
+    int r_slot[kColsPerProducer], r_src[kColsPerProducer];
+    float r_sc[kColsPerProducer];
+    auto fetch = [&](int it) {
+      tab = item_tab[it];
+      const int b0 = item_begin[it];
+      ncol = item_cnt[it];
 #pragma unroll
       for (int e = 0; e < kColsPerProducer; ++e) {
         const int c = pt + e * kProducers;
         r_slot[e] = c < ncol ? tc_pair[b0 + c] : 0;
+        r_src[e] = c < ncol ? tc_src[b0 + c] : 0;
       }
 #pragma unroll
-      for (int e = 0; e < kColsPerProducer; ++e) r_src[e] = (pt + e * kProducers) < ncol ? m2l_src[r_slot[e]] : 0;
-#pragma unroll
       for (int e = 0; e < kColsPerProducer; ++e) r_sc[e] = (pt + e * kProducers) < ncol ? escale[r_src[e]] : 0.f;
+    };
+    if (i0 < i1) fetch(i0);
+    for (int it = i0; it < i1; ++it) {
+      const int li = it - i0, b = li & 1;
       if (ok && li > 0) ok = mbar_wait(&bar_free, (li - 1) & 1, kWaitTries);
       if (ok && li > 1) ok = mbar_wait(&bar_acce[b], ((li >> 1) - 1) & 1, kWaitTries);
       if (named_bar_or(1, kProducers, ok ? 0 : 1)) {
@@ -278,18 +287,19 @@ __global__ void __launch_bounds__(256, 1)
           s_slot[b][c] = r_slot[e];
         }
       }
-      const int nquad = (ncol + 3) >> 2;
-      const bool load_tab = tab != last_tab;
-      last_tab = tab;
+      const int cur_tab = tab, cur_ncol = ncol;
+      const int nquad = (cur_ncol + 3) >> 2;
+      const bool load_tab = cur_tab != last_tab;
+      last_tab = cur_tab;
       if (pt == 0) {
-        s_ncol[b] = ncol;
+        s_ncol[b] = cur_ncol;
         const uint32_t bytes = (load_tab ? (uint32_t)D::TAB_BYTES : 0u) + (uint32_t)nquad * 4u * 128u * 2u * D::KA;
         mbar_arrive_expect_tx(&bar_full, bytes);
       }
       named_bar_sync(1, kProducers);
       if (pt == 0) {
         mbar_arrive(&bar_meta[b]);
-        if (load_tab) bulk_copy_g2s(sT, reinterpret_cast<const unsigned char*>(Ttab) + (size_t)tab * D::TAB_BYTES, D::TAB_BYTES, &bar_full);
+        if (load_tab) bulk_copy_g2s(sT, reinterpret_cast<const unsigned char*>(Ttab) + (size_t)cur_tab * D::TAB_BYTES, D::TAB_BYTES, &bar_full);
       }
       // gather4: quad q of rows, part (hi/lo), atom a -> region (part, a), rows 4q..4q+3
       for (int g = pt; g < nquad * 2 * D::KA; g += kProducers) {
@@ -298,31 +308,30 @@ __global__ void __launch_bounds__(256, 1)
         int y[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          const int c = min(4 * q + i, ncol - 1);
+          const int c = min(4 * q + i, cur_ncol - 1);
           y[i] = s_row[c] * 2 + part;
         }
         tma_gather4(sB + (part * D::KA + a) * D::REGION + q * 4 * 128, &rows_map, a * 64, y[0], y[1], y[2], y[3], &bar_full);
       }
+      if (it + 1 < i1) fetch(it + 1);  // next item's metadata while this one loads and runs
       if (pt == 0) {
         if (mbar_wait(&bar_full, li & 1, kWaitTries)) {
           tc_fence_after();
-          constexpr uint32_t idesc = make_idesc_f16_f32(128, kRows);
+          const int npad = (cur_ncol + 15) & ~15;
+          const uint32_t idesc = make_idesc_f16_f32(kRows, npad);
           constexpr uint32_t SBO_T = D::KP * 16;
-          const uint32_t aBase = smem_u32(sB);
-          const uint32_t bH = smem_u32(sT), bL = bH + kRows * D::KP * 2;
-          for (int u = 0; u * 128 < ncol; ++u) {
-            const uint32_t dt = tbase + (uint32_t)(b * 256 + u * 128);
-            const uint32_t ro = (uint32_t)(u * 128 * 128);  // row block offset inside a region
+          const uint32_t bBase = smem_u32(sB);
+          const uint32_t aH = smem_u32(sT), aL = aH + kRows * D::KP * 2;
+          const uint32_t dt = tbase + (uint32_t)(b * 256);
 #pragma unroll 1
-            for (int pass = 0; pass < 3; ++pass) {
-              const int apart = pass == 2 ? 1 : 0;      // A: hi, hi, lo
-              const uint32_t bT = pass == 1 ? bL : bH;  // T: hi, lo, hi
+          for (int pass = 0; pass < 3; ++pass) {
+            const uint32_t aT = pass == 2 ? aL : aH;  // T: hi, hi, lo
+            const int bpart = pass == 1 ? 1 : 0;     // rows: hi, lo, hi
 #pragma unroll 1
-              for (int k = 0; k < D::KP / 16; ++k) {
-                const uint32_t aaddr = aBase + (uint32_t)((apart * D::KA + (k >> 2)) * D::REGION) + ro + (uint32_t)((k & 3) * 32);
-                tc_mma_f16(dt, make_smem_desc_sw128(aaddr, 1024), make_smem_desc(bT + 256 * k, 128, SBO_T), idesc,
-                           (pass > 0 || k > 0) ? 1u : 0u);
-              }
+            for (int k = 0; k < D::KP / 16; ++k) {
+              const uint32_t baddr = bBase + (uint32_t)((bpart * D::KA + (k >> 2)) * D::REGION) + (uint32_t)((k & 3) * 32);
+              tc_mma_f16(dt, make_smem_desc(aT + 256 * k, 128, SBO_T), make_smem_desc_sw128(baddr, 1024), idesc,
+                         (pass > 0 || k > 0) ? 1u : 0u);
             }
           }
           tc_commit(&bar_free);
@@ -334,9 +343,12 @@ __global__ void __launch_bounds__(256, 1)
       }
     }
     if (!ok) atomicExch(err, 1);
-    // on an early exit, let copies and MMAs already issued finish before the CTA leaves
+    // on an early exit, let MMAs already issued finish before the CTA leaves
     if (pt == 0 && !ok && issued > 0) mbar_wait(&bar_free, (issued - 1) & 1, kWaitTries);
   } else {
+    const int quad = warp & 3, half = warp >> 2;
+    const int i = quad * 32 + lane;  // output coefficient of this thread's TMEM lane
+    const uint32_t lane_base = tbase + ((uint32_t)(quad * 32) << 16);
     for (int it = i0; it < i1; ++it) {
       const int li = it - i0, b = li & 1;
       bool ok = mbar_wait(&bar_meta[b], (li >> 1) & 1, kWaitTries);
@@ -347,21 +359,33 @@ __global__ void __launch_bounds__(256, 1)
       }
       tc_fence_after();
       const int ncol = s_ncol[b];
-      for (int u = 0; u * 128 < ncol; ++u) {
-        const int c = u * 128 + warp * 32 + lane;
-        const bool valid = c < ncol;
-        const int slot = valid ? s_slot[b][c] : 0;
-        const float sc = valid ? s_sc[b][c] : 0.f;
-        float* yrow = Y + (size_t)slot * D::KP;
-#pragma unroll 1
-        for (int q = 0; q * 32 < D::KP; ++q) {
-          float v[32];
-          tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * 256 + u * 128 + q * 32), v);
-          if (valid) {
+      if (quad * 32 < D::KP) {
+        const uint32_t col0 = (uint32_t)(b * 256);
+        uint32_t ra[32], rb[32];
+        int c0 = half * 32;
+        if (c0 < ncol) {
+          tmem_ld32_issue(lane_base + col0 + c0, ra);
+          tmem_ld32_wait(ra);
+        }
+        auto store = [&](const uint32_t* r, int cbase) {
 #pragma unroll
-            for (int e = 0; e < 32; e += 4)
-              *reinterpret_cast<float4*>(yrow + q * 32 + e) = make_float4(v[e] * sc, v[e + 1] * sc, v[e + 2] * sc, v[e + 3] * sc);
+          for (int q = 0; q < 32; ++q) {
+            const int j = cbase + q;
+            if (j < ncol) Y[(size_t)s_slot[b][j] * D::KP + i] = __uint_as_float(r[q]) * s_sc[b][j];
           }
+        };
+        while (c0 < ncol) {
+          const int c1 = c0 + 64;
+          if (c1 < ncol) tmem_ld32_issue(lane_base + col0 + c1, rb);
+          store(ra, c0);
+          if (c1 >= ncol) break;
+          tmem_ld32_wait(rb);
+          const int c2 = c1 + 64;
+          if (c2 < ncol) tmem_ld32_issue(lane_base + col0 + c2, ra);
+          store(rb, c1);
+          if (c2 >= ncol) break;
+          tmem_ld32_wait(ra);
+          c0 = c2;
         }
       }
       tc_fence_before();
@@ -453,7 +477,7 @@ int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts) {
     const int grid = a.n_tc_items < a.tc_grid ? a.n_tc_items : a.tc_grid;
     CUtensorMap map;
     std::memcpy(&map, a.tc_rows_map, sizeof(map));
-    k_m2l_tc<P><<<grid, 256, D::SMEM, st>>>(map, a.n_tc_items, a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt, a.tc_pair, a.m2l_src,
+    k_m2l_tc<P><<<grid, kEpilogue + kProducers, D::SMEM, st>>>(map, a.n_tc_items, a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt, a.tc_pair, a.tc_src,
                                              static_cast<const __half*>(a.tc_tab), a.tc_escale, a.tc_Y, a.tc_err);
     ++launches;
   }
