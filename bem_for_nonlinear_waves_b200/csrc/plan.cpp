@@ -4,6 +4,7 @@
 #include "plan.hpp"
 
 #include <algorithm>
+#include <parallel/algorithm>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -523,40 +524,50 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   }
   P.m2l_pairs = P.m2l_off[nb];
   lap(3);
-  // M2L grouped by (level, lattice offset); groups sorted by key, pairs in slot order
+  // M2L grouped by lattice offset r = (X_t - X_s) / dL_t and level; groups ordered by key,
+  // pairs within a group in slot order.  One parallel sort of packed 64-bit values
+  // (offset key | level | slot; a pair off the lattice gets a value of its own, sorted last)
+  // serves both the FP64 groups (level, r) and the tensor-core tables (r on every level).
   {
     const int64_t npair = P.m2l_pairs;
-    std::vector<std::pair<long long, int>> keyed(npair);
-    std::vector<char> lattice_ok(npair, 1);
+    if (npair >= (int64_t(1) << 29)) {
+      P.error = "too many M2L pairs";
+      return false;
+    }
+    std::vector<int> pair_tgt(npair);
 #pragma omp parallel for schedule(static)
     for (int t = 0; t < nb; ++t)
-      for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) {
-        const int s = P.m2l_src[k];
-        long long r[3];
-        for (int a = 0; a < 3; ++a) {
-          const double q = (B[t].X[a] - B[s].X[a]) / B[t].dL;
-          r[a] = std::llround(q);
-          if (std::abs(q - (double)r[a]) > 1e-9 || std::abs(r[a]) > 500) lattice_ok[k] = 0;
-        }
-        const long long key = ((long long)B[t].level << 30) | ((r[0] + 512) << 20) | ((r[1] + 512) << 10) | (r[2] + 512);
-        keyed[k] = {lattice_ok[k] ? key : ((1LL << 50) + k), k};
+      for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) pair_tgt[k] = t;
+    std::vector<uint64_t>& keyed = P.m2l_key_sorted;
+    keyed.resize(npair);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < npair; ++k) {
+      const int t = pair_tgt[k], s = P.m2l_src[k];
+      bool lattice = std::abs(B[s].dL - B[t].dL) <= 1e-12 * B[t].dL;
+      long long r[3];
+      for (int a = 0; a < 3; ++a) {
+        const double q = (B[t].X[a] - B[s].X[a]) / B[t].dL;
+        r[a] = std::llround(q);
+        if (std::abs(q - (double)r[a]) > 1e-9 || std::abs(r[a]) > 500) lattice = false;
       }
-    std::stable_sort(keyed.begin(), keyed.end());
+      const uint64_t rkey = (uint64_t)(((r[0] + 512) << 20) | ((r[1] + 512) << 10) | (r[2] + 512));
+      keyed[k] = lattice ? ((((rkey << 4) | (uint64_t)B[t].level) << 29) | (uint64_t)k) : ((uint64_t(1) << 63) | (uint64_t)k);
+    }
+    __gnu_parallel::sort(keyed.begin(), keyed.end());
     P.grp_vec.clear();
     P.grp_off.assign(1, 0);
     P.grp_pair.resize(npair);
-    std::vector<int> pair_tgt(npair);
-    for (int t = 0; t < nb; ++t)
-      for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) pair_tgt[k] = t;
     for (int64_t i = 0; i < npair;) {
       int64_t j = i;
-      const int k0 = keyed[i].second;
+      const int k0 = (int)(keyed[i] & ((uint64_t(1) << 29) - 1));
       const int t0 = pair_tgt[k0], s0 = P.m2l_src[k0];
       for (int a = 0; a < 3; ++a) P.grp_vec.push_back(B[t0].X[a] - B[s0].X[a]);
-      while (j < npair && keyed[j].first == keyed[i].first) {
-        P.grp_pair[j] = keyed[j].second;
+      const bool lattice = (keyed[i] >> 63) == 0;
+      const uint64_t g = keyed[i] >> 29;
+      do {
+        P.grp_pair[j] = (int)(keyed[j] & ((uint64_t(1) << 29) - 1));
         ++j;
-      }
+      } while (lattice && j < npair && (keyed[j] >> 29) == g);
       P.grp_off.push_back((int)j);
       i = j;
     }
@@ -656,20 +667,31 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
       std::sort(dl.begin(), dl.end());
     }
   }
-  int64_t woff = 0;
+  // offsets first, then one parallel copy into arrays sized once
+  int64_t woff = 0, roff = 0, doff = 0, toff = 0;
   for (int bi = 0; bi < nblk; ++bi) {
     Plan::NearBlock& nbk = P.blocks[bi];
-    nbk.rng_off = (int)P.nb_ranges.size() / 2;
+    nbk.rng_off = (int)(roff / 2);
     nbk.nrng = (int)blk_rng[bi].size() / 2;
-    P.nb_ranges.insert(P.nb_ranges.end(), blk_rng[bi].begin(), blk_rng[bi].end());
-    nbk.dof_off = (int)P.nb_dofs.size();
+    roff += (int64_t)blk_rng[bi].size();
+    nbk.dof_off = (int)doff;
     nbk.ndof = (int)blk_dofs[bi].size();
-    P.nb_dofs.insert(P.nb_dofs.end(), blk_dofs[bi].begin(), blk_dofs[bi].end());
-    nbk.tgt_off = (int)P.nb_targets.size();
+    doff += nbk.ndof;
+    nbk.tgt_off = (int)toff;
     nbk.ntgt = (int)btargets[bi].size();
-    P.nb_targets.insert(P.nb_targets.end(), btargets[bi].begin(), btargets[bi].end());
+    toff += nbk.ntgt;
     nbk.w_off = woff;
     woff += (int64_t)nbk.ntgt * nbk.ndof;
+  }
+  P.nb_ranges.resize(roff);
+  P.nb_dofs.resize(doff);
+  P.nb_targets.resize(toff);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int bi = 0; bi < nblk; ++bi) {
+    const Plan::NearBlock& nbk = P.blocks[bi];
+    std::copy(blk_rng[bi].begin(), blk_rng[bi].end(), P.nb_ranges.begin() + 2 * (int64_t)nbk.rng_off);
+    std::copy(blk_dofs[bi].begin(), blk_dofs[bi].end(), P.nb_dofs.begin() + nbk.dof_off);
+    std::copy(btargets[bi].begin(), btargets[bi].end(), P.nb_targets.begin() + nbk.tgt_off);
   }
   P.nnz = woff;
   lap(5);
@@ -689,38 +711,25 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
 }
 
 void build_tc_groups(Plan& P, int max_pairs) {
+  // tables = runs of one lattice offset over all levels in the sorted pair order of the FP64
+  // groups (the pairs of one offset are contiguous there); pairs off the lattice get one each
   const int nb = (int)P.nodes.size();
-  const int64_t npair = P.m2l_pairs;
+  const int64_t npair = (int64_t)P.m2l_key_sorted.size();
+  const uint64_t kmask = (uint64_t(1) << 29) - 1;
   std::vector<int> pair_tgt(npair);
   for (int t = 0; t < nb; ++t)
     for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) pair_tgt[k] = t;
-  // key: lattice offset r = (X_t - X_s)/dL_t of equal-size buckets (any level), else unique
-  std::vector<std::pair<long long, int>> keyed(npair);
-#pragma omp parallel for schedule(static)
-  for (int64_t k = 0; k < npair; ++k) {
-    const auto& T = P.nodes[pair_tgt[k]];
-    const auto& S = P.nodes[P.m2l_src[k]];
-    bool lattice = std::abs(S.dL - T.dL) <= 1e-12 * T.dL;
-    long long r[3];
-    for (int a = 0; a < 3; ++a) {
-      const double q = (T.X[a] - S.X[a]) / T.dL;
-      r[a] = std::llround(q);
-      if (std::abs(q - (double)r[a]) > 1e-9 || std::abs(r[a]) > 500) lattice = false;
-    }
-    const long long key = ((r[0] + 512) << 20) | ((r[1] + 512) << 10) | (r[2] + 512);
-    keyed[k] = {lattice ? key : ((1LL << 40) + k), (int)k};
-  }
-  std::stable_sort(keyed.begin(), keyed.end());
   P.tc_tab.clear();
   P.tc_pair.resize(npair);
   P.tc_item_tab.clear();
   P.tc_item_begin.clear();
   P.tc_item_cnt.clear();
   for (int64_t i = 0; i < npair;) {
-    const int k0 = keyed[i].second;
+    const uint64_t v0 = P.m2l_key_sorted[i];
+    const bool lattice = (v0 >> 63) == 0;
+    const int k0 = (int)(v0 & kmask);
     const auto& T = P.nodes[pair_tgt[k0]];
     const auto& S = P.nodes[P.m2l_src[k0]];
-    const bool lattice = keyed[i].first < (1LL << 40);
     for (int a = 0; a < 3; ++a) {
       const double q = (T.X[a] - S.X[a]) / T.dL;
       P.tc_tab.push_back(lattice ? (double)std::llround(q) : q);
@@ -728,10 +737,10 @@ void build_tc_groups(Plan& P, int max_pairs) {
     P.tc_tab.push_back(lattice ? 1.0 : S.dL / T.dL);
     const int tab = (int)(P.tc_tab.size() / 4) - 1;
     int64_t j = i;
-    while (j < npair && keyed[j].first == keyed[i].first) {
-      P.tc_pair[j] = keyed[j].second;
+    do {
+      P.tc_pair[j] = (int)(P.m2l_key_sorted[j] & kmask);
       ++j;
-    }
+    } while (lattice && j < npair && (P.m2l_key_sorted[j] >> 33) == (v0 >> 33));
     for (int64_t b = i; b < j; b += max_pairs) {
       P.tc_item_tab.push_back(tab);
       P.tc_item_begin.push_back((int)b);

@@ -80,6 +80,9 @@ struct Plan {
   std::vector<int32_t> chunk_begin;  // first index into grp_pair
   std::vector<int32_t> chunk_cnt;    // pairs in the chunk
   std::vector<int32_t> m2l_targets;  // targets with at least one pair
+  // pairs in group order as packed values (offset key << 33 | level << 29 | slot; bit 63 set
+  // for a pair off the lattice), kept for the tensor-core grouping
+  std::vector<uint64_t> m2l_key_sorted;
   // tensor-core M2L (mixed precision): pairs grouped by their translation measured in
   // target-bucket sizes, so one table serves a lattice offset on every level; work items of
   // at most tc_item_max pairs of one table.  Filled by build_tc_groups().
