@@ -1137,7 +1137,7 @@ int profile_matvec(bem_gpu_ctx* ctx, int repeats, bool tc, double* stage_ms) {
     const int parts[3] = {TC_EXPAND, TC_CONTRACT, TC_REDUCE};
     for (int k = 0; k < 3; ++k) {
       CK(cudaEventRecord(e0, s));
-      for (int r = 0; r < repeats; ++r) launch_m2l_tc(ctx->plan.opt.p, a, s, parts[k]);
+      for (int r = 0; r < repeats; ++r) launch_m2l_tc(ctx->plan.opt.p, a, s, parts[k], 1);
       CK(cudaEventRecord(e1, s));
       CK(cudaEventSynchronize(e1));
       float ms = 0.f;

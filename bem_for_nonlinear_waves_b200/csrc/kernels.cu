@@ -60,7 +60,9 @@ __global__ void k_densities(int n, int mode, const double* __restrict__ x, const
 // P2M: one block (4 warps) per leaf; each half-warp carries one P2M point, lane m its
 // column m of F_n^m, advanced degree by degree in lock-step so that the gradient
 // terms F_{n-1}^{m-1}, F_{n-1}^{m+1} come from the neighbouring lanes by shuffles.
-template <int P>
+// ND = 2: the monopole (phin) and dipole (phi) expansions M[0], M[1] separately; ND = 1: only
+// their difference M[0] - M[1] (in M[0]), all that a mat-vec row GPhin - GnPhi needs.
+template <int P, int ND>
 __global__ void __launch_bounds__(128) k_p2m(const int* __restrict__ leaves, const int* __restrict__ node_fb, const int* __restrict__ node_fe,
                                              const double* __restrict__ node_X, const double* __restrict__ e_q,
                                              const double* __restrict__ e_W, const double* __restrict__ e_n,
@@ -68,7 +70,7 @@ __global__ void __launch_bounds__(128) k_p2m(const int* __restrict__ leaves, con
                                              const double* __restrict__ phin, double2* __restrict__ M) {
   constexpr int NC = ncoef(P);
   static_assert(P <= 14, "column lanes live in a half warp");
-  __shared__ double2 red[4][2][NC];
+  __shared__ double2 red[4][ND][NC];
   const int leaf = leaves[blockIdx.x];
   const int fb = node_fb[leaf], fe = node_fe[leaf];
   const double cx = node_X[3 * leaf], cy = node_X[3 * leaf + 1], cz = node_X[3 * leaf + 2];
@@ -122,10 +124,15 @@ __global__ void __launch_bounds__(128) k_p2m(const int* __restrict__ leaves, con
       g = cadd(g, cscale(cmul(make_double2(nx, ny), up), 0.5));
       g = csub(g, cscale(cmul(make_double2(nx, -ny), dn), 0.5));
       if (n >= m) {
-        accM[n].x += wphin * cur.x;
-        accM[n].y -= wphin * cur.y;
-        accD[n].x += wphi * g.x;
-        accD[n].y -= wphi * g.y;
+        if (ND == 2) {
+          accM[n].x += wphin * cur.x;
+          accM[n].y -= wphin * cur.y;
+          accD[n].x += wphi * g.x;
+          accD[n].y -= wphi * g.y;
+        } else {
+          accM[n].x += wphin * cur.x - wphi * g.x;
+          accM[n].y -= wphin * cur.y - wphi * g.y;
+        }
       }
       prev2 = prev;
       prev = cur;
@@ -134,18 +141,18 @@ __global__ void __launch_bounds__(128) k_p2m(const int* __restrict__ leaves, con
 #pragma unroll
   for (int n = 0; n <= P; ++n) {
     accM[n] = cadd(accM[n], shfl_down2(accM[n], 16, 32));
-    accD[n] = cadd(accD[n], shfl_down2(accD[n], 16, 32));
+    if (ND == 2) accD[n] = cadd(accD[n], shfl_down2(accD[n], 16, 32));
   }
   if (half == 0 && m <= P) {
 #pragma unroll
     for (int n = 0; n <= P; ++n)
       if (n >= m) {
         red[warp][0][cidx(n, m)] = accM[n];
-        red[warp][1][cidx(n, m)] = accD[n];
+        if (ND == 2) red[warp][ND - 1][cidx(n, m)] = accD[n];
       }
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < 2 * NC; t += blockDim.x) {
+  for (int t = threadIdx.x; t < ND * NC; t += blockDim.x) {
     const int d = t / NC, c = t % NC;
     double2 s = red[0][d][c];
     s = cadd(s, red[1][d][c]);
@@ -156,10 +163,10 @@ __global__ void __launch_bounds__(128) k_p2m(const int* __restrict__ leaves, con
 }
 
 // expand half-stored coefficients [2][NC] into full [2][(P+1)^2]
-template <int P>
+template <int P, int ND>
 __device__ __forceinline__ void expand_full(const double2* __restrict__ src, double2* dst) {
   constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
-  for (int t = threadIdx.x; t < 2 * NF; t += blockDim.x) {
+  for (int t = threadIdx.x; t < ND * NF; t += blockDim.x) {
     const int d = t / NF, i = t % NF;
     int n = 0;
     while ((n + 1) * (n + 1) <= i) ++n;
@@ -178,10 +185,10 @@ __device__ __forceinline__ void decode_nm(int t, int& n, int& m) {
 
 // ---------------------------------------------------------------------------
 // warp-level expansion of half-stored coefficients [2][NC] into full [2][(P+1)^2]
-template <int P>
+template <int P, int ND>
 __device__ __forceinline__ void expand_full_warp(const double2* __restrict__ src, double2* dst, int lane) {
   constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
-  for (int t = lane; t < 2 * NF; t += 32) {
+  for (int t = lane; t < ND * NF; t += 32) {
     const int d = t / NF, i = t % NF;
     int n = 0;
     while ((n + 1) * (n + 1) <= i) ++n;
@@ -202,7 +209,7 @@ constexpr int kTreeWarps = 8;
 template <int P>
 constexpr int m2m_warps() { return kTreeWarps * 3 * (P + 1) * (P + 1) * 16 <= 48 * 1024 ? kTreeWarps : kTreeWarps / 2; }
 
-template <int P>
+template <int P, int ND>
 __global__ void __launch_bounds__(32 * m2m_warps<P>()) k_m2m(const int* __restrict__ parents, const int* __restrict__ child_begin,
                                                        const int* __restrict__ child_end, const int* __restrict__ node_children,
                                                        const double* __restrict__ node_X, double2* __restrict__ M) {
@@ -220,7 +227,7 @@ __global__ void __launch_bounds__(32 * m2m_warps<P>()) k_m2m(const int* __restri
     const int c = node_children[ci];
     F_full_column<P>(lane, node_X[3 * c] - node_X[3 * par], node_X[3 * c + 1] - node_X[3 * par + 1],
                      node_X[3 * c + 2] - node_X[3 * par + 2], sF);
-    expand_full_warp<P>(M + (size_t)c * 2 * NC, sM, lane);
+    expand_full_warp<P, ND>(M + (size_t)c * 2 * NC, sM, lane);
     __syncwarp();
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -235,12 +242,15 @@ __global__ void __launch_bounds__(32 * m2m_warps<P>()) k_m2m(const int* __restri
           for (int m1 = lo; m1 <= hi; ++m1) {
             const double2 f = sF[n1 * (n1 + 1) + m1];
             const int i2 = n2 * (n2 + 1) + (m - m1);
-            const double2 x0 = sM[i2], x1 = sM[NF + i2];
+            const double2 x0 = sM[i2];
             // conj(f) * x
             a0.x += f.x * x0.x + f.y * x0.y;
             a0.y += f.x * x0.y - f.y * x0.x;
-            a1.x += f.x * x1.x + f.y * x1.y;
-            a1.y += f.x * x1.y - f.y * x1.x;
+            if (ND == 2) {
+              const double2 x1 = sM[NF + i2];
+              a1.x += f.x * x1.x + f.y * x1.y;
+              a1.y += f.x * x1.y - f.y * x1.x;
+            }
           }
         }
         acc[r][0] = a0;
@@ -256,11 +266,11 @@ __global__ void __launch_bounds__(32 * m2m_warps<P>()) k_m2m(const int* __restri
     const int t = lane + 32 * r;
     if (t < NC) {
       part[warp * 2 * NC + t] = acc[r][0];
-      part[warp * 2 * NC + NC + t] = acc[r][1];
+      if (ND == 2) part[warp * 2 * NC + NC + t] = acc[r][1];
     }
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < 2 * NC; t += blockDim.x) {
+  for (int t = threadIdx.x; t < ND * NC; t += blockDim.x) {
     double2 s = part[t];
     for (int w = 1; w < W; ++w) s = cadd(s, part[w * 2 * NC + t]);
     M[(size_t)par * 2 * NC + t] = s;
@@ -282,13 +292,13 @@ __global__ void k_s_tables(int ngroups, const double* __restrict__ gvec, double2
   if (g < ngroups && threadIdx.x < 32) S_full_column<Q>(threadIdx.x, gvec[3 * g], gvec[3 * g + 1], gvec[3 * g + 2], Sg + (size_t)g * NS);
 }
 
-template <int P>
+template <int P, int ND>
 __global__ void k_expand_full(int nnodes, const double2* __restrict__ M, double2* __restrict__ Mf) {
   constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
-  const int64_t total = (int64_t)nnodes * 2 * NF;
+  const int64_t total = (int64_t)nnodes * ND * NF;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t node = e / (2 * NF);
-    const int r = (int)(e - node * 2 * NF);
+    const int64_t node = e / (ND * NF);
+    const int r = (int)(e - node * ND * NF);
     const int d = r / NF, i = r - d * NF;
     int n = (int)sqrtf((float)i);
     while (n * n > i) --n;
@@ -305,7 +315,7 @@ constexpr int m2l_grp_smem_bytes() {
   return (int)sizeof(double2) * ((2 * P + 1) * (2 * P + 1) + 8 * 2 * (P + 1) * (P + 1));
 }
 
-template <int P>
+template <int P, int ND>
 __global__ void __launch_bounds__(((2 * ncoef(P) + 31) / 32) * 32) k_m2l_grp(const int* __restrict__ chunk_grp, const int* __restrict__ chunk_begin,
                                                                              const int* __restrict__ chunk_cnt, const int* __restrict__ grp_pair,
                                                                              const int* __restrict__ m2l_src, const double2* __restrict__ Sg,
@@ -313,7 +323,7 @@ __global__ void __launch_bounds__(((2 * ncoef(P) + 31) / 32) * 32) k_m2l_grp(con
   constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), Q = 2 * P, NS = (Q + 1) * (Q + 1);
   extern __shared__ double2 smem_grp[];
   double2* sS = smem_grp;        // [NS]
-  double2* sM = smem_grp + NS;   // [8][2][NF]
+  double2* sM = smem_grp + NS;   // [8][ND][NF]
   const int c = blockIdx.x;
   const int g = chunk_grp[c], b0 = chunk_begin[c], cnt = chunk_cnt[c];
   const int t = threadIdx.x;
@@ -321,12 +331,12 @@ __global__ void __launch_bounds__(((2 * ncoef(P) + 31) / 32) * 32) k_m2l_grp(con
     const double2* src = Sg + (size_t)g * NS;
     for (int i = t; i < NS; i += blockDim.x) sS[i] = src[i];
     for (int j = 0; j < cnt; ++j) {
-      const double2* m = Mf + (size_t)m2l_src[grp_pair[b0 + j]] * 2 * NF;
-      for (int i = t; i < 2 * NF; i += blockDim.x) sM[j * 2 * NF + i] = m[i];
+      const double2* m = Mf + (size_t)m2l_src[grp_pair[b0 + j]] * ND * NF;
+      for (int i = t; i < ND * NF; i += blockDim.x) sM[j * ND * NF + i] = m[i];
     }
   }
   __syncthreads();
-  if (t >= 2 * NC) return;
+  if (t >= ND * NC) return;
   const int dd = (t < NC) ? 0 : 1;
   const int o = t - dd * NC;
   int n = 0, m = 0;
@@ -343,7 +353,7 @@ __global__ void __launch_bounds__(((2 * ncoef(P) + 31) / 32) * 32) k_m2l_grp(con
       for (int m1 = -n1; m1 <= n1; ++m1) {
         const double2 s = Srow[m1];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) cfma(acc[j], s, sMd[j * 2 * NF + mb + m1]);
+        for (int j = 0; j < 8; ++j) cfma(acc[j], s, sMd[j * ND * NF + mb + m1]);
       }
     }
   } else {
@@ -355,7 +365,7 @@ __global__ void __launch_bounds__(((2 * ncoef(P) + 31) / 32) * 32) k_m2l_grp(con
         const double2 s = Srow[m1];
 #pragma unroll
         for (int j = 0; j < 8; ++j)
-          if (j < cnt) cfma(acc[j], s, sMd[j * 2 * NF + mb + m1]);
+          if (j < cnt) cfma(acc[j], s, sMd[j * ND * NF + mb + m1]);
       }
     }
   }
@@ -365,14 +375,14 @@ __global__ void __launch_bounds__(((2 * ncoef(P) + 31) / 32) * 32) k_m2l_grp(con
     if (j < cnt) Y[(size_t)grp_pair[b0 + j] * 2 * NC + t] = make_double2(sg * acc[j].x, sg * acc[j].y);
 }
 
-template <int P>
+template <int P, int ND>
 __global__ void k_m2l_reduce(int ntargets, const int* __restrict__ targets, const int* __restrict__ m2l_off, const double2* __restrict__ Y,
                              double2* __restrict__ L) {
   constexpr int NC = ncoef(P);
-  const int64_t total = (int64_t)ntargets * 2 * NC;
+  const int64_t total = (int64_t)ntargets * ND * NC;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int ti = (int)(e / (2 * NC));
-    const int r = (int)(e - (int64_t)ti * 2 * NC);
+    const int ti = (int)(e / (ND * NC));
+    const int r = (int)(e - (int64_t)ti * ND * NC);
     const int tgt = targets[ti];
     double2 s = make_double2(0.0, 0.0);
     for (int k = m2l_off[tgt]; k < m2l_off[tgt + 1]; ++k) s = cadd(s, Y[(size_t)k * 2 * NC + r]);
@@ -383,7 +393,7 @@ __global__ void k_m2l_reduce(int ntargets, const int* __restrict__ targets, cons
 // ---------------------------------------------------------------------------
 // L2L: one block of 8 warps per parent, warp w shifting the parent's local expansion to
 // child w (lane per output coefficient): L'_k^j += sum_{n>=k} L_n^m conj(F_{n-k}^{m-j}).
-template <int P>
+template <int P, int ND>
 __global__ void __launch_bounds__(32 * kTreeWarps) k_l2l(const int* __restrict__ parents, const int* __restrict__ child_begin,
                                                        const int* __restrict__ child_end, const int* __restrict__ node_children,
                                                        const double* __restrict__ node_X, double2* __restrict__ L) {
@@ -392,7 +402,7 @@ __global__ void __launch_bounds__(32 * kTreeWarps) k_l2l(const int* __restrict__
   __shared__ double2 sFw[kTreeWarps * NF];
   const int par = parents[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  expand_full<P>(L + (size_t)par * 2 * NC, sL);
+  expand_full<P, ND>(L + (size_t)par * 2 * NC, sL);
   __syncthreads();
   double2* sF = sFw + warp * NF;
   const int cb = child_begin[par], ce = child_end[par];
@@ -414,16 +424,19 @@ __global__ void __launch_bounds__(32 * kTreeWarps) k_l2l(const int* __restrict__
           const int lo = max(-n, j - dn), hi = min(n, j + dn);
           for (int m = lo; m <= hi; ++m) {
             const double2 f = sF[dn * (dn + 1) + (m - j)];
-            const double2 x0 = sL[n * (n + 1) + m], x1 = sL[NF + n * (n + 1) + m];
+            const double2 x0 = sL[n * (n + 1) + m];
             // x * conj(f)
             a0.x += x0.x * f.x + x0.y * f.y;
             a0.y += x0.y * f.x - x0.x * f.y;
-            a1.x += x1.x * f.x + x1.y * f.y;
-            a1.y += x1.y * f.x - x1.x * f.y;
+            if (ND == 2) {
+              const double2 x1 = sL[NF + n * (n + 1) + m];
+              a1.x += x1.x * f.x + x1.y * f.y;
+              a1.y += x1.y * f.x - x1.x * f.y;
+            }
           }
         }
         dst[t] = cadd(dst[t], a0);
-        dst[NC + t] = cadd(dst[NC + t], a1);
+        if (ND == 2) dst[NC + t] = cadd(dst[NC + t], a1);
       }
     }
     __syncwarp();
@@ -434,7 +447,7 @@ __global__ void __launch_bounds__(32 * kTreeWarps) k_l2l(const int* __restrict__
 // Targets: one block per near block (targets sharing a deepest bucket).  The block
 // stages (phi, phin) of its DOF set in shared memory chunk by chunk, each warp reduces
 // the cached weight rows of its targets, then evaluates L2P and writes the BIE rows.
-template <int P>
+template <int P, int ND>
 __global__ void __launch_bounds__(128) k_targets(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs,
                                                  const int* __restrict__ nb_targets, const double* __restrict__ WG,
                                                  const double* __restrict__ WGn, const double* __restrict__ Xs,
@@ -452,7 +465,7 @@ __global__ void __launch_bounds__(128) k_targets(const NearBlockDev* __restrict_
   const NearBlockDev B = blocks[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarp = blockDim.x >> 5;
-  for (int i = threadIdx.x; i < 2 * NC; i += blockDim.x) sL[i] = L[(size_t)B.node * 2 * NC + i];
+  for (int i = threadIdx.x; i < ND * NC; i += blockDim.x) sL[i] = L[(size_t)B.node * 2 * NC + i];
   for (int i = threadIdx.x; i < B.ntgt; i += blockDim.x) accs[i] = make_double2(0, 0);
   for (int c0 = 0; c0 < B.ndof; c0 += chunk) {
     const int cn = min(chunk, B.ndof - c0);
@@ -504,15 +517,18 @@ __global__ void __launch_bounds__(128) k_targets(const NearBlockDev* __restrict_
           cur = nx;
         }
         // Re(L conj(F))
-        const double2 l0 = sL[cidx(n, m)], l1 = sL[NC + cidx(n, m)];
+        const double2 l0 = sL[cidx(n, m)];
         f0 += w * (l0.x * cur.x + l0.y * cur.y);
-        f1 += w * (l1.x * cur.x + l1.y * cur.y);
+        if (ND == 2) {
+          const double2 l1 = sL[NC + cidx(n, m)];
+          f1 += w * (l1.x * cur.x + l1.y * cur.y);
+        }
       }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       f0 += __shfl_xor_sync(0xffffffffu, f0, o);
-      f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+      if (ND == 2) f1 += __shfl_xor_sync(0xffffffffu, f1, o);
     }
     const double GPhin = accs[tl].x + f0, GnPhi = accs[tl].y + f1;
     if (GPhin_out && lane == 0) {
@@ -771,38 +787,38 @@ __global__ void k_fp64_probe(int iters, double seed, double* __restrict__ sink) 
 
 // ---------------------------------------------------------------------------
 // launchers
-template <int P>
+template <int P, int ND>
 int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
   constexpr int NC = ncoef(P);
   const int tpb_coef = ((NC + 31) / 32) * 32;
   int launches = 0;
   if ((stages & STAGE_P2M) && a.n_leaves > 0) {
-    k_p2m<P><<<a.n_leaves, 128, 0, st>>>(a.leaves, a.node_fb, a.node_fe, a.node_X, a.e_q, a.e_W, a.e_n, a.e_dof, a.phi, a.phin, a.M);
+    k_p2m<P, ND><<<a.n_leaves, 128, 0, st>>>(a.leaves, a.node_fb, a.node_fe, a.node_X, a.e_q, a.e_W, a.e_n, a.e_dof, a.phi, a.phin, a.M);
     ++launches;
   }
   if (stages & STAGE_M2M)
     for (int l = a.n_levels - 1; l >= 0; --l) {
       const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
       if (cnt > 0) {
-        k_m2m<P><<<cnt, 32 * m2m_warps<P>(), 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.M);
+        k_m2m<P, ND><<<cnt, 32 * m2m_warps<P>(), 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.M);
         ++launches;
       }
     }
   if (stages & STAGE_M2L) {
     cudaMemsetAsync(a.L, 0, sizeof(double2) * 2 * NC * (size_t)a.n_nodes, st);
     if (a.use_tc) {
-      launches += launch_m2l_tc(P, a, st);
+      launches += launch_m2l_tc(P, a, st, TC_ALL, ND);
     } else if (a.n_chunks > 0) {
       constexpr int NF = (P + 1) * (P + 1);
-      const int64_t tot = (int64_t)a.n_nodes * 2 * NF;
+      const int64_t tot = (int64_t)a.n_nodes * ND * NF;
       int ge = (int)std::min<int64_t>((tot + 255) / 256, 148 * 16);
-      k_expand_full<P><<<ge, 256, 0, st>>>(a.n_nodes, a.M, a.Mf);
-      const int tpb2 = ((2 * NC + 31) / 32) * 32;
-      k_m2l_grp<P><<<a.n_chunks, tpb2, m2l_grp_smem_bytes<P>(), st>>>(a.chunk_grp, a.chunk_begin, a.chunk_cnt, a.grp_pair, a.m2l_src, a.Sg,
-                                                                    a.Mf, a.Y);
-      const int64_t tr = (int64_t)a.n_m2l_targets * 2 * NC;
+      k_expand_full<P, ND><<<ge, 256, 0, st>>>(a.n_nodes, a.M, a.Mf);
+      const int tpb2 = ((ND * NC + 31) / 32) * 32;
+      k_m2l_grp<P, ND><<<a.n_chunks, tpb2, m2l_grp_smem_bytes<P>(), st>>>(a.chunk_grp, a.chunk_begin, a.chunk_cnt, a.grp_pair, a.m2l_src,
+                                                                        a.Sg, a.Mf, a.Y);
+      const int64_t tr = (int64_t)a.n_m2l_targets * ND * NC;
       int gr = (int)std::min<int64_t>((tr + 255) / 256, 148 * 16);
-      k_m2l_reduce<P><<<gr, 256, 0, st>>>(a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.Y, a.L);
+      k_m2l_reduce<P, ND><<<gr, 256, 0, st>>>(a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.Y, a.L);
       launches += 3;
     }
   }
@@ -810,13 +826,13 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     for (int l = 0; l < a.n_levels; ++l) {
       const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
       if (cnt > 0) {
-        k_l2l<P><<<cnt, 32 * kTreeWarps, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.L);
+        k_l2l<P, ND><<<cnt, 32 * kTreeWarps, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.L);
         ++launches;
       }
     }
   if ((stages & STAGE_TARGETS) && a.n_blocks > 0) {
     const size_t shm = sizeof(double2) * (size_t)(a.chunk + a.max_ntgt);
-    k_targets<P><<<a.n_blocks, 128, shm, st>>>(a.blocks, a.nb_dofs, a.nb_targets, a.WG, a.WGn, a.Xs, a.node_X, a.L, a.phi, a.phin,
+    k_targets<P, ND><<<a.n_blocks, 128, shm, st>>>(a.blocks, a.nb_dofs, a.nb_targets, a.WG, a.WGn, a.Xs, a.node_X, a.L, a.phi, a.phin,
                                                a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.GPhin, a.GnPhi, a.chunk);
     ++launches;
   }
@@ -825,14 +841,15 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
 
 template <int P>
 void set_target_smem(int bytes) {
-  cudaFuncSetAttribute(k_targets<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_targets<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_targets<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages) {
   switch (p) {
 #define BEMB200_CASE(PP) \
   case PP:               \
-    return launch_matvec_fmm<PP>(a, st, stages);
+    return (a.GPhin || a.GnPhi) ? launch_matvec_fmm<PP, 2>(a, st, stages) : launch_matvec_fmm<PP, 1>(a, st, stages);
     BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5) BEMB200_CASE(6)
     BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10) BEMB200_CASE(11) BEMB200_CASE(12)
 #undef BEMB200_CASE
@@ -843,7 +860,8 @@ int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages) {
 
 template <int P>
 void set_m2l_smem() {
-  cudaFuncSetAttribute(k_m2l_grp<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, m2l_grp_smem_bytes<P>());
+  cudaFuncSetAttribute(k_m2l_grp<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, m2l_grp_smem_bytes<P>());
+  cudaFuncSetAttribute(k_m2l_grp<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, m2l_grp_smem_bytes<P>());
 }
 
 template <int P>

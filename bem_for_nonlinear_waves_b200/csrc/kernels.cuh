@@ -104,6 +104,9 @@ void configure_m2l_smem(int p);
 void launch_s_tables(int p, int ngroups, const double* gvec, double2* Sg, cudaStream_t st);
 enum { STAGE_P2M = 1, STAGE_M2M = 2, STAGE_M2L = 4, STAGE_L2L = 8, STAGE_TARGETS = 16, STAGE_ALL = 31 };
 // returns the number of kernels launched
+// One operator application; returns the number of kernel launches.  A call that asks for
+// GPhin / GnPhi carries both densities through the tree; a call for the rows alone carries
+// their difference only (half the P2M, M2M, M2L, L2L and L2P work).
 int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages = STAGE_ALL);
 
 // tensor-core M2L (m2l_tc.cu)
@@ -116,7 +119,8 @@ int tc_max_pairs();                 // pairs per work item
 void tc_alpha_host(int p, double* alpha /*[tc_kp(p)]*/);
 void launch_tc_tables(int p, int ntab, const double* tab, const double* alpha, void* T, unsigned int* maxbits, cudaStream_t st);
 constexpr int TC_EXPAND = 1, TC_CONTRACT = 2, TC_REDUCE = 4, TC_ALL = 7;
-int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st, int parts = TC_ALL);
+// nd = 2: M[0], M[1] separate, their difference is translated; nd = 1: M[0] already holds it
+int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st, int parts = TC_ALL, int nd = 2);
 void launch_densities(int n, int mode, const double* x, const double* known, const int* kind, double* phi, double* phin, cudaStream_t st);
 void launch_near_weights(const NearArgs& a, cudaStream_t st);
 void launch_diag(int n, const int* dof_point, const double* GnPhi, double* diag, cudaStream_t st);

@@ -139,9 +139,10 @@ __global__ void __launch_bounds__(128) k_tc_tables(int ntab, const double* __res
 }
 
 // ---------------------------------------------------------------------------
-// Per mat-vec: FP64 multipoles -> combined M[0] - M[1], normalised, power-of-two scaled FP16
-// hi/lo rows.  One warp per bucket; row layout [hi KP][lo KP] halves.
-template <int P>
+// Per mat-vec: FP64 multipoles -> combined M[0] - M[1] (ND = 2) or M[0] as given (ND = 1),
+// normalised, power-of-two scaled FP16 hi/lo rows.  One warp per bucket; row layout
+// [hi KP][lo KP] halves.
+template <int P, int ND>
 __global__ void k_tc_expand(int nnodes, const double2* __restrict__ M, const double* __restrict__ node_dL,
                             const double* __restrict__ alpha, __half* __restrict__ Mt, float* __restrict__ escale) {
   using D = TcDims<P>;
@@ -160,7 +161,8 @@ __global__ void k_tc_expand(int nnodes, const double2* __restrict__ M, const dou
       if (k < D::NR) {
         int n1, m1, part;
         decode_real(k, n1, m1, part);
-        const double2 c0 = M0[cidx(n1, m1)], c1 = M0[NC + cidx(n1, m1)];
+        const double2 c0 = M0[cidx(n1, m1)];
+        const double2 c1 = ND == 2 ? M0[NC + cidx(n1, m1)] : make_double2(0.0, 0.0);
         double ip = 1.0;
         for (int t = 0; t < n1; ++t) ip *= inv_a;
         x = (part ? (c0.y - c1.y) : (c0.x - c1.x)) * alpha[k] * ip;
@@ -463,14 +465,17 @@ __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, c
 }
 
 template <int P>
-int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts) {
+int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts, int nd) {
   using D = TcDims<P>;
   if (a.n_tc_items <= 0) return 0;
   int launches = 0;
   __half* Mt = static_cast<__half*>(a.tc_Mt);
   if (parts & TC_EXPAND) {
     const int ge = (int)std::min<int64_t>(((int64_t)a.n_nodes * 32 + 255) / 256, 148 * 8);
-    k_tc_expand<P><<<ge, 256, 0, st>>>(a.n_nodes, a.M, a.node_dL, a.tc_alpha, Mt, a.tc_escale);
+    if (nd == 1)
+      k_tc_expand<P, 1><<<ge, 256, 0, st>>>(a.n_nodes, a.M, a.node_dL, a.tc_alpha, Mt, a.tc_escale);
+    else
+      k_tc_expand<P, 2><<<ge, 256, 0, st>>>(a.n_nodes, a.M, a.node_dL, a.tc_alpha, Mt, a.tc_escale);
     ++launches;
   }
   if (parts & TC_CONTRACT) {
@@ -558,11 +563,11 @@ void launch_tc_tables(int p, int ntab, const double* tab, const double* alpha, v
   }
 }
 
-int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st, int parts) {
+int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st, int parts, int nd) {
   switch (p) {
 #define BEMB200_CASE(PP) \
   case PP:               \
-    return m2l_tc_launch<PP>(a, st, parts);
+    return m2l_tc_launch<PP>(a, st, parts, nd);
     BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5)
     BEMB200_CASE(6) BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10)
 #undef BEMB200_CASE
