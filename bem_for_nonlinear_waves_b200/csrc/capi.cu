@@ -92,7 +92,8 @@ struct bem_gpu_ctx {
   double time_setup = 0.0;
 
   // geometry / tree
-  DBuf<double> Xs, e_q, e_W, e_n, e_near, node_X, WG, WGn, diag;
+  DBuf<double> Xs, e_q, e_W, e_n, e_near, node_X, WG, WGn, Wc, diag;
+  DBuf<float> Wc32;  // combined near weights of A.x in FP32 (mixed precision)
   DBuf<int> e_dof, e_vtx, node_fb, node_fe, leaves, level_parents, child_begin, child_end, node_children;
   DBuf<int> m2l_targets, m2l_off, m2l_src, nb_dofs, nb_targets, nb_ranges, dof_inc_off, dof_inc;
   DBuf<int> point_dof_off, point_dof, dof_kind, dof_point;
@@ -195,6 +196,12 @@ struct bem_gpu_ctx {
     a.GnPhi = d_gnphi;
     return a;
   }
+  // marks an argument set as A.x of mv_in (combined near weights, FP32 ones when lowp)
+  void set_ax(MatvecArgs& a, bool lowp) const {
+    a.ax = mv_in.p;
+    a.Wc = lowp ? nullptr : Wc.p;
+    a.Wc32 = lowp ? Wc32.p : nullptr;
+  }
   // switches an argument set to the tensor-core M2L
   void set_tc(MatvecArgs& a) const {
     a.use_tc = 1;
@@ -279,6 +286,7 @@ int capture_matvec(bem_gpu_ctx* ctx, bool tc, cudaGraph_t& graph, cudaGraphExec_
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   launch_densities(ctx->plan.ndof, 0, ctx->mv_in.p, nullptr, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, ctx->stream);
   MatvecArgs a = ctx->args(ctx->phi.p, ctx->phin.p, ctx->mv_out.p, nullptr, nullptr);
+  ctx->set_ax(a, tc);
   if (tc) ctx->set_tc(a);
   launch_matvec(ctx->plan.opt.p, a, ctx->stream);
   CK(cudaStreamEndCapture(ctx->stream, &graph));
@@ -544,6 +552,8 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   CK(cudaMemsetAsync(ctx->M.p, 0, sizeof(double2) * ctx->M.n, s));
   CK(ctx->WG.alloc(std::max<int64_t>(P.nnz, 1)));
   CK(ctx->WGn.alloc(std::max<int64_t>(P.nnz, 1)));
+  CK(ctx->Wc.alloc(std::max<int64_t>(P.nnz, 1)));
+  if (ctx->opts.precision == 1) CK(ctx->Wc32.alloc(std::max<int64_t>(P.nnz, 1)));
   const int N = P.ndof;
   CK(ctx->phi.alloc(N));
   CK(ctx->phin.alloc(N));
@@ -577,6 +587,9 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   na.WG = ctx->WG.p;
   na.WGn = ctx->WGn.p;
   launch_near_weights(na, s);
+  launch_combine_weights((int)P.blocks.size(), ctx->blocks.p, ctx->nb_dofs.p, ctx->dof_kind.p, ctx->WG.p, ctx->WGn.p, ctx->Wc.p,
+                         ctx->opts.precision == 1 ? ctx->Wc32.p : nullptr, s);
+  ctx->launches += ctx->opts.precision == 1 ? 2 : 1;
   CK(cudaGetLastError());
   // rigid-mode diagonal (BEM_solveBVP_GMRES_FMM.hpp:2661-2716)
   launch_densities(N, 2, nullptr, nullptr, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, s);
@@ -1118,6 +1131,7 @@ int profile_matvec(bem_gpu_ctx* ctx, int repeats, bool tc, double* stage_ms) {
   CK(cudaEventCreate(&e1));
   const int stages[5] = {STAGE_P2M, STAGE_M2M, STAGE_M2L, STAGE_L2L, STAGE_TARGETS};
   MatvecArgs a = ctx->args(ctx->phi.p, ctx->phin.p, ctx->mv_out.p, nullptr, nullptr);
+  ctx->set_ax(a, tc);
   if (tc) ctx->set_tc(a);
   for (int k = 0; k < 6; ++k) {
     CK(cudaEventRecord(e0, s));

@@ -544,6 +544,92 @@ __global__ void __launch_bounds__(128) k_targets(const NearBlockDev* __restrict_
   }
 }
 
+// Targets for A.x (the Krylov operator): with the known values zero, each DOF enters the
+// rows through one weight only -- WG (times phin = x) for a Dirichlet DOF, -WGn (times
+// phi = x) otherwise -- so the near sum of a row is one dot product with the combined weights
+// Wc = [Dirichlet] WG - [other] WGn (half the weight bytes of the general kernel), read
+// straight from the unknown vector x; the far field is the L2P of the combined local
+// expansion L[0]; a CORNER row is its own unknown (phi_i = x_i).
+template <int P, typename WT>
+__global__ void __launch_bounds__(128) k_targets_ax(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs,
+                                                    const int* __restrict__ nb_targets, const WT* __restrict__ Wc,
+                                                    const double* __restrict__ Xs, const double* __restrict__ node_X,
+                                                    const double2* __restrict__ L, const double* __restrict__ x,
+                                                    const int* __restrict__ point_dof_off, const int* __restrict__ point_dof,
+                                                    const int* __restrict__ dof_kind, const double* __restrict__ diag,
+                                                    double* __restrict__ rows, int chunk) {
+  constexpr int NC = ncoef(P);
+  extern __shared__ double2 smem[];
+  double* xs = reinterpret_cast<double*>(smem);  // [chunk] x of the block's DOFs
+  double* accs = xs + chunk;                      // [ntgt] near sums
+  __shared__ double2 sL[NC];
+  const NearBlockDev B = blocks[blockIdx.x];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarp = blockDim.x >> 5;
+  for (int i = threadIdx.x; i < NC; i += blockDim.x) sL[i] = L[(size_t)B.node * 2 * NC + i];
+  for (int i = threadIdx.x; i < B.ntgt; i += blockDim.x) accs[i] = 0.0;
+  for (int c0 = 0; c0 < B.ndof; c0 += chunk) {
+    const int cn = min(chunk, B.ndof - c0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < cn; i += blockDim.x) xs[i] = x[nb_dofs[B.dof_off + c0 + i]];
+    __syncthreads();
+    for (int tl = warp; tl < B.ntgt; tl += nwarp) {
+      const WT* w = Wc + B.w_off + (int64_t)tl * B.ndof + c0;
+      double s0 = 0.0;
+      for (int i = lane; i < cn; i += 32) s0 = fma((double)w[i], xs[i], s0);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      if (lane == 0) accs[tl] += s0;
+    }
+  }
+  __syncthreads();
+  const double cx = node_X[3 * B.node], cy = node_X[3 * B.node + 1], cz = node_X[3 * B.node + 2];
+  for (int tl = warp; tl < B.ntgt; tl += nwarp) {
+    const int p = nb_targets[B.tgt_off + tl];
+    const double px = Xs[3 * p] - cx, py = Xs[3 * p + 1] - cy, pz = Xs[3 * p + 2] - cz;
+    double f0 = 0.0;
+    const int m = lane;
+    if (m <= P) {
+      const double r2 = px * px + py * py + pz * pz;
+      double2 cur = make_double2(1.0, 0.0);
+      for (int k = 1; k <= m; ++k) cur = cscale(cmul(cur, make_double2(px, py)), 1.0 / (2.0 * k));
+      double2 prev = make_double2(0.0, 0.0);
+      const double w = (m == 0) ? 1.0 : 2.0;
+      for (int n = m; n <= P; ++n) {
+        if (n > m) {
+          const double inv = 1.0 / double(n * n - m * m);
+          double2 nx = make_double2(((2 * n - 1) * pz * cur.x - r2 * prev.x) * inv, ((2 * n - 1) * pz * cur.y - r2 * prev.y) * inv);
+          prev = cur;
+          cur = nx;
+        }
+        const double2 l0 = sL[cidx(n, m)];
+        f0 += w * (l0.x * cur.x + l0.y * cur.y);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) f0 += __shfl_xor_sync(0xffffffffu, f0, o);
+    const double g = accs[tl] + f0;
+    for (int k = point_dof_off[p] + lane; k < point_dof_off[p + 1]; k += 32) {
+      const int i = point_dof[k];
+      const int kd = dof_kind[i];
+      rows[i] = (kd == 2) ? x[i] : g - (kd == 0 ? 0.0 : diag[i] * x[i]);
+    }
+  }
+}
+
+// Combined near weights of A.x (set-up): Wc = WG for a Dirichlet DOF column, -WGn otherwise.
+template <typename WT>
+__global__ void k_combine_weights(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs, const int* __restrict__ dof_kind,
+                                  const double* __restrict__ WG, const double* __restrict__ WGn, WT* __restrict__ Wc) {
+  const NearBlockDev B = blocks[blockIdx.x];
+  const int64_t total = (int64_t)B.ntgt * B.ndof;
+  for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
+    const int j = (int)(e % B.ndof);
+    const int64_t w = B.w_off + e;
+    Wc[w] = (WT)(dof_kind[nb_dofs[B.dof_off + j]] == 0 ? WG[w] : -WGn[w]);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Near-field quadrature (set-up).  One block per near block; one thread per
 // (target, DOF) weight, summing every incident element vertex whose element lies in the
@@ -830,7 +916,16 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
         ++launches;
       }
     }
-  if ((stages & STAGE_TARGETS) && a.n_blocks > 0) {
+  if ((stages & STAGE_TARGETS) && a.n_blocks > 0 && ND == 1 && a.ax && (a.Wc || a.Wc32)) {
+    const size_t shm = sizeof(double) * (size_t)(a.chunk + a.max_ntgt);
+    if (a.Wc32)
+      k_targets_ax<P, float><<<a.n_blocks, 128, shm, st>>>(a.blocks, a.nb_dofs, a.nb_targets, a.Wc32, a.Xs, a.node_X, a.L, a.ax,
+                                                           a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk);
+    else
+      k_targets_ax<P, double><<<a.n_blocks, 128, shm, st>>>(a.blocks, a.nb_dofs, a.nb_targets, a.Wc, a.Xs, a.node_X, a.L, a.ax,
+                                                            a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk);
+    ++launches;
+  } else if ((stages & STAGE_TARGETS) && a.n_blocks > 0) {
     const size_t shm = sizeof(double2) * (size_t)(a.chunk + a.max_ntgt);
     k_targets<P, ND><<<a.n_blocks, 128, shm, st>>>(a.blocks, a.nb_dofs, a.nb_targets, a.WG, a.WGn, a.Xs, a.node_X, a.L, a.phi, a.phin,
                                                a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.GPhin, a.GnPhi, a.chunk);
@@ -841,6 +936,8 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
 
 template <int P>
 void set_target_smem(int bytes) {
+  cudaFuncSetAttribute(k_targets_ax<P, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_targets_ax<P, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(k_targets<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(k_targets<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
@@ -903,6 +1000,13 @@ void configure_targets_smem(int p, int bytes) {
 #undef BEMB200_CASE
     default: break;
   }
+}
+
+void launch_combine_weights(int nblocks, const NearBlockDev* blocks, const int* nb_dofs, const int* dof_kind, const double* WG,
+                            const double* WGn, double* Wc, float* Wc32, cudaStream_t st) {
+  if (nblocks <= 0) return;
+  if (Wc) k_combine_weights<double><<<nblocks, 256, 0, st>>>(blocks, nb_dofs, dof_kind, WG, WGn, Wc);
+  if (Wc32) k_combine_weights<float><<<nblocks, 256, 0, st>>>(blocks, nb_dofs, dof_kind, WG, WGn, Wc32);
 }
 
 void launch_densities(int n, int mode, const double* x, const double* known, const int* kind, double* phi, double* phin, cudaStream_t st) {

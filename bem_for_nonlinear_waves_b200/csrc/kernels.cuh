@@ -80,6 +80,10 @@ struct MatvecArgs {
   double* rows = nullptr;   // may be null
   double* GPhin = nullptr;  // may be null
   double* GnPhi = nullptr;
+  // A.x application (rows only): unknown vector and combined near weights (either precision)
+  const double* ax = nullptr;
+  const double* Wc = nullptr;
+  const float* Wc32 = nullptr;
 };
 
 struct NearArgs {
@@ -121,6 +125,8 @@ void launch_tc_tables(int p, int ntab, const double* tab, const double* alpha, v
 constexpr int TC_EXPAND = 1, TC_CONTRACT = 2, TC_REDUCE = 4, TC_ALL = 7;
 // nd = 2: M[0], M[1] separate, their difference is translated; nd = 1: M[0] already holds it
 int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st, int parts = TC_ALL, int nd = 2);
+void launch_combine_weights(int nblocks, const NearBlockDev* blocks, const int* nb_dofs, const int* dof_kind, const double* WG,
+                            const double* WGn, double* Wc, float* Wc32, cudaStream_t st);
 void launch_densities(int n, int mode, const double* x, const double* known, const int* kind, double* phi, double* phin, cudaStream_t st);
 void launch_near_weights(const NearArgs& a, cudaStream_t st);
 void launch_diag(int n, const int* dof_point, const double* GnPhi, double* diag, cudaStream_t st);
