@@ -94,6 +94,8 @@ struct bem_gpu_ctx {
   // geometry / tree
   DBuf<double> Xs, e_q, e_W, e_n, e_near, node_X, WG, WGn, Wc, diag;
   DBuf<float> Wc32;  // combined near weights of A.x in FP32 (mixed precision)
+  DBuf<int> leaf_dof_off, leaf_dof, e_slot;  // P2M operator of A.x: DOFs per leaf
+  DBuf<double2> p2m_C;                       // [(leaf, DOF)][NC]
   DBuf<int> e_dof, e_vtx, node_fb, node_fe, leaves, level_parents, child_begin, child_end, node_children;
   DBuf<int> m2l_targets, m2l_off, m2l_src, nb_dofs, nb_targets, nb_ranges, dof_inc_off, dof_inc;
   DBuf<int> point_dof_off, point_dof, dof_kind, dof_point;
@@ -199,6 +201,9 @@ struct bem_gpu_ctx {
   // marks an argument set as A.x of mv_in (combined near weights, FP32 ones when lowp)
   void set_ax(MatvecArgs& a, bool lowp) const {
     a.ax = mv_in.p;
+    a.leaf_dof_off = leaf_dof_off.p;
+    a.leaf_dof = leaf_dof.p;
+    a.p2m_C = p2m_C.p;
     a.Wc = lowp ? nullptr : Wc.p;
     a.Wc32 = lowp ? Wc32.p : nullptr;
   }
@@ -547,6 +552,29 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     launch_tc_tables(p, ntab, ctx->tc_tabvec.p, ctx->tc_alpha.p, ctx->tc_T.p, ctx->tc_max.p, s);
     ctx->launches += 1;
   }
+  {  // P2M operator of A.x: the DOFs of each leaf's elements, and the slot of every vertex
+    const int nl = (int)P.leaves.size();
+    std::vector<int> ldo(nl + 1, 0), ld, es(3 * (size_t)P.nf, 0);
+    std::vector<int> seen(P.ndof, -1);
+    for (int li = 0; li < nl; ++li) {
+      const auto& Nd = P.nodes[P.leaves[li]];
+      for (int s2 = Nd.fb; s2 < Nd.fe; ++s2)
+        for (int a = 0; a < 3; ++a) {
+          const int d = P.e_dof[3 * s2 + a];
+          if (seen[d] < ldo[li]) {  // first time in this leaf
+            seen[d] = (int)ld.size();
+            ld.push_back(d);
+          }
+          es[3 * s2 + a] = seen[d] - ldo[li];
+        }
+      ldo[li + 1] = (int)ld.size();
+    }
+    CK(up(ctx, ctx->leaf_dof_off, ldo));
+    CK(up(ctx, ctx->leaf_dof, ld));
+    CK(up(ctx, ctx->e_slot, es));
+    CK(ctx->p2m_C.alloc(std::max<size_t>(ld.size(), 1) * NC));
+    CK(cudaMemsetAsync(ctx->p2m_C.p, 0, sizeof(double2) * std::max<size_t>(ld.size(), 1) * NC, s));
+  }
   CK(ctx->M.alloc((size_t)nb * 2 * NC));
   CK(ctx->L.alloc((size_t)nb * 2 * NC));
   CK(cudaMemsetAsync(ctx->M.p, 0, sizeof(double2) * ctx->M.n, s));
@@ -586,6 +614,12 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   na.near_region = P.near_region;
   na.WG = ctx->WG.p;
   na.WGn = ctx->WGn.p;
+  {
+    MatvecArgs pa = ctx->args(nullptr, nullptr, nullptr, nullptr, nullptr);
+    ctx->set_ax(pa, false);
+    launch_p2m_op(P.opt.p, pa, ctx->e_slot.p, s);
+    ctx->launches += 1;
+  }
   launch_near_weights(na, s);
   launch_combine_weights((int)P.blocks.size(), ctx->blocks.p, ctx->nb_dofs.p, ctx->dof_kind.p, ctx->WG.p, ctx->WGn.p, ctx->Wc.p,
                          ctx->opts.precision == 1 ? ctx->Wc32.p : nullptr, s);

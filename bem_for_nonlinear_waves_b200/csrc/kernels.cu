@@ -162,6 +162,102 @@ __global__ void __launch_bounds__(128) k_p2m(const int* __restrict__ leaves, con
   }
 }
 
+__device__ __forceinline__ void decode_nm(int t, int& n, int& m) {
+  n = 0;
+  while ((n + 1) * (n + 2) / 2 <= t) ++n;
+  m = t - n * (n + 1) / 2;
+}
+
+// P2M of A.x as a precomputed operator.  With the known values zero, a DOF d of a leaf enters
+// the leaf's combined multipole M[0] - M[1] linearly through its unknown x_d:
+//   C_{leaf,d} = sum over the leaf's element vertices a with DOF d and P2M points k of
+//                W_k N_a(k) conj(F(y_k - c))      (Dirichlet DOF: phin = x_d)
+//             or -W_k N_a(k) conj(nu . grad F)    (otherwise: phi = x_d)
+// so each A.x computes M_leaf = sum_d x_d C_{leaf,d}: one pass over C (a few bytes per
+// source point) instead of the harmonics of every P2M point.  k_p2m_op builds C at set-up:
+// block per leaf, four points at a time (a warp fills the F table of one point), thread per
+// coefficient adding the points in order into its own entries of C (deterministic).
+template <int P>
+__global__ void __launch_bounds__(128) k_p2m_op(const int* __restrict__ leaves, const int* __restrict__ node_fb, const int* __restrict__ node_fe,
+                                                const double* __restrict__ node_X, const double* __restrict__ e_q,
+                                                const double* __restrict__ e_W, const double* __restrict__ e_n,
+                                                const int* __restrict__ e_dof, const int* __restrict__ e_slot,
+                                                const int* __restrict__ dof_kind, const int* __restrict__ leaf_dof_off,
+                                                double2* __restrict__ C) {
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
+  __shared__ double2 sF[4][NF];
+  __shared__ double spt[4][8];  // W, nx, ny, nz, element, point of each staged point
+  const int li = blockIdx.x, leaf = leaves[li];
+  const int fb = node_fb[leaf], fe = node_fe[leaf];
+  const double cx = node_X[3 * leaf], cy = node_X[3 * leaf + 1], cz = node_X[3 * leaf + 2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, t = threadIdx.x;
+  double2* Cl = C + (size_t)leaf_dof_off[li] * NC;
+  int n = 0, m = 0;
+  if (t < NC) decode_nm(t, n, m);
+  const int npts = (fe - fb) * 6;
+  for (int base = 0; base < npts; base += 4) {
+    const int pt = base + warp;
+    if (pt < npts) {
+      const int s = fb + pt / 6, k = pt % 6;
+      F_full_column<P>(lane, e_q[s * 18 + 3 * k] - cx, e_q[s * 18 + 3 * k + 1] - cy, e_q[s * 18 + 3 * k + 2] - cz, sF[warp]);
+      if (lane == 0) {
+        spt[warp][0] = e_W[s * 6 + k];
+        spt[warp][1] = e_n[3 * s];
+        spt[warp][2] = e_n[3 * s + 1];
+        spt[warp][3] = e_n[3 * s + 2];
+      }
+    }
+    __syncthreads();
+    if (t < NC) {
+      for (int w = 0; w < 4; ++w) {
+        const int q = base + w;
+        if (q >= npts) break;
+        const int s = fb + q / 6, k = q % 6;
+        const double2* T = sF[w];
+        const double2 F = T[n * (n + 1) + m];
+        // nu . grad F_n^m = nu_z F_{n-1}^m + 1/2 (nu_x + i nu_y) F_{n-1}^{m-1} - 1/2 (nu_x - i nu_y) F_{n-1}^{m+1}
+        double2 g = make_double2(0.0, 0.0);
+        if (n >= 1) {
+          const double nx = spt[w][1], ny = spt[w][2], nz = spt[w][3];
+          const int b = (n - 1) * n;
+          if (m <= n - 1) g = cscale(T[b + m], nz);
+          if (m - 1 >= -(n - 1)) g = cadd(g, cscale(cmul(make_double2(nx, ny), T[b + m - 1]), 0.5));
+          if (m + 1 <= n - 1) g = csub(g, cscale(cmul(make_double2(nx, -ny), T[b + m + 1]), 0.5));
+        }
+        const double W = spt[w][0];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const int d = e_dof[3 * s + a];
+          const double wa = W * c_dv[k][a];
+          const double2 v = dof_kind[d] == 0 ? make_double2(wa * F.x, -wa * F.y) : make_double2(-wa * g.x, wa * g.y);
+          double2* c = Cl + (size_t)e_slot[3 * s + a] * NC + t;
+          *c = cadd(*c, v);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// M_leaf[0] = sum_d x_d C_{leaf,d} (block per leaf, thread per coefficient)
+template <int P>
+__global__ void k_p2m_apply(const int* __restrict__ leaves, const int* __restrict__ leaf_dof_off, const int* __restrict__ leaf_dof,
+                            const double2* __restrict__ C, const double* __restrict__ x, double2* __restrict__ M) {
+  constexpr int NC = ncoef(P);
+  const int li = blockIdx.x, leaf = leaves[li];
+  const int t = threadIdx.x;
+  if (t >= NC) return;
+  const int d0 = leaf_dof_off[li], d1 = leaf_dof_off[li + 1];
+  double2 acc = make_double2(0.0, 0.0);
+  for (int j = d0; j < d1; ++j) {
+    const double xv = x[leaf_dof[j]];
+    const double2 c = C[(size_t)j * NC + t];
+    acc.x = fma(xv, c.x, acc.x);
+    acc.y = fma(xv, c.y, acc.y);
+  }
+  M[(size_t)leaf * 2 * NC + t] = acc;
+}
+
 // expand half-stored coefficients [2][NC] into full [2][(P+1)^2]
 template <int P, int ND>
 __device__ __forceinline__ void expand_full(const double2* __restrict__ src, double2* dst) {
@@ -177,11 +273,6 @@ __device__ __forceinline__ void expand_full(const double2* __restrict__ src, dou
   }
 }
 
-__device__ __forceinline__ void decode_nm(int t, int& n, int& m) {
-  n = 0;
-  while ((n + 1) * (n + 2) / 2 <= t) ++n;
-  m = t - n * (n + 1) / 2;
-}
 
 // ---------------------------------------------------------------------------
 // warp-level expansion of half-stored coefficients [2][NC] into full [2][(P+1)^2]
@@ -878,7 +969,10 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
   constexpr int NC = ncoef(P);
   const int tpb_coef = ((NC + 31) / 32) * 32;
   int launches = 0;
-  if ((stages & STAGE_P2M) && a.n_leaves > 0) {
+  if ((stages & STAGE_P2M) && a.n_leaves > 0 && ND == 1 && a.ax && a.p2m_C) {
+    k_p2m_apply<P><<<a.n_leaves, ((NC + 31) / 32) * 32, 0, st>>>(a.leaves, a.leaf_dof_off, a.leaf_dof, a.p2m_C, a.ax, a.M);
+    ++launches;
+  } else if ((stages & STAGE_P2M) && a.n_leaves > 0) {
     k_p2m<P, ND><<<a.n_leaves, 128, 0, st>>>(a.leaves, a.node_fb, a.node_fe, a.node_X, a.e_q, a.e_W, a.e_n, a.e_dof, a.phi, a.phin, a.M);
     ++launches;
   }
@@ -995,6 +1089,25 @@ void configure_targets_smem(int p, int bytes) {
 #define BEMB200_CASE(PP) \
   case PP:               \
     set_target_smem<PP>(bytes); break;
+    BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5) BEMB200_CASE(6)
+    BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10) BEMB200_CASE(11) BEMB200_CASE(12)
+#undef BEMB200_CASE
+    default: break;
+  }
+}
+
+template <int P>
+void p2m_op(const MatvecArgs& a, const int* e_slot, cudaStream_t st) {
+  if (a.n_leaves > 0)
+    k_p2m_op<P><<<a.n_leaves, 128, 0, st>>>(a.leaves, a.node_fb, a.node_fe, a.node_X, a.e_q, a.e_W, a.e_n, a.e_dof, e_slot, a.dof_kind,
+                                            a.leaf_dof_off, a.p2m_C);
+}
+
+void launch_p2m_op(int p, const MatvecArgs& a, const int* e_slot, cudaStream_t st) {
+  switch (p) {
+#define BEMB200_CASE(PP) \
+  case PP:               \
+    p2m_op<PP>(a, e_slot, st); break;
     BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5) BEMB200_CASE(6)
     BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10) BEMB200_CASE(11) BEMB200_CASE(12)
 #undef BEMB200_CASE

@@ -84,6 +84,11 @@ struct MatvecArgs {
   const double* ax = nullptr;
   const double* Wc = nullptr;
   const float* Wc32 = nullptr;
+  // P2M operator of A.x: per leaf, the DOFs of its elements (CSR over leaf index) and the
+  // multipole column of each (leaf, DOF)
+  const int* leaf_dof_off = nullptr;
+  const int* leaf_dof = nullptr;
+  double2* p2m_C = nullptr;
 };
 
 struct NearArgs {
@@ -125,6 +130,9 @@ void launch_tc_tables(int p, int ntab, const double* tab, const double* alpha, v
 constexpr int TC_EXPAND = 1, TC_CONTRACT = 2, TC_REDUCE = 4, TC_ALL = 7;
 // nd = 2: M[0], M[1] separate, their difference is translated; nd = 1: M[0] already holds it
 int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st, int parts = TC_ALL, int nd = 2);
+// builds the P2M operator (a.p2m_C zeroed beforehand); e_slot[3 s + a]: slot of the DOF of
+// vertex a of element s within its leaf's DOF list
+void launch_p2m_op(int p, const MatvecArgs& a, const int* e_slot, cudaStream_t st);
 void launch_combine_weights(int nblocks, const NearBlockDev* blocks, const int* nb_dofs, const int* dof_kind, const double* WG,
                             const double* WGn, double* Wc, float* Wc32, cudaStream_t st);
 void launch_densities(int n, int mode, const double* x, const double* known, const int* kind, double* phi, double* phin, cudaStream_t st);
