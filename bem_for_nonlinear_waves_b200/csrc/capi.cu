@@ -94,7 +94,7 @@ struct bem_gpu_ctx {
   // geometry / tree
   DBuf<double> Xs, e_q, e_W, e_n, e_near, node_X, WG, WGn, Wc, diag;
   DBuf<float> Wc32;  // combined near weights of A.x in FP32 (mixed precision)
-  DBuf<int> leaf_dof_off, leaf_dof, e_slot;  // P2M operator of A.x: DOFs per leaf
+  DBuf<int> leaf_dof_off, leaf_dof, e_slot, slot_block;  // P2M operator of A.x: DOFs per leaf
   DBuf<double2> p2m_C;                       // [(leaf, DOF)][NC]
   DBuf<int> e_dof, e_vtx, node_fb, node_fe, leaves, level_parents, child_begin, child_end, node_children;
   DBuf<int> m2l_targets, m2l_off, m2l_src, nb_dofs, nb_targets, nb_ranges, dof_inc_off, dof_inc;
@@ -614,6 +614,19 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   na.near_region = P.near_region;
   na.WG = ctx->WG.p;
   na.WGn = ctx->WGn.p;
+  {
+    std::vector<int> sb(P.nb_targets.size());
+    int mr = 0;
+    for (int bi = 0; bi < (int)P.blocks.size(); ++bi) {
+      const auto& nbk = P.blocks[bi];
+      for (int tl = 0; tl < nbk.ntgt; ++tl) sb[nbk.tgt_off + tl] = bi;
+      mr = std::max(mr, nbk.nrng);
+    }
+    CK(up(ctx, ctx->slot_block, sb));
+    na.n_slots = (int)sb.size();
+    na.slot_block = ctx->slot_block.p;
+    na.max_nrng = mr;
+  }
   {
     MatvecArgs pa = ctx->args(nullptr, nullptr, nullptr, nullptr, nullptr);
     ctx->set_ax(pa, false);

@@ -722,24 +722,26 @@ __global__ void k_combine_weights(const NearBlockDev* __restrict__ blocks, const
 }
 
 // ---------------------------------------------------------------------------
-// Near-field quadrature (set-up).  One block per near block; one thread per
-// (target, DOF) weight, summing every incident element vertex whose element lies in the
-// block's near element ranges.
+// Near-field quadrature (set-up): the weights of a target over the DOFs of its near block,
+// summing every incident element vertex whose element lies in the block's near element ranges.
 __device__ __forceinline__ double dnorm3(double x, double y, double z) { return sqrt(x * x + y * y + z * z); }
 
-__device__ void elem_vertex_weight(int s, int a, int t, const double* __restrict__ Xs, const int* __restrict__ e_vtx,
-                                   const double* __restrict__ e_near, double near_region, double& wG, double& wGn) {
+// All three vertex weights of element s for target t at once (the kernel evaluations at the
+// quadrature points are shared).  Adjacent element (target is a vertex): rotated so the
+// target is vertex 0, Duffy-collapsed 5x5 Gauss rule, and the Gn weight of the element's first
+// vertex dropped (rigid-mode diagonal); near element (centroid within near_region): 5x5 rule;
+// otherwise the Dunavant 6-point rule (fill_direct_linear / fill_nonadj_linear,
+// BEM_solveBVP_GMRES_FMM.hpp:1824-1891).
+__device__ void elem_weights3(int s, int t, const double* __restrict__ Xs, const int* __restrict__ e_vtx,
+                              const double* __restrict__ e_near, double near_region, double wG[3], double wGn[3]) {
   const int v[3] = {e_vtx[3 * s], e_vtx[3 * s + 1], e_vtx[3 * s + 2]};
   const double J = e_near[8 * s];
   const double crx = e_near[8 * s + 1], cry = e_near[8 * s + 2], crz = e_near[8 * s + 3];
   const double xt = Xs[3 * t], yt = Xs[3 * t + 1], zt = Xs[3 * t + 2];
-  double G = 0.0, Gn = 0.0;
+  double G[3] = {0.0, 0.0, 0.0}, Gn[3] = {0.0, 0.0, 0.0};
   if (v[0] == t || v[1] == t || v[2] == t) {
-    // fill_direct_linear: rotate so the target is vertex 0; Duffy-collapsed 5x5 rule;
-    // the Gn weight of the element's first vertex is dropped (rigid-mode diagonal)
-    int o = (v[0] == t) ? 0 : (v[1] == t ? 1 : 2);
+    const int o = (v[0] == t) ? 0 : (v[1] == t ? 1 : 2);
     const int r0 = v[o], r1 = v[(o + 1) % 3], r2 = v[(o + 2) % 3];
-    const int ia = (a - o + 3) % 3;  // rotated position of original vertex a
     const double X0[3] = {Xs[3 * r0], Xs[3 * r0 + 1], Xs[3 * r0 + 2]};
     const double X1[3] = {Xs[3 * r1], Xs[3 * r1 + 1], Xs[3 * r1 + 2]};
     const double X2[3] = {Xs[3 * r2], Xs[3 * r2 + 1], Xs[3 * r2 + 2]};
@@ -750,81 +752,157 @@ __device__ void elem_vertex_weight(int s, int a, int t, const double* __restrict
       const double Ry = N[0] * X0[1] + N[1] * X1[1] + N[2] * X2[1] - yt;
       const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
       const double nr_inv = rsqrt(Rx * Rx + Ry * Ry + Rz * Rz);
-      const double tmp = ww * (1. - t0) * nr_inv * N[ia];
-      G += J * tmp;
-      Gn += -((Rx * crx + Ry * cry + Rz * crz) * nr_inv) * tmp * nr_inv;
+      const double base = ww * (1. - t0) * nr_inv;
+      const double dn = -((Rx * crx + Ry * cry + Rz * crz) * nr_inv);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const double tmp = base * N[(a - o + 3) % 3];
+        G[a] += J * tmp;
+        Gn[a] += dn * tmp * nr_inv;
+      }
     }
-    wG = G;
-    wGn = (a == 0) ? 0.0 : Gn;
-    return;
-  }
-  const double X0[3] = {Xs[3 * v[0]], Xs[3 * v[0] + 1], Xs[3 * v[0] + 2]};
-  const double X1[3] = {Xs[3 * v[1]], Xs[3 * v[1] + 1], Xs[3 * v[1] + 2]};
-  const double X2[3] = {Xs[3 * v[2]], Xs[3 * v[2] + 1], Xs[3 * v[2] + 2]};
-  const double dcx = e_near[8 * s + 4] - xt, dcy = e_near[8 * s + 5] - yt, dcz = e_near[8 * s + 6] - zt;
-  if (dnorm3(dcx, dcy, dcz) < near_region) {  // fill_nonadj_linear, near element: 5x5 rule
-    for (int g = 0; g < 25; ++g) {
-      const double t0 = c_gw[g][0], t1 = c_gw[g][1], ww = c_gw[g][2];
-      const double N[3] = {t0, t1 * (1. - t0), (t0 - 1.) * (t1 - 1.)};
-      const double Rx = N[0] * X0[0] + N[1] * X1[0] + N[2] * X2[0] - xt;
-      const double Ry = N[0] * X0[1] + N[1] * X1[1] + N[2] * X2[1] - yt;
-      const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
-      const double nr_inv = rsqrt(Rx * Rx + Ry * Ry + Rz * Rz);
-      const double tmp = ww * (1. - t0) * N[a] * nr_inv;
-      G += J * tmp;
-      Gn -= ((Rx * crx + Ry * cry + Rz * crz) * nr_inv) * (tmp * nr_inv);
-    }
-  } else {  // Dunavant 6-point rule
-    for (int q = 0; q < 6; ++q) {
-      const double N[3] = {c_dv[q][0], c_dv[q][1], c_dv[q][2]};
-      const double Rx = N[0] * X0[0] + N[1] * X1[0] + N[2] * X2[0] - xt;
-      const double Ry = N[0] * X0[1] + N[1] * X1[1] + N[2] * X2[1] - yt;
-      const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
-      const double nr_inv = rsqrt(Rx * Rx + Ry * Ry + Rz * Rz);
-      const double tmp = c_dv[q][3] * N[a] * nr_inv;
-      G += J * tmp;
-      Gn -= ((Rx * crx + Ry * cry + Rz * crz) * nr_inv) * (tmp * nr_inv);
-    }
-  }
-  wG = G;
-  wGn = Gn;
-}
-
-__global__ void k_near_weights(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs, const int* __restrict__ nb_targets,
-                               const int* __restrict__ nb_ranges, const int* __restrict__ dof_inc_off, const int* __restrict__ dof_inc,
-                               const double* __restrict__ Xs, const int* __restrict__ e_vtx, const double* __restrict__ e_near,
-                               double near_region, double* __restrict__ WG, double* __restrict__ WGn) {
-  const NearBlockDev B = blocks[blockIdx.x];
-  const int64_t total = (int64_t)B.ntgt * B.ndof;
-  const int* rng = nb_ranges + 2 * B.rng_off;
-  for (int64_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int tl = (int)(idx / B.ndof), j = (int)(idx % B.ndof);
-    const int dof = nb_dofs[B.dof_off + j];
-    const int t = nb_targets[B.tgt_off + tl];
-    double G = 0.0, Gn = 0.0;
-    for (int k = dof_inc_off[dof]; k < dof_inc_off[dof + 1]; ++k) {
-      const int s = dof_inc[k] / 3, a = dof_inc[k] % 3;
-      // s in one of the sorted half-open ranges?
-      int lo = 0, hi = B.nrng - 1, hit = 0;
-      while (lo <= hi) {
-        const int mid = (lo + hi) >> 1;
-        if (s < rng[2 * mid])
-          hi = mid - 1;
-        else if (s >= rng[2 * mid + 1])
-          lo = mid + 1;
-        else {
-          hit = 1;
-          break;
+    Gn[0] = 0.0;  // the element's first vertex: dropped (rigid-mode diagonal)
+  } else {
+    const double X0[3] = {Xs[3 * v[0]], Xs[3 * v[0] + 1], Xs[3 * v[0] + 2]};
+    const double X1[3] = {Xs[3 * v[1]], Xs[3 * v[1] + 1], Xs[3 * v[1] + 2]};
+    const double X2[3] = {Xs[3 * v[2]], Xs[3 * v[2] + 1], Xs[3 * v[2] + 2]};
+    const double dcx = e_near[8 * s + 4] - xt, dcy = e_near[8 * s + 5] - yt, dcz = e_near[8 * s + 6] - zt;
+    if (dnorm3(dcx, dcy, dcz) < near_region) {
+      for (int g = 0; g < 25; ++g) {
+        const double t0 = c_gw[g][0], t1 = c_gw[g][1], ww = c_gw[g][2];
+        const double N[3] = {t0, t1 * (1. - t0), (t0 - 1.) * (t1 - 1.)};
+        const double Rx = N[0] * X0[0] + N[1] * X1[0] + N[2] * X2[0] - xt;
+        const double Ry = N[0] * X0[1] + N[1] * X1[1] + N[2] * X2[1] - yt;
+        const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
+        const double nr_inv = rsqrt(Rx * Rx + Ry * Ry + Rz * Rz);
+        const double wt = ww * (1. - t0);
+        const double dn = (Rx * crx + Ry * cry + Rz * crz) * nr_inv;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const double tmp = wt * N[a] * nr_inv;
+          G[a] += J * tmp;
+          Gn[a] -= dn * (tmp * nr_inv);
         }
       }
-      if (!hit) continue;
-      double g, gn;
-      elem_vertex_weight(s, a, t, Xs, e_vtx, e_near, near_region, g, gn);
-      G += g;
-      Gn += gn;
+    } else {
+      for (int q = 0; q < 6; ++q) {
+        const double N[3] = {c_dv[q][0], c_dv[q][1], c_dv[q][2]};
+        const double Rx = N[0] * X0[0] + N[1] * X1[0] + N[2] * X2[0] - xt;
+        const double Ry = N[0] * X0[1] + N[1] * X1[1] + N[2] * X2[1] - yt;
+        const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
+        const double nr_inv = rsqrt(Rx * Rx + Ry * Ry + Rz * Rz);
+        const double dn = (Rx * crx + Ry * cry + Rz * crz) * nr_inv;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const double tmp = c_dv[q][3] * N[a] * nr_inv;
+          G[a] += J * tmp;
+          Gn[a] -= dn * (tmp * nr_inv);
+        }
+      }
     }
-    WG[B.w_off + idx] = G;
-    WGn[B.w_off + idx] = Gn;
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    wG[a] = G[a];
+    wGn[a] = Gn[a];
+  }
+}
+
+// Near-field weights, one block per target: the block's near elements are taken in chunks;
+// each element is integrated once for its three vertices into shared memory, then every
+// thread adds, for the DOF columns it owns, the vertices of the chunk's incident elements
+// (in the DOF's incidence order, chunk after chunk) to register accumulators.  The quadrature
+// work is one evaluation per (target, element) instead of one per (target, DOF, element).
+constexpr int kNearChunk = 1024;  // elements per chunk: 1024 x 3 x (G, Gn) doubles = 48 KB
+constexpr int kNearThreads = 256;
+constexpr int kNearCols = 8;      // DOF columns per thread per pass: 2048 per pass
+
+__global__ void __launch_bounds__(kNearThreads) k_near_weights(const NearBlockDev* __restrict__ blocks, const int* __restrict__ slot_block,
+                                                              const int* __restrict__ nb_dofs, const int* __restrict__ nb_targets,
+                                                              const int* __restrict__ nb_ranges, const int* __restrict__ dof_inc_off,
+                                                              const int* __restrict__ dof_inc, const double* __restrict__ Xs,
+                                                              const int* __restrict__ e_vtx, const double* __restrict__ e_near,
+                                                              double near_region, double* __restrict__ WG, double* __restrict__ WGn) {
+  extern __shared__ double2 sE[];  // [kNearChunk][3] (G, Gn), then the range prefix [nrng + 1]
+  int* sR = reinterpret_cast<int*>(sE + 3 * kNearChunk);
+  const int slot = blockIdx.x;
+  const NearBlockDev B = blocks[slot_block[slot]];
+  const int tl = slot - B.tgt_off;
+  const int t = nb_targets[slot];
+  const int* rng = nb_ranges + 2 * B.rng_off;
+  const int nrng = B.nrng;
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int r = 0; r < nrng; ++r) {
+      sR[r] = acc;
+      acc += rng[2 * r + 1] - rng[2 * r];
+    }
+    sR[nrng] = acc;
+  }
+  __syncthreads();
+  const int nel = sR[nrng];
+  for (int j0 = 0; j0 < B.ndof; j0 += kNearThreads * kNearCols) {
+    double aG[kNearCols], aGn[kNearCols];
+#pragma unroll
+    for (int q = 0; q < kNearCols; ++q) aG[q] = aGn[q] = 0.0;
+    for (int e0 = 0; e0 < nel; e0 += kNearChunk) {
+      const int ec = min(kNearChunk, nel - e0);
+      __syncthreads();
+      for (int le = threadIdx.x; le < ec; le += blockDim.x) {
+        const int li = e0 + le;
+        int lo = 0, hi = nrng - 1;  // the range r with sR[r] <= li < sR[r + 1]
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (sR[mid] <= li)
+            lo = mid;
+          else
+            hi = mid - 1;
+        }
+        const int r = lo;
+        const int s = rng[2 * r] + (li - sR[r]);
+        double g[3], gn[3];
+        elem_weights3(s, t, Xs, e_vtx, e_near, near_region, g, gn);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) sE[3 * le + a] = make_double2(g[a], gn[a]);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < kNearCols; ++q) {
+        const int j = j0 + threadIdx.x + q * kNearThreads;
+        if (j < B.ndof) {
+          const int dof = nb_dofs[B.dof_off + j];
+          for (int k = dof_inc_off[dof]; k < dof_inc_off[dof + 1]; ++k) {
+            const int s = dof_inc[k] / 3, a = dof_inc[k] % 3;
+            // local index of s among the block's near elements (sorted half-open ranges)
+            int lo = 0, hi = nrng - 1, li = -1;
+            while (lo <= hi) {
+              const int mid = (lo + hi) >> 1;
+              if (s < rng[2 * mid])
+                hi = mid - 1;
+              else if (s >= rng[2 * mid + 1])
+                lo = mid + 1;
+              else {
+                li = sR[mid] + (s - rng[2 * mid]);
+                break;
+              }
+            }
+            if (li >= e0 && li < e0 + ec) {
+              const double2 w = sE[3 * (li - e0) + a];
+              aG[q] += w.x;
+              aGn[q] += w.y;
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kNearCols; ++q) {
+      const int j = j0 + threadIdx.x + q * kNearThreads;
+      if (j < B.ndof) {
+        WG[B.w_off + (int64_t)tl * B.ndof + j] = aG[q];
+        WGn[B.w_off + (int64_t)tl * B.ndof + j] = aGn[q];
+      }
+    }
   }
 }
 
@@ -1128,9 +1206,12 @@ void launch_densities(int n, int mode, const double* x, const double* known, con
 }
 
 void launch_near_weights(const NearArgs& a, cudaStream_t st) {
-  if (a.n_blocks > 0)
-    k_near_weights<<<a.n_blocks, 256, 0, st>>>(a.blocks, a.nb_dofs, a.nb_targets, a.nb_ranges, a.dof_inc_off, a.dof_inc, a.Xs, a.e_vtx,
-                                                a.e_near, a.near_region, a.WG, a.WGn);
+  const size_t shm = sizeof(double2) * 3 * kNearChunk + sizeof(int) * (size_t)(a.max_nrng + 1);
+  cudaFuncSetAttribute(k_near_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  if (a.n_slots > 0)
+    k_near_weights<<<a.n_slots, kNearThreads, shm, st>>>(
+        a.blocks, a.slot_block, a.nb_dofs, a.nb_targets, a.nb_ranges, a.dof_inc_off, a.dof_inc, a.Xs, a.e_vtx, a.e_near, a.near_region,
+        a.WG, a.WGn);
 }
 
 void launch_diag(int n, const int* dof_point, const double* GnPhi, double* diag, cudaStream_t st) {

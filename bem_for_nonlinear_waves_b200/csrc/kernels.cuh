@@ -93,6 +93,9 @@ struct MatvecArgs {
 
 struct NearArgs {
   int n_blocks = 0;
+  int n_slots = 0;                  // targets over all blocks (rows of the weight arrays)
+  const int* slot_block = nullptr;  // [n_slots] block of each target slot
+  int max_nrng = 0;                 // most element ranges of one block
   const NearBlockDev* blocks = nullptr;
   const int* nb_dofs = nullptr;
   const int* nb_targets = nullptr;
