@@ -96,6 +96,7 @@ struct bem_gpu_ctx {
   DBuf<float> Wc32;  // combined near weights of A.x in FP32 (mixed precision)
   DBuf<int> leaf_dof_off, leaf_dof, e_slot, slot_block;  // P2M operator of A.x: DOFs per leaf
   DBuf<double2> p2m_C;                       // [(leaf, DOF)][NC]
+  DBuf<double2> near_scratch;                // element values of the near-weight kernel
   DBuf<int> e_dof, e_vtx, node_fb, node_fe, leaves, level_parents, child_begin, child_end, node_children;
   DBuf<int> m2l_targets, m2l_off, m2l_src, nb_dofs, nb_targets, nb_ranges, dof_inc_off, dof_inc;
   DBuf<int> point_dof_off, point_dof, dof_kind, dof_point;
@@ -617,15 +618,22 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   {
     std::vector<int> sb(P.nb_targets.size());
     int mr = 0;
+    int64_t mel = 1;
     for (int bi = 0; bi < (int)P.blocks.size(); ++bi) {
       const auto& nbk = P.blocks[bi];
       for (int tl = 0; tl < nbk.ntgt; ++tl) sb[nbk.tgt_off + tl] = bi;
       mr = std::max(mr, nbk.nrng);
+      int64_t ne = 0;
+      for (int r = 0; r < nbk.nrng; ++r) ne += P.nb_ranges[2 * (nbk.rng_off + r) + 1] - P.nb_ranges[2 * (nbk.rng_off + r)];
+      mel = std::max(mel, ne);
     }
     CK(up(ctx, ctx->slot_block, sb));
     na.n_slots = (int)sb.size();
     na.slot_block = ctx->slot_block.p;
     na.max_nrng = mr;
+    na.scratch_stride = 3 * mel;
+    CK(ctx->near_scratch.alloc((size_t)near_weights_grid() * na.scratch_stride));
+    na.scratch = ctx->near_scratch.p;
   }
   {
     MatvecArgs pa = ctx->args(nullptr, nullptr, nullptr, nullptr, nullptr);

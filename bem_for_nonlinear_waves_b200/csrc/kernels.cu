@@ -808,101 +808,90 @@ __device__ void elem_weights3(int s, int t, const double* __restrict__ Xs, const
   }
 }
 
-// Near-field weights, one block per target: the block's near elements are taken in chunks;
-// each element is integrated once for its three vertices into shared memory, then every
-// thread adds, for the DOF columns it owns, the vertices of the chunk's incident elements
-// (in the DOF's incidence order, chunk after chunk) to register accumulators.  The quadrature
-// work is one evaluation per (target, element) instead of one per (target, DOF, element).
-constexpr int kNearChunk = 1024;  // elements per chunk: 1024 x 3 x (G, Gn) doubles = 48 KB
+// Near-field weights.  Persistent CTAs walk the targets; for each target the CTA integrates
+// every near element of its block once for its three vertices into a per-CTA scratch row in
+// global memory (L2-resident), then each thread sums, for the DOF columns it owns, the
+// vertices of the DOF's incident elements in incidence order.  The block's element ranges
+// and their prefix sums sit in shared memory.  The quadrature work is one evaluation per
+// (target, element) instead of one per (target, DOF, element).
 constexpr int kNearThreads = 256;
-constexpr int kNearCols = 8;      // DOF columns per thread per pass: 2048 per pass
 
-__global__ void __launch_bounds__(kNearThreads) k_near_weights(const NearBlockDev* __restrict__ blocks, const int* __restrict__ slot_block,
-                                                              const int* __restrict__ nb_dofs, const int* __restrict__ nb_targets,
-                                                              const int* __restrict__ nb_ranges, const int* __restrict__ dof_inc_off,
-                                                              const int* __restrict__ dof_inc, const double* __restrict__ Xs,
-                                                              const int* __restrict__ e_vtx, const double* __restrict__ e_near,
-                                                              double near_region, double* __restrict__ WG, double* __restrict__ WGn) {
-  extern __shared__ double2 sE[];  // [kNearChunk][3] (G, Gn), then the range prefix [nrng + 1]
-  int* sR = reinterpret_cast<int*>(sE + 3 * kNearChunk);
-  const int slot = blockIdx.x;
-  const NearBlockDev B = blocks[slot_block[slot]];
-  const int tl = slot - B.tgt_off;
-  const int t = nb_targets[slot];
-  const int* rng = nb_ranges + 2 * B.rng_off;
-  const int nrng = B.nrng;
-  if (threadIdx.x == 0) {
-    int acc = 0;
-    for (int r = 0; r < nrng; ++r) {
-      sR[r] = acc;
-      acc += rng[2 * r + 1] - rng[2 * r];
-    }
-    sR[nrng] = acc;
-  }
-  __syncthreads();
-  const int nel = sR[nrng];
-  for (int j0 = 0; j0 < B.ndof; j0 += kNearThreads * kNearCols) {
-    double aG[kNearCols], aGn[kNearCols];
-#pragma unroll
-    for (int q = 0; q < kNearCols; ++q) aG[q] = aGn[q] = 0.0;
-    for (int e0 = 0; e0 < nel; e0 += kNearChunk) {
-      const int ec = min(kNearChunk, nel - e0);
+__global__ void __launch_bounds__(kNearThreads) k_near_weights(int nslots, const NearBlockDev* __restrict__ blocks,
+                                                              const int* __restrict__ slot_block, const int* __restrict__ nb_dofs,
+                                                              const int* __restrict__ nb_targets, const int* __restrict__ nb_ranges,
+                                                              const int* __restrict__ dof_inc_off, const int* __restrict__ dof_inc,
+                                                              const double* __restrict__ Xs, const int* __restrict__ e_vtx,
+                                                              const double* __restrict__ e_near, double near_region, double2* __restrict__ scratch,
+                                                              int64_t scratch_stride, double* __restrict__ WG, double* __restrict__ WGn) {
+  extern __shared__ int sm_near[];  // ranges [2 nrng], prefix [nrng + 1]
+  double2* E = scratch + (int64_t)blockIdx.x * scratch_stride;  // [3 * near elements] (G, Gn)
+  int cur_block = -1, nrng = 0, nel = 0;
+  int* sRng = sm_near;
+  int* sR = nullptr;
+  for (int slot = blockIdx.x; slot < nslots; slot += gridDim.x) {
+    const int bi = slot_block[slot];
+    const NearBlockDev B = blocks[bi];
+    if (bi != cur_block) {  // stage the block's ranges
       __syncthreads();
-      for (int le = threadIdx.x; le < ec; le += blockDim.x) {
-        const int li = e0 + le;
-        int lo = 0, hi = nrng - 1;  // the range r with sR[r] <= li < sR[r + 1]
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (sR[mid] <= li)
-            lo = mid;
-          else
-            hi = mid - 1;
+      nrng = B.nrng;
+      sR = sm_near + 2 * nrng;
+      const int* rng = nb_ranges + 2 * B.rng_off;
+      for (int i = threadIdx.x; i < 2 * nrng; i += blockDim.x) sRng[i] = rng[i];
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int r = 0; r < nrng; ++r) {
+          sR[r] = acc;
+          acc += sRng[2 * r + 1] - sRng[2 * r];
         }
-        const int r = lo;
-        const int s = rng[2 * r] + (li - sR[r]);
-        double g[3], gn[3];
-        elem_weights3(s, t, Xs, e_vtx, e_near, near_region, g, gn);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) sE[3 * le + a] = make_double2(g[a], gn[a]);
+        sR[nrng] = acc;
       }
       __syncthreads();
+      nel = sR[nrng];
+      cur_block = bi;
+    }
+    const int tl = slot - B.tgt_off;
+    const int t = nb_targets[slot];
+    for (int li = threadIdx.x; li < nel; li += blockDim.x) {
+      int lo = 0, hi = nrng - 1;  // the range r with sR[r] <= li < sR[r + 1]
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sR[mid] <= li)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      const int s = sRng[2 * lo] + (li - sR[lo]);
+      double g[3], gn[3];
+      elem_weights3(s, t, Xs, e_vtx, e_near, near_region, g, gn);
 #pragma unroll
-      for (int q = 0; q < kNearCols; ++q) {
-        const int j = j0 + threadIdx.x + q * kNearThreads;
-        if (j < B.ndof) {
-          const int dof = nb_dofs[B.dof_off + j];
-          for (int k = dof_inc_off[dof]; k < dof_inc_off[dof + 1]; ++k) {
-            const int s = dof_inc[k] / 3, a = dof_inc[k] % 3;
-            // local index of s among the block's near elements (sorted half-open ranges)
-            int lo = 0, hi = nrng - 1, li = -1;
-            while (lo <= hi) {
-              const int mid = (lo + hi) >> 1;
-              if (s < rng[2 * mid])
-                hi = mid - 1;
-              else if (s >= rng[2 * mid + 1])
-                lo = mid + 1;
-              else {
-                li = sR[mid] + (s - rng[2 * mid]);
-                break;
-              }
-            }
-            if (li >= e0 && li < e0 + ec) {
-              const double2 w = sE[3 * (li - e0) + a];
-              aG[q] += w.x;
-              aGn[q] += w.y;
-            }
+      for (int a = 0; a < 3; ++a) E[3 * li + a] = make_double2(g[a], gn[a]);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < B.ndof; j += blockDim.x) {
+      const int dof = nb_dofs[B.dof_off + j];
+      double G = 0.0, Gn = 0.0;
+      for (int k = dof_inc_off[dof]; k < dof_inc_off[dof + 1]; ++k) {
+        const int s = dof_inc[k] / 3, a = dof_inc[k] % 3;
+        int lo = 0, hi = nrng - 1;  // s in one of the sorted half-open ranges?
+        while (lo <= hi) {
+          const int mid = (lo + hi) >> 1;
+          if (s < sRng[2 * mid])
+            hi = mid - 1;
+          else if (s >= sRng[2 * mid + 1])
+            lo = mid + 1;
+          else {
+            const double2 w = E[3 * (sR[mid] + (s - sRng[2 * mid])) + a];
+            G += w.x;
+            Gn += w.y;
+            break;
           }
         }
       }
+      WG[B.w_off + (int64_t)tl * B.ndof + j] = G;
+      WGn[B.w_off + (int64_t)tl * B.ndof + j] = Gn;
     }
-#pragma unroll
-    for (int q = 0; q < kNearCols; ++q) {
-      const int j = j0 + threadIdx.x + q * kNearThreads;
-      if (j < B.ndof) {
-        WG[B.w_off + (int64_t)tl * B.ndof + j] = aG[q];
-        WGn[B.w_off + (int64_t)tl * B.ndof + j] = aGn[q];
-      }
-    }
+    __syncthreads();  // E is rewritten by the next target
   }
 }
 
@@ -1205,13 +1194,14 @@ void launch_densities(int n, int mode, const double* x, const double* known, con
   k_densities<<<g > 0 ? g : 1, 256, 0, st>>>(n, mode, x, known, kind, phi, phin);
 }
 
+int near_weights_grid() { return 148 * 2; }
+
 void launch_near_weights(const NearArgs& a, cudaStream_t st) {
-  const size_t shm = sizeof(double2) * 3 * kNearChunk + sizeof(int) * (size_t)(a.max_nrng + 1);
-  cudaFuncSetAttribute(k_near_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  const size_t shm = sizeof(int) * (size_t)(3 * a.max_nrng + 1);
   if (a.n_slots > 0)
-    k_near_weights<<<a.n_slots, kNearThreads, shm, st>>>(
-        a.blocks, a.slot_block, a.nb_dofs, a.nb_targets, a.nb_ranges, a.dof_inc_off, a.dof_inc, a.Xs, a.e_vtx, a.e_near, a.near_region,
-        a.WG, a.WGn);
+    k_near_weights<<<std::min(a.n_slots, near_weights_grid()), kNearThreads, shm, st>>>(
+        a.n_slots, a.blocks, a.slot_block, a.nb_dofs, a.nb_targets, a.nb_ranges, a.dof_inc_off, a.dof_inc, a.Xs, a.e_vtx, a.e_near,
+        a.near_region, a.scratch, a.scratch_stride, a.WG, a.WGn);
 }
 
 void launch_diag(int n, const int* dof_point, const double* GnPhi, double* diag, cudaStream_t st) {

@@ -96,6 +96,8 @@ struct NearArgs {
   int n_slots = 0;                  // targets over all blocks (rows of the weight arrays)
   const int* slot_block = nullptr;  // [n_slots] block of each target slot
   int max_nrng = 0;                 // most element ranges of one block
+  double2* scratch = nullptr;       // near_weights_grid() rows of 3 x scratch_stride/3 element values
+  int64_t scratch_stride = 0;       // >= 3 x most near elements of one block
   const NearBlockDev* blocks = nullptr;
   const int* nb_dofs = nullptr;
   const int* nb_targets = nullptr;
@@ -110,6 +112,7 @@ struct NearArgs {
   double* WGn = nullptr;
 };
 
+int near_weights_grid();  // CTAs of the near-weight kernel (one scratch row each)
 void upload_quadrature(const double dv[6][4], const double gw[25][3], cudaStream_t s);
 void configure_targets_smem(int p, int bytes);
 void configure_m2l_smem(int p);
