@@ -647,8 +647,8 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   ctx->launches += ctx->opts.precision == 1 ? 2 : 1;
   CK(cudaGetLastError());
   // rigid-mode diagonal (BEM_solveBVP_GMRES_FMM.hpp:2661-2716)
-  launch_densities(N, 2, nullptr, nullptr, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, s);
-  run_fmm(ctx, nullptr, ctx->GPhin.p, ctx->GnPhi.p);
+  launch_densities(N, 2, nullptr, nullptr, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, s);  // phi = 1, phin = 0
+  run_fmm(ctx, nullptr, nullptr, ctx->GnPhi.p);
   launch_diag(N, ctx->dof_point.p, ctx->GnPhi.p, ctx->diag.p, s);
   ctx->launches += 3;
   CK(cudaGetLastError());

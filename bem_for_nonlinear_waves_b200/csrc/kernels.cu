@@ -622,9 +622,14 @@ __global__ void __launch_bounds__(128) k_targets(const NearBlockDev* __restrict_
       if (ND == 2) f1 += __shfl_xor_sync(0xffffffffu, f1, o);
     }
     const double GPhin = accs[tl].x + f0, GnPhi = accs[tl].y + f1;
-    if (GPhin_out && lane == 0) {
-      GPhin_out[p] = GPhin;
-      GnPhi_out[p] = GnPhi;
+    if (lane == 0) {
+      if (ND == 2) {
+        if (GPhin_out) GPhin_out[p] = GPhin;
+        if (GnPhi_out) GnPhi_out[p] = GnPhi;
+      } else if (GnPhi_out) {
+        // GnPhi alone from the combined expansion: valid when phin = 0 (far of M[0] - M[1] = -far of M[1])
+        GnPhi_out[p] = accs[tl].y - f0;
+      }
     }
     if (rows) {
       for (int k = point_dof_off[p] + lane; k < point_dof_off[p + 1]; k += 32) {
@@ -1107,7 +1112,7 @@ int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages) {
   switch (p) {
 #define BEMB200_CASE(PP) \
   case PP:               \
-    return (a.GPhin || a.GnPhi) ? launch_matvec_fmm<PP, 2>(a, st, stages) : launch_matvec_fmm<PP, 1>(a, st, stages);
+    return a.GPhin ? launch_matvec_fmm<PP, 2>(a, st, stages) : launch_matvec_fmm<PP, 1>(a, st, stages);
     BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5) BEMB200_CASE(6)
     BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10) BEMB200_CASE(11) BEMB200_CASE(12)
 #undef BEMB200_CASE

@@ -120,8 +120,9 @@ void launch_s_tables(int p, int ngroups, const double* gvec, double2* Sg, cudaSt
 enum { STAGE_P2M = 1, STAGE_M2M = 2, STAGE_M2L = 4, STAGE_L2L = 8, STAGE_TARGETS = 16, STAGE_ALL = 31 };
 // returns the number of kernels launched
 // One operator application; returns the number of kernel launches.  A call that asks for
-// GPhin / GnPhi carries both densities through the tree; a call for the rows alone carries
-// their difference only (half the P2M, M2M, M2L, L2L and L2P work).
+// GPhin carries both densities through the tree; any other call carries their difference
+// only (half the P2M, M2M, M2L, L2L and L2P work) -- a call for GnPhi alone must then have
+// phin = 0 (the rigid-mode diagonal).
 int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages = STAGE_ALL);
 
 // tensor-core M2L (m2l_tc.cu)
