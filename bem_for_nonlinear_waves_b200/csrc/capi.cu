@@ -83,6 +83,8 @@ double now_s() { return std::chrono::duration<double>(std::chrono::steady_clock:
 
 }  // namespace
 
+constexpr int kErrRing = 8;  // residual estimates in flight (>= the read-back lag + 1)
+
 struct bem_gpu_ctx {
   bem_gpu_opts opts{};
   cudaStream_t stream = nullptr;
@@ -129,6 +131,17 @@ struct bem_gpu_ctx {
   cudaGraph_t graph_lo = nullptr;
   cudaGraphExec_t graph_exec_lo = nullptr;
   int graph_kernels_lo = 0;
+  // device-resident Arnoldi: state, rotations, g, R; one graph per step; pinned ring of
+  // residual estimates with an event per slot
+  DBuf<ArnoldiState> arn_state;
+  DBuf<double> arn_g, arn_cs, arn_sn, arn_R, xbase;
+  cudaGraph_t arn_graph = nullptr;
+  cudaGraphExec_t arn_exec = nullptr;
+  int arn_kernels = 0;
+  const void* arn_key_V = nullptr;
+  int arn_key_cols = 0, arn_key_jacobi = -1, arn_key_mixed = -1;
+  double* arn_err_host = nullptr;
+  cudaEvent_t arn_ev[kErrRing] = {};
   // accounting of the current setup + solve
   int64_t h2d = 0, d2h = 0, launches = 0;
   int64_t setup_h2d = 0, setup_launches = 0;
@@ -145,6 +158,11 @@ struct bem_gpu_ctx {
     if (graph) cudaGraphDestroy(graph);
     if (graph_exec_lo) cudaGraphExecDestroy(graph_exec_lo);
     if (graph_lo) cudaGraphDestroy(graph_lo);
+    if (arn_exec) cudaGraphExecDestroy(arn_exec);
+    if (arn_graph) cudaGraphDestroy(arn_graph);
+    for (auto& e : arn_ev)
+      if (e) cudaEventDestroy(e);
+    if (arn_err_host) cudaFreeHost(arn_err_host);
     if (stream) cudaStreamDestroy(stream);
   }
   MatvecArgs args(const double* d_phi, const double* d_phin, double* d_rows, double* d_gphin, double* d_gnphi) const {
@@ -311,9 +329,75 @@ int capture_matvec(bem_gpu_ctx* ctx, bool tc, cudaGraph_t& graph, cudaGraphExec_
 }
 
 int build_graph(bem_gpu_ctx* ctx) {
+  ctx->arn_key_V = nullptr;  // the Arnoldi step graph holds this set-up's buffers: recapture at the next solve
   int rc = capture_matvec(ctx, false, ctx->graph, ctx->graph_exec, ctx->graph_kernels);
   if (rc != BEM_OK || !ctx->mixed) return rc;
   return capture_matvec(ctx, true, ctx->graph_lo, ctx->graph_exec_lo, ctx->graph_kernels_lo);
+}
+
+// (Re)captures the Arnoldi step graph when the basis, its capacity or the operator changed.
+int ensure_arnoldi_graph(bem_gpu_ctx* ctx, bool jacobi, bool lowp, int cols) {
+  const int N = ctx->plan.ndof;
+  if (ctx->arn_cs.n < (size_t)cols) {
+    CK(ctx->arn_state.alloc(1));
+    CK(ctx->arn_g.alloc((size_t)cols + 1));
+    CK(ctx->arn_cs.alloc(cols));
+    CK(ctx->arn_sn.alloc(cols));
+    CK(ctx->arn_R.alloc((size_t)cols * cols));
+  }
+  if (ctx->xbase.n < (size_t)N) CK(ctx->xbase.alloc(N));
+  if (!ctx->arn_err_host) {
+    CK(cudaHostAlloc((void**)&ctx->arn_err_host, sizeof(double) * kErrRing, cudaHostAllocDefault));
+    for (auto& e : ctx->arn_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  if (ctx->arn_exec && ctx->arn_key_V == ctx->V.p && ctx->arn_key_cols == cols && ctx->arn_key_jacobi == (int)jacobi &&
+      ctx->arn_key_mixed == (int)lowp)
+    return BEM_OK;
+  if (ctx->arn_exec) {
+    cudaGraphExecDestroy(ctx->arn_exec);
+    ctx->arn_exec = nullptr;
+  }
+  if (ctx->arn_graph) {
+    cudaGraphDestroy(ctx->arn_graph);
+    ctx->arn_graph = nullptr;
+  }
+  ArnoldiArgs a;
+  a.nrow = N;
+  a.cols = cols;
+  a.p = ctx->plan.opt.p;
+  a.V = ctx->V.p;
+  a.dinv = jacobi ? ctx->dinv.p : nullptr;
+  a.state = ctx->arn_state.p;
+  a.x = ctx->mv_in.p;
+  a.w = ctx->mv_out.p;
+  a.mv = ctx->args(ctx->phi.p, ctx->phin.p, ctx->mv_out.p, nullptr, nullptr);
+  ctx->set_ax(a.mv, lowp);
+  if (lowp) ctx->set_tc(a.mv);
+  a.h = ctx->hdev.p;
+  a.partial = ctx->partial.p;
+  a.cs = ctx->arn_cs.p;
+  a.sn = ctx->arn_sn.p;
+  a.g = ctx->arn_g.p;
+  a.R = ctx->arn_R.p;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  launch_arnoldi_step(a, ctx->stream);
+  CK(cudaStreamEndCapture(ctx->stream, &ctx->arn_graph));
+  CK(cudaGraphInstantiate(&ctx->arn_exec, ctx->arn_graph, 0));
+  size_t nn = 0;
+  CK(cudaGraphGetNodes(ctx->arn_graph, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (nn) CK(cudaGraphGetNodes(ctx->arn_graph, nodes.data(), &nn));
+  ctx->arn_kernels = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType ty;
+    CK(cudaGraphNodeGetType(nd, &ty));
+    if (ty == cudaGraphNodeTypeKernel) ++ctx->arn_kernels;
+  }
+  ctx->arn_key_V = ctx->V.p;
+  ctx->arn_key_cols = cols;
+  ctx->arn_key_jacobi = (int)jacobi;
+  ctx->arn_key_mixed = (int)lowp;
+  return BEM_OK;
 }
 
 // y = A_lo x on device buffers (tensor-core M2L), on the context's stream
@@ -659,11 +743,12 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
       bop[p] = std::max(P.block_of_point[p], 0);
       rop[p] = std::max(P.row_of_point[p], 0);
     }
-    DBuf<int> d_bop, d_rop;
+    DBuf<int> d_bop, d_rop, d_self;
     CK(up(ctx, d_bop, bop));
     CK(up(ctx, d_rop, rop));
+    CK(up(ctx, d_self, P.self_col));
     CK(ctx->dinv.alloc(N));
-    launch_jacobi(N, ctx->dof_point.p, ctx->dof_kind.p, ctx->diag.p, d_bop.p, d_rop.p, ctx->blocks.p, ctx->nb_dofs.p, ctx->WG.p, ctx->WGn.p,
+    launch_jacobi(N, ctx->dof_point.p, ctx->dof_kind.p, ctx->diag.p, d_bop.p, d_rop.p, ctx->blocks.p, d_self.p, ctx->WG.p, ctx->WGn.p,
                   ctx->dinv.p, s);
     ctx->launches += 1;
     CK(cudaGetLastError());
@@ -756,11 +841,20 @@ int bem_gpu_near_row(bem_gpu_ctx* ctx, int32_t point, int32_t cap, int32_t* dof,
   const int n = std::min(cap, b.ndof);
   if (n > 0) {
     if (!dof || !wG || !wGn) return BEM_ERR_INVALID_ARGUMENT;
-    std::memcpy(dof, &P.nb_dofs[b.dof_off], sizeof(int32_t) * n);
+    // the row in ascending DOF order (the block keeps its DOFs in first-appearance order)
     const int64_t off = b.w_off + (int64_t)P.row_of_point[point] * b.ndof;
-    CK(cudaMemcpyAsync(wG, ctx->WG.p + off, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(wGn, ctx->WGn.p + off, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<double> g(b.ndof), gn(b.ndof);
+    CK(cudaMemcpyAsync(g.data(), ctx->WG.p + off, sizeof(double) * b.ndof, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(gn.data(), ctx->WGn.p + off, sizeof(double) * b.ndof, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<int> ord(b.ndof);
+    for (int j = 0; j < b.ndof; ++j) ord[j] = j;
+    std::sort(ord.begin(), ord.end(), [&](int x, int y) { return P.nb_dofs[b.dof_off + x] < P.nb_dofs[b.dof_off + y]; });
+    for (int j = 0; j < n; ++j) {
+      dof[j] = P.nb_dofs[b.dof_off + ord[j]];
+      wG[j] = g[ord[j]];
+      wGn[j] = gn[ord[j]];
+    }
   }
   return b.ndof;
 }
@@ -892,7 +986,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   }
   CK(ctx->hdev.alloc((size_t)3 * cols + 8));
   CK(ctx->ydev.alloc(cols));
-  CK(ctx->partial.alloc((size_t)mdot_blocks(N) * cols));
+  CK(ctx->partial.alloc((size_t)std::max(mdot_blocks(N), arnoldi_dot_blocks(N)) * cols));
   int matvecs = 0;
   // b = -(A*0 - b) with corner rows replaced by the point's phi (:2025-2047)
   launch_densities(N, 1, nullptr, ctx->known_s.p, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, s);
@@ -925,22 +1019,8 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     ctx->launches += ctx->graph_kernels;
     return bem_gpu_matvec_device(ctx, din, dout);
   };
-  // the Krylov operator: FP64, or the tensor-core M2L one in mixed precision
   const bool mixed = ctx->mixed;
   int matvecs_lo = 0;
-  auto kmatvec = [&](const double* din, double* dout) -> int {
-    if (!mixed) return matvec(din, dout);
-    ++matvecs_lo;
-    ctx->launches += ctx->graph_kernels_lo;
-    return matvec_lo(ctx, din, dout);
-  };
-  // operator seen by GMRES: A D^{-1} with right Jacobi scaling, else A
-  auto opmatvec = [&](const double* din, double* dout) -> int {
-    if (!jacobi) return kmatvec(din, dout);
-    launch_mul(N, ctx->dinv.p, din, ctx->tmp.p, s);
-    ctx->launches += 1;
-    return kmatvec(ctx->tmp.p, dout);
-  };
   // Mixed precision is iterative refinement: each GMRES cycle solves A_lo d = r to
   // max(tol, kInnerRtol |r|) and the cycle ends with the FP64 true residual, from which the
   // next cycle starts (that residual is reused, not recomputed).
@@ -957,9 +1037,32 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   };
   int iters = 0, rc = BEM_OK;
   double r_true = 1e300, err = 1e300;
-  std::vector<double> hh(2 * cols + 2);
+  // Arnoldi steps run as one graph each (operator + orthogonalisation + Givens update, all
+  // state on the device); the host reads each step's residual estimate kLag steps behind.
+  if ((rc = ensure_arnoldi_graph(ctx, jacobi, mixed, cols)) != BEM_OK) return rc;
+  constexpr int kLag = 3;
+  auto x_update = [&]() -> int {  // x = x_base + (D^{-1}) V R^{-1} g over the cycle's steps
+    CK(cudaMemcpyAsync(ctx->xdev.p, ctx->xbase.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    launch_arnoldi_solve_y(ctx->arn_state.p, ctx->arn_R.p, cols, ctx->arn_g.p, ctx->ydev.p, s);
+    if (!jacobi) {
+      launch_arnoldi_update(ctx->V.p, N, cols, ctx->arn_state.p, ctx->ydev.p, ctx->xdev.p, s);
+      ctx->launches += 2;
+    } else {
+      CK(cudaMemsetAsync(ctx->tmp.p, 0, sizeof(double) * N, s));
+      launch_arnoldi_update(ctx->V.p, N, cols, ctx->arn_state.p, ctx->ydev.p, ctx->tmp.p, s);
+      launch_add_mul(N, ctx->xdev.p, ctx->dinv.p, ctx->tmp.p, ctx->xdev.p, s);
+      ctx->launches += 3;
+    }
+    return BEM_OK;
+  };
+  auto true_res = [&](double* out) -> int {
+    int r;
+    if ((r = matvec(ctx->xdev.p, ctx->rdev.p)) != BEM_OK) return r;
+    launch_axpby(N, -1.0, ctx->bdev.p, 1.0, ctx->rdev.p, s);
+    ctx->launches += 1;
+    return norm_of(ctx->rdev.p, out);
+  };
   while (iters < max_iter && r_true > tol) {
-    const int k_cycle_max = std::min(100, max_iter - iters);
     double beta = 0.0;
     if (have_res) {  // rdev = A x - b from the true-residual check that ended the last cycle
       launch_axpby(N, 0.0, ctx->bdev.p, -1.0, ctx->rdev.p, s);
@@ -983,116 +1086,48 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
       break;
     }
     launch_axpby(N, 1.0 / beta, ctx->rdev.p, 0.0, ctx->V.p, s);
-    ctx->launches += 1;
-    std::vector<double> cs, sn, g{beta};
-    std::vector<std::vector<double>> Rc;
-    int n = 0;  // basis vectors beyond V[0] added in this cycle
-    auto add_basis = [&]() -> int {
-      double* vk = ctx->V.p + (size_t)n * N;
-      double* vn = ctx->V.p + (size_t)(n + 1) * N;
-      int r;
-      if ((r = opmatvec(vk, ctx->w.p)) != BEM_OK) return r;
-      const int k = n + 1;
-      double* h1 = ctx->hdev.p;
-      double* h2 = ctx->hdev.p + cols;
-      double* hn = ctx->hdev.p + 2 * cols;
-      launch_mdot(ctx->V.p, N, k, ctx->w.p, N, ctx->partial.p, h1, s);
-      launch_maxpy(ctx->V.p, N, k, h1, ctx->w.p, N, s);
-      launch_mdot(ctx->V.p, N, k, ctx->w.p, N, ctx->partial.p, h2, s);
-      launch_maxpy(ctx->V.p, N, k, h2, ctx->w.p, N, s);
-      launch_mdot(ctx->w.p, N, 1, ctx->w.p, N, ctx->partial.p, hn, s);
-      CK(cudaMemcpyAsync(hh.data(), h1, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpyAsync(hh.data() + cols, h2, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
-      double hn2 = 0.0;
-      CK(cudaMemcpyAsync(&hn2, hn, sizeof(double), cudaMemcpyDeviceToHost, s));
+    launch_arnoldi_init(ctx->arn_state.p, ctx->arn_g.p, beta, s);
+    // x_base: the iterate this cycle's corrections start from
+    CK(cudaMemcpyAsync(ctx->xbase.p, ctx->xdev.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    ctx->launches += 2;
+    const int cycle_cap = std::min(cols - 2, max_iter - iters);  // steps this cycle may take
+    const double check_at = mixed ? std::max(tol, kInnerRtol * beta) : tol * 10.;
+    int launched = 0, done = 0, sat = 0;
+    auto launch_step = [&]() -> int {
+      CK(cudaGraphLaunch(ctx->arn_exec, s));
+      const int slot = launched % kErrRing;
+      CK(cudaMemcpyAsync(ctx->arn_err_host + slot, &ctx->arn_state.p->err, sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaEventRecord(ctx->arn_ev[slot], s));
+      ctx->launches += ctx->arn_kernels;
+      ctx->d2h += 8;
+      ++launched;
+      if (mixed)
+        ++matvecs_lo;
+      else
+        ++matvecs;
+      return BEM_OK;
+    };
+    auto drain = [&]() -> int {  // all launched steps finished; err of the last one
       CK(cudaStreamSynchronize(s));
-      ctx->launches += 8;
-      ctx->d2h += 8LL * (2 * k + 1);
-      std::vector<double> hcol(k + 1);
-      for (int i = 0; i < k; ++i) hcol[i] = hh[i] + hh[cols + i];
-      hcol[k] = std::sqrt(hn2);
-      if (!std::isfinite(hcol[k])) {
+      err = ctx->arn_err_host[(launched - 1) % kErrRing];
+      iters += launched - done;
+      done = launched;
+      return BEM_OK;
+    };
+    while (true) {
+      while (launched - done < kLag && launched < cycle_cap)
+        if ((rc = launch_step()) != BEM_OK) return rc;
+      CK(cudaEventSynchronize(ctx->arn_ev[done % kErrRing]));
+      err = ctx->arn_err_host[done % kErrRing];
+      ++done;
+      ++iters;
+      if (!std::isfinite(err)) {
         ctx->err = "non-finite Arnoldi vector";
         return BEM_ERR_NAN;
       }
-      launch_axpby(N, hcol[k] > 0 ? 1.0 / hcol[k] : 0.0, ctx->w.p, 0.0, vn, s);
-      ctx->launches += 1;
-      for (int i = 0; i < k - 1; ++i) {
-        const double t = std::fma(cs[i], hcol[i], sn[i] * hcol[i + 1]);
-        hcol[i + 1] = std::fma(cs[i], hcol[i + 1], -sn[i] * hcol[i]);
-        hcol[i] = t;
-      }
-      const double a = hcol[k - 1], bb = hcol[k];
-      const double rr = std::hypot(a, bb);
-      double c = 1.0, sv = 0.0;
-      if (rr != 0.0) {
-        c = a / rr;
-        sv = bb / rr;
-      }
-      cs.push_back(c);
-      sn.push_back(sv);
-      {
-        const double t = std::fma(c, hcol[k - 1], sv * hcol[k]);
-        hcol[k] = std::fma(c, hcol[k], -sv * hcol[k - 1]);
-        hcol[k - 1] = t;
-      }
-      g.push_back(0.0);
-      {
-        const double t = std::fma(c, g[k - 1], sv * g[k]);
-        g[k] = std::fma(c, g[k], -sv * g[k - 1]);
-        g[k - 1] = t;
-      }
-      Rc.push_back(hcol);
-      err = std::abs(g.back());
-      ++n;
-      return BEM_OK;
-    };
-    auto update_x = [&]() -> int {
-      const int k = (int)Rc.size();
-      std::vector<double> y(k, 0.0);
-      for (int i = k - 1; i >= 0; --i) {
-        double sum = g[i];
-        for (int j = i + 1; j < k; ++j) sum -= Rc[j][i] * y[j];
-        y[i] = sum / Rc[i][i];
-      }
-      for (auto& v : y) v = -v;  // maxpy subtracts
-      CK(cudaMemcpyAsync(ctx->ydev.p, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
-      ctx->h2d += 8LL * k;
-      if (!jacobi) {
-        launch_maxpy(ctx->V.p, N, k, ctx->ydev.p, ctx->xdev.p, N, s);
-        ctx->launches += 1;
-      } else {  // x = x_base + D^{-1} (V y)
-        CK(cudaMemsetAsync(ctx->tmp.p, 0, sizeof(double) * N, s));
-        launch_maxpy(ctx->V.p, N, k, ctx->ydev.p, ctx->tmp.p, N, s);
-        launch_add_mul(N, ctx->xdev.p, ctx->dinv.p, ctx->tmp.p, ctx->xdev.p, s);
-        ctx->launches += 2;
-      }
-      return BEM_OK;
-    };
-    auto true_res = [&](double* out) -> int {
-      int r;
-      if ((r = matvec(ctx->xdev.p, ctx->rdev.p)) != BEM_OK) return r;
-      launch_axpby(N, -1.0, ctx->bdev.p, 1.0, ctx->rdev.p, s);
-      ctx->launches += 1;
-      return norm_of(ctx->rdev.p, out);
-    };
-    // x_base is committed into xdev only when the solution is updated; keep a copy
-    DBuf<double> xb;
-    CK(xb.alloc(N));
-    CK(cudaMemcpyAsync(xb.p, ctx->xdev.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
-    auto update_from_base = [&]() -> int {
-      CK(cudaMemcpyAsync(ctx->xdev.p, xb.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
-      return update_x();
-    };
-    if ((rc = add_basis()) != BEM_OK) return rc;
-    iters += 1;
-    int sat = 0;
-    const double check_at = mixed ? std::max(tol, kInnerRtol * beta) : tol * 10.;
-    while (true) {
-      if ((rc = add_basis()) != BEM_OK) return rc;
-      ++iters;
-      if (err <= check_at) {
-        if ((rc = update_from_base()) != BEM_OK) return rc;
+      if (done > 1 && err <= check_at) {
+        if ((rc = drain()) != BEM_OK) return rc;
+        if ((rc = x_update()) != BEM_OK) return rc;
         if ((rc = true_res(&r_true)) != BEM_OK) return rc;
         if (r_true <= tol) break;
         if (mixed) {  // refine: next cycle from this residual
@@ -1100,17 +1135,16 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
           break;
         }
         if (sat++ >= 5) break;
+        if (launched >= cycle_cap) break;
+        continue;
       }
-      if (iters >= max_iter && (int)Rc.size() >= k_cycle_max) {
-        if ((rc = update_from_base()) != BEM_OK) return rc;
+      if (done >= cycle_cap) {  // basis full or iteration cap: finish the cycle at this iterate
+        if ((rc = drain()) != BEM_OK) return rc;
+        if ((rc = x_update()) != BEM_OK) return rc;
         if (err <= tol * 10.) {
           if ((rc = true_res(&r_true)) != BEM_OK) return rc;
         } else
           r_true = err;
-        break;
-      }
-      if (n + 2 > ctx->V_cols) {  // basis full: restart from the current iterate
-        if ((rc = update_from_base()) != BEM_OK) return rc;
         break;
       }
     }

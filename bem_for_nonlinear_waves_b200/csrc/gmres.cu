@@ -1,0 +1,240 @@
+// Device-resident Arnoldi step of the GMRES driver (solveSystemGMRES,
+// bem/BEM_solveBVP_GMRES_FMM.hpp:2007-2649; ArnoldiProcess::AddBasisVector and the Givens
+// update of gmres, lib/include/basic_linear_systems.hpp:3242-3260, 3369-3433).
+//
+// One step = prepare the operator input from basis column n, apply the operator (the mat-vec
+// kernels are captured into the same graph), orthogonalise against columns 0..n by classical
+// Gram-Schmidt applied twice, normalise into column n+1, and update the QR factor of the
+// Hessenberg matrix by Givens rotations.  The step count n, the rotations, the rotated
+// right-hand side g and the triangular factor R live in device memory, so consecutive steps
+// are graph launches with no host round trip; the host reads the residual estimate |g[n]|
+// a few steps behind.  The arithmetic of the rotations is the reference's, term by term.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+
+namespace bemb200 {
+namespace {
+
+constexpr int kDotCols = 8;  // basis columns per pass of the multi-dot
+
+// partial[b][c] = sum over block b's rows of V[:, c] . w, c = 0..ncol-1 with ncol = st->n + 1
+__global__ void __launch_bounds__(256) k_mdot_dev(const double* __restrict__ V, int ldv, const ArnoldiState* __restrict__ st,
+                                                  const double* __restrict__ w, int nrow, double* __restrict__ partial, int pstride) {
+  __shared__ double red[8][kDotCols];
+  const int ncol = st->n + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c0 = 0; c0 < ncol; c0 += kDotCols) {
+    double s[kDotCols];
+#pragma unroll
+    for (int j = 0; j < kDotCols; ++j) s[j] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) {
+      const double wi = w[i];
+#pragma unroll
+      for (int j = 0; j < kDotCols; ++j)
+        if (c0 + j < ncol) s[j] = fma(V[(size_t)(c0 + j) * ldv + i], wi, s[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < kDotCols; ++j) {
+      double v = s[j];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) red[warp][j] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kDotCols && c0 + (int)threadIdx.x < ncol) {
+      double t = 0.0;
+      for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k][threadIdx.x];
+      partial[(size_t)blockIdx.x * pstride + c0 + threadIdx.x] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// out[c] = sum_b partial[b][c], block per column (columns beyond st->n are skipped)
+__global__ void k_mdot_final_dev(const double* __restrict__ partial, int nblk, int pstride, const ArnoldiState* __restrict__ st,
+                                 int self_dot, double* __restrict__ out) {
+  const int c = blockIdx.x;
+  const int ncol = self_dot ? 1 : st->n + 1;
+  if (c >= ncol) return;
+  __shared__ double red[32];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += partial[(size_t)b * pstride + c];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    out[c] = t;
+  }
+}
+
+// partial[b][0] = w . w over block b's rows
+__global__ void __launch_bounds__(256) k_selfdot(const double* __restrict__ w, int nrow, double* __restrict__ partial, int pstride) {
+  __shared__ double red[8];
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) s = fma(w[i], w[i], s);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k];
+    partial[(size_t)blockIdx.x * pstride] = t;
+  }
+}
+
+// w -= V[:, 0..n] h
+__global__ void k_maxpy_dev(const double* __restrict__ V, int ldv, const ArnoldiState* __restrict__ st, const double* __restrict__ h,
+                            double* __restrict__ w, int nrow) {
+  extern __shared__ double sh[];
+  const int ncol = st->n + 1;
+  for (int c = threadIdx.x; c < ncol; c += blockDim.x) sh[c] = h[c];
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) {
+    double s = w[i];
+    for (int c = 0; c < ncol; ++c) s = fma(-sh[c], V[(size_t)c * ldv + i], s);
+    w[i] = s;
+  }
+}
+
+// operator input: x = (dinv .*) V[:, n]
+__global__ void k_arn_prep(int nrow, const double* __restrict__ V, const double* __restrict__ dinv, const ArnoldiState* __restrict__ st,
+                           double* __restrict__ x) {
+  const double* v = V + (size_t)st->n * nrow;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) x[i] = dinv ? dinv[i] * v[i] : v[i];
+}
+
+// Hessenberg column from the two Gram-Schmidt passes, rotations, new rotation, g update,
+// R column, residual estimate; n advances by one.  Single thread (the column is short).
+__global__ void k_arn_givens(ArnoldiState* __restrict__ st, const double* __restrict__ h1, const double* __restrict__ h2,
+                             const double* __restrict__ hn, double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
+                             double* __restrict__ R, int ldr) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int n = st->n, k = n + 1;
+  double* h = R + (size_t)n * ldr;  // this step's column, rotated in place
+  for (int i = 0; i < k; ++i) h[i] = h1[i] + h2[i];
+  h[k] = sqrt(hn[0]);
+  st->inv_h = h[k] > 0.0 ? 1.0 / h[k] : 0.0;
+  if (!isfinite(h[k])) st->bad = 1;
+  for (int i = 0; i < k - 1; ++i) {
+    const double t = fma(cs[i], h[i], sn[i] * h[i + 1]);
+    h[i + 1] = fma(cs[i], h[i + 1], -sn[i] * h[i]);
+    h[i] = t;
+  }
+  const double a = h[k - 1], bb = h[k];
+  const double rr = hypot(a, bb);
+  double c = 1.0, sv = 0.0;
+  if (rr != 0.0) {
+    c = a / rr;
+    sv = bb / rr;
+  }
+  cs[k - 1] = c;
+  sn[k - 1] = sv;
+  {
+    const double t = fma(c, h[k - 1], sv * h[k]);
+    h[k] = fma(c, h[k], -sv * h[k - 1]);
+    h[k - 1] = t;
+  }
+  g[k] = 0.0;
+  {
+    const double t = fma(c, g[k - 1], sv * g[k]);
+    g[k] = fma(c, g[k], -sv * g[k - 1]);
+    g[k - 1] = t;
+  }
+  st->err = fabs(g[k]);
+  st->n = k;
+}
+
+// V[:, n] = w / h_{n,n-1} (n already advanced)
+__global__ void k_arn_normalize(int nrow, const double* __restrict__ w, const ArnoldiState* __restrict__ st, double* __restrict__ V) {
+  double* v = V + (size_t)st->n * nrow;
+  const double s = st->inv_h;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) v[i] = w[i] * s;
+}
+
+// start of a cycle: g = (beta, 0, ...), n = 0
+__global__ void k_arn_init(ArnoldiState* __restrict__ st, double* __restrict__ g, double beta) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    st->n = 0;
+    st->err = beta;
+    st->inv_h = 0.0;
+    st->bad = 0;
+    g[0] = beta;
+  }
+}
+
+// y = -R^{-1} g over the cycle's n steps (negated: the update subtracts V y)
+__global__ void k_arn_backsub(const ArnoldiState* __restrict__ st, const double* __restrict__ R, int ldr, const double* __restrict__ g,
+                              double* __restrict__ y) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int k = st->n;
+  for (int i = k - 1; i >= 0; --i) {
+    double sum = g[i];
+    for (int j = i + 1; j < k; ++j) sum -= R[(size_t)j * ldr + i] * y[j];
+    y[i] = sum / R[(size_t)i * ldr + i];
+  }
+  for (int i = 0; i < k; ++i) y[i] = -y[i];
+}
+
+// w -= V[:, 0..n-1] y over the cycle's n columns (x update from the basis)
+__global__ void k_maxpy_steps(const double* __restrict__ V, int ldv, const ArnoldiState* __restrict__ st, const double* __restrict__ y,
+                              double* __restrict__ w, int nrow) {
+  extern __shared__ double sh[];
+  const int ncol = st->n;
+  for (int c = threadIdx.x; c < ncol; c += blockDim.x) sh[c] = y[c];
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) {
+    double s = w[i];
+    for (int c = 0; c < ncol; ++c) s = fma(-sh[c], V[(size_t)c * ldv + i], s);
+    w[i] = s;
+  }
+}
+
+int grid_rows(int n) {
+  const int b = (n + 255) / 256;
+  return b < 1 ? 1 : (b > 148 * 4 ? 148 * 4 : b);
+}
+
+}  // namespace
+
+int arnoldi_dot_blocks(int n) {
+  const int b = (n + 1023) / 1024;
+  return b < 1 ? 1 : (b > 296 ? 296 : b);
+}
+
+int launch_arnoldi_step(const ArnoldiArgs& a, cudaStream_t st) {
+  const int g = grid_rows(a.nrow);
+  const int db = arnoldi_dot_blocks(a.nrow);
+  k_arn_prep<<<g, 256, 0, st>>>(a.nrow, a.V, a.dinv, a.state, a.x);
+  int launches = 1 + launch_matvec(a.p, a.mv, st);
+  double* h1 = a.h;
+  double* h2 = a.h + a.cols;
+  double* hn = a.h + 2 * a.cols;
+  for (int pass = 0; pass < 2; ++pass) {
+    double* hp = pass == 0 ? h1 : h2;
+    k_mdot_dev<<<db, 256, 0, st>>>(a.V, a.nrow, a.state, a.w, a.nrow, a.partial, a.cols);
+    k_mdot_final_dev<<<a.cols, 256, 0, st>>>(a.partial, db, a.cols, a.state, 0, hp);
+    k_maxpy_dev<<<g, 256, sizeof(double) * a.cols, st>>>(a.V, a.nrow, a.state, hp, a.w, a.nrow);
+    launches += 3;
+  }
+  k_selfdot<<<db, 256, 0, st>>>(a.w, a.nrow, a.partial, a.cols);
+  k_mdot_final_dev<<<1, 256, 0, st>>>(a.partial, db, a.cols, a.state, 1, hn);
+  k_arn_givens<<<1, 32, 0, st>>>(a.state, h1, h2, hn, a.cs, a.sn, a.g, a.R, a.cols);
+  k_arn_normalize<<<g, 256, 0, st>>>(a.nrow, a.w, a.state, a.V);
+  return launches + 4;
+}
+
+void launch_arnoldi_init(ArnoldiState* state, double* g, double beta, cudaStream_t st) { k_arn_init<<<1, 32, 0, st>>>(state, g, beta); }
+
+void launch_arnoldi_solve_y(const ArnoldiState* state, const double* R, int ldr, const double* g, double* y, cudaStream_t st) {
+  k_arn_backsub<<<1, 32, 0, st>>>(state, R, ldr, g, y);
+}
+
+void launch_arnoldi_update(const double* V, int n, int cols, const ArnoldiState* state, const double* y, double* w, cudaStream_t st) {
+  k_maxpy_steps<<<grid_rows(n), 256, sizeof(double) * cols, st>>>(V, n, state, y, w, n);
+}
+
+}  // namespace bemb200

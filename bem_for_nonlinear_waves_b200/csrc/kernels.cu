@@ -988,7 +988,7 @@ __global__ void k_add_mul(int n, const double* __restrict__ xb, const double* __
 // -(w_Gn(i,i) + diag_i); constraint rows 1.
 __global__ void k_jacobi(int n, const int* __restrict__ dof_point, const int* __restrict__ dof_kind, const double* __restrict__ diag,
                          const int* __restrict__ block_of_point, const int* __restrict__ row_of_point, const NearBlockDev* __restrict__ blocks,
-                         const int* __restrict__ nb_dofs, const double* __restrict__ WG, const double* __restrict__ WGn,
+                         const int* __restrict__ self_col, const double* __restrict__ WG, const double* __restrict__ WGn,
                          double* __restrict__ dinv) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int k = dof_kind[i];
@@ -996,19 +996,7 @@ __global__ void k_jacobi(int n, const int* __restrict__ dof_point, const int* __
     if (k != 2) {
       const int t = dof_point[i];
       const NearBlockDev B = blocks[block_of_point[t]];
-      int lo = 0, hi = B.ndof - 1, j = -1;
-      while (lo <= hi) {
-        const int mid = (lo + hi) >> 1;
-        const int v = nb_dofs[B.dof_off + mid];
-        if (v < i)
-          lo = mid + 1;
-        else if (v > i)
-          hi = mid - 1;
-        else {
-          j = mid;
-          break;
-        }
-      }
+      const int j = self_col[i];
       const int64_t w = B.w_off + (int64_t)row_of_point[t] * B.ndof + j;
       if (j >= 0) a = (k == 0) ? WG[w] : -(WGn[w] + diag[i]);
     }
@@ -1250,9 +1238,9 @@ void launch_add_mul(int n, const double* xb, const double* a, const double* u, d
 }
 
 void launch_jacobi(int n, const int* dof_point, const int* dof_kind, const double* diag, const int* block_of_point, const int* row_of_point,
-                   const NearBlockDev* blocks, const int* nb_dofs, const double* WG, const double* WGn, double* dinv, cudaStream_t st) {
+                   const NearBlockDev* blocks, const int* self_col, const double* WG, const double* WGn, double* dinv, cudaStream_t st) {
   int g = (n + 255) / 256;
-  k_jacobi<<<g > 0 ? g : 1, 256, 0, st>>>(n, dof_point, dof_kind, diag, block_of_point, row_of_point, blocks, nb_dofs, WG, WGn, dinv);
+  k_jacobi<<<g > 0 ? g : 1, 256, 0, st>>>(n, dof_point, dof_kind, diag, block_of_point, row_of_point, blocks, self_col, WG, WGn, dinv);
 }
 
 double fp64_probe_tflops(cudaStream_t st, double* sink) {

@@ -153,7 +153,35 @@ void launch_scale_inv(int n, const double* x, const double* s, double* y, cudaSt
 void launch_mul(int n, const double* a, const double* x, double* y, cudaStream_t st);
 void launch_add_mul(int n, const double* xb, const double* a, const double* u, double* y, cudaStream_t st);
 void launch_jacobi(int n, const int* dof_point, const int* dof_kind, const double* diag, const int* block_of_point, const int* row_of_point,
-                   const NearBlockDev* blocks, const int* nb_dofs, const double* WG, const double* WGn, double* dinv, cudaStream_t st);
+                   const NearBlockDev* blocks, const int* self_col, const double* WG, const double* WGn, double* dinv, cudaStream_t st);
 double fp64_probe_tflops(cudaStream_t st, double* sink);
+
+// ---- device-resident Arnoldi step (gmres.cu) ----
+struct ArnoldiState {
+  int n;         // basis vectors beyond V[:, 0] in this cycle
+  int bad;       // a non-finite Arnoldi vector was met
+  double err;    // |g[n]|: the GMRES residual estimate
+  double inv_h;  // 1 / h_{n, n-1} of the last step
+};
+struct ArnoldiArgs {
+  int nrow = 0, cols = 0, p = 0;  // unknowns, basis capacity (columns), expansion order
+  double* V = nullptr;            // [cols][nrow] basis
+  const double* dinv = nullptr;   // right Jacobi scaling or null
+  ArnoldiState* state = nullptr;
+  double* x = nullptr;            // operator input (the mat-vec's ax)
+  double* w = nullptr;            // operator output (the mat-vec's rows)
+  MatvecArgs mv;                  // the operator
+  double* h = nullptr;            // [3][cols]: the two Gram-Schmidt passes and |w|^2
+  double* partial = nullptr;      // [arnoldi_dot_blocks(nrow)][cols]
+  double* cs = nullptr;           // [cols] rotations
+  double* sn = nullptr;
+  double* g = nullptr;            // [cols + 1] rotated right-hand side
+  double* R = nullptr;            // [cols][cols] triangular factor, column j at R + j * cols
+};
+int arnoldi_dot_blocks(int nrow);
+int launch_arnoldi_step(const ArnoldiArgs& a, cudaStream_t st);  // returns kernel launches
+void launch_arnoldi_init(ArnoldiState* state, double* g, double beta, cudaStream_t st);
+void launch_arnoldi_solve_y(const ArnoldiState* state, const double* R, int ldr, const double* g, double* y, cudaStream_t st);
+void launch_arnoldi_update(const double* V, int nrow, int cols, const ArnoldiState* state, const double* y, double* w, cudaStream_t st);
 
 }  // namespace bemb200

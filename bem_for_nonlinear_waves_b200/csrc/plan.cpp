@@ -431,9 +431,41 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
       B[i].off = 0.0;
       for (int c : B[i].kids) B[i].off = std::max(B[i].off, B[c].off);
     }
-  // lists (moments.hpp:983-997)
-  for (int a : B[0].kids)
-    for (int b : B[0].kids) lists(opt, B, a, b);
+  // lists (moments.hpp:983-997).  lists(a, b) only appends to the lists of a and of a's
+  // descendants, so the traversal runs serially down to the calls whose target is at level
+  // kSplit, records those calls in order, and then runs each such target's calls (in the
+  // recorded order) in parallel: every list ends up in the serial order.
+  {
+    constexpr int kSplit = 2;
+    std::vector<std::pair<int, int>> tasks;
+    std::function<void(int, int)> top = [&](int a, int b) {
+      if (B[a].level >= kSplit) {
+        tasks.push_back({a, b});
+        return;
+      }
+      if (is_far(opt, B[a], B[b])) return;
+      if (a != b) B[a].near.push_back(b);
+      for (int ac : B[a].kids)
+        for (int bc : B[b].kids) {
+          if (ac != bc && is_far(opt, B[ac], B[bc]))
+            B[ac].m2l.push_back(bc);
+          else
+            top(ac, bc);
+        }
+    };
+    for (int a : B[0].kids)
+      for (int b : B[0].kids) top(a, b);
+    std::vector<int> torder(tasks.size());
+    std::iota(torder.begin(), torder.end(), 0);
+    std::stable_sort(torder.begin(), torder.end(), [&](int x, int y) { return tasks[x].first < tasks[y].first; });
+    std::vector<int> starts;
+    for (size_t i = 0; i < torder.size(); ++i)
+      if (i == 0 || tasks[torder[i]].first != tasks[torder[i - 1]].first) starts.push_back((int)i);
+    starts.push_back((int)torder.size());
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int g = 0; g < (int)starts.size() - 1; ++g)
+      for (int i = starts[g]; i < starts[g + 1]; ++i) lists(opt, B, tasks[torder[i]].first, tasks[torder[i]].second);
+  }
   for (auto& lv : lvl)
     for (int a : lv)
       for (int b : B[a].m2l) B[b].l2m.push_back(a);
@@ -471,6 +503,7 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   P.e_dof.resize(ne * 3);
   P.e_vtx.resize(ne * 3);
   P.e_near.resize(ne * 8);
+#pragma omp parallel for schedule(static)
   for (int s = 0; s < ne; ++s) {
     const int f = P.face_of_pos[s];
     std::memcpy(&P.e_q[s * 18], &q[f * 18], 18 * sizeof(double));
@@ -664,7 +697,6 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
             }
           }
       }
-      std::sort(dl.begin(), dl.end());
     }
   }
   // offsets first, then one parallel copy into arrays sized once
@@ -694,6 +726,16 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     std::copy(btargets[bi].begin(), btargets[bi].end(), P.nb_targets.begin() + nbk.tgt_off);
   }
   P.nnz = woff;
+  // column of each DOF in its own point's block row (the diagonal entry of the operator)
+  P.self_col.assign(ndof, -1);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int bi = 0; bi < nblk; ++bi) {
+    const Plan::NearBlock& nbk = P.blocks[bi];
+    for (int j = 0; j < nbk.ndof; ++j) {
+      const int d = P.nb_dofs[nbk.dof_off + j];
+      if (P.block_of_point[dof_point[d]] == bi) P.self_col[d] = j;
+    }
+  }
   lap(5);
   // DOF -> incident element vertices
   P.dof_inc_off.assign(ndof + 1, 0);

@@ -103,8 +103,9 @@ struct Plan {
     int rng_off, nrng;  // into nb_ranges (element ranges [a,b) in tree order, sorted)
   };
   std::vector<NearBlock> blocks;
-  std::vector<int32_t> nb_dofs, nb_targets, nb_ranges;
+  std::vector<int32_t> nb_dofs, nb_targets, nb_ranges;  // nb_dofs: per block, in first-appearance order
   std::vector<int32_t> block_of_point, row_of_point;  // [np]
+  std::vector<int32_t> self_col;  // [ndof] column of the DOF in its point's block row, -1 if none
   int64_t nnz = 0;
 
   // DOF -> incident (element position, vertex slot)
