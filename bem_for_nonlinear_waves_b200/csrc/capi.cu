@@ -105,7 +105,7 @@ struct bem_gpu_ctx {
   DBuf<NearBlockDev> blocks;
   DBuf<int> chunk_grp, chunk_begin, chunk_cnt, grp_pair;
   DBuf<double> grp_vec;
-  DBuf<double2> Sg, Mf, Y;
+  DBuf<double2> Sg, Y;
   DBuf<double2> M, L;
   std::vector<int> level_parent_off;
   int n_m2l_targets = 0, max_ntgt = 0, chunk = 0;
@@ -193,7 +193,6 @@ struct bem_gpu_ctx {
     a.chunk_cnt = chunk_cnt.p;
     a.grp_pair = grp_pair.p;
     a.Sg = Sg.p;
-    a.Mf = Mf.p;
     a.Y = Y.p;
     a.M = M.p;
     a.L = L.p;
@@ -590,7 +589,6 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     const int ngroups = (int)P.grp_off.size() - 1;
     const int Q = 2 * P.opt.p;
     CK(ctx->Sg.alloc((size_t)std::max(ngroups, 1) * (Q + 1) * (Q + 1)));
-    CK(ctx->Mf.alloc((size_t)nb * 2 * (P.opt.p + 1) * (P.opt.p + 1)));
     // per-pair slots; the tensor-core path stores tc_kp floats per pair in the same buffer
     const size_t y64 = (size_t)std::max<int64_t>(P.m2l_pairs, 1) * 2 * NC;
     const size_t ytc = ((size_t)std::max<int64_t>(P.m2l_pairs, 1) * tc_kp(P.opt.p) * sizeof(float) + sizeof(double2) - 1) / sizeof(double2);

@@ -371,10 +371,9 @@ __global__ void __launch_bounds__(32 * m2m_warps<P>()) k_m2m(const int* __restri
 // ---------------------------------------------------------------------------
 // M2L grouped by translation vector.
 //   k_s_tables    (set-up) one irregular-harmonic table S(d_g) per group, all orders
-//   k_expand_full multipoles of every bucket expanded to negative orders
 //   k_m2l_grp     block per chunk of <= 8 pairs of one group: the group's table in shared
-//                 memory is applied to the 8 source multipoles (one S load feeds 8 complex
-//                 multiply-adds per density); partial locals to slot k of each pair
+//                 memory is applied to the 8 source multipoles (one S load feeds 8 pairs);
+//                 partial locals to slot k of each pair
 //   k_m2l_reduce  per target bucket: L = sum of its slots (CSR order, deterministic)
 template <int P>
 __global__ void k_s_tables(int ngroups, const double* __restrict__ gvec, double2* __restrict__ Sg) {
@@ -383,38 +382,26 @@ __global__ void k_s_tables(int ngroups, const double* __restrict__ gvec, double2
   if (g < ngroups && threadIdx.x < 32) S_full_column<Q>(threadIdx.x, gvec[3 * g], gvec[3 * g + 1], gvec[3 * g + 2], Sg + (size_t)g * NS);
 }
 
-template <int P, int ND>
-__global__ void k_expand_full(int nnodes, const double2* __restrict__ M, double2* __restrict__ Mf) {
-  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
-  const int64_t total = (int64_t)nnodes * ND * NF;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t node = e / (ND * NF);
-    const int r = (int)(e - node * ND * NF);
-    const int d = r / NF, i = r - d * NF;
-    int n = (int)sqrtf((float)i);
-    while (n * n > i) --n;
-    while ((n + 1) * (n + 1) <= i) ++n;
-    const int m = i - n * (n + 1);
-    double2 v = M[node * 2 * NC + d * NC + cidx(n, m < 0 ? -m : m)];
-    if (m < 0) v = ((-m) & 1) ? make_double2(-v.x, v.y) : make_double2(v.x, -v.y);
-    Mf[e] = v;
-  }
-}
 
 template <int P>
 constexpr int m2l_grp_smem_bytes() {
-  return (int)sizeof(double2) * ((2 * P + 1) * (2 * P + 1) + 8 * 2 * (P + 1) * (P + 1));
+  return (int)sizeof(double2) * ((2 * P + 1) * (2 * P + 1) + 8 * 2 * ncoef(P));
 }
 
+// Thread per output coefficient L_n^m (m >= 0) of one density, applied to the chunk's <= 8
+// source multipoles in their m >= 0 half: with M^{-m'} = (-1)^{m'} conj(M^{m'}) the terms of
+// m' and -m' combine into one real 2x2 block on (Re M^{m'}, Im M^{m'}),
+//   [[Re(S+ + s S-), -Im(S+) + s Im(S-)], [Im(S+ + s S-), Re(S+ - s S-)]],
+// S+- = S_{n+n'}^{m+-m'}, s = (-1)^{m'}: 4 real multiply-adds per term and pair instead of 8.
 template <int P, int ND>
 __global__ void __launch_bounds__(((2 * ncoef(P) + 31) / 32) * 32) k_m2l_grp(const int* __restrict__ chunk_grp, const int* __restrict__ chunk_begin,
                                                                              const int* __restrict__ chunk_cnt, const int* __restrict__ grp_pair,
                                                                              const int* __restrict__ m2l_src, const double2* __restrict__ Sg,
-                                                                             const double2* __restrict__ Mf, double2* __restrict__ Y) {
-  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), Q = 2 * P, NS = (Q + 1) * (Q + 1);
+                                                                             const double2* __restrict__ M, double2* __restrict__ Y) {
+  constexpr int NC = ncoef(P), Q = 2 * P, NS = (Q + 1) * (Q + 1);
   extern __shared__ double2 smem_grp[];
   double2* sS = smem_grp;        // [NS]
-  double2* sM = smem_grp + NS;   // [8][ND][NF]
+  double2* sM = smem_grp + NS;   // [8][ND][NC] half-stored multipoles
   const int c = blockIdx.x;
   const int g = chunk_grp[c], b0 = chunk_begin[c], cnt = chunk_cnt[c];
   const int t = threadIdx.x;
@@ -422,9 +409,11 @@ __global__ void __launch_bounds__(((2 * ncoef(P) + 31) / 32) * 32) k_m2l_grp(con
     const double2* src = Sg + (size_t)g * NS;
     for (int i = t; i < NS; i += blockDim.x) sS[i] = src[i];
     for (int j = 0; j < cnt; ++j) {
-      const double2* m = Mf + (size_t)m2l_src[grp_pair[b0 + j]] * ND * NF;
-      for (int i = t; i < ND * NF; i += blockDim.x) sM[j * ND * NF + i] = m[i];
+      const double2* mp = M + (size_t)m2l_src[grp_pair[b0 + j]] * 2 * NC;
+      for (int i = t; i < ND * NC; i += blockDim.x) sM[j * ND * NC + i] = mp[i];
     }
+    for (int j = cnt; j < 8; ++j)
+      for (int i = t; i < ND * NC; i += blockDim.x) sM[j * ND * NC + i] = make_double2(0.0, 0.0);
   }
   __syncthreads();
   if (t >= ND * NC) return;
@@ -435,28 +424,30 @@ __global__ void __launch_bounds__(((2 * ncoef(P) + 31) / 32) * 32) k_m2l_grp(con
   double2 acc[8];
 #pragma unroll
   for (int j = 0; j < 8; ++j) acc[j] = make_double2(0.0, 0.0);
-  const double2* sMd = sM + dd * NF;
-  if (cnt == 8) {
-    for (int n1 = 0; n1 <= P; ++n1) {
-      const int l = n + n1;
-      const double2* Srow = sS + l * (l + 1) + m;
-      const int mb = n1 * (n1 + 1);
-      for (int m1 = -n1; m1 <= n1; ++m1) {
-        const double2 s = Srow[m1];
+  const double2* sMd = sM + dd * NC;
+  for (int n1 = 0; n1 <= P; ++n1) {
+    const int l = n + n1;
+    const double2* Srow = sS + l * (l + 1) + m;
+    const int cb = n1 * (n1 + 1) / 2;
+    {
+      const double2 s0 = Srow[0];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) cfma(acc[j], s, sMd[j * ND * NF + mb + m1]);
+      for (int j = 0; j < 8; ++j) {
+        const double a = sMd[j * ND * NC + cb].x;
+        acc[j].x = fma(s0.x, a, acc[j].x);
+        acc[j].y = fma(s0.y, a, acc[j].y);
       }
     }
-  } else {
-    for (int n1 = 0; n1 <= P; ++n1) {
-      const int l = n + n1;
-      const double2* Srow = sS + l * (l + 1) + m;
-      const int mb = n1 * (n1 + 1);
-      for (int m1 = -n1; m1 <= n1; ++m1) {
-        const double2 s = Srow[m1];
+    for (int m1 = 1; m1 <= n1; ++m1) {
+      const double2 sp = Srow[m1], sm = Srow[-m1];
+      const double sg = (m1 & 1) ? -1.0 : 1.0;
+      const double b00 = sp.x + sg * sm.x, b01 = -sp.y + sg * sm.y;
+      const double b10 = sp.y + sg * sm.y, b11 = sp.x - sg * sm.x;
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (j < cnt) cfma(acc[j], s, sMd[j * ND * NF + mb + m1]);
+      for (int j = 0; j < 8; ++j) {
+        const double2 x = sMd[j * ND * NC + cb + m1];
+        acc[j].x = fma(b00, x.x, fma(b01, x.y, acc[j].x));
+        acc[j].y = fma(b10, x.x, fma(b11, x.y, acc[j].y));
       }
     }
   }
@@ -1049,17 +1040,13 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     if (a.use_tc) {
       launches += launch_m2l_tc(P, a, st, TC_ALL, ND);
     } else if (a.n_chunks > 0) {
-      constexpr int NF = (P + 1) * (P + 1);
-      const int64_t tot = (int64_t)a.n_nodes * ND * NF;
-      int ge = (int)std::min<int64_t>((tot + 255) / 256, 148 * 16);
-      k_expand_full<P, ND><<<ge, 256, 0, st>>>(a.n_nodes, a.M, a.Mf);
       const int tpb2 = ((ND * NC + 31) / 32) * 32;
       k_m2l_grp<P, ND><<<a.n_chunks, tpb2, m2l_grp_smem_bytes<P>(), st>>>(a.chunk_grp, a.chunk_begin, a.chunk_cnt, a.grp_pair, a.m2l_src,
-                                                                        a.Sg, a.Mf, a.Y);
+                                                                        a.Sg, a.M, a.Y);
       const int64_t tr = (int64_t)a.n_m2l_targets * ND * NC;
       int gr = (int)std::min<int64_t>((tr + 255) / 256, 148 * 16);
       k_m2l_reduce<P, ND><<<gr, 256, 0, st>>>(a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.Y, a.L);
-      launches += 3;
+      launches += 2;
     }
   }
   if (stages & STAGE_L2L)

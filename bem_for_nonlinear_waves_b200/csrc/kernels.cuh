@@ -42,7 +42,6 @@ struct MatvecArgs {
   const int* chunk_cnt = nullptr;
   const int* grp_pair = nullptr;
   const double2* Sg = nullptr;  // per-group S tables
-  double2* Mf = nullptr;        // expanded multipoles
   double2* Y = nullptr;         // per-pair partial locals
   double2* M = nullptr;
   double2* L = nullptr;
