@@ -105,7 +105,8 @@ struct bem_gpu_ctx {
   DBuf<NearBlockDev> blocks;
   DBuf<int> chunk_grp, chunk_begin, chunk_cnt, grp_pair;
   DBuf<double> grp_vec;
-  DBuf<double2> Sg, Y;
+  DBuf<double2> Sg, Y, Ftab;
+  DBuf<double> ftab_vec;
   DBuf<double2> M, L;
   std::vector<int> level_parent_off;
   int n_m2l_targets = 0, max_ntgt = 0, chunk = 0;
@@ -183,6 +184,7 @@ struct bem_gpu_ctx {
     a.child_begin = child_begin.p;
     a.child_end = child_end.p;
     a.node_children = node_children.p;
+    a.Ftab = Ftab.p;
     a.n_m2l_targets = n_m2l_targets;
     a.m2l_targets = m2l_targets.p;
     a.m2l_off = m2l_off.p;
@@ -378,6 +380,10 @@ int ensure_arnoldi_graph(bem_gpu_ctx* ctx, bool jacobi, bool lowp, int cols) {
   a.sn = ctx->arn_sn.p;
   a.g = ctx->arn_g.p;
   a.R = ctx->arn_R.p;
+  if (configure_arnoldi(cols) != 0) {
+    ctx->err = "GMRES basis too large for the on-device Givens step (max_iter > 9000)";
+    return BEM_ERR_UNSUPPORTED;
+  }
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   launch_arnoldi_step(a, ctx->stream);
   CK(cudaStreamEndCapture(ctx->stream, &ctx->arn_graph));
@@ -522,6 +528,30 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     for (int i : P.level_nodes[l])
       if (P.nodes[i].child_end > P.nodes[i].child_begin) lp.push_back(i);
     ctx->level_parent_off.push_back((int)lp.size());
+  }
+  {  // parent-to-child F tables per (level, octant), from the first pair met of each
+    const int nlev = (int)ctx->level_parent_off.size() - 1;
+    std::vector<double> fv((size_t)std::max(nlev, 1) * 8 * 3, 0.0);
+    std::vector<char> seen((size_t)std::max(nlev, 1) * 8, 0);
+    for (int l = 0; l < nlev; ++l)
+      for (int q = ctx->level_parent_off[l]; q < ctx->level_parent_off[l + 1]; ++q) {
+        const int par = lp[q];
+        for (int ci = P.nodes[par].child_begin; ci < P.nodes[par].child_end; ++ci) {
+          const int c = P.node_children[ci];
+          double d[3];
+          for (int a2 = 0; a2 < 3; ++a2) d[a2] = P.nodes[c].X[a2] - P.nodes[par].X[a2];
+          const int o = (d[0] > 0 ? 1 : 0) | (d[1] > 0 ? 2 : 0) | (d[2] > 0 ? 4 : 0);
+          if (!seen[l * 8 + o]) {
+            seen[l * 8 + o] = 1;
+            for (int a2 = 0; a2 < 3; ++a2) fv[(l * 8 + o) * 3 + a2] = d[a2];
+          }
+        }
+      }
+    CK(up(ctx, ctx->ftab_vec, fv));
+    const int NFt = (P.opt.p + 1) * (P.opt.p + 1);
+    CK(ctx->Ftab.alloc((size_t)std::max(nlev, 1) * 8 * NFt));
+    launch_f_tables(P.opt.p, std::max(nlev, 1) * 8, ctx->ftab_vec.p, ctx->Ftab.p, s);
+    ctx->launches += 1;
   }
   const std::vector<int>& mt = P.m2l_targets;
   ctx->n_m2l_targets = (int)mt.size();
@@ -1035,6 +1065,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   };
   int iters = 0, rc = BEM_OK;
   double r_true = 1e300, err = 1e300;
+  bool x_zero = (x0 == nullptr);
   // Arnoldi steps run as one graph each (operator + orthogonalisation + Givens update, all
   // state on the device); the host reads each step's residual estimate kLag steps behind.
   if ((rc = ensure_arnoldi_graph(ctx, jacobi, mixed, cols)) != BEM_OK) return rc;
@@ -1067,6 +1098,9 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
       ctx->launches += 1;
       beta = r_true;
       have_res = false;
+    } else if (x_zero) {  // r0 = b for the zero start: no operator application
+      CK(cudaMemcpyAsync(ctx->rdev.p, ctx->bdev.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+      if ((rc = norm_of(ctx->rdev.p, &beta)) != BEM_OK) return rc;
     } else {
       // r0 = b - A x
       if ((rc = matvec(ctx->xdev.p, ctx->rdev.p)) != BEM_OK) return rc;
@@ -1083,6 +1117,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
       err = 0.0;
       break;
     }
+    x_zero = false;
     launch_axpby(N, 1.0 / beta, ctx->rdev.p, 0.0, ctx->V.p, s);
     launch_arnoldi_init(ctx->arn_state.p, ctx->arn_g.p, beta, s);
     // x_base: the iterate this cycle's corrections start from

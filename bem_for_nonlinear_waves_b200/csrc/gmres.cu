@@ -112,40 +112,55 @@ __global__ void k_arn_prep(int nrow, const double* __restrict__ V, const double*
 __global__ void k_arn_givens(ArnoldiState* __restrict__ st, const double* __restrict__ h1, const double* __restrict__ h2,
                              const double* __restrict__ hn, double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
                              double* __restrict__ R, int ldr) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  // the warp stages the column and the rotations in shared memory, lane 0 runs the serial
+  // rotation chain there, the warp stores the rotated column into R
+  extern __shared__ double sg[];  // h [k+1], cs [k], sn [k]
   const int n = st->n, k = n + 1;
-  double* h = R + (size_t)n * ldr;  // this step's column, rotated in place
-  for (int i = 0; i < k; ++i) h[i] = h1[i] + h2[i];
-  h[k] = sqrt(hn[0]);
-  st->inv_h = h[k] > 0.0 ? 1.0 / h[k] : 0.0;
-  if (!isfinite(h[k])) st->bad = 1;
-  for (int i = 0; i < k - 1; ++i) {
-    const double t = fma(cs[i], h[i], sn[i] * h[i + 1]);
-    h[i + 1] = fma(cs[i], h[i + 1], -sn[i] * h[i]);
-    h[i] = t;
+  const int lane = threadIdx.x;
+  double* h = sg;
+  double* c_ = sg + k + 1;
+  double* s_ = c_ + k;
+  for (int i = lane; i < k; i += 32) {
+    h[i] = h1[i] + h2[i];
+    c_[i] = cs[i];
+    s_[i] = sn[i];
   }
-  const double a = h[k - 1], bb = h[k];
-  const double rr = hypot(a, bb);
-  double c = 1.0, sv = 0.0;
-  if (rr != 0.0) {
-    c = a / rr;
-    sv = bb / rr;
+  __syncwarp();
+  if (lane == 0) {
+    h[k] = sqrt(hn[0]);
+    st->inv_h = h[k] > 0.0 ? 1.0 / h[k] : 0.0;
+    if (!isfinite(h[k])) st->bad = 1;
+    for (int i = 0; i < k - 1; ++i) {
+      const double t = fma(c_[i], h[i], s_[i] * h[i + 1]);
+      h[i + 1] = fma(c_[i], h[i + 1], -s_[i] * h[i]);
+      h[i] = t;
+    }
+    const double a = h[k - 1], bb = h[k];
+    const double rr = hypot(a, bb);
+    double c = 1.0, sv = 0.0;
+    if (rr != 0.0) {
+      c = a / rr;
+      sv = bb / rr;
+    }
+    cs[k - 1] = c;
+    sn[k - 1] = sv;
+    {
+      const double t = fma(c, h[k - 1], sv * h[k]);
+      h[k] = fma(c, h[k], -sv * h[k - 1]);
+      h[k - 1] = t;
+    }
+    g[k] = 0.0;
+    {
+      const double t = fma(c, g[k - 1], sv * g[k]);
+      g[k] = fma(c, g[k], -sv * g[k - 1]);
+      g[k - 1] = t;
+    }
+    st->err = fabs(g[k]);
+    st->n = k;
   }
-  cs[k - 1] = c;
-  sn[k - 1] = sv;
-  {
-    const double t = fma(c, h[k - 1], sv * h[k]);
-    h[k] = fma(c, h[k], -sv * h[k - 1]);
-    h[k - 1] = t;
-  }
-  g[k] = 0.0;
-  {
-    const double t = fma(c, g[k - 1], sv * g[k]);
-    g[k] = fma(c, g[k], -sv * g[k - 1]);
-    g[k - 1] = t;
-  }
-  st->err = fabs(g[k]);
-  st->n = k;
+  __syncwarp();
+  double* Rc = R + (size_t)n * ldr;
+  for (int i = lane; i <= k; i += 32) Rc[i] = h[i];
 }
 
 // V[:, n] = w / h_{n,n-1} (n already advanced)
@@ -201,8 +216,8 @@ int grid_rows(int n) {
 }  // namespace
 
 int arnoldi_dot_blocks(int n) {
-  const int b = (n + 1023) / 1024;
-  return b < 1 ? 1 : (b > 296 ? 296 : b);
+  const int b = (n + 255) / 256;  // one row per thread per column pass: the basis read is spread over many SMs
+  return b < 1 ? 1 : (b > 592 ? 592 : b);
 }
 
 int launch_arnoldi_step(const ArnoldiArgs& a, cudaStream_t st) {
@@ -222,9 +237,15 @@ int launch_arnoldi_step(const ArnoldiArgs& a, cudaStream_t st) {
   }
   k_selfdot<<<db, 256, 0, st>>>(a.w, a.nrow, a.partial, a.cols);
   k_mdot_final_dev<<<1, 256, 0, st>>>(a.partial, db, a.cols, a.state, 1, hn);
-  k_arn_givens<<<1, 32, 0, st>>>(a.state, h1, h2, hn, a.cs, a.sn, a.g, a.R, a.cols);
+  k_arn_givens<<<1, 32, sizeof(double) * (3 * a.cols + 1), st>>>(a.state, h1, h2, hn, a.cs, a.sn, a.g, a.R, a.cols);
   k_arn_normalize<<<g, 256, 0, st>>>(a.nrow, a.w, a.state, a.V);
   return launches + 4;
+}
+
+int configure_arnoldi(int cols) {
+  const size_t bytes = sizeof(double) * (3 * (size_t)cols + 1);
+  if (bytes > 227 * 1024) return -1;
+  return cudaFuncSetAttribute(k_arn_givens, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess ? 0 : -1;
 }
 
 void launch_arnoldi_init(ArnoldiState* state, double* g, double beta, cudaStream_t st) { k_arn_init<<<1, 32, 0, st>>>(state, g, beta); }

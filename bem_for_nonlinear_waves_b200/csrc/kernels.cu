@@ -290,6 +290,21 @@ __device__ __forceinline__ void expand_full_warp(const double2* __restrict__ src
   }
 }
 
+// Parent-to-child translation tables.  A child bucket sits at one of eight offsets from its
+// parent, the same on a level up to rounding, so F(c - c') is tabulated once per (level,
+// octant) at set-up; the tree passes read the table instead of running the recurrence.
+template <int P>
+__global__ void k_ftab(int ntab, const double* __restrict__ vec, double2* __restrict__ Ftab) {
+  constexpr int NF = (P + 1) * (P + 1);
+  const int t = blockIdx.x;
+  if (t < ntab && threadIdx.x < 32) F_full_column<P>(threadIdx.x, vec[3 * t], vec[3 * t + 1], vec[3 * t + 2], Ftab + (size_t)t * NF);
+}
+
+__device__ __forceinline__ int child_octant(const double* __restrict__ node_X, int c, int par) {
+  return (node_X[3 * c] > node_X[3 * par] ? 1 : 0) | (node_X[3 * c + 1] > node_X[3 * par + 1] ? 2 : 0) |
+         (node_X[3 * c + 2] > node_X[3 * par + 2] ? 4 : 0);
+}
+
 // M2M: one block of 8 warps per parent, warp w translating child w (lane per output
 // coefficient); the children's partial multipoles are summed in child order.  The upward
 // pass is level by level, so the time of one block is the time of a level: splitting the
@@ -303,7 +318,8 @@ constexpr int m2m_warps() { return kTreeWarps * 3 * (P + 1) * (P + 1) * 16 <= 48
 template <int P, int ND>
 __global__ void __launch_bounds__(32 * m2m_warps<P>()) k_m2m(const int* __restrict__ parents, const int* __restrict__ child_begin,
                                                        const int* __restrict__ child_end, const int* __restrict__ node_children,
-                                                       const double* __restrict__ node_X, double2* __restrict__ M) {
+                                                       const double* __restrict__ node_X, const double2* __restrict__ Ftab,
+                                                       double2* __restrict__ M) {
   constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), R = (NC + 31) / 32, W = m2m_warps<P>();
   __shared__ double2 sbuf[W * 3 * NF];  // per warp: F [NF], child multipole [2][NF]
   const int par = parents[blockIdx.x];
@@ -316,8 +332,8 @@ __global__ void __launch_bounds__(32 * m2m_warps<P>()) k_m2m(const int* __restri
   const int cb = child_begin[par], ce = child_end[par];
   for (int ci = cb + warp; ci < ce; ci += W) {
     const int c = node_children[ci];
-    F_full_column<P>(lane, node_X[3 * c] - node_X[3 * par], node_X[3 * c + 1] - node_X[3 * par + 1],
-                     node_X[3 * c + 2] - node_X[3 * par + 2], sF);
+    const double2* Ft = Ftab + (size_t)child_octant(node_X, c, par) * NF;
+    for (int i = lane; i < NF; i += 32) sF[i] = Ft[i];
     expand_full_warp<P, ND>(M + (size_t)c * 2 * NC, sM, lane);
     __syncwarp();
 #pragma unroll
@@ -478,7 +494,8 @@ __global__ void k_m2l_reduce(int ntargets, const int* __restrict__ targets, cons
 template <int P, int ND>
 __global__ void __launch_bounds__(32 * kTreeWarps) k_l2l(const int* __restrict__ parents, const int* __restrict__ child_begin,
                                                        const int* __restrict__ child_end, const int* __restrict__ node_children,
-                                                       const double* __restrict__ node_X, double2* __restrict__ L) {
+                                                       const double* __restrict__ node_X, const double2* __restrict__ Ftab,
+                                                       double2* __restrict__ L) {
   constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), R = (NC + 31) / 32;
   __shared__ double2 sL[2 * NF];
   __shared__ double2 sFw[kTreeWarps * NF];
@@ -490,8 +507,8 @@ __global__ void __launch_bounds__(32 * kTreeWarps) k_l2l(const int* __restrict__
   const int cb = child_begin[par], ce = child_end[par];
   for (int ci = cb + warp; ci < ce; ci += kTreeWarps) {
     const int c = node_children[ci];
-    F_full_column<P>(lane, node_X[3 * c] - node_X[3 * par], node_X[3 * c + 1] - node_X[3 * par + 1],
-                     node_X[3 * c + 2] - node_X[3 * par + 2], sF);
+    const double2* Ft = Ftab + (size_t)child_octant(node_X, c, par) * NF;
+    for (int i = lane; i < NF; i += 32) sF[i] = Ft[i];
     __syncwarp();
     double2* dst = L + (size_t)c * 2 * NC;
 #pragma unroll
@@ -1031,7 +1048,8 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     for (int l = a.n_levels - 1; l >= 0; --l) {
       const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
       if (cnt > 0) {
-        k_m2m<P, ND><<<cnt, 32 * m2m_warps<P>(), 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.M);
+        k_m2m<P, ND><<<cnt, 32 * m2m_warps<P>(), 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end,
+                                                          a.node_children, a.node_X, a.Ftab + (size_t)l * 8 * (P + 1) * (P + 1), a.M);
         ++launches;
       }
     }
@@ -1053,7 +1071,8 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     for (int l = 0; l < a.n_levels; ++l) {
       const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
       if (cnt > 0) {
-        k_l2l<P, ND><<<cnt, 32 * kTreeWarps, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end, a.node_children, a.node_X, a.L);
+        k_l2l<P, ND><<<cnt, 32 * kTreeWarps, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end,
+                                                      a.node_children, a.node_X, a.Ftab + (size_t)l * 8 * (P + 1) * (P + 1), a.L);
         ++launches;
       }
     }
@@ -1100,6 +1119,23 @@ template <int P>
 void set_m2l_smem() {
   cudaFuncSetAttribute(k_m2l_grp<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, m2l_grp_smem_bytes<P>());
   cudaFuncSetAttribute(k_m2l_grp<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, m2l_grp_smem_bytes<P>());
+}
+
+template <int P>
+void f_tables(int ntab, const double* vec, double2* Ftab, cudaStream_t st) {
+  if (ntab > 0) k_ftab<P><<<ntab, 32, 0, st>>>(ntab, vec, Ftab);
+}
+
+void launch_f_tables(int p, int ntab, const double* vec, double2* Ftab, cudaStream_t st) {
+  switch (p) {
+#define BEMB200_CASE(PP) \
+  case PP:               \
+    f_tables<PP>(ntab, vec, Ftab, st); break;
+    BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5) BEMB200_CASE(6)
+    BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10) BEMB200_CASE(11) BEMB200_CASE(12)
+#undef BEMB200_CASE
+    default: break;
+  }
 }
 
 template <int P>

@@ -32,6 +32,7 @@ struct MatvecArgs {
   const int* child_begin = nullptr;
   const int* child_end = nullptr;
   const int* node_children = nullptr;
+  const double2* Ftab = nullptr;           // [level][octant][(P+1)^2] parent-to-child F tables
   int n_m2l_targets = 0;
   const int* m2l_targets = nullptr;
   const int* m2l_off = nullptr;
@@ -116,6 +117,8 @@ void upload_quadrature(const double dv[6][4], const double gw[25][3], cudaStream
 void configure_targets_smem(int p, int bytes);
 void configure_m2l_smem(int p);
 void launch_s_tables(int p, int ngroups, const double* gvec, double2* Sg, cudaStream_t st);
+// F(child - parent) per (level, octant) from one representative offset each: vec [ntab][3]
+void launch_f_tables(int p, int ntab, const double* vec, double2* Ftab, cudaStream_t st);
 enum { STAGE_P2M = 1, STAGE_M2M = 2, STAGE_M2L = 4, STAGE_L2L = 8, STAGE_TARGETS = 16, STAGE_ALL = 31 };
 // returns the number of kernels launched
 // One operator application; returns the number of kernel launches.  A call that asks for
@@ -178,6 +181,7 @@ struct ArnoldiArgs {
   double* R = nullptr;            // [cols][cols] triangular factor, column j at R + j * cols
 };
 int arnoldi_dot_blocks(int nrow);
+int configure_arnoldi(int cols);  // before capture: shared memory of the Givens step; -1 if cols is too large
 int launch_arnoldi_step(const ArnoldiArgs& a, cudaStream_t st);  // returns kernel launches
 void launch_arnoldi_init(ArnoldiState* state, double* g, double beta, cudaStream_t st);
 void launch_arnoldi_solve_y(const ArnoldiState* state, const double* R, int ldr, const double* g, double* y, cudaStream_t st);
