@@ -20,6 +20,7 @@ P_i64 = ctypes.POINTER(ctypes.c_int64)
 BEM_OK = 0
 BEM_ERR_INVALID_ARGUMENT = -1
 BEM_ERR_NOT_CONVERGED = -3
+BEM_ERR_NOT_READY = -6
 BEM_ERR_UNSUPPORTED = -7
 STATUS = {0: "ok", -1: "invalid argument", -2: "out of memory", -3: "not converged", -4: "non-finite value",
           -5: "device error", -6: "not ready", -7: "unsupported"}
@@ -69,6 +70,12 @@ EXPORTS = {
     "bem_gpu_check_device_status": (c_int, [ctypes.c_void_p]),
     "bem_gpu_fp64_peak_tflops": (c_dbl, [c_int]),
     "bem_plan_inspect": (c_int, [ctypes.POINTER(Opts), ctypes.POINTER(Desc), P_int, P_dbl, P_i64]),
+    "bem_gpu_batch_create": (ctypes.c_void_p, [ctypes.POINTER(Opts), c_int]),
+    "bem_gpu_batch_submit": (c_int, [ctypes.c_void_p, ctypes.POINTER(Desc), P_dbl, P_dbl, P_dbl, ctypes.POINTER(Stats),
+                                     ctypes.POINTER(ctypes.c_int64)]),
+    "bem_gpu_batch_poll": (c_int, [ctypes.c_void_p, ctypes.c_int64, c_int]),
+    "bem_gpu_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "bem_gpu_batch_destroy": (None, [ctypes.c_void_p]),
 }
 
 _lib = None

@@ -19,10 +19,10 @@ BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
-CXXFLAGS = ["-O2", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-Wall", "-fopenmp"]
+CXXFLAGS = ["-O2", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-Wall", "-fopenmp", "-pthread"]
 
 CU_SOURCES = ["kernels.cu", "m2l_tc.cu", "gmres.cu", "capi.cu"]
-CXX_SOURCES = ["plan.cpp"]
+CXX_SOURCES = ["plan.cpp", "batch.cpp"]
 
 
 def _run(cmd):
@@ -62,7 +62,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         if _stale(o, [s] + headers):
             _run(["g++"] + CXXFLAGS + ["-c", "-o", o, s])
     if _stale(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-cudart=static", "-o", LIB] + objs + ["-lstdc++", "-lgomp"])
+        _run([NVCC] + ARCH + ["-shared", "-cudart=static", "-o", LIB] + objs + ["-lstdc++", "-lgomp", "-lpthread"])
     return LIB
 
 

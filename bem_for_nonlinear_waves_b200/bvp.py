@@ -39,6 +39,23 @@ def build_dofs(X, tri, face_dirichlet):
                 point_flags=pfl)
 
 
+def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter, device,
+               tol_relative, preconditioner, precision):
+    o = L.Opts()
+    lib.bem_gpu_default_opts(ctypes.byref(o))
+    o.expansion_order = int(expansion_order)
+    o.mac_theta = float(mac_theta)
+    o.leaf_max_elements = int(fmm_bucket_max_points)
+    o.max_level = int(fmm_max_level)
+    o.tol = float(solver_tol)
+    o.max_iter = int(solver_max_iter)
+    o.device = int(device)
+    o.tol_relative = 1 if tol_relative else 0
+    o.preconditioner = {"none": 0, "jacobi": 1}[preconditioner]
+    o.precision = {"fp64": 0, "mixed": 1}[precision]
+    return o
+
+
 class BEM_BVP:
     """GMRES-FMM Laplace BVP on one B200."""
 
@@ -51,18 +68,8 @@ class BEM_BVP:
         self.X = np.ascontiguousarray(X, np.float64)
         self.tri = np.ascontiguousarray(tri, np.int32)
         self.face_dirichlet = np.ascontiguousarray(face_dirichlet, np.uint8)
-        o = L.Opts()
-        self.lib.bem_gpu_default_opts(ctypes.byref(o))
-        o.expansion_order = int(expansion_order)
-        o.mac_theta = float(mac_theta)
-        o.leaf_max_elements = int(fmm_bucket_max_points)
-        o.max_level = int(fmm_max_level)
-        o.tol = float(solver_tol)
-        o.max_iter = int(solver_max_iter)
-        o.device = int(device)
-        o.tol_relative = 1 if tol_relative else 0
-        o.preconditioner = {"none": 0, "jacobi": 1}[preconditioner]
-        o.precision = {"fp64": 0, "mixed": 1}[precision]
+        o = _make_opts(self.lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter,
+                       device, tol_relative, preconditioner, precision)
         self.opts = o
         self.ctx = self.lib.bem_gpu_create(ctypes.byref(o))
         if not self.ctx:
@@ -225,3 +232,65 @@ def inspect_plan(X, tri, face_dirichlet, dofs=None, *, expansion_order=10, mac_t
         raise ValueError("plan construction failed: " + L.STATUS.get(rc, str(rc)))
     keys = ["nodes", "leaves", "depth", "n_added", "m2l_pairs", "near_pairs", "nnz", "near_blocks", "m2l_chunks", "m2l_groups"]
     return lv, corner.reshape(-1, 3), {k: int(v) for k, v in zip(keys, st)}
+
+
+class BatchSolver:
+    """Many independent BVPs through bem_gpu_batch_*: `n_workers` solver contexts, each with
+    its own host thread and CUDA stream, take submitted problems in FIFO order, so the host
+    set-up of one problem overlaps the GPU solve of another.  `submit` returns a ticket;
+    `result(ticket)` waits for it and returns (phi, phin, stats) in physical units, like the
+    phi / phin fields BEM_BVP::solve() leaves behind (bem/BEM_solveBVP.hpp:376-410)."""
+
+    def __init__(self, n_workers=2, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30, fmm_max_level=7,
+                 solver_tol=1e-9, solver_max_iter=500, device=0, tol_relative=False, preconditioner="none", precision="fp64"):
+        self.lib = L.load()
+        if not self.lib.bem_gpu_is_available():
+            raise RuntimeError("no sm_100 CUDA device visible: the GMRES-FMM solver runs only on the GPU")
+        o = _make_opts(self.lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter,
+                       device, tol_relative, preconditioner, precision)
+        self.handle = self.lib.bem_gpu_batch_create(ctypes.byref(o), int(n_workers))
+        if not self.handle:
+            raise RuntimeError("bem_gpu_batch_create failed")
+        self._pending = {}  # ticket -> arrays the worker reads or writes until the ticket is done
+
+    def submit(self, X, tri, face_dirichlet, known, dofs=None):
+        X = np.ascontiguousarray(X, np.float64)
+        tri = np.ascontiguousarray(tri, np.int32)
+        fd = np.ascontiguousarray(face_dirichlet, np.uint8)
+        if dofs is None:
+            dofs = build_dofs(X, tri, fd)
+        keep = [np.ascontiguousarray(dofs[k], np.int32).reshape(-1) for k in ("dof_point", "dof_face", "dof_kind", "face_dof")]
+        n = keep[0].shape[0]
+        known = np.ascontiguousarray(known, np.float64)
+        if known.shape[0] != n:
+            raise ValueError("known values must have one entry per DOF")
+        phi, phin, st = np.zeros(n), np.zeros(n), L.Stats()
+        desc = L.Desc(X.shape[0], L.ptr(X, L.P_dbl), tri.shape[0], L.ptr(tri, L.P_int), L.ptr(fd, L.P_u8), n,
+                      L.ptr(keep[0], L.P_int), L.ptr(keep[1], L.P_int), L.ptr(keep[2], L.P_int), L.ptr(keep[3], L.P_int))
+        t = ctypes.c_int64(0)
+        rc = self.lib.bem_gpu_batch_submit(self.handle, ctypes.byref(desc), L.ptr(known, L.P_dbl), L.ptr(phi, L.P_dbl),
+                                           L.ptr(phin, L.P_dbl), ctypes.byref(st), ctypes.byref(t))
+        if rc != L.BEM_OK:
+            raise RuntimeError(f"batch submit: {L.STATUS.get(rc, rc)}")
+        self._pending[t.value] = (X, tri, fd, keep, known, phi, phin, st)
+        return t.value
+
+    def done(self, ticket):
+        return self.lib.bem_gpu_batch_poll(self.handle, int(ticket), 0) != L.BEM_ERR_NOT_READY
+
+    def result(self, ticket):
+        rc = self.lib.bem_gpu_batch_poll(self.handle, int(ticket), 1)
+        item = self._pending.pop(int(ticket))
+        if rc not in (L.BEM_OK, L.BEM_ERR_NOT_CONVERGED):
+            msg = self.lib.bem_gpu_batch_last_error(self.handle)
+            raise RuntimeError(f"batch solve {ticket}: {L.STATUS.get(rc, rc)}: {msg.decode() if msg else ''}")
+        return item[5], item[6], item[7]
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.bem_gpu_batch_destroy(self.handle)  # finishes queued problems before the arrays go
+            self.handle = None
+            self._pending.clear()
+
+    def __del__(self):
+        self.close()

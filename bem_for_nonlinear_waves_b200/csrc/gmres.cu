@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "kernels.cuh"
 
@@ -243,9 +244,16 @@ int launch_arnoldi_step(const ArnoldiArgs& a, cudaStream_t st) {
 }
 
 int configure_arnoldi(int cols) {
+  // the permission only grows (contexts on other threads may use larger bases)
+  static std::mutex mu;
+  static size_t granted = 0;
   const size_t bytes = sizeof(double) * (3 * (size_t)cols + 1);
   if (bytes > 227 * 1024) return -1;
-  return cudaFuncSetAttribute(k_arn_givens, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess ? 0 : -1;
+  std::lock_guard<std::mutex> lk(mu);
+  if (bytes <= granted) return 0;
+  if (cudaFuncSetAttribute(k_arn_givens, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) return -1;
+  granted = bytes;
+  return 0;
 }
 
 void launch_arnoldi_init(ArnoldiState* state, double* g, double beta, cudaStream_t st) { k_arn_init<<<1, 32, 0, st>>>(state, g, beta); }

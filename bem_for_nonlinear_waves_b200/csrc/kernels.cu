@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
 
 #include "fmm_math.cuh"
 #include "kernels.cuh"
@@ -1096,6 +1097,13 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
 
 template <int P>
 void set_target_smem(int bytes) {
+  // the permission only grows: contexts of different problems (batch workers on other
+  // threads) may launch these kernels with their own sizes at any time
+  static std::mutex mu;
+  static int granted = 0;
+  std::lock_guard<std::mutex> lk(mu);
+  if (bytes <= granted) return;
+  granted = bytes;
   cudaFuncSetAttribute(k_targets_ax<P, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(k_targets_ax<P, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(k_targets<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);

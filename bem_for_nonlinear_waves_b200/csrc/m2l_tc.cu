@@ -513,14 +513,14 @@ int tc_make_rows_map(void* map_out, void* Mt, int nrows, int p) {
   using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
                                 const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-  static EncodeFn encode = nullptr;
-  if (!encode) {
+  static const EncodeFn encode = [] {  // thread-safe one-time lookup
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
-      return -1;
-    encode = reinterpret_cast<EncodeFn>(fn);
-  }
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+      return static_cast<EncodeFn>(nullptr);
+    return reinterpret_cast<EncodeFn>(fn);
+  }();
+  if (!encode) return -1;
   const int kp = tc_kp(p);
   const cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)nrows};
   const cuuint64_t strides[1] = {(cuuint64_t)kp * 2};

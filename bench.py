@@ -10,6 +10,7 @@ the true residual; after the timed steps the FP64 GPU path solves the same tank 
 the line reports the mixed result's error against it (fp64_gpu).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --batch P --workers W [--config tank_15k]   # serving mode, one GPU
 
 Multi-GPU: independent BVPs per rank (replicas, weak scaling, no collective on the data
 path); time is the max over ranks.  `--impl reference` times the reference algorithm on
@@ -204,6 +205,60 @@ def load_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
+def run_batch(args, cfg, local):
+    """Serving mode: `--batch P` seeded tanks of the workload's size (different free
+    surfaces) go to a BatchSolver with `--workers W` contexts at once; reports whole-batch
+    solves/s and per-problem latency from submission to result (p50 / p99), next to the same
+    problems solved one after another on one context."""
+    from bem_for_nonlinear_waves_b200 import BEM_BVP, BatchSolver
+    rank = 0
+    probs = [make_problem(cfg, rank + 1000 + i) for i in range(args.batch)]
+    kw = dict(expansion_order=cfg["p"], solver_tol=cfg["rel_tol"], tol_relative=True, solver_max_iter=args.max_iter,
+              preconditioner=args.precond, device=local, precision=args.precision)
+    one = BEM_BVP(probs[0][0].X, probs[0][0].tri, probs[0][0].face_dirichlet, dofs=probs[0][1], **kw)
+    for _ in range(args.warmup):
+        one.setup()
+        one.solve(probs[0][2])
+    w0 = time.perf_counter()
+    seq_lat = []
+    for t, d, kv in probs:
+        b = BEM_BVP(t.X, t.tri, t.face_dirichlet, dofs=d, **kw)
+        s0 = time.perf_counter()
+        b.solve(kv)
+        seq_lat.append(time.perf_counter() - s0)
+        del b
+    seq_s = time.perf_counter() - w0
+    bs = BatchSolver(args.workers, **kw)
+    for _ in range(args.warmup):  # every worker context warm
+        for tk in [bs.submit(t.X, t.tri, t.face_dirichlet, kv, dofs=d) for t, d, kv in probs[:args.workers]]:
+            bs.result(tk)
+    with ClockSampler(local) as clk:
+        w0 = time.perf_counter()
+        sub = {}
+        for t, d, kv in probs:
+            sub[bs.submit(t.X, t.tri, t.face_dirichlet, kv, dofs=d)] = time.perf_counter()
+        lat = {}
+        while len(lat) < len(sub):
+            for tk in sub:
+                if tk not in lat and bs.done(tk):
+                    lat[tk] = time.perf_counter() - sub[tk]
+            time.sleep(0.0005)
+        batch_s = time.perf_counter() - w0
+    conv = all(bs.result(tk)[2].converged for tk in sub)
+    bs.close()
+    lats = sorted(lat.values())
+    pct = lambda v, q: float(np.percentile(np.asarray(v), q))  # noqa: E731
+    line = {"metric": "bvp_solves_per_s", "value": len(probs) / batch_s, "unit": "solves/s", "n_gpus": 1, "mode": "batch",
+            "higher_is_better": True, "dtype": "f64/f16x3-tc" if args.precision == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": args.config, "problems": len(probs), "workers": args.workers, "precision": args.precision,
+                       "preconditioner": args.precond, "converged": bool(conv)},
+            "latency_s": {"p50": pct(lats, 50), "p99": pct(lats, 99), "max": lats[-1]},
+            "sequential": {"solves_per_s": len(probs) / seq_s, "latency_p50_s": pct(seq_lat, 50)},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -217,10 +272,14 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-check", action="store_true")
+    ap.add_argument("--batch", type=int, default=0, help="serving mode: number of problems (one GPU)")
+    ap.add_argument("--workers", type=int, default=2)
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference(args, cfg)
+    if args.batch > 0:
+        return run_batch(args, cfg, int(os.environ.get("LOCAL_RANK", "0")))
 
     rank, world, local = dist_init()
     from bem_for_nonlinear_waves_b200 import BEM_BVP

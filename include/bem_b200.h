@@ -175,6 +175,22 @@ int bem_plan_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* desc, int32_t
  * stage_ms = [p2m, m2m, m2l, l2l, near+l2p+rows, whole graph-launched mat-vec]. */
 int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[6]*/);
 
+/* Batch / asynchronous solving (the reference solves one BVP per call; BEM_BVP::solve(),
+ * bem/BEM_solveBVP.hpp:565-630).  A batch owns n_workers contexts (one CUDA stream and one
+ * host thread each) created with *opts; submitted problems queue FIFO and the next free
+ * worker runs bem_gpu_solve_bvp on it, so one problem's host set-up overlaps another's GPU
+ * work and the GPU work of different workers overlaps on the device.  The caller keeps every
+ * array of the submitted problem (desc arrays, known, outputs, stats) alive and untouched
+ * until its ticket polls done.  bem_gpu_batch_poll returns the solve's status (as
+ * bem_gpu_solve_bvp), or BEM_ERR_NOT_READY while it is pending and wait == 0. */
+typedef struct bem_gpu_batch bem_gpu_batch;
+bem_gpu_batch* bem_gpu_batch_create(const bem_gpu_opts* opts, int32_t n_workers);
+int bem_gpu_batch_submit(bem_gpu_batch* batch, const bem_bvp_desc* desc, const double* known, double* out_phi, double* out_phin,
+                         bem_gpu_stats* stats, int64_t* ticket);
+int bem_gpu_batch_poll(bem_gpu_batch* batch, int64_t ticket, int32_t wait);
+const char* bem_gpu_batch_last_error(const bem_gpu_batch* batch);  /* message of the last polled failure */
+void bem_gpu_batch_destroy(bem_gpu_batch* batch);                  /* finishes queued problems first */
+
 /* Mixed precision (context set up with opts.precision = 1).  No reference counterpart: the
  * reference's M2L is FP64 only (lib/include/moments.hpp:732-764).
  * bem_gpu_matvec_device_mixed: y = A_lo x on device buffers (tensor-core M2L, everything
