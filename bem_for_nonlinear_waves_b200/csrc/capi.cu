@@ -101,6 +101,7 @@ struct bem_gpu_ctx {
   DBuf<double2> near_scratch;                // element values of the near-weight kernel
   DBuf<int> e_dof, e_vtx, node_fb, node_fe, leaves, level_parents, child_begin, child_end, node_children;
   DBuf<int> m2l_targets, m2l_off, m2l_src, nb_dofs, nb_targets, nb_ranges, dof_inc_off, dof_inc;
+  DBuf<int> block_of_point, row_of_point, self_col;  // right-Jacobi inputs
   DBuf<int> point_dof_off, point_dof, dof_kind, dof_point;
   DBuf<NearBlockDev> blocks;
   DBuf<int> chunk_grp, chunk_begin, chunk_cnt, grp_pair;
@@ -122,7 +123,7 @@ struct bem_gpu_ctx {
   int graph_kernels = 0;
   // mixed precision: tensor-core M2L tables and buffers; graph of the low-precision A.x
   bool mixed = false;
-  DBuf<int> tc_item_tab, tc_item_begin, tc_item_cnt, tc_pair, tc_src, tc_err;
+  DBuf<int> tc_item_tab, tc_item_begin, tc_item_cnt, tc_pos, tc_src, tc_err;
   DBuf<double> tc_tabvec, tc_alpha, node_dL;
   DBuf<uint16_t> tc_T, tc_Mt;
   DBuf<float> tc_escale;
@@ -235,7 +236,8 @@ struct bem_gpu_ctx {
     a.tc_item_tab = tc_item_tab.p;
     a.tc_item_begin = tc_item_begin.p;
     a.tc_item_cnt = tc_item_cnt.p;
-    a.tc_pair = tc_pair.p;
+    a.tc_pos = tc_pos.p;
+    a.n_tc_pairs = (int)plan.tc_pair.size();
     a.tc_src = tc_src.p;
     a.tc_tab = tc_T.p;
     a.tc_Mt = tc_Mt.p;
@@ -623,8 +625,6 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     const size_t y64 = (size_t)std::max<int64_t>(P.m2l_pairs, 1) * 2 * NC;
     const size_t ytc = ((size_t)std::max<int64_t>(P.m2l_pairs, 1) * tc_kp(P.opt.p) * sizeof(float) + sizeof(double2) - 1) / sizeof(double2);
     CK(ctx->Y.alloc(ctx->opts.precision == 1 ? std::max(y64, ytc) : y64));
-    launch_s_tables(P.opt.p, ngroups, ctx->grp_vec.p, ctx->Sg.p, s);
-    ctx->launches += 1;
   }
   ctx->mixed = ctx->opts.precision == 1;
   if (ctx->mixed) {  // tensor-core M2L: translation tables, multipole rows, work items
@@ -637,18 +637,20 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     CK(up(ctx, ctx->tc_item_tab, P.tc_item_tab));
     CK(up(ctx, ctx->tc_item_begin, P.tc_item_begin));
     CK(up(ctx, ctx->tc_item_cnt, P.tc_item_cnt));
-    CK(up(ctx, ctx->tc_pair, P.tc_pair));
-    {
-      std::vector<int> src(P.tc_pair.size());
-      for (size_t j = 0; j < src.size(); ++j) src[j] = P.m2l_src[P.tc_pair[j]];
+    {  // work-item order j -> source bucket; pair slot k -> its position j (the row of its partial)
+      std::vector<int> src(P.tc_pair.size()), pos(P.tc_pair.size());
+      for (size_t j = 0; j < src.size(); ++j) {
+        src[j] = P.m2l_src[P.tc_pair[j]];
+        pos[P.tc_pair[j]] = (int)j;
+      }
       CK(up(ctx, ctx->tc_src, src));
+      CK(up(ctx, ctx->tc_pos, pos));
     }
     CK(up(ctx, ctx->tc_tabvec, P.tc_tab));
     CK(up(ctx, ctx->tc_alpha, al));
     CK(up(ctx, ctx->node_dL, dl));
     CK(ctx->tc_T.alloc((size_t)std::max(ntab, 1) * tc_table_bytes(p) / 2));
     CK(ctx->tc_Mt.alloc((size_t)(nb + 1) * 2 * kp));
-    CK(cudaMemsetAsync(ctx->tc_Mt.p, 0, sizeof(uint16_t) * ctx->tc_Mt.n, s));
     ctx->tc_map.assign(tc_rows_map_bytes(), 0);
     if (tc_make_rows_map(ctx->tc_map.data(), ctx->tc_Mt.p, 2 * (nb + 1), p) != 0) {
       ctx->err = "mixed precision: could not encode the TMA tensor map of the multipole rows";
@@ -656,14 +658,10 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     }
     CK(ctx->tc_escale.alloc((size_t)nb + 1));
     CK(ctx->tc_err.alloc(1));
-    CK(cudaMemsetAsync(ctx->tc_err.p, 0, sizeof(int), s));
     CK(ctx->tc_max.alloc(1));
-    CK(cudaMemsetAsync(ctx->tc_max.p, 0, sizeof(unsigned int), s));
     int sms = 148;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->opts.device));
     ctx->tc_grid = sms;
-    launch_tc_tables(p, ntab, ctx->tc_tabvec.p, ctx->tc_alpha.p, ctx->tc_T.p, ctx->tc_max.p, s);
-    ctx->launches += 1;
   }
   {  // P2M operator of A.x: the DOFs of each leaf's elements, and the slot of every vertex
     const int nl = (int)P.leaves.size();
@@ -686,11 +684,9 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     CK(up(ctx, ctx->leaf_dof, ld));
     CK(up(ctx, ctx->e_slot, es));
     CK(ctx->p2m_C.alloc(std::max<size_t>(ld.size(), 1) * NC));
-    CK(cudaMemsetAsync(ctx->p2m_C.p, 0, sizeof(double2) * std::max<size_t>(ld.size(), 1) * NC, s));
   }
   CK(ctx->M.alloc((size_t)nb * 2 * NC));
   CK(ctx->L.alloc((size_t)nb * 2 * NC));
-  CK(cudaMemsetAsync(ctx->M.p, 0, sizeof(double2) * ctx->M.n, s));
   CK(ctx->WG.alloc(std::max<int64_t>(P.nnz, 1)));
   CK(ctx->WGn.alloc(std::max<int64_t>(P.nnz, 1)));
   CK(ctx->Wc.alloc(std::max<int64_t>(P.nnz, 1)));
@@ -705,14 +701,7 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   CK(ctx->GnPhi.alloc(P.np));
   CK(ctx->mv_in.alloc(N));
   CK(ctx->mv_out.alloc(N));
-  CK(cudaMemsetAsync(ctx->GPhin.p, 0, sizeof(double) * P.np, s));
-  CK(cudaMemsetAsync(ctx->GnPhi.p, 0, sizeof(double) * P.np, s));
-
-  CK(cudaStreamSynchronize(s));
-  ctx->time_upload = now_s() - t0 - ctx->time_plan;
-  // device part of the set-up starts here (inputs resident)
-  CK(cudaEventRecord(ctx->ev[0], s));
-  // near-field weights
+  // near-field weights: work partition and scratch
   NearArgs na;
   na.n_blocks = (int)P.blocks.size();
   na.blocks = ctx->blocks.p;
@@ -747,6 +736,35 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     CK(ctx->near_scratch.alloc((size_t)near_weights_grid() * na.scratch_stride));
     na.scratch = ctx->near_scratch.p;
   }
+  {  // right-Jacobi scaling inputs: each point's near-field block row
+    std::vector<int> bop(P.np), rop(P.np);
+    for (int p = 0; p < P.np; ++p) {
+      bop[p] = std::max(P.block_of_point[p], 0);
+      rop[p] = std::max(P.row_of_point[p], 0);
+    }
+    CK(up(ctx, ctx->block_of_point, bop));
+    CK(up(ctx, ctx->row_of_point, rop));
+    CK(up(ctx, ctx->self_col, P.self_col));
+    CK(ctx->dinv.alloc(N));
+  }
+  CK(cudaStreamSynchronize(s));
+  ctx->time_upload = now_s() - t0 - ctx->time_plan;
+  // device part of the set-up starts here (inputs resident): every kernel that derives the
+  // operator's tables and weights from the uploaded plan
+  CK(cudaEventRecord(ctx->ev[0], s));
+  CK(cudaMemsetAsync(ctx->GPhin.p, 0, sizeof(double) * P.np, s));
+  CK(cudaMemsetAsync(ctx->GnPhi.p, 0, sizeof(double) * P.np, s));
+  CK(cudaMemsetAsync(ctx->M.p, 0, sizeof(double2) * ctx->M.n, s));
+  CK(cudaMemsetAsync(ctx->p2m_C.p, 0, sizeof(double2) * ctx->p2m_C.n, s));
+  launch_s_tables(P.opt.p, (int)P.grp_off.size() - 1, ctx->grp_vec.p, ctx->Sg.p, s);
+  ctx->launches += 1;
+  if (ctx->mixed) {
+    CK(cudaMemsetAsync(ctx->tc_Mt.p, 0, sizeof(uint16_t) * ctx->tc_Mt.n, s));
+    CK(cudaMemsetAsync(ctx->tc_err.p, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(ctx->tc_max.p, 0, sizeof(unsigned int), s));
+    launch_tc_tables(P.opt.p, (int)(P.tc_tab.size() / 4), ctx->tc_tabvec.p, ctx->tc_alpha.p, ctx->tc_T.p, ctx->tc_max.p, s);
+    ctx->launches += 1;
+  }
   {
     MatvecArgs pa = ctx->args(nullptr, nullptr, nullptr, nullptr, nullptr);
     ctx->set_ax(pa, false);
@@ -765,23 +783,10 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   ctx->launches += 3;
   CK(cudaGetLastError());
   // right-Jacobi scaling from the near-field diagonal entries
-  {
-    std::vector<int> bop(P.np), rop(P.np);
-    for (int p = 0; p < P.np; ++p) {
-      bop[p] = std::max(P.block_of_point[p], 0);
-      rop[p] = std::max(P.row_of_point[p], 0);
-    }
-    DBuf<int> d_bop, d_rop, d_self;
-    CK(up(ctx, d_bop, bop));
-    CK(up(ctx, d_rop, rop));
-    CK(up(ctx, d_self, P.self_col));
-    CK(ctx->dinv.alloc(N));
-    launch_jacobi(N, ctx->dof_point.p, ctx->dof_kind.p, ctx->diag.p, d_bop.p, d_rop.p, ctx->blocks.p, d_self.p, ctx->WG.p, ctx->WGn.p,
-                  ctx->dinv.p, s);
-    ctx->launches += 1;
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(s));
-  }
+  launch_jacobi(N, ctx->dof_point.p, ctx->dof_kind.p, ctx->diag.p, ctx->block_of_point.p, ctx->row_of_point.p, ctx->blocks.p,
+                ctx->self_col.p, ctx->WG.p, ctx->WGn.p, ctx->dinv.p, s);
+  ctx->launches += 1;
+  CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev[1], s));
   if (ctx->mixed) {  // FP16 tables must stay far from the FP16 range limit (65504)
     unsigned int bits = 0;

@@ -1036,10 +1036,10 @@ __global__ void k_fp64_probe(int iters, double seed, double* __restrict__ sink) 
 template <int P, int ND>
 int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
   constexpr int NC = ncoef(P);
-  const int tpb_coef = ((NC + 31) / 32) * 32;
+  constexpr int tpb_coef = ((NC + 31) / 32) * 32;
   int launches = 0;
   if ((stages & STAGE_P2M) && a.n_leaves > 0 && ND == 1 && a.ax && a.p2m_C) {
-    k_p2m_apply<P><<<a.n_leaves, ((NC + 31) / 32) * 32, 0, st>>>(a.leaves, a.leaf_dof_off, a.leaf_dof, a.p2m_C, a.ax, a.M);
+    k_p2m_apply<P><<<a.n_leaves, tpb_coef, 0, st>>>(a.leaves, a.leaf_dof_off, a.leaf_dof, a.p2m_C, a.ax, a.M);
     ++launches;
   } else if ((stages & STAGE_P2M) && a.n_leaves > 0) {
     k_p2m<P, ND><<<a.n_leaves, 128, 0, st>>>(a.leaves, a.node_fb, a.node_fe, a.node_X, a.e_q, a.e_W, a.e_n, a.e_dof, a.phi, a.phin, a.M);

@@ -52,12 +52,13 @@ struct MatvecArgs {
   const int* tc_item_tab = nullptr;
   const int* tc_item_begin = nullptr;
   const int* tc_item_cnt = nullptr;
-  const int* tc_pair = nullptr;
-  const int* tc_src = nullptr;   // source bucket of each tc_pair entry
+  int n_tc_pairs = 0;
+  const int* tc_pos = nullptr;   // [pairs] position of pair slot k in work-item order
+  const int* tc_src = nullptr;   // [pairs] source bucket, in work-item order
   const void* tc_tab = nullptr;  // FP16 hi/lo table images
   void* tc_Mt = nullptr;         // FP16 hi/lo rows of M[0] - M[1] [n_nodes+1][2][KP]
   float* tc_escale = nullptr;    // [n_nodes] power-of-two column scales
-  float* tc_Y = nullptr;         // per-pair partial locals [pairs][KP]
+  float* tc_Y = nullptr;         // per-pair partial locals [pairs][KP], in work-item order
   int* tc_err = nullptr;         // set when a bounded wait gave up
   const double* node_dL = nullptr;
   const double* tc_alpha = nullptr;  // [KP] sqrt((n+m)!(n-m)!) per real coefficient

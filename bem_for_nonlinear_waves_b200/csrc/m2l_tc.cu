@@ -49,7 +49,7 @@ namespace bemb200 {
 namespace {
 
 constexpr int kRows = 128;          // table rows = MMA N: output coefficients (NR <= 128, p <= 10)
-constexpr int kMaxPairs = 256;      // pairs per work item = gathered rows (one per pair)
+constexpr int kMaxPairs = 80;       // pairs per work item = gathered rows (one per pair)
 constexpr int kMaxCols = kMaxPairs;
 constexpr uint32_t kWaitTries = 1u << 22;
 
@@ -61,12 +61,14 @@ struct TcDims {
   static constexpr int TAB_BYTES = 2 * kRows * KP * 2;    // hi + lo images of one table
   static constexpr int REGION = kMaxCols * 128;           // one (part, atom) region of gathered rows
   static constexpr int B_BYTES = 2 * KA * REGION;         // hi + lo gathered rows
-  // plus 1 KB to align the gathered rows to the 1024-byte swizzle atom; at least half the
-  // SM's shared memory, so one CTA (and one TMEM allocation) per SM
-  static constexpr int NEED = TAB_BYTES + B_BYTES + 1024;
+  // two table slots and two stages of gathered rows, plus 1 KB to align them to the 1024-byte
+  // swizzle atom; at least half the SM's shared memory, so one CTA (and one TMEM allocation)
+  // per SM
+  static constexpr int NEED = 2 * TAB_BYTES + 2 * B_BYTES + 1024;
   static constexpr int SMEM = NEED > 116 * 1024 ? NEED : 116 * 1024;
   static_assert(NR <= kRows, "tensor-core M2L needs (p+1)^2 <= 128");
-  static_assert(TAB_BYTES % 1024 == 0, "gathered rows must start on a swizzle atom");
+  static_assert(TAB_BYTES % 1024 == 0 && B_BYTES % 1024 == 0, "gathered rows must start on a swizzle atom");
+  static_assert(NEED + 4096 <= 227 * 1024, "shared memory of one CTA");
 };
 
 // real index i -> (n, m, part) with part 0 = Re, 1 = Im
@@ -192,55 +194,68 @@ __global__ void k_tc_expand(int nnodes, const double2* __restrict__ M, const dou
 // ---------------------------------------------------------------------------
 // The contraction: persistent, warp-specialised CTAs, each over a contiguous range of work
 // items (consecutive items mostly share a table, which then stays in shared memory).
-//   warps 0-7  epilogue: TMEM lane = output coefficient, column = pair; warp w reads lane
-//              quadrant w % 4 and every other 32-column chunk (w / 4 picks which); for each
-//              pair it stores 32 consecutive coefficients (one 128-byte line) of the pair's
-//              slot with the pair's column scale undone.  The next chunk's TMEM load is in
-//              flight while the current chunk is stored.
-//   warps 8-11 producers: the next item's metadata is loaded while the current one runs;
-//              TMA: one bulk copy of the table image when the table changes, and
-//              tile::gather4 loads of the multipole rows of the item's sources into 128-byte
-//              swizzled K-major tiles; producer thread 0 also issues the MMAs
+//   warps 0-7   epilogue: TMEM lane = output coefficient, column = pair; warp w reads lane
+//               quadrant w % 4 and every other 32-column chunk (w / 4 picks which); for
+//               each pair it stores 32 consecutive coefficients (one 128-byte line) of the
+//               pair's partial.  Partials are stored in work-item order, so a CTA writes one
+//               contiguous stream; the reduction gathers them per target and undoes the
+//               column scales.  The next chunk's TMEM load is in flight while the current
+//               chunk is stored.
+//   warps 8-11  producers (thread = gathered row): metadata is loaded two items ahead;
+//               TMA: one bulk copy of the table image when the table changes, and
+//               tile::gather4 loads of the multipole rows of the item's sources into
+//               128-byte swizzled K-major tiles
+//   warp 12     MMA issuer (one elected lane)
 // MMA per item: D[128 coefficients x N pairs] = T~ * B^T with A = T~ (no swizzle, K-major)
 // and B = gathered rows (SW128 K-major), N = pairs rounded up to 16, three passes
-// hi*hi + hi*lo + lo*hi.  Shared memory holds one item, TMEM two (buffer b = item parity,
-// 256 columns each), so the epilogue of an item overlaps the loads and MMAs of the next.
-// Barriers:
-//   full         all TMA bytes of the item landed                 -> MMA issuer
-//   smem_free    MMAs of the item finished reading shared memory  -> producers
-//   acc_full[b]  accumulator buffer b written                      -> epilogue
-//   acc_empty[b] epilogue drained buffer b                         -> producers / MMA issuer
-//   meta[b]      metadata of buffer b published                    -> epilogue
+// hi*hi + hi*lo + lo*hi.  Shared memory holds two table images and two item stages of
+// gathered rows, TMEM four accumulators (128 columns each): the loads of item i+1 (and of
+// its table, when it differs) overlap the MMAs of item i, and the epilogue of item i
+// overlaps both.
+// Barriers (s = item stage = i % 2, t = table slot, b = accumulator = i % 4):
+//   full[s]    all TMA bytes of the item landed                   -> MMA issuer
+//   bfree[s]   MMAs of the item finished reading its gathered rows -> producers
+//   tfree[t]   MMAs of every item of the table in slot t finished  -> producers
+//   accf[b]    accumulator b written                               -> epilogue
+//   acce[b]    epilogue drained accumulator b                      -> producers, MMA issuer
+//   meta[b]    epilogue metadata of accumulator b published        -> epilogue
 // Every wait is bounded; a timeout records *err and ends the waiting role's loop, and the
 // roles waiting on it then time out as well rather than wait forever.
 constexpr int kProducers = 128;
 constexpr int kEpilogue = 256;
-constexpr int kColsPerProducer = kMaxCols / kProducers;
+constexpr int kIssuer = 32;
+constexpr int kStages = 2;
+constexpr int kAcc = 4;
+constexpr int kAccCols = 128;
+static_assert(kMaxCols <= kAccCols, "one accumulator holds an item");
+static_assert(kMaxCols <= kProducers, "one producer thread per gathered row");
 
 template <int P>
-__global__ void __launch_bounds__(kEpilogue + kProducers, 1)
+__global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
     k_m2l_tc(const __grid_constant__ CUtensorMap rows_map, int nitems, const int* __restrict__ item_tab, const int* __restrict__ item_begin,
-             const int* __restrict__ item_cnt, const int* __restrict__ tc_pair, const int* __restrict__ tc_src,
-             const __half* __restrict__ Ttab, const float* __restrict__ escale, float* __restrict__ Y, int* __restrict__ err) {
+             const int* __restrict__ item_cnt, int npairs, const int* __restrict__ tc_src, const __half* __restrict__ Ttab,
+             const __half* __restrict__ Mt, float* __restrict__ Y, int* __restrict__ err) {
   using D = TcDims<P>;
   extern __shared__ __align__(128) unsigned char sm_raw[];
   unsigned char* sm_tc = sm_raw + ((1024u - (smem_u32(sm_raw) & 1023u)) & 1023u);
-  unsigned char* sT = sm_tc;                 // [hi | lo] table images, kRows rows each
-  unsigned char* sB = sm_tc + D::TAB_BYTES;  // regions (part, atom): kMaxCols rows x 128 B
+  unsigned char* sT = sm_tc;                     // two table slots: [hi | lo] images, kRows rows each
+  unsigned char* sB = sm_tc + 2 * D::TAB_BYTES;  // kStages stages of regions (part, atom): kMaxCols rows x 128 B
   __shared__ int s_row[kMaxCols];
-  __shared__ float s_sc[2][kMaxCols];
-  __shared__ int s_slot[2][kMaxCols];
-  __shared__ int s_ncol[2];
-  __shared__ uint64_t bar_full, bar_free, bar_accf[2], bar_acce[2], bar_meta[2];
+  __shared__ int s_ncol[kAcc], s_b0[kAcc];
+  __shared__ int s_tsl[kStages], s_icol[kStages];
+  __shared__ uint64_t bar_full[kStages], bar_bfree[kStages], bar_tfree[2], bar_accf[kAcc], bar_acce[kAcc], bar_meta[kAcc];
   __shared__ uint32_t tslot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int i0 = (int)((int64_t)nitems * blockIdx.x / gridDim.x);
   const int i1 = (int)((int64_t)nitems * (blockIdx.x + 1) / gridDim.x);
-  if (warp == 0) tmem_alloc(&tslot, 512);
+  if (warp == 0) tmem_alloc(&tslot, kAcc * kAccCols);
   if (tid == 0) {
-    mbar_init(&bar_full, 1);
-    mbar_init(&bar_free, 1);
-    for (int b = 0; b < 2; ++b) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&bar_full[s], 1);
+      mbar_init(&bar_bfree[s], 1);
+    }
+    for (int t = 0; t < 2; ++t) mbar_init(&bar_tfree[t], 1);
+    for (int b = 0; b < kAcc; ++b) {
       mbar_init(&bar_accf[b], 1);
       mbar_init(&bar_acce[b], kEpilogue);
       mbar_init(&bar_meta[b], 1);
@@ -250,119 +265,141 @@ __global__ void __launch_bounds__(kEpilogue + kProducers, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = tslot;
-  if (tid >= kEpilogue) {
-    const int pt = tid - kEpilogue;  // producer thread
-    int last_tab = -1, issued = 0;
-    bool ok = true;
-    // metadata of item `it` in registers (loaded one item ahead)
-    int tab = 0, ncol = 0;
-    int r_slot[kColsPerProducer], r_src[kColsPerProducer];
-    float r_sc[kColsPerProducer];
-    auto fetch = [&](int it) {
-      tab = item_tab[it];
-      const int b0 = item_begin[it];
-      ncol = item_cnt[it];
+  if (tid >= kEpilogue + kProducers) {
+    // MMA issuer
+    if (lane == 0) {
+      int cur_tsl = -1, issued = 0;
+      bool ok = true;
+      for (int it = i0; it < i1; ++it) {
+        const int li = it - i0, s = li % kStages, b = li % kAcc;
+        ok = mbar_wait(&bar_full[s], (li / kStages) & 1, kWaitTries);
+        if (ok && li >= kAcc) ok = mbar_wait(&bar_acce[b], ((li / kAcc) - 1) & 1, kWaitTries);
+        if (!ok) break;
+        tc_fence_after();
+        const int tsl = s_tsl[s], ncol = s_icol[s];
+        // the previous table's last MMAs were issued before this point: release its slot
+        if (cur_tsl >= 0 && tsl != cur_tsl) tc_commit(&bar_tfree[cur_tsl]);
+        cur_tsl = tsl;
+        const int npad = (ncol + 15) & ~15;
+        const uint32_t idesc = make_idesc_f16_f32(kRows, npad);
+        constexpr uint32_t SBO_T = D::KP * 16;
+        const uint32_t bBase = smem_u32(sB + s * D::B_BYTES);
+        const uint32_t aH = smem_u32(sT + tsl * D::TAB_BYTES), aL = aH + kRows * D::KP * 2;
+        const uint32_t dt = tbase + (uint32_t)(b * kAccCols);
+        // descriptors of the item's operands; every MMA's start address is a compile-time
+        // offset from them (the address field counts 16-byte units and cannot carry: shared
+        // memory is below 256 KB)
+        const uint64_t dAh = make_smem_desc(aH, 128, SBO_T), dAl = make_smem_desc(aL, 128, SBO_T);
+        const uint64_t dB = make_smem_desc_sw128(bBase, 1024);
 #pragma unroll
-      for (int e = 0; e < kColsPerProducer; ++e) {
-        const int c = pt + e * kProducers;
-        r_slot[e] = c < ncol ? tc_pair[b0 + c] : 0;
-        r_src[e] = c < ncol ? tc_src[b0 + c] : 0;
+        for (int pass = 0; pass < 3; ++pass) {
+          const uint64_t a0 = pass == 2 ? dAl : dAh;                                     // T: hi, hi, lo
+          const uint64_t b0 = dB + (pass == 1 ? (uint64_t)((D::KA * D::REGION) >> 4) : 0);  // rows: hi, lo, hi
+#pragma unroll
+          for (int k = 0; k < D::KP / 16; ++k)
+            tc_mma_f16(dt, a0 + (uint64_t)(16 * k), b0 + (uint64_t)((((k >> 2) * D::REGION) + (k & 3) * 32) >> 4), idesc,
+                       (pass > 0 || k > 0) ? 1u : 0u);
+        }
+        tc_commit(&bar_bfree[s]);
+        tc_commit(&bar_accf[b]);
+        ++issued;
       }
-#pragma unroll
-      for (int e = 0; e < kColsPerProducer; ++e) r_sc[e] = (pt + e * kProducers) < ncol ? escale[r_src[e]] : 0.f;
+      if (!ok) {
+        atomicExch(err, 1);
+        // let MMAs already issued finish before the CTA leaves
+        if (issued > 0) mbar_wait(&bar_bfree[(issued - 1) % kStages], ((issued - 1) / kStages) & 1, kWaitTries);
+      }
+    }
+    __syncwarp();
+  } else if (tid >= kEpilogue) {
+    const int pt = tid - kEpilogue;  // producer thread = gathered row
+    int last_tab = -1, ntab_loaded = 0;
+    bool ok = true;
+    // metadata of the current item (c_) and of the next one (n_), loaded two items ahead;
+    // the items of a CTA are consecutive in work-item order, so each begins where the
+    // previous one ends
+    int c_tab = 0, c_b0 = 0, c_n = 0, c_src = 0, n_tab = 0, n_b0 = 0, n_n = 0, n_src = 0;
+    auto load_item = [&](int it, int b0, int& tb, int& n, int& src) {
+      tb = item_tab[it];
+      n = item_cnt[it];
+      src = tc_src[min(b0 + pt, npairs - 1)];
     };
-    if (i0 < i1) fetch(i0);
+    if (i0 < i1) {
+      c_b0 = item_begin[i0];
+      load_item(i0, c_b0, c_tab, c_n, c_src);
+    }
+    if (i0 + 1 < i1) {
+      n_b0 = c_b0 + c_n;
+      load_item(i0 + 1, n_b0, n_tab, n_n, n_src);
+    }
     for (int it = i0; it < i1; ++it) {
-      const int li = it - i0, b = li & 1;
-      if (ok && li > 0) ok = mbar_wait(&bar_free, (li - 1) & 1, kWaitTries);
-      if (ok && li > 1) ok = mbar_wait(&bar_acce[b], ((li >> 1) - 1) & 1, kWaitTries);
+      const int li = it - i0, s = li % kStages, b = li % kAcc;
+      const bool load_tab = c_tab != last_tab;
+      const int tsl = load_tab ? (ntab_loaded & 1) : ((ntab_loaded - 1) & 1);
+      if (ok && li >= kStages) ok = mbar_wait(&bar_bfree[s], ((li / kStages) - 1) & 1, kWaitTries);
+      if (ok && li >= kAcc) ok = mbar_wait(&bar_acce[b], ((li / kAcc) - 1) & 1, kWaitTries);
+      if (ok && load_tab && ntab_loaded >= 2) ok = mbar_wait(&bar_tfree[tsl], ((ntab_loaded >> 1) - 1) & 1, kWaitTries);
       if (named_bar_or(1, kProducers, ok ? 0 : 1)) {
         ok = false;
         break;
       }
-#pragma unroll
-      for (int e = 0; e < kColsPerProducer; ++e) {
-        const int c = pt + e * kProducers;
-        if (c < ncol) {
-          s_row[c] = r_src[e];
-          s_sc[b][c] = r_sc[e];
-          s_slot[b][c] = r_slot[e];
-        }
-      }
-      const int cur_tab = tab, cur_ncol = ncol;
+      if (pt < c_n) s_row[pt] = c_src;
+      const int cur_tab = c_tab, cur_ncol = c_n;
       const int nquad = (cur_ncol + 3) >> 2;
-      const bool load_tab = cur_tab != last_tab;
+      if (load_tab) ++ntab_loaded;
       last_tab = cur_tab;
       if (pt == 0) {
         s_ncol[b] = cur_ncol;
+        s_b0[b] = c_b0;
+        s_tsl[s] = tsl;
+        s_icol[s] = cur_ncol;
         const uint32_t bytes = (load_tab ? (uint32_t)D::TAB_BYTES : 0u) + (uint32_t)nquad * 4u * 128u * 2u * D::KA;
-        mbar_arrive_expect_tx(&bar_full, bytes);
+        mbar_arrive_expect_tx(&bar_full[s], bytes);
       }
       named_bar_sync(1, kProducers);
       if (pt == 0) {
         mbar_arrive(&bar_meta[b]);
-        if (load_tab) bulk_copy_g2s(sT, reinterpret_cast<const unsigned char*>(Ttab) + (size_t)cur_tab * D::TAB_BYTES, D::TAB_BYTES, &bar_full);
+        if (load_tab)
+          bulk_copy_g2s(sT + tsl * D::TAB_BYTES, reinterpret_cast<const unsigned char*>(Ttab) + (size_t)cur_tab * D::TAB_BYTES,
+                        D::TAB_BYTES, &bar_full[s]);
       }
       // gather4: quad q of rows, part (hi/lo), atom a -> region (part, a), rows 4q..4q+3
+      unsigned char* sBs = sB + s * D::B_BYTES;
       for (int g = pt; g < nquad * 2 * D::KA; g += kProducers) {
         const int q = g / (2 * D::KA), pa = g - q * (2 * D::KA);
         const int part = pa / D::KA, a = pa - part * D::KA;
         int y[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int c = min(4 * q + i, cur_ncol - 1);
-          y[i] = s_row[c] * 2 + part;
-        }
-        tma_gather4(sB + (part * D::KA + a) * D::REGION + q * 4 * 128, &rows_map, a * 64, y[0], y[1], y[2], y[3], &bar_full);
+        for (int i = 0; i < 4; ++i) y[i] = s_row[min(4 * q + i, cur_ncol - 1)] * 2 + part;
+        tma_gather4(sBs + (part * D::KA + a) * D::REGION + q * 4 * 128, &rows_map, a * 64, y[0], y[1], y[2], y[3], &bar_full[s]);
       }
-      if (it + 1 < i1) fetch(it + 1);  // next item's metadata while this one loads and runs
-      if (pt == 0) {
-        if (mbar_wait(&bar_full, li & 1, kWaitTries)) {
-          tc_fence_after();
-          const int npad = (cur_ncol + 15) & ~15;
-          const uint32_t idesc = make_idesc_f16_f32(kRows, npad);
-          constexpr uint32_t SBO_T = D::KP * 16;
-          const uint32_t bBase = smem_u32(sB);
-          const uint32_t aH = smem_u32(sT), aL = aH + kRows * D::KP * 2;
-          const uint32_t dt = tbase + (uint32_t)(b * 256);
-#pragma unroll 1
-          for (int pass = 0; pass < 3; ++pass) {
-            const uint32_t aT = pass == 2 ? aL : aH;  // T: hi, hi, lo
-            const int bpart = pass == 1 ? 1 : 0;     // rows: hi, lo, hi
-#pragma unroll 1
-            for (int k = 0; k < D::KP / 16; ++k) {
-              const uint32_t baddr = bBase + (uint32_t)((bpart * D::KA + (k >> 2)) * D::REGION) + (uint32_t)((k & 3) * 32);
-              tc_mma_f16(dt, make_smem_desc(aT + 256 * k, 128, SBO_T), make_smem_desc_sw128(baddr, 1024), idesc,
-                         (pass > 0 || k > 0) ? 1u : 0u);
-            }
-          }
-          tc_commit(&bar_free);
-          tc_commit(&bar_accf[b]);
-          ++issued;
-        } else {
-          ok = false;  // the other producers learn of it at the next vote
-        }
+      c_tab = n_tab;
+      c_b0 = n_b0;
+      c_n = n_n;
+      c_src = n_src;
+      if (it + 2 < i1) {
+        n_b0 = c_b0 + c_n;
+        load_item(it + 2, n_b0, n_tab, n_n, n_src);
       }
     }
     if (!ok) atomicExch(err, 1);
-    // on an early exit, let MMAs already issued finish before the CTA leaves
-    if (pt == 0 && !ok && issued > 0) mbar_wait(&bar_free, (issued - 1) & 1, kWaitTries);
   } else {
     const int quad = warp & 3, half = warp >> 2;
     const int i = quad * 32 + lane;  // output coefficient of this thread's TMEM lane
     const uint32_t lane_base = tbase + ((uint32_t)(quad * 32) << 16);
     for (int it = i0; it < i1; ++it) {
-      const int li = it - i0, b = li & 1;
-      bool ok = mbar_wait(&bar_meta[b], (li >> 1) & 1, kWaitTries);
-      if (ok) ok = mbar_wait(&bar_accf[b], (li >> 1) & 1, kWaitTries);
+      const int li = it - i0, b = li % kAcc;
+      bool ok = mbar_wait(&bar_meta[b], (li / kAcc) & 1, kWaitTries);
+      if (ok) ok = mbar_wait(&bar_accf[b], (li / kAcc) & 1, kWaitTries);
       if (!__all_sync(0xffffffffu, ok ? 1 : 0)) {
         if (lane == 0) atomicExch(err, 1);
         break;
       }
       tc_fence_after();
       const int ncol = s_ncol[b];
+      float* Yb = Y + (size_t)s_b0[b] * D::KP + i;
       if (quad * 32 < D::KP) {
-        const uint32_t col0 = (uint32_t)(b * 256);
+        const uint32_t col0 = (uint32_t)(b * kAccCols);
         uint32_t ra[32], rb[32];
         int c0 = half * 32;
         if (c0 < ncol) {
@@ -373,7 +410,7 @@ __global__ void __launch_bounds__(kEpilogue + kProducers, 1)
 #pragma unroll
           for (int q = 0; q < 32; ++q) {
             const int j = cbase + q;
-            if (j < ncol) Y[(size_t)s_slot[b][j] * D::KP + i] = __uint_as_float(r[q]) * s_sc[b][j];
+            if (j < ncol) Yb[(size_t)j * D::KP] = __uint_as_float(r[q]);
           }
         };
         while (c0 < ncol) {
@@ -398,22 +435,24 @@ __global__ void __launch_bounds__(kEpilogue + kProducers, 1)
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    tmem_dealloc(tbase, 512);
+    tmem_dealloc(tbase, kAcc * kAccCols);
   }
 }
 
-// Per target bucket: L[0] = sum of its slots (target-major CSR order, deterministic), back to
-// the FP64 complex layout [node][density][NC] with the normalisation and a_t^{n+1} undone;
-// L[1] stays zero (the combined density carries both; L is cleared before the M2L).
-// One warp per target: lane l sums real coefficients [l*V, l*V+V) of every slot with vector
-// loads (a warp reads one whole slot row per instruction), four slots in flight.
+// Per target bucket: L[0] = sum of its pair partials (target-major CSR order of the pairs,
+// deterministic), each with its source's column scale undone, back to the FP64 complex
+// layout [node][density][NC] with the normalisation and a_t^{n+1} undone; L[1] stays zero
+// (the combined density carries both; L is cleared before the M2L).  One warp per target:
+// lane l sums real coefficients [l*V, l*V+V) of every partial with vector loads (a warp
+// reads one whole partial row per instruction), four partials in flight.
 template <int P>
 __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, const int* __restrict__ m2l_off,
+                                const int* __restrict__ m2l_src, const int* __restrict__ pos, const float* __restrict__ escale,
                                 const double* __restrict__ node_dL, const double* __restrict__ alpha, const float* __restrict__ Y,
                                 double2* __restrict__ L) {
   using D = TcDims<P>;
   constexpr int NC = ncoef(P), V = D::KP / 32;
-  static_assert(V == 2 || V == 4, "slot rows of 64 or 128 floats");
+  static_assert(V == 2 || V == 4, "partial rows of 64 or 128 floats");
   const int lane = threadIdx.x & 31;
   const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   for (int ti = w0; ti < ntargets; ti += nw) {
@@ -423,7 +462,7 @@ __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, c
 #pragma unroll
     for (int v = 0; v < V; ++v) acc[v] = 0.0;
     auto load = [&](int k, float out[V]) {
-      const float* row = Y + (size_t)k * D::KP + lane * V;
+      const float* row = Y + (size_t)pos[k] * D::KP + lane * V;
       if constexpr (V == 4) {
         const float4 q = __ldcs(reinterpret_cast<const float4*>(row));
         out[0] = q.x; out[1] = q.y; out[2] = q.z; out[3] = q.w;
@@ -439,14 +478,16 @@ __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, c
       load(k + 1, a1);
       load(k + 2, a2);
       load(k + 3, a3);
+      const double s0 = escale[m2l_src[k]], s1 = escale[m2l_src[k + 1]], s2 = escale[m2l_src[k + 2]], s3 = escale[m2l_src[k + 3]];
 #pragma unroll
-      for (int v = 0; v < V; ++v) acc[v] += ((double)a0[v] + (double)a1[v]) + ((double)a2[v] + (double)a3[v]);
+      for (int v = 0; v < V; ++v) acc[v] += ((double)a0[v] * s0 + (double)a1[v] * s1) + ((double)a2[v] * s2 + (double)a3[v] * s3);
     }
     for (; k < k1; ++k) {
       float a0[V];
       load(k, a0);
+      const double s0 = escale[m2l_src[k]];
 #pragma unroll
-      for (int v = 0; v < V; ++v) acc[v] += (double)a0[v];
+      for (int v = 0; v < V; ++v) acc[v] += (double)a0[v] * s0;
     }
     const double a = node_dL[tgt];
     double* Lr = reinterpret_cast<double*>(L + (size_t)tgt * 2 * NC);
@@ -482,13 +523,15 @@ int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts, int nd) {
     const int grid = a.n_tc_items < a.tc_grid ? a.n_tc_items : a.tc_grid;
     CUtensorMap map;
     std::memcpy(&map, a.tc_rows_map, sizeof(map));
-    k_m2l_tc<P><<<grid, kEpilogue + kProducers, D::SMEM, st>>>(map, a.n_tc_items, a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt, a.tc_pair, a.tc_src,
-                                             static_cast<const __half*>(a.tc_tab), a.tc_escale, a.tc_Y, a.tc_err);
+    k_m2l_tc<P><<<grid, kEpilogue + kProducers + kIssuer, D::SMEM, st>>>(map, a.n_tc_items, a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt,
+                                                                         a.n_tc_pairs, a.tc_src, static_cast<const __half*>(a.tc_tab),
+                                                                         static_cast<const __half*>(a.tc_Mt), a.tc_Y, a.tc_err);
     ++launches;
   }
   if (parts & TC_REDUCE) {
     const int gr = (int)std::min<int64_t>(((int64_t)a.n_m2l_targets * 32 + 255) / 256, 148 * 16);
-    k_m2l_tc_reduce<P><<<gr, 256, 0, st>>>(a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.node_dL, a.tc_alpha, a.tc_Y, a.L);
+    k_m2l_tc_reduce<P><<<gr, 256, 0, st>>>(a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.m2l_src, a.tc_pos, a.tc_escale, a.node_dL,
+                                           a.tc_alpha, a.tc_Y, a.L);
     ++launches;
   }
   return launches;

@@ -304,13 +304,18 @@ def main():
     dev_s = e2e_s = plan_s = upload_s = 0.0
     launches = h2d = d2h = iters = mv = mv_lo = 0
     converged = True
+    steps_detail = []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             w0 = time.perf_counter()
             bvp.setup()
+            w1 = time.perf_counter()
             bvp.solve(kv)
-            e2e_s += time.perf_counter() - w0
+            w2 = time.perf_counter()
+            e2e_s += w2 - w0
             st = bvp.stats
+            steps_detail.append({"setup_wall_ms": 1e3 * (w1 - w0), "solve_wall_ms": 1e3 * (w2 - w1),
+                                 "device_ms": 1e3 * st.time_device_s})
             dev_s += st.time_device_s
             plan_s += st.time_plan_s
             upload_s += st.time_upload_s
@@ -377,6 +382,7 @@ def main():
         "e2e": {"value": world * args.steps / e2e_max, "unit": "solves/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "gpu_launches": launches,
+        "steps_detail": steps_detail,
         "roofline": roof,
         "clocks": clk.summary(),
     }
