@@ -100,6 +100,7 @@ struct bem_gpu_ctx {
   DBuf<double2> p2m_C;                       // [(leaf, DOF)][NC]
   DBuf<double2> near_scratch;                // element values of the near-weight kernel
   DBuf<int> e_dof, e_vtx, node_fb, node_fe, leaves, level_parents, child_begin, child_end, node_children;
+  DBuf<int> node_parent, node_level, m2m_nsig, m2m_cnt;
   DBuf<int> m2l_targets, m2l_off, m2l_src, nb_dofs, nb_targets, nb_ranges, dof_inc_off, dof_inc;
   DBuf<int> block_of_point, row_of_point, self_col;  // right-Jacobi inputs
   DBuf<int> point_dof_off, point_dof, dof_kind, dof_point;
@@ -186,6 +187,11 @@ struct bem_gpu_ctx {
     a.child_end = child_end.p;
     a.node_children = node_children.p;
     a.Ftab = Ftab.p;
+    a.node_parent = node_parent.p;
+    a.node_level = node_level.p;
+    a.m2m_nsig = m2m_nsig.p;
+    a.m2m_cnt = m2m_cnt.p;
+
     a.n_m2l_targets = n_m2l_targets;
     a.m2l_targets = m2l_targets.p;
     a.m2l_off = m2l_off.p;
@@ -598,6 +604,26 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   CK(up(ctx, ctx->child_end, ce));
   CK(up(ctx, ctx->node_children, P.node_children));
   CK(up(ctx, ctx->leaves, P.leaves));
+  {  // upward pass: parent, Ftab row and the number of children whose multipole completes
+    std::vector<int> par(nb, -1), lev(nb, 0), nsig(nb, 0);
+    std::vector<char> sig(nb, 0), leaf(nb, 0);
+    for (int l : P.leaves) leaf[l] = 1;
+    for (int l = 0; l < (int)P.level_nodes.size(); ++l)
+      for (int i : P.level_nodes[l]) lev[i] = l;
+    for (int i = 0; i < nb; ++i)
+      for (int ci = P.nodes[i].child_begin; ci < P.nodes[i].child_end; ++ci) par[P.node_children[ci]] = i;
+    // a child signals its parent if it is a leaf (its multipole comes from the P2M) or if one of
+    // its own children signals it; deepest levels first
+    for (int l = (int)P.level_nodes.size() - 1; l >= 0; --l)
+      for (int i : P.level_nodes[l]) {
+        sig[i] = leaf[i] || nsig[i] > 0;
+        if (sig[i] && par[i] >= 0) ++nsig[par[i]];
+      }
+    CK(up(ctx, ctx->node_parent, par));
+    CK(up(ctx, ctx->node_level, lev));
+    CK(up(ctx, ctx->m2m_nsig, nsig));
+    CK(ctx->m2m_cnt.alloc(std::max(nb, 1)));
+  }
   CK(up(ctx, ctx->level_parents, lp));
   CK(up(ctx, ctx->m2l_targets, mt));
   CK(up(ctx, ctx->m2l_off, P.m2l_off));
@@ -755,6 +781,7 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   CK(cudaMemsetAsync(ctx->GPhin.p, 0, sizeof(double) * P.np, s));
   CK(cudaMemsetAsync(ctx->GnPhi.p, 0, sizeof(double) * P.np, s));
   CK(cudaMemsetAsync(ctx->M.p, 0, sizeof(double2) * ctx->M.n, s));
+  CK(cudaMemsetAsync(ctx->m2m_cnt.p, 0, sizeof(int) * ctx->m2m_cnt.n, s));
   CK(cudaMemsetAsync(ctx->p2m_C.p, 0, sizeof(double2) * ctx->p2m_C.n, s));
   launch_s_tables(P.opt.p, (int)P.grp_off.size() - 1, ctx->grp_vec.p, ctx->Sg.p, s);
   ctx->launches += 1;

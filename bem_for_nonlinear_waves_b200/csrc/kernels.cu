@@ -3,7 +3,8 @@
 // Per mat-vec (return_A_dot_v, bem/BEM_solveBVP_GMRES_FMM.hpp:2124-2155):
 //   k_densities   per-DOF phi/phin from the unknown vector (setUnknowns/setKnowns, :1142-1176)
 //   k_p2m         leaf multipoles from the 6 Dunavant points of every element (moments.hpp:307-368)
-//   k_m2m         one launch per level, bottom-up (moments.hpp:419-436, 912-915)
+//   k_m2m_up      the whole upward pass in one launch, parents completed by arrival counts
+//                 (moments.hpp:419-436, 912-915)
 //   k_m2l         every M2L pair of every level in one launch (moments.hpp:732-764)
 //   k_l2l         one launch per level, top-down (moments.hpp:869-884, 925-929)
 //   k_targets     near-field block SpMV + L2P + BIE rows (compute_Ax_minus_b, :34-158)
@@ -259,38 +260,7 @@ __global__ void k_p2m_apply(const int* __restrict__ leaves, const int* __restric
   M[(size_t)leaf * 2 * NC + t] = acc;
 }
 
-// expand half-stored coefficients [2][NC] into full [2][(P+1)^2]
-template <int P, int ND>
-__device__ __forceinline__ void expand_full(const double2* __restrict__ src, double2* dst) {
-  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
-  for (int t = threadIdx.x; t < ND * NF; t += blockDim.x) {
-    const int d = t / NF, i = t % NF;
-    int n = 0;
-    while ((n + 1) * (n + 1) <= i) ++n;
-    const int m = i - n * (n + 1);
-    double2 v = src[d * NC + cidx(n, m < 0 ? -m : m)];
-    if (m < 0) v = ((-m) & 1) ? make_double2(-v.x, v.y) : make_double2(v.x, -v.y);
-    dst[t] = v;
-  }
-}
-
-
 // ---------------------------------------------------------------------------
-// warp-level expansion of half-stored coefficients [2][NC] into full [2][(P+1)^2]
-template <int P, int ND>
-__device__ __forceinline__ void expand_full_warp(const double2* __restrict__ src, double2* dst, int lane) {
-  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
-  for (int t = lane; t < ND * NF; t += 32) {
-    const int d = t / NF, i = t % NF;
-    int n = 0;
-    while ((n + 1) * (n + 1) <= i) ++n;
-    const int m = i - n * (n + 1);
-    double2 v = src[d * NC + cidx(n, m < 0 ? -m : m)];
-    if (m < 0) v = ((-m) & 1) ? make_double2(-v.x, v.y) : make_double2(v.x, -v.y);
-    dst[t] = v;
-  }
-}
-
 // Parent-to-child translation tables.  A child bucket sits at one of eight offsets from its
 // parent, the same on a level up to rounding, so F(c - c') is tabulated once per (level,
 // octant) at set-up; the tree passes read the table instead of running the recurrence.
@@ -306,82 +276,178 @@ __device__ __forceinline__ int child_octant(const double* __restrict__ node_X, i
          (node_X[3 * c + 2] > node_X[3 * par + 2] ? 4 : 0);
 }
 
-// M2M: one block of 8 warps per parent, warp w translating child w (lane per output
-// coefficient); the children's partial multipoles are summed in child order.  The upward
-// pass is level by level, so the time of one block is the time of a level: splitting the
-// children over warps shortens it eightfold against one thread per coefficient looping over
-// the children.
-constexpr int kTreeWarps = 8;
-// warps of the M2M block: 8 while the per-warp tables fit the 48 KB of static shared memory
+// Tree translations with a thread per output coefficient.  A translation of order P has
+// (P+1)(P+2)/2 output coefficients of up to ~(P+1)^2/2 terms each; a block runs kTreeGroups
+// translations side by side, each by a group of coefficient threads, and every thread sums
+// its terms in two interleaved chains so that consecutive multiply-adds do not wait on one
+// another.
+constexpr int kTreeGroups = 4;
 template <int P>
-constexpr int m2m_warps() { return kTreeWarps * 3 * (P + 1) * (P + 1) * 16 <= 48 * 1024 ? kTreeWarps : kTreeWarps / 2; }
+constexpr int tree_group_threads() { return (ncoef(P) + 31) / 32 * 32; }
 
+// one output coefficient (n, m) of an M2M shift: sum conj(F_{n1}^{m1}) M_{n-n1}^{m-m1}
 template <int P, int ND>
-__global__ void __launch_bounds__(32 * m2m_warps<P>()) k_m2m(const int* __restrict__ parents, const int* __restrict__ child_begin,
-                                                       const int* __restrict__ child_end, const int* __restrict__ node_children,
-                                                       const double* __restrict__ node_X, const double2* __restrict__ Ftab,
-                                                       double2* __restrict__ M) {
-  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), R = (NC + 31) / 32, W = m2m_warps<P>();
-  __shared__ double2 sbuf[W * 3 * NF];  // per warp: F [NF], child multipole [2][NF]
-  const int par = parents[blockIdx.x];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double2* sF = sbuf + warp * 3 * NF;
-  double2* sM = sF + NF;
-  double2 acc[R][2];
-#pragma unroll
-  for (int r = 0; r < R; ++r) acc[r][0] = acc[r][1] = make_double2(0.0, 0.0);
-  const int cb = child_begin[par], ce = child_end[par];
-  for (int ci = cb + warp; ci < ce; ci += W) {
-    const int c = node_children[ci];
-    const double2* Ft = Ftab + (size_t)child_octant(node_X, c, par) * NF;
-    for (int i = lane; i < NF; i += 32) sF[i] = Ft[i];
-    expand_full_warp<P, ND>(M + (size_t)c * 2 * NC, sM, lane);
-    __syncwarp();
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int t = lane + 32 * r;
-      if (t < NC) {
-        int n, m;
-        decode_nm(t, n, m);
-        double2 a0 = acc[r][0], a1 = acc[r][1];
-        for (int n1 = 0; n1 <= n; ++n1) {
-          const int n2 = n - n1;
-          const int lo = max(-n1, m - n2), hi = min(n1, m + n2);
-          for (int m1 = lo; m1 <= hi; ++m1) {
-            const double2 f = sF[n1 * (n1 + 1) + m1];
-            const int i2 = n2 * (n2 + 1) + (m - m1);
-            const double2 x0 = sM[i2];
-            // conj(f) * x
-            a0.x += f.x * x0.x + f.y * x0.y;
-            a0.y += f.x * x0.y - f.y * x0.x;
-            if (ND == 2) {
-              const double2 x1 = sM[NF + i2];
-              a1.x += f.x * x1.x + f.y * x1.y;
-              a1.y += f.x * x1.y - f.y * x1.x;
-            }
-          }
-        }
-        acc[r][0] = a0;
-        acc[r][1] = a1;
+__device__ __forceinline__ void m2m_coef(int n, int m, const double2* __restrict__ sF, const double2* __restrict__ sM, double2& o0,
+                                         double2& o1) {
+  constexpr int NF = (P + 1) * (P + 1);
+  double2 a0 = make_double2(0.0, 0.0), a1 = a0, b0 = a0, b1 = a0;
+  for (int n1 = 0; n1 <= n; ++n1) {
+    const int n2 = n - n1;
+    const int lo = max(-n1, m - n2), hi = min(n1, m + n2);
+    const double2* f = sF + n1 * (n1 + 1);
+    const double2* x = sM + n2 * (n2 + 1) + m;
+    int m1 = lo;
+    for (; m1 < hi; m1 += 2) {
+      const double2 f0 = f[m1], f1 = f[m1 + 1];
+      const double2 x0 = x[-m1], y0 = x[-m1 - 1];
+      a0.x += f0.x * x0.x + f0.y * x0.y;
+      a0.y += f0.x * x0.y - f0.y * x0.x;
+      b0.x += f1.x * y0.x + f1.y * y0.y;
+      b0.y += f1.x * y0.y - f1.y * y0.x;
+      if (ND == 2) {
+        const double2 x1 = x[NF - m1], y1 = x[NF - m1 - 1];
+        a1.x += f0.x * x1.x + f0.y * x1.y;
+        a1.y += f0.x * x1.y - f0.y * x1.x;
+        b1.x += f1.x * y1.x + f1.y * y1.y;
+        b1.y += f1.x * y1.y - f1.y * y1.x;
       }
     }
-    __syncwarp();
-  }
-  __syncthreads();
-  double2* part = sbuf;  // [warp][2][NC] partial multipoles
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int t = lane + 32 * r;
-    if (t < NC) {
-      part[warp * 2 * NC + t] = acc[r][0];
-      if (ND == 2) part[warp * 2 * NC + NC + t] = acc[r][1];
+    if (m1 == hi) {
+      const double2 f0 = f[m1], x0 = x[-m1];
+      a0.x += f0.x * x0.x + f0.y * x0.y;
+      a0.y += f0.x * x0.y - f0.y * x0.x;
+      if (ND == 2) {
+        const double2 x1 = x[NF - m1];
+        a1.x += f0.x * x1.x + f0.y * x1.y;
+        a1.y += f0.x * x1.y - f0.y * x1.x;
+      }
     }
   }
-  __syncthreads();
-  for (int t = threadIdx.x; t < ND * NC; t += blockDim.x) {
-    double2 s = part[t];
-    for (int w = 1; w < W; ++w) s = cadd(s, part[w * 2 * NC + t]);
-    M[(size_t)par * 2 * NC + t] = s;
+  o0 = cadd(o0, cadd(a0, b0));
+  if (ND == 2) o1 = cadd(o1, cadd(a1, b1));
+}
+
+// one output coefficient (k, j) of an L2L shift: sum_{n>=k} L_n^m conj(F_{n-k}^{m-j})
+template <int P, int ND>
+__device__ __forceinline__ void l2l_coef(int k, int j, const double2* __restrict__ sF, const double2* __restrict__ sL, double2& o0,
+                                         double2& o1) {
+  constexpr int NF = (P + 1) * (P + 1);
+  double2 a0 = make_double2(0.0, 0.0), a1 = a0, b0 = a0, b1 = a0;
+  for (int n = k; n <= P; ++n) {
+    const int dn = n - k;
+    const int lo = max(-n, j - dn), hi = min(n, j + dn);
+    const double2* f = sF + dn * (dn + 1) - j;
+    const double2* x = sL + n * (n + 1);
+    int m = lo;
+    for (; m < hi; m += 2) {
+      const double2 f0 = f[m], f1 = f[m + 1];
+      const double2 x0 = x[m], y0 = x[m + 1];
+      a0.x += x0.x * f0.x + x0.y * f0.y;
+      a0.y += x0.y * f0.x - x0.x * f0.y;
+      b0.x += y0.x * f1.x + y0.y * f1.y;
+      b0.y += y0.y * f1.x - y0.x * f1.y;
+      if (ND == 2) {
+        const double2 x1 = x[NF + m], y1 = x[NF + m + 1];
+        a1.x += x1.x * f0.x + x1.y * f0.y;
+        a1.y += x1.y * f0.x - x1.x * f0.y;
+        b1.x += y1.x * f1.x + y1.y * f1.y;
+        b1.y += y1.y * f1.x - y1.x * f1.y;
+      }
+    }
+    if (m == hi) {
+      const double2 f0 = f[m], x0 = x[m];
+      a0.x += x0.x * f0.x + x0.y * f0.y;
+      a0.y += x0.y * f0.x - x0.x * f0.y;
+      if (ND == 2) {
+        const double2 x1 = x[NF + m];
+        a1.x += x1.x * f0.x + x1.y * f0.y;
+        a1.y += x1.y * f0.x - x1.x * f0.y;
+      }
+    }
+  }
+  o0 = cadd(o0, cadd(a0, b0));
+  if (ND == 2) o1 = cadd(o1, cadd(a1, b1));
+}
+
+// half-stored [ND][NC] -> full [ND][(P+1)^2] by the threads [0, nthr) of a group
+template <int P, int ND, bool kThroughL2>
+__device__ __forceinline__ void expand_full_group(const double2* __restrict__ src, double2* dst, int tid, int nthr) {
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
+  for (int t = tid; t < ND * NF; t += nthr) {
+    const int d = t / NF, i = t % NF;
+    int n = 0;
+    while ((n + 1) * (n + 1) <= i) ++n;
+    const int m = i - n * (n + 1);
+    const double2* q = src + d * NC + cidx(n, m < 0 ? -m : m);
+    double2 v = kThroughL2 ? __ldcg(q) : *q;
+    if (m < 0) v = ((-m) & 1) ? make_double2(-v.x, v.y) : make_double2(v.x, -v.y);
+    dst[t] = v;
+  }
+}
+
+// M2M: the upward pass in one launch.  A block starts at a leaf and climbs: after the
+// multipole of its node is complete it counts the node in at the parent (a counter per
+// node), and the block whose count completes the parent computes the parent's multipole
+// (group g translating children g, g + 4, ...; partial multipoles summed in group order,
+// so the result does not depend on which block arrives last), then climbs on.  Nothing
+// waits: a block that does not complete its parent stops.  The last arrival resets the
+// parent's counter, so every launch starts from zero.  Children's multipoles written by
+// other blocks of the launch are read through L2.
+template <int P, int ND>
+__global__ void __launch_bounds__(kTreeGroups * tree_group_threads<P>()) k_m2m_up(
+    const int* __restrict__ leaves, const int* __restrict__ node_parent, const int* __restrict__ node_level,
+    const int* __restrict__ nsig, int* __restrict__ cnt, const int* __restrict__ child_begin, const int* __restrict__ child_end,
+    const int* __restrict__ node_children, const double* __restrict__ node_X, const double2* __restrict__ Ftab, double2* __restrict__ M) {
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), G = kTreeGroups, GT = tree_group_threads<P>();
+  __shared__ double2 sF[G][NF];
+  __shared__ double2 sM[G][ND * NF];
+  __shared__ double2 part[G][ND * NC];
+  __shared__ int s_go;
+  const int g = threadIdx.x / GT, t = threadIdx.x - g * GT;
+  int n = 0, m = 0;
+  if (t < NC) decode_nm(t, n, m);
+  int node = leaves[blockIdx.x];
+  for (;;) {
+    const int par = node_parent[node];
+    if (par < 0) return;
+    __threadfence();  // this node's multipole (written by this block, or by the P2M launch) before the count
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int go = atomicAdd(&cnt[par], 1) == nsig[par] - 1;
+      if (go) {
+        cnt[par] = 0;
+        __threadfence();
+      }
+      s_go = go;
+    }
+    __syncthreads();
+    if (!s_go) return;
+    const double2* Fl = Ftab + (size_t)node_level[par] * 8 * NF;
+    const int cb = child_begin[par], ce = child_end[par];
+    double2 o0 = make_double2(0.0, 0.0), o1 = o0;
+    for (int c0 = cb; c0 < ce; c0 += G) {
+      const int ci = c0 + g;
+      if (ci < ce) {
+        const int c = node_children[ci];
+        const double2* Ft = Fl + (size_t)child_octant(node_X, c, par) * NF;
+        for (int i = t; i < NF; i += GT) sF[g][i] = Ft[i];
+        expand_full_group<P, ND, true>(M + (size_t)c * 2 * NC, sM[g], t, GT);
+      }
+      __syncthreads();
+      if (ci < ce && t < NC) m2m_coef<P, ND>(n, m, sF[g], sM[g], o0, o1);
+      __syncthreads();
+    }
+    if (t < NC) {
+      part[g][t] = o0;
+      if (ND == 2) part[g][NC + t] = o1;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < ND * NC; i += blockDim.x) {
+      double2 v = part[0][i];
+      for (int w = 1; w < G; ++w) v = cadd(v, part[w][i]);
+      M[(size_t)par * 2 * NC + i] = v;
+    }
+    node = par;
   }
 }
 
@@ -490,56 +556,39 @@ __global__ void k_m2l_reduce(int ntargets, const int* __restrict__ targets, cons
 }
 
 // ---------------------------------------------------------------------------
-// L2L: one block of 8 warps per parent, warp w shifting the parent's local expansion to
-// child w (lane per output coefficient): L'_k^j += sum_{n>=k} L_n^m conj(F_{n-k}^{m-j}).
+// L2L: one launch per level, top-down; block per parent, its expanded local expansion shared
+// by the groups, group g shifting it to children g, g + 4, ... (thread per output
+// coefficient): L'_k^j += sum_{n>=k} L_n^m conj(F_{n-k}^{m-j}).
 template <int P, int ND>
-__global__ void __launch_bounds__(32 * kTreeWarps) k_l2l(const int* __restrict__ parents, const int* __restrict__ child_begin,
-                                                       const int* __restrict__ child_end, const int* __restrict__ node_children,
-                                                       const double* __restrict__ node_X, const double2* __restrict__ Ftab,
-                                                       double2* __restrict__ L) {
-  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), R = (NC + 31) / 32;
-  __shared__ double2 sL[2 * NF];
-  __shared__ double2 sFw[kTreeWarps * NF];
+__global__ void __launch_bounds__(kTreeGroups * tree_group_threads<P>()) k_l2l(
+    const int* __restrict__ parents, const int* __restrict__ child_begin, const int* __restrict__ child_end,
+    const int* __restrict__ node_children, const double* __restrict__ node_X, const double2* __restrict__ Ftab,
+    double2* __restrict__ L) {
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), G = kTreeGroups, GT = tree_group_threads<P>();
+  __shared__ double2 sF[G][NF];
+  __shared__ double2 sL[ND * NF];
   const int par = parents[blockIdx.x];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  expand_full<P, ND>(L + (size_t)par * 2 * NC, sL);
-  __syncthreads();
-  double2* sF = sFw + warp * NF;
+  const int g = threadIdx.x / GT, t = threadIdx.x - g * GT;
+  int k = 0, j = 0;
+  if (t < NC) decode_nm(t, k, j);
+  expand_full_group<P, ND, false>(L + (size_t)par * 2 * NC, sL, threadIdx.x, blockDim.x);
   const int cb = child_begin[par], ce = child_end[par];
-  for (int ci = cb + warp; ci < ce; ci += kTreeWarps) {
-    const int c = node_children[ci];
-    const double2* Ft = Ftab + (size_t)child_octant(node_X, c, par) * NF;
-    for (int i = lane; i < NF; i += 32) sF[i] = Ft[i];
-    __syncwarp();
-    double2* dst = L + (size_t)c * 2 * NC;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int t = lane + 32 * r;
-      if (t < NC) {
-        int k, j;
-        decode_nm(t, k, j);
-        double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
-        for (int n = k; n <= P; ++n) {
-          const int dn = n - k;
-          const int lo = max(-n, j - dn), hi = min(n, j + dn);
-          for (int m = lo; m <= hi; ++m) {
-            const double2 f = sF[dn * (dn + 1) + (m - j)];
-            const double2 x0 = sL[n * (n + 1) + m];
-            // x * conj(f)
-            a0.x += x0.x * f.x + x0.y * f.y;
-            a0.y += x0.y * f.x - x0.x * f.y;
-            if (ND == 2) {
-              const double2 x1 = sL[NF + n * (n + 1) + m];
-              a1.x += x1.x * f.x + x1.y * f.y;
-              a1.y += x1.y * f.x - x1.x * f.y;
-            }
-          }
-        }
-        dst[t] = cadd(dst[t], a0);
-        if (ND == 2) dst[NC + t] = cadd(dst[NC + t], a1);
-      }
+  for (int c0 = cb; c0 < ce; c0 += G) {
+    const int ci = c0 + g;
+    const int c = ci < ce ? node_children[ci] : 0;
+    if (ci < ce) {
+      const double2* Ft = Ftab + (size_t)child_octant(node_X, c, par) * NF;
+      for (int i = t; i < NF; i += GT) sF[g][i] = Ft[i];
     }
-    __syncwarp();
+    __syncthreads();
+    if (ci < ce && t < NC) {
+      double2 o0 = make_double2(0.0, 0.0), o1 = o0;
+      l2l_coef<P, ND>(k, j, sF[g], sL, o0, o1);
+      double2* dst = L + (size_t)c * 2 * NC;
+      dst[t] = cadd(dst[t], o0);
+      if (ND == 2) dst[NC + t] = cadd(dst[NC + t], o1);
+    }
+    __syncthreads();
   }
 }
 
@@ -1045,15 +1094,12 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     k_p2m<P, ND><<<a.n_leaves, 128, 0, st>>>(a.leaves, a.node_fb, a.node_fe, a.node_X, a.e_q, a.e_W, a.e_n, a.e_dof, a.phi, a.phin, a.M);
     ++launches;
   }
-  if (stages & STAGE_M2M)
-    for (int l = a.n_levels - 1; l >= 0; --l) {
-      const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
-      if (cnt > 0) {
-        k_m2m<P, ND><<<cnt, 32 * m2m_warps<P>(), 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end,
-                                                          a.node_children, a.node_X, a.Ftab + (size_t)l * 8 * (P + 1) * (P + 1), a.M);
-        ++launches;
-      }
-    }
+  if ((stages & STAGE_M2M) && a.n_leaves > 0) {
+    k_m2m_up<P, ND><<<a.n_leaves, kTreeGroups * tree_group_threads<P>(), 0, st>>>(a.leaves, a.node_parent, a.node_level, a.m2m_nsig,
+                                                                                  a.m2m_cnt, a.child_begin, a.child_end, a.node_children,
+                                                                                  a.node_X, a.Ftab, a.M);
+    ++launches;
+  }
   if (stages & STAGE_M2L) {
     cudaMemsetAsync(a.L, 0, sizeof(double2) * 2 * NC * (size_t)a.n_nodes, st);
     if (a.use_tc) {
@@ -1072,8 +1118,9 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     for (int l = 0; l < a.n_levels; ++l) {
       const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
       if (cnt > 0) {
-        k_l2l<P, ND><<<cnt, 32 * kTreeWarps, 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin, a.child_end,
-                                                      a.node_children, a.node_X, a.Ftab + (size_t)l * 8 * (P + 1) * (P + 1), a.L);
+        k_l2l<P, ND><<<cnt, kTreeGroups * tree_group_threads<P>(), 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin,
+                                                                            a.child_end, a.node_children, a.node_X,
+                                                                            a.Ftab + (size_t)l * 8 * (P + 1) * (P + 1), a.L);
         ++launches;
       }
     }

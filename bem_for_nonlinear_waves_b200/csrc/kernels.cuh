@@ -33,6 +33,11 @@ struct MatvecArgs {
   const int* child_end = nullptr;
   const int* node_children = nullptr;
   const double2* Ftab = nullptr;           // [level][octant][(P+1)^2] parent-to-child F tables
+  const int* node_parent = nullptr;        // [n_nodes] parent bucket, -1 at the root
+  const int* node_level = nullptr;         // [n_nodes] level (row block of Ftab)
+  const int* m2m_nsig = nullptr;           // [n_nodes] children whose multipole completes in the upward pass
+  int* m2m_cnt = nullptr;                  // [n_nodes] upward-pass arrival counters (zero between launches)
+
   int n_m2l_targets = 0;
   const int* m2l_targets = nullptr;
   const int* m2l_off = nullptr;

@@ -360,6 +360,9 @@ def main():
                 "algorithmic_flops_per_launch": m2l_flops,
                 "tensor_flops_issued_per_launch": tree["m2l_pairs"] * 128.0 * kp * 2 * 3,
                 "kernel_ms": prof["m2l_contract"]}
+        if roof["traffic"]:  # the same launch against HBM: DRAM bytes (ncu) / CUDA-event time
+            roof["hbm_gbs_of_traffic"] = roof["traffic"] / t_k / 1e9
+            roof["hbm_frac_of_traffic"] = roof["hbm_gbs_of_traffic"] / peaks["hbm_gbs"]
     else:
         t_k = prof["m2l"] * 1e-3
         achieved = m2l_flops / t_k / 1e12
