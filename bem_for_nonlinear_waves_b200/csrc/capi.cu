@@ -112,6 +112,7 @@ struct bem_gpu_ctx {
   DBuf<double2> M, L;
   std::vector<int> level_parent_off;
   int n_m2l_targets = 0, max_ntgt = 0, chunk = 0;
+  int64_t w4_total = 0;  // size of the row-padded FP32 near weights
   // state
   DBuf<double> phi, phin, known_s, rows, GPhin, GnPhi;
   // graph-captured A.x : mv_in -> mv_out
@@ -566,9 +567,12 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   std::vector<NearBlockDev> bd(P.blocks.size());
   ctx->max_ntgt = 1;
   int max_ndof = 1;
+  int64_t w4_total = 0;
   for (size_t i = 0; i < P.blocks.size(); ++i) {
     const auto& b = P.blocks[i];
     bd[i].w_off = b.w_off;
+    bd[i].w4_off = w4_total;
+    w4_total += (int64_t)b.ntgt * ((b.ndof + 3) & ~3);
     bd[i].node = b.node;
     bd[i].dof_off = b.dof_off;
     bd[i].ndof = b.ndof;
@@ -579,13 +583,15 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     ctx->max_ntgt = std::max(ctx->max_ntgt, b.ntgt);
     max_ndof = std::max(max_ndof, b.ndof);
   }
+  ctx->w4_total = w4_total;
   // shared memory budget of k_targets: chunk of (phi, phin) + per-target sums
   const int smem_cap = 160 * 1024;
   if (ctx->max_ntgt * 16 > smem_cap / 2) {
     ctx->err = "too many targets in one bucket";
     return BEM_ERR_UNSUPPORTED;
   }
-  ctx->chunk = std::min(max_ndof, (smem_cap - ctx->max_ntgt * 16) / 16);
+  // a multiple of 4 columns (the FP32 rows are read 4 columns at a time)
+  ctx->chunk = std::min((max_ndof + 3) & ~3, ((smem_cap - ctx->max_ntgt * 16) / 16) & ~3);
   configure_targets_smem(P.opt.p, (ctx->chunk + ctx->max_ntgt) * 16);
   configure_m2l_smem(P.opt.p);
 
@@ -716,7 +722,7 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   CK(ctx->WG.alloc(std::max<int64_t>(P.nnz, 1)));
   CK(ctx->WGn.alloc(std::max<int64_t>(P.nnz, 1)));
   CK(ctx->Wc.alloc(std::max<int64_t>(P.nnz, 1)));
-  if (ctx->opts.precision == 1) CK(ctx->Wc32.alloc(std::max<int64_t>(P.nnz, 1)));
+  if (ctx->opts.precision == 1) CK(ctx->Wc32.alloc(std::max<int64_t>(ctx->w4_total, 1)));
   const int N = P.ndof;
   CK(ctx->phi.alloc(N));
   CK(ctx->phin.alloc(N));

@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
+#include <type_traits>
 
 #include "fmm_math.cuh"
 #include "kernels.cuh"
@@ -725,12 +726,35 @@ __global__ void __launch_bounds__(128) k_targets_ax(const NearBlockDev* __restri
   for (int c0 = 0; c0 < B.ndof; c0 += chunk) {
     const int cn = min(chunk, B.ndof - c0);
     __syncthreads();
-    for (int i = threadIdx.x; i < cn; i += blockDim.x) xs[i] = x[nb_dofs[B.dof_off + c0 + i]];
+    if constexpr (std::is_same<WT, float>::value) {
+      // four planes: column c at xs[(c % 4) * chunk / 4 + c / 4], so that the lanes reading
+      // consecutive groups of 4 columns hit consecutive words; the tail of the last group is 0
+      const int q = chunk >> 2, cn4 = (cn + 3) & ~3;
+      for (int i = threadIdx.x; i < cn4; i += blockDim.x) xs[(i & 3) * q + (i >> 2)] = i < cn ? x[nb_dofs[B.dof_off + c0 + i]] : 0.0;
+    } else {
+      for (int i = threadIdx.x; i < cn; i += blockDim.x) xs[i] = x[nb_dofs[B.dof_off + c0 + i]];
+    }
     __syncthreads();
     for (int tl = warp; tl < B.ntgt; tl += nwarp) {
-      const WT* w = Wc + B.w_off + (int64_t)tl * B.ndof + c0;
       double s0 = 0.0;
-      for (int i = lane; i < cn; i += 32) s0 = fma((double)w[i], xs[i], s0);
+      if constexpr (std::is_same<WT, float>::value) {
+        // padded rows: chunk and row starts are multiples of 4 columns, so 16-byte loads
+        const int stride = (B.ndof + 3) & ~3;
+        const float4* w4 = reinterpret_cast<const float4*>(Wc + B.w4_off + (int64_t)tl * stride + c0);
+        const int n4 = (cn + 3) >> 2, qs = chunk >> 2;
+        double s1 = 0.0;
+        for (int i = lane; i < n4; i += 32) {
+          const float4 q = __ldcs(w4 + i);
+          s0 = fma((double)q.x, xs[i], s0);
+          s1 = fma((double)q.y, xs[qs + i], s1);
+          s0 = fma((double)q.z, xs[2 * qs + i], s0);
+          s1 = fma((double)q.w, xs[3 * qs + i], s1);
+        }
+        s0 += s1;
+      } else {
+        const WT* w = Wc + B.w_off + (int64_t)tl * B.ndof + c0;
+        for (int i = lane; i < cn; i += 32) s0 = fma((double)w[i], xs[i], s0);
+      }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, o);
       if (lane == 0) accs[tl] += s0;
@@ -775,12 +799,22 @@ __global__ void __launch_bounds__(128) k_targets_ax(const NearBlockDev* __restri
 template <typename WT>
 __global__ void k_combine_weights(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs, const int* __restrict__ dof_kind,
                                   const double* __restrict__ WG, const double* __restrict__ WGn, WT* __restrict__ Wc) {
+  // the FP32 copy keeps each row padded with zeros to a multiple of 4 columns (16-byte rows
+  // for vector loads), from the block's own offset w4_off
+  constexpr bool kPad = std::is_same<WT, float>::value;
   const NearBlockDev B = blocks[blockIdx.x];
-  const int64_t total = (int64_t)B.ntgt * B.ndof;
+  const int stride = kPad ? (B.ndof + 3) & ~3 : B.ndof;
+  const int64_t base = kPad ? B.w4_off : B.w_off;
+  const int64_t total = (int64_t)B.ntgt * stride;
   for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
-    const int j = (int)(e % B.ndof);
-    const int64_t w = B.w_off + e;
-    Wc[w] = (WT)(dof_kind[nb_dofs[B.dof_off + j]] == 0 ? WG[w] : -WGn[w]);
+    const int64_t tl = e / stride;
+    const int j = (int)(e - tl * stride);
+    if (j < B.ndof) {
+      const int64_t w = B.w_off + tl * B.ndof + j;
+      Wc[base + e] = (WT)(dof_kind[nb_dofs[B.dof_off + j]] == 0 ? WG[w] : -WGn[w]);
+    } else {
+      Wc[base + e] = (WT)0;
+    }
   }
 }
 

@@ -7,7 +7,8 @@
 namespace bemb200 {
 
 struct NearBlockDev {
-  int64_t w_off;  // first weight of this block's rows
+  int64_t w_off;   // first weight of this block's rows
+  int64_t w4_off;  // same in the FP32 copy, whose rows are padded to a multiple of 4 columns
   int node;       // deepest bucket shared by the block's targets
   int dof_off, ndof;
   int tgt_off, ntgt;

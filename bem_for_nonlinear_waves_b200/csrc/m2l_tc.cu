@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
 // layout [node][density][NC] with the normalisation and a_t^{n+1} undone; L[1] stays zero
 // (the combined density carries both; L is cleared before the M2L).  One warp per target:
 // lane l sums real coefficients [l*V, l*V+V) of every partial with vector loads (a warp
-// reads one whole partial row per instruction), four partials in flight.
+// reads one whole partial row per instruction), eight partials in flight.
 template <int P>
 __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, const int* __restrict__ m2l_off,
                                 const int* __restrict__ m2l_src, const int* __restrict__ pos, const float* __restrict__ escale,
@@ -461,8 +461,8 @@ __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, c
     double acc[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) acc[v] = 0.0;
-    auto load = [&](int k, float out[V]) {
-      const float* row = Y + (size_t)pos[k] * D::KP + lane * V;
+    auto load = [&](int r, float out[V]) {
+      const float* row = Y + (size_t)r * D::KP + lane * V;
       if constexpr (V == 4) {
         const float4 q = __ldcs(reinterpret_cast<const float4*>(row));
         out[0] = q.x; out[1] = q.y; out[2] = q.z; out[3] = q.w;
@@ -471,23 +471,37 @@ __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, c
         out[0] = q.x; out[1] = q.y;
       }
     };
-    int k = k0;
-    for (; k + 4 <= k1; k += 4) {
-      float a0[V], a1[V], a2[V], a3[V];
-      load(k, a0);
-      load(k + 1, a1);
-      load(k + 2, a2);
-      load(k + 3, a3);
-      const double s0 = escale[m2l_src[k]], s1 = escale[m2l_src[k + 1]], s2 = escale[m2l_src[k + 2]], s3 = escale[m2l_src[k + 3]];
+    // 32 partials at a time: lane l fetches the row position and column scale of partial
+    // kb + l (one coalesced load each), then the warp walks them eight rows in flight
+    for (int kb = k0; kb < k1; kb += 32) {
+      const int nk = min(32, k1 - kb);
+      int my_row = 0;
+      double my_sc = 0.0;
+      if (lane < nk) {
+        my_row = pos[kb + lane];
+        my_sc = escale[m2l_src[kb + lane]];
+      }
+      int j = 0;
+      for (; j + 8 <= nk; j += 8) {
+        float a[8][V];
+        double sc[8];
 #pragma unroll
-      for (int v = 0; v < V; ++v) acc[v] += ((double)a0[v] * s0 + (double)a1[v] * s1) + ((double)a2[v] * s2 + (double)a3[v] * s3);
-    }
-    for (; k < k1; ++k) {
-      float a0[V];
-      load(k, a0);
-      const double s0 = escale[m2l_src[k]];
+        for (int u = 0; u < 8; ++u) {
+          load(__shfl_sync(0xffffffffu, my_row, j + u), a[u]);
+          sc[u] = __shfl_sync(0xffffffffu, my_sc, j + u);
+        }
 #pragma unroll
-      for (int v = 0; v < V; ++v) acc[v] += (double)a0[v] * s0;
+        for (int v = 0; v < V; ++v)
+          acc[v] += (((double)a[0][v] * sc[0] + (double)a[1][v] * sc[1]) + ((double)a[2][v] * sc[2] + (double)a[3][v] * sc[3])) +
+                    (((double)a[4][v] * sc[4] + (double)a[5][v] * sc[5]) + ((double)a[6][v] * sc[6] + (double)a[7][v] * sc[7]));
+      }
+      for (; j < nk; ++j) {
+        float a0[V];
+        load(__shfl_sync(0xffffffffu, my_row, j), a0);
+        const double s0 = __shfl_sync(0xffffffffu, my_sc, j);
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[v] += (double)a0[v] * s0;
+      }
     }
     const double a = node_dL[tgt];
     double* Lr = reinterpret_cast<double*>(L + (size_t)tgt * 2 * NC);
