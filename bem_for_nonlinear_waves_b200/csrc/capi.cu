@@ -113,6 +113,7 @@ struct bem_gpu_ctx {
   std::vector<int> level_parent_off;
   int n_m2l_targets = 0, max_ntgt = 0, chunk = 0;
   int64_t w4_total = 0;  // size of the row-padded FP32 near weights
+  int n_tc_items = 0;    // tensor-core work items (every table-row-tile image's pair chunks)
   // state
   DBuf<double> phi, phin, known_s, rows, GPhin, GnPhi;
   // graph-captured A.x : mv_in -> mv_out
@@ -238,7 +239,7 @@ struct bem_gpu_ctx {
   // switches an argument set to the tensor-core M2L
   void set_tc(MatvecArgs& a) const {
     a.use_tc = 1;
-    a.n_tc_items = (int)plan.tc_item_tab.size();
+    a.n_tc_items = n_tc_items;
     a.tc_grid = tc_grid;
     a.tc_item_tab = tc_item_tab.p;
     a.tc_item_begin = tc_item_begin.p;
@@ -498,7 +499,7 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   ctx->h2d = ctx->d2h = ctx->launches = 0;
   const double t0 = now_s();
   if (ctx->opts.precision == 1 && !tc_supported(ctx->opts.expansion_order)) {
-    ctx->err = "mixed precision needs (expansion_order+1)^2 <= 128 (p <= 10)";
+    ctx->err = "mixed precision needs expansion_order <= 12";
     return BEM_ERR_UNSUPPORTED;
   }
   if (ctx->opts.precision != 0 && ctx->opts.precision != 1) {
@@ -653,9 +654,9 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     const int ngroups = (int)P.grp_off.size() - 1;
     const int Q = 2 * P.opt.p;
     CK(ctx->Sg.alloc((size_t)std::max(ngroups, 1) * (Q + 1) * (Q + 1)));
-    // per-pair slots; the tensor-core path stores tc_kp floats per pair in the same buffer
+    // per-pair slots; the tensor-core path stores tc_kpo floats per pair in the same buffer
     const size_t y64 = (size_t)std::max<int64_t>(P.m2l_pairs, 1) * 2 * NC;
-    const size_t ytc = ((size_t)std::max<int64_t>(P.m2l_pairs, 1) * tc_kp(P.opt.p) * sizeof(float) + sizeof(double2) - 1) / sizeof(double2);
+    const size_t ytc = ((size_t)std::max<int64_t>(P.m2l_pairs, 1) * tc_kpo(P.opt.p) * sizeof(float) + sizeof(double2) - 1) / sizeof(double2);
     CK(ctx->Y.alloc(ctx->opts.precision == 1 ? std::max(y64, ytc) : y64));
   }
   ctx->mixed = ctx->opts.precision == 1;
@@ -666,9 +667,27 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     std::vector<double> dl(nb), al(kp);
     for (int i = 0; i < nb; ++i) dl[i] = P.nodes[i].dL;
     tc_alpha_host(p, al.data());
-    CK(up(ctx, ctx->tc_item_tab, P.tc_item_tab));
-    CK(up(ctx, ctx->tc_item_begin, P.tc_item_begin));
-    CK(up(ctx, ctx->tc_item_cnt, P.tc_item_cnt));
+    {  // work items over table images: every item once per row tile, row tiles of a table
+       // consecutive (image = table * tiles + tile), so each image is loaded once per CTA range
+      const int rt = tc_row_tiles(p);
+      std::vector<int> itab, ibeg, icnt;
+      const size_t ni = P.tc_item_tab.size();
+      for (size_t i0 = 0; i0 < ni;) {
+        size_t i1 = i0;
+        while (i1 < ni && P.tc_item_tab[i1] == P.tc_item_tab[i0]) ++i1;
+        for (int r = 0; r < rt; ++r)
+          for (size_t i = i0; i < i1; ++i) {
+            itab.push_back(P.tc_item_tab[i] * rt + r);
+            ibeg.push_back(P.tc_item_begin[i]);
+            icnt.push_back(P.tc_item_cnt[i]);
+          }
+        i0 = i1;
+      }
+      ctx->n_tc_items = (int)itab.size();
+      CK(up(ctx, ctx->tc_item_tab, itab));
+      CK(up(ctx, ctx->tc_item_begin, ibeg));
+      CK(up(ctx, ctx->tc_item_cnt, icnt));
+    }
     {  // work-item order j -> source bucket; pair slot k -> its position j (the row of its partial)
       std::vector<int> src(P.tc_pair.size()), pos(P.tc_pair.size());
       for (size_t j = 0; j < src.size(); ++j) {
@@ -681,7 +700,7 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     CK(up(ctx, ctx->tc_tabvec, P.tc_tab));
     CK(up(ctx, ctx->tc_alpha, al));
     CK(up(ctx, ctx->node_dL, dl));
-    CK(ctx->tc_T.alloc((size_t)std::max(ntab, 1) * tc_table_bytes(p) / 2));
+    CK(ctx->tc_T.alloc((size_t)std::max(ntab, 1) * tc_row_tiles(p) * tc_table_bytes(p) / 2));
     CK(ctx->tc_Mt.alloc((size_t)(nb + 1) * 2 * kp));
     ctx->tc_map.assign(tc_rows_map_bytes(), 0);
     if (tc_make_rows_map(ctx->tc_map.data(), ctx->tc_Mt.p, 2 * (nb + 1), p) != 0) {

@@ -64,7 +64,7 @@ struct MatvecArgs {
   const void* tc_tab = nullptr;  // FP16 hi/lo table images
   void* tc_Mt = nullptr;         // FP16 hi/lo rows of M[0] - M[1] [n_nodes+1][2][KP]
   float* tc_escale = nullptr;    // [n_nodes] power-of-two column scales
-  float* tc_Y = nullptr;         // per-pair partial locals [pairs][KP], in work-item order
+  float* tc_Y = nullptr;         // per-pair partial locals [pairs][KPO], in work-item order
   int* tc_err = nullptr;         // set when a bounded wait gave up
   const double* node_dL = nullptr;
   const double* tc_alpha = nullptr;  // [KP] sqrt((n+m)!(n-m)!) per real coefficient
@@ -135,11 +135,13 @@ enum { STAGE_P2M = 1, STAGE_M2M = 2, STAGE_M2L = 4, STAGE_L2L = 8, STAGE_TARGETS
 int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages = STAGE_ALL);
 
 // tensor-core M2L (m2l_tc.cu)
-int tc_supported(int p);            // 1 if (p+1)^2 <= 128
+int tc_supported(int p);            // 1 for 1 <= p <= 12
 int tc_kp(int p);                   // real coefficients per row, padded to 64
 size_t tc_rows_map_bytes();         // size of the TMA tensor map over the multipole rows
 int tc_make_rows_map(void* map_out, void* Mt, int nrows, int p);
-size_t tc_table_bytes(int p);       // bytes of one table (hi + lo images)
+size_t tc_table_bytes(int p);       // bytes of one table image (hi + lo, one row tile of 128 outputs)
+int tc_row_tiles(int p);            // table images per translation (1 for p <= 10, 2 for p = 11, 12)
+int tc_kpo(int p);                  // floats per pair partial
 int tc_max_pairs();                 // pairs per work item
 void tc_alpha_host(int p, double* alpha /*[tc_kp(p)]*/);
 void launch_tc_tables(int p, int ntab, const double* tab, const double* alpha, void* T, unsigned int* maxbits, cudaStream_t st);

@@ -58,15 +58,21 @@ struct TcDims {
   static constexpr int NR = (P + 1) * (P + 1);
   static constexpr int KP = (NR + 63) / 64 * 64;  // K padded to whole 128-byte swizzle atoms
   static constexpr int KA = KP / 64;              // K atoms (64 halves) per operand row
-  static constexpr int TAB_BYTES = 2 * kRows * KP * 2;    // hi + lo images of one table
+  static constexpr int RT = (NR + kRows - 1) / kRows;  // row tiles of 128 output coefficients per table
+  // floats per pair partial: the padded coefficient count (a multiple of 64, so every lane of
+  // the reduction reads an even number of floats at an 8-byte aligned offset)
+  static constexpr int KPO = KP;
+  static constexpr int TAB_BYTES = 2 * kRows * KP * 2;    // hi + lo images of one row tile of a table
   static constexpr int REGION = kMaxCols * 128;           // one (part, atom) region of gathered rows
   static constexpr int B_BYTES = 2 * KA * REGION;         // hi + lo gathered rows
-  // two table slots and two stages of gathered rows, plus 1 KB to align them to the 1024-byte
-  // swizzle atom; at least half the SM's shared memory, so one CTA (and one TMEM allocation)
-  // per SM
-  static constexpr int NEED = 2 * TAB_BYTES + 2 * B_BYTES + 1024;
+  // two table slots when they fit beside two stages of gathered rows (one slot for the
+  // 96 KB images of p = 11, 12), plus 1 KB to align them to the 1024-byte swizzle atom; at
+  // least half the SM's shared memory, so one CTA (and one TMEM allocation) per SM
+  static constexpr int TAB_SLOTS = 2 * TAB_BYTES + 2 * B_BYTES + 1024 + 4096 <= 227 * 1024 ? 2 : 1;
+  static constexpr int NEED = TAB_SLOTS * TAB_BYTES + 2 * B_BYTES + 1024;
   static constexpr int SMEM = NEED > 116 * 1024 ? NEED : 116 * 1024;
-  static_assert(NR <= kRows, "tensor-core M2L needs (p+1)^2 <= 128");
+  static_assert(RT <= 2, "tensor-core M2L needs (p+1)^2 <= 256");
+  static_assert(KPO % 64 == 0 && KPO / 32 <= 6, "partial rows of 64, 128 or 192 floats");
   static_assert(TAB_BYTES % 1024 == 0 && B_BYTES % 1024 == 0, "gathered rows must start on a swizzle atom");
   static_assert(NEED + 4096 <= 227 * 1024, "shared memory of one CTA");
 };
@@ -92,15 +98,16 @@ __global__ void __launch_bounds__(128) k_tc_tables(int ntab, const double* __res
   constexpr int Q = 2 * P, NS = (Q + 1) * (Q + 1);
   __shared__ double2 sS[NS];
   __shared__ float red[4];
-  const int g = blockIdx.x;
-  if (g >= ntab) return;
-  const double x = tab[4 * g], y = tab[4 * g + 1], z = tab[4 * g + 2], ratio = tab[4 * g + 3];
+  const int g = blockIdx.x;  // image: table g / RT, output rows [128 (g % RT), 128 (g % RT) + 128)
+  if (g >= ntab * D::RT) return;
+  const int tb = g / D::RT, r0 = (g % D::RT) * kRows;
+  const double x = tab[4 * tb], y = tab[4 * tb + 1], z = tab[4 * tb + 2], ratio = tab[4 * tb + 3];
   if (threadIdx.x < 32) S_full_column<Q>(threadIdx.x, x, y, z, sS);
   __syncthreads();
   unsigned char* base = reinterpret_cast<unsigned char*>(T) + (size_t)g * D::TAB_BYTES;
   float vmax = 0.f;
   for (int e = threadIdx.x; e < kRows * D::KP; e += blockDim.x) {
-    const int i = e / D::KP, k = e - (e / D::KP) * D::KP;
+    const int il = e / D::KP, k = e - (e / D::KP) * D::KP, i = r0 + il;
     double v = 0.0;
     if (i < D::NR && k < D::NR) {
       int n, m, po, n1, m1, pi;
@@ -125,7 +132,7 @@ __global__ void __launch_bounds__(128) k_tc_tables(int ntab, const double* __res
     }
     const __half h = __double2half(v);
     const __half l = __double2half(v - (double)__half2float(h));
-    const uint32_t off = kmajor_offset(i, k, D::KP);
+    const uint32_t off = kmajor_offset(il, k, D::KP);
     *reinterpret_cast<__half*>(base + off) = h;
     *reinterpret_cast<__half*>(base + kRows * D::KP * 2 + off) = l;
     vmax = fmaxf(vmax, (float)fabs(v));
@@ -238,11 +245,12 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
   using D = TcDims<P>;
   extern __shared__ __align__(128) unsigned char sm_raw[];
   unsigned char* sm_tc = sm_raw + ((1024u - (smem_u32(sm_raw) & 1023u)) & 1023u);
-  unsigned char* sT = sm_tc;                     // two table slots: [hi | lo] images, kRows rows each
-  unsigned char* sB = sm_tc + 2 * D::TAB_BYTES;  // kStages stages of regions (part, atom): kMaxCols rows x 128 B
+  constexpr int NS = D::TAB_SLOTS;
+  unsigned char* sT = sm_tc;                      // table slots: [hi | lo] images, kRows rows each
+  unsigned char* sB = sm_tc + NS * D::TAB_BYTES;  // kStages stages of regions (part, atom): kMaxCols rows x 128 B
   __shared__ int s_row[kMaxCols];
-  __shared__ int s_ncol[kAcc], s_b0[kAcc];
-  __shared__ int s_tsl[kStages], s_icol[kStages];
+  __shared__ int s_ncol[kAcc], s_b0[kAcc], s_rt[kAcc];
+  __shared__ int s_tsl[kStages], s_icol[kStages], s_last[kStages];
   __shared__ uint64_t bar_full[kStages], bar_bfree[kStages], bar_tfree[2], bar_accf[kAcc], bar_acce[kAcc], bar_meta[kAcc];
   __shared__ uint32_t tslot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -254,7 +262,7 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
       mbar_init(&bar_full[s], 1);
       mbar_init(&bar_bfree[s], 1);
     }
-    for (int t = 0; t < 2; ++t) mbar_init(&bar_tfree[t], 1);
+    for (int t = 0; t < NS; ++t) mbar_init(&bar_tfree[t], 1);
     for (int b = 0; b < kAcc; ++b) {
       mbar_init(&bar_accf[b], 1);
       mbar_init(&bar_acce[b], kEpilogue);
@@ -268,7 +276,7 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
   if (tid >= kEpilogue + kProducers) {
     // MMA issuer
     if (lane == 0) {
-      int cur_tsl = -1, issued = 0;
+      int issued = 0;
       bool ok = true;
       for (int it = i0; it < i1; ++it) {
         const int li = it - i0, s = li % kStages, b = li % kAcc;
@@ -276,10 +284,7 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
         if (ok && li >= kAcc) ok = mbar_wait(&bar_acce[b], ((li / kAcc) - 1) & 1, kWaitTries);
         if (!ok) break;
         tc_fence_after();
-        const int tsl = s_tsl[s], ncol = s_icol[s];
-        // the previous table's last MMAs were issued before this point: release its slot
-        if (cur_tsl >= 0 && tsl != cur_tsl) tc_commit(&bar_tfree[cur_tsl]);
-        cur_tsl = tsl;
+        const int tsl = s_tsl[s], ncol = s_icol[s], last = s_last[s];
         const int npad = (ncol + 15) & ~15;
         const uint32_t idesc = make_idesc_f16_f32(kRows, npad);
         constexpr uint32_t SBO_T = D::KP * 16;
@@ -302,6 +307,7 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
         }
         tc_commit(&bar_bfree[s]);
         tc_commit(&bar_accf[b]);
+        if (last) tc_commit(&bar_tfree[tsl]);  // the table's last item: its slot is free once these MMAs end
         ++issued;
       }
       if (!ok) {
@@ -316,9 +322,9 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
     int last_tab = -1, ntab_loaded = 0;
     bool ok = true;
     // metadata of the current item (c_) and of the next one (n_), loaded two items ahead;
-    // the items of a CTA are consecutive in work-item order, so each begins where the
-    // previous one ends
-    int c_tab = 0, c_b0 = 0, c_n = 0, c_src = 0, n_tab = 0, n_b0 = 0, n_n = 0, n_src = 0;
+    // an item's first pair (nn_b0) is loaded one iteration before its rows are, so no load
+    // waits on another inside the loop
+    int c_tab = 0, c_b0 = 0, c_n = 0, c_src = 0, n_tab = 0, n_b0 = 0, n_n = 0, n_src = 0, nn_b0 = 0;
     auto load_item = [&](int it, int b0, int& tb, int& n, int& src) {
       tb = item_tab[it];
       n = item_cnt[it];
@@ -329,16 +335,17 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
       load_item(i0, c_b0, c_tab, c_n, c_src);
     }
     if (i0 + 1 < i1) {
-      n_b0 = c_b0 + c_n;
+      n_b0 = item_begin[i0 + 1];
       load_item(i0 + 1, n_b0, n_tab, n_n, n_src);
     }
+    if (i0 + 2 < i1) nn_b0 = item_begin[i0 + 2];
     for (int it = i0; it < i1; ++it) {
       const int li = it - i0, s = li % kStages, b = li % kAcc;
       const bool load_tab = c_tab != last_tab;
-      const int tsl = load_tab ? (ntab_loaded & 1) : ((ntab_loaded - 1) & 1);
+      const int tsl = load_tab ? (ntab_loaded % NS) : ((ntab_loaded - 1) % NS);
       if (ok && li >= kStages) ok = mbar_wait(&bar_bfree[s], ((li / kStages) - 1) & 1, kWaitTries);
       if (ok && li >= kAcc) ok = mbar_wait(&bar_acce[b], ((li / kAcc) - 1) & 1, kWaitTries);
-      if (ok && load_tab && ntab_loaded >= 2) ok = mbar_wait(&bar_tfree[tsl], ((ntab_loaded >> 1) - 1) & 1, kWaitTries);
+      if (ok && load_tab && ntab_loaded >= NS) ok = mbar_wait(&bar_tfree[tsl], ((ntab_loaded / NS) - 1) & 1, kWaitTries);
       if (named_bar_or(1, kProducers, ok ? 0 : 1)) {
         ok = false;
         break;
@@ -351,8 +358,10 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
       if (pt == 0) {
         s_ncol[b] = cur_ncol;
         s_b0[b] = c_b0;
+        s_rt[b] = cur_tab % D::RT;
         s_tsl[s] = tsl;
         s_icol[s] = cur_ncol;
+        s_last[s] = (it + 1 >= i1) || (n_tab != cur_tab);
         const uint32_t bytes = (load_tab ? (uint32_t)D::TAB_BYTES : 0u) + (uint32_t)nquad * 4u * 128u * 2u * D::KA;
         mbar_arrive_expect_tx(&bar_full[s], bytes);
       }
@@ -378,14 +387,14 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
       c_n = n_n;
       c_src = n_src;
       if (it + 2 < i1) {
-        n_b0 = c_b0 + c_n;
+        n_b0 = nn_b0;
         load_item(it + 2, n_b0, n_tab, n_n, n_src);
+        if (it + 3 < i1) nn_b0 = item_begin[it + 3];
       }
     }
     if (!ok) atomicExch(err, 1);
   } else {
-    const int quad = warp & 3, half = warp >> 2;
-    const int i = quad * 32 + lane;  // output coefficient of this thread's TMEM lane
+    const int quad = warp & 3, half = warp >> 2;  // TMEM lane quad * 32 + lane: output row of the tile
     const uint32_t lane_base = tbase + ((uint32_t)(quad * 32) << 16);
     for (int it = i0; it < i1; ++it) {
       const int li = it - i0, b = li % kAcc;
@@ -397,8 +406,9 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
       }
       tc_fence_after();
       const int ncol = s_ncol[b];
-      float* Yb = Y + (size_t)s_b0[b] * D::KP + i;
-      if (quad * 32 < D::KP) {
+      const int row0 = s_rt[b] * kRows + quad * 32;  // first output coefficient of this warp's lanes
+      float* Yb = Y + (size_t)s_b0[b] * D::KPO + row0 + lane;
+      if (row0 < D::KPO) {
         const uint32_t col0 = (uint32_t)(b * kAccCols);
         uint32_t ra[32], rb[32];
         int c0 = half * 32;
@@ -410,7 +420,7 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
 #pragma unroll
           for (int q = 0; q < 32; ++q) {
             const int j = cbase + q;
-            if (j < ncol) Yb[(size_t)j * D::KP] = __uint_as_float(r[q]);
+            if (j < ncol) Yb[(size_t)j * D::KPO] = __uint_as_float(r[q]);
           }
         };
         while (c0 < ncol) {
@@ -451,8 +461,7 @@ __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, c
                                 const double* __restrict__ node_dL, const double* __restrict__ alpha, const float* __restrict__ Y,
                                 double2* __restrict__ L) {
   using D = TcDims<P>;
-  constexpr int NC = ncoef(P), V = D::KP / 32;
-  static_assert(V == 2 || V == 4, "partial rows of 64 or 128 floats");
+  constexpr int NC = ncoef(P), V = D::KPO / 32;
   const int lane = threadIdx.x & 31;
   const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   for (int ti = w0; ti < ntargets; ti += nw) {
@@ -462,13 +471,17 @@ __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, c
 #pragma unroll
     for (int v = 0; v < V; ++v) acc[v] = 0.0;
     auto load = [&](int r, float out[V]) {
-      const float* row = Y + (size_t)r * D::KP + lane * V;
+      const float* row = Y + (size_t)r * D::KPO + lane * V;
       if constexpr (V == 4) {
         const float4 q = __ldcs(reinterpret_cast<const float4*>(row));
         out[0] = q.x; out[1] = q.y; out[2] = q.z; out[3] = q.w;
       } else {
-        const float2 q = __ldcs(reinterpret_cast<const float2*>(row));
-        out[0] = q.x; out[1] = q.y;
+#pragma unroll
+        for (int h = 0; h < V / 2; ++h) {
+          const float2 q = __ldcs(reinterpret_cast<const float2*>(row) + h);
+          out[2 * h] = q.x;
+          out[2 * h + 1] = q.y;
+        }
       }
     };
     // 32 partials at a time: lane l fetches the row position and column scale of partial
@@ -554,12 +567,12 @@ int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts, int nd) {
 template <int P>
 void tc_tables_launch(int ntab, const double* tab, const double* alpha, __half* T, unsigned int* maxbits, cudaStream_t st) {
   cudaFuncSetAttribute(k_m2l_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcDims<P>::SMEM);
-  if (ntab > 0) k_tc_tables<P><<<ntab, 128, 0, st>>>(ntab, tab, alpha, T, maxbits);
+  if (ntab > 0) k_tc_tables<P><<<ntab * TcDims<P>::RT, 128, 0, st>>>(ntab, tab, alpha, T, maxbits);
 }
 
 }  // namespace
 
-int tc_supported(int p) { return p >= 1 && (p + 1) * (p + 1) <= kRows; }
+int tc_supported(int p) { return p >= 1 && p <= 12; }
 int tc_kp(int p) { return ((p + 1) * (p + 1) + 63) / 64 * 64; }
 
 size_t tc_rows_map_bytes() { return sizeof(CUtensorMap); }
@@ -589,6 +602,8 @@ int tc_make_rows_map(void* map_out, void* Mt, int nrows, int p) {
   return r == CUDA_SUCCESS ? 0 : -1;
 }
 size_t tc_table_bytes(int p) { return (size_t)2 * kRows * tc_kp(p) * 2; }
+int tc_row_tiles(int p) { return ((p + 1) * (p + 1) + kRows - 1) / kRows; }
+int tc_kpo(int p) { return tc_kp(p); }
 int tc_max_pairs() { return kMaxPairs; }
 
 void tc_alpha_host(int p, double* alpha) {
@@ -615,6 +630,7 @@ void launch_tc_tables(int p, int ntab, const double* tab, const double* alpha, v
     tc_tables_launch<PP>(ntab, tab, alpha, t, maxbits, st); break;
     BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5)
     BEMB200_CASE(6) BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10)
+    BEMB200_CASE(11) BEMB200_CASE(12)
 #undef BEMB200_CASE
     default: break;
   }
@@ -627,6 +643,7 @@ int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st, int parts, int nd
     return m2l_tc_launch<PP>(a, st, parts, nd);
     BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5)
     BEMB200_CASE(6) BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10)
+    BEMB200_CASE(11) BEMB200_CASE(12)
 #undef BEMB200_CASE
     default: break;
   }

@@ -39,6 +39,10 @@ CONFIGS = {
     "tank_2800": dict(tank=dict(length=2.0, width=1.0, depth=0.5, h=0.05, noise=0.0, seed=1), p=8, rel_tol=1e-10),
     # a quarter of tank_60k (same tank, h doubled): small enough for full ncu captures
     "tank_15k": dict(tank=dict(length=2.0, width=1.0, depth=0.5, h=2.0 / 92, noise=0.2, seed=1), p=10, rel_tol=1e-8),
+    # tank_60k at expansion order 12 (two 128-row tiles per tensor-core table)
+    "tank_60k_p12": dict(tank=dict(length=2.0, width=1.0, depth=0.5, h=2.0 / 185, noise=0.2, seed=1), p=12, rel_tol=1e-8),
+    # the large-tank size class: 10 x 4 x 1 m, ~500k points, p = 12 (a plain box, no cylinder)
+    "tank_500k": dict(tank=dict(length=10.0, width=4.0, depth=1.0, h=0.0147, noise=0.2, seed=1), p=12, rel_tol=1e-8),
 }
 # GMRES iterations of the unpreconditioned reference algorithm on each workload (the same
 # Krylov iteration on the same operator), measured by the CUDA path; used to turn the
@@ -329,6 +333,13 @@ def main():
     barrier(world)
     dev_max, e2e_max = allreduce_max([dev_s, e2e_s], world)
     ans = bvp.ans.copy()
+    # a second right-hand side on the same set-up (phi_t BVP / next stage with unchanged
+    # geometry): the solve alone, host arrays in and out
+    kv2 = -0.7 * kv + 0.01 * np.random.default_rng(7).standard_normal(kv.shape)
+    w0 = time.perf_counter()
+    bvp.solve(kv2)
+    resolve = {"wall_ms": 1e3 * (time.perf_counter() - w0), "solves_per_s": 1.0 / (time.perf_counter() - w0),
+               "gmres_iterations": bvp.stats.iterations, "converged": bool(bvp.stats.converged)}
 
     # the FP64 GPU path on the same tank: the oracle of the mixed result, and its own speed
     fp64 = None
@@ -386,6 +397,7 @@ def main():
                 "d2h_bytes_per_step": d2h // args.steps},
         "gpu_launches": launches,
         "steps_detail": steps_detail,
+        "resolve_same_setup": resolve,
         "roofline": roof,
         "clocks": clk.summary(),
     }

@@ -59,7 +59,7 @@ typedef struct {
   int32_t preconditioner;    /* 0: none (reference default); 1: right Jacobi from the near-field diagonal */
   int32_t precision;         /* 0: FP64 throughout; 1: mixed -- GMRES corrections use the tensor-core
                                 M2L (FP16 split operands, FP32 accumulate), FP64 outer refinement on the
-                                true residual, same stopping test; needs p <= 10 */
+                                true residual, same stopping test; needs p <= 12 */
   int32_t reserved[2];
 } bem_gpu_opts;
 

@@ -15,7 +15,7 @@ def _tank(h=0.04, seed=5):
     return make_tank(1.0, 0.5, 0.4, h, amplitude=0.02, wavelength=0.7, noise_sigma=0.1, seed=seed)
 
 
-@pytest.mark.parametrize("p", [6, 10])
+@pytest.mark.parametrize("p", [6, 10, 11, 12])
 def test_mixed_matvec_close_to_fp64(product_lib, p):
     import torch
 
@@ -40,10 +40,12 @@ def test_mixed_matvec_close_to_fp64(product_lib, p):
 
 
 def test_mixed_rejects_high_order(product_lib):
+    # every order the solver accepts (1..12) has a tensor-core path; beyond it the context
+    # is refused at creation, for either precision
     t = _tank(h=0.1)
-    bvp = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=11, precision="mixed")
-    with pytest.raises(RuntimeError, match="unsupported"):
-        bvp.setup()
+    for prec in ("mixed", "fp64"):
+        with pytest.raises(RuntimeError, match="bem_gpu_create failed"):
+            BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=13, precision=prec)
 
 
 @pytest.mark.parametrize("precond,tol,agree", [("jacobi", 1e-11, 1e-8), ("jacobi", 1e-8, 1e-5)])
