@@ -32,6 +32,11 @@ class Opts(ctypes.Structure):
                 ("precision", c_int), ("reserved", c_int * 2)]
 
 
+class MelSurface(ctypes.Structure):
+    _fields_ = [("n_points", c_int), ("X", P_dbl), ("n_faces", c_int), ("tri", P_int), ("face_dirichlet", P_u8),
+                ("point_flags", P_u8), ("n_dof", c_int), ("face_dof", P_int), ("phi", P_dbl), ("phin", P_dbl)]
+
+
 class Desc(ctypes.Structure):
     _fields_ = [("n_points", c_int), ("X", P_dbl), ("n_faces", c_int), ("tri", P_int), ("face_dirichlet", P_u8),
                 ("n_dof", c_int), ("dof_point", P_int), ("dof_face", P_int), ("dof_kind", P_int), ("face_dof", P_int)]
@@ -70,6 +75,12 @@ EXPORTS = {
     "bem_gpu_check_device_status": (c_int, [ctypes.c_void_p]),
     "bem_gpu_fp64_peak_tflops": (c_dbl, [c_int]),
     "bem_plan_inspect": (c_int, [ctypes.POINTER(Opts), ctypes.POINTER(Desc), P_int, P_dbl, P_i64]),
+    "bem_gpu_mel_create": (ctypes.c_void_p, [c_int]),
+    "bem_gpu_mel_destroy": (None, [ctypes.c_void_p]),
+    "bem_gpu_mel_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "bem_gpu_mel_velocity": (c_int, [ctypes.c_void_p, ctypes.POINTER(MelSurface), P_dbl, P_dbl]),
+    "bem_gpu_mel_stage": (c_int, [ctypes.c_void_p, ctypes.POINTER(MelSurface), c_int, c_dbl, c_dbl, P_dbl, P_dbl, P_dbl, P_dbl,
+                                  P_dbl, P_dbl, P_dbl, P_dbl, P_dbl, P_dbl]),
     "bem_gpu_batch_create": (ctypes.c_void_p, [ctypes.POINTER(Opts), c_int]),
     "bem_gpu_batch_submit": (c_int, [ctypes.c_void_p, ctypes.POINTER(Desc), P_dbl, P_dbl, P_dbl, ctypes.POINTER(Stats),
                                      ctypes.POINTER(ctypes.c_int64)]),

@@ -294,3 +294,73 @@ class BatchSolver:
 
     def __del__(self):
         self.close()
+
+
+class MELStage:
+    """The Mixed-Eulerian-Lagrangian update that follows each BVP solve of a BEM-MEL time step,
+    on the GPU (bem_gpu_mel_*): point velocities u = grad phi (gradPhi(p),
+    bem/BEM_BoundaryValues.hpp:500-563), Dphi/Dt on the points that are not all-Neumann
+    (DphiDt_damped, lib/include/Network.hpp:224-235) and the RK4 stage push of phi and of the
+    point positions (pushPhi / pushPosition, bem/main_time_domain.cpp:2410-2510).  Holds the RK
+    state of one time step; `stage(k, ...)` for k = 0..3 returns the positions and point phi at
+    which the next BVP is solved (after stage 3: the state at t + dt)."""
+
+    def __init__(self, X, tri, face_dirichlet, dofs=None, device=0, gravity=9.81):
+        self.lib = L.load()
+        if not self.lib.bem_gpu_is_available():
+            raise RuntimeError("no sm_100 CUDA device visible: the MEL update runs only on the GPU")
+        self.tri = np.ascontiguousarray(tri, np.int32)
+        self.fd = np.ascontiguousarray(face_dirichlet, np.uint8)
+        self.dofs = dofs if dofs is not None else build_dofs(X, tri, face_dirichlet)
+        self.flags = np.ascontiguousarray(self.dofs["point_flags"], np.uint8)
+        self.face_dof = np.ascontiguousarray(self.dofs["face_dof"], np.int32).reshape(-1)
+        self.np = int(np.asarray(X).shape[0])
+        self.gravity = float(gravity)
+        self.handle = self.lib.bem_gpu_mel_create(int(device))
+        if not self.handle:
+            raise RuntimeError("bem_gpu_mel_create failed")
+        self.X0 = np.zeros(3 * self.np)
+        self.phi0 = np.zeros(self.np)
+        self.accX = np.zeros(3 * self.np)
+        self.accphi = np.zeros(self.np)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            self.lib.bem_gpu_mel_destroy(h)
+            self.handle = None
+
+    def _surface(self, X, phi, phin):
+        X = np.ascontiguousarray(X, np.float64).reshape(-1)
+        phi = np.ascontiguousarray(phi, np.float64)
+        phin = np.ascontiguousarray(phin, np.float64)
+        self._keep = (X, phi, phin)
+        return L.MelSurface(self.np, L.ptr(X, L.P_dbl), self.tri.shape[0], L.ptr(self.tri, L.P_int), L.ptr(self.fd, L.P_u8),
+                            L.ptr(self.flags, L.P_u8), phi.shape[0], L.ptr(self.face_dof, L.P_int), L.ptr(phi, L.P_dbl),
+                            L.ptr(phin, L.P_dbl))
+
+    def _check(self, rc, what):
+        if rc != L.BEM_OK:
+            msg = self.lib.bem_gpu_mel_last_error(self.handle)
+            raise RuntimeError(f"{what}: {L.STATUS.get(rc, rc)}: {msg.decode() if msg else ''}")
+
+    def velocity(self, X, phi, phin):
+        """(phi per point, u per point [n, 3]) from per-DOF phi / phin at positions X."""
+        s = self._surface(X, phi, phin)
+        pp, u = np.zeros(self.np), np.zeros(3 * self.np)
+        self._check(self.lib.bem_gpu_mel_velocity(self.handle, ctypes.byref(s), L.ptr(pp, L.P_dbl), L.ptr(u, L.P_dbl)), "mel velocity")
+        return pp, u.reshape(-1, 3)
+
+    def stage(self, k, dt, X, phi, phin, u_node=None, damping=None):
+        """RK4 stage k (0..3): returns (X_next [n, 3], phi_next per point, u [n, 3], Dphi/Dt)."""
+        s = self._surface(X, phi, phin)
+        Xo, po, u, dp = np.zeros(3 * self.np), np.zeros(self.np), np.zeros(3 * self.np), np.zeros(self.np)
+        un = None if u_node is None else np.ascontiguousarray(u_node, np.float64).reshape(-1)
+        dm = None if damping is None else np.ascontiguousarray(damping, np.float64).reshape(-1)
+        rc = self.lib.bem_gpu_mel_stage(self.handle, ctypes.byref(s), int(k), float(dt), self.gravity,
+                                        None if un is None else L.ptr(un, L.P_dbl), None if dm is None else L.ptr(dm, L.P_dbl),
+                                        L.ptr(self.X0, L.P_dbl), L.ptr(self.phi0, L.P_dbl), L.ptr(self.accX, L.P_dbl),
+                                        L.ptr(self.accphi, L.P_dbl), L.ptr(Xo, L.P_dbl), L.ptr(po, L.P_dbl), L.ptr(u, L.P_dbl),
+                                        L.ptr(dp, L.P_dbl))
+        self._check(rc, "mel stage")
+        return Xo.reshape(-1, 3), po, u.reshape(-1, 3), dp

@@ -191,6 +191,45 @@ int bem_gpu_batch_poll(bem_gpu_batch* batch, int64_t ticket, int32_t wait);
 const char* bem_gpu_batch_last_error(const bem_gpu_batch* batch);  /* message of the last polled failure */
 void bem_gpu_batch_destroy(bem_gpu_batch* batch);                  /* finishes queued problems first */
 
+/* Mixed-Eulerian-Lagrangian stage update (the step that follows each BVP solve of a BEM-MEL
+ * time step; set_u_potential_BEM, DphiDt_damped, pushPhi, pushPosition:
+ * bem/BEM_calculateVelocities.hpp:1027-1044, lib/include/Network.hpp:224-235,
+ * bem/main_time_domain.cpp:2410-2510).  Physical units.  The surface is the BVP's mesh with its
+ * DOF table and solution: phi / phin per DOF as bem_gpu_solve returns them, face_dof as
+ * bem_gpu_build_dofs, point_flags bits 1 all-Neumann, 2 all-Dirichlet, 4 CORNER. */
+typedef struct {
+  int32_t n_points;
+  const double* X; /* [n_points*3] current positions */
+  int32_t n_faces;
+  const int32_t* tri;            /* [n_faces*3] */
+  const uint8_t* face_dirichlet; /* [n_faces] */
+  const uint8_t* point_flags;    /* [n_points] */
+  int32_t n_dof;
+  const int32_t* face_dof; /* [n_faces*3] DOF of each face vertex */
+  const double* phi;       /* [n_dof] */
+  const double* phin;      /* [n_dof] */
+} bem_mel_surface;
+typedef struct bem_gpu_mel bem_gpu_mel;
+bem_gpu_mel* bem_gpu_mel_create(int32_t device);
+void bem_gpu_mel_destroy(bem_gpu_mel* mel);
+const char* bem_gpu_mel_last_error(const bem_gpu_mel* mel);
+/* phi per point (storePhiPhin: all-Neumann points average their face DOFs by area,
+ * bem/BEM_setBoundaryTypes.hpp:967-983) and velocity u = grad phi per point (gradPhi(p),
+ * bem/BEM_BoundaryValues.hpp:500-563: per adjacent face the surface gradient of the linear
+ * interpolant plus phin times the normal, fitted by area-weighted least squares as
+ * optimalVector does, lib/include/rootFinding.hpp:119-205).  out_phi_point may be NULL. */
+int bem_gpu_mel_velocity(bem_gpu_mel* mel, const bem_mel_surface* s, double* out_phi_point, double* out_u);
+/* RK4 stage `stage` (0..3) of step dt: u as above, Dphi/Dt = -|u|^2/2 - gravity z + u_node.u
+ * - gamma (phi - phi_ref) on points that are not all-Neumann (u_node [n_points*3] defaults to u
+ * when NULL, damping [n_points*2] = (gamma, phi_ref) to 0 when NULL), then phi (those points) and
+ * X (all points) advance as RungeKuttaCommon::push with steps = 4
+ * (lib/include/integrationOfODE.hpp:227-300).  rk_* is the caller's RK state, in and out: stage
+ * 0 sets rk_X0 / rk_phi0 from the current state, rk_acc* hold the weighted sums of f dt.
+ * out_u and out_dphidt may be NULL. */
+int bem_gpu_mel_stage(bem_gpu_mel* mel, const bem_mel_surface* s, int32_t stage, double dt, double gravity, const double* u_node,
+                      const double* damping, double* rk_X0, double* rk_phi0, double* rk_accX, double* rk_accphi, double* out_X,
+                      double* out_phi, double* out_u, double* out_dphidt);
+
 /* Mixed precision (context set up with opts.precision = 1).  No reference counterpart: the
  * reference's M2L is FP64 only (lib/include/moments.hpp:732-764).
  * bem_gpu_matvec_device_mixed: y = A_lo x on device buffers (tensor-core M2L, everything

@@ -36,6 +36,11 @@ def lib():
         llp = ctypes.POINTER(ctypes.c_longlong)
         L.oracle_build_dofs.restype = i32
         L.oracle_build_dofs.argtypes = [i32, dp, i32, ip, u8p, ip, ip, ip, ip, u8p]
+        L.oracle_mel_velocity.restype = i32
+        L.oracle_mel_velocity.argtypes = [i32, dp, i32, ip, u8p, u8p, ip, dp, dp, dp, dp]
+        L.oracle_mel_stage.restype = i32
+        L.oracle_mel_stage.argtypes = [i32, dp, i32, ip, u8p, u8p, ip, dp, dp, i32, ctypes.c_double, ctypes.c_double, dp, dp, dp,
+                                       dp, dp, dp, dp]
         L.oracle_create.restype = P
         L.oracle_create.argtypes = [i32, dp, i32, ip, u8p, i32, ip, ip, ip, ip, i32, ctypes.c_double, i32, i32]
         L.oracle_destroy.argtypes = [P]
@@ -79,6 +84,52 @@ def build_dofs(X, tri, face_dirichlet):
                                 _p(fdof, ctypes.c_int), _p(pflags, ctypes.c_uint8))
     return dict(dof_point=dp_[:n].copy(), dof_face=df[:n].copy(), dof_kind=dk[:n].copy(),
                 face_dof=fdof.reshape(nf, 3), point_flags=pflags)
+
+
+def mel_velocity(X, tri, face_dirichlet, point_flags, face_dof, phi, phin):
+    """Oracle restatement of the MEL point velocities (mel_oracle.cpp)."""
+    L = lib()
+    X = np.ascontiguousarray(X, np.float64).reshape(-1)
+    tri = np.ascontiguousarray(tri, np.int32).reshape(-1)
+    fd = np.ascontiguousarray(face_dirichlet, np.uint8)
+    fl = np.ascontiguousarray(point_flags, np.uint8)
+    fdof = np.ascontiguousarray(face_dof, np.int32).reshape(-1)
+    phi = np.ascontiguousarray(phi, np.float64)
+    phin = np.ascontiguousarray(phin, np.float64)
+    n = X.shape[0] // 3
+    pp, u = np.zeros(n), np.zeros(3 * n)
+    L.oracle_mel_velocity(n, _p(X, ctypes.c_double), tri.shape[0] // 3, _p(tri, ctypes.c_int), _p(fd, ctypes.c_uint8),
+                          _p(fl, ctypes.c_uint8), _p(fdof, ctypes.c_int), _p(phi, ctypes.c_double), _p(phin, ctypes.c_double),
+                          _p(pp, ctypes.c_double), _p(u, ctypes.c_double))
+    return pp, u.reshape(-1, 3)
+
+
+class MelOracle:
+    """RK4 MEL stages on the CPU (mel_oracle.cpp), holding the step's RK state."""
+
+    def __init__(self, n_points):
+        self.n = n_points
+        self.X0 = np.zeros(3 * n_points)
+        self.phi0 = np.zeros(n_points)
+        self.dX = np.zeros(4 * n_points * 4)
+
+    def stage(self, k, dt, gravity, X, tri, face_dirichlet, point_flags, face_dof, phi, phin):
+        L = lib()
+        X = np.ascontiguousarray(X, np.float64).reshape(-1)
+        tri = np.ascontiguousarray(tri, np.int32).reshape(-1)
+        fd = np.ascontiguousarray(face_dirichlet, np.uint8)
+        fl = np.ascontiguousarray(point_flags, np.uint8)
+        fdof = np.ascontiguousarray(face_dof, np.int32).reshape(-1)
+        phi = np.ascontiguousarray(phi, np.float64)
+        phin = np.ascontiguousarray(phin, np.float64)
+        n = self.n
+        Xo, po, u, dp = np.zeros(3 * n), np.zeros(n), np.zeros(3 * n), np.zeros(n)
+        L.oracle_mel_stage(n, _p(X, ctypes.c_double), tri.shape[0] // 3, _p(tri, ctypes.c_int), _p(fd, ctypes.c_uint8),
+                           _p(fl, ctypes.c_uint8), _p(fdof, ctypes.c_int), _p(phi, ctypes.c_double), _p(phin, ctypes.c_double),
+                           int(k), float(dt), float(gravity), _p(self.X0, ctypes.c_double), _p(self.phi0, ctypes.c_double),
+                           _p(self.dX, ctypes.c_double), _p(Xo, ctypes.c_double), _p(po, ctypes.c_double), _p(u, ctypes.c_double),
+                           _p(dp, ctypes.c_double))
+        return Xo.reshape(-1, 3), po, u.reshape(-1, 3), dp
 
 
 class Oracle:
