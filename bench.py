@@ -340,6 +340,28 @@ def main():
     bvp.solve(kv2)
     resolve = {"wall_ms": 1e3 * (time.perf_counter() - w0), "solves_per_s": 1.0 / (time.perf_counter() - w0),
                "gmres_iterations": bvp.stats.iterations, "converged": bool(bvp.stats.converged)}
+    # the MEL update after a solve (point velocities, Dphi/Dt, RK4 push; host arrays in and out),
+    # then one full RK4 step of the BEM-MEL loop: four (set-up + solve + update) at the stage
+    # positions with the stage's free-surface phi
+    from bem_for_nonlinear_waves_b200 import MELStage
+    mel = MELStage(t.X, t.tri, t.face_dirichlet, dofs=d, device=local)
+    mel.stage(0, 1e-3, t.X, bvp.phi, bvp.phin)
+    w0 = time.perf_counter()
+    for k in range(4):
+        mel.stage(k, 1e-3, t.X, bvp.phi, bvp.phin)
+    mel_ms = 1e3 * (time.perf_counter() - w0) / 4
+    dirichlet = d["dof_kind"] == 0
+    Xs, known = t.X.copy(), kv.copy()
+    w0 = time.perf_counter()
+    for k in range(4):  # the same context, set up again at the stage positions
+        bvp.X = np.ascontiguousarray(Xs, np.float64)
+        bvp.setup()
+        bvp.solve(known)
+        Xs, pnext, _, _ = mel.stage(k, 1e-3, Xs, bvp.phi, bvp.phin)
+        known = known.copy()
+        known[dirichlet] = pnext[d["dof_point"][dirichlet]]
+    rk4 = {"mel_stage_wall_ms": mel_ms, "rk4_step_wall_s": time.perf_counter() - w0, "dt": 1e-3,
+           "note": "4 x (set-up at the stage positions + solve + MEL update), host arrays in and out"}
 
     # the FP64 GPU path on the same tank: the oracle of the mixed result, and its own speed
     fp64 = None
@@ -398,6 +420,7 @@ def main():
         "gpu_launches": launches,
         "steps_detail": steps_detail,
         "resolve_same_setup": resolve,
+        "mel_rk4": rk4,
         "roofline": roof,
         "clocks": clk.summary(),
     }
