@@ -115,8 +115,9 @@ class BEM_BVP:
         self._setup_done = True
 
     def solve(self, known, x0=None):
-        """known: per-DOF phi (Dirichlet DOFs) or phin (Neumann DOFs), physical units.
-        Returns (time_setup, time_solve, unknowns) like BEM_BVP::solve()."""
+        """known: per-DOF phi (Dirichlet DOFs) or phin (Neumann DOFs), physical units; x0: optional
+        initial guess of the unknowns (phin for Dirichlet DOFs, phi for the others), e.g. the
+        previous solution's `ans`.  Returns (time_setup, time_solve, unknowns) like BEM_BVP::solve()."""
         if not self._setup_done:
             self.setup()
         known = np.ascontiguousarray(known, np.float64)

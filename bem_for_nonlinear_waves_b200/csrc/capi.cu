@@ -1093,8 +1093,17 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     for (int i = 0; i < N; ++i) bn = std::fma(b[i], b[i], bn);
     tol *= std::sqrt(bn);
   }
-  if (x0) {
-    CK(cudaMemcpyAsync(ctx->xdev.p, x0, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  std::vector<double> x0s;
+  if (x0) {  // initial guess in physical units (phin for Dirichlet DOFs, phi otherwise) -> scaled
+    x0s.resize(N);
+    for (int i = 0; i < N; ++i) {
+      if (!std::isfinite(x0[i])) {
+        ctx->err = "non-finite initial guess";
+        return BEM_ERR_NAN;
+      }
+      x0s[i] = (P.dof_kind[i] == 0) ? x0[i] * P.L : x0[i];
+    }
+    CK(cudaMemcpyAsync(ctx->xdev.p, x0s.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
     ctx->h2d += 8LL * N;
   } else
     CK(cudaMemsetAsync(ctx->xdev.p, 0, sizeof(double) * N, s));
@@ -1169,9 +1178,9 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
       ctx->err = "non-finite residual";
       return BEM_ERR_NAN;
     }
-    if (beta == 0.0) {
-      r_true = 0.0;
-      err = 0.0;
+    if (beta <= tol) {  // the iterate (a good initial guess, or zero data) already meets the tolerance
+      r_true = beta;
+      err = beta;
       break;
     }
     x_zero = false;

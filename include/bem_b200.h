@@ -125,7 +125,10 @@ int bem_gpu_build_dofs(int32_t n_points, const double* X, int32_t n_faces, const
 int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* desc);
 
 /* Solve with known boundary values (physical units; phi for Dirichlet DOFs, phin for
- * Neumann and corner-Neumann DOFs).  x0 may be NULL (zero initial guess).  out_phi and
+ * Neumann and corner-Neumann DOFs).  x0: initial guess of the unknowns in the same units
+ * (phin for Dirichlet DOFs, phi for the others), e.g. the previous stage's solution as the
+ * reference starts from the current boundary values (BEM_solveBVP_GMRES_FMM.hpp:3450-3454);
+ * NULL for a zero initial guess.  out_phi and
  * out_phin get every DOF's phi and phin (known values copied through).  Replaces
  * solveSystemGMRES + the unscaling in solveGMRES (BEM_solveBVP_GMRES_FMM.hpp:2007-2649,
  * 3462-3486).  Returns BEM_OK, or BEM_ERR_NOT_CONVERGED with the outputs still written. */

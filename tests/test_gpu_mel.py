@@ -75,10 +75,12 @@ def test_mel_rk4_step_with_bvp(product_lib):
     X = t.X.copy()
     known = kv.copy()
     dirichlet = d["dof_kind"] == 0
+    prev = None
     for k in range(4):
         b = BEM_BVP(X, t.tri, t.face_dirichlet, expansion_order=8, solver_tol=1e-10, tol_relative=True, preconditioner="jacobi",
                     dofs=d)
-        b.solve(known)
+        b.solve(known, x0=prev)  # warm start from the previous stage, as the reference does
+        prev = b.ans.copy()
         assert b.last_gmres_converged
         X, pnext, u, dphi = m.stage(k, 0.01, X, b.phi, b.phin)
         known = known.copy()

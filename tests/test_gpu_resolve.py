@@ -33,3 +33,17 @@ def test_resolve_on_one_setup(product_lib, precision):
     a12 = b.ans
     rel = np.abs(a12 - (a1 + a2)).max() / np.abs(a12).max()
     assert rel < 1e-8, rel
+
+
+def test_warm_start_from_solution(product_lib):
+    t = make_tank(1.0, 0.5, 0.4, 0.05, amplitude=0.02, wavelength=0.7, noise_sigma=0.1, seed=12)
+    d = build_dofs(t.X, t.tri, t.face_dirichlet)
+    k1 = known_values(t, d["dof_point"], d["dof_face"], d["dof_kind"], point_normals(t))
+    b = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=8, solver_tol=1e-10, tol_relative=True, preconditioner="jacobi", dofs=d)
+    b.solve(k1)
+    cold_iters, a1 = b.last_gmres_total_iter, b.ans.copy()
+    b.solve(k1, x0=a1)  # the solution itself: already converged
+    assert b.last_gmres_converged and b.last_gmres_total_iter <= 1
+    assert np.abs(b.ans - a1).max() <= 1e-9 * np.abs(a1).max()
+    b.solve(1.01 * k1, x0=a1)  # a nearby right-hand side starts close
+    assert b.last_gmres_converged and b.last_gmres_total_iter < cold_iters
