@@ -100,7 +100,8 @@ struct bem_gpu_ctx {
   DBuf<double2> p2m_C;                       // [(leaf, DOF)][NC]
   DBuf<double2> near_scratch;                // element values of the near-weight kernel
   DBuf<int> e_dof, e_vtx, node_fb, node_fe, leaves, level_parents, child_begin, child_end, node_children;
-  DBuf<int> node_parent, node_level, m2m_nsig, m2m_cnt;
+  DBuf<int> node_parent, node_level, m2m_nsig, m2m_cnt, m2m_ready;
+  int n_m2m_ready = 0;
   DBuf<int> m2l_targets, m2l_off, m2l_src, nb_dofs, nb_targets, nb_ranges, dof_inc_off, dof_inc;
   DBuf<int> block_of_point, row_of_point, self_col;  // right-Jacobi inputs
   DBuf<int> point_dof_off, point_dof, dof_kind, dof_point;
@@ -193,6 +194,8 @@ struct bem_gpu_ctx {
     a.node_level = node_level.p;
     a.m2m_nsig = m2m_nsig.p;
     a.m2m_cnt = m2m_cnt.p;
+    a.n_m2m_ready = n_m2m_ready;
+    a.m2m_ready = m2m_ready.p;
 
     a.n_m2l_targets = n_m2l_targets;
     a.m2l_targets = m2l_targets.p;
@@ -619,13 +622,24 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
       for (int i : P.level_nodes[l]) lev[i] = l;
     for (int i = 0; i < nb; ++i)
       for (int ci = P.nodes[i].child_begin; ci < P.nodes[i].child_end; ++ci) par[P.node_children[ci]] = i;
-    // a child signals its parent if it is a leaf (its multipole comes from the P2M) or if one of
-    // its own children signals it; deepest levels first
+    // a node has a multipole if it is a leaf (from the P2M) or one of its children has one;
+    // a parent waits for its children with multipoles that are not leaves (nsig), and the
+    // parents that wait for none start the pass; deepest levels first
+    std::vector<int> nch(nb, 0), ready;
     for (int l = (int)P.level_nodes.size() - 1; l >= 0; --l)
       for (int i : P.level_nodes[l]) {
-        sig[i] = leaf[i] || nsig[i] > 0;
-        if (sig[i] && par[i] >= 0) ++nsig[par[i]];
+        sig[i] = leaf[i] || nch[i] > 0;
+        if (sig[i] && par[i] >= 0) {
+          ++nch[par[i]];
+          if (!leaf[i]) ++nsig[par[i]];
+        }
       }
+    for (int l = (int)P.level_nodes.size() - 1; l >= 0; --l)
+      for (int i : P.level_nodes[l])
+        if (!leaf[i] && nch[i] > 0 && nsig[i] == 0) ready.push_back(i);
+    ctx->n_m2m_ready = (int)ready.size();
+    if (ready.empty()) ready.push_back(0);
+    CK(up(ctx, ctx->m2m_ready, ready));
     CK(up(ctx, ctx->node_parent, par));
     CK(up(ctx, ctx->node_level, lev));
     CK(up(ctx, ctx->m2m_nsig, nsig));

@@ -386,17 +386,17 @@ __device__ __forceinline__ void expand_full_group(const double2* __restrict__ sr
   }
 }
 
-// M2M: the upward pass in one launch.  A block starts at a leaf and climbs: after the
-// multipole of its node is complete it counts the node in at the parent (a counter per
-// node), and the block whose count completes the parent computes the parent's multipole
-// (group g translating children g, g + 4, ...; partial multipoles summed in group order,
-// so the result does not depend on which block arrives last), then climbs on.  Nothing
-// waits: a block that does not complete its parent stops.  The last arrival resets the
-// parent's counter, so every launch starts from zero.  Children's multipoles written by
-// other blocks of the launch are read through L2.
+// M2M: the upward pass in one launch.  A block starts at a parent whose children with
+// multipoles are all leaves (ready from the P2M), computes its multipole (group g translating
+// children g, g + 4, ...; partial multipoles summed in group order, so the result does not
+// depend on which block computes it) and climbs: it counts the node in at the parent (a
+// counter per node over the parent's non-leaf children), and the block whose count completes
+// the parent computes the parent next.  Nothing waits: a block that does not complete its
+// parent stops.  The last arrival resets the parent's counter, so every launch starts from
+// zero.  Children's multipoles written by other blocks of the launch are read through L2.
 template <int P, int ND>
 __global__ void __launch_bounds__(kTreeGroups * tree_group_threads<P>()) k_m2m_up(
-    const int* __restrict__ leaves, const int* __restrict__ node_parent, const int* __restrict__ node_level,
+    const int* __restrict__ ready, const int* __restrict__ node_parent, const int* __restrict__ node_level,
     const int* __restrict__ nsig, int* __restrict__ cnt, const int* __restrict__ child_begin, const int* __restrict__ child_end,
     const int* __restrict__ node_children, const double* __restrict__ node_X, const double2* __restrict__ Ftab, double2* __restrict__ M) {
   constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), G = kTreeGroups, GT = tree_group_threads<P>();
@@ -407,30 +407,16 @@ __global__ void __launch_bounds__(kTreeGroups * tree_group_threads<P>()) k_m2m_u
   const int g = threadIdx.x / GT, t = threadIdx.x - g * GT;
   int n = 0, m = 0;
   if (t < NC) decode_nm(t, n, m);
-  int node = leaves[blockIdx.x];
+  int node = ready[blockIdx.x];
   for (;;) {
-    const int par = node_parent[node];
-    if (par < 0) return;
-    __threadfence();  // this node's multipole (written by this block, or by the P2M launch) before the count
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int go = atomicAdd(&cnt[par], 1) == nsig[par] - 1;
-      if (go) {
-        cnt[par] = 0;
-        __threadfence();
-      }
-      s_go = go;
-    }
-    __syncthreads();
-    if (!s_go) return;
-    const double2* Fl = Ftab + (size_t)node_level[par] * 8 * NF;
-    const int cb = child_begin[par], ce = child_end[par];
+    const double2* Fl = Ftab + (size_t)node_level[node] * 8 * NF;
+    const int cb = child_begin[node], ce = child_end[node];
     double2 o0 = make_double2(0.0, 0.0), o1 = o0;
     for (int c0 = cb; c0 < ce; c0 += G) {
       const int ci = c0 + g;
       if (ci < ce) {
         const int c = node_children[ci];
-        const double2* Ft = Fl + (size_t)child_octant(node_X, c, par) * NF;
+        const double2* Ft = Fl + (size_t)child_octant(node_X, c, node) * NF;
         for (int i = t; i < NF; i += GT) sF[g][i] = Ft[i];
         expand_full_group<P, ND, true>(M + (size_t)c * 2 * NC, sM[g], t, GT);
       }
@@ -446,8 +432,22 @@ __global__ void __launch_bounds__(kTreeGroups * tree_group_threads<P>()) k_m2m_u
     for (int i = threadIdx.x; i < ND * NC; i += blockDim.x) {
       double2 v = part[0][i];
       for (int w = 1; w < G; ++w) v = cadd(v, part[w][i]);
-      M[(size_t)par * 2 * NC + i] = v;
+      M[(size_t)node * 2 * NC + i] = v;
     }
+    const int par = node_parent[node];
+    if (par < 0) return;
+    __threadfence();  // this node's multipole before the count
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int go = atomicAdd(&cnt[par], 1) == nsig[par] - 1;
+      if (go) {
+        cnt[par] = 0;
+        __threadfence();
+      }
+      s_go = go;
+    }
+    __syncthreads();
+    if (!s_go) return;
     node = par;
   }
 }
@@ -1128,8 +1128,8 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     k_p2m<P, ND><<<a.n_leaves, 128, 0, st>>>(a.leaves, a.node_fb, a.node_fe, a.node_X, a.e_q, a.e_W, a.e_n, a.e_dof, a.phi, a.phin, a.M);
     ++launches;
   }
-  if ((stages & STAGE_M2M) && a.n_leaves > 0) {
-    k_m2m_up<P, ND><<<a.n_leaves, kTreeGroups * tree_group_threads<P>(), 0, st>>>(a.leaves, a.node_parent, a.node_level, a.m2m_nsig,
+  if ((stages & STAGE_M2M) && a.n_m2m_ready > 0) {
+    k_m2m_up<P, ND><<<a.n_m2m_ready, kTreeGroups * tree_group_threads<P>(), 0, st>>>(a.m2m_ready, a.node_parent, a.node_level, a.m2m_nsig,
                                                                                   a.m2m_cnt, a.child_begin, a.child_end, a.node_children,
                                                                                   a.node_X, a.Ftab, a.M);
     ++launches;

@@ -36,7 +36,9 @@ struct MatvecArgs {
   const double2* Ftab = nullptr;           // [level][octant][(P+1)^2] parent-to-child F tables
   const int* node_parent = nullptr;        // [n_nodes] parent bucket, -1 at the root
   const int* node_level = nullptr;         // [n_nodes] level (row block of Ftab)
-  const int* m2m_nsig = nullptr;           // [n_nodes] children whose multipole completes in the upward pass
+  const int* m2m_nsig = nullptr;           // [n_nodes] non-leaf children whose multipole completes in the upward pass
+  int n_m2m_ready = 0;                     // parents whose children with multipoles are all leaves
+  const int* m2m_ready = nullptr;
   int* m2m_cnt = nullptr;                  // [n_nodes] upward-pass arrival counters (zero between launches)
 
   int n_m2l_targets = 0;
