@@ -612,6 +612,12 @@ __global__ void __launch_bounds__(128) k_targets(const NearBlockDev* __restrict_
   double2* xs = smem;                   // [chunk] (phi, phin)
   double2* accs = smem + chunk;         // [ntgt] near sums (G.phin, Gn.phi)
   __shared__ double2 sL[2 * NC];
+  __shared__ double sHalf[P + 1], sRec[(P + 1) * (P + 1)];  // 1/(2k), 1/(n^2 - m^2) of the L2P recurrence
+  for (int i = threadIdx.x; i < (P + 1) * (P + 1); i += blockDim.x) {
+    const int n = i / (P + 1), m = i - n * (P + 1);
+    sRec[i] = n > m ? 1.0 / double(n * n - m * m) : 0.0;
+    if (i <= P) sHalf[i] = i > 0 ? 1.0 / (2.0 * i) : 0.0;
+  }
   const NearBlockDev B = blocks[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarp = blockDim.x >> 5;
@@ -656,12 +662,12 @@ __global__ void __launch_bounds__(128) k_targets(const NearBlockDev* __restrict_
     if (m <= P) {
       const double r2 = x * x + y * y + z * z;
       double2 cur = make_double2(1.0, 0.0);
-      for (int k = 1; k <= m; ++k) cur = cscale(cmul(cur, make_double2(x, y)), 1.0 / (2.0 * k));
+      for (int k = 1; k <= m; ++k) cur = cscale(cmul(cur, make_double2(x, y)), sHalf[k]);
       double2 prev = make_double2(0.0, 0.0);
       const double w = (m == 0) ? 1.0 : 2.0;
       for (int n = m; n <= P; ++n) {
         if (n > m) {
-          const double inv = 1.0 / double(n * n - m * m);
+          const double inv = sRec[n * (P + 1) + m];
           double2 nx = make_double2(((2 * n - 1) * z * cur.x - r2 * prev.x) * inv, ((2 * n - 1) * z * cur.y - r2 * prev.y) * inv);
           prev = cur;
           cur = nx;
@@ -718,6 +724,12 @@ __global__ void __launch_bounds__(128) k_targets_ax(const NearBlockDev* __restri
   double* xs = reinterpret_cast<double*>(smem);  // [chunk] x of the block's DOFs
   double* accs = xs + chunk;                      // [ntgt] near sums
   __shared__ double2 sL[NC];
+  __shared__ double sHalf[P + 1], sRec[(P + 1) * (P + 1)];  // 1/(2k), 1/(n^2 - m^2) of the L2P recurrence
+  for (int i = threadIdx.x; i < (P + 1) * (P + 1); i += blockDim.x) {
+    const int n = i / (P + 1), m = i - n * (P + 1);
+    sRec[i] = n > m ? 1.0 / double(n * n - m * m) : 0.0;
+    if (i <= P) sHalf[i] = i > 0 ? 1.0 / (2.0 * i) : 0.0;
+  }
   const NearBlockDev B = blocks[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarp = blockDim.x >> 5;
@@ -770,12 +782,12 @@ __global__ void __launch_bounds__(128) k_targets_ax(const NearBlockDev* __restri
     if (m <= P) {
       const double r2 = px * px + py * py + pz * pz;
       double2 cur = make_double2(1.0, 0.0);
-      for (int k = 1; k <= m; ++k) cur = cscale(cmul(cur, make_double2(px, py)), 1.0 / (2.0 * k));
+      for (int k = 1; k <= m; ++k) cur = cscale(cmul(cur, make_double2(px, py)), sHalf[k]);
       double2 prev = make_double2(0.0, 0.0);
       const double w = (m == 0) ? 1.0 : 2.0;
       for (int n = m; n <= P; ++n) {
         if (n > m) {
-          const double inv = 1.0 / double(n * n - m * m);
+          const double inv = sRec[n * (P + 1) + m];
           double2 nx = make_double2(((2 * n - 1) * pz * cur.x - r2 * prev.x) * inv, ((2 * n - 1) * pz * cur.y - r2 * prev.y) * inv);
           prev = cur;
           cur = nx;
