@@ -209,6 +209,24 @@ def load_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
+def mixed_problems(n, seed):
+    """Tanks of mixed sizes drawn from one seed (the batch size class of the reference's
+    hot-path table, without its floating box): length U[1, 4], width 1, depth U[0.3, 1.0], h
+    chosen so the point count is log-uniform in [2k, 80k], amplitude U[0.005, 0.05],
+    wavelength U[0.5, 2]."""
+    from bem_for_nonlinear_waves_b200 import build_dofs, known_values, make_tank, point_normals
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        L, W, D = rng.uniform(1, 4), 1.0, rng.uniform(0.3, 1.0)
+        pts = math.exp(rng.uniform(math.log(2e3), math.log(8e4)))
+        h = math.sqrt(2 * (L * W + L * D + W * D) / pts)
+        t = make_tank(L, W, D, h, amplitude=rng.uniform(0.005, 0.05), wavelength=rng.uniform(0.5, 2.0))
+        d = build_dofs(t.X, t.tri, t.face_dirichlet)
+        out.append((t, d, known_values(t, d["dof_point"], d["dof_face"], d["dof_kind"], point_normals(t))))
+    return out
+
+
 def run_batch(args, cfg, local):
     """Serving mode: `--batch P` seeded tanks of the workload's size (different free
     surfaces) go to a BatchSolver with `--workers W` contexts at once; reports whole-batch
@@ -216,7 +234,11 @@ def run_batch(args, cfg, local):
     problems solved one after another on one context."""
     from bem_for_nonlinear_waves_b200 import BEM_BVP, BatchSolver
     rank = 0
-    probs = [make_problem(cfg, rank + 1000 + i) for i in range(args.batch)]
+    if args.mixed_sizes:
+        probs = mixed_problems(args.batch, 2024)
+        cfg = dict(cfg, p=8, rel_tol=1e-8)
+    else:
+        probs = [make_problem(cfg, rank + 1000 + i) for i in range(args.batch)]
     kw = dict(expansion_order=cfg["p"], solver_tol=cfg["rel_tol"], tol_relative=True, solver_max_iter=args.max_iter,
               preconditioner=args.precond, device=local, precision=args.precision)
     one = BEM_BVP(probs[0][0].X, probs[0][0].tri, probs[0][0].face_dirichlet, dofs=probs[0][1], **kw)
@@ -254,7 +276,8 @@ def run_batch(args, cfg, local):
     pct = lambda v, q: float(np.percentile(np.asarray(v), q))  # noqa: E731
     line = {"metric": "bvp_solves_per_s", "value": len(probs) / batch_s, "unit": "solves/s", "n_gpus": 1, "mode": "batch",
             "higher_is_better": True, "dtype": "f64/f16x3-tc" if args.precision == "mixed" else "f64", "data": "synthetic",
-            "config": {"workload": args.config, "problems": len(probs), "workers": args.workers, "precision": args.precision,
+            "config": {"workload": "mixed_2k_80k_p8" if args.mixed_sizes else args.config, "problems": len(probs),
+                       "points": [int(p[0].n_points) for p in probs], "workers": args.workers, "precision": args.precision,
                        "preconditioner": args.precond, "converged": bool(conv)},
             "latency_s": {"p50": pct(lats, 50), "p99": pct(lats, 99), "max": lats[-1]},
             "sequential": {"solves_per_s": len(probs) / seq_s, "latency_p50_s": pct(seq_lat, 50)},
@@ -278,6 +301,7 @@ def main():
     ap.add_argument("--no-fp64-check", action="store_true")
     ap.add_argument("--batch", type=int, default=0, help="serving mode: number of problems (one GPU)")
     ap.add_argument("--workers", type=int, default=2)
+    ap.add_argument("--mixed-sizes", action="store_true", help="serving mode over tanks of 2k-80k points (p = 8)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
