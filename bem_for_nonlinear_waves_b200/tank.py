@@ -26,6 +26,7 @@ class Tank:
     amplitude: float
     wavenumber: float
     g: float = 9.81
+    body: "Body | None" = None
 
     @property
     def omega(self) -> float:
@@ -123,6 +124,34 @@ def make_tank(length: float = 2.0, width: float = 1.0, depth: float = 0.5, h: fl
                 amplitude=amplitude, wavenumber=2.0 * math.pi / wavelength)
 
 
+@dataclasses.dataclass
+class Body:
+    """A rigid box inside the fluid: its faces are Neumann with phin = (U + Omega x (x - c)) . n."""
+    point_begin: int            # first point of the body surface in the tank's point array
+    face_begin: int             # first face of the body surface
+    center: np.ndarray
+    U: np.ndarray
+    Omega: np.ndarray
+
+
+def add_box_body(tank: Tank, center, size, h: float, U=(0.0, 0.0, 0.0), Omega=(0.0, 0.0, 0.0)) -> Tank:
+    """Adds a closed box surface (sizes `size`, centred at `center`, fully submerged) to a tank
+    as a second boundary of the fluid.  Its triangles face into the box (out of the fluid),
+    all Neumann; the tank's `body` carries the rigid velocity for the known values.  The
+    floating bodies of the reference's BEM-MEL runs are such closed Neumann surfaces with
+    phin = (U + Omega x r) . n (bem/BEM_setBoundaryTypes.hpp:753-847)."""
+    c = np.asarray(center, dtype=np.float64)
+    sz = np.asarray(size, dtype=np.float64)
+    sub = make_tank(sz[0], sz[1], sz[2], h)  # outward box [0,a]x[0,b]x[-c,0]
+    Xb = sub.X + (c - np.array([sz[0] / 2, sz[1] / 2, -sz[2] / 2]))
+    tri_b = sub.tri[:, [0, 2, 1]] + tank.X.shape[0]  # reversed: normals into the box
+    t = dataclasses.replace(tank, X=np.vstack([tank.X, Xb]), tri=np.vstack([tank.tri, tri_b]).astype(np.int32),
+                            face_dirichlet=np.concatenate([tank.face_dirichlet, np.zeros(tri_b.shape[0], np.uint8)]))
+    t.body = Body(point_begin=tank.X.shape[0], face_begin=tank.tri.shape[0], center=c, U=np.asarray(U, np.float64),
+                  Omega=np.asarray(Omega, np.float64))
+    return t
+
+
 # Named workloads (tank sizes, spacing, expansion order).
 CONFIGS = {
     # ~2,800 nodes / 5,600 triangles, p=8 (the reference's CPU-runnable case)
@@ -147,6 +176,12 @@ def known_values(tank: Tank, dof_point: np.ndarray, dof_face: np.ndarray, dof_ki
     f = dof_face[nd]
     nrm = np.where((f >= 0)[:, None], fn[np.maximum(f, 0)], point_normal[dof_point[nd]])
     kv[nd] = np.einsum("ij,ij->i", g, nrm)
+    b = getattr(tank, "body", None)
+    if b is not None:  # rigid-body Neumann data on the body surface
+        on = nd & (dof_point >= b.point_begin)
+        xb = X[dof_point[on]]
+        vel = b.U[None, :] + np.cross(b.Omega[None, :], xb - b.center[None, :])
+        kv[on] = np.einsum("ij,ij->i", vel, nrm[on[nd]])
     return kv
 
 

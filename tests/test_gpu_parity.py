@@ -148,3 +148,25 @@ def test_gpu_full_size_properties(product_lib):
     bvp.solve(kv)
     assert bvp.last_gmres_converged
     assert np.isfinite(bvp.ans).all()
+
+
+def test_gpu_tank_with_submerged_body_matches_oracle(product_lib, oracle_mod):
+    """Two boundaries: the tank and a closed box inside the fluid (Neumann, rigid-body
+    velocity), the floating-body configuration; operator and solution against the oracle."""
+    from bem_for_nonlinear_waves_b200 import add_box_body
+    t = make_tank(1.0, 0.5, 0.4, 0.05, amplitude=0.02, wavelength=0.7, noise_sigma=0.003, seed=4)
+    t = add_box_body(t, (0.45, 0.25, -0.2), (0.2, 0.15, 0.1), 0.05, U=(0.1, 0.0, -0.05), Omega=(0.0, 0.3, 0.1))
+    d = build_dofs(t.X, t.tri, t.face_dirichlet)
+    kv = known_values(t, d["dof_point"], d["dof_face"], d["dof_kind"], point_normals(t))
+    bvp = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=8, dofs=d, solver_tol=1e-12, solver_max_iter=1500)
+    bvp.setup()
+    o = oracle_mod.Oracle(t.X, t.tri, t.face_dirichlet, d, p=8)
+    rng = np.random.default_rng(8)
+    phi, phin = rng.normal(size=bvp.matrix_size), rng.normal(size=bvp.matrix_size)
+    got, exp = bvp.apply(phi, phin), o.apply(phi, phin)
+    assert np.abs(got - exp).max() <= 1e-10 * np.abs(exp).max()
+    bvp.solve(kv)
+    assert bvp.last_gmres_converged
+    ph, pn, st = o.solve(kv, tol=1e-12, max_iter=1500)
+    ref = np.where(d["dof_kind"] == 0, pn, ph)
+    assert np.abs(bvp.ans - ref).max() <= 1e-8 * np.abs(ref).max()
