@@ -1303,6 +1303,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     stats->kernel_launches = ctx->launches;
     stats->time_plan_s = ctx->time_plan;
     stats->time_upload_s = ctx->time_upload;
+    stats->time_setup_device_s = 1e-3 * (double)ctx->setup_dev_ms;
   }
   if (!finite) {
     ctx->err = "non-finite solution";

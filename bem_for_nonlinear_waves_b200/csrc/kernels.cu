@@ -1311,7 +1311,7 @@ void launch_densities(int n, int mode, const double* x, const double* known, con
   k_densities<<<g > 0 ? g : 1, 256, 0, st>>>(n, mode, x, known, kind, phi, phin);
 }
 
-int near_weights_grid() { return 148 * 2; }
+int near_weights_grid() { return 148 * 3; }  // three 256-thread CTAs per SM (80 registers a thread)
 
 void launch_near_weights(const NearArgs& a, cudaStream_t st) {
   const size_t shm = sizeof(int) * (size_t)(3 * a.max_nrng + 1);

@@ -343,7 +343,7 @@ def main():
             e2e_s += w2 - w0
             st = bvp.stats
             steps_detail.append({"setup_wall_ms": 1e3 * (w1 - w0), "solve_wall_ms": 1e3 * (w2 - w1),
-                                 "device_ms": 1e3 * st.time_device_s})
+                                 "device_ms": 1e3 * st.time_device_s, "setup_device_ms": 1e3 * st.time_setup_device_s})
             dev_s += st.time_device_s
             plan_s += st.time_plan_s
             upload_s += st.time_upload_s

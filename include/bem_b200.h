@@ -98,6 +98,7 @@ typedef struct {
   int64_t kernel_launches;/* kernels launched by setup + solve (graph nodes counted) */
   double time_plan_s;     /* host part of the set-up: tree, lists, near-field sparsity */
   double time_upload_s;   /* host->device copies of the set-up */
+  double time_setup_device_s; /* device part of the set-up (near weights, tables, diagonal) */
 } bem_gpu_stats;
 
 /* 1 if a CUDA device of compute capability 10.x is visible. */
