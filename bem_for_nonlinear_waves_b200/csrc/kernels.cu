@@ -246,6 +246,7 @@ __global__ void __launch_bounds__(128) k_p2m_op(const int* __restrict__ leaves, 
 template <int P>
 __global__ void k_p2m_apply(const int* __restrict__ leaves, const int* __restrict__ leaf_dof_off, const int* __restrict__ leaf_dof,
                             const double2* __restrict__ C, const double* __restrict__ x, double2* __restrict__ M) {
+  pdl_enter();
   constexpr int NC = ncoef(P);
   const int li = blockIdx.x, leaf = leaves[li];
   const int t = threadIdx.x;
@@ -399,6 +400,7 @@ __global__ void __launch_bounds__(kTreeGroups * tree_group_threads<P>()) k_m2m_u
     const int* __restrict__ ready, const int* __restrict__ node_parent, const int* __restrict__ node_level,
     const int* __restrict__ nsig, int* __restrict__ cnt, const int* __restrict__ child_begin, const int* __restrict__ child_end,
     const int* __restrict__ node_children, const double* __restrict__ node_X, const double2* __restrict__ Ftab, double2* __restrict__ M) {
+  pdl_enter();
   constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), G = kTreeGroups, GT = tree_group_threads<P>();
   __shared__ double2 sF[G][NF];
   __shared__ double2 sM[G][ND * NF];
@@ -565,6 +567,7 @@ __global__ void __launch_bounds__(kTreeGroups * tree_group_threads<P>()) k_l2l(
     const int* __restrict__ parents, const int* __restrict__ child_begin, const int* __restrict__ child_end,
     const int* __restrict__ node_children, const double* __restrict__ node_X, const double2* __restrict__ Ftab,
     double2* __restrict__ L) {
+  pdl_enter();
   constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), G = kTreeGroups, GT = tree_group_threads<P>();
   __shared__ double2 sF[G][NF];
   __shared__ double2 sL[ND * NF];
@@ -719,6 +722,7 @@ __global__ void __launch_bounds__(128) k_targets_ax(const NearBlockDev* __restri
                                                     const int* __restrict__ point_dof_off, const int* __restrict__ point_dof,
                                                     const int* __restrict__ dof_kind, const double* __restrict__ diag,
                                                     double* __restrict__ rows, int chunk) {
+  pdl_enter();
   constexpr int NC = ncoef(P);
   extern __shared__ double2 smem[];
   double* xs = reinterpret_cast<double*>(smem);  // [chunk] x of the block's DOFs
@@ -1134,16 +1138,15 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
   constexpr int tpb_coef = ((NC + 31) / 32) * 32;
   int launches = 0;
   if ((stages & STAGE_P2M) && a.n_leaves > 0 && ND == 1 && a.ax && a.p2m_C) {
-    k_p2m_apply<P><<<a.n_leaves, tpb_coef, 0, st>>>(a.leaves, a.leaf_dof_off, a.leaf_dof, a.p2m_C, a.ax, a.M);
+    launch_pdl(k_p2m_apply<P>, a.n_leaves, tpb_coef, 0, st, a.leaves, a.leaf_dof_off, a.leaf_dof, a.p2m_C, a.ax, a.M);
     ++launches;
   } else if ((stages & STAGE_P2M) && a.n_leaves > 0) {
     k_p2m<P, ND><<<a.n_leaves, 128, 0, st>>>(a.leaves, a.node_fb, a.node_fe, a.node_X, a.e_q, a.e_W, a.e_n, a.e_dof, a.phi, a.phin, a.M);
     ++launches;
   }
   if ((stages & STAGE_M2M) && a.n_m2m_ready > 0) {
-    k_m2m_up<P, ND><<<a.n_m2m_ready, kTreeGroups * tree_group_threads<P>(), 0, st>>>(a.m2m_ready, a.node_parent, a.node_level, a.m2m_nsig,
-                                                                                  a.m2m_cnt, a.child_begin, a.child_end, a.node_children,
-                                                                                  a.node_X, a.Ftab, a.M);
+    launch_pdl(k_m2m_up<P, ND>, a.n_m2m_ready, kTreeGroups * tree_group_threads<P>(), 0, st, a.m2m_ready, a.node_parent, a.node_level,
+               a.m2m_nsig, a.m2m_cnt, a.child_begin, a.child_end, a.node_children, a.node_X, a.Ftab, a.M);
     ++launches;
   }
   if (stages & STAGE_M2L) {
@@ -1164,7 +1167,7 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     for (int l = 0; l < a.n_levels; ++l) {
       const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
       if (cnt > 0) {
-        k_l2l<P, ND><<<cnt, kTreeGroups * tree_group_threads<P>(), 0, st>>>(a.level_parents + a.level_parent_off[l], a.child_begin,
+        launch_pdl(k_l2l<P, ND>, cnt, kTreeGroups * tree_group_threads<P>(), 0, st, a.level_parents + a.level_parent_off[l], a.child_begin,
                                                                             a.child_end, a.node_children, a.node_X,
                                                                             a.Ftab + (size_t)l * 8 * (P + 1) * (P + 1), a.L);
         ++launches;
@@ -1173,10 +1176,10 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
   if ((stages & STAGE_TARGETS) && a.n_blocks > 0 && ND == 1 && a.ax && (a.Wc || a.Wc32)) {
     const size_t shm = sizeof(double) * (size_t)(a.chunk + a.max_ntgt);
     if (a.Wc32)
-      k_targets_ax<P, float><<<a.n_blocks, 128, shm, st>>>(a.blocks, a.nb_dofs, a.nb_targets, a.Wc32, a.Xs, a.node_X, a.L, a.ax,
+      launch_pdl(k_targets_ax<P, float>, a.n_blocks, 128, shm, st, a.blocks, a.nb_dofs, a.nb_targets, a.Wc32, a.Xs, a.node_X, a.L, a.ax,
                                                            a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk);
     else
-      k_targets_ax<P, double><<<a.n_blocks, 128, shm, st>>>(a.blocks, a.nb_dofs, a.nb_targets, a.Wc, a.Xs, a.node_X, a.L, a.ax,
+      launch_pdl(k_targets_ax<P, double>, a.n_blocks, 128, shm, st, a.blocks, a.nb_dofs, a.nb_targets, a.Wc, a.Xs, a.node_X, a.L, a.ax,
                                                             a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk);
     ++launches;
   } else if ((stages & STAGE_TARGETS) && a.n_blocks > 0) {

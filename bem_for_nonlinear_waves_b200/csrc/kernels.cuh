@@ -4,7 +4,36 @@
 
 #include <cstdint>
 
+#include <utility>
+
 namespace bemb200 {
+
+// Programmatic dependent launch for the kernels of an operator application: each is launched
+// with programmatic stream serialisation and starts with pdl_enter(), which waits until the
+// previous kernel in the stream has completed and its writes are visible, then lets the next
+// kernel's blocks be scheduled while this one runs.  The chain stays ordered (every kernel
+// waits for its predecessor before touching memory); only the launch latency between
+// consecutive kernels is hidden.  Kernels launched this way must call pdl_enter() first.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+#endif
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 struct NearBlockDev {
   int64_t w_off;   // first weight of this block's rows

@@ -154,6 +154,7 @@ __global__ void __launch_bounds__(128) k_tc_tables(int ntab, const double* __res
 template <int P, int ND>
 __global__ void k_tc_expand(int nnodes, const double2* __restrict__ M, const double* __restrict__ node_dL,
                             const double* __restrict__ alpha, __half* __restrict__ Mt, float* __restrict__ escale) {
+  pdl_enter();
   using D = TcDims<P>;
   constexpr int NC = ncoef(P), PER = (D::KP + 31) / 32;
   const int lane = threadIdx.x & 31;
@@ -242,6 +243,7 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
     k_m2l_tc(const __grid_constant__ CUtensorMap rows_map, int nitems, const int* __restrict__ item_tab, const int* __restrict__ item_begin,
              const int* __restrict__ item_cnt, int npairs, const int* __restrict__ tc_src, const __half* __restrict__ Ttab,
              const __half* __restrict__ Mt, float* __restrict__ Y, int* __restrict__ err) {
+  pdl_enter();
   using D = TcDims<P>;
   extern __shared__ __align__(128) unsigned char sm_raw[];
   unsigned char* sm_tc = sm_raw + ((1024u - (smem_u32(sm_raw) & 1023u)) & 1023u);
@@ -460,6 +462,7 @@ __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, c
                                 const int* __restrict__ m2l_src, const int* __restrict__ pos, const float* __restrict__ escale,
                                 const double* __restrict__ node_dL, const double* __restrict__ alpha, const float* __restrict__ Y,
                                 double2* __restrict__ L) {
+  pdl_enter();
   using D = TcDims<P>;
   constexpr int NC = ncoef(P), V = D::KPO / 32;
   const int lane = threadIdx.x & 31;
@@ -541,23 +544,25 @@ int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts, int nd) {
   if (parts & TC_EXPAND) {
     const int ge = (int)std::min<int64_t>(((int64_t)a.n_nodes * 32 + 255) / 256, 148 * 8);
     if (nd == 1)
-      k_tc_expand<P, 1><<<ge, 256, 0, st>>>(a.n_nodes, a.M, a.node_dL, a.tc_alpha, Mt, a.tc_escale);
+      launch_pdl(k_tc_expand<P, 1>, ge, 256, 0, st, a.n_nodes, (const double2*)a.M, (const double*)a.node_dL, (const double*)a.tc_alpha,
+                 Mt, a.tc_escale);
     else
-      k_tc_expand<P, 2><<<ge, 256, 0, st>>>(a.n_nodes, a.M, a.node_dL, a.tc_alpha, Mt, a.tc_escale);
+      launch_pdl(k_tc_expand<P, 2>, ge, 256, 0, st, a.n_nodes, (const double2*)a.M, (const double*)a.node_dL, (const double*)a.tc_alpha,
+                 Mt, a.tc_escale);
     ++launches;
   }
   if (parts & TC_CONTRACT) {
     const int grid = a.n_tc_items < a.tc_grid ? a.n_tc_items : a.tc_grid;
     CUtensorMap map;
     std::memcpy(&map, a.tc_rows_map, sizeof(map));
-    k_m2l_tc<P><<<grid, kEpilogue + kProducers + kIssuer, D::SMEM, st>>>(map, a.n_tc_items, a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt,
+    launch_pdl(k_m2l_tc<P>, grid, kEpilogue + kProducers + kIssuer, D::SMEM, st, map, a.n_tc_items, a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt,
                                                                          a.n_tc_pairs, a.tc_src, static_cast<const __half*>(a.tc_tab),
                                                                          static_cast<const __half*>(a.tc_Mt), a.tc_Y, a.tc_err);
     ++launches;
   }
   if (parts & TC_REDUCE) {
     const int gr = (int)std::min<int64_t>(((int64_t)a.n_m2l_targets * 32 + 255) / 256, 148 * 16);
-    k_m2l_tc_reduce<P><<<gr, 256, 0, st>>>(a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.m2l_src, a.tc_pos, a.tc_escale, a.node_dL,
+    launch_pdl(k_m2l_tc_reduce<P>, gr, 256, 0, st, a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.m2l_src, a.tc_pos, a.tc_escale, a.node_dL,
                                            a.tc_alpha, a.tc_Y, a.L);
     ++launches;
   }
