@@ -24,6 +24,7 @@ constexpr int kDotCols = 8;  // basis columns per pass of the multi-dot
 // partial[b][c] = sum over block b's rows of V[:, c] . w, c = 0..ncol-1 with ncol = st->n + 1
 __global__ void __launch_bounds__(256) k_mdot_dev(const double* __restrict__ V, int ldv, const ArnoldiState* __restrict__ st,
                                                   const double* __restrict__ w, int nrow, double* __restrict__ partial, int pstride) {
+  pdl_enter();
   __shared__ double red[8][kDotCols];
   const int ncol = st->n + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -56,6 +57,7 @@ __global__ void __launch_bounds__(256) k_mdot_dev(const double* __restrict__ V, 
 // out[c] = sum_b partial[b][c], block per column (columns beyond st->n are skipped)
 __global__ void k_mdot_final_dev(const double* __restrict__ partial, int nblk, int pstride, const ArnoldiState* __restrict__ st,
                                  int self_dot, double* __restrict__ out) {
+  pdl_enter();
   const int c = blockIdx.x;
   const int ncol = self_dot ? 1 : st->n + 1;
   if (c >= ncol) return;
@@ -74,6 +76,7 @@ __global__ void k_mdot_final_dev(const double* __restrict__ partial, int nblk, i
 
 // partial[b][0] = w . w over block b's rows
 __global__ void __launch_bounds__(256) k_selfdot(const double* __restrict__ w, int nrow, double* __restrict__ partial, int pstride) {
+  pdl_enter();
   __shared__ double red[8];
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) s = fma(w[i], w[i], s);
@@ -90,6 +93,7 @@ __global__ void __launch_bounds__(256) k_selfdot(const double* __restrict__ w, i
 // w -= V[:, 0..n] h
 __global__ void k_maxpy_dev(const double* __restrict__ V, int ldv, const ArnoldiState* __restrict__ st, const double* __restrict__ h,
                             double* __restrict__ w, int nrow) {
+  pdl_enter();
   extern __shared__ double sh[];
   const int ncol = st->n + 1;
   for (int c = threadIdx.x; c < ncol; c += blockDim.x) sh[c] = h[c];
@@ -104,6 +108,7 @@ __global__ void k_maxpy_dev(const double* __restrict__ V, int ldv, const Arnoldi
 // operator input: x = (dinv .*) V[:, n]
 __global__ void k_arn_prep(int nrow, const double* __restrict__ V, const double* __restrict__ dinv, const ArnoldiState* __restrict__ st,
                            double* __restrict__ x) {
+  pdl_enter();
   const double* v = V + (size_t)st->n * nrow;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) x[i] = dinv ? dinv[i] * v[i] : v[i];
 }
@@ -113,6 +118,7 @@ __global__ void k_arn_prep(int nrow, const double* __restrict__ V, const double*
 __global__ void k_arn_givens(ArnoldiState* __restrict__ st, const double* __restrict__ h1, const double* __restrict__ h2,
                              const double* __restrict__ hn, double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
                              double* __restrict__ R, int ldr) {
+  pdl_enter();
   // the warp stages the column and the rotations in shared memory, lane 0 runs the serial
   // rotation chain there, the warp stores the rotated column into R
   extern __shared__ double sg[];  // h [k+1], cs [k], sn [k]
@@ -166,6 +172,7 @@ __global__ void k_arn_givens(ArnoldiState* __restrict__ st, const double* __rest
 
 // V[:, n] = w / h_{n,n-1} (n already advanced)
 __global__ void k_arn_normalize(int nrow, const double* __restrict__ w, const ArnoldiState* __restrict__ st, double* __restrict__ V) {
+  pdl_enter();
   double* v = V + (size_t)st->n * nrow;
   const double s = st->inv_h;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) v[i] = w[i] * s;
@@ -224,22 +231,22 @@ int arnoldi_dot_blocks(int n) {
 int launch_arnoldi_step(const ArnoldiArgs& a, cudaStream_t st) {
   const int g = grid_rows(a.nrow);
   const int db = arnoldi_dot_blocks(a.nrow);
-  k_arn_prep<<<g, 256, 0, st>>>(a.nrow, a.V, a.dinv, a.state, a.x);
+  launch_pdl(k_arn_prep, g, 256, 0, st, a.nrow, a.V, a.dinv, a.state, a.x);
   int launches = 1 + launch_matvec(a.p, a.mv, st);
   double* h1 = a.h;
   double* h2 = a.h + a.cols;
   double* hn = a.h + 2 * a.cols;
   for (int pass = 0; pass < 2; ++pass) {
     double* hp = pass == 0 ? h1 : h2;
-    k_mdot_dev<<<db, 256, 0, st>>>(a.V, a.nrow, a.state, a.w, a.nrow, a.partial, a.cols);
-    k_mdot_final_dev<<<a.cols, 256, 0, st>>>(a.partial, db, a.cols, a.state, 0, hp);
-    k_maxpy_dev<<<g, 256, sizeof(double) * a.cols, st>>>(a.V, a.nrow, a.state, hp, a.w, a.nrow);
+    launch_pdl(k_mdot_dev, db, 256, 0, st, a.V, a.nrow, a.state, a.w, a.nrow, a.partial, a.cols);
+    launch_pdl(k_mdot_final_dev, a.cols, 256, 0, st, a.partial, db, a.cols, a.state, 0, hp);
+    launch_pdl(k_maxpy_dev, g, 256, sizeof(double) * a.cols, st, a.V, a.nrow, a.state, hp, a.w, a.nrow);
     launches += 3;
   }
-  k_selfdot<<<db, 256, 0, st>>>(a.w, a.nrow, a.partial, a.cols);
-  k_mdot_final_dev<<<1, 256, 0, st>>>(a.partial, db, a.cols, a.state, 1, hn);
-  k_arn_givens<<<1, 32, sizeof(double) * (3 * a.cols + 1), st>>>(a.state, h1, h2, hn, a.cs, a.sn, a.g, a.R, a.cols);
-  k_arn_normalize<<<g, 256, 0, st>>>(a.nrow, a.w, a.state, a.V);
+  launch_pdl(k_selfdot, db, 256, 0, st, a.w, a.nrow, a.partial, a.cols);
+  launch_pdl(k_mdot_final_dev, 1, 256, 0, st, a.partial, db, a.cols, a.state, 1, hn);
+  launch_pdl(k_arn_givens, 1, 32, sizeof(double) * (3 * a.cols + 1), st, a.state, h1, h2, hn, a.cs, a.sn, a.g, a.R, a.cols);
+  launch_pdl(k_arn_normalize, g, 256, 0, st, a.nrow, a.w, a.state, a.V);
   return launches + 4;
 }
 
