@@ -261,13 +261,25 @@ def run_batch(args, cfg, local):
     with ClockSampler(local) as clk:
         w0 = time.perf_counter()
         sub = {}
-        for t, d, kv in probs:
-            sub[bs.submit(t.X, t.tri, t.face_dirichlet, kv, dofs=d)] = time.perf_counter()
         lat = {}
-        while len(lat) < len(sub):
+
+        def reap():
             for tk in sub:
                 if tk not in lat and bs.done(tk):
                     lat[tk] = time.perf_counter() - sub[tk]
+
+        # all at once, or Poisson arrivals at --arrival-rate requests/s (seeded)
+        gaps = np.random.default_rng(77).exponential(1.0 / args.arrival_rate, len(probs)) if args.arrival_rate > 0 else None
+        t_next = w0
+        for i, (t, d, kv) in enumerate(probs):
+            if gaps is not None:
+                t_next += gaps[i]
+                while time.perf_counter() < t_next:
+                    reap()
+                    time.sleep(0.0002)
+            sub[bs.submit(t.X, t.tri, t.face_dirichlet, kv, dofs=d)] = time.perf_counter()
+        while len(lat) < len(sub):
+            reap()
             time.sleep(0.0005)
         batch_s = time.perf_counter() - w0
     conv = all(bs.result(tk)[2].converged for tk in sub)
@@ -278,7 +290,8 @@ def run_batch(args, cfg, local):
             "higher_is_better": True, "dtype": "f64/f16x3-tc" if args.precision == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": "mixed_2k_80k_p8" if args.mixed_sizes else args.config, "problems": len(probs),
                        "points": [int(p[0].n_points) for p in probs], "workers": args.workers, "precision": args.precision,
-                       "preconditioner": args.precond, "converged": bool(conv)},
+                       "preconditioner": args.precond, "converged": bool(conv),
+                       "arrivals": f"poisson {args.arrival_rate}/s" if args.arrival_rate > 0 else "all at once"},
             "latency_s": {"p50": pct(lats, 50), "p99": pct(lats, 99), "max": lats[-1]},
             "sequential": {"solves_per_s": len(probs) / seq_s, "latency_p50_s": pct(seq_lat, 50)},
             "clocks": clk.summary()}
@@ -302,6 +315,7 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="serving mode: number of problems (one GPU)")
     ap.add_argument("--workers", type=int, default=2)
     ap.add_argument("--mixed-sizes", action="store_true", help="serving mode over tanks of 2k-80k points (p = 8)")
+    ap.add_argument("--arrival-rate", type=float, default=0.0, help="serving mode: Poisson arrivals per second (0: all at once)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
