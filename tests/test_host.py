@@ -12,7 +12,8 @@ from bem_for_nonlinear_waves_b200.bvp import inspect_plan
 
 
 def header_functions():
-    src = open(os.path.join(ROOT, "include", "bem_b200.h")).read()
+    with open(os.path.join(ROOT, "include", "bem_b200.h")) as fh:
+        src = fh.read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(bem_\w+)\s*\(", src)))
 

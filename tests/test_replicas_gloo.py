@@ -36,7 +36,7 @@ def _worker(rank, world, port, out):
 
 def test_two_gloo_replicas():
     world = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_worker, args=(world, _free_port(), out), nprocs=world, join=True)
         r = dict(out)
