@@ -371,6 +371,20 @@ def main():
     barrier(world)
     dev_max, e2e_max = allreduce_max([dev_s, e2e_s], world)
     ans = bvp.ans.copy()
+    # the same solves through the batch API with two worker contexts: the host set-up of one
+    # problem overlaps the device solve of the previous one (host arrays in and out)
+    from bem_for_nonlinear_waves_b200 import BatchSolver
+    bs = BatchSolver(2, expansion_order=cfg["p"], solver_tol=cfg["rel_tol"], tol_relative=True, solver_max_iter=args.max_iter,
+                     preconditioner=args.precond, device=local, precision=args.precision)
+    for tk in [bs.submit(t.X, t.tri, t.face_dirichlet, kv, dofs=d) for _ in range(2)]:
+        bs.result(tk)
+    nb = max(2 * args.steps, 4)
+    w0 = time.perf_counter()
+    for tk in [bs.submit(t.X, t.tri, t.face_dirichlet, kv, dofs=d) for _ in range(nb)]:
+        bs.result(tk)
+    e2e_batch = {"value": nb / (time.perf_counter() - w0), "unit": "solves/s", "workers": 2, "solves": nb,
+                 "note": "the same problem submitted nb times through bem_gpu_batch_*; host arrays in and out"}
+    bs.close()
     # a second right-hand side on the same set-up (phi_t BVP / next stage with unchanged
     # geometry): the solve alone, host arrays in and out
     kv2 = -0.7 * kv + 0.01 * np.random.default_rng(7).standard_normal(kv.shape)
@@ -459,6 +473,7 @@ def main():
         "matvec_stage_ms": prof,
         "e2e": {"value": world * args.steps / e2e_max, "unit": "solves/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
+        "e2e_batch": e2e_batch,
         "gpu_launches": launches,
         "steps_detail": steps_detail,
         "resolve_same_setup": resolve,
