@@ -22,7 +22,7 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-rela
 CXXFLAGS = ["-O2", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-Wall", "-fopenmp", "-pthread"]
 
 CU_SOURCES = ["kernels.cu", "m2l_tc.cu", "gmres.cu", "capi.cu", "mel.cu"]
-CXX_SOURCES = ["plan.cpp", "batch.cpp"]
+CXX_SOURCES = ["plan.cpp", "batch.cpp", "poly.cpp"]
 
 
 def _run(cmd):

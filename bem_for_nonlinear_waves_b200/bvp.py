@@ -40,7 +40,7 @@ def build_dofs(X, tri, face_dirichlet):
 
 
 def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter, device,
-               tol_relative, preconditioner, precision):
+               tol_relative, preconditioner, precision, poly_degree=8):
     o = L.Opts()
     lib.bem_gpu_default_opts(ctypes.byref(o))
     o.expansion_order = int(expansion_order)
@@ -51,7 +51,8 @@ def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_l
     o.max_iter = int(solver_max_iter)
     o.device = int(device)
     o.tol_relative = 1 if tol_relative else 0
-    o.preconditioner = {"none": 0, "jacobi": 1}[preconditioner]
+    o.preconditioner = {"none": 0, "jacobi": 1, "near_poly": 2}[preconditioner]
+    o.poly_degree = int(poly_degree)
     o.precision = {"fp64": 0, "mixed": 1}[precision]
     return o
 
@@ -61,7 +62,7 @@ class BEM_BVP:
 
     def __init__(self, X, tri, face_dirichlet, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30,
                  fmm_max_level=7, solver_tol=1e-9, solver_max_iter=500, device=0, dofs=None, tol_relative=False, preconditioner="none",
-                 precision="fp64"):
+                 precision="fp64", poly_degree=8):
         self.lib = L.load()
         if not self.lib.bem_gpu_is_available():
             raise RuntimeError("no sm_100 CUDA device visible: the GMRES-FMM solver runs only on the GPU")
@@ -69,7 +70,7 @@ class BEM_BVP:
         self.tri = np.ascontiguousarray(tri, np.int32)
         self.face_dirichlet = np.ascontiguousarray(face_dirichlet, np.uint8)
         o = _make_opts(self.lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter,
-                       device, tol_relative, preconditioner, precision)
+                       device, tol_relative, preconditioner, precision, poly_degree)
         self.opts = o
         self.ctx = self.lib.bem_gpu_create(ctypes.byref(o))
         if not self.ctx:
@@ -155,6 +156,16 @@ class BEM_BVP:
         self._check(self.lib.bem_gpu_point_integrals(self.ctx, L.ptr(phi, L.P_dbl), L.ptr(phin, L.P_dbl), L.ptr(a, L.P_dbl),
                                                      L.ptr(b, L.P_dbl)), "point_integrals")
         return a, b
+
+    def poly_roots(self):
+        """Roots of the near-field polynomial preconditioner (preconditioner="near_poly") formed by
+        the last set-up, in the order they are applied; a conjugate pair is one complex entry
+        with positive imaginary part.  Empty when none was formed (Jacobi scaling alone)."""
+        re = np.zeros(32)
+        im = np.zeros(32)
+        n = self.lib.bem_gpu_poly_roots(self.ctx, 32, L.ptr(re, L.P_dbl), L.ptr(im, L.P_dbl))
+        self._check(min(n, 0), "bem_gpu_poly_roots")
+        return re[:n] + 1j * im[:n]
 
     def diag(self):
         out = np.zeros(self.matrix_size)
@@ -243,12 +254,13 @@ class BatchSolver:
     phi / phin fields BEM_BVP::solve() leaves behind (bem/BEM_solveBVP.hpp:376-410)."""
 
     def __init__(self, n_workers=2, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30, fmm_max_level=7,
-                 solver_tol=1e-9, solver_max_iter=500, device=0, tol_relative=False, preconditioner="none", precision="fp64"):
+                 solver_tol=1e-9, solver_max_iter=500, device=0, tol_relative=False, preconditioner="none", precision="fp64",
+                 poly_degree=8):
         self.lib = L.load()
         if not self.lib.bem_gpu_is_available():
             raise RuntimeError("no sm_100 CUDA device visible: the GMRES-FMM solver runs only on the GPU")
         o = _make_opts(self.lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter,
-                       device, tol_relative, preconditioner, precision)
+                       device, tol_relative, preconditioner, precision, poly_degree)
         self.handle = self.lib.bem_gpu_batch_create(ctypes.byref(o), int(n_workers))
         if not self.handle:
             raise RuntimeError("bem_gpu_batch_create failed")

@@ -84,6 +84,8 @@ double now_s() { return std::chrono::duration<double>(std::chrono::steady_clock:
 }  // namespace
 
 constexpr int kErrRing = 8;  // residual estimates in flight (>= the read-back lag + 1)
+constexpr int kMaxPolyDegree = 24;
+inline int poly_degree(const bem_gpu_opts& o) { return o.poly_degree > 0 ? o.poly_degree : 8; }
 
 struct bem_gpu_ctx {
   bem_gpu_opts opts{};
@@ -95,7 +97,7 @@ struct bem_gpu_ctx {
 
   // geometry / tree
   DBuf<double> Xs, e_q, e_W, e_n, e_near, node_X, WG, WGn, Wc, diag;
-  DBuf<float> Wc32;  // combined near weights of A.x in FP32 (mixed precision)
+  DBuf<float> Wc32;  // combined near weights of A.x in FP32 (mixed precision, polynomial preconditioner)
   DBuf<int> leaf_dof_off, leaf_dof, e_slot, slot_block;  // P2M operator of A.x: DOFs per leaf
   DBuf<double2> p2m_C;                       // [(leaf, DOF)][NC]
   DBuf<double2> near_scratch;                // element values of the near-weight kernel
@@ -145,7 +147,11 @@ struct bem_gpu_ctx {
   cudaGraphExec_t arn_exec = nullptr;
   int arn_kernels = 0;
   const void* arn_key_V = nullptr;
-  int arn_key_cols = 0, arn_key_jacobi = -1, arn_key_mixed = -1;
+  int arn_key_cols = 0, arn_key_prec = -1, arn_key_mixed = -1;
+  // polynomial preconditioner: roots (from the set-up), Arnoldi basis of the root run,
+  // apply scratch, and Z = M V (the iterate is updated from Z)
+  PolyRoots poly;
+  DBuf<double> poly_V, poly_h, poly_part, poly_prod, poly_y, Z;
   double* arn_err_host = nullptr;
   cudaEvent_t arn_ev[kErrRing] = {};
   // accounting of the current setup + solve
@@ -238,6 +244,12 @@ struct bem_gpu_ctx {
     a.p2m_C = p2m_C.p;
     a.Wc = lowp ? nullptr : Wc.p;
     a.Wc32 = lowp ? Wc32.p : nullptr;
+  }
+  // the near-field part of A.x (FP32 weights where built): mv_in -> mv_out
+  MatvecArgs near_args() const {
+    MatvecArgs a = args(nullptr, nullptr, mv_out.p, nullptr, nullptr);
+    set_ax(a, Wc32.p != nullptr);
+    return a;
   }
   // switches an argument set to the tensor-core M2L
   void set_tc(MatvecArgs& a) const {
@@ -349,8 +361,9 @@ int build_graph(bem_gpu_ctx* ctx) {
   return capture_matvec(ctx, true, ctx->graph_lo, ctx->graph_exec_lo, ctx->graph_kernels_lo);
 }
 
-// (Re)captures the Arnoldi step graph when the basis, its capacity or the operator changed.
-int ensure_arnoldi_graph(bem_gpu_ctx* ctx, bool jacobi, bool lowp, int cols) {
+// (Re)captures the Arnoldi step graph when the basis, its capacity, the operator or the
+// preconditioner (0 none, 1 Jacobi, 2 polynomial) changed.
+int ensure_arnoldi_graph(bem_gpu_ctx* ctx, int prec, bool lowp, int cols) {
   const int N = ctx->plan.ndof;
   if (ctx->arn_cs.n < (size_t)cols) {
     CK(ctx->arn_state.alloc(1));
@@ -364,7 +377,11 @@ int ensure_arnoldi_graph(bem_gpu_ctx* ctx, bool jacobi, bool lowp, int cols) {
     CK(cudaHostAlloc((void**)&ctx->arn_err_host, sizeof(double) * kErrRing, cudaHostAllocDefault));
     for (auto& e : ctx->arn_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
-  if (ctx->arn_exec && ctx->arn_key_V == ctx->V.p && ctx->arn_key_cols == cols && ctx->arn_key_jacobi == (int)jacobi &&
+  if (prec == 2 && ctx->poly_prod.n < (size_t)N) {
+    CK(ctx->poly_prod.alloc(N));
+    CK(ctx->poly_y.alloc(N));
+  }
+  if (ctx->arn_exec && ctx->arn_key_V == ctx->V.p && ctx->arn_key_cols == cols && ctx->arn_key_prec == prec &&
       ctx->arn_key_mixed == (int)lowp)
     return BEM_OK;
   if (ctx->arn_exec) {
@@ -380,7 +397,7 @@ int ensure_arnoldi_graph(bem_gpu_ctx* ctx, bool jacobi, bool lowp, int cols) {
   a.cols = cols;
   a.p = ctx->plan.opt.p;
   a.V = ctx->V.p;
-  a.dinv = jacobi ? ctx->dinv.p : nullptr;
+  a.dinv = prec != 0 ? ctx->dinv.p : nullptr;
   a.state = ctx->arn_state.p;
   a.x = ctx->mv_in.p;
   a.w = ctx->mv_out.p;
@@ -393,6 +410,13 @@ int ensure_arnoldi_graph(bem_gpu_ctx* ctx, bool jacobi, bool lowp, int cols) {
   a.sn = ctx->arn_sn.p;
   a.g = ctx->arn_g.p;
   a.R = ctx->arn_R.p;
+  if (prec == 2) {
+    a.poly = &ctx->poly;
+    a.near = ctx->near_args();
+    a.prod = ctx->poly_prod.p;
+    a.y = ctx->poly_y.p;
+    a.Z = ctx->Z.p;
+  }
   if (configure_arnoldi(cols) != 0) {
     ctx->err = "GMRES basis too large for the on-device Givens step (max_iter > 9000)";
     return BEM_ERR_UNSUPPORTED;
@@ -413,7 +437,7 @@ int ensure_arnoldi_graph(bem_gpu_ctx* ctx, bool jacobi, bool lowp, int cols) {
   }
   ctx->arn_key_V = ctx->V.p;
   ctx->arn_key_cols = cols;
-  ctx->arn_key_jacobi = (int)jacobi;
+  ctx->arn_key_prec = prec;
   ctx->arn_key_mixed = (int)lowp;
   return BEM_OK;
 }
@@ -495,6 +519,72 @@ int bem_gpu_build_dofs(int32_t n_points, const double* X, int32_t n_faces, const
   return n < 0 ? BEM_ERR_INVALID_ARGUMENT : n;
 }
 
+// Roots of the near-field polynomial preconditioner: k Arnoldi steps (classical Gram-Schmidt
+// twice) on B = A_near D^{-1} from a fixed pseudo-random start, the Hessenberg matrix read
+// back after each step; harmonic Ritz values of the run in Leja order.  A breakdown ends the
+// run early (lower degree); roots that cannot be formed leave the polynomial empty and the
+// solve falls back to the Jacobi scaling.
+static int build_poly(bem_gpu_ctx* ctx) {
+  const int N = ctx->plan.ndof, k = poly_degree(ctx->opts), p = ctx->plan.opt.p;
+  cudaStream_t s = ctx->stream;
+  const MatvecArgs nm = ctx->near_args();
+  double* Vp = ctx->poly_V.p;
+  double* hd = ctx->poly_h.p;
+  std::vector<double> H((size_t)(k + 1) * k, 0.0), hh((size_t)3 * (k + 1));
+  launch_hash_fill(N, 0x5eedULL, ctx->mv_out.p, s);
+  launch_mdot(ctx->mv_out.p, N, 1, ctx->mv_out.p, N, ctx->poly_part.p, hd, s);
+  CK(cudaMemcpyAsync(hh.data(), hd, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  launch_axpby(N, 1.0 / std::sqrt(hh[0]), ctx->mv_out.p, 0.0, Vp, s);
+  ctx->launches += 4;
+  int steps = 0;
+  double hscale = 0.0;
+  for (int j = 0; j < k; ++j) {
+    launch_mul(N, ctx->dinv.p, Vp + (size_t)j * N, ctx->mv_in.p, s);
+    ctx->launches += 1 + launch_near_only(p, nm, s);
+    double* w = ctx->mv_out.p;
+    for (int pass = 0; pass < 2; ++pass) {
+      launch_mdot(Vp, N, j + 1, w, N, ctx->poly_part.p, hd + pass * (k + 1), s);
+      launch_maxpy(Vp, N, j + 1, hd + pass * (k + 1), w, N, s);
+    }
+    launch_mdot(w, N, 1, w, N, ctx->poly_part.p, hd + 2 * (k + 1), s);
+    ctx->launches += 8;
+    CK(cudaMemcpyAsync(hh.data(), hd, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int i = 0; i <= j; ++i) {
+      H[(size_t)i * k + j] = hh[i] + hh[(k + 1) + i];
+      hscale = std::max(hscale, std::abs(H[(size_t)i * k + j]));
+    }
+    const double hn = std::sqrt(std::max(hh[2 * (k + 1)], 0.0));
+    H[(size_t)(j + 1) * k + j] = hn;
+    steps = j + 1;
+    if (!std::isfinite(hn) || !(hn > 1e-12 * hscale)) break;  // (near-)invariant subspace
+    if (j + 1 < k) {
+      launch_axpby(N, 1.0 / hn, w, 0.0, Vp + (size_t)(j + 1) * N, s);
+      ctx->launches += 1;
+    }
+  }
+  CK(cudaGetLastError());
+  if (steps < k) {  // the leading steps x steps block with its own subdiagonal entry
+    std::vector<double> Hs((size_t)(steps + 1) * steps);
+    for (int i = 0; i <= steps; ++i)
+      for (int j = 0; j < steps; ++j) Hs[(size_t)i * steps + j] = H[(size_t)i * k + j];
+    H.swap(Hs);
+  }
+  if (poly_roots_from_hessenberg(steps, H.data(), steps, ctx->poly) != 0) ctx->poly.n = 0;
+  return BEM_OK;
+}
+
+int bem_gpu_poly_roots(bem_gpu_ctx* ctx, int32_t cap, double* re, double* im) {
+  if (!ctx || cap < 0 || (cap > 0 && (!re || !im))) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  for (int i = 0; i < ctx->poly.n && i < cap; ++i) {
+    re[i] = ctx->poly.re[i];
+    im[i] = ctx->poly.im[i];
+  }
+  return ctx->poly.n;
+}
+
 int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   if (!ctx || !d) return BEM_ERR_INVALID_ARGUMENT;
   CK(cudaSetDevice(ctx->opts.device));
@@ -507,6 +597,11 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   }
   if (ctx->opts.precision != 0 && ctx->opts.precision != 1) {
     ctx->err = "precision must be 0 (fp64) or 1 (mixed)";
+    return BEM_ERR_INVALID_ARGUMENT;
+  }
+  if (ctx->opts.preconditioner < 0 || ctx->opts.preconditioner > 2 || ctx->opts.poly_degree < 0 ||
+      ctx->opts.poly_degree > kMaxPolyDegree) {
+    ctx->err = "preconditioner must be 0 (none), 1 (Jacobi) or 2 (near-field polynomial, degree 0..24; 0: 8)";
     return BEM_ERR_INVALID_ARGUMENT;
   }
   PlanOptions po;
@@ -755,8 +850,15 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   CK(ctx->WG.alloc(std::max<int64_t>(P.nnz, 1)));
   CK(ctx->WGn.alloc(std::max<int64_t>(P.nnz, 1)));
   CK(ctx->Wc.alloc(std::max<int64_t>(P.nnz, 1)));
-  if (ctx->opts.precision == 1) CK(ctx->Wc32.alloc(std::max<int64_t>(ctx->w4_total, 1)));
+  const bool want_w32 = ctx->opts.precision == 1 || ctx->opts.preconditioner == 2;
+  if (want_w32) CK(ctx->Wc32.alloc(std::max<int64_t>(ctx->w4_total, 1)));
   const int N = P.ndof;
+  if (ctx->opts.preconditioner == 2) {
+    const int k = poly_degree(ctx->opts);
+    CK(ctx->poly_V.alloc((size_t)(k + 1) * N));
+    CK(ctx->poly_h.alloc((size_t)3 * (k + 1)));
+    CK(ctx->poly_part.alloc((size_t)mdot_blocks(N) * (k + 1)));
+  }
   CK(ctx->phi.alloc(N));
   CK(ctx->phin.alloc(N));
   CK(ctx->known_s.alloc(N));
@@ -839,8 +941,8 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   }
   launch_near_weights(na, s);
   launch_combine_weights((int)P.blocks.size(), ctx->blocks.p, ctx->nb_dofs.p, ctx->dof_kind.p, ctx->WG.p, ctx->WGn.p, ctx->Wc.p,
-                         ctx->opts.precision == 1 ? ctx->Wc32.p : nullptr, s);
-  ctx->launches += ctx->opts.precision == 1 ? 2 : 1;
+                         want_w32 ? ctx->Wc32.p : nullptr, s);
+  ctx->launches += want_w32 ? 2 : 1;
   CK(cudaGetLastError());
   // rigid-mode diagonal (BEM_solveBVP_GMRES_FMM.hpp:2661-2716)
   launch_densities(N, 2, nullptr, nullptr, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, s);  // phi = 1, phin = 0
@@ -853,6 +955,11 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
                 ctx->self_col.p, ctx->WG.p, ctx->WGn.p, ctx->dinv.p, s);
   ctx->launches += 1;
   CK(cudaGetLastError());
+  ctx->poly.n = 0;
+  if (ctx->opts.preconditioner == 2) {
+    const int rc = build_poly(ctx);
+    if (rc != BEM_OK) return rc;
+  }
   CK(cudaEventRecord(ctx->ev[1], s));
   if (ctx->mixed) {  // FP16 tables must stay far from the FP16 range limit (65504)
     unsigned int bits = 0;
@@ -1057,7 +1164,9 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   ctx->h2d = ctx->setup_h2d;
   ctx->d2h = 0;
   ctx->launches = ctx->setup_launches;
-  const bool jacobi = ctx->opts.preconditioner == 1;
+  // preconditioner: 2 falls back to the Jacobi scaling when the set-up formed no polynomial
+  const int prec = (ctx->opts.preconditioner == 2 && ctx->poly.n == 0) ? 1 : ctx->opts.preconditioner;
+  const bool jacobi = prec == 1;
   double tol = ctx->opts.tol;
   const int max_iter = ctx->opts.max_iter;
   for (int i = 0; i < N; ++i)
@@ -1072,8 +1181,9 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   ctx->h2d += 8LL * N;
   CK(cudaEventRecord(ctx->ev[2], s));
   const int cols = max_iter + 2;
-  if (ctx->V_cols < cols || ctx->V.n < (size_t)cols * N) {
+  if (ctx->V_cols < cols || ctx->V.n < (size_t)cols * N || (prec == 2 && ctx->Z.n < (size_t)cols * N)) {
     CK(ctx->V.alloc((size_t)cols * N));
+    if (prec == 2) CK(ctx->Z.alloc((size_t)cols * N));
     ctx->V_cols = cols;
   }
   if (ctx->w.n < (size_t)N) {
@@ -1148,12 +1258,15 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   bool x_zero = (x0 == nullptr);
   // Arnoldi steps run as one graph each (operator + orthogonalisation + Givens update, all
   // state on the device); the host reads each step's residual estimate kLag steps behind.
-  if ((rc = ensure_arnoldi_graph(ctx, jacobi, mixed, cols)) != BEM_OK) return rc;
+  if ((rc = ensure_arnoldi_graph(ctx, prec, mixed, cols)) != BEM_OK) return rc;
   constexpr int kLag = 3;
-  auto x_update = [&]() -> int {  // x = x_base + (D^{-1}) V R^{-1} g over the cycle's steps
+  auto x_update = [&]() -> int {  // x = x_base + M V R^{-1} g over the cycle's steps (M V = Z stored)
     CK(cudaMemcpyAsync(ctx->xdev.p, ctx->xbase.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
     launch_arnoldi_solve_y(ctx->arn_state.p, ctx->arn_R.p, cols, ctx->arn_g.p, ctx->ydev.p, s);
-    if (!jacobi) {
+    if (prec == 2) {
+      launch_arnoldi_update(ctx->Z.p, N, cols, ctx->arn_state.p, ctx->ydev.p, ctx->xdev.p, s);
+      ctx->launches += 2;
+    } else if (!jacobi) {
       launch_arnoldi_update(ctx->V.p, N, cols, ctx->arn_state.p, ctx->ydev.p, ctx->xdev.p, s);
       ctx->launches += 2;
     } else {

@@ -113,6 +113,49 @@ __global__ void k_arn_prep(int nrow, const double* __restrict__ V, const double*
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) x[i] = dinv ? dinv[i] * v[i] : v[i];
 }
 
+// One factor of the polynomial preconditioner p(B) applied to u = V[:, n] (B = A_near D^{-1},
+// 1 - B p(B) = prod over roots of (1 - B / theta)); r = B(prod) or B(w) from the launch before.
+//   mode 0, real root:        y += prod / theta; prod -= r / theta             (c = 1 / theta)
+//   mode 1, pair, first half: w = 2a prod - r; y += w / |theta|^2; next B input w  (c = 1 / |theta|^2)
+//   mode 2, pair, second half: prod -= r / |theta|^2
+// first: prod is V[:, n] and y starts at zero.  last: no further B; x = Z[:, n] = D^{-1} y.
+// Otherwise x = D^{-1} (next B input).
+__global__ void k_poly_factor(int nrow, int mode, int first, int last, double c, double two_a, const double* __restrict__ V,
+                              const ArnoldiState* __restrict__ st, double* __restrict__ prod, const double* __restrict__ r,
+                              double* __restrict__ y, const double* __restrict__ dinv, double* __restrict__ x, double* __restrict__ Z) {
+  pdl_enter();
+  const size_t col = (size_t)st->n * nrow;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) {
+    const double p = first ? V[col + i] : prod[i];
+    double yi = first ? 0.0 : y[i];
+    double nxt = 0.0;
+    if (mode == 0) {
+      yi = fma(p, c, yi);
+      if (!last) {
+        nxt = fma(-r[i], c, p);
+        prod[i] = nxt;
+      }
+    } else if (mode == 1) {
+      const double w = fma(two_a, p, -r[i]);
+      yi = fma(w, c, yi);
+      nxt = w;
+      if (first && !last) prod[i] = p;
+    } else {
+      nxt = fma(-r[i], c, p);
+      prod[i] = nxt;
+    }
+    const double d = dinv ? dinv[i] : 1.0;
+    if (last) {
+      const double z = d * yi;
+      x[i] = z;
+      Z[col + i] = z;
+    } else {
+      if (mode != 2) y[i] = yi;
+      x[i] = d * nxt;
+    }
+  }
+}
+
 // Hessenberg column from the two Gram-Schmidt passes, rotations, new rotation, g update,
 // R column, residual estimate; n advances by one.  Single thread (the column is short).
 __global__ void k_arn_givens(ArnoldiState* __restrict__ st, const double* __restrict__ h1, const double* __restrict__ h2,
@@ -228,11 +271,51 @@ int arnoldi_dot_blocks(int n) {
   return b < 1 ? 1 : (b > 592 ? 592 : b);
 }
 
+// x = Z[:, n] = D^{-1} p(B) V[:, n]: d - 1 applications of the near-field operator for a
+// polynomial of degree d (a conjugate pair takes two, the last factor none after it)
+int launch_poly_apply(const ArnoldiArgs& a, cudaStream_t st) {
+  const int g = grid_rows(a.nrow);
+  const PolyRoots& R = *a.poly;
+  launch_pdl(k_arn_prep, g, 256, 0, st, a.nrow, a.V, a.dinv, a.state, a.x);  // x = D^{-1} V[:, n]
+  int launches = 1;
+  bool first = true;
+  for (int k = 0; k < R.n; ++k) {
+    const bool last = k == R.n - 1;
+    const double re = R.re[k], im = R.im[k];
+    if (im == 0.0) {
+      if (!last) launches += launch_near_only(a.p, a.near, st);
+      launch_pdl(k_poly_factor, g, 256, 0, st, a.nrow, 0, (int)first, (int)last, 1.0 / re, 0.0, (const double*)a.V,
+                 (const ArnoldiState*)a.state, a.prod, (const double*)a.w, a.y, a.dinv, a.x, a.Z);
+      ++launches;
+    } else {
+      const double c = 1.0 / (re * re + im * im);
+      launches += launch_near_only(a.p, a.near, st);
+      launch_pdl(k_poly_factor, g, 256, 0, st, a.nrow, 1, (int)first, (int)last, c, 2.0 * re, (const double*)a.V,
+                 (const ArnoldiState*)a.state, a.prod, (const double*)a.w, a.y, a.dinv, a.x, a.Z);
+      ++launches;
+      if (!last) {
+        launches += launch_near_only(a.p, a.near, st);
+        launch_pdl(k_poly_factor, g, 256, 0, st, a.nrow, 2, 0, 0, c, 0.0, (const double*)a.V, (const ArnoldiState*)a.state, a.prod,
+                   (const double*)a.w, a.y, a.dinv, a.x, a.Z);
+        ++launches;
+      }
+    }
+    first = false;
+  }
+  return launches;
+}
+
 int launch_arnoldi_step(const ArnoldiArgs& a, cudaStream_t st) {
   const int g = grid_rows(a.nrow);
   const int db = arnoldi_dot_blocks(a.nrow);
-  launch_pdl(k_arn_prep, g, 256, 0, st, a.nrow, a.V, a.dinv, a.state, a.x);
-  int launches = 1 + launch_matvec(a.p, a.mv, st);
+  int launches;
+  if (a.poly && a.poly->n > 0)
+    launches = launch_poly_apply(a, st);
+  else {
+    launch_pdl(k_arn_prep, g, 256, 0, st, a.nrow, a.V, a.dinv, a.state, a.x);
+    launches = 1;
+  }
+  launches += launch_matvec(a.p, a.mv, st);
   double* h1 = a.h;
   double* h2 = a.h + a.cols;
   double* hn = a.h + 2 * a.cols;

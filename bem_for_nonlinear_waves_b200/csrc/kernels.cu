@@ -737,7 +737,8 @@ __global__ void __launch_bounds__(128) k_targets_ax(const NearBlockDev* __restri
   const NearBlockDev B = blocks[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarp = blockDim.x >> 5;
-  for (int i = threadIdx.x; i < NC; i += blockDim.x) sL[i] = L[(size_t)B.node * 2 * NC + i];
+  if (L)  // L == nullptr: the near-field part of the operator only (no L2P)
+    for (int i = threadIdx.x; i < NC; i += blockDim.x) sL[i] = L[(size_t)B.node * 2 * NC + i];
   for (int i = threadIdx.x; i < B.ntgt; i += blockDim.x) accs[i] = 0.0;
   for (int c0 = 0; c0 < B.ndof; c0 += chunk) {
     const int cn = min(chunk, B.ndof - c0);
@@ -783,7 +784,7 @@ __global__ void __launch_bounds__(128) k_targets_ax(const NearBlockDev* __restri
     const double px = Xs[3 * p] - cx, py = Xs[3 * p + 1] - cy, pz = Xs[3 * p + 2] - cz;
     double f0 = 0.0;
     const int m = lane;
-    if (m <= P) {
+    if (m <= P && L) {
       const double r2 = px * px + py * py + pz * pz;
       double2 cur = make_double2(1.0, 0.0);
       for (int k = 1; k <= m; ++k) cur = cscale(cmul(cur, make_double2(px, py)), sHalf[k]);
@@ -1219,6 +1220,35 @@ int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages) {
   return 0;
 }
 
+// y = A_near x: the near-field rows of the A.x operator (combined weights, diagonal and
+// constraint rows as k_targets_ax, no far field); a.ax -> a.rows, FP32 weights when present
+template <int P>
+int launch_near_only_t(const MatvecArgs& a, cudaStream_t st) {
+  if (a.n_blocks <= 0 || !a.ax || !(a.Wc || a.Wc32)) return 0;
+  const size_t shm = sizeof(double) * (size_t)(a.chunk + a.max_ntgt);
+  const double2* noL = nullptr;
+  if (a.Wc32)
+    launch_pdl(k_targets_ax<P, float>, a.n_blocks, 128, shm, st, a.blocks, a.nb_dofs, a.nb_targets, a.Wc32, a.Xs, a.node_X, noL, a.ax,
+               a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk);
+  else
+    launch_pdl(k_targets_ax<P, double>, a.n_blocks, 128, shm, st, a.blocks, a.nb_dofs, a.nb_targets, a.Wc, a.Xs, a.node_X, noL, a.ax,
+               a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk);
+  return 1;
+}
+
+int launch_near_only(int p, const MatvecArgs& a, cudaStream_t st) {
+  switch (p) {
+#define BEMB200_CASE(PP) \
+  case PP:               \
+    return launch_near_only_t<PP>(a, st);
+    BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5) BEMB200_CASE(6)
+    BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10) BEMB200_CASE(11) BEMB200_CASE(12)
+#undef BEMB200_CASE
+    default: break;
+  }
+  return 0;
+}
+
 template <int P>
 void set_m2l_smem() {
   cudaFuncSetAttribute(k_m2l_grp<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, m2l_grp_smem_bytes<P>());
@@ -1350,6 +1380,23 @@ void launch_axpby(int n, double a, const double* x, double b, double* y, cudaStr
   int g = (n + 255) / 256;
   if (g > 1184) g = 1184;
   k_axpby<<<g > 0 ? g : 1, 256, 0, st>>>(n, a, x, b, y);
+}
+
+// y[i] in [-0.5, 0.5): a fixed pseudo-random vector (splitmix64 of seed + i)
+__global__ void k_hash_fill(int n, unsigned long long seed, double* __restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    unsigned long long z = seed + 0x9e3779b97f4a7c15ull * (unsigned long long)(i + 1);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    y[i] = (double)(z >> 11) * 0x1.0p-53 - 0.5;
+  }
+}
+
+void launch_hash_fill(int n, unsigned long long seed, double* y, cudaStream_t st) {
+  int g = (n + 255) / 256;
+  if (g > 1184) g = 1184;
+  k_hash_fill<<<g > 0 ? g : 1, 256, 0, st>>>(n, seed, y);
 }
 
 void launch_mul(int n, const double* a, const double* x, double* y, cudaStream_t st) {

@@ -6,6 +6,8 @@
 
 #include <utility>
 
+#include "poly.hpp"
+
 namespace bemb200 {
 
 // Programmatic dependent launch for the kernels of an operator application: each is launched
@@ -164,6 +166,7 @@ enum { STAGE_P2M = 1, STAGE_M2M = 2, STAGE_M2L = 4, STAGE_L2L = 8, STAGE_TARGETS
 // only (half the P2M, M2M, M2L, L2L and L2P work) -- a call for GnPhi alone must then have
 // phin = 0 (the rigid-mode diagonal).
 int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages = STAGE_ALL);
+int launch_near_only(int p, const MatvecArgs& a, cudaStream_t st);  // a.rows = A_near a.ax (no far field)
 
 // tensor-core M2L (m2l_tc.cu)
 int tc_supported(int p);            // 1 for 1 <= p <= 12
@@ -193,6 +196,7 @@ void launch_maxpy(const double* V, int ldv, int k, const double* h, double* w, i
 void launch_axpby(int n, double a, const double* x, double b, double* y, cudaStream_t st);
 void launch_scale_inv(int n, const double* x, const double* s, double* y, cudaStream_t st);
 void launch_mul(int n, const double* a, const double* x, double* y, cudaStream_t st);
+void launch_hash_fill(int n, unsigned long long seed, double* y, cudaStream_t st);  // fixed pseudo-random [-0.5, 0.5)
 void launch_add_mul(int n, const double* xb, const double* a, const double* u, double* y, cudaStream_t st);
 void launch_jacobi(int n, const int* dof_point, const int* dof_kind, const double* diag, const int* block_of_point, const int* row_of_point,
                    const NearBlockDev* blocks, const int* self_col, const double* WG, const double* WGn, double* dinv, cudaStream_t st);
@@ -219,6 +223,13 @@ struct ArnoldiArgs {
   double* sn = nullptr;
   double* g = nullptr;            // [cols + 1] rotated right-hand side
   double* R = nullptr;            // [cols][cols] triangular factor, column j at R + j * cols
+  // polynomial preconditioner: x = D^{-1} p(B) V[:, n] with B = A_near D^{-1}, written to the
+  // operator input and to Z[:, n] (flexible storage: the iterate is updated from Z)
+  const PolyRoots* poly = nullptr;  // null: x = (D^{-1}) V[:, n]
+  MatvecArgs near;                  // B: a.x (with D^{-1} applied) -> a.w, near field only
+  double* prod = nullptr;           // [nrow] running product of the root factors
+  double* y = nullptr;              // [nrow] polynomial accumulator
+  double* Z = nullptr;              // [cols][nrow]
 };
 int arnoldi_dot_blocks(int nrow);
 int configure_arnoldi(int cols);  // before capture: shared memory of the Givens step; -1 if cols is too large

@@ -240,7 +240,7 @@ def run_batch(args, cfg, local):
     else:
         probs = [make_problem(cfg, rank + 1000 + i) for i in range(args.batch)]
     kw = dict(expansion_order=cfg["p"], solver_tol=cfg["rel_tol"], tol_relative=True, solver_max_iter=args.max_iter,
-              preconditioner=args.precond, device=local, precision=args.precision)
+              preconditioner=args.precond, poly_degree=args.poly_degree, device=local, precision=args.precision)
     one = BEM_BVP(probs[0][0].X, probs[0][0].tri, probs[0][0].face_dirichlet, dofs=probs[0][1], **kw)
     for _ in range(args.warmup):
         one.setup()
@@ -307,7 +307,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="tank_60k", choices=list(CONFIGS))
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--precond", default="jacobi", choices=["jacobi", "none"])
+    ap.add_argument("--precond", default="jacobi", choices=["jacobi", "none", "near_poly"])
+    ap.add_argument("--poly-degree", type=int, default=8, help="degree of the near_poly preconditioner")
     ap.add_argument("--max-iter", type=int, default=1500)
     ap.add_argument("--ref-iters", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -331,7 +332,7 @@ def main():
 
     def make(prec):
         return BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=cfg["p"], solver_tol=cfg["rel_tol"], tol_relative=True,
-                       solver_max_iter=args.max_iter, preconditioner=args.precond, dofs=d, device=local, precision=prec)
+                       solver_max_iter=args.max_iter, preconditioner=args.precond, poly_degree=args.poly_degree, dofs=d, device=local, precision=prec)
 
     bvp = make(args.precision)
     for _ in range(args.warmup):
@@ -375,7 +376,7 @@ def main():
     # problem overlaps the device solve of the previous one (host arrays in and out)
     from bem_for_nonlinear_waves_b200 import BatchSolver
     bs = BatchSolver(2, expansion_order=cfg["p"], solver_tol=cfg["rel_tol"], tol_relative=True, solver_max_iter=args.max_iter,
-                     preconditioner=args.precond, device=local, precision=args.precision)
+                     preconditioner=args.precond, poly_degree=args.poly_degree, device=local, precision=args.precision)
     for tk in [bs.submit(t.X, t.tri, t.face_dirichlet, kv, dofs=d) for _ in range(2)]:
         bs.result(tk)
     nb = max(2 * args.steps, 4)
@@ -465,7 +466,8 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f64/f16x3-tc" if mixed else "f64", "data": "synthetic",
         "config": {"workload": args.config, "n_points": int(t.n_points), "n_faces": int(t.n_faces), "n_dof": int(bvp.matrix_size),
                    "p": p, "theta": 0.25, "leaf_max": 30, "rel_tol": cfg["rel_tol"], "precision": args.precision,
-                   "preconditioner": args.precond, "gmres_iterations": iters / args.steps, "matvecs_fp64": mv / args.steps,
+                   "preconditioner": args.precond + (f" (degree {args.poly_degree})" if args.precond == "near_poly" else ""),
+                   "gmres_iterations": iters / args.steps, "matvecs_fp64": mv / args.steps,
                    "matvecs_lowp": mv_lo / args.steps, "converged": converged, "parallelism": f"replicas{world}",
                    "l2": "working set > L2 (near-field weights %.1f GB)" % (tree["nnz"] * 16 / 1e9)},
         "matvecs_per_s": world * 1e3 / prof["total"],

@@ -56,11 +56,16 @@ typedef struct {
   int32_t max_iter;          /* GMRES iteration cap (solver_max_iter) */
   int32_t device;            /* CUDA device ordinal */
   int32_t tol_relative;      /* 0: stop at |A x - b| <= tol (reference semantics); 1: at <= tol*|b| */
-  int32_t preconditioner;    /* 0: none (reference default); 1: right Jacobi from the near-field diagonal */
+  int32_t preconditioner;    /* 0: none (reference default); 1: right Jacobi from the near-field diagonal;
+                                2: right near-field polynomial -- D^-1 p(A_near D^-1), p the GMRES
+                                polynomial (harmonic Ritz roots) of a poly_degree-step Arnoldi run on
+                                A_near D^-1; the device counterpart of the reference's near-field
+                                ILU/Schwarz preconditioners (bem/BEM_solveBVP_GMRES_FMM.hpp:215-1050) */
   int32_t precision;         /* 0: FP64 throughout; 1: mixed -- GMRES corrections use the tensor-core
                                 M2L (FP16 split operands, FP32 accumulate), FP64 outer refinement on the
                                 true residual, same stopping test; needs p <= 12 */
-  int32_t reserved[2];
+  int32_t poly_degree;       /* preconditioner 2: polynomial degree 1..24 (0: 8) */
+  int32_t reserved;
 } bem_gpu_opts;
 
 /* One boundary-value problem.  The DOF table is what the reference's setNodeFaceIndices()
@@ -245,6 +250,15 @@ int bem_gpu_mel_stage(bem_gpu_mel* mel, const bem_mel_surface* s, int32_t stage,
 int bem_gpu_matvec_device_mixed(bem_gpu_ctx* ctx, const double* d_x, double* d_y);
 int bem_gpu_profile_matvec_mixed(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[9]*/);
 int bem_gpu_check_device_status(bem_gpu_ctx* ctx);
+
+/* Near-field polynomial preconditioner (opts.preconditioner = 2).
+ * bem_gpu_poly_roots: the roots formed by the last set-up, in the order they are applied (a
+ *   conjugate pair a +- bi is one entry with im = b > 0); returns the number of entries, 0 when
+ *   none could be formed (the solve then uses the Jacobi scaling alone), or an error code.
+ * bem_harmonic_ritz_values: host helper -- harmonic Ritz values of a (k+1) x k Arnoldi
+ *   Hessenberg matrix (row-major, leading dimension ldh, k <= 32); 0 or -1. */
+int bem_gpu_poly_roots(bem_gpu_ctx* ctx, int32_t cap, double* re, double* im);
+int bem_harmonic_ritz_values(int32_t k, const double* H, int32_t ldh, double* re, double* im);
 
 /* FP64 FMA throughput of the device (TFLOP/s), measured by a short probe kernel. */
 double bem_gpu_fp64_peak_tflops(int32_t device);
