@@ -58,6 +58,7 @@ EXPORTS = {
     "bem_gpu_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "bem_gpu_build_dofs": (c_int, [c_int, P_dbl, c_int, P_int, P_u8, P_int, P_int, P_int, P_int, P_u8]),
     "bem_gpu_setup": (c_int, [ctypes.c_void_p, ctypes.POINTER(Desc)]),
+    "bem_gpu_setup_refresh": (c_int, [ctypes.c_void_p, ctypes.POINTER(Desc)]),
     "bem_gpu_solve": (c_int, [ctypes.c_void_p, P_dbl, P_dbl, P_dbl, P_dbl, ctypes.POINTER(Stats)]),
     "bem_gpu_solve_bvp": (c_int, [ctypes.c_void_p, ctypes.POINTER(Desc), P_dbl, P_dbl, P_dbl, P_dbl, ctypes.POINTER(Stats)]),
     "bem_gpu_apply": (c_int, [ctypes.c_void_p, P_dbl, P_dbl, P_dbl]),
@@ -77,6 +78,7 @@ EXPORTS = {
     "bem_gpu_poly_roots": (c_int, [ctypes.c_void_p, c_int, P_dbl, P_dbl]),
     "bem_harmonic_ritz_values": (c_int, [c_int, P_dbl, c_int, P_dbl, P_dbl]),
     "bem_plan_inspect": (c_int, [ctypes.POINTER(Opts), ctypes.POINTER(Desc), P_int, P_dbl, P_i64]),
+    "bem_plan_refresh_inspect": (c_int, [ctypes.POINTER(Opts), ctypes.POINTER(Desc), ctypes.POINTER(Desc), P_i64]),
     "bem_gpu_mel_create": (ctypes.c_void_p, [c_int]),
     "bem_gpu_mel_destroy": (None, [ctypes.c_void_p]),
     "bem_gpu_mel_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),

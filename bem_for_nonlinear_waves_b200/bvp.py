@@ -115,6 +115,27 @@ class BEM_BVP:
         self._check(self.lib.bem_gpu_setup(self.ctx, ctypes.byref(desc)), "setup")
         self._setup_done = True
 
+    def refresh(self, X):
+        """Set-up at new point coordinates X of the same mesh (a Runge-Kutta stage or the next time
+        step), keeping the octree's root bucket as the reference's rebin path does
+        (bem/BEM_solveBVP_GMRES_FMM.hpp:3125-3346).  Returns what the device kept: 2 (tree, lists
+        and targets unchanged: only the geometry was uploaded), 1 (tree and lists; near-field
+        blocks rebuilt) or 0 (full set-up)."""
+        X = np.ascontiguousarray(X, np.float64)
+        if X.shape != self.X.shape:
+            raise ValueError("refresh needs the same points (n_points x 3)")
+        if not self._setup_done:
+            self.X = X
+            self.setup()
+            return 0
+        self.X = X
+        desc = L.Desc(self.X.shape[0], L.ptr(self.X, L.P_dbl), self.tri.shape[0], L.ptr(self.tri, L.P_int),
+                      L.ptr(self.face_dirichlet, L.P_u8), self.matrix_size, L.ptr(self._keep[0], L.P_int),
+                      L.ptr(self._keep[1], L.P_int), L.ptr(self._keep[2], L.P_int), L.ptr(self._keep[3], L.P_int))
+        rc = self.lib.bem_gpu_setup_refresh(self.ctx, ctypes.byref(desc))
+        self._check(min(rc, 0), "setup_refresh")
+        return int(rc)
+
     def solve(self, known, x0=None):
         """known: per-DOF phi (Dirichlet DOFs) or phin (Neumann DOFs), physical units; x0: optional
         initial guess of the unknowns (phin for Dirichlet DOFs, phi for the others), e.g. the

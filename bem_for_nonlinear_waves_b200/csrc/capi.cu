@@ -585,9 +585,13 @@ int bem_gpu_poly_roots(bem_gpu_ctx* ctx, int32_t cap, double* re, double* im) {
   return ctx->poly.n;
 }
 
-int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
+// Set-up of a BVP (refresh: same mesh as the last set-up at new coordinates; see
+// bem_gpu_setup_refresh).  With an unchanged structure only the geometry-dependent arrays are
+// uploaded and only the geometry-dependent device tables rebuilt.
+static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   if (!ctx || !d) return BEM_ERR_INVALID_ARGUMENT;
   CK(cudaSetDevice(ctx->opts.device));
+  const bool had_plan = ctx->ready;
   ctx->ready = false;
   ctx->h2d = ctx->d2h = ctx->launches = 0;
   const double t0 = now_s();
@@ -609,13 +613,22 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   po.theta = ctx->opts.mac_theta;
   po.leaf_max = ctx->opts.leaf_max_elements;
   po.max_level = ctx->opts.max_level;
-  if (!build_plan(ctx->plan, po, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face,
-                  d->dof_kind, d->face_dof)) {
-    ctx->err = ctx->plan.error;
-    return BEM_ERR_INVALID_ARGUMENT;
+  {
+    Plan fresh;
+    if (!build_plan(fresh, po, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face,
+                    d->dof_kind, d->face_dof, refresh && had_plan ? &ctx->plan : nullptr)) {
+      ctx->err = fresh.error;
+      return BEM_ERR_INVALID_ARGUMENT;
+    }
+    ctx->plan = std::move(fresh);
   }
   ctx->time_plan = now_s() - t0;
   Plan& P = ctx->plan;
+  // a refresh that kept the tree and lists (reuse) and the L2P targets (reuse_near) skips the
+  // uploads of what it kept: the buffers still hold the same data
+  const bool reuse = P.reused_m2l, reuse_near = P.reused_near;
+  auto ups = [&](auto& buf, const auto& v) -> cudaError_t { return reuse ? cudaSuccess : up(ctx, buf, v); };
+  auto upn = [&](auto& buf, const auto& v) -> cudaError_t { return reuse_near ? cudaSuccess : up(ctx, buf, v); };
   cudaStream_t s = ctx->stream;
   const int NC = ncoef(P.opt.p);
   const int nb = (int)P.nodes.size();
@@ -655,11 +668,13 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
           }
         }
       }
-    CK(up(ctx, ctx->ftab_vec, fv));
-    const int NFt = (P.opt.p + 1) * (P.opt.p + 1);
-    CK(ctx->Ftab.alloc((size_t)std::max(nlev, 1) * 8 * NFt));
-    launch_f_tables(P.opt.p, std::max(nlev, 1) * 8, ctx->ftab_vec.p, ctx->Ftab.p, s);
-    ctx->launches += 1;
+    if (!reuse) {
+      CK(up(ctx, ctx->ftab_vec, fv));
+      const int NFt = (P.opt.p + 1) * (P.opt.p + 1);
+      CK(ctx->Ftab.alloc((size_t)std::max(nlev, 1) * 8 * NFt));
+      launch_f_tables(P.opt.p, std::max(nlev, 1) * 8, ctx->ftab_vec.p, ctx->Ftab.p, s);
+      ctx->launches += 1;
+    }
   }
   const std::vector<int>& mt = P.m2l_targets;
   ctx->n_m2l_targets = (int)mt.size();
@@ -700,15 +715,15 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   CK(up(ctx, ctx->e_W, P.e_W));
   CK(up(ctx, ctx->e_n, P.e_n));
   CK(up(ctx, ctx->e_near, P.e_near));
-  CK(up(ctx, ctx->e_dof, P.e_dof));
-  CK(up(ctx, ctx->e_vtx, P.e_vtx));
-  CK(up(ctx, ctx->node_X, nX));
-  CK(up(ctx, ctx->node_fb, nfb));
-  CK(up(ctx, ctx->node_fe, nfe));
-  CK(up(ctx, ctx->child_begin, cb));
-  CK(up(ctx, ctx->child_end, ce));
-  CK(up(ctx, ctx->node_children, P.node_children));
-  CK(up(ctx, ctx->leaves, P.leaves));
+  CK(ups(ctx->e_dof, P.e_dof));
+  CK(ups(ctx->e_vtx, P.e_vtx));
+  CK(ups(ctx->node_X, nX));
+  CK(ups(ctx->node_fb, nfb));
+  CK(ups(ctx->node_fe, nfe));
+  CK(ups(ctx->child_begin, cb));
+  CK(ups(ctx->child_end, ce));
+  CK(ups(ctx->node_children, P.node_children));
+  CK(ups(ctx->leaves, P.leaves));
   {  // upward pass: parent, Ftab row and the number of children whose multipole completes
     std::vector<int> par(nb, -1), lev(nb, 0), nsig(nb, 0);
     std::vector<char> sig(nb, 0), leaf(nb, 0);
@@ -734,31 +749,31 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
         if (!leaf[i] && nch[i] > 0 && nsig[i] == 0) ready.push_back(i);
     ctx->n_m2m_ready = (int)ready.size();
     if (ready.empty()) ready.push_back(0);
-    CK(up(ctx, ctx->m2m_ready, ready));
-    CK(up(ctx, ctx->node_parent, par));
-    CK(up(ctx, ctx->node_level, lev));
-    CK(up(ctx, ctx->m2m_nsig, nsig));
+    CK(ups(ctx->m2m_ready, ready));
+    CK(ups(ctx->node_parent, par));
+    CK(ups(ctx->node_level, lev));
+    CK(ups(ctx->m2m_nsig, nsig));
     CK(ctx->m2m_cnt.alloc(std::max(nb, 1)));
   }
-  CK(up(ctx, ctx->level_parents, lp));
-  CK(up(ctx, ctx->m2l_targets, mt));
-  CK(up(ctx, ctx->m2l_off, P.m2l_off));
-  CK(up(ctx, ctx->m2l_src, P.m2l_src));
-  CK(up(ctx, ctx->nb_dofs, P.nb_dofs));
-  CK(up(ctx, ctx->nb_targets, P.nb_targets));
-  CK(up(ctx, ctx->nb_ranges, P.nb_ranges));
-  CK(up(ctx, ctx->dof_inc_off, P.dof_inc_off));
-  CK(up(ctx, ctx->dof_inc, P.dof_inc));
-  CK(up(ctx, ctx->point_dof_off, P.point_dof_off));
-  CK(up(ctx, ctx->point_dof, P.point_dof));
-  CK(up(ctx, ctx->dof_kind, P.dof_kind));
-  CK(up(ctx, ctx->dof_point, P.dof_point));
-  CK(up(ctx, ctx->blocks, bd));
-  CK(up(ctx, ctx->chunk_grp, P.chunk_grp));
-  CK(up(ctx, ctx->chunk_begin, P.chunk_begin));
-  CK(up(ctx, ctx->chunk_cnt, P.chunk_cnt));
-  CK(up(ctx, ctx->grp_pair, P.grp_pair));
-  CK(up(ctx, ctx->grp_vec, P.grp_vec));
+  CK(ups(ctx->level_parents, lp));
+  CK(ups(ctx->m2l_targets, mt));
+  CK(ups(ctx->m2l_off, P.m2l_off));
+  CK(ups(ctx->m2l_src, P.m2l_src));
+  CK(upn(ctx->nb_dofs, P.nb_dofs));
+  CK(upn(ctx->nb_targets, P.nb_targets));
+  CK(upn(ctx->nb_ranges, P.nb_ranges));
+  CK(ups(ctx->dof_inc_off, P.dof_inc_off));
+  CK(ups(ctx->dof_inc, P.dof_inc));
+  CK(ups(ctx->point_dof_off, P.point_dof_off));
+  CK(ups(ctx->point_dof, P.point_dof));
+  CK(ups(ctx->dof_kind, P.dof_kind));
+  CK(ups(ctx->dof_point, P.dof_point));
+  CK(upn(ctx->blocks, bd));
+  CK(ups(ctx->chunk_grp, P.chunk_grp));
+  CK(ups(ctx->chunk_begin, P.chunk_begin));
+  CK(ups(ctx->chunk_cnt, P.chunk_cnt));
+  CK(ups(ctx->grp_pair, P.grp_pair));
+  CK(ups(ctx->grp_vec, P.grp_vec));
   {
     const int ngroups = (int)P.grp_off.size() - 1;
     const int Q = 2 * P.opt.p;
@@ -771,7 +786,7 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   ctx->mixed = ctx->opts.precision == 1;
   if (ctx->mixed) {  // tensor-core M2L: translation tables, multipole rows, work items
     const int p = P.opt.p, kp = tc_kp(p);
-    build_tc_groups(P, tc_max_pairs());
+    if (!reuse) build_tc_groups(P, tc_max_pairs());
     const int ntab = (int)(P.tc_tab.size() / 4);
     std::vector<double> dl(nb), al(kp);
     for (int i = 0; i < nb; ++i) dl[i] = P.nodes[i].dL;
@@ -793,9 +808,9 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
         i0 = i1;
       }
       ctx->n_tc_items = (int)itab.size();
-      CK(up(ctx, ctx->tc_item_tab, itab));
-      CK(up(ctx, ctx->tc_item_begin, ibeg));
-      CK(up(ctx, ctx->tc_item_cnt, icnt));
+      CK(ups(ctx->tc_item_tab, itab));
+      CK(ups(ctx->tc_item_begin, ibeg));
+      CK(ups(ctx->tc_item_cnt, icnt));
     }
     {  // work-item order j -> source bucket; pair slot k -> its position j (the row of its partial)
       std::vector<int> src(P.tc_pair.size()), pos(P.tc_pair.size());
@@ -803,12 +818,12 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
         src[j] = P.m2l_src[P.tc_pair[j]];
         pos[P.tc_pair[j]] = (int)j;
       }
-      CK(up(ctx, ctx->tc_src, src));
-      CK(up(ctx, ctx->tc_pos, pos));
+      CK(ups(ctx->tc_src, src));
+      CK(ups(ctx->tc_pos, pos));
     }
-    CK(up(ctx, ctx->tc_tabvec, P.tc_tab));
-    CK(up(ctx, ctx->tc_alpha, al));
-    CK(up(ctx, ctx->node_dL, dl));
+    CK(ups(ctx->tc_tabvec, P.tc_tab));
+    CK(ups(ctx->tc_alpha, al));
+    CK(ups(ctx->node_dL, dl));
     CK(ctx->tc_T.alloc((size_t)std::max(ntab, 1) * tc_row_tiles(p) * tc_table_bytes(p) / 2));
     CK(ctx->tc_Mt.alloc((size_t)(nb + 1) * 2 * kp));
     ctx->tc_map.assign(tc_rows_map_bytes(), 0);
@@ -840,9 +855,9 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
         }
       ldo[li + 1] = (int)ld.size();
     }
-    CK(up(ctx, ctx->leaf_dof_off, ldo));
-    CK(up(ctx, ctx->leaf_dof, ld));
-    CK(up(ctx, ctx->e_slot, es));
+    CK(ups(ctx->leaf_dof_off, ldo));
+    CK(ups(ctx->leaf_dof, ld));
+    CK(ups(ctx->e_slot, es));
     CK(ctx->p2m_C.alloc(std::max<size_t>(ld.size(), 1) * NC));
   }
   CK(ctx->M.alloc((size_t)nb * 2 * NC));
@@ -895,7 +910,7 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
       for (int r = 0; r < nbk.nrng; ++r) ne += P.nb_ranges[2 * (nbk.rng_off + r) + 1] - P.nb_ranges[2 * (nbk.rng_off + r)];
       mel = std::max(mel, ne);
     }
-    CK(up(ctx, ctx->slot_block, sb));
+    CK(upn(ctx->slot_block, sb));
     na.n_slots = (int)sb.size();
     na.slot_block = ctx->slot_block.p;
     na.max_nrng = mr;
@@ -909,9 +924,9 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
       bop[p] = std::max(P.block_of_point[p], 0);
       rop[p] = std::max(P.row_of_point[p], 0);
     }
-    CK(up(ctx, ctx->block_of_point, bop));
-    CK(up(ctx, ctx->row_of_point, rop));
-    CK(up(ctx, ctx->self_col, P.self_col));
+    CK(upn(ctx->block_of_point, bop));
+    CK(upn(ctx->row_of_point, rop));
+    CK(upn(ctx->self_col, P.self_col));
     CK(ctx->dinv.alloc(N));
   }
   CK(cudaStreamSynchronize(s));
@@ -924,14 +939,18 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   CK(cudaMemsetAsync(ctx->M.p, 0, sizeof(double2) * ctx->M.n, s));
   CK(cudaMemsetAsync(ctx->m2m_cnt.p, 0, sizeof(int) * ctx->m2m_cnt.n, s));
   CK(cudaMemsetAsync(ctx->p2m_C.p, 0, sizeof(double2) * ctx->p2m_C.n, s));
-  launch_s_tables(P.opt.p, (int)P.grp_off.size() - 1, ctx->grp_vec.p, ctx->Sg.p, s);
-  ctx->launches += 1;
+  if (!reuse) {  // translation tables depend on the bucket geometry alone
+    launch_s_tables(P.opt.p, (int)P.grp_off.size() - 1, ctx->grp_vec.p, ctx->Sg.p, s);
+    ctx->launches += 1;
+  }
   if (ctx->mixed) {
     CK(cudaMemsetAsync(ctx->tc_Mt.p, 0, sizeof(uint16_t) * ctx->tc_Mt.n, s));
     CK(cudaMemsetAsync(ctx->tc_err.p, 0, sizeof(int), s));
-    CK(cudaMemsetAsync(ctx->tc_max.p, 0, sizeof(unsigned int), s));
-    launch_tc_tables(P.opt.p, (int)(P.tc_tab.size() / 4), ctx->tc_tabvec.p, ctx->tc_alpha.p, ctx->tc_T.p, ctx->tc_max.p, s);
-    ctx->launches += 1;
+    if (!reuse) {
+      CK(cudaMemsetAsync(ctx->tc_max.p, 0, sizeof(unsigned int), s));
+      launch_tc_tables(P.opt.p, (int)(P.tc_tab.size() / 4), ctx->tc_tabvec.p, ctx->tc_alpha.p, ctx->tc_T.p, ctx->tc_max.p, s);
+      ctx->launches += 1;
+    }
   }
   {
     MatvecArgs pa = ctx->args(nullptr, nullptr, nullptr, nullptr, nullptr);
@@ -961,7 +980,7 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
     if (rc != BEM_OK) return rc;
   }
   CK(cudaEventRecord(ctx->ev[1], s));
-  if (ctx->mixed) {  // FP16 tables must stay far from the FP16 range limit (65504)
+  if (ctx->mixed && !reuse) {  // FP16 tables must stay far from the FP16 range limit (65504)
     unsigned int bits = 0;
     CK(cudaMemcpyAsync(&bits, ctx->tc_max.p, sizeof(bits), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -981,6 +1000,13 @@ int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
   ctx->time_setup = now_s() - t0;
   ctx->ready = true;
   return BEM_OK;
+}
+
+int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* d) { return setup_impl(ctx, d, false); }
+
+int bem_gpu_setup_refresh(bem_gpu_ctx* ctx, const bem_bvp_desc* d) {
+  const int rc = setup_impl(ctx, d, true);
+  return rc != BEM_OK ? rc : (int)ctx->plan.reused_m2l + (int)ctx->plan.reused_near;
 }
 
 int bem_gpu_apply(bem_gpu_ctx* ctx, const double* phi, const double* phin, double* Av) {
@@ -1102,6 +1128,53 @@ int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out) {
   out[7] = (int64_t)P.blocks.size();
   out[8] = (int64_t)P.chunk_grp.size();
   out[9] = (int64_t)P.grp_off.size() - 1;
+  return BEM_OK;
+}
+
+int bem_plan_refresh_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* d0, const bem_bvp_desc* d1, int64_t* out) {
+  if (!opts || !d0 || !d1 || !out) return BEM_ERR_INVALID_ARGUMENT;
+  PlanOptions po;
+  po.p = opts->expansion_order;
+  po.theta = opts->mac_theta;
+  po.leaf_max = opts->leaf_max_elements;
+  po.max_level = opts->max_level;
+  auto build = [&](Plan& P, const bem_bvp_desc* d, Plan* prev, bool take) {
+    PlanOptions o = po;
+    o.take_structure = take;
+    if (!build_plan(P, o, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face, d->dof_kind,
+                    d->face_dof, prev))
+      return false;
+    if (!P.reused_m2l) build_tc_groups(P, tc_max_pairs());
+    return true;
+  };
+  Plan a0, b0, a1, b1;
+  if (!build(a0, d0, nullptr, true) || !build(b0, d0, nullptr, true)) return BEM_ERR_INVALID_ARGUMENT;
+  if (!build(a1, d1, &a0, true) || !build(b1, d1, &b0, false)) return BEM_ERR_INVALID_ARGUMENT;
+  int64_t diff = 0;
+#define BEMB200_CMP(f) diff += (a1.f == b1.f) ? 0 : 1;
+  BEMB200_CMP(Xs) BEMB200_CMP(L) BEMB200_CMP(scale) BEMB200_CMP(near_region) BEMB200_CMP(face_of_pos) BEMB200_CMP(pos_of_face)
+  BEMB200_CMP(owner_of_pos) BEMB200_CMP(e_q) BEMB200_CMP(e_W) BEMB200_CMP(e_n) BEMB200_CMP(e_dof) BEMB200_CMP(e_vtx)
+  BEMB200_CMP(e_near) BEMB200_CMP(node_children) BEMB200_CMP(level_nodes) BEMB200_CMP(leaves) BEMB200_CMP(m2l_off)
+  BEMB200_CMP(m2l_src) BEMB200_CMP(near_off) BEMB200_CMP(near_nodes) BEMB200_CMP(m2l_pairs) BEMB200_CMP(near_pairs)
+  BEMB200_CMP(grp_vec) BEMB200_CMP(grp_off) BEMB200_CMP(grp_pair) BEMB200_CMP(chunk_grp) BEMB200_CMP(chunk_begin)
+  BEMB200_CMP(chunk_cnt) BEMB200_CMP(m2l_targets) BEMB200_CMP(m2l_key_sorted) BEMB200_CMP(tc_tab) BEMB200_CMP(tc_pair)
+  BEMB200_CMP(tc_item_tab) BEMB200_CMP(tc_item_begin) BEMB200_CMP(tc_item_cnt) BEMB200_CMP(target_box) BEMB200_CMP(nb_dofs)
+  BEMB200_CMP(nb_targets) BEMB200_CMP(nb_ranges) BEMB200_CMP(block_of_point) BEMB200_CMP(row_of_point) BEMB200_CMP(self_col)
+  BEMB200_CMP(nnz) BEMB200_CMP(dof_inc_off) BEMB200_CMP(dof_inc)
+#undef BEMB200_CMP
+  diff += a1.nodes.size() != b1.nodes.size() || a1.blocks.size() != b1.blocks.size();
+  for (size_t i = 0; i < a1.nodes.size() && i < b1.nodes.size(); ++i)
+    diff += std::memcmp(&a1.nodes[i], &b1.nodes[i], sizeof(Plan::Node)) != 0;
+  for (size_t i = 0; i < a1.blocks.size() && i < b1.blocks.size(); ++i) {
+    const auto &x = a1.blocks[i], &y = b1.blocks[i];
+    diff += x.node != y.node || x.w_off != y.w_off || x.dof_off != y.dof_off || x.ndof != y.ndof || x.tgt_off != y.tgt_off ||
+            x.ntgt != y.ntgt || x.rng_off != y.rng_off || x.nrng != y.nrng;
+  }
+  bool same_root = true;
+  for (int k = 0; k < 3; ++k) same_root = same_root && a1.root_C[k] == a0.root_C[k];
+  out[0] = same_root && a1.root_R == a0.root_R;
+  out[1] = (int)a1.reused_m2l + (int)a1.reused_near;
+  out[2] = diff;
   return BEM_OK;
 }
 

@@ -283,8 +283,23 @@ int build_dofs(int np, const double* X, int nf, const int32_t* tri, const uint8_
   return n;
 }
 
+// the tree, element order and interaction lists a refresh must reproduce to take over the
+// previous plan's M2L structure
+static bool same_tree(const Plan& a, const Plan& b) {
+  if (a.nodes.size() != b.nodes.size()) return false;
+  for (size_t i = 0; i < a.nodes.size(); ++i) {
+    const Plan::Node &x = a.nodes[i], &y = b.nodes[i];
+    if (x.level != y.level || x.parent != y.parent || x.child_begin != y.child_begin || x.child_end != y.child_end || x.fb != y.fb ||
+        x.fe != y.fe || x.n_data != y.n_data)
+      return false;
+  }
+  return a.node_children == b.node_children && a.face_of_pos == b.face_of_pos && a.m2l_off == b.m2l_off && a.m2l_src == b.m2l_src &&
+         a.near_off == b.near_off && a.near_nodes == b.near_nodes && a.e_vtx == b.e_vtx && a.e_dof == b.e_dof &&
+         a.leaves == b.leaves && a.level_nodes == b.level_nodes;
+}
+
 bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int ndof,
-                const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof) {
+                const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof, Plan* prev) {
   P = Plan();
   P.opt = opt;
   auto clk = std::chrono::steady_clock::now();
@@ -363,6 +378,10 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     }
   P.scale = hypot3(mx[0] - mn[0], mx[1] - mn[1], mx[2] - mn[2]);
   const double C[3] = {(mn[0] + mx[0]) / 2., (mn[1] + mx[1]) / 2., (mn[2] + mx[2]) / 2.};
+  bool keep_root = prev && !prev->nodes.empty() && prev->np == np && prev->nf == nf && prev->ndof == ndof && prev->opt.p == opt.p &&
+                   prev->opt.theta == opt.theta && prev->opt.leaf_max == opt.leaf_max && prev->opt.max_level == opt.max_level &&
+                   prev->dof_point == P.dof_point && prev->dof_face == P.dof_face && prev->dof_kind == P.dof_kind &&
+                   prev->face_dof == P.face_dof;
   P.near_region = P.scale / 25.;
 
   // element sources (BEM_solveBVP_GMRES_FMM.hpp:1799-1937)
@@ -398,19 +417,28 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   lap(0);
   // octree (BEM_solveBVP_GMRES_FMM.hpp:1178-1201; lib_spatial_partitioning.hpp)
   TreeBuilder T(opt, pole);
-  {
-    const double dLr = 1.05 * P.scale / 2.;
+  auto grow_from = [&](const double* rc, double dLr) {
+    T.B.clear();
+    T.drops = 0;
+    P.n_added = 0;
     double lo[3], hi[3];
     for (int a = 0; a < 3; ++a) {
-      lo[a] = C[a] - dLr;
-      hi[a] = C[a] + dLr;
+      lo[a] = rc[a] - dLr;
+      hi[a] = rc[a] + dLr;
+      P.root_C[a] = rc[a];
     }
+    P.root_R = dLr;
     Bucket root;
     bucket_init(root, lo, hi, dLr);
     T.B.push_back(std::move(root));
+    for (int f = 0; f < nf; ++f) P.n_added += T.add(0, f);
+    T.grow(0);
+  };
+  if (keep_root) {
+    grow_from(prev->root_C, prev->root_R);
+    if (P.n_added != nf) keep_root = false;  // a centroid left the old root: the reference re-initialises
   }
-  for (int f = 0; f < nf; ++f) P.n_added += T.add(0, f);
-  T.grow(0);
+  if (!keep_root) grow_from(C, 1.05 * P.scale / 2.);
   P.n_child_drops = T.drops;
   std::vector<Bucket>& B = T.B;
   const int nb = (int)B.size();
@@ -556,12 +584,41 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     std::copy(B[i].near.begin(), B[i].near.end(), P.near_nodes.begin() + P.near_off[i]);
   }
   P.m2l_pairs = P.m2l_off[nb];
+  // targets (target4FMM::setL2P / setDirectIntegration: getBucketAtDeepest)
+  P.target_box.assign(np, -1);
+  for (int p = 0; p < np; ++p) {
+    if (P.point_dof_off[p] == P.point_dof_off[p + 1]) continue;
+    const double* x = &P.Xs[3 * p];
+    int cur = 0;
+    while (!B[cur].kids.empty()) {
+      const int nx = B[cur].kid_of_cell[cell_of(B[cur], x)];
+      if (nx < 0) break;
+      cur = nx;
+    }
+    P.target_box[p] = cur;
+  }
   lap(3);
+  P.reused_m2l = keep_root && opt.take_structure && same_tree(P, *prev);
+  if (P.reused_m2l) {  // refresh, unchanged tree and lists: the M2L grouping is the previous one
+    P.m2l_key_sorted = std::move(prev->m2l_key_sorted);
+    P.grp_vec = std::move(prev->grp_vec);
+    P.grp_off = std::move(prev->grp_off);
+    P.grp_pair = std::move(prev->grp_pair);
+    P.chunk_grp = std::move(prev->chunk_grp);
+    P.chunk_begin = std::move(prev->chunk_begin);
+    P.chunk_cnt = std::move(prev->chunk_cnt);
+    P.m2l_targets = std::move(prev->m2l_targets);
+    P.tc_tab = std::move(prev->tc_tab);
+    P.tc_pair = std::move(prev->tc_pair);
+    P.tc_item_tab = std::move(prev->tc_item_tab);
+    P.tc_item_begin = std::move(prev->tc_item_begin);
+    P.tc_item_cnt = std::move(prev->tc_item_cnt);
+  }
   // M2L grouped by lattice offset r = (X_t - X_s) / dL_t and level; groups ordered by key,
   // pairs within a group in slot order.  One parallel sort of packed 64-bit values
   // (offset key | level | slot; a pair off the lattice gets a value of its own, sorted last)
   // serves both the FP64 groups (level, r) and the tensor-core tables (r on every level).
-  {
+  if (!P.reused_m2l) {
     const int64_t npair = P.m2l_pairs;
     if (npair >= (int64_t(1) << 29)) {
       P.error = "too many M2L pairs";
@@ -622,18 +679,19 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   for (int i = 0; i < nb; ++i)
     if (B[i].data.empty()) P.near_pairs -= (int)B[i].near.size();
   lap(4);
-  // targets (target4FMM::setL2P / setDirectIntegration: getBucketAtDeepest)
-  P.target_box.assign(np, -1);
-  for (int p = 0; p < np; ++p) {
-    if (P.point_dof_off[p] == P.point_dof_off[p + 1]) continue;
-    const double* x = &P.Xs[3 * p];
-    int cur = 0;
-    while (!B[cur].kids.empty()) {
-      const int nx = B[cur].kid_of_cell[cell_of(B[cur], x)];
-      if (nx < 0) break;
-      cur = nx;
-    }
-    P.target_box[p] = cur;
+  P.reused_near = P.reused_m2l && P.target_box == prev->target_box;
+  if (P.reused_near) {  // and the same L2P targets: the near-field blocks are the previous ones
+    P.blocks = std::move(prev->blocks);
+    P.nb_dofs = std::move(prev->nb_dofs);
+    P.nb_targets = std::move(prev->nb_targets);
+    P.nb_ranges = std::move(prev->nb_ranges);
+    P.block_of_point = std::move(prev->block_of_point);
+    P.row_of_point = std::move(prev->row_of_point);
+    P.self_col = std::move(prev->self_col);
+    P.nnz = prev->nnz;
+    P.dof_inc_off = std::move(prev->dof_inc_off);
+    P.dof_inc = std::move(prev->dof_inc);
+    return true;
   }
   // near blocks (lib_multipole_expansion.hpp:1180-1213)
   std::vector<int> block_of_node(nb, -1);

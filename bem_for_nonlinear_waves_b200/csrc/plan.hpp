@@ -19,6 +19,7 @@ struct PlanOptions {
   double theta = 0.25;
   int leaf_max = 30;
   int max_level = 7;
+  bool take_structure = true;  // refresh: take over the previous plan's unchanged structure (false: rebuild it)
 };
 
 struct Plan {
@@ -113,6 +114,13 @@ struct Plan {
 
   double phase_s[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // host set-up phase timings
 
+  // root bucket (centre, half-width) the tree was grown in; a refresh keeps it
+  double root_C[3] = {0, 0, 0}, root_R = 0.0;
+  // set by a refresh whose tree and lists came out identical to the previous plan's: the M2L
+  // grouping and tensor-core items were taken over from it; reused_near: the L2P targets too,
+  // and with them the near-field blocks
+  bool reused_m2l = false, reused_near = false;
+
   std::string error;
 };
 
@@ -121,8 +129,18 @@ int build_dofs(int np, const double* X, int nf, const int32_t* tri, const uint8_
                int32_t* dof_kind, int32_t* face_dof, uint8_t* point_flags);
 
 // Builds the plan; returns false and sets plan.error on invalid input.
+//
+// prev (refresh): the previous plan of the same mesh (same options, DOF tables and faces) at
+// other coordinates.  The tree is then grown in prev's root bucket, as the reference keeps its
+// Buckets root across time steps and rebins the moved sources into it
+// (bem/BEM_solveBVP_GMRES_FMM.hpp:3125-3346: initializeBucket once, rebin when the topology is
+// unchanged); a fresh root is taken only if an element centroid left the old one.  When the
+// tree and lists come out identical to prev's, the M2L structure is moved out of prev (prev is
+// left partly empty; plan.reused_m2l), and with identical L2P targets the near-field blocks too
+// (plan.reused_near).
 bool build_plan(Plan& plan, const PlanOptions& opt, int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int ndof,
-                const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof);
+                const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof,
+                Plan* prev = nullptr);
 
 // Groups the M2L pairs for the tensor-core path (tc_* fields); items hold <= max_pairs pairs.
 void build_tc_groups(Plan& plan, int max_pairs);

@@ -130,6 +130,18 @@ int bem_gpu_build_dofs(int32_t n_points, const double* X, int32_t n_faces, const
  * solveGMRES() before solveSystemGMRES (BEM_solveBVP_GMRES_FMM.hpp:3056-3447). */
 int bem_gpu_setup(bem_gpu_ctx* ctx, const bem_bvp_desc* desc);
 
+/* Set-up at new coordinates of the mesh of the last set-up (a Runge-Kutta stage or time step:
+ * same faces, boundary types and DOF tables, moved points), as the reference's solveGMRES does
+ * when the topology is unchanged (bem/BEM_solveBVP_GMRES_FMM.hpp:3125-3346): the octree is
+ * regrown in the root bucket of the previous set-up (a fresh root only if an element centroid
+ * left it), lists, sources, near-field weights and the rigid-mode diagonal are recomputed.
+ * What came out unchanged stays on the device: returns 2 (tree, lists and L2P targets kept:
+ * only the geometry is uploaded; near-field weights, P2M operator and diagonal recomputed),
+ * 1 (tree and lists kept, near-field blocks rebuilt), 0 (full set-up; also without a previous
+ * set-up or for another mesh) or a negative error code.  Either way the operator is the one a
+ * full set-up builds in that root bucket, bit for bit. */
+int bem_gpu_setup_refresh(bem_gpu_ctx* ctx, const bem_bvp_desc* desc);
+
 /* Solve with known boundary values (physical units; phi for Dirichlet DOFs, phin for
  * Neumann and corner-Neumann DOFs).  x0: initial guess of the unknowns in the same units
  * (phin for Dirichlet DOFs, phi for the others), e.g. the previous stage's solution as the
@@ -179,6 +191,12 @@ int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out /*[10]: nodes, leaves, dep
  * near-field sparsity for desc with opts and reports, per face, the level and lower corner
  * of the leaf bucket holding it (-1 if none), plus stats[10] as bem_gpu_tree_stats. */
 int bem_plan_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* desc, int32_t* face_level, double* face_corner, int64_t* stats);
+/* Host check of the refresh path (no device needed): plans desc0, then desc1 as a refresh of
+ * it, once taking over the unchanged structure and once rebuilding it in the same root.
+ * out[0] = 1 if the root bucket was kept, out[1] = the structure taken over (as the return
+ * value of bem_gpu_setup_refresh), out[2] = number of plan arrays in which the two desc1 plans
+ * differ (0 expected). */
+int bem_plan_refresh_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* desc0, const bem_bvp_desc* desc1, int64_t* out);
 
 /* Mat-vec stage timing with CUDA events on the context stream, averaged over repeats:
  * stage_ms = [p2m, m2m, m2l, l2l, near+l2p+rows, whole graph-launched mat-vec]. */
