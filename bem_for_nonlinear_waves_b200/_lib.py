@@ -29,7 +29,7 @@ STATUS = {0: "ok", -1: "invalid argument", -2: "out of memory", -3: "not converg
 class Opts(ctypes.Structure):
     _fields_ = [("expansion_order", c_int), ("mac_theta", c_dbl), ("leaf_max_elements", c_int), ("max_level", c_int),
                 ("tol", c_dbl), ("max_iter", c_int), ("device", c_int), ("tol_relative", c_int), ("preconditioner", c_int),
-                ("precision", c_int), ("poly_degree", c_int), ("reserved", c_int)]
+                ("precision", c_int), ("poly_degree", c_int), ("tree_on_host", c_int)]
 
 
 class MelSurface(ctypes.Structure):
@@ -79,6 +79,7 @@ EXPORTS = {
     "bem_harmonic_ritz_values": (c_int, [c_int, P_dbl, c_int, P_dbl, P_dbl]),
     "bem_plan_inspect": (c_int, [ctypes.POINTER(Opts), ctypes.POINTER(Desc), P_int, P_dbl, P_i64]),
     "bem_plan_refresh_inspect": (c_int, [ctypes.POINTER(Opts), ctypes.POINTER(Desc), ctypes.POINTER(Desc), P_i64]),
+    "bem_gpu_tree_check": (c_int, [ctypes.POINTER(Opts), ctypes.POINTER(Desc), P_i64]),
     "bem_gpu_mel_create": (ctypes.c_void_p, [c_int]),
     "bem_gpu_mel_destroy": (None, [ctypes.c_void_p]),
     "bem_gpu_mel_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),

@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 CXXFLAGS = ["-O2", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-Wall", "-fopenmp", "-pthread"]
 
-CU_SOURCES = ["kernels.cu", "m2l_tc.cu", "gmres.cu", "capi.cu", "mel.cu"]
+CU_SOURCES = ["kernels.cu", "m2l_tc.cu", "gmres.cu", "capi.cu", "mel.cu", "tree.cu"]
 CXX_SOURCES = ["plan.cpp", "batch.cpp", "poly.cpp"]
 
 

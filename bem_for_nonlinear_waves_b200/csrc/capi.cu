@@ -15,6 +15,7 @@
 #include "../../include/bem_b200.h"
 #include "fmm_math.cuh"
 #include "kernels.cuh"
+#include "tree_dev.hpp"
 #include "plan.hpp"
 
 using namespace bemb200;
@@ -53,9 +54,23 @@ struct DBuf {
 // the driver's pageable bounce buffer.  Grown on demand (after draining the stream).
 struct PinnedStage {
   unsigned char* p = nullptr;
-  size_t cap = 0, off = 0;
+  size_t cap = 0, off = 0, used = 0;  // used: bytes staged since begin()
   ~PinnedStage() {
     if (p) cudaFreeHost(p);
+  }
+  // start of a set-up's uploads: the area from its beginning, grown to `bytes` (the previous
+  // set-up's total) so that the uploads of one set-up do not wait for each other
+  cudaError_t begin(size_t bytes, cudaStream_t s) {
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    off = used = 0;
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    e = cudaHostAlloc((void**)&p, bytes, cudaHostAllocDefault);
+    if (e == cudaSuccess) cap = bytes;
+    return e;
   }
   // space for `bytes`, synchronising `s` when the area must be reused or grown
   cudaError_t reserve(size_t bytes, cudaStream_t s, unsigned char** out) {
@@ -75,6 +90,7 @@ struct PinnedStage {
     }
     *out = p + off;
     off += (bytes + 255) & ~size_t(255);
+    used += (bytes + 255) & ~size_t(255);
     return cudaSuccess;
   }
 };
@@ -161,7 +177,9 @@ struct bem_gpu_ctx {
   float setup_dev_ms = 0.f;
   double time_plan = 0.0, time_upload = 0.0;
 
+  DeviceTree* dtree = nullptr;  // octree growth on the device (set-up)
   PinnedStage stage;  // set-up uploads
+  size_t stage_bytes = 0;  // staged bytes of the last set-up (with alignment padding)
   ~bem_gpu_ctx() {
     if (stream) cudaStreamSynchronize(stream);
     for (auto& e : ev)
@@ -175,6 +193,7 @@ struct bem_gpu_ctx {
     for (auto& e : arn_ev)
       if (e) cudaEventDestroy(e);
     if (arn_err_host) cudaFreeHost(arn_err_host);
+    if (dtree) dtree_destroy(dtree);
     if (stream) cudaStreamDestroy(stream);
   }
   MatvecArgs args(const double* d_phi, const double* d_phin, double* d_rows, double* d_gphin, double* d_gnphi) const {
@@ -319,7 +338,7 @@ cudaError_t up(bem_gpu_ctx* ctx, DBuf<T>& b, const std::vector<T>& v) {
   if (e != cudaSuccess || v.empty()) return e;
   unsigned char* h = nullptr;
   if ((e = ctx->stage.reserve(bytes, ctx->stream, &h)) != cudaSuccess) return e;
-  std::memcpy(h, v.data(), bytes);
+  parallel_copy(h, v.data(), bytes);
   return cudaMemcpyAsync(b.p, h, bytes, cudaMemcpyHostToDevice, ctx->stream);
 }
 
@@ -613,6 +632,10 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   po.theta = ctx->opts.mac_theta;
   po.leaf_max = ctx->opts.leaf_max_elements;
   po.max_level = ctx->opts.max_level;
+  if (ctx->opts.tree_on_host == 0) {
+    if (!ctx->dtree) ctx->dtree = dtree_create(ctx->stream);
+    po.device_tree = ctx->dtree;
+  }
   {
     Plan fresh;
     if (!build_plan(fresh, po, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face,
@@ -627,6 +650,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   // a refresh that kept the tree and lists (reuse) and the L2P targets (reuse_near) skips the
   // uploads of what it kept: the buffers still hold the same data
   const bool reuse = P.reused_m2l, reuse_near = P.reused_near;
+  CK(ctx->stage.begin(ctx->stage_bytes, ctx->stream));
   auto ups = [&](auto& buf, const auto& v) -> cudaError_t { return reuse ? cudaSuccess : up(ctx, buf, v); };
   auto upn = [&](auto& buf, const auto& v) -> cudaError_t { return reuse_near ? cudaSuccess : up(ctx, buf, v); };
   cudaStream_t s = ctx->stream;
@@ -931,6 +955,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   }
   CK(cudaStreamSynchronize(s));
   ctx->time_upload = now_s() - t0 - ctx->time_plan;
+  ctx->stage_bytes = std::max(ctx->stage_bytes, ctx->stage.used);
   // device part of the set-up starts here (inputs resident): every kernel that derives the
   // operator's tables and weights from the uploaded plan
   CK(cudaEventRecord(ctx->ev[0], s));
@@ -1131,25 +1156,36 @@ int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out) {
   return BEM_OK;
 }
 
-int bem_plan_refresh_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* d0, const bem_bvp_desc* d1, int64_t* out) {
-  if (!opts || !d0 || !d1 || !out) return BEM_ERR_INVALID_ARGUMENT;
+static int64_t plan_diffs(const Plan& a1, const Plan& b1);
+
+int bem_gpu_tree_check(const bem_gpu_opts* opts, const bem_bvp_desc* d, int64_t* out) {
+  if (!opts || !d || !out) return BEM_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = nullptr;
+  if (cudaSetDevice(opts->device) != cudaSuccess || cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+    return BEM_ERR_DEVICE;
+  DeviceTree* dt = dtree_create(st);
   PlanOptions po;
   po.p = opts->expansion_order;
   po.theta = opts->mac_theta;
   po.leaf_max = opts->leaf_max_elements;
   po.max_level = opts->max_level;
-  auto build = [&](Plan& P, const bem_bvp_desc* d, Plan* prev, bool take) {
-    PlanOptions o = po;
-    o.take_structure = take;
-    if (!build_plan(P, o, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face, d->dof_kind,
-                    d->face_dof, prev))
-      return false;
-    if (!P.reused_m2l) build_tc_groups(P, tc_max_pairs());
-    return true;
-  };
-  Plan a0, b0, a1, b1;
-  if (!build(a0, d0, nullptr, true) || !build(b0, d0, nullptr, true)) return BEM_ERR_INVALID_ARGUMENT;
-  if (!build(a1, d1, &a0, true) || !build(b1, d1, &b0, false)) return BEM_ERR_INVALID_ARGUMENT;
+  Plan host, dev;
+  bool ok = build_plan(host, po, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face,
+                       d->dof_kind, d->face_dof);
+  po.device_tree = dt;
+  ok = ok && build_plan(dev, po, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face,
+                        d->dof_kind, d->face_dof);
+  dtree_destroy(dt);
+  cudaStreamDestroy(st);
+  if (!ok) return BEM_ERR_INVALID_ARGUMENT;
+  out[0] = dev.tree_on_device;
+  out[1] = plan_diffs(host, dev) + (host.n_child_drops != dev.n_child_drops) + (host.n_added != dev.n_added);
+  out[2] = (int64_t)dev.nodes.size();
+  out[3] = dev.n_child_drops;
+  return BEM_OK;
+}
+
+static int64_t plan_diffs(const Plan& a1, const Plan& b1) {
   int64_t diff = 0;
 #define BEMB200_CMP(f) diff += (a1.f == b1.f) ? 0 : 1;
   BEMB200_CMP(Xs) BEMB200_CMP(L) BEMB200_CMP(scale) BEMB200_CMP(near_region) BEMB200_CMP(face_of_pos) BEMB200_CMP(pos_of_face)
@@ -1170,6 +1206,29 @@ int bem_plan_refresh_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* d0, c
     diff += x.node != y.node || x.w_off != y.w_off || x.dof_off != y.dof_off || x.ndof != y.ndof || x.tgt_off != y.tgt_off ||
             x.ntgt != y.ntgt || x.rng_off != y.rng_off || x.nrng != y.nrng;
   }
+  return diff;
+}
+
+int bem_plan_refresh_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* d0, const bem_bvp_desc* d1, int64_t* out) {
+  if (!opts || !d0 || !d1 || !out) return BEM_ERR_INVALID_ARGUMENT;
+  PlanOptions po;
+  po.p = opts->expansion_order;
+  po.theta = opts->mac_theta;
+  po.leaf_max = opts->leaf_max_elements;
+  po.max_level = opts->max_level;
+  auto build = [&](Plan& P, const bem_bvp_desc* d, Plan* prev, bool take) {
+    PlanOptions o = po;
+    o.take_structure = take;
+    if (!build_plan(P, o, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face, d->dof_kind,
+                    d->face_dof, prev))
+      return false;
+    if (!P.reused_m2l) build_tc_groups(P, tc_max_pairs());
+    return true;
+  };
+  Plan a0, b0, a1, b1;
+  if (!build(a0, d0, nullptr, true) || !build(b0, d0, nullptr, true)) return BEM_ERR_INVALID_ARGUMENT;
+  if (!build(a1, d1, &a0, true) || !build(b1, d1, &b0, false)) return BEM_ERR_INVALID_ARGUMENT;
+  const int64_t diff = plan_diffs(a1, b1);
   bool same_root = true;
   for (int k = 0; k < 3; ++k) same_root = same_root && a1.root_C[k] == a0.root_C[k];
   out[0] = same_root && a1.root_R == a0.root_R;

@@ -3,6 +3,8 @@
 // reference's so that the octree is the same tree.
 #include "plan.hpp"
 
+#include "tree_dev.hpp"
+
 #include <algorithm>
 #include <parallel/algorithm>
 #include <cmath>
@@ -163,6 +165,127 @@ struct TreeBuilder {
   }
 };
 
+// The same growth with the element classification on the device (tree.cu), level by level:
+// buckets are created per level (breadth first) and renumbered depth first at the end, which
+// is the order grow() creates them in.  The root holds its elements already.  Returns false
+// (tree left as the root alone) if a device step fails or a bucket is not 2x2x2 cells.
+bool grow_on_device(TreeBuilder& T, DeviceTree* dt, int nf, const std::vector<V3>& pole) {
+  std::vector<Bucket>& B = T.B;
+  const PlanOptions& opt = T.opt;
+  if (B.size() != 1) return false;
+  std::vector<double> P3(3 * (size_t)nf);
+  for (int f = 0; f < nf; ++f)
+    for (int a = 0; a < 3; ++a) P3[3 * (size_t)f + a] = pole[f][a];
+  const std::vector<int> root_data = B[0].data;
+  if (!dtree_begin(dt, nf, P3.data(), (int)root_data.size(), root_data.data(), opt.max_level)) return false;
+  // breadth-first buckets: index 0 = root; per bucket its segment in its level's array
+  std::vector<Bucket> Q;
+  Q.push_back(B[0]);
+  std::vector<int> seg_b{0}, seg_e{(int)root_data.size()}, level_of{0};
+  std::vector<size_t> level_base{0};
+  std::vector<int> cur{0};
+  size_t base = 0, cur_n = root_data.size();
+  int drops = 0;
+  while (!cur.empty()) {
+    std::vector<int> split;
+    for (int q : cur) {
+      const int n = seg_e[q] - seg_b[q];
+      if (n > 0 && n > opt.leaf_max && Q[q].level < opt.max_level) split.push_back(q);
+    }
+    if (split.empty()) break;
+    const int ns = (int)split.size();
+    std::vector<int> sb(ns), se(ns), ca(8 * (size_t)ns), cp(8 * (size_t)ns);
+    std::vector<double> geo(63 * (size_t)ns);
+    std::vector<Bucket> kid(8 * (size_t)ns);
+    for (int k = 0; k < ns; ++k) {
+      const Bucket& b = Q[split[k]];
+      if (b.size[0] != 2 || b.size[1] != 2 || b.size[2] != 2) return false;
+      sb[k] = seg_b[split[k]];
+      se[k] = seg_e[split[k]];
+      double* g = &geo[63 * (size_t)k];
+      for (int a = 0; a < 3; ++a) {
+        g[a] = b.xmin[a];
+        g[4 + a] = b.size[a];
+      }
+      g[3] = b.inv_dL;
+      for (int c = 0; c < 8; ++c) {  // the child grow() would create for cell c
+        const int i = c / (b.size[1] * b.size[2]), j = (c / b.size[2]) % b.size[1], kk = c % b.size[2];
+        const int ijk[3] = {i, j, kk};
+        double lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) {
+          lo[a] = b.dL * ijk[a] + b.xmin[a];
+          hi[a] = b.dL * (ijk[a] + 1) + b.xmin[a];
+        }
+        Bucket& ch = kid[8 * (size_t)k + c];
+        bucket_init(ch, lo, hi, b.dL * (0.5 + 1e-13));
+        double* gc = g + 7 * (1 + c);
+        for (int a = 0; a < 3; ++a) {
+          gc[a] = ch.xmin[a];
+          gc[4 + a] = ch.size[a];
+        }
+        gc[3] = ch.inv_dL;
+      }
+    }
+    if (!dtree_count(dt, ns, sb.data(), se.data(), geo.data(), ca.data(), cp.data())) return false;
+    std::vector<int> off(8 * (size_t)ns, 0);
+    int total = 0;
+    std::vector<int> next;
+    for (int k = 0; k < ns; ++k)
+      for (int c = 0; c < 8; ++c) {
+        const size_t kc = 8 * (size_t)k + c;
+        off[kc] = total;
+        if (ca[kc] == 0) continue;
+        Bucket ch = std::move(kid[kc]);
+        ch.level = Q[split[k]].level + 1;
+        ch.parent = split[k];
+        const int qi = (int)Q.size();
+        Q.push_back(std::move(ch));
+        Q[split[k]].kids.push_back(qi);
+        Q[split[k]].kid_of_cell[c] = qi;
+        seg_b.push_back(total);
+        seg_e.push_back(total + cp[kc]);
+        level_of.push_back(Q[qi].level);
+        next.push_back(qi);
+        drops += ca[kc] - cp[kc];
+        total += cp[kc];
+      }
+    if (!dtree_scatter(dt, ns, off.data(), total)) return false;
+    base += cur_n;
+    cur_n = (size_t)total;
+    level_base.push_back(base);
+    cur.swap(next);
+  }
+  std::vector<int> all(base + cur_n);
+  if (!dtree_download(dt, all.data(), all.size())) return false;
+  for (size_t q = 1; q < Q.size(); ++q) {
+    const size_t lb = level_base[level_of[q]];
+    Q[q].data.assign(all.begin() + lb + seg_b[q], all.begin() + lb + seg_e[q]);
+  }
+  // depth-first renumbering (grow() creates a bucket, then its subtree, then its next sibling)
+  std::vector<int> id(Q.size(), -1), order;
+  order.reserve(Q.size());
+  std::vector<int> stack{0};
+  while (!stack.empty()) {
+    const int q = stack.back();
+    stack.pop_back();
+    id[q] = (int)order.size();
+    order.push_back(q);
+    for (auto it = Q[q].kids.rbegin(); it != Q[q].kids.rend(); ++it) stack.push_back(*it);
+  }
+  B.clear();
+  B.reserve(Q.size());
+  for (int q : order) {
+    Bucket b = std::move(Q[q]);
+    if (b.parent >= 0) b.parent = id[b.parent];
+    for (int& k : b.kids) k = id[k];
+    for (int& k : b.kid_of_cell)
+      if (k >= 0) k = id[k];
+    B.push_back(std::move(b));
+  }
+  T.drops = drops;
+  return true;
+}
+
 bool is_far(const PlanOptions& o, const Bucket& A, const Bucket& Bk) {  // moments.hpp:950-956
   const double eff = std::max(A.dL + 2.0 * A.off, Bk.dL + 2.0 * Bk.off);
   const V3 d{Bk.X[0] - A.X[0], Bk.X[1] - A.X[1], Bk.X[2] - A.X[2]};
@@ -188,6 +311,20 @@ void lists(const PlanOptions& o, std::vector<Bucket>& B, int a, int b) {  // mom
 }
 
 }  // namespace
+
+void parallel_copy(void* dst, const void* src, size_t bytes) {
+  constexpr size_t kPiece = size_t(1) << 20;
+  if (bytes < 4 * kPiece) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  const int64_t n = (int64_t)((bytes + kPiece - 1) / kPiece);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    const size_t a = (size_t)i * kPiece, b = std::min(bytes, a + kPiece);
+    std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a);
+  }
+}
 
 int build_dofs(int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int32_t* dof_point, int32_t* dof_face,
                int32_t* dof_kind, int32_t* face_dof, uint8_t* point_flags) {
@@ -432,6 +569,16 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     bucket_init(root, lo, hi, dLr);
     T.B.push_back(std::move(root));
     for (int f = 0; f < nf; ++f) P.n_added += T.add(0, f);
+    if (opt.device_tree && grow_on_device(T, static_cast<DeviceTree*>(opt.device_tree), nf, pole)) {
+      P.tree_on_device = true;
+      return;
+    }
+    P.tree_on_device = false;
+    if (T.B.size() != 1) {  // a device step failed part-way: grow on the host from the root alone
+      T.B.resize(1);
+      T.B[0].kids.clear();
+      T.B[0].kid_of_cell.assign(T.B[0].kid_of_cell.size(), -1);
+    }
     T.grow(0);
   };
   if (keep_root) {

@@ -8,6 +8,7 @@
 // 1078-1111) and this file is compiled without fast-math.
 #pragma once
 #include <array>
+#include <cstddef>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -20,6 +21,7 @@ struct PlanOptions {
   int leaf_max = 30;
   int max_level = 7;
   bool take_structure = true;  // refresh: take over the previous plan's unchanged structure (false: rebuild it)
+  void* device_tree = nullptr;  // DeviceTree (tree_dev.hpp): grow the octree on the device; null: on the host
 };
 
 struct Plan {
@@ -120,6 +122,7 @@ struct Plan {
   // grouping and tensor-core items were taken over from it; reused_near: the L2P targets too,
   // and with them the near-field blocks
   bool reused_m2l = false, reused_near = false;
+  bool tree_on_device = false;  // the octree was grown on the device
 
   std::string error;
 };
@@ -141,6 +144,9 @@ int build_dofs(int np, const double* X, int nf, const int32_t* tri, const uint8_
 bool build_plan(Plan& plan, const PlanOptions& opt, int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int ndof,
                 const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof,
                 Plan* prev = nullptr);
+
+// memcpy in 1 MiB pieces over the OpenMP threads (staging of the set-up uploads)
+void parallel_copy(void* dst, const void* src, size_t bytes);
 
 // Groups the M2L pairs for the tensor-core path (tc_* fields); items hold <= max_pairs pairs.
 void build_tc_groups(Plan& plan, int max_pairs);

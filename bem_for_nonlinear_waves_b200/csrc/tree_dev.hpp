@@ -1,0 +1,22 @@
+// Octree growth on the device (tree.cu), driven level by level from plan.cpp.  No CUDA types:
+// plan.cpp is host C++.
+#pragma once
+#include <cstddef>
+
+namespace bemb200 {
+
+struct DeviceTree;
+DeviceTree* dtree_create(void* stream);  // stream: a cudaStream_t
+void dtree_destroy(DeviceTree* t);
+// poles [3*nf]; the root bucket's elements in data order; levels below the root <= max_level
+bool dtree_begin(DeviceTree* t, int nf, const double* poles, int n_root, const int* root_elems, int max_level);
+// n splitting buckets of the current level: segments into the level's element array and the
+// geometry of each (parent, then its 8 children: xmin[3], 1/dL, size[3]); per (bucket, cell)
+// the elements of the cell (cnt_all) and those the child keeps (cnt_pass)
+bool dtree_count(DeviceTree* t, int n, const int* seg_beg, const int* seg_end, const double* geo, int* cnt_all, int* cnt_pass);
+// the next level's array: kept elements of (bucket, cell) at off[bucket * 8 + cell], stable
+bool dtree_scatter(DeviceTree* t, int n, const int* off, int total);
+// every level's array, back to back from the root's
+bool dtree_download(DeviceTree* t, int* out, size_t count);
+
+}  // namespace bemb200

@@ -65,7 +65,7 @@ typedef struct {
                                 M2L (FP16 split operands, FP32 accumulate), FP64 outer refinement on the
                                 true residual, same stopping test; needs p <= 12 */
   int32_t poly_degree;       /* preconditioner 2: polynomial degree 1..24 (0: 8) */
-  int32_t reserved;
+  int32_t tree_on_host;      /* 0: the octree is grown on the device (tree.cu), 1: on the host; same tree */
 } bem_gpu_opts;
 
 /* One boundary-value problem.  The DOF table is what the reference's setNodeFaceIndices()
@@ -197,6 +197,12 @@ int bem_plan_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* desc, int32_t
  * value of bem_gpu_setup_refresh), out[2] = number of plan arrays in which the two desc1 plans
  * differ (0 expected). */
 int bem_plan_refresh_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* desc0, const bem_bvp_desc* desc1, int64_t* out);
+
+/* The octree grown on the device against the host's growth of the same BVP (both bit-exact
+ * restatements of the reference's Buckets::generateTree): out[0] = 1 if the device growth ran,
+ * out[1] = number of plan arrays that differ (0 expected), out[2] = buckets, out[3] = elements
+ * a child refused (the reference's InsideQ edge case).  Needs a device. */
+int bem_gpu_tree_check(const bem_gpu_opts* opts, const bem_bvp_desc* desc, int64_t* out);
 
 /* Mat-vec stage timing with CUDA events on the context stream, averaged over repeats:
  * stage_ms = [p2m, m2m, m2l, l2l, near+l2p+rows, whole graph-launched mat-vec]. */
