@@ -68,8 +68,9 @@ struct PinnedStage {
     if (p) cudaFreeHost(p);
     p = nullptr;
     cap = 0;
-    e = cudaHostAlloc((void**)&p, bytes, cudaHostAllocDefault);
-    if (e == cudaSuccess) cap = bytes;
+    const size_t want = bytes + bytes / 4;  // headroom: pinning is slow, the next mesh may be a little larger
+    e = cudaHostAlloc((void**)&p, want, cudaHostAllocDefault);
+    if (e == cudaSuccess) cap = want;
     return e;
   }
   // space for `bytes`, synchronising `s` when the area must be reused or grown
@@ -1178,7 +1179,7 @@ int bem_gpu_tree_check(const bem_gpu_opts* opts, const bem_bvp_desc* d, int64_t*
   dtree_destroy(dt);
   cudaStreamDestroy(st);
   if (!ok) return BEM_ERR_INVALID_ARGUMENT;
-  out[0] = dev.tree_on_device;
+  out[0] = (int)dev.tree_on_device + 2 * (int)dev.lists_on_device;
   out[1] = plan_diffs(host, dev) + (host.n_child_drops != dev.n_child_drops) + (host.n_added != dev.n_added);
   out[2] = (int64_t)dev.nodes.size();
   out[3] = dev.n_child_drops;

@@ -610,7 +610,30 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   // descendants, so the traversal runs serially down to the calls whose target is at level
   // kSplit, records those calls in order, and then runs each such target's calls (in the
   // recorded order) in parallel: every list ends up in the serial order.
-  {
+  bool lists_done = false;
+  if (opt.device_tree) {  // level by level on the device (tree.cu), same lists in the same order
+    std::vector<double> nXv(3 * (size_t)nb), ndl(nb), nof(nb);
+    std::vector<int> cbv(nb), cev(nb), chv;
+    for (int i = 0; i < nb; ++i) {
+      for (int a = 0; a < 3; ++a) nXv[3 * (size_t)i + a] = B[i].X[a];
+      ndl[i] = B[i].dL;
+      nof[i] = B[i].off;
+      cbv[i] = (int)chv.size();
+      chv.insert(chv.end(), B[i].kids.begin(), B[i].kids.end());
+      cev[i] = (int)chv.size();
+    }
+    std::vector<std::vector<int>> nr, ml;
+    if (dtree_lists(static_cast<DeviceTree*>(opt.device_tree), nb, nXv.data(), ndl.data(), nof.data(), cbv.data(), cev.data(), chv.data(),
+                    (int)chv.size(), opt.theta, nr, ml)) {
+      for (int i = 0; i < nb; ++i) {
+        B[i].near.swap(nr[i]);
+        B[i].m2l.swap(ml[i]);
+      }
+      lists_done = true;
+      P.lists_on_device = true;
+    }
+  }
+  if (!lists_done) {
     constexpr int kSplit = 2;
     std::vector<std::pair<int, int>> tasks;
     std::function<void(int, int)> top = [&](int a, int b) {

@@ -122,7 +122,8 @@ struct Plan {
   // grouping and tensor-core items were taken over from it; reused_near: the L2P targets too,
   // and with them the near-field blocks
   bool reused_m2l = false, reused_near = false;
-  bool tree_on_device = false;  // the octree was grown on the device
+  bool tree_on_device = false;   // the octree was grown on the device
+  bool lists_on_device = false;  // and the interaction lists built there
 
   std::string error;
 };

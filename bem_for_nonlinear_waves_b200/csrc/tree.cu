@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <algorithm>
 #include <vector>
 
 #include "tree_dev.hpp"
@@ -109,6 +110,105 @@ __global__ void __launch_bounds__(256) k_tree_scatter(const int* __restrict__ se
   }
 }
 
+// ---- interaction lists (moments.hpp:950-997) ----
+// isFar with the host's arithmetic (plan.cpp is_far as g++ compiles it: the squared distance and
+// the hypot sum contracted as fma(z, z, fma(y, y, x * x)), eff as dL + 2 off), so the decisions
+// are the host's, including the pairs within 1e-9 of the threshold that take the exact form
+struct NodeGeo {
+  const double* X;  // [3 * nb]
+  const double* dL;
+  const double* off;
+  const int* cb;  // children of node i: children[cb[i] .. ce[i])
+  const int* ce;
+  const int* children;
+};
+
+__device__ __forceinline__ double hypot3_dev(double x, double y, double z) {
+  x = fabs(x);
+  y = fabs(y);
+  z = fabs(z);
+  const double a = x < y ? (y < z ? z : y) : (x < z ? z : x);
+  if (a == 0.0) return 0.0;
+  const double xa = __ddiv_rn(x, a), ya = __ddiv_rn(y, a), za = __ddiv_rn(z, a);
+  return __dmul_rn(a, __dsqrt_rn(fma(za, za, fma(ya, ya, __dmul_rn(xa, xa)))));
+}
+
+__device__ __forceinline__ bool is_far_dev(const NodeGeo& g, double theta, int a, int b) {
+  const double ea = fma(2.0, g.off[a], g.dL[a]), eb = fma(2.0, g.off[b], g.dL[b]);
+  const double eff = ea > eb ? ea : eb;  // std::max(ea, eb)
+  const double d0 = __dsub_rn(g.X[3 * b], g.X[3 * a]), d1 = __dsub_rn(g.X[3 * b + 1], g.X[3 * a + 1]),
+               d2 = __dsub_rn(g.X[3 * b + 2], g.X[3 * a + 2]);
+  const double s3e = __dmul_rn(1.7320508075688772, eff);
+  const double thr = __ddiv_rn(s3e, theta);
+  const double dd = fma(d2, d2, fma(d1, d1, __dmul_rn(d0, d0)));
+  const double t2 = __dmul_rn(thr, thr);
+  if (dd > __dmul_rn(t2, 1.0 + 1e-9)) return true;
+  if (dd < __dmul_rn(t2, 1.0 - 1e-9)) return false;
+  return theta > __ddiv_rn(s3e, hypot3_dev(d0, d1, d2));
+}
+
+// one warp per target x: for each candidate b (lists(x, b) calls, in order) that is not far:
+// near[x] += b (b != x); for each child pair (ac, bc) of (x, b): far -> m2l[ac] += bc, else
+// lists(ac, bc) is called (candidate of ac at the next level).  fill = 0: counts only.
+template <bool kFill>
+__global__ void __launch_bounds__(128) k_lists(int n, const int* __restrict__ tgt, const int* __restrict__ cand_off,
+                                               const int* __restrict__ cand, NodeGeo g, double theta, int* __restrict__ cnt_near,
+                                               int* __restrict__ cnt_m2l, int* __restrict__ cnt_next, const int* __restrict__ near_off,
+                                               const int* __restrict__ m2l_off, const int* __restrict__ next_off,
+                                               int* __restrict__ near_out, int* __restrict__ m2l_out, int* __restrict__ next_out) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= n) return;
+  const unsigned lt = (1u << lane) - 1u;
+  const int x = tgt[w];
+  const int kx0 = g.cb[x], nkx = g.ce[x] - g.cb[x];
+  int cn = 0, rm[8], rn[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) rm[s] = rn[s] = 0;
+  for (int k = cand_off[w]; k < cand_off[w + 1]; ++k) {
+    const int b = cand[k];
+    if (is_far_dev(g, theta, x, b)) continue;
+    if (x != b) {
+      if (kFill && lane == 0) near_out[near_off[w] + cn] = b;
+      ++cn;
+    }
+    const int kb0 = g.cb[b], nkb = g.ce[b] - g.cb[b];
+    const int combos = nkx * nkb;
+    for (int base = 0; base < combos; base += 32) {
+      const int j = base + lane;
+      const bool valid = j < combos;
+      int ai = -1, bc = -1;
+      bool f = false;
+      if (valid) {
+        ai = j / nkb;
+        const int ac = g.children[kx0 + ai];
+        bc = g.children[kb0 + (j - ai * nkb)];
+        f = ac != bc && is_far_dev(g, theta, ac, bc);
+      }
+#pragma unroll
+      for (int s = 0; s < 8; ++s) {
+        const unsigned mm = __ballot_sync(0xffffffffu, valid && ai == s && f);
+        const unsigned mn = __ballot_sync(0xffffffffu, valid && ai == s && !f);
+        if (kFill && valid && ai == s) {
+          if (f)
+            m2l_out[m2l_off[8 * w + s] + rm[s] + __popc(mm & lt)] = bc;
+          else
+            next_out[next_off[8 * w + s] + rn[s] + __popc(mn & lt)] = bc;
+        }
+        rm[s] += __popc(mm);
+        rn[s] += __popc(mn);
+      }
+    }
+  }
+  if (!kFill && lane == 0) {
+    cnt_near[w] = cn;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      cnt_m2l[8 * w + s] = rm[s];
+      cnt_next[8 * w + s] = rn[s];
+    }
+  }
+}
+
 template <typename T>
 struct Buf {
   T* p = nullptr;
@@ -134,6 +234,8 @@ struct DeviceTree {
   Buf<double> poles, geo;
   Buf<int> elems, seg_beg, seg_end, cnt, off;  // elems: every level's array, back to back
   Buf<uint8_t> tag;
+  Buf<double> nX, ndL, noff;                              // interaction lists: node geometry
+  Buf<int> ncb, nce, nch, lt, lco, lc, lcnt, loff, lno, lmo, lxo;  // and per-level work arrays
   size_t cur = 0, cur_n = 0;  // current level: offset into elems, length
   std::vector<int> h_beg, h_end;
 };
@@ -201,6 +303,95 @@ bool dtree_scatter(DeviceTree* t, int n, const int* off, int total) {
   }
   t->cur = next;
   t->cur_n = (size_t)total;
+  return true;
+}
+
+bool dtree_lists(DeviceTree* t, int nb, const double* X, const double* dL, const double* off, const int* cb, const int* ce,
+                 const int* children, int n_children, double theta, std::vector<std::vector<int>>& near,
+                 std::vector<std::vector<int>>& m2l) {
+  cudaStream_t s = t->stream;
+  near.assign(nb, {});
+  m2l.assign(nb, {});
+  if (nb <= 0) return true;
+  for (int i = 0; i < nb; ++i)
+    if (cb[i] < 0 || ce[i] < cb[i] || ce[i] - cb[i] > 8 || ce[i] > n_children) return false;
+  for (int i = 0; i < n_children; ++i)
+    if (children[i] < 0 || children[i] >= nb) return false;
+  if (!t->nX.fit((size_t)3 * nb) || !t->ndL.fit(nb) || !t->noff.fit(nb) || !t->ncb.fit(nb) || !t->nce.fit(nb) ||
+      !t->nch.fit((size_t)std::max(n_children, 1)))
+    return false;
+  if (cudaMemcpyAsync(t->nX.p, X, sizeof(double) * 3 * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(t->ndL.p, dL, sizeof(double) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(t->noff.p, off, sizeof(double) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(t->ncb.p, cb, sizeof(int) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(t->nce.p, ce, sizeof(int) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      (n_children && cudaMemcpyAsync(t->nch.p, children, sizeof(int) * n_children, cudaMemcpyHostToDevice, s) != cudaSuccess))
+    return false;
+  const NodeGeo g{t->nX.p, t->ndL.p, t->noff.p, t->ncb.p, t->nce.p, t->nch.p};
+  // level 1: every child of the root against every child of the root, in order
+  std::vector<int> tg(children + cb[0], children + ce[0]), coff(1, 0), cd;
+  for (size_t i = 0; i < tg.size(); ++i) {
+    cd.insert(cd.end(), children + cb[0], children + ce[0]);
+    coff.push_back((int)cd.size());
+  }
+  while (!tg.empty()) {
+    const int n = (int)tg.size();
+    if (!t->lt.fit(n) || !t->lco.fit((size_t)n + 1) || !t->lc.fit(std::max<size_t>(cd.size(), 1)) || !t->lcnt.fit((size_t)17 * n) ||
+        !t->loff.fit((size_t)17 * n + 1))
+      return false;
+    if (cudaMemcpyAsync(t->lt.p, tg.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(t->lco.p, coff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        (!cd.empty() && cudaMemcpyAsync(t->lc.p, cd.data(), sizeof(int) * cd.size(), cudaMemcpyHostToDevice, s) != cudaSuccess))
+      return false;
+    const int blocks = (n + 3) / 4;  // 4 warps per block
+    int* cnt = t->lcnt.p;
+    k_lists<false><<<blocks, 128, 0, s>>>(n, t->lt.p, t->lco.p, t->lc.p, g, theta, cnt, cnt + n, cnt + 9 * n, nullptr, nullptr, nullptr,
+                                          nullptr, nullptr, nullptr);
+    if (cudaGetLastError() != cudaSuccess) return false;
+    std::vector<int> hc((size_t)17 * n);
+    if (cudaMemcpyAsync(hc.data(), cnt, sizeof(int) * 17 * n, cudaMemcpyDeviceToHost, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+      return false;
+    // offsets: near per target, m2l and next candidates per (target, child slot)
+    std::vector<int> ho((size_t)17 * n);
+    int tn = 0, tm = 0, tx = 0;
+    for (int w = 0; w < n; ++w) {
+      ho[w] = tn;
+      tn += hc[w];
+    }
+    for (int i = 0; i < 8 * n; ++i) {
+      ho[n + i] = tm;
+      tm += hc[n + i];
+      ho[9 * n + i] = tx;
+      tx += hc[9 * n + i];
+    }
+    if (!t->lno.fit(std::max(tn, 1)) || !t->lmo.fit(std::max(tm, 1)) || !t->lxo.fit(std::max(tx, 1))) return false;
+    if (cudaMemcpyAsync(t->loff.p, ho.data(), sizeof(int) * 17 * n, cudaMemcpyHostToDevice, s) != cudaSuccess) return false;
+    k_lists<true><<<blocks, 128, 0, s>>>(n, t->lt.p, t->lco.p, t->lc.p, g, theta, nullptr, nullptr, nullptr, t->loff.p, t->loff.p + n,
+                                         t->loff.p + 9 * n, t->lno.p, t->lmo.p, t->lxo.p);
+    if (cudaGetLastError() != cudaSuccess) return false;
+    std::vector<int> hn(tn), hm(tm), hx(tx);
+    if ((tn && cudaMemcpyAsync(hn.data(), t->lno.p, sizeof(int) * tn, cudaMemcpyDeviceToHost, s) != cudaSuccess) ||
+        (tm && cudaMemcpyAsync(hm.data(), t->lmo.p, sizeof(int) * tm, cudaMemcpyDeviceToHost, s) != cudaSuccess) ||
+        (tx && cudaMemcpyAsync(hx.data(), t->lxo.p, sizeof(int) * tx, cudaMemcpyDeviceToHost, s) != cudaSuccess) ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      return false;
+    std::vector<int> ntg, ncoff(1, 0), ncd;
+    for (int w = 0; w < n; ++w) {
+      const int x = tg[w];
+      near[x].insert(near[x].end(), hn.begin() + ho[w], hn.begin() + ho[w] + hc[w]);
+      for (int sl = 0; sl < ce[x] - cb[x]; ++sl) {
+        const int ac = children[cb[x] + sl], i = 8 * w + sl;
+        m2l[ac].insert(m2l[ac].end(), hm.begin() + ho[n + i], hm.begin() + ho[n + i] + hc[n + i]);
+        if (hc[9 * n + i] == 0) continue;
+        ntg.push_back(ac);
+        ncd.insert(ncd.end(), hx.begin() + ho[9 * n + i], hx.begin() + ho[9 * n + i] + hc[9 * n + i]);
+        ncoff.push_back((int)ncd.size());
+      }
+    }
+    tg.swap(ntg);
+    coff.swap(ncoff);
+    cd.swap(ncd);
+  }
   return true;
 }
 

@@ -2,6 +2,7 @@
 // plan.cpp is host C++.
 #pragma once
 #include <cstddef>
+#include <vector>
 
 namespace bemb200 {
 
@@ -16,6 +17,12 @@ bool dtree_begin(DeviceTree* t, int nf, const double* poles, int n_root, const i
 bool dtree_count(DeviceTree* t, int n, const int* seg_beg, const int* seg_end, const double* geo, int* cnt_all, int* cnt_pass);
 // the next level's array: kept elements of (bucket, cell) at off[bucket * 8 + cell], stable
 bool dtree_scatter(DeviceTree* t, int n, const int* off, int total);
+// interaction lists of lists() (moments.hpp:967-997) from the level-1 pairs, level by level on
+// the device: near[x], m2l[x] in the order the reference's recursion appends them.  Nodes in
+// creation order; children[cb[i] .. ce[i]) in cell order (at most 8)
+bool dtree_lists(DeviceTree* t, int nb, const double* X, const double* dL, const double* off, const int* cb, const int* ce,
+                 const int* children, int n_children, double theta, std::vector<std::vector<int>>& near,
+                 std::vector<std::vector<int>>& m2l);
 // every level's array, back to back from the root's
 bool dtree_download(DeviceTree* t, int* out, size_t count);
 

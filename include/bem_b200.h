@@ -199,7 +199,8 @@ int bem_plan_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* desc, int32_t
 int bem_plan_refresh_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* desc0, const bem_bvp_desc* desc1, int64_t* out);
 
 /* The octree grown on the device against the host's growth of the same BVP (both bit-exact
- * restatements of the reference's Buckets::generateTree): out[0] = 1 if the device growth ran,
+ * restatements of the reference's Buckets::generateTree and list traversal): out[0] = 1 if the
+ * device grew the tree, + 2 if it built the interaction lists,
  * out[1] = number of plan arrays that differ (0 expected), out[2] = buckets, out[3] = elements
  * a child refused (the reference's InsideQ edge case).  Needs a device. */
 int bem_gpu_tree_check(const bem_gpu_opts* opts, const bem_bvp_desc* desc, int64_t* out);
