@@ -76,6 +76,7 @@ EXPORTS = {
     "bem_gpu_check_device_status": (c_int, [ctypes.c_void_p]),
     "bem_gpu_fp64_peak_tflops": (c_dbl, [c_int]),
     "bem_gpu_poly_roots": (c_int, [ctypes.c_void_p, c_int, P_dbl, P_dbl]),
+    "bem_gpu_setup_phases": (c_int, [ctypes.c_void_p, P_dbl]),
     "bem_harmonic_ritz_values": (c_int, [c_int, P_dbl, c_int, P_dbl, P_dbl]),
     "bem_plan_inspect": (c_int, [ctypes.POINTER(Opts), ctypes.POINTER(Desc), P_int, P_dbl, P_i64]),
     "bem_plan_refresh_inspect": (c_int, [ctypes.POINTER(Opts), ctypes.POINTER(Desc), ctypes.POINTER(Desc), P_i64]),

@@ -40,7 +40,7 @@ def build_dofs(X, tri, face_dirichlet):
 
 
 def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter, device,
-               tol_relative, preconditioner, precision, poly_degree=8):
+               tol_relative, preconditioner, precision, poly_degree=8, tree_on_device=True):
     o = L.Opts()
     lib.bem_gpu_default_opts(ctypes.byref(o))
     o.expansion_order = int(expansion_order)
@@ -53,6 +53,7 @@ def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_l
     o.tol_relative = 1 if tol_relative else 0
     o.preconditioner = {"none": 0, "jacobi": 1, "near_poly": 2}[preconditioner]
     o.poly_degree = int(poly_degree)
+    o.tree_on_host = 0 if tree_on_device else 1
     o.precision = {"fp64": 0, "mixed": 1}[precision]
     return o
 
@@ -62,7 +63,7 @@ class BEM_BVP:
 
     def __init__(self, X, tri, face_dirichlet, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30,
                  fmm_max_level=7, solver_tol=1e-9, solver_max_iter=500, device=0, dofs=None, tol_relative=False, preconditioner="none",
-                 precision="fp64", poly_degree=8):
+                 precision="fp64", poly_degree=8, tree_on_device=True):
         self.lib = L.load()
         if not self.lib.bem_gpu_is_available():
             raise RuntimeError("no sm_100 CUDA device visible: the GMRES-FMM solver runs only on the GPU")
@@ -70,7 +71,7 @@ class BEM_BVP:
         self.tri = np.ascontiguousarray(tri, np.int32)
         self.face_dirichlet = np.ascontiguousarray(face_dirichlet, np.uint8)
         o = _make_opts(self.lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter,
-                       device, tol_relative, preconditioner, precision, poly_degree)
+                       device, tol_relative, preconditioner, precision, poly_degree, tree_on_device)
         self.opts = o
         self.ctx = self.lib.bem_gpu_create(ctypes.byref(o))
         if not self.ctx:
@@ -177,6 +178,16 @@ class BEM_BVP:
         self._check(self.lib.bem_gpu_point_integrals(self.ctx, L.ptr(phi, L.P_dbl), L.ptr(phin, L.P_dbl), L.ptr(a, L.P_dbl),
                                                      L.ptr(b, L.P_dbl)), "point_integrals")
         return a, b
+
+    def setup_phases(self):
+        """Seconds spent in each part of the last set-up (host plan phases, uploads, device part)."""
+        out = np.zeros(10)
+        self._check(self.lib.bem_gpu_setup_phases(self.ctx, L.ptr(out, L.P_dbl)), "bem_gpu_setup_phases")
+        keys = ["sources", "octree", "lists", "order_nodes", "m2l_groups", "near_blocks", "dof_incidence", "upload", "device"]
+        d = {k: float(v) for k, v in zip(keys, out)}
+        d["tree_on_device"] = bool(int(out[9]) & 1)
+        d["lists_on_device"] = bool(int(out[9]) & 2)
+        return d
 
     def poly_roots(self):
         """Roots of the near-field polynomial preconditioner (preconditioner="near_poly") formed by

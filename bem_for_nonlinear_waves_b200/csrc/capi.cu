@@ -595,6 +595,16 @@ static int build_poly(bem_gpu_ctx* ctx) {
   return BEM_OK;
 }
 
+int bem_gpu_setup_phases(bem_gpu_ctx* ctx, double* out) {
+  if (!ctx || !out) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  for (int k = 0; k < 7; ++k) out[k] = ctx->plan.phase_s[k];
+  out[7] = ctx->time_upload;
+  out[8] = 1e-3 * ctx->setup_dev_ms;
+  out[9] = (ctx->plan.tree_on_device ? 1 : 0) + (ctx->plan.lists_on_device ? 2 : 0);
+  return BEM_OK;
+}
+
 int bem_gpu_poly_roots(bem_gpu_ctx* ctx, int32_t cap, double* re, double* im) {
   if (!ctx || cap < 0 || (cap > 0 && (!re || !im))) return BEM_ERR_INVALID_ARGUMENT;
   if (!ctx->ready) return BEM_ERR_NOT_READY;

@@ -357,8 +357,11 @@ def main():
             w2 = time.perf_counter()
             e2e_s += w2 - w0
             st = bvp.stats
+            ph = bvp.setup_phases()
             steps_detail.append({"setup_wall_ms": 1e3 * (w1 - w0), "solve_wall_ms": 1e3 * (w2 - w1),
-                                 "device_ms": 1e3 * st.time_device_s, "setup_device_ms": 1e3 * st.time_setup_device_s})
+                                 "device_ms": 1e3 * st.time_device_s, "setup_device_ms": 1e3 * st.time_setup_device_s,
+                                 "setup_parts_ms": {k: round(1e3 * v, 2) for k, v in ph.items() if isinstance(v, float)},
+                                 "tree_and_lists_on_device": ph["tree_on_device"] and ph["lists_on_device"]})
             dev_s += st.time_device_s
             plan_s += st.time_plan_s
             upload_s += st.time_upload_s

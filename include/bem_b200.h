@@ -283,6 +283,12 @@ int bem_gpu_check_device_status(bem_gpu_ctx* ctx);
  * bem_harmonic_ritz_values: host helper -- harmonic Ritz values of a (k+1) x k Arnoldi
  *   Hessenberg matrix (row-major, leading dimension ldh, k <= 32); 0 or -1. */
 int bem_gpu_poly_roots(bem_gpu_ctx* ctx, int32_t cap, double* re, double* im);
+
+/* Set-up time by part (seconds) of the last set-up: [0] element sources, [1] octree, [2] lists,
+ * [3] element order and node arrays, [4] M2L grouping, [5] near-field blocks, [6] DOF incidence
+ * (host plan), [7] uploads, [8] device set-up; [9] = 1 if the octree was grown on the device
+ * + 2 if the lists were built there. */
+int bem_gpu_setup_phases(bem_gpu_ctx* ctx, double* out /*[10]*/);
 int bem_harmonic_ritz_values(int32_t k, const double* H, int32_t ldh, double* re, double* im);
 
 /* FP64 FMA throughput of the device (TFLOP/s), measured by a short probe kernel. */
