@@ -108,7 +108,7 @@ struct bem_gpu_ctx {
   bem_gpu_opts opts{};
   cudaStream_t stream = nullptr;
   std::string err;
-  Plan plan;
+  Plan plan, plan_spare;
   bool ready = false;
   double time_setup = 0.0;
 
@@ -647,21 +647,28 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     if (!ctx->dtree) ctx->dtree = dtree_create(ctx->stream);
     po.device_tree = ctx->dtree;
   }
-  {
-    Plan fresh;
-    if (!build_plan(fresh, po, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face,
-                    d->dof_kind, d->face_dof, refresh && had_plan ? &ctx->plan : nullptr)) {
-      ctx->err = fresh.error;
-      return BEM_ERR_INVALID_ARGUMENT;
-    }
-    ctx->plan = std::move(fresh);
+  // built into the spare plan (the one before the current: its arrays' memory is reused), then
+  // swapped in; the current plan is the refresh's previous plan
+  if (!build_plan(ctx->plan_spare, po, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face,
+                  d->dof_kind, d->face_dof, refresh && had_plan ? &ctx->plan : nullptr)) {
+    ctx->err = ctx->plan_spare.error;
+    return BEM_ERR_INVALID_ARGUMENT;
   }
+  std::swap(ctx->plan, ctx->plan_spare);
   ctx->time_plan = now_s() - t0;
   Plan& P = ctx->plan;
   // a refresh that kept the tree and lists (reuse) and the L2P targets (reuse_near) skips the
   // uploads of what it kept: the buffers still hold the same data
   const bool reuse = P.reused_m2l, reuse_near = P.reused_near;
-  CK(ctx->stage.begin(ctx->stage_bytes, ctx->stream));
+  {  // pinned area for this set-up's uploads: the previous set-up's total, or an estimate from the
+     // plan's array sizes for the first one (pinning a larger area later is slow)
+    const size_t ne = (size_t)P.nf, pairs = (size_t)P.m2l_pairs;
+    const size_t est = ne * (18 + 6 + 3 + 8) * 8 + ne * 3 * 4 * 4 + (size_t)P.np * 3 * 8 + P.nb_dofs.size() * 4 +
+                       pairs * 4 * (ctx->opts.precision == 1 ? 4 : 2) + P.chunk_grp.size() * 12 + P.dof_inc.size() * 4 +
+                       P.blocks.size() * sizeof(NearBlockDev) + P.nb_targets.size() * 8 + P.nb_ranges.size() * 4 +
+                       (size_t)P.ndof * 16 + (size_t)P.np * 12 + P.nodes.size() * 64 + (size_t)(4 << 20);
+    CK(ctx->stage.begin(std::max(ctx->stage_bytes, reuse ? 0 : est), ctx->stream));
+  }
   auto ups = [&](auto& buf, const auto& v) -> cudaError_t { return reuse ? cudaSuccess : up(ctx, buf, v); };
   auto upn = [&](auto& buf, const auto& v) -> cudaError_t { return reuse_near ? cudaSuccess : up(ctx, buf, v); };
   cudaStream_t s = ctx->stream;

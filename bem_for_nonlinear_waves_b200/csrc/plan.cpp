@@ -12,6 +12,7 @@
 #include <functional>
 #include <chrono>
 #include <numeric>
+#include <omp.h>
 
 namespace bemb200 {
 namespace {
@@ -286,6 +287,82 @@ bool grow_on_device(TreeBuilder& T, DeviceTree* dt, int nf, const std::vector<V3
   return true;
 }
 
+// Sorts the packed M2L pair keys (offset key << 33 | level << 29 | slot; bit 63 for a pair off
+// the lattice).  The slots are unique and the keys arrive in slot order, so the sorted order is
+// a stable sort by the part above the slot: a counting sort over a dense table of lattice
+// offsets |r| <= 31 and levels, with the off-lattice pairs last.  Falls back to a comparison
+// sort for larger offsets.
+void sort_pair_keys(std::vector<uint64_t>& keyed) {
+  constexpr int R = 31, W = 2 * R + 1;
+  constexpr int64_t kOff = (int64_t)W * W * W * 16;  // dense bucket index; kOff = off the lattice
+  const int64_t n = (int64_t)keyed.size();
+  std::vector<int32_t> bucket(n);
+  bool dense = true;
+#pragma omp parallel for schedule(static) reduction(&& : dense)
+  for (int64_t k = 0; k < n; ++k) {
+    const uint64_t v = keyed[k];
+    if (v >> 63) {
+      bucket[k] = (int32_t)kOff;
+      continue;
+    }
+    const int lev = (int)((v >> 29) & 15);
+    const uint64_t rk = v >> 33;
+    const int r0 = (int)((rk >> 20) & 1023) - 512, r1 = (int)((rk >> 10) & 1023) - 512, r2 = (int)(rk & 1023) - 512;
+    if (std::abs(r0) > R || std::abs(r1) > R || std::abs(r2) > R) {
+      dense = false;
+      bucket[k] = 0;
+      continue;
+    }
+    bucket[k] = (int32_t)((((int64_t)(r0 + R) * W + (r1 + R)) * W + (r2 + R)) * 16 + lev);
+  }
+  if (!dense || n < 4096) {
+    __gnu_parallel::sort(keyed.begin(), keyed.end());
+    return;
+  }
+  // ranks of the used buckets, in bucket order: a bitmap of the used ones and per-word prefix
+  // counts (rank = used buckets before b)
+  const int64_t nw = kOff / 64 + 1;
+  std::vector<uint64_t> used(nw, 0);
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < n; ++k) {
+    const int64_t b = bucket[k];
+    const uint64_t bit = uint64_t(1) << (b & 63);
+    if (!(used[b >> 6] & bit)) __atomic_fetch_or(&used[b >> 6], bit, __ATOMIC_RELAXED);
+  }
+  std::vector<int32_t> wpre(nw + 1, 0);
+  for (int64_t w = 0; w < nw; ++w) wpre[w + 1] = wpre[w] + __builtin_popcountll(used[w]);
+  const int32_t nr = wpre[nw];
+  auto rank_of = [&](int64_t b) {
+    const uint64_t below = used[b >> 6] & ((uint64_t(1) << (b & 63)) - 1);
+    return wpre[b >> 6] + __builtin_popcountll(below);
+  };
+  std::vector<int32_t> rank(n);
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < n; ++k) rank[k] = rank_of(bucket[k]);
+  // stable scatter: histograms over contiguous slot ranges (slices), prefix in (rank, slice) order
+  const int ns = std::max(1, std::min(omp_get_max_threads(), 64));
+  std::vector<int64_t> hist((size_t)ns * nr, 0);
+#pragma omp parallel for schedule(static)
+  for (int t = 0; t < ns; ++t) {
+    int64_t* h = &hist[(size_t)t * nr];
+    for (int64_t k = n * t / ns, e = n * (t + 1) / ns; k < e; ++k) ++h[rank[k]];
+  }
+  int64_t run = 0;
+  for (int32_t r = 0; r < nr; ++r)
+    for (int t = 0; t < ns; ++t) {
+      const int64_t c = hist[(size_t)t * nr + r];
+      hist[(size_t)t * nr + r] = run;
+      run += c;
+    }
+  std::vector<uint64_t> out(n);
+#pragma omp parallel for schedule(static)
+  for (int t = 0; t < ns; ++t) {
+    int64_t* h = &hist[(size_t)t * nr];
+    for (int64_t k = n * t / ns, e = n * (t + 1) / ns; k < e; ++k) out[h[rank[k]]++] = keyed[k];
+  }
+  keyed.swap(out);
+}
+
 bool is_far(const PlanOptions& o, const Bucket& A, const Bucket& Bk) {  // moments.hpp:950-956
   const double eff = std::max(A.dL + 2.0 * A.off, Bk.dL + 2.0 * Bk.off);
   const V3 d{Bk.X[0] - A.X[0], Bk.X[1] - A.X[1], Bk.X[2] - A.X[2]};
@@ -437,7 +514,16 @@ static bool same_tree(const Plan& a, const Plan& b) {
 
 bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int ndof,
                 const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof, Plan* prev) {
-  P = Plan();
+  {  // start from an empty plan that keeps the capacity of P's arrays: a plan of similar size
+     // then reuses memory whose pages are already mapped
+    Plan fresh;
+#define BEMB200_KEEP(v) \
+  fresh.v.swap(P.v);    \
+  fresh.v.clear();
+    BEMB200_PLAN_ARRAYS(BEMB200_KEEP)
+#undef BEMB200_KEEP
+    P = std::move(fresh);
+  }
   P.opt = opt;
   auto clk = std::chrono::steady_clock::now();
   auto lap = [&](int k) {
@@ -800,20 +886,27 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
       for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) pair_tgt[k] = t;
     std::vector<uint64_t>& keyed = P.m2l_key_sorted;
     keyed.resize(npair);
+    std::vector<double> bx(4 * (size_t)nb);  // bucket centre and size, packed (the pair loop reads them at random)
+    for (int i = 0; i < nb; ++i) {
+      for (int a = 0; a < 3; ++a) bx[4 * (size_t)i + a] = B[i].X[a];
+      bx[4 * (size_t)i + 3] = B[i].dL;
+    }
 #pragma omp parallel for schedule(static)
     for (int64_t k = 0; k < npair; ++k) {
       const int t = pair_tgt[k], s = P.m2l_src[k];
-      bool lattice = std::abs(B[s].dL - B[t].dL) <= 1e-12 * B[t].dL;
+      const double* xt = &bx[4 * (size_t)t];
+      const double* xs = &bx[4 * (size_t)s];
+      bool lattice = std::abs(xs[3] - xt[3]) <= 1e-12 * xt[3];
       long long r[3];
       for (int a = 0; a < 3; ++a) {
-        const double q = (B[t].X[a] - B[s].X[a]) / B[t].dL;
+        const double q = (xt[a] - xs[a]) / xt[3];
         r[a] = std::llround(q);
         if (std::abs(q - (double)r[a]) > 1e-9 || std::abs(r[a]) > 500) lattice = false;
       }
       const uint64_t rkey = (uint64_t)(((r[0] + 512) << 20) | ((r[1] + 512) << 10) | (r[2] + 512));
-      keyed[k] = lattice ? ((((rkey << 4) | (uint64_t)B[t].level) << 29) | (uint64_t)k) : ((uint64_t(1) << 63) | (uint64_t)k);
+      keyed[k] = lattice ? ((((rkey << 4) | (uint64_t)P.nodes[t].level) << 29) | (uint64_t)k) : ((uint64_t(1) << 63) | (uint64_t)k);
     }
-    __gnu_parallel::sort(keyed.begin(), keyed.end());
+    sort_pair_keys(keyed);
     P.grp_vec.clear();
     P.grp_off.assign(1, 0);
     P.grp_pair.resize(npair);
