@@ -657,6 +657,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   std::swap(ctx->plan, ctx->plan_spare);
   ctx->time_plan = now_s() - t0;
   Plan& P = ctx->plan;
+  ctx->launches += P.device_launches;  // octree and list kernels of the plan
   // a refresh that kept the tree and lists (reuse) and the L2P targets (reuse_near) skips the
   // uploads of what it kept: the buffers still hold the same data
   const bool reuse = P.reused_m2l, reuse_near = P.reused_near;

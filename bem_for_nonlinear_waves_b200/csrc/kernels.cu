@@ -14,6 +14,8 @@
 //                   BEM_solveBVP_GMRES_FMM.hpp:1824-1891)
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
@@ -1380,6 +1382,14 @@ void launch_axpby(int n, double a, const double* x, double b, double* y, cudaStr
   int g = (n + 255) / 256;
   if (g > 1184) g = 1184;
   k_axpby<<<g > 0 ? g : 1, 256, 0, st>>>(n, a, x, b, y);
+}
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("BEMB200_NO_PDL");
+    return !(v && v[0] && v[0] != '0');
+  }();
+  return on;
 }
 
 // y[i] in [-0.5, 0.5): a fixed pseudo-random vector (splitmix64 of seed + i)

@@ -718,6 +718,7 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
       lists_done = true;
       P.lists_on_device = true;
     }
+    P.device_launches = dtree_take_launches(static_cast<DeviceTree*>(opt.device_tree));
   }
   if (!lists_done) {
     constexpr int kSplit = 2;

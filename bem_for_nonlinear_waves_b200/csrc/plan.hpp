@@ -124,6 +124,7 @@ struct Plan {
   bool reused_m2l = false, reused_near = false;
   bool tree_on_device = false;   // the octree was grown on the device
   bool lists_on_device = false;  // and the interaction lists built there
+  int device_launches = 0;       // kernels those two launched (during the host plan)
 
   std::string error;
 };

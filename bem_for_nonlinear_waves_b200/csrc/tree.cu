@@ -237,6 +237,7 @@ struct DeviceTree {
   Buf<double> nX, ndL, noff;                              // interaction lists: node geometry
   Buf<int> ncb, nce, nch, lt, lco, lc, lcnt, loff, lno, lmo, lxo;  // and per-level work arrays
   size_t cur = 0, cur_n = 0;  // current level: offset into elems, length
+  int launches = 0;
   std::vector<int> h_beg, h_end;
 };
 
@@ -277,6 +278,7 @@ bool dtree_count(DeviceTree* t, int n, const int* seg_beg, const int* seg_end, c
       cudaMemcpyAsync(t->geo.p, geo, sizeof(double) * kGeo * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
     return false;
   // tags are indexed by position in the elems buffer relative to the current level
+  ++t->launches;
   k_tree_count<<<n, 256, 0, s>>>(t->seg_beg.p, t->seg_end.p, t->geo.p, t->elems.p, t->poles.p, (int)t->cur, t->tag.p, t->cnt.p,
                                  t->cnt.p + 8 * n);
   if (cudaGetLastError() != cudaSuccess) return false;
@@ -297,6 +299,7 @@ bool dtree_scatter(DeviceTree* t, int n, const int* off, int total) {
       v += (int)next;
     }
     if (cudaMemcpyAsync(t->off.p, o.data(), sizeof(int) * 8 * n, cudaMemcpyHostToDevice, s) != cudaSuccess) return false;
+    ++t->launches;
     k_tree_scatter<<<n, 256, 0, s>>>(t->seg_beg.p, t->seg_end.p, t->elems.p, (int)t->cur, t->tag.p, t->off.p, t->elems.p);
     if (cudaGetLastError() != cudaSuccess) return false;
     if (cudaStreamSynchronize(s) != cudaSuccess) return false;  // o is freed on return
@@ -345,6 +348,7 @@ bool dtree_lists(DeviceTree* t, int nb, const double* X, const double* dL, const
       return false;
     const int blocks = (n + 3) / 4;  // 4 warps per block
     int* cnt = t->lcnt.p;
+    t->launches += 2;
     k_lists<false><<<blocks, 128, 0, s>>>(n, t->lt.p, t->lco.p, t->lc.p, g, theta, cnt, cnt + n, cnt + 9 * n, nullptr, nullptr, nullptr,
                                           nullptr, nullptr, nullptr);
     if (cudaGetLastError() != cudaSuccess) return false;
@@ -393,6 +397,12 @@ bool dtree_lists(DeviceTree* t, int nb, const double* X, const double* dL, const
     cd.swap(ncd);
   }
   return true;
+}
+
+int dtree_take_launches(DeviceTree* t) {
+  const int n = t ? t->launches : 0;
+  if (t) t->launches = 0;
+  return n;
 }
 
 bool dtree_download(DeviceTree* t, int* out, size_t count) {

@@ -23,6 +23,8 @@ bool dtree_scatter(DeviceTree* t, int n, const int* off, int total);
 bool dtree_lists(DeviceTree* t, int nb, const double* X, const double* dL, const double* off, const int* cb, const int* ce,
                  const int* children, int n_children, double theta, std::vector<std::vector<int>>& near,
                  std::vector<std::vector<int>>& m2l);
+// kernels launched since the last call (octree growth and lists)
+int dtree_take_launches(DeviceTree* t);
 // every level's array, back to back from the root's
 bool dtree_download(DeviceTree* t, int* out, size_t count);
 
