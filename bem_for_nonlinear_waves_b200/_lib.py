@@ -29,7 +29,8 @@ STATUS = {0: "ok", -1: "invalid argument", -2: "out of memory", -3: "not converg
 class Opts(ctypes.Structure):
     _fields_ = [("expansion_order", c_int), ("mac_theta", c_dbl), ("leaf_max_elements", c_int), ("max_level", c_int),
                 ("tol", c_dbl), ("max_iter", c_int), ("device", c_int), ("tol_relative", c_int), ("preconditioner", c_int),
-                ("precision", c_int), ("poly_degree", c_int), ("tree_on_host", c_int)]
+                ("precision", c_int), ("poly_degree", c_int), ("tree_on_host", c_int),
+                ("tc_item_pairs", c_int), ("reserved", c_int)]
 
 
 class MelSurface(ctypes.Structure):
@@ -77,6 +78,7 @@ EXPORTS = {
     "bem_gpu_fp64_peak_tflops": (c_dbl, [c_int]),
     "bem_gpu_poly_roots": (c_int, [ctypes.c_void_p, c_int, P_dbl, P_dbl]),
     "bem_gpu_setup_phases": (c_int, [ctypes.c_void_p, P_dbl]),
+    "bem_gpu_tc_tuning": (c_int, [ctypes.c_void_p, P_int, P_int, P_dbl]),
     "bem_harmonic_ritz_values": (c_int, [c_int, P_dbl, c_int, P_dbl, P_dbl]),
     "bem_plan_inspect": (c_int, [ctypes.POINTER(Opts), ctypes.POINTER(Desc), P_int, P_dbl, P_i64]),
     "bem_plan_refresh_inspect": (c_int, [ctypes.POINTER(Opts), ctypes.POINTER(Desc), ctypes.POINTER(Desc), P_i64]),

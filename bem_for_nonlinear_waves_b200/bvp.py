@@ -40,7 +40,7 @@ def build_dofs(X, tri, face_dirichlet):
 
 
 def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter, device,
-               tol_relative, preconditioner, precision, poly_degree=8, tree_on_device=True):
+               tol_relative, preconditioner, precision, poly_degree=8, tree_on_device=True, tc_item_pairs=0):
     o = L.Opts()
     lib.bem_gpu_default_opts(ctypes.byref(o))
     o.expansion_order = int(expansion_order)
@@ -54,6 +54,7 @@ def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_l
     o.preconditioner = {"none": 0, "jacobi": 1, "near_poly": 2}[preconditioner]
     o.poly_degree = int(poly_degree)
     o.tree_on_host = 0 if tree_on_device else 1
+    o.tc_item_pairs = int(tc_item_pairs)
     o.precision = {"fp64": 0, "mixed": 1}[precision]
     return o
 
@@ -63,7 +64,7 @@ class BEM_BVP:
 
     def __init__(self, X, tri, face_dirichlet, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30,
                  fmm_max_level=7, solver_tol=1e-9, solver_max_iter=500, device=0, dofs=None, tol_relative=False, preconditioner="none",
-                 precision="fp64", poly_degree=8, tree_on_device=True):
+                 precision="fp64", poly_degree=8, tree_on_device=True, tc_item_pairs=0):
         self.lib = L.load()
         if not self.lib.bem_gpu_is_available():
             raise RuntimeError("no sm_100 CUDA device visible: the GMRES-FMM solver runs only on the GPU")
@@ -71,7 +72,7 @@ class BEM_BVP:
         self.tri = np.ascontiguousarray(tri, np.int32)
         self.face_dirichlet = np.ascontiguousarray(face_dirichlet, np.uint8)
         o = _make_opts(self.lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter,
-                       device, tol_relative, preconditioner, precision, poly_degree, tree_on_device)
+                       device, tol_relative, preconditioner, precision, poly_degree, tree_on_device, tc_item_pairs)
         self.opts = o
         self.ctx = self.lib.bem_gpu_create(ctypes.byref(o))
         if not self.ctx:
@@ -178,6 +179,16 @@ class BEM_BVP:
         self._check(self.lib.bem_gpu_point_integrals(self.ctx, L.ptr(phi, L.P_dbl), L.ptr(phin, L.P_dbl), L.ptr(a, L.P_dbl),
                                                      L.ptr(b, L.P_dbl)), "point_integrals")
         return a, b
+
+    def tc_tuning(self):
+        """Tensor-core M2L work-item size in use and the autotuner's candidate timings (ms)."""
+        used = ctypes.c_int(0)
+        cand = np.zeros(4, np.int32)
+        ms = np.zeros(4)
+        rc = self.lib.bem_gpu_tc_tuning(self.ctx, ctypes.byref(used), L.ptr(cand, L.P_int), L.ptr(ms, L.P_dbl))
+        self._check(min(rc, 0), "bem_gpu_tc_tuning")
+        return {"pairs_per_item": int(used.value), "tuned_in_this_setup": bool(rc == 1),
+                "candidates_ms": {int(c): round(float(m), 4) for c, m in zip(cand, ms)}}
 
     def setup_phases(self):
         """Seconds spent in each part of the last set-up (host plan phases, uploads, device part)."""

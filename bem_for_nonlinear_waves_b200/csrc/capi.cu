@@ -8,7 +8,9 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -102,6 +104,11 @@ double now_s() { return std::chrono::duration<double>(std::chrono::steady_clock:
 
 constexpr int kErrRing = 8;  // residual estimates in flight (>= the read-back lag + 1)
 constexpr int kMaxPolyDegree = 24;
+// pairs per tensor-core work item tried by the autotuner: orders <= 10 have a kernel variant for
+// items of up to 128 pairs (one table slot in shared memory), higher orders up to 80
+constexpr int kTuneCandWide[4] = {64, 80, 112, 128};
+constexpr int kTuneCandNarrow[4] = {32, 48, 64, 80};
+inline const int* tune_cand(int p) { return p <= 10 ? kTuneCandWide : kTuneCandNarrow; }
 inline int poly_degree(const bem_gpu_opts& o) { return o.poly_degree > 0 ? o.poly_degree : 8; }
 
 struct bem_gpu_ctx {
@@ -152,6 +159,9 @@ struct bem_gpu_ctx {
   DBuf<float> tc_escale;
   DBuf<unsigned int> tc_max;
   int tc_grid = 148;
+  int tc_tune = 0;                 // pairs per tensor-core work item in use
+  bool tc_tuned_here = false;      // this set-up ran the tuning
+  float tc_tune_ms[4] = {0, 0, 0, 0};
   std::vector<unsigned char> tc_map;  // TMA tensor map over tc_Mt (host copy, passed by value)
   cudaGraph_t graph_lo = nullptr;
   cudaGraphExec_t graph_exec_lo = nullptr;
@@ -281,6 +291,7 @@ struct bem_gpu_ctx {
     a.tc_item_cnt = tc_item_cnt.p;
     a.tc_pos = tc_pos.p;
     a.n_tc_pairs = (int)plan.tc_pair.size();
+    a.tc_item_pairs = tc_tune > 0 ? tc_tune : 80;
     a.tc_src = tc_src.p;
     a.tc_tab = tc_T.p;
     a.tc_Mt = tc_Mt.p;
@@ -595,6 +606,17 @@ static int build_poly(bem_gpu_ctx* ctx) {
   return BEM_OK;
 }
 
+int bem_gpu_tc_tuning(bem_gpu_ctx* ctx, int32_t* pairs_in_use, int32_t* candidates, double* ms) {
+  if (!ctx || !pairs_in_use || !candidates || !ms) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  *pairs_in_use = ctx->mixed ? ctx->tc_tune : 0;
+  for (int c = 0; c < 4; ++c) {
+    candidates[c] = tune_cand(ctx->plan.opt.p)[c];
+    ms[c] = ctx->tc_tune_ms[c];
+  }
+  return ctx->tc_tuned_here ? 1 : 0;
+}
+
 int bem_gpu_setup_phases(bem_gpu_ctx* ctx, double* out) {
   if (!ctx || !out) return BEM_ERR_INVALID_ARGUMENT;
   if (!ctx->ready) return BEM_ERR_NOT_READY;
@@ -618,6 +640,95 @@ int bem_gpu_poly_roots(bem_gpu_ctx* ctx, int32_t cap, double* re, double* im) {
 // Set-up of a BVP (refresh: same mesh as the last set-up at new coordinates; see
 // bem_gpu_setup_refresh).  With an unchanged structure only the geometry-dependent arrays are
 // uploaded and only the geometry-dependent device tables rebuilt.
+// Work items of the tensor-core M2L over table images: every item once per row tile, the row
+// tiles of a table consecutive (image = table * tiles + tile), so each image is loaded once
+// per CTA range.
+static cudaError_t upload_tc_items(bem_gpu_ctx* ctx, bool skip) {
+  const Plan& P = ctx->plan;
+  const int rt = tc_row_tiles(P.opt.p);
+  std::vector<int> itab, ibeg, icnt;
+  const size_t ni = P.tc_item_tab.size();
+  for (size_t i0 = 0; i0 < ni;) {
+    size_t i1 = i0;
+    while (i1 < ni && P.tc_item_tab[i1] == P.tc_item_tab[i0]) ++i1;
+    for (int r = 0; r < rt; ++r)
+      for (size_t i = i0; i < i1; ++i) {
+        itab.push_back(P.tc_item_tab[i] * rt + r);
+        ibeg.push_back(P.tc_item_begin[i]);
+        icnt.push_back(P.tc_item_cnt[i]);
+      }
+    i0 = i1;
+  }
+  ctx->n_tc_items = (int)itab.size();
+  if (skip) return cudaSuccess;
+  cudaError_t e;
+  if ((e = up(ctx, ctx->tc_item_tab, itab)) != cudaSuccess || (e = up(ctx, ctx->tc_item_begin, ibeg)) != cudaSuccess) return e;
+  return up(ctx, ctx->tc_item_cnt, icnt);
+}
+
+// Autotuning of the tensor-core M2L work-item size (pairs per item = the MMA's N, 16..80):
+// each candidate's items are timed on the contraction kernel alone (CUDA events, after a
+// warm-up launch), once per process for each device, expansion order and problem-size class
+// (powers of two of the pair count); the best is cached.  The item size changes which CTA
+// computes a pair, not the pair's arithmetic: the M2L result is the same bit for bit.
+struct TuneEntry {
+  int best = 0;
+  float ms[4] = {0, 0, 0, 0};
+};
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int>, TuneEntry> g_tune;
+
+static std::tuple<int, int, int> tune_key(const bem_gpu_ctx* ctx) {
+  int lg = 0;
+  for (int64_t n = ctx->plan.m2l_pairs; n > 1; n >>= 1) ++lg;
+  return {ctx->opts.device, ctx->plan.opt.p, lg};
+}
+
+static int tune_tc_items(bem_gpu_ctx* ctx) {
+  cudaStream_t s = ctx->stream;
+  const int p = ctx->plan.opt.p;
+  MatvecArgs a = ctx->args(ctx->phi.p, ctx->phin.p, ctx->mv_out.p, nullptr, nullptr);
+  ctx->set_ax(a, true);
+  ctx->set_tc(a);
+  launch_m2l_tc(p, a, s, TC_EXPAND, 1);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  TuneEntry t;
+  float best = 1e30f;
+  const int* cand = tune_cand(p);
+  for (int c = 0; c < 4; ++c) {
+    retile_tc_items(ctx->plan, cand[c]);
+    ctx->tc_tune = cand[c];
+    CK(upload_tc_items(ctx, false));
+    ctx->set_tc(a);
+    launch_m2l_tc(p, a, s, TC_CONTRACT, 1);
+    CK(cudaEventRecord(e0, s));
+    for (int r = 0; r < 5; ++r) launch_m2l_tc(p, a, s, TC_CONTRACT, 1);
+    CK(cudaEventRecord(e1, s));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    t.ms[c] = ms / 5;
+    if (t.ms[c] < best) {
+      best = t.ms[c];
+      t.best = cand[c];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  retile_tc_items(ctx->plan, t.best);
+  CK(upload_tc_items(ctx, false));
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[tune_key(ctx)] = t;
+  }
+  ctx->tc_tune = t.best;
+  ctx->tc_tuned_here = true;
+  for (int c = 0; c < 4; ++c) ctx->tc_tune_ms[c] = t.ms[c];
+  return BEM_OK;
+}
+
 static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   if (!ctx || !d) return BEM_ERR_INVALID_ARGUMENT;
   CK(cudaSetDevice(ctx->opts.device));
@@ -631,6 +742,10 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   }
   if (ctx->opts.precision != 0 && ctx->opts.precision != 1) {
     ctx->err = "precision must be 0 (fp64) or 1 (mixed)";
+    return BEM_ERR_INVALID_ARGUMENT;
+  }
+  if (ctx->opts.tc_item_pairs < 0 || ctx->opts.tc_item_pairs > tc_max_pairs(ctx->opts.expansion_order)) {
+    ctx->err = "tc_item_pairs must be 0 (autotuned) or 1..128 (p <= 10), 1..80 (p 11, 12)";
     return BEM_ERR_INVALID_ARGUMENT;
   }
   if (ctx->opts.preconditioner < 0 || ctx->opts.preconditioner > 2 || ctx->opts.poly_degree < 0 ||
@@ -829,32 +944,27 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   ctx->mixed = ctx->opts.precision == 1;
   if (ctx->mixed) {  // tensor-core M2L: translation tables, multipole rows, work items
     const int p = P.opt.p, kp = tc_kp(p);
-    if (!reuse) build_tc_groups(P, tc_max_pairs());
+    if (!reuse) {  // item size: forced, tuned earlier for this class, or the kernel's maximum until tuned
+      int mp = 80;
+      ctx->tc_tuned_here = false;
+      if (ctx->opts.tc_item_pairs > 0) {
+        mp = std::min(ctx->opts.tc_item_pairs, tc_max_pairs(P.opt.p));
+      } else {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(tune_key(ctx));
+        if (it != g_tune.end()) {
+          mp = it->second.best;
+          for (int c = 0; c < 4; ++c) ctx->tc_tune_ms[c] = it->second.ms[c];
+        }
+      }
+      ctx->tc_tune = mp;
+      build_tc_groups(P, mp);
+    }
     const int ntab = (int)(P.tc_tab.size() / 4);
     std::vector<double> dl(nb), al(kp);
     for (int i = 0; i < nb; ++i) dl[i] = P.nodes[i].dL;
     tc_alpha_host(p, al.data());
-    {  // work items over table images: every item once per row tile, row tiles of a table
-       // consecutive (image = table * tiles + tile), so each image is loaded once per CTA range
-      const int rt = tc_row_tiles(p);
-      std::vector<int> itab, ibeg, icnt;
-      const size_t ni = P.tc_item_tab.size();
-      for (size_t i0 = 0; i0 < ni;) {
-        size_t i1 = i0;
-        while (i1 < ni && P.tc_item_tab[i1] == P.tc_item_tab[i0]) ++i1;
-        for (int r = 0; r < rt; ++r)
-          for (size_t i = i0; i < i1; ++i) {
-            itab.push_back(P.tc_item_tab[i] * rt + r);
-            ibeg.push_back(P.tc_item_begin[i]);
-            icnt.push_back(P.tc_item_cnt[i]);
-          }
-        i0 = i1;
-      }
-      ctx->n_tc_items = (int)itab.size();
-      CK(ups(ctx->tc_item_tab, itab));
-      CK(ups(ctx->tc_item_begin, ibeg));
-      CK(ups(ctx->tc_item_cnt, icnt));
-    }
+    CK(upload_tc_items(ctx, reuse));
     {  // work-item order j -> source bucket; pair slot k -> its position j (the row of its partial)
       std::vector<int> src(P.tc_pair.size()), pos(P.tc_pair.size());
       for (size_t j = 0; j < src.size(); ++j) {
@@ -1033,6 +1143,17 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     if (!(mx < 1024.f)) {
       ctx->err = "mixed precision: translation table entry " + std::to_string(mx) + " too large for FP16 operands";
       return BEM_ERR_UNSUPPORTED;
+    }
+  }
+  if (ctx->mixed && !reuse && ctx->opts.tc_item_pairs <= 0) {
+    bool known;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      known = g_tune.count(tune_key(ctx)) > 0;
+    }
+    if (!known) {  // once per process and problem class, after the device-time window
+      const int trc = tune_tc_items(ctx);
+      if (trc != BEM_OK) return trc;
     }
   }
   int rc = build_graph(ctx);
@@ -1241,7 +1362,7 @@ int bem_plan_refresh_inspect(const bem_gpu_opts* opts, const bem_bvp_desc* d0, c
     if (!build_plan(P, o, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face, d->dof_kind,
                     d->face_dof, prev))
       return false;
-    if (!P.reused_m2l) build_tc_groups(P, tc_max_pairs());
+    if (!P.reused_m2l) build_tc_groups(P, 80);
     return true;
   };
   Plan a0, b0, a1, b1;

@@ -96,6 +96,7 @@ struct MatvecArgs {
   const int* tc_item_begin = nullptr;
   const int* tc_item_cnt = nullptr;
   int n_tc_pairs = 0;
+  int tc_item_pairs = 80;  // largest item (selects the tensor-core kernel variant)
   const int* tc_pos = nullptr;   // [pairs] position of pair slot k in work-item order
   const int* tc_src = nullptr;   // [pairs] source bucket, in work-item order
   const void* tc_tab = nullptr;  // FP16 hi/lo table images
@@ -180,7 +181,7 @@ int tc_make_rows_map(void* map_out, void* Mt, int nrows, int p);
 size_t tc_table_bytes(int p);       // bytes of one table image (hi + lo, one row tile of 128 outputs)
 int tc_row_tiles(int p);            // table images per translation (1 for p <= 10, 2 for p = 11, 12)
 int tc_kpo(int p);                  // floats per pair partial
-int tc_max_pairs();                 // pairs per work item
+int tc_max_pairs(int p);            // largest pairs per work item at order p
 void tc_alpha_host(int p, double* alpha /*[tc_kp(p)]*/);
 void launch_tc_tables(int p, int ntab, const double* tab, const double* alpha, void* T, unsigned int* maxbits, cudaStream_t st);
 constexpr int TC_EXPAND = 1, TC_CONTRACT = 2, TC_REDUCE = 4, TC_ALL = 7;

@@ -49,11 +49,13 @@ namespace bemb200 {
 namespace {
 
 constexpr int kRows = 128;          // table rows = MMA N: output coefficients (NR <= 128, p <= 10)
-constexpr int kMaxPairs = 80;       // pairs per work item = gathered rows (one per pair)
-constexpr int kMaxCols = kMaxPairs;
+// pairs per work item = gathered rows (one per pair) = MMA N: at most 80 with two table slots
+// in shared memory, at most 128 with one (p <= 10; the kernel variant is chosen per launch)
+constexpr int kMaxPairs = 80;
+constexpr int kMaxPairsWide = 128;
 constexpr uint32_t kWaitTries = 1u << 22;
 
-template <int P>
+template <int P, int MC = kMaxPairs>
 struct TcDims {
   static constexpr int NR = (P + 1) * (P + 1);
   static constexpr int KP = (NR + 63) / 64 * 64;  // K padded to whole 128-byte swizzle atoms
@@ -63,7 +65,7 @@ struct TcDims {
   // the reduction reads an even number of floats at an 8-byte aligned offset)
   static constexpr int KPO = KP;
   static constexpr int TAB_BYTES = 2 * kRows * KP * 2;    // hi + lo images of one row tile of a table
-  static constexpr int REGION = kMaxCols * 128;           // one (part, atom) region of gathered rows
+  static constexpr int REGION = MC * 128;                 // one (part, atom) region of gathered rows
   static constexpr int B_BYTES = 2 * KA * REGION;         // hi + lo gathered rows
   // two table slots when they fit beside two stages of gathered rows (one slot for the
   // 96 KB images of p = 11, 12), plus 1 KB to align them to the 1024-byte swizzle atom; at
@@ -235,22 +237,22 @@ constexpr int kIssuer = 32;
 constexpr int kStages = 2;
 constexpr int kAcc = 4;
 constexpr int kAccCols = 128;
-static_assert(kMaxCols <= kAccCols, "one accumulator holds an item");
-static_assert(kMaxCols <= kProducers, "one producer thread per gathered row");
+static_assert(kMaxPairsWide <= kAccCols, "one accumulator holds an item");
+static_assert(kMaxPairsWide <= kProducers, "one producer thread per gathered row");
 
-template <int P>
+template <int P, int MC>
 __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
     k_m2l_tc(const __grid_constant__ CUtensorMap rows_map, int nitems, const int* __restrict__ item_tab, const int* __restrict__ item_begin,
              const int* __restrict__ item_cnt, int npairs, const int* __restrict__ tc_src, const __half* __restrict__ Ttab,
              const __half* __restrict__ Mt, float* __restrict__ Y, int* __restrict__ err) {
   pdl_enter();
-  using D = TcDims<P>;
+  using D = TcDims<P, MC>;
   extern __shared__ __align__(128) unsigned char sm_raw[];
   unsigned char* sm_tc = sm_raw + ((1024u - (smem_u32(sm_raw) & 1023u)) & 1023u);
   constexpr int NS = D::TAB_SLOTS;
   unsigned char* sT = sm_tc;                      // table slots: [hi | lo] images, kRows rows each
-  unsigned char* sB = sm_tc + NS * D::TAB_BYTES;  // kStages stages of regions (part, atom): kMaxCols rows x 128 B
-  __shared__ int s_row[kMaxCols];
+  unsigned char* sB = sm_tc + NS * D::TAB_BYTES;  // kStages stages of regions (part, atom): MC rows x 128 B
+  __shared__ int s_row[MC];
   __shared__ int s_ncol[kAcc], s_b0[kAcc], s_rt[kAcc];
   __shared__ int s_tsl[kStages], s_icol[kStages], s_last[kStages];
   __shared__ uint64_t bar_full[kStages], bar_bfree[kStages], bar_tfree[2], bar_accf[kAcc], bar_acce[kAcc], bar_meta[kAcc];
@@ -555,9 +557,18 @@ int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts, int nd) {
     const int grid = a.n_tc_items < a.tc_grid ? a.n_tc_items : a.tc_grid;
     CUtensorMap map;
     std::memcpy(&map, a.tc_rows_map, sizeof(map));
-    launch_pdl(k_m2l_tc<P>, grid, kEpilogue + kProducers + kIssuer, D::SMEM, st, map, a.n_tc_items, a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt,
-                                                                         a.n_tc_pairs, a.tc_src, static_cast<const __half*>(a.tc_tab),
-                                                                         static_cast<const __half*>(a.tc_Mt), a.tc_Y, a.tc_err);
+    bool wide = false;
+    if constexpr (P <= 10) wide = a.tc_item_pairs > kMaxPairs;
+    if (wide) {
+      if constexpr (P <= 10)
+        launch_pdl(k_m2l_tc<P, kMaxPairsWide>, grid, kEpilogue + kProducers + kIssuer, TcDims<P, kMaxPairsWide>::SMEM, st, map, a.n_tc_items,
+                   a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt, a.n_tc_pairs, a.tc_src, static_cast<const __half*>(a.tc_tab),
+                   static_cast<const __half*>(a.tc_Mt), a.tc_Y, a.tc_err);
+    } else {
+      launch_pdl(k_m2l_tc<P, kMaxPairs>, grid, kEpilogue + kProducers + kIssuer, D::SMEM, st, map, a.n_tc_items, a.tc_item_tab,
+                 a.tc_item_begin, a.tc_item_cnt, a.n_tc_pairs, a.tc_src, static_cast<const __half*>(a.tc_tab),
+                 static_cast<const __half*>(a.tc_Mt), a.tc_Y, a.tc_err);
+    }
     ++launches;
   }
   if (parts & TC_REDUCE) {
@@ -571,7 +582,9 @@ int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts, int nd) {
 
 template <int P>
 void tc_tables_launch(int ntab, const double* tab, const double* alpha, __half* T, unsigned int* maxbits, cudaStream_t st) {
-  cudaFuncSetAttribute(k_m2l_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcDims<P>::SMEM);
+  cudaFuncSetAttribute(k_m2l_tc<P, kMaxPairs>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcDims<P>::SMEM);
+  if constexpr (P <= 10)
+    cudaFuncSetAttribute(k_m2l_tc<P, kMaxPairsWide>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcDims<P, kMaxPairsWide>::SMEM);
   if (ntab > 0) k_tc_tables<P><<<ntab * TcDims<P>::RT, 128, 0, st>>>(ntab, tab, alpha, T, maxbits);
 }
 
@@ -609,7 +622,7 @@ int tc_make_rows_map(void* map_out, void* Mt, int nrows, int p) {
 size_t tc_table_bytes(int p) { return (size_t)2 * kRows * tc_kp(p) * 2; }
 int tc_row_tiles(int p) { return ((p + 1) * (p + 1) + kRows - 1) / kRows; }
 int tc_kpo(int p) { return tc_kp(p); }
-int tc_max_pairs() { return kMaxPairs; }
+int tc_max_pairs(int p) { return p <= 10 ? kMaxPairsWide : kMaxPairs; }
 
 void tc_alpha_host(int p, double* alpha) {
   // alpha(i) = sqrt((n+m)! (n-m)!) for the real index i of (n, m, part)

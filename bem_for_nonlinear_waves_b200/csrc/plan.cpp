@@ -1074,6 +1074,25 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   return true;
 }
 
+void retile_tc_items(Plan& P, int max_pairs) {
+  std::vector<int32_t> tab, beg, cnt;
+  const size_t n = P.tc_item_tab.size();
+  for (size_t i = 0; i < n;) {  // the items of one table cover one run of tc_pair
+    size_t j = i;
+    int64_t total = 0;
+    while (j < n && P.tc_item_tab[j] == P.tc_item_tab[i]) total += P.tc_item_cnt[j++];
+    for (int64_t b = 0; b < total; b += max_pairs) {
+      tab.push_back(P.tc_item_tab[i]);
+      beg.push_back(P.tc_item_begin[i] + (int)b);
+      cnt.push_back((int)std::min<int64_t>(max_pairs, total - b));
+    }
+    i = j;
+  }
+  P.tc_item_tab.swap(tab);
+  P.tc_item_begin.swap(beg);
+  P.tc_item_cnt.swap(cnt);
+}
+
 void build_tc_groups(Plan& P, int max_pairs) {
   // tables = runs of one lattice offset over all levels in the sorted pair order of the FP64
   // groups (the pairs of one offset are contiguous there); pairs off the lattice get one each

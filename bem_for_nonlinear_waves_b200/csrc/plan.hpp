@@ -155,5 +155,8 @@ void parallel_copy(void* dst, const void* src, size_t bytes);
 
 // Groups the M2L pairs for the tensor-core path (tc_* fields); items hold <= max_pairs pairs.
 void build_tc_groups(Plan& plan, int max_pairs);
+// Re-splits the tensor-core work items of build_tc_groups into items of <= max_pairs pairs
+// (tables and pair order unchanged).
+void retile_tc_items(Plan& plan, int max_pairs);
 
 }  // namespace bemb200

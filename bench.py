@@ -491,6 +491,7 @@ def main():
         "matvecs_per_s": world * 1e3 / prof["total"],
         "host_setup_s_per_step": {"plan": plan_s / args.steps, "upload": upload_s / args.steps},
         "matvec_stage_ms": prof,
+        "tc_item_tuning": bvp.tc_tuning() if mixed else None,
         "e2e": {"value": world * args.steps / e2e_max, "unit": "solves/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "e2e_batch": e2e_batch,

@@ -66,6 +66,9 @@ typedef struct {
                                 true residual, same stopping test; needs p <= 12 */
   int32_t poly_degree;       /* preconditioner 2: polynomial degree 1..24 (0: 8) */
   int32_t tree_on_host;      /* 0: the octree is grown on the device (tree.cu), 1: on the host; same tree */
+  int32_t tc_item_pairs;     /* mixed: pairs per tensor-core M2L work item, 1..80; 0: autotuned (once
+                                per process and problem class; the result does not depend on it) */
+  int32_t reserved;
 } bem_gpu_opts;
 
 /* One boundary-value problem.  The DOF table is what the reference's setNodeFaceIndices()
@@ -283,6 +286,11 @@ int bem_gpu_check_device_status(bem_gpu_ctx* ctx);
  * bem_harmonic_ritz_values: host helper -- harmonic Ritz values of a (k+1) x k Arnoldi
  *   Hessenberg matrix (row-major, leading dimension ldh, k <= 32); 0 or -1. */
 int bem_gpu_poly_roots(bem_gpu_ctx* ctx, int32_t cap, double* re, double* im);
+
+/* Tensor-core M2L work-item size of a mixed context: *pairs_in_use, and the 4 candidates with
+ * their contraction-kernel times (ms; zeros if never tuned in this process).  Returns 1 if the
+ * last set-up ran the tuning, 0 if it used a cached or forced size. */
+int bem_gpu_tc_tuning(bem_gpu_ctx* ctx, int32_t* pairs_in_use, int32_t* candidates /*[4]*/, double* ms /*[4]*/);
 
 /* Set-up time by part (seconds) of the last set-up: [0] element sources, [1] octree, [2] lists,
  * [3] element order and node arrays, [4] M2L grouping, [5] near-field blocks, [6] DOF incidence
