@@ -30,7 +30,7 @@ class Opts(ctypes.Structure):
     _fields_ = [("expansion_order", c_int), ("mac_theta", c_dbl), ("leaf_max_elements", c_int), ("max_level", c_int),
                 ("tol", c_dbl), ("max_iter", c_int), ("device", c_int), ("tol_relative", c_int), ("preconditioner", c_int),
                 ("precision", c_int), ("poly_degree", c_int), ("tree_on_host", c_int),
-                ("tc_item_pairs", c_int), ("reserved", c_int)]
+                ("tc_item_pairs", c_int), ("overlap_near", c_int)]
 
 
 class MelSurface(ctypes.Structure):

@@ -40,7 +40,7 @@ def build_dofs(X, tri, face_dirichlet):
 
 
 def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter, device,
-               tol_relative, preconditioner, precision, poly_degree=8, tree_on_device=True, tc_item_pairs=0):
+               tol_relative, preconditioner, precision, poly_degree=8, tree_on_device=True, tc_item_pairs=0, overlap_near=False):
     o = L.Opts()
     lib.bem_gpu_default_opts(ctypes.byref(o))
     o.expansion_order = int(expansion_order)
@@ -55,6 +55,7 @@ def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_l
     o.poly_degree = int(poly_degree)
     o.tree_on_host = 0 if tree_on_device else 1
     o.tc_item_pairs = int(tc_item_pairs)
+    o.overlap_near = 1 if overlap_near else 0
     o.precision = {"fp64": 0, "mixed": 1}[precision]
     return o
 
@@ -64,7 +65,7 @@ class BEM_BVP:
 
     def __init__(self, X, tri, face_dirichlet, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30,
                  fmm_max_level=7, solver_tol=1e-9, solver_max_iter=500, device=0, dofs=None, tol_relative=False, preconditioner="none",
-                 precision="fp64", poly_degree=8, tree_on_device=True, tc_item_pairs=0):
+                 precision="fp64", poly_degree=8, tree_on_device=True, tc_item_pairs=0, overlap_near=False):
         self.lib = L.load()
         if not self.lib.bem_gpu_is_available():
             raise RuntimeError("no sm_100 CUDA device visible: the GMRES-FMM solver runs only on the GPU")
@@ -72,7 +73,8 @@ class BEM_BVP:
         self.tri = np.ascontiguousarray(tri, np.int32)
         self.face_dirichlet = np.ascontiguousarray(face_dirichlet, np.uint8)
         o = _make_opts(self.lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter,
-                       device, tol_relative, preconditioner, precision, poly_degree, tree_on_device, tc_item_pairs)
+                       device, tol_relative, preconditioner, precision, poly_degree, tree_on_device, tc_item_pairs,
+                       overlap_near)
         self.opts = o
         self.ctx = self.lib.bem_gpu_create(ctypes.byref(o))
         if not self.ctx:

@@ -114,6 +114,8 @@ inline int poly_degree(const bem_gpu_opts& o) { return o.poly_degree > 0 ? o.pol
 struct bem_gpu_ctx {
   bem_gpu_opts opts{};
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;                         // near field of the low-precision A.x
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;    // fork / join of the side stream
   std::string err;
   Plan plan, plan_spare;
   bool ready = false;
@@ -205,6 +207,9 @@ struct bem_gpu_ctx {
       if (e) cudaEventDestroy(e);
     if (arn_err_host) cudaFreeHost(arn_err_host);
     if (dtree) dtree_destroy(dtree);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
   }
   MatvecArgs args(const double* d_phi, const double* d_phin, double* d_rows, double* d_gphin, double* d_gnphi) const {
@@ -292,6 +297,11 @@ struct bem_gpu_ctx {
     a.tc_pos = tc_pos.p;
     a.n_tc_pairs = (int)plan.tc_pair.size();
     a.tc_item_pairs = tc_tune > 0 ? tc_tune : 80;
+    if (opts.overlap_near == 1) {  // near field on the side stream, concurrent with the FMM passes
+      a.side = side;
+      a.ev_fork = ev_fork;
+      a.ev_join = ev_join;
+    }
     a.tc_src = tc_src.p;
     a.tc_tab = tc_T.p;
     a.tc_Mt = tc_Mt.p;
@@ -519,7 +529,10 @@ bem_gpu_ctx* bem_gpu_create(const bem_gpu_opts* opts) {
   auto* ctx = new (std::nothrow) bem_gpu_ctx();
   if (!ctx) return nullptr;
   ctx->opts = *opts;
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess) {
     delete ctx;
     return nullptr;
   }

@@ -814,6 +814,60 @@ __global__ void __launch_bounds__(128) k_targets_ax(const NearBlockDev* __restri
   }
 }
 
+// Far-field part of A.x rows when the near part ran on its own (k_targets_ax with L = null, on
+// a second stream while the FMM passes run): rows[i] += L2P of the target's bucket at its point
+// for every row that is not a corner row.  One CTA per near block (= target bucket), one warp per
+// target, the L2P recurrence of k_targets_ax.
+template <int P>
+__global__ void __launch_bounds__(128) k_l2p_add(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_targets,
+                                                 const double* __restrict__ Xs, const double* __restrict__ node_X,
+                                                 const double2* __restrict__ L, const int* __restrict__ point_dof_off,
+                                                 const int* __restrict__ point_dof, const int* __restrict__ dof_kind,
+                                                 double* __restrict__ rows) {
+  constexpr int NC = ncoef(P);
+  __shared__ double2 sL[NC];
+  __shared__ double sHalf[P + 1], sRec[(P + 1) * (P + 1)];
+  for (int i = threadIdx.x; i < (P + 1) * (P + 1); i += blockDim.x) {
+    const int n = i / (P + 1), m = i - n * (P + 1);
+    sRec[i] = n > m ? 1.0 / double(n * n - m * m) : 0.0;
+    if (i <= P) sHalf[i] = i > 0 ? 1.0 / (2.0 * i) : 0.0;
+  }
+  const NearBlockDev B = blocks[blockIdx.x];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  for (int i = threadIdx.x; i < NC; i += blockDim.x) sL[i] = L[(size_t)B.node * 2 * NC + i];
+  __syncthreads();
+  const double cx = node_X[3 * B.node], cy = node_X[3 * B.node + 1], cz = node_X[3 * B.node + 2];
+  for (int tl = warp; tl < B.ntgt; tl += nwarp) {
+    const int p = nb_targets[B.tgt_off + tl];
+    const double px = Xs[3 * p] - cx, py = Xs[3 * p + 1] - cy, pz = Xs[3 * p + 2] - cz;
+    double f0 = 0.0;
+    const int m = lane;
+    if (m <= P) {
+      const double r2 = px * px + py * py + pz * pz;
+      double2 cur = make_double2(1.0, 0.0);
+      for (int k = 1; k <= m; ++k) cur = cscale(cmul(cur, make_double2(px, py)), sHalf[k]);
+      double2 prev = make_double2(0.0, 0.0);
+      const double w = (m == 0) ? 1.0 : 2.0;
+      for (int n = m; n <= P; ++n) {
+        if (n > m) {
+          const double inv = sRec[n * (P + 1) + m];
+          double2 nx = make_double2(((2 * n - 1) * pz * cur.x - r2 * prev.x) * inv, ((2 * n - 1) * pz * cur.y - r2 * prev.y) * inv);
+          prev = cur;
+          cur = nx;
+        }
+        const double2 l0 = sL[cidx(n, m)];
+        f0 += w * (l0.x * cur.x + l0.y * cur.y);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) f0 += __shfl_xor_sync(0xffffffffu, f0, o);
+    for (int k = point_dof_off[p] + lane; k < point_dof_off[p + 1]; k += 32) {
+      const int i = point_dof[k];
+      if (dof_kind[i] != 2) rows[i] += f0;
+    }
+  }
+}
+
 // Combined near weights of A.x (set-up): Wc = WG for a Dirichlet DOF column, -WGn otherwise.
 template <typename WT>
 __global__ void k_combine_weights(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs, const int* __restrict__ dof_kind,
@@ -1135,11 +1189,24 @@ __global__ void k_fp64_probe(int iters, double seed, double* __restrict__ sink) 
 
 // ---------------------------------------------------------------------------
 // launchers
+template <int P>
+int launch_near_only_t(const MatvecArgs& a, cudaStream_t st);
+
 template <int P, int ND>
 int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
   constexpr int NC = ncoef(P);
   constexpr int tpb_coef = ((NC + 31) / 32) * 32;
   int launches = 0;
+  // overlap: the near-field part of the rows (HBM-bound) runs on the side stream while the FMM
+  // passes run here; the far-field part is added once both are done
+  const bool overlap = stages == STAGE_ALL && ND == 1 && a.side && a.ev_fork && a.ev_join && a.Wc32 && a.ax && a.n_blocks > 0;
+  if (overlap) {
+    cudaEventRecord(a.ev_fork, st);
+    cudaStreamWaitEvent(a.side, a.ev_fork, 0);
+    launches += launch_near_only_t<P>(a, a.side);
+    cudaEventRecord(a.ev_join, a.side);
+    stages &= ~STAGE_TARGETS;
+  }
   if ((stages & STAGE_P2M) && a.n_leaves > 0 && ND == 1 && a.ax && a.p2m_C) {
     launch_pdl(k_p2m_apply<P>, a.n_leaves, tpb_coef, 0, st, a.leaves, a.leaf_dof_off, a.leaf_dof, a.p2m_C, a.ax, a.M);
     ++launches;
@@ -1189,6 +1256,11 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     const size_t shm = sizeof(double2) * (size_t)(a.chunk + a.max_ntgt);
     k_targets<P, ND><<<a.n_blocks, 128, shm, st>>>(a.blocks, a.nb_dofs, a.nb_targets, a.WG, a.WGn, a.Xs, a.node_X, a.L, a.phi, a.phin,
                                                a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.GPhin, a.GnPhi, a.chunk);
+    ++launches;
+  }
+  if (overlap) {
+    cudaStreamWaitEvent(st, a.ev_join, 0);
+    k_l2p_add<P><<<a.n_blocks, 128, 0, st>>>(a.blocks, a.nb_targets, a.Xs, a.node_X, a.L, a.point_dof_off, a.point_dof, a.dof_kind, a.rows);
     ++launches;
   }
   return launches;

@@ -97,6 +97,10 @@ struct MatvecArgs {
   const int* tc_item_cnt = nullptr;
   int n_tc_pairs = 0;
   int tc_item_pairs = 80;  // largest item (selects the tensor-core kernel variant)
+  // overlap of the near field with the FMM passes (low-precision A.x): a second stream and the
+  // two events that fork it from and join it to the launching stream; null: one stream
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   const int* tc_pos = nullptr;   // [pairs] position of pair slot k in work-item order
   const int* tc_src = nullptr;   // [pairs] source bucket, in work-item order
   const void* tc_tab = nullptr;  // FP16 hi/lo table images

@@ -66,9 +66,11 @@ typedef struct {
                                 true residual, same stopping test; needs p <= 12 */
   int32_t poly_degree;       /* preconditioner 2: polynomial degree 1..24 (0: 8) */
   int32_t tree_on_host;      /* 0: the octree is grown on the device (tree.cu), 1: on the host; same tree */
-  int32_t tc_item_pairs;     /* mixed: pairs per tensor-core M2L work item, 1..80; 0: autotuned (once
-                                per process and problem class; the result does not depend on it) */
-  int32_t reserved;
+  int32_t tc_item_pairs;     /* mixed: pairs per tensor-core M2L work item, 1..128 (p <= 10) or 1..80;
+                                0: autotuned (once per process and problem class; the result does not
+                                depend on it) */
+  int32_t overlap_near;      /* mixed: 1 = the near field of A.x runs on a second stream while the FMM
+                                passes run, its far part added after; 0 = one fused kernel after them */
 } bem_gpu_opts;
 
 /* One boundary-value problem.  The DOF table is what the reference's setNodeFaceIndices()
