@@ -309,6 +309,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "none", "near_poly"])
     ap.add_argument("--poly-degree", type=int, default=8, help="degree of the near_poly preconditioner")
+    ap.add_argument("--overlap-near", type=int, default=0, help="1: near field of the mixed A.x on a second stream")
     ap.add_argument("--max-iter", type=int, default=1500)
     ap.add_argument("--ref-iters", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -332,7 +333,7 @@ def main():
 
     def make(prec):
         return BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=cfg["p"], solver_tol=cfg["rel_tol"], tol_relative=True,
-                       solver_max_iter=args.max_iter, preconditioner=args.precond, poly_degree=args.poly_degree, dofs=d, device=local, precision=prec)
+                       solver_max_iter=args.max_iter, preconditioner=args.precond, poly_degree=args.poly_degree, overlap_near=args.overlap_near, dofs=d, device=local, precision=prec)
 
     bvp = make(args.precision)
     for _ in range(args.warmup):
@@ -485,7 +486,7 @@ def main():
         "config": {"workload": args.config, "n_points": int(t.n_points), "n_faces": int(t.n_faces), "n_dof": int(bvp.matrix_size),
                    "p": p, "theta": 0.25, "leaf_max": 30, "rel_tol": cfg["rel_tol"], "precision": args.precision,
                    "preconditioner": args.precond + (f" (degree {args.poly_degree})" if args.precond == "near_poly" else ""),
-                   "gmres_iterations": iters / args.steps, "matvecs_fp64": mv / args.steps,
+                   "gmres_iterations": iters / args.steps, "overlap_near": bool(args.overlap_near), "matvecs_fp64": mv / args.steps,
                    "matvecs_lowp": mv_lo / args.steps, "converged": converged, "parallelism": f"replicas{world}",
                    "l2": "working set > L2 (near-field weights %.1f GB)" % (tree["nnz"] * 16 / 1e9)},
         "matvecs_per_s": world * 1e3 / prof["total"],
