@@ -24,6 +24,7 @@ namespace {
 // per splitting bucket: parent geometry then the 8 children's (xmin[3], inv_dL, size[3]) as
 // doubles, 7 + 8 * 7 values
 constexpr int kGeo = 7 * 9;
+constexpr int kChunk = 4096;  // elements per CTA of the classification and the scatter
 
 __device__ __forceinline__ int cell_index_clamped(const double* g, const double* x) {
   int ijk[3];
@@ -44,15 +45,17 @@ __device__ __forceinline__ bool inside_box(const double* g, const double* x) {
   return true;
 }
 
-// one CTA per splitting bucket: cell and inside flag of each element; counts per cell
+// one CTA per chunk of a splitting bucket's elements (at most kChunk, in order): cell and inside
+// flag of each element; counts per cell of the chunk
 __global__ void __launch_bounds__(256) k_tree_count(const int* __restrict__ seg_beg, const int* __restrict__ seg_end,
-                                                    const double* __restrict__ geo, const int* __restrict__ elems,
+                                                    const int* __restrict__ seg_geo, const double* __restrict__ geo,
+                                                    const int* __restrict__ elems,
                                                     const double* __restrict__ poles, int tag_base, uint8_t* __restrict__ tag,
                                                     int* __restrict__ cnt_all, int* __restrict__ cnt_pass) {
   __shared__ double g[kGeo];
   __shared__ int ca[8], cp[8];
   const int node = blockIdx.x;
-  for (int i = threadIdx.x; i < kGeo; i += blockDim.x) g[i] = geo[(size_t)node * kGeo + i];
+  for (int i = threadIdx.x; i < kGeo; i += blockDim.x) g[i] = geo[(size_t)seg_geo[node] * kGeo + i];
   if (threadIdx.x < 8) ca[threadIdx.x] = cp[threadIdx.x] = 0;
   __syncthreads();
   for (int i = seg_beg[node] + threadIdx.x; i < seg_end[node]; i += blockDim.x) {
@@ -71,7 +74,8 @@ __global__ void __launch_bounds__(256) k_tree_count(const int* __restrict__ seg_
   }
 }
 
-// stable scatter of the kept elements of each (bucket, cell) to off[bucket * 8 + cell] onwards
+// stable scatter of the kept elements of each (chunk, cell) to off[chunk * 8 + cell] onwards (the
+// chunks of a bucket follow each other, so the bucket's partition is stable as a whole)
 __global__ void __launch_bounds__(256) k_tree_scatter(const int* __restrict__ seg_beg, const int* __restrict__ seg_end,
                                                       const int* __restrict__ elems, int tag_base, const uint8_t* __restrict__ tag,
                                                       const int* __restrict__ off, int* __restrict__ next) {
@@ -232,13 +236,13 @@ struct Buf {
 struct DeviceTree {
   cudaStream_t stream = nullptr;
   Buf<double> poles, geo;
-  Buf<int> elems, seg_beg, seg_end, cnt, off;  // elems: every level's array, back to back
+  Buf<int> elems, seg_beg, seg_end, seg_geo, cnt, off;  // elems: every level's array, back to back; segments = chunks
   Buf<uint8_t> tag;
   Buf<double> nX, ndL, noff;                              // interaction lists: node geometry
   Buf<int> ncb, nce, nch, lt, lco, lc, lcnt, loff, lno, lmo, lxo;  // and per-level work arrays
   size_t cur = 0, cur_n = 0;  // current level: offset into elems, length
   int launches = 0;
-  std::vector<int> h_beg, h_end;
+  std::vector<int> h_beg, h_end, h_geo, h_cnt;  // chunks of the current level and their counts
 };
 
 DeviceTree* dtree_create(void* stream) {
@@ -264,43 +268,67 @@ bool dtree_begin(DeviceTree* t, int nf, const double* poles, int n_root, const i
 bool dtree_count(DeviceTree* t, int n, const int* seg_beg, const int* seg_end, const double* geo, int* cnt_all, int* cnt_pass) {
   if (n <= 0) return true;
   cudaStream_t s = t->stream;
-  if (!t->seg_beg.fit(n) || !t->seg_end.fit(n) || !t->geo.fit((size_t)n * kGeo) || !t->cnt.fit((size_t)16 * n) || !t->off.fit((size_t)8 * n))
-    return false;
-  t->h_beg.assign(seg_beg, seg_beg + n);
-  t->h_end.assign(seg_end, seg_end + n);
+  // chunks of at most kChunk elements, in bucket order and, within a bucket, in element order
+  t->h_beg.clear();
+  t->h_end.clear();
+  t->h_geo.clear();
   for (int i = 0; i < n; ++i) {  // segments are offsets into the current level's array
     if (seg_beg[i] < 0 || seg_end[i] < seg_beg[i] || (size_t)seg_end[i] > t->cur_n) return false;
-    t->h_beg[i] += (int)t->cur;
-    t->h_end[i] += (int)t->cur;
+    for (int b = seg_beg[i]; b < seg_end[i]; b += kChunk) {
+      t->h_beg.push_back(b + (int)t->cur);
+      t->h_end.push_back(std::min(b + kChunk, seg_end[i]) + (int)t->cur);
+      t->h_geo.push_back(i);
+    }
   }
-  if (cudaMemcpyAsync(t->seg_beg.p, t->h_beg.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(t->seg_end.p, t->h_end.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+  const int nc = (int)t->h_beg.size();
+  std::fill(cnt_all, cnt_all + 8 * (size_t)n, 0);
+  std::fill(cnt_pass, cnt_pass + 8 * (size_t)n, 0);
+  t->h_cnt.assign(16 * (size_t)nc, 0);
+  if (nc == 0) return true;
+  if (!t->seg_beg.fit(nc) || !t->seg_end.fit(nc) || !t->seg_geo.fit(nc) || !t->geo.fit((size_t)n * kGeo) || !t->cnt.fit((size_t)16 * nc) ||
+      !t->off.fit((size_t)8 * nc))
+    return false;
+  if (cudaMemcpyAsync(t->seg_beg.p, t->h_beg.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(t->seg_end.p, t->h_end.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(t->seg_geo.p, t->h_geo.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s) != cudaSuccess ||
       cudaMemcpyAsync(t->geo.p, geo, sizeof(double) * kGeo * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
     return false;
   // tags are indexed by position in the elems buffer relative to the current level
   ++t->launches;
-  k_tree_count<<<n, 256, 0, s>>>(t->seg_beg.p, t->seg_end.p, t->geo.p, t->elems.p, t->poles.p, (int)t->cur, t->tag.p, t->cnt.p,
-                                 t->cnt.p + 8 * n);
+  k_tree_count<<<nc, 256, 0, s>>>(t->seg_beg.p, t->seg_end.p, t->seg_geo.p, t->geo.p, t->elems.p, t->poles.p, (int)t->cur, t->tag.p,
+                                  t->cnt.p, t->cnt.p + 8 * nc);
   if (cudaGetLastError() != cudaSuccess) return false;
-  if (cudaMemcpyAsync(cnt_all, t->cnt.p, sizeof(int) * 8 * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaMemcpyAsync(cnt_pass, t->cnt.p + 8 * n, sizeof(int) * 8 * n, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+  if (cudaMemcpyAsync(t->h_cnt.data(), t->cnt.p, sizeof(int) * 16 * nc, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
     return false;
-  return cudaStreamSynchronize(s) == cudaSuccess;
+  for (int c = 0; c < nc; ++c)
+    for (int k = 0; k < 8; ++k) {
+      cnt_all[8 * t->h_geo[c] + k] += t->h_cnt[8 * (size_t)c + k];
+      cnt_pass[8 * t->h_geo[c] + k] += t->h_cnt[8 * (size_t)nc + 8 * (size_t)c + k];
+    }
+  return true;
 }
 
 bool dtree_scatter(DeviceTree* t, int n, const int* off, int total) {
   cudaStream_t s = t->stream;
   const size_t next = t->cur + t->cur_n;
   if (next + (size_t)total > t->elems.cap) return false;
-  if (n > 0) {
-    std::vector<int> o(off, off + 8 * (size_t)n);
-    for (auto& v : o) {
-      if (v < 0 || v > total) return false;
-      v += (int)next;
-    }
-    if (cudaMemcpyAsync(t->off.p, o.data(), sizeof(int) * 8 * n, cudaMemcpyHostToDevice, s) != cudaSuccess) return false;
+  const int nc = (int)t->h_beg.size();
+  if (n > 0 && nc > 0) {
+    // each chunk's kept elements of cell k start after those of the bucket's earlier chunks
+    for (int i = 0; i < 8 * n; ++i)
+      if (off[i] < 0 || off[i] > total) return false;
+    std::vector<int> o(8 * (size_t)nc), run(off, off + 8 * (size_t)n);
+    for (int c = 0; c < nc; ++c)
+      for (int k = 0; k < 8; ++k) {
+        int& r = run[8 * (size_t)t->h_geo[c] + k];
+        o[8 * (size_t)c + k] = r + (int)next;
+        r += t->h_cnt[8 * (size_t)nc + 8 * (size_t)c + k];
+        if (r > total) return false;
+      }
+    if (cudaMemcpyAsync(t->off.p, o.data(), sizeof(int) * 8 * nc, cudaMemcpyHostToDevice, s) != cudaSuccess) return false;
     ++t->launches;
-    k_tree_scatter<<<n, 256, 0, s>>>(t->seg_beg.p, t->seg_end.p, t->elems.p, (int)t->cur, t->tag.p, t->off.p, t->elems.p);
+    k_tree_scatter<<<nc, 256, 0, s>>>(t->seg_beg.p, t->seg_end.p, t->elems.p, (int)t->cur, t->tag.p, t->off.p, t->elems.p);
     if (cudaGetLastError() != cudaSuccess) return false;
     if (cudaStreamSynchronize(s) != cudaSuccess) return false;  // o is freed on return
   }
