@@ -757,10 +757,23 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
 
   lap(2);
   // element order: DFS pre-order of the deepest bucket holding each element
+  // (the buckets of one level hold disjoint elements, and a deeper bucket is created after its
+  // ancestors: assigning level by level leaves each element with the last bucket in creation
+  // order that holds it)
   std::vector<int> owner(nf, -1);
-  for (int i = 0; i < nb; ++i)
-    for (int e : B[i].data) owner[e] = i;  // children come after parents in creation order
+  {
+    int maxl = 0;
+    for (int i = 0; i < nb; ++i) maxl = std::max(maxl, B[i].level);
+    std::vector<std::vector<int>> by_level(maxl + 1);
+    for (int i = 0; i < nb; ++i) by_level[B[i].level].push_back(i);
+    for (const auto& lv : by_level) {
+#pragma omp parallel for schedule(dynamic, 16)
+      for (int k = 0; k < (int)lv.size(); ++k)
+        for (int e : B[lv[k]].data) owner[e] = lv[k];
+    }
+  }
   std::vector<std::vector<int>> owned(nb);
+#pragma omp parallel for schedule(dynamic, 16)
   for (int i = 0; i < nb; ++i)
     for (int e : B[i].data)
       if (owner[e] == i) owned[i].push_back(e);
