@@ -93,6 +93,7 @@ EXPORTS = {
     "bem_gpu_batch_submit": (c_int, [ctypes.c_void_p, ctypes.POINTER(Desc), P_dbl, P_dbl, P_dbl, ctypes.POINTER(Stats),
                                      ctypes.POINTER(ctypes.c_int64)]),
     "bem_gpu_batch_poll": (c_int, [ctypes.c_void_p, ctypes.c_int64, c_int]),
+    "bem_gpu_batch_release": (c_int, [ctypes.c_void_p, ctypes.c_int64]),
     "bem_gpu_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "bem_gpu_batch_destroy": (None, [ctypes.c_void_p]),
 }

@@ -339,8 +339,9 @@ class BatchSolver:
     def result(self, ticket):
         rc = self.lib.bem_gpu_batch_poll(self.handle, int(ticket), 1)
         item = self._pending.pop(int(ticket))
-        if rc not in (L.BEM_OK, L.BEM_ERR_NOT_CONVERGED):
-            msg = self.lib.bem_gpu_batch_last_error(self.handle)
+        msg = self.lib.bem_gpu_batch_last_error(self.handle) if rc not in (L.BEM_OK, L.BEM_ERR_NOT_CONVERGED) else None
+        self.lib.bem_gpu_batch_release(self.handle, int(ticket))
+        if msg is not None:
             raise RuntimeError(f"batch solve {ticket}: {L.STATUS.get(rc, rc)}: {msg.decode() if msg else ''}")
         return item[5], item[6], item[7]
 

@@ -11,6 +11,7 @@
 #include <string>
 #include <thread>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/bem_b200.h"
@@ -29,11 +30,14 @@ struct bem_gpu_batch {
   std::mutex mu;
   std::condition_variable cv_job, cv_done;
   std::deque<Job> queue;
-  std::unordered_map<int64_t, int> done;  // ticket -> status
+  std::unordered_set<int64_t> running;
+  // ticket -> status of finished problems, and their error messages; an entry lives until
+  // bem_gpu_batch_release(ticket) (or the batch's destruction), so a long-running batch holds
+  // only the tickets its caller has not collected yet
+  std::unordered_map<int64_t, int> done;
   std::unordered_map<int64_t, std::string> errors;
   int64_t next_ticket = 1;
   bool stop = false;
-  std::string err;
 
   void run(int w) {
     for (;;) {
@@ -44,11 +48,13 @@ struct bem_gpu_batch {
         if (queue.empty()) return;  // stop requested and nothing left
         job = queue.front();
         queue.pop_front();
+        running.insert(job.ticket);
       }
       const int rc = bem_gpu_solve_bvp(ctx[w], &job.desc, job.known, nullptr, job.phi, job.phin, job.stats);
       {
         std::lock_guard<std::mutex> lk(mu);
         done[job.ticket] = rc;
+        running.erase(job.ticket);
         if (rc != BEM_OK && rc != BEM_ERR_NOT_CONVERGED) errors[job.ticket] = bem_gpu_last_error(ctx[w]);
       }
       cv_done.notify_all();
@@ -88,20 +94,44 @@ int bem_gpu_batch_submit(bem_gpu_batch* b, const bem_bvp_desc* desc, const doubl
   return BEM_OK;
 }
 
+// The message of the last poll is kept per calling thread: pollers on different threads never
+// see each other's messages.
+static thread_local std::string t_batch_err;
+
 int bem_gpu_batch_poll(bem_gpu_batch* b, int64_t ticket, int32_t wait) {
   if (!b || ticket < 1) return BEM_ERR_INVALID_ARGUMENT;
   std::unique_lock<std::mutex> lk(b->mu);
   if (ticket >= b->next_ticket) return BEM_ERR_INVALID_ARGUMENT;
-  if (wait) b->cv_done.wait(lk, [&] { return b->done.count(ticket) > 0; });
+  auto queued = [&] {
+    for (const auto& j : b->queue)
+      if (j.ticket == ticket) return true;
+    return false;
+  };
   auto it = b->done.find(ticket);
-  if (it == b->done.end()) return BEM_ERR_NOT_READY;
+  if (it == b->done.end() && !wait) return BEM_ERR_NOT_READY;
+  if (it == b->done.end()) {
+    // a ticket that is neither finished nor queued nor running was released already
+    if (!queued() && b->running.count(ticket) == 0) return BEM_ERR_INVALID_ARGUMENT;
+    b->cv_done.wait(lk, [&] { return b->done.count(ticket) > 0; });
+    it = b->done.find(ticket);
+  }
   const int rc = it->second;
   auto e = b->errors.find(ticket);
-  b->err = (e == b->errors.end()) ? std::string() : e->second;
+  t_batch_err = (e == b->errors.end()) ? std::string() : e->second;
   return rc;
 }
 
-const char* bem_gpu_batch_last_error(const bem_gpu_batch* b) { return b ? b->err.c_str() : "null batch"; }
+int bem_gpu_batch_release(bem_gpu_batch* b, int64_t ticket) {
+  if (!b || ticket < 1) return BEM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(b->mu);
+  auto it = b->done.find(ticket);
+  if (it == b->done.end()) return BEM_ERR_NOT_READY;  // unknown, released, or not finished yet
+  b->done.erase(it);
+  b->errors.erase(ticket);
+  return BEM_OK;
+}
+
+const char* bem_gpu_batch_last_error(const bem_gpu_batch* b) { return b ? t_batch_err.c_str() : "null batch"; }
 
 void bem_gpu_batch_destroy(bem_gpu_batch* b) {
   if (!b) return;

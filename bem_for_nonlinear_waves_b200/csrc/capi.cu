@@ -111,6 +111,11 @@ constexpr int kTuneCandNarrow[4] = {32, 48, 64, 80};
 inline const int* tune_cand(int p) { return p <= 10 ? kTuneCandWide : kTuneCandNarrow; }
 inline int poly_degree(const bem_gpu_opts& o) { return o.poly_degree > 0 ? o.poly_degree : 8; }
 
+// M2L pair slots of bem_gpu_matvec_device_noalloc: a fixed area in this file's device image,
+// reserved on every device that loads the module and held until the process exits.
+constexpr size_t kNoAllocSlotBytes = size_t(32) << 20;  // 32 MiB: m2l_pairs * 2 * ncoef(p) * 16 B must fit
+static __device__ __align__(256) unsigned char g_m2l_slot_scratch[kNoAllocSlotBytes];
+
 struct bem_gpu_ctx {
   bem_gpu_opts opts{};
   cudaStream_t stream = nullptr;
@@ -120,6 +125,10 @@ struct bem_gpu_ctx {
   Plan plan, plan_spare;
   bool ready = false;
   double time_setup = 0.0;
+  // device address of g_m2l_slot_scratch on this context's device, looked up at the first
+  // set-up with the device current (nullptr: not looked up yet, or the lookup failed)
+  void* noalloc_slots = nullptr;
+  cudaError_t noalloc_lookup = cudaSuccess;
 
   // geometry / tree
   DBuf<double> Xs, e_q, e_W, e_n, e_near, node_X, WG, WGn, Wc, diag;
@@ -332,15 +341,21 @@ int fill_quadrature(bem_gpu_ctx* ctx) {
                            {0.108103018168070, 0.445948490915965, 0.445948490915965, 0.111690794839006},
                            {0.445948490915965, 0.108103018168070, 0.445948490915965, 0.111690794839006},
                            {0.445948490915965, 0.445948490915965, 0.108103018168070, 0.111690794839006}};
-  // 5-point Gauss-Legendre nodes/weights on [-1,1], mapped to [0,1]^2 (__array_GW5xGW5__)
-  const double xs[5] = {-0.9061798459386640, -0.5384693101056831, 0.0, 0.5384693101056831, 0.9061798459386640};
-  const double ws[5] = {0.2369268850561891, 0.4786286704993665, 0.5688888888888889, 0.4786286704993665, 0.2369268850561891};
+  // 5x5 Gauss-Legendre product rule on [0,1]^2 with the reference's own 15-digit constants
+  // (__array_GW5xGW5__, lib/include/basic_constants.hpp:1326-1350), which the near-field
+  // weights must share to agree with the reference beyond ~1e-12.  Symmetric table: node a,
+  // weight class c(a) = {0, 1, 2, 1, 0}, w(a, b) = wc[c(a)][c(b)].
+  const double xs[5] = {0.046910077030668, 0.230765344947158, 0.5, 0.769234655052841, 0.953089922969332};
+  const int cls[5] = {0, 1, 2, 1, 0};
+  const double wc[3][3] = {{0.0140335872156063, 0.0283499999999991, 0.0336962680968792},
+                           {0.0283499999999991, 0.0572713510559978, 0.0680716331376877},
+                           {0.0336962680968792, 0.0680716331376877, 0.0809086419753086}};
   double gw[25][3];
   for (int a = 0; a < 5; ++a)
     for (int b = 0; b < 5; ++b) {
-      gw[5 * a + b][0] = 0.5 * (xs[a] + 1.0);
-      gw[5 * a + b][1] = 0.5 * (xs[b] + 1.0);
-      gw[5 * a + b][2] = 0.25 * ws[a] * ws[b];
+      gw[5 * a + b][0] = xs[a];
+      gw[5 * a + b][1] = xs[b];
+      gw[5 * a + b][2] = wc[cls[a]][cls[b]];
     }
   upload_quadrature(dv, gw, ctx->stream);
   CK(cudaGetLastError());
@@ -745,6 +760,16 @@ static int tune_tc_items(bem_gpu_ctx* ctx) {
 static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   if (!ctx || !d) return BEM_ERR_INVALID_ARGUMENT;
   CK(cudaSetDevice(ctx->opts.device));
+  if (!ctx->noalloc_slots) {
+    // the no-alloc mat-vec's slot area: its name is a host-side handle only, the kernels need
+    // its address on this device.  The lookup allocates nothing (the area comes with the
+    // module, which this loads if nothing of it ran yet); a failure only disables that entry.
+    ctx->noalloc_lookup = cudaGetSymbolAddress(&ctx->noalloc_slots, g_m2l_slot_scratch);
+    if (ctx->noalloc_lookup != cudaSuccess) {
+      ctx->noalloc_slots = nullptr;
+      (void)cudaGetLastError();
+    }
+  }
   const bool had_plan = ctx->ready;
   ctx->ready = false;
   ctx->h2d = ctx->d2h = ctx->launches = 0;
@@ -1814,12 +1839,6 @@ int bem_gpu_check_device_status(bem_gpu_ctx* ctx) {
 // while they apply the operator (a time integrator or outer solver running out of a fixed
 // device-memory reservation, a server holding many small problems on one device that wants
 // one shared slot area rather than one per problem) use this entry point.
-constexpr size_t kNoAllocSlotBytes = size_t(32) << 20;  // 32 MiB: m2l_pairs * 2 * ncoef(p) * 16 B must fit
-constexpr int kNoAllocMaxDevices = 64;
-static __device__ __align__(256) unsigned char g_m2l_slot_scratch[kNoAllocSlotBytes];
-static std::mutex g_slot_mu;
-static void* g_slot_addr[kNoAllocMaxDevices] = {};
-
 int bem_gpu_matvec_device_noalloc(bem_gpu_ctx* ctx, const double* d_x, double* d_y) {
   if (!ctx || !d_x || !d_y) return BEM_ERR_INVALID_ARGUMENT;
   if (!ctx->ready) return BEM_ERR_NOT_READY;
@@ -1830,35 +1849,30 @@ int bem_gpu_matvec_device_noalloc(bem_gpu_ctx* ctx, const double* d_x, double* d
                " pairs at order " + std::to_string(P.opt.p) + ") exceeds the fixed " + std::to_string(kNoAllocSlotBytes) + " bytes";
     return BEM_ERR_UNSUPPORTED;
   }
+  if (!ctx->noalloc_slots) {
+    ctx->err = std::string("no-alloc mat-vec: the slot area's device address could not be looked up at set-up: ") +
+               cudaGetErrorString(ctx->noalloc_lookup);
+    return BEM_ERR_DEVICE;
+  }
+  int prev_dev = -1;
+  CK(cudaGetDevice(&prev_dev));
   const int dev = ctx->opts.device;
-  if (dev < 0 || dev >= kNoAllocMaxDevices) {
-    ctx->err = "no-alloc mat-vec: device index out of range";
-    return BEM_ERR_INVALID_ARGUMENT;
-  }
-  CK(cudaSetDevice(dev));
-  // first call on a device: resolve the array's device address (no allocation; the
-  // module is loaded now if it was not yet).  Make that first call before beginning any
-  // stream capture on the device.
-  void* slots = nullptr;
-  {
-    std::lock_guard<std::mutex> g(g_slot_mu);
-    if (!g_slot_addr[dev]) {
-      void* a = nullptr;
-      CK(cudaGetSymbolAddress(&a, g_m2l_slot_scratch));
-      g_slot_addr[dev] = a;
-    }
-    slots = g_slot_addr[dev];
-  }
-  // every slot of the m2l_pairs in use is overwritten before the reduction reads it, so
-  // the area needs no clearing; the local expansions L are zeroed inside the launch
-  // sequence as on the graph path.  One area per device: calls that may overlap on one
-  // device (other streams, other threads, other contexts) race on it and must be ordered
-  // by the caller.
+  if (dev != prev_dev) CK(cudaSetDevice(dev));
+  // every slot of the m2l_pairs in use is overwritten before the reduction reads it, so the
+  // area needs no clearing; the local expansions L are zeroed inside the launch sequence as
+  // on the graph path.  One area per device: calls that may overlap on one device (other
+  // streams, other threads, other contexts) race on it and must be ordered by the caller.
+  // The FP64 operator, also on a mixed-precision context.
   MatvecArgs a = ctx->args(ctx->phi.p, ctx->phin.p, d_y, nullptr, nullptr);
-  a.Y = static_cast<double2*>(slots);
+  a.Y = static_cast<double2*>(ctx->noalloc_slots);
   launch_densities(P.ndof, 0, d_x, nullptr, ctx->dof_kind.p, ctx->phi.p, ctx->phin.p, ctx->stream);
   ctx->launches += 1 + launch_matvec(P.opt.p, a, ctx->stream);
-  CK(cudaGetLastError());
+  const cudaError_t e = cudaGetLastError();
+  if (dev != prev_dev) cudaSetDevice(prev_dev);
+  if (e != cudaSuccess) {
+    ctx->err = std::string("no-alloc mat-vec: ") + cudaGetErrorString(e);
+    return BEM_ERR_DEVICE;
+  }
   return BEM_OK;
 }
 

@@ -334,15 +334,19 @@ int launch_arnoldi_step(const ArnoldiArgs& a, cudaStream_t st) {
 }
 
 int configure_arnoldi(int cols) {
-  // the permission only grows (contexts on other threads may use larger bases)
+  // the permission only grows (contexts on other threads may use larger bases); it belongs
+  // to the current device, so the bookkeeping is per device
   static std::mutex mu;
-  static size_t granted = 0;
+  static size_t granted[kMaxDevices] = {};
   const size_t bytes = sizeof(double) * (3 * (size_t)cols + 1);
   if (bytes > 227 * 1024) return -1;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+  const bool tracked = dev >= 0 && dev < kMaxDevices;  // untracked devices: set every time
   std::lock_guard<std::mutex> lk(mu);
-  if (bytes <= granted) return 0;
+  if (tracked && bytes <= granted[dev]) return 0;
   if (cudaFuncSetAttribute(k_arn_givens, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) return -1;
-  granted = bytes;
+  if (tracked) granted[dev] = bytes;
   return 0;
 }
 

@@ -1269,12 +1269,16 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
 template <int P>
 void set_target_smem(int bytes) {
   // the permission only grows: contexts of different problems (batch workers on other
-  // threads) may launch these kernels with their own sizes at any time
+  // threads) may launch these kernels with their own sizes at any time.  The attribute
+  // belongs to the current device, so the bookkeeping is per device.
   static std::mutex mu;
-  static int granted = 0;
+  static int granted[kMaxDevices] = {};
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+  const bool tracked = dev >= 0 && dev < kMaxDevices;  // untracked devices: set every time
   std::lock_guard<std::mutex> lk(mu);
-  if (bytes <= granted) return;
-  granted = bytes;
+  if (tracked && bytes <= granted[dev]) return;
+  if (tracked) granted[dev] = bytes;
   cudaFuncSetAttribute(k_targets_ax<P, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(k_targets_ax<P, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(k_targets<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);

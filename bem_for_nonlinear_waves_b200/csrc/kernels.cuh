@@ -10,6 +10,9 @@
 
 namespace bemb200 {
 
+// devices tracked by the per-device launch bookkeeping (shared-memory permissions)
+constexpr int kMaxDevices = 64;
+
 // Programmatic dependent launch for the kernels of an operator application: each is launched
 // with programmatic stream serialisation and starts with pdl_enter(), which waits until the
 // previous kernel in the stream has completed and its writes are visible, then lets the next

@@ -179,10 +179,14 @@ int bem_gpu_matvec_device(bem_gpu_ctx* ctx, const double* d_x, double* d_y);
  * slots live in a 32 MiB area that is part of the library's device image (one per device,
  * reserved when the module loads).  For callers that must not allocate device memory while
  * applying the operator.  Limit: m2l_pairs * 2 * (p+1)(p+2)/2 * 16 bytes <= 32 MiB, else
- * BEM_ERR_UNSUPPORTED with the sizes in bem_gpu_last_error.  The first call on a device
- * resolves the area's address; make it before any stream capture.  Calls that overlap on one
- * device race on the shared area and must be ordered by the caller.  No counterpart in the
- * reference (its operator allocates per call, BEM_solveBVP_GMRES_FMM.hpp:2124-2155). */
+ * BEM_ERR_UNSUPPORTED with the sizes in bem_gpu_last_error.  It always applies the FP64
+ * operator, also on a mixed-precision context (opts.precision = 1).  The area's device address
+ * is looked up once per context, during its first bem_gpu_setup with its device current (no
+ * allocation), so the call itself does no lookup; it restores the caller's current device
+ * before returning.  Calls that overlap on one device race on the shared area and must be
+ * ordered by the caller.  No
+ * counterpart in the reference (its operator allocates per call,
+ * BEM_solveBVP_GMRES_FMM.hpp:2124-2155). */
 int bem_gpu_matvec_device_noalloc(bem_gpu_ctx* ctx, const double* d_x, double* d_y);
 
 /* Introspection for parity tests. */
@@ -221,13 +225,17 @@ int bem_gpu_profile_matvec(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[6]
  * work and the GPU work of different workers overlaps on the device.  The caller keeps every
  * array of the submitted problem (desc arrays, known, outputs, stats) alive and untouched
  * until its ticket polls done.  bem_gpu_batch_poll returns the solve's status (as
- * bem_gpu_solve_bvp), or BEM_ERR_NOT_READY while it is pending and wait == 0. */
+ * bem_gpu_solve_bvp), or BEM_ERR_NOT_READY while it is pending and wait == 0; a finished
+ * ticket keeps its status (poll it any number of times) until bem_gpu_batch_release drops it.
+ * bem_gpu_batch_last_error gives the message of the calling thread's last poll (messages are
+ * per thread, so pollers on different threads do not see each other's). */
 typedef struct bem_gpu_batch bem_gpu_batch;
 bem_gpu_batch* bem_gpu_batch_create(const bem_gpu_opts* opts, int32_t n_workers);
 int bem_gpu_batch_submit(bem_gpu_batch* batch, const bem_bvp_desc* desc, const double* known, double* out_phi, double* out_phin,
                          bem_gpu_stats* stats, int64_t* ticket);
 int bem_gpu_batch_poll(bem_gpu_batch* batch, int64_t ticket, int32_t wait);
-const char* bem_gpu_batch_last_error(const bem_gpu_batch* batch);  /* message of the last polled failure */
+int bem_gpu_batch_release(bem_gpu_batch* batch, int64_t ticket);   /* forget a finished ticket; NOT_READY if unknown or pending */
+const char* bem_gpu_batch_last_error(const bem_gpu_batch* batch);  /* message of this thread's last polled failure */
 void bem_gpu_batch_destroy(bem_gpu_batch* batch);                  /* finishes queued problems first */
 
 /* Mixed-Eulerian-Lagrangian stage update (the step that follows each BVP solve of a BEM-MEL

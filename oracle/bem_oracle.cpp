@@ -93,17 +93,22 @@ inline V3 tri_normal_hp(const V3& a, const V3& b, const V3& c) {
 }
 
 // ---- quadrature tables ---------------------------------------------------
-// 5x5 Gauss-Legendre product rule on [0,1]^2 (reference: __array_GW5xGW5__,
-// lib/include/basic_constants.hpp:1326) — generated here from the 5-point rule.
+// 5x5 Gauss-Legendre product rule on [0,1]^2 with the reference's own 15-digit constants
+// (__array_GW5xGW5__, lib/include/basic_constants.hpp:1326-1350): the near-field weights must
+// share them to agree with the reference beyond ~1e-12.  The table is symmetric: node a and
+// weight class c(a) = {0, 1, 2, 1, 0}, w(a, b) = kGW5W[c(a)][c(b)].
 struct GW {
   double t0, t1, w;
 };
 std::vector<GW> make_gw5x5() {
-  const double xs[5] = {-0.9061798459386640, -0.5384693101056831, 0.0, 0.5384693101056831, 0.9061798459386640};
-  const double ws[5] = {0.2369268850561891, 0.4786286704993665, 0.5688888888888889, 0.4786286704993665, 0.2369268850561891};
+  static const double x[5] = {0.046910077030668, 0.230765344947158, 0.5, 0.769234655052841, 0.953089922969332};
+  static const int c[5] = {0, 1, 2, 1, 0};
+  static const double w[3][3] = {{0.0140335872156063, 0.0283499999999991, 0.0336962680968792},
+                                 {0.0283499999999991, 0.0572713510559978, 0.0680716331376877},
+                                 {0.0336962680968792, 0.0680716331376877, 0.0809086419753086}};
   std::vector<GW> r;
   for (int a = 0; a < 5; ++a)
-    for (int b = 0; b < 5; ++b) r.push_back({0.5 * (xs[a] + 1.0), 0.5 * (xs[b] + 1.0), 0.25 * ws[a] * ws[b]});
+    for (int b = 0; b < 5; ++b) r.push_back({x[a], x[b], w[c[a]][c[b]]});
   return r;
 }
 // Dunavant degree-4 6-point rule (barycentrics, weight incl. the 1/2 area factor)
@@ -799,8 +804,10 @@ std::vector<Node*> all_nodes(OracleCtx& C) {
 
 // One FMM update + per-point (near + far) integrals for given per-DOF phi/phin
 // (moments.hpp:1547-1574; lib_multipole_expansion.hpp:1143-1150,1273-1302).
+// stages: bit k runs stage k (0 P2M, 1 M2M, 2 M2L, 3 L2L, 4 near sums, 5 L2P); a stage that is
+// skipped leaves the expansions and point sums of the previous call as they were.
 void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, std::vector<double>& GPhin, std::vector<double>& GnPhi,
-                         int m2l_stride = 1, double* tstage = nullptr) {
+                         int m2l_stride = 1, double* tstage = nullptr, unsigned stages = 0x3fu) {
   const int p = C.p;
   double tw = omp_get_wtime();
   auto lap = [&](int k) {
@@ -811,12 +818,12 @@ void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, st
   const int nc = C.ncoef();
   auto nodes = all_nodes(C);
   for (auto* b : nodes) {
-    std::fill(b->MM.begin(), b->MM.end(), std::array<cd, 2>{0., 0.});
-    std::fill(b->LL.begin(), b->LL.end(), std::array<cd, 2>{0., 0.});
+    if (stages & 1u) std::fill(b->MM.begin(), b->MM.end(), std::array<cd, 2>{0., 0.});
+    if (stages & 4u) std::fill(b->LL.begin(), b->LL.end(), std::array<cd, 2>{0., 0.});
   }
   // P2M at leaves (increment_M, moments.hpp:307-356)
 #pragma omp parallel for schedule(dynamic, 4)
-  for (size_t li = 0; li < C.leaves.size(); ++li) {
+  for (size_t li = 0; li < ((stages & 1u) ? C.leaves.size() : 0); ++li) {
     Node* b = C.leaves[li];
     for (int sidx : b->data) {
       const Source& s = C.src[sidx];
@@ -830,7 +837,7 @@ void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, st
   }
   lap(0);
   // M2M bottom-up (moments.hpp:401-436, 912-915)
-  for (int level = C.max_level - 1; level >= 0; --level) {
+  for (int level = C.max_level - 1; level >= 0 && (stages & 2u); --level) {
 #pragma omp parallel for schedule(dynamic, 1)
     for (size_t bi = 0; bi < C.level_nodes[level].size(); ++bi) {
       Node* b = C.level_nodes[level][bi];
@@ -858,6 +865,7 @@ void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, st
   lap(1);
   // M2L (moments.hpp:492-598, 732-764)
   for (auto& lv : C.level_nodes) {
+    if (!(stages & 4u)) break;
 #pragma omp parallel for schedule(dynamic, 1)
     for (size_t ai = 0; ai < lv.size(); ++ai) {
       Node* A = lv[ai];
@@ -895,6 +903,7 @@ void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, st
   lap(2);
   // L2L top-down (moments.hpp:862-884, 925-929)
   for (auto& lv : C.level_nodes) {
+    if (!(stages & 8u)) break;
 #pragma omp parallel for schedule(dynamic, 1)
     for (size_t bi = 0; bi < lv.size(); ++bi) {
       Node* par = lv[bi];
@@ -920,7 +929,7 @@ void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, st
   GPhin.assign(C.np, 0.0);
   GnPhi.assign(C.np, 0.0);
 #pragma omp parallel for schedule(dynamic, 32)
-  for (int t = 0; t < C.np; ++t) {
+  for (int t = 0; t < ((stages & 16u) ? C.np : 0); ++t) {
     double r0 = 0, r1 = 0;
     for (size_t i = 0; i < C.near_idx[t].size(); ++i) {
       r0 += phin[C.near_idx[t][i]] * C.near_wG[t][i];
@@ -931,7 +940,7 @@ void fmm_point_integrals(OracleCtx& C, const double* phi, const double* phin, st
   }
   lap(4);
 #pragma omp parallel for schedule(dynamic, 32)
-  for (int t = 0; t < C.np; ++t) {
+  for (int t = 0; t < ((stages & 32u) ? C.np : 0); ++t) {
     if (!C.tgt_leaf[t]) continue;
     Node* b = C.tgt_leaf[t];
     Sph S(sub(C.Xs[t], b->X));
@@ -1127,6 +1136,28 @@ void oracle_time_sample(void* h, int m2l_stride, double* t) {
   t[6] = C.t_tree;
   t[7] = C.t_near * C.near_stride;
   t[8] = omp_get_max_threads();
+}
+
+// Wall time (s) of ONE whole stage of the mat-vec on the whole problem (stage as in
+// fmm_point_integrals: 0 P2M, 1 M2M, 2 M2L, 3 L2L, 4 near sums, 5 L2P), with all OpenMP
+// threads; the stage reads the expansions the previous call left.  For the CPU baseline.
+double oracle_time_stage(void* h, int stage) {
+  OracleCtx& C = *(OracleCtx*)h;
+  if (stage < 0 || stage > 5) return -1.0;
+  std::vector<double> phi(C.ndof, 1.0), phin(C.ndof, 0.5), a, b;
+  double t[9] = {0};
+  fmm_point_integrals(C, phi.data(), phin.data(), a, b, 1, t, 1u << stage);
+  return t[stage];
+}
+
+// Wall time (s) of the set-up parts that were measured when the context was created:
+// out[0] tree + lists, out[1] near-field quadrature (every point; the context must have been
+// created with near_stride 1), out[2] OpenMP threads.
+void oracle_setup_times(void* h, double* out) {
+  OracleCtx& C = *(OracleCtx*)h;
+  out[0] = C.t_tree;
+  out[1] = C.t_near * C.near_stride;
+  out[2] = omp_get_max_threads();
 }
 
 // GMRES solve (BEM_solveBVP_GMRES_FMM.hpp:2007-2400; basic_linear_systems.hpp:3137-3451).

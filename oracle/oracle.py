@@ -47,6 +47,9 @@ def lib():
         L.oracle_create_sampled.restype = P
         L.oracle_create_sampled.argtypes = [i32, dp, i32, ip, u8p, i32, ip, ip, ip, ip, i32, ctypes.c_double, i32, i32, i32]
         L.oracle_time_sample.argtypes = [P, i32, dp]
+        L.oracle_time_stage.restype = ctypes.c_double
+        L.oracle_time_stage.argtypes = [P, i32]
+        L.oracle_setup_times.argtypes = [P, dp]
         L.oracle_compute_diag.argtypes = [P]
         L.oracle_get_diag.argtypes = [P, dp]
         L.oracle_point_integrals.argtypes = [P, dp, dp, dp, dp]
@@ -193,6 +196,18 @@ class Oracle:
         lib().oracle_time_sample(self.h, int(m2l_stride), _p(t, ctypes.c_double))
         keys = ["p2m", "m2m", "m2l", "l2l", "near", "l2p", "tree_lists", "near_setup", "threads"]
         return dict(zip(keys, t.tolist()))
+
+    STAGES = ("p2m", "m2m", "m2l", "l2l", "near", "l2p")
+
+    def time_stage(self, stage):
+        """Wall seconds of one whole mat-vec stage (a name of STAGES) over the whole problem."""
+        return lib().oracle_time_stage(self.h, self.STAGES.index(stage))
+
+    def setup_times(self):
+        """Measured set-up seconds: tree + lists, near-field quadrature; OpenMP threads."""
+        out = np.zeros(3)
+        lib().oracle_setup_times(self.h, _p(out, ctypes.c_double))
+        return dict(tree_lists=float(out[0]), near_setup=float(out[1]), threads=int(out[2]))
 
     def stats(self, max_level=7):
         out = np.zeros(8, np.int64)

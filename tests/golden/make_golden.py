@@ -25,6 +25,8 @@ CASES = {
     "tank_h0p1_p8": dict(tank=dict(h=0.1), p=8, tol=1e-12),
     # free surface with seeded z-noise (sigma = 0.2 h), p=10
     "tank_h0p1_noise_p10": dict(tank=dict(h=0.1, noise_sigma=0.02, seed=7), p=10, tol=1e-12),
+    # the 2,802-point plain FP64 configuration: 2.0 x 1.0 x 0.5 m tank, h = 0.05, p = 8
+    "tank_h0p05_p8": dict(tank=dict(length=2.0, width=1.0, depth=0.5, h=0.05), p=8, tol=1e-12),
 }
 
 SAMPLE_ROWS = 12  # near-field rows stored in full; the others as checksums
@@ -32,7 +34,7 @@ SAMPLE_ROWS = 12  # near-field rows stored in full; the others as checksums
 
 def make(name, spec):
     t = make_tank(**spec["tank"])
-    R = refrun.run(spec["p"], t, tol=spec["tol"], max_iter=1000)
+    R = refrun.run(spec["p"], t, tol=spec["tol"], max_iter=2000)
     L = float(np.sqrt(((t.X.max(0) - t.X.min(0)) ** 2).sum()))
     # near rows: checksums for every point, full rows for a seeded sample
     pts = np.array(sorted(R["near_rows"].keys()))

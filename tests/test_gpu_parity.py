@@ -1,6 +1,8 @@
 """CUDA path (lib/libbem_b200.so through its C ABI) against the reference's golden outputs
 and the oracle.  Tolerances: FP64 everywhere; near weights and single mat-vecs agree to
-rounding (1e-11 relative to the row/vector maximum), solutions to 1e-9 relative with both
+rounding (1e-11 relative to the row/vector maximum; near-row checksums 1e-11 against the
+reference, which uses the same 15-digit 5x5 Gauss-Legendre constants), solutions to 1e-10
+relative -- the parity bar for the plain FP64 path at the same order and tree -- with both
 sides solved to an absolute residual of 1e-12."""
 import numpy as np
 import pytest
@@ -49,7 +51,7 @@ def test_gpu_near_weights_match_reference_checksums(case):
         idx, wg, wgn = bvp.near_row(p)
         assert len(idx) == z["near_count"][i]
         np.testing.assert_allclose(wg.sum(), z["near_sum_g"][i], rtol=1e-11, atol=1e-14)
-        np.testing.assert_allclose(wgn.sum(), z["near_sum_gn"][i], rtol=1e-9, atol=1e-11)
+        np.testing.assert_allclose(wgn.sum(), z["near_sum_gn"][i], rtol=1e-11, atol=1e-11 * np.abs(wgn).sum())
 
 
 def test_gpu_diag_matches_reference(case):
@@ -81,7 +83,7 @@ def test_gpu_solution_matches_reference(case):
     assert bvp.last_gmres_converged, bvp.last_gmres_residual_norm
     ref = g.solution(d)
     err = np.abs(bvp.ans - ref).max() / np.abs(ref).max()
-    assert err <= 1e-9, err
+    assert err <= 1e-10, err
     # known values pass through unchanged
     kind = d["dof_kind"]
     np.testing.assert_array_equal(bvp.phi[kind == 0], kv[kind == 0])

@@ -40,7 +40,7 @@ def test_oracle_near_rows_match_reference(golden_case):
         assert len(idx) == z["near_count"][i]
         np.testing.assert_allclose(wg.sum(), z["near_sum_g"][i], rtol=1e-11, atol=1e-14)
         np.testing.assert_allclose(np.abs(wg).sum(), z["near_sumabs_g"][i], rtol=1e-11)
-        np.testing.assert_allclose(wgn.sum(), z["near_sum_gn"][i], rtol=1e-9, atol=1e-11)
+        np.testing.assert_allclose(wgn.sum(), z["near_sum_gn"][i], rtol=1e-11, atol=1e-11 * np.abs(wgn).sum())
     off = z["sample_off"]
     for k, p in enumerate(z["sample_points"]):
         ridx = ours[z["sample_idx"][off[k]:off[k + 1]]]
@@ -54,25 +54,29 @@ def test_oracle_near_rows_match_reference(golden_case):
 
 def test_oracle_diag_matches_reference(golden_case):
     g, d, o = golden_case
-    np.testing.assert_allclose(o.compute_diag(), g.diag(d), rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(o.compute_diag(), g.diag(d), rtol=1e-13, atol=1e-13)
 
 
 def test_oracle_matvec_matches_reference(golden_case):
     g, d, o = golden_case
     phi, phin, expect = g.matvec_input(d)
     got = o.apply(phi, phin)
-    assert np.abs(got - expect).max() <= 1e-11 * np.abs(expect).max()
+    assert np.abs(got - expect).max() <= 2e-12 * np.abs(expect).max()
 
 
 @pytest.mark.slow
 def test_oracle_solution_matches_reference(golden_case):
     g, d, o = golden_case
+    if g.tank.X.shape[0] > 1000:
+        # the 2,802-point golden takes the CPU oracle ~6 minutes (it passes at 1e-10); the CPU
+        # suite keeps to the small tanks and the GPU parity tests cover every golden
+        pytest.skip("large golden: solution parity checked by the GPU tests")
     kv = known_values(g.tank, d["dof_point"], d["dof_face"], d["dof_kind"], point_normals(g.tank))
     phi, phin, st = o.solve(kv, tol=g.tol, max_iter=1000)
     assert st["converged"]
     sol = np.where(d["dof_kind"] == 0, phin, phi)
     ref = g.solution(d)
-    assert np.abs(sol - ref).max() <= 1e-9 * np.abs(ref).max()
+    assert np.abs(sol - ref).max() <= 1e-10 * np.abs(ref).max()
 
 
 @pytest.mark.parametrize("p,bound", [(4, 2e-4), (8, 5e-9), (12, 5e-12)])
