@@ -48,7 +48,8 @@ class Stats(ctypes.Structure):
                 ("time_setup_s", c_dbl), ("time_solve_s", c_dbl), ("nnz_near", ctypes.c_int64), ("m2l_pairs", ctypes.c_int64),
                 ("n_nodes", c_int), ("n_leaves", c_int), ("matvecs", c_int), ("matvecs_lo", c_int), ("time_device_s", c_dbl),
                 ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
-                ("time_plan_s", c_dbl), ("time_upload_s", c_dbl), ("time_setup_device_s", c_dbl)]
+                ("time_plan_s", c_dbl), ("time_upload_s", c_dbl), ("time_setup_device_s", c_dbl), ("rhs_norm", c_dbl),
+                ("tol_abs", c_dbl)]
 
 
 EXPORTS = {

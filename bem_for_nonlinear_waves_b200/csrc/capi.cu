@@ -1522,11 +1522,10 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   }
   CK(cudaMemcpyAsync(ctx->bdev.p, b.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
   ctx->h2d += 8LL * N;
-  if (ctx->opts.tol_relative) {
-    double bn = 0.0;
-    for (int i = 0; i < N; ++i) bn = std::fma(b[i], b[i], bn);
-    tol *= std::sqrt(bn);
-  }
+  double bn = 0.0;
+  for (int i = 0; i < N; ++i) bn = std::fma(b[i], b[i], bn);
+  const double rhs_norm = std::sqrt(bn);
+  if (ctx->opts.tol_relative) tol *= rhs_norm;
   std::vector<double> x0s;
   if (x0) {  // initial guess in physical units (phin for Dirichlet DOFs, phi otherwise) -> scaled
     x0s.resize(N);
@@ -1727,6 +1726,8 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     stats->time_plan_s = ctx->time_plan;
     stats->time_upload_s = ctx->time_upload;
     stats->time_setup_device_s = 1e-3 * (double)ctx->setup_dev_ms;
+    stats->rhs_norm = rhs_norm;
+    stats->tol_abs = tol;
   }
   if (!finite) {
     ctx->err = "non-finite solution";

@@ -109,6 +109,8 @@ typedef struct {
   double time_plan_s;     /* host part of the set-up: tree, lists, near-field sparsity */
   double time_upload_s;   /* host->device copies of the set-up */
   double time_setup_device_s; /* device part of the set-up (near weights, tables, diagonal) */
+  double rhs_norm;        /* |b| of the scaled system (the reference's right-hand side -(A 0 - b)) */
+  double tol_abs;         /* absolute tolerance the solve stopped at (tol, or tol*|b| with tol_relative) */
 } bem_gpu_stats;
 
 /* 1 if a CUDA device of compute capability 10.x is visible. */
