@@ -244,6 +244,15 @@ class BEM_BVP:
         keys = ["nodes", "leaves", "depth", "n_added", "m2l_pairs", "near_pairs", "nnz", "near_blocks", "m2l_chunks", "m2l_groups"]
         return {k: int(v) for k, v in zip(keys, out)}
 
+    def near_bytes(self):
+        """Algorithmic bytes of one near-field SpMV of A.x: stored weight blocks in FP64 and in FP32
+        (rows padded to 4 columns), the gathered unknowns (8 B per block column) and the rows
+        written (8 B per DOF)."""
+        out = np.zeros(6, np.int64)
+        self._check(self.lib.bem_gpu_near_stats(self.ctx, L.ptr(out, L.P_i64)), "near_stats")
+        return {"weights_fp64": 8 * int(out[0]), "weights_fp32": 4 * int(out[1]), "x_gather": 8 * int(out[2]),
+                "rows": 8 * int(out[5]), "blocks": int(out[3]), "targets": int(out[4])}
+
     def matvec_time_ms(self, repeats=10):
         return self.profile_matvec(repeats)["total"]
 

@@ -1311,6 +1311,26 @@ int bem_gpu_face_leaf(bem_gpu_ctx* ctx, int32_t* level, double* corner) {
   return BEM_OK;
 }
 
+int bem_gpu_near_stats(bem_gpu_ctx* ctx, int64_t* out) {
+  if (!ctx || !out) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ctx->ready) return BEM_ERR_NOT_READY;
+  const Plan& P = ctx->plan;
+  int64_t w = 0, w4 = 0, cols = 0, tg = 0;
+  for (const Plan::NearBlock& b : P.blocks) {
+    w += (int64_t)b.ntgt * b.ndof;
+    w4 += (int64_t)b.ntgt * ((b.ndof + 3) & ~3);
+    cols += b.ndof;
+    tg += b.ntgt;
+  }
+  out[0] = w;
+  out[1] = w4;
+  out[2] = cols;
+  out[3] = (int64_t)P.blocks.size();
+  out[4] = tg;
+  out[5] = P.ndof;
+  return BEM_OK;
+}
+
 int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out) {
   if (!ctx || !out) return BEM_ERR_INVALID_ARGUMENT;
   if (!ctx->ready) return BEM_ERR_NOT_READY;

@@ -197,6 +197,10 @@ double bem_gpu_scale_factor(const bem_gpu_ctx* ctx);                  /* L */
 int bem_gpu_near_row(bem_gpu_ctx* ctx, int32_t point, int32_t cap, int32_t* dof, double* wG, double* wGn);
 int bem_gpu_face_leaf(bem_gpu_ctx* ctx, int32_t* level, double* corner); /* [n_faces], [3*n_faces] */
 int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out /*[10]: nodes, leaves, depth, added, m2l pairs, near pairs, nnz, near blocks, M2L chunks, M2L translation groups*/);
+/* Near-field block sizes of the A.x kernel: out[6] = stored FP64 weights (sum over blocks of
+ * targets x DOF columns), FP32 weights (rows padded to 4 columns), DOF columns gathered (sum
+ * over blocks), blocks, targets, DOFs. */
+int bem_gpu_near_stats(bem_gpu_ctx* ctx, int64_t* out /*[6]*/);
 
 /* Host-only inspection of the set-up plan (no GPU needed): builds the octree, lists and
  * near-field sparsity for desc with opts and reports, per face, the level and lower corner
