@@ -73,6 +73,7 @@ EXPORTS = {
     "bem_gpu_face_leaf": (c_int, [ctypes.c_void_p, P_int, P_dbl]),
     "bem_gpu_tree_stats": (c_int, [ctypes.c_void_p, P_i64]),
     "bem_gpu_near_stats": (c_int, [ctypes.c_void_p, P_i64]),
+    "bem_gpu_set_wait_limit": (c_int, [ctypes.c_void_p, ctypes.c_int64]),
     "bem_gpu_profile_matvec": (c_int, [ctypes.c_void_p, c_int, P_dbl]),
     "bem_gpu_matvec_device_mixed": (c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "bem_gpu_profile_matvec_mixed": (c_int, [ctypes.c_void_p, c_int, P_dbl]),

@@ -129,6 +129,7 @@ struct bem_gpu_ctx {
   // set-up with the device current (nullptr: not looked up yet, or the lookup failed)
   void* noalloc_slots = nullptr;
   cudaError_t noalloc_lookup = cudaSuccess;
+  uint32_t tc_wait_tries = tc_default_wait_tries();  // bem_gpu_set_wait_limit
 
   // geometry / tree
   DBuf<double> Xs, e_q, e_W, e_n, e_near, node_X, WG, WGn, Wc, diag;
@@ -149,7 +150,7 @@ struct bem_gpu_ctx {
   DBuf<double> ftab_vec;
   DBuf<double2> M, L;
   std::vector<int> level_parent_off;
-  int n_m2l_targets = 0, max_ntgt = 0, chunk = 0;
+  int n_m2l_targets = 0, max_ntgt = 0, chunk = 0, chunk_ax = 0;
   int64_t w4_total = 0;  // size of the row-padded FP32 near weights
   int n_tc_items = 0;    // tensor-core work items (every table-row-tile image's pair chunks)
   // state
@@ -262,6 +263,7 @@ struct bem_gpu_ctx {
     a.L = L.p;
     a.n_blocks = (int)plan.blocks.size();
     a.chunk = chunk;
+    a.chunk_ax = chunk_ax;
     a.max_ntgt = max_ntgt;
     a.blocks = blocks.p;
     a.nb_dofs = nb_dofs.p;
@@ -317,6 +319,7 @@ struct bem_gpu_ctx {
     a.tc_escale = tc_escale.p;
     a.tc_Y = reinterpret_cast<float*>(Y.p);
     a.tc_err = tc_err.p;
+    a.tc_wait_tries = tc_wait_tries;
     a.node_dL = node_dL.p;
     a.tc_alpha = tc_alpha.p;
     a.tc_rows_map = tc_map.data();
@@ -902,7 +905,10 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   }
   // a multiple of 4 columns (the FP32 rows are read 4 columns at a time)
   ctx->chunk = std::min((max_ndof + 3) & ~3, ((smem_cap - ctx->max_ntgt * 16) / 16) & ~3);
-  configure_targets_smem(P.opt.p, (ctx->chunk + ctx->max_ntgt) * 16);
+  // k_targets_ax stages at most 4,096 x values at a time (32 KB, so several CTAs share an SM)
+  ctx->chunk_ax = std::min((max_ndof + 3) & ~3, 4096);
+  const int ax_bytes = 8 * (ctx->chunk_ax + ctx->max_ntgt * 8);
+  configure_targets_smem(P.opt.p, std::max((ctx->chunk + ctx->max_ntgt) * 16, ax_bytes));
   configure_m2l_smem(P.opt.p);
 
 
@@ -1836,6 +1842,17 @@ int bem_gpu_matvec_device_mixed(bem_gpu_ctx* ctx, const double* d_x, double* d_y
     return BEM_ERR_UNSUPPORTED;
   }
   return matvec_lo(ctx, d_x, d_y);
+}
+
+int bem_gpu_set_wait_limit(bem_gpu_ctx* ctx, int64_t tries) {
+  if (!ctx) return BEM_ERR_INVALID_ARGUMENT;
+  ctx->tc_wait_tries = tries < 0 ? tc_default_wait_tries() : (uint32_t)std::min<int64_t>(tries, 0xffffffffLL);
+  if (!ctx->ready) return BEM_OK;
+  CK(cudaSetDevice(ctx->opts.device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->mixed) CK(cudaMemsetAsync(ctx->tc_err.p, 0, sizeof(int), ctx->stream));
+  // the limit is a kernel argument: recapture the operator graphs that launch the contraction
+  return build_graph(ctx);
 }
 
 int bem_gpu_check_device_status(bem_gpu_ctx* ctx) {

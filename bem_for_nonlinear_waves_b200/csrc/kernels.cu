@@ -716,72 +716,131 @@ __global__ void __launch_bounds__(128) k_targets(const NearBlockDev* __restrict_
 // Wc = [Dirichlet] WG - [other] WGn (half the weight bytes of the general kernel), read
 // straight from the unknown vector x; the far field is the L2P of the combined local
 // expansion L[0]; a CORNER row is its own unknown (phi_i = x_i).
+//
+// HBM-bound: the weight blocks are read once per application (375 MB in FP32 at tank_60k,
+// about 11 rows x 1,550 columns = 67 KB per block).  One CTA of kAxThreads per near block:
+// the block's x values are gathered into shared memory, then every thread takes column
+// groups (4 FP32 columns = one 16-byte load, or 1 FP64 column) strided over the CTA and
+// kAxRows rows at a time, kAxRows x kAxUnroll independent loads in flight per thread; each
+// x value is read from shared memory once per row group.  Per-row partial sums go through a
+// warp reduction into per-(row, warp) slots and are summed in warp order (fixed order, no
+// atomics); then one warp per target adds the L2P of the bucket's local expansion and
+// writes the target's rows.
+constexpr int kAxThreads = 256;
+constexpr int kAxWarps = kAxThreads / 32;
+constexpr int kAxRows = 4;
+template <typename WT>
+struct AxVec {
+  static constexpr int cols = 4;  // FP32: a 16-byte load carries 4 columns (rows padded to 4)
+  static constexpr int unroll = 2;
+};
+template <>
+struct AxVec<double> {
+  static constexpr int cols = 1;  // FP64 rows are not padded: one column per load
+  static constexpr int unroll = 4;
+};
+
+// dynamic shared memory of k_targets_ax: the x chunk and the per-(row, warp) partial sums
+inline size_t ax_smem_bytes(const MatvecArgs& a) { return sizeof(double) * ((size_t)a.chunk_ax + (size_t)a.max_ntgt * kAxWarps); }
+
 template <int P, typename WT>
-__global__ void __launch_bounds__(128) k_targets_ax(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs,
-                                                    const int* __restrict__ nb_targets, const WT* __restrict__ Wc,
-                                                    const double* __restrict__ Xs, const double* __restrict__ node_X,
-                                                    const double2* __restrict__ L, const double* __restrict__ x,
-                                                    const int* __restrict__ point_dof_off, const int* __restrict__ point_dof,
-                                                    const int* __restrict__ dof_kind, const double* __restrict__ diag,
-                                                    double* __restrict__ rows, int chunk) {
+__global__ void __launch_bounds__(kAxThreads, 2) k_targets_ax(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs,
+                                                              const int* __restrict__ nb_targets, const WT* __restrict__ Wc,
+                                                              const double* __restrict__ Xs, const double* __restrict__ node_X,
+                                                              const double2* __restrict__ L, const double* __restrict__ x,
+                                                              const int* __restrict__ point_dof_off, const int* __restrict__ point_dof,
+                                                              const int* __restrict__ dof_kind, const double* __restrict__ diag,
+                                                              double* __restrict__ rows, int chunk) {
   pdl_enter();
   constexpr int NC = ncoef(P);
+  constexpr int VC = AxVec<WT>::cols, UN = AxVec<WT>::unroll;
   extern __shared__ double2 smem[];
-  double* xs = reinterpret_cast<double*>(smem);  // [chunk] x of the block's DOFs
-  double* accs = xs + chunk;                      // [ntgt] near sums
+  double* xs = reinterpret_cast<double*>(smem);  // [chunk] x of the block's DOF columns (chunk: a multiple of 4)
+  double* part = xs + chunk;  // [ntgt][kAxWarps] per-warp partial row sums
   __shared__ double2 sL[NC];
   __shared__ double sHalf[P + 1], sRec[(P + 1) * (P + 1)];  // 1/(2k), 1/(n^2 - m^2) of the L2P recurrence
-  for (int i = threadIdx.x; i < (P + 1) * (P + 1); i += blockDim.x) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < (P + 1) * (P + 1); i += kAxThreads) {
     const int n = i / (P + 1), m = i - n * (P + 1);
     sRec[i] = n > m ? 1.0 / double(n * n - m * m) : 0.0;
     if (i <= P) sHalf[i] = i > 0 ? 1.0 / (2.0 * i) : 0.0;
   }
   const NearBlockDev B = blocks[blockIdx.x];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nwarp = blockDim.x >> 5;
   if (L)  // L == nullptr: the near-field part of the operator only (no L2P)
-    for (int i = threadIdx.x; i < NC; i += blockDim.x) sL[i] = L[(size_t)B.node * 2 * NC + i];
-  for (int i = threadIdx.x; i < B.ntgt; i += blockDim.x) accs[i] = 0.0;
+    for (int i = tid; i < NC; i += kAxThreads) sL[i] = L[(size_t)B.node * 2 * NC + i];
+  for (int i = tid; i < B.ntgt * kAxWarps; i += kAxThreads) part[i] = 0.0;
+  const int stride = VC == 4 ? ((B.ndof + 3) & ~3) : B.ndof;
+  const WT* Wb = Wc + (VC == 4 ? B.w4_off : B.w_off);
   for (int c0 = 0; c0 < B.ndof; c0 += chunk) {
-    const int cn = min(chunk, B.ndof - c0);
+    const int cn = min(chunk, B.ndof - c0), cnv = (cn + VC - 1) / VC * VC;
+    __syncthreads();  // the previous chunk's x values are no longer read
+    for (int i = tid; i < cnv; i += kAxThreads) xs[i] = i < cn ? x[nb_dofs[B.dof_off + c0 + i]] : 0.0;
     __syncthreads();
-    if constexpr (std::is_same<WT, float>::value) {
-      // four planes: column c at xs[(c % 4) * chunk / 4 + c / 4], so that the lanes reading
-      // consecutive groups of 4 columns hit consecutive words; the tail of the last group is 0
-      const int q = chunk >> 2, cn4 = (cn + 3) & ~3;
-      for (int i = threadIdx.x; i < cn4; i += blockDim.x) xs[(i & 3) * q + (i >> 2)] = i < cn ? x[nb_dofs[B.dof_off + c0 + i]] : 0.0;
-    } else {
-      for (int i = threadIdx.x; i < cn; i += blockDim.x) xs[i] = x[nb_dofs[B.dof_off + c0 + i]];
-    }
-    __syncthreads();
-    for (int tl = warp; tl < B.ntgt; tl += nwarp) {
-      double s0 = 0.0;
-      if constexpr (std::is_same<WT, float>::value) {
-        // padded rows: chunk and row starts are multiples of 4 columns, so 16-byte loads
-        const int stride = (B.ndof + 3) & ~3;
-        const float4* w4 = reinterpret_cast<const float4*>(Wc + B.w4_off + (int64_t)tl * stride + c0);
-        const int n4 = (cn + 3) >> 2, qs = chunk >> 2;
-        double s1 = 0.0;
-        for (int i = lane; i < n4; i += 32) {
-          const float4 q = __ldcs(w4 + i);
-          s0 = fma((double)q.x, xs[i], s0);
-          s1 = fma((double)q.y, xs[qs + i], s1);
-          s0 = fma((double)q.z, xs[2 * qs + i], s0);
-          s1 = fma((double)q.w, xs[3 * qs + i], s1);
+    const int ng = cnv / VC;  // column groups of this chunk
+    for (int r0 = 0; r0 < B.ntgt; r0 += kAxRows) {
+      const int nr = min(kAxRows, B.ntgt - r0);
+      double acc[kAxRows];
+#pragma unroll
+      for (int r = 0; r < kAxRows; ++r) acc[r] = 0.0;
+      for (int g0 = tid; g0 < ng; g0 += kAxThreads * UN) {
+        if constexpr (VC == 4) {
+          float4 w[UN][kAxRows];
+#pragma unroll
+          for (int u = 0; u < UN; ++u)
+#pragma unroll
+            for (int r = 0; r < kAxRows; ++r) {
+              const int g = g0 + u * kAxThreads;
+              w[u][r] = (g < ng && r < nr)
+                            ? __ldcs(reinterpret_cast<const float4*>(Wb + (int64_t)(r0 + r) * stride + c0) + g)
+                            : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+          for (int u = 0; u < UN; ++u) {
+            const int g = g0 + u * kAxThreads;
+            if (g < ng) {
+              const double2 xa = *reinterpret_cast<const double2*>(xs + 4 * g);
+              const double2 xb = *reinterpret_cast<const double2*>(xs + 4 * g + 2);
+#pragma unroll
+              for (int r = 0; r < kAxRows; ++r) {
+                acc[r] = fma((double)w[u][r].x, xa.x, acc[r]);
+                acc[r] = fma((double)w[u][r].y, xa.y, acc[r]);
+                acc[r] = fma((double)w[u][r].z, xb.x, acc[r]);
+                acc[r] = fma((double)w[u][r].w, xb.y, acc[r]);
+              }
+            }
+          }
+        } else {
+          double w[UN][kAxRows];
+#pragma unroll
+          for (int u = 0; u < UN; ++u)
+#pragma unroll
+            for (int r = 0; r < kAxRows; ++r) {
+              const int g = g0 + u * kAxThreads;
+              w[u][r] = (g < ng && r < nr) ? __ldcs(Wb + (int64_t)(r0 + r) * stride + c0 + g) : 0.0;
+            }
+#pragma unroll
+          for (int u = 0; u < UN; ++u) {
+            const int g = g0 + u * kAxThreads;
+            if (g < ng) {
+              const double xv = xs[g];
+#pragma unroll
+              for (int r = 0; r < kAxRows; ++r) acc[r] = fma(w[u][r], xv, acc[r]);
+            }
+          }
         }
-        s0 += s1;
-      } else {
-        const WT* w = Wc + B.w_off + (int64_t)tl * B.ndof + c0;
-        for (int i = lane; i < cn; i += 32) s0 = fma((double)w[i], xs[i], s0);
       }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-      if (lane == 0) accs[tl] += s0;
+      for (int r = 0; r < kAxRows; ++r) {
+        double v = acc[r];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && r < nr) part[(r0 + r) * kAxWarps + warp] += v;
+      }
     }
   }
   __syncthreads();
   const double cx = node_X[3 * B.node], cy = node_X[3 * B.node + 1], cz = node_X[3 * B.node + 2];
-  for (int tl = warp; tl < B.ntgt; tl += nwarp) {
+  for (int tl = warp; tl < B.ntgt; tl += kAxWarps) {
     const int p = nb_targets[B.tgt_off + tl];
     const double px = Xs[3 * p] - cx, py = Xs[3 * p + 1] - cy, pz = Xs[3 * p + 2] - cz;
     double f0 = 0.0;
@@ -805,7 +864,10 @@ __global__ void __launch_bounds__(128) k_targets_ax(const NearBlockDev* __restri
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) f0 += __shfl_xor_sync(0xffffffffu, f0, o);
-    const double g = accs[tl] + f0;
+    double near = 0.0;
+#pragma unroll
+    for (int w = 0; w < kAxWarps; ++w) near += part[tl * kAxWarps + w];
+    const double g = near + f0;
     for (int k = point_dof_off[p] + lane; k < point_dof_off[p + 1]; k += 32) {
       const int i = point_dof[k];
       const int kd = dof_kind[i];
@@ -1244,13 +1306,13 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
       }
     }
   if ((stages & STAGE_TARGETS) && a.n_blocks > 0 && ND == 1 && a.ax && (a.Wc || a.Wc32)) {
-    const size_t shm = sizeof(double) * (size_t)(a.chunk + a.max_ntgt);
+    const size_t shm = ax_smem_bytes(a);
     if (a.Wc32)
-      launch_pdl(k_targets_ax<P, float>, a.n_blocks, 128, shm, st, a.blocks, a.nb_dofs, a.nb_targets, a.Wc32, a.Xs, a.node_X, a.L, a.ax,
-                                                           a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk);
+      launch_pdl(k_targets_ax<P, float>, a.n_blocks, kAxThreads, shm, st, a.blocks, a.nb_dofs, a.nb_targets, a.Wc32, a.Xs, a.node_X, a.L, a.ax,
+                                                           a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk_ax);
     else
-      launch_pdl(k_targets_ax<P, double>, a.n_blocks, 128, shm, st, a.blocks, a.nb_dofs, a.nb_targets, a.Wc, a.Xs, a.node_X, a.L, a.ax,
-                                                            a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk);
+      launch_pdl(k_targets_ax<P, double>, a.n_blocks, kAxThreads, shm, st, a.blocks, a.nb_dofs, a.nb_targets, a.Wc, a.Xs, a.node_X, a.L, a.ax,
+                                                            a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk_ax);
     ++launches;
   } else if ((stages & STAGE_TARGETS) && a.n_blocks > 0) {
     const size_t shm = sizeof(double2) * (size_t)(a.chunk + a.max_ntgt);
@@ -1303,14 +1365,14 @@ int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages) {
 template <int P>
 int launch_near_only_t(const MatvecArgs& a, cudaStream_t st) {
   if (a.n_blocks <= 0 || !a.ax || !(a.Wc || a.Wc32)) return 0;
-  const size_t shm = sizeof(double) * (size_t)(a.chunk + a.max_ntgt);
+  const size_t shm = ax_smem_bytes(a);
   const double2* noL = nullptr;
   if (a.Wc32)
-    launch_pdl(k_targets_ax<P, float>, a.n_blocks, 128, shm, st, a.blocks, a.nb_dofs, a.nb_targets, a.Wc32, a.Xs, a.node_X, noL, a.ax,
-               a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk);
+    launch_pdl(k_targets_ax<P, float>, a.n_blocks, kAxThreads, shm, st, a.blocks, a.nb_dofs, a.nb_targets, a.Wc32, a.Xs, a.node_X, noL, a.ax,
+               a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk_ax);
   else
-    launch_pdl(k_targets_ax<P, double>, a.n_blocks, 128, shm, st, a.blocks, a.nb_dofs, a.nb_targets, a.Wc, a.Xs, a.node_X, noL, a.ax,
-               a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk);
+    launch_pdl(k_targets_ax<P, double>, a.n_blocks, kAxThreads, shm, st, a.blocks, a.nb_dofs, a.nb_targets, a.Wc, a.Xs, a.node_X, noL, a.ax,
+               a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.chunk_ax);
   return 1;
 }
 

@@ -111,11 +111,13 @@ struct MatvecArgs {
   float* tc_escale = nullptr;    // [n_nodes] power-of-two column scales
   float* tc_Y = nullptr;         // per-pair partial locals [pairs][KPO], in work-item order
   int* tc_err = nullptr;         // set when a bounded wait gave up
+  uint32_t tc_wait_tries = 0;    // iteration limit of the contraction's pipeline waits
   const double* node_dL = nullptr;
   const double* tc_alpha = nullptr;  // [KP] sqrt((n+m)!(n-m)!) per real coefficient
   const void* tc_rows_map = nullptr; // host copy of the TMA tensor map over tc_Mt
   // targets
   int n_blocks = 0, chunk = 0, max_ntgt = 0;
+  int chunk_ax = 0;  // x values staged at a time by k_targets_ax (a multiple of 4)
   const NearBlockDev* blocks = nullptr;
   const int* nb_dofs = nullptr;
   const int* nb_targets = nullptr;
@@ -182,6 +184,7 @@ int launch_near_only(int p, const MatvecArgs& a, cudaStream_t st);  // a.rows = 
 
 // tensor-core M2L (m2l_tc.cu)
 int tc_supported(int p);            // 1 for 1 <= p <= 12
+uint32_t tc_default_wait_tries();   // iteration limit of the contraction's pipeline waits
 int tc_kp(int p);                   // real coefficients per row, padded to 64
 size_t tc_rows_map_bytes();         // size of the TMA tensor map over the multipole rows
 int tc_make_rows_map(void* map_out, void* Mt, int nrows, int p);

@@ -53,7 +53,11 @@ constexpr int kRows = 128;          // table rows = MMA N: output coefficients (
 // in shared memory, at most 128 with one (p <= 10; the kernel variant is chosen per launch)
 constexpr int kMaxPairs = 80;
 constexpr int kMaxPairsWide = 128;
+// Bounded waits: the pipeline waits use the launch's wait_tries (kWaitTries unless a caller set
+// a test limit); after a wait gave up, the waits that drain the CTA's own copies and MMAs still
+// in flight always use kDrainTries, so a CTA never leaves with asynchronous work pending.
 constexpr uint32_t kWaitTries = 1u << 22;
+constexpr uint32_t kDrainTries = 1u << 22;
 
 template <int P, int MC = kMaxPairs>
 struct TcDims {
@@ -244,7 +248,7 @@ template <int P, int MC>
 __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
     k_m2l_tc(const __grid_constant__ CUtensorMap rows_map, int nitems, const int* __restrict__ item_tab, const int* __restrict__ item_begin,
              const int* __restrict__ item_cnt, int npairs, const int* __restrict__ tc_src, const __half* __restrict__ Ttab,
-             const __half* __restrict__ Mt, float* __restrict__ Y, int* __restrict__ err) {
+             const __half* __restrict__ Mt, float* __restrict__ Y, int* __restrict__ err, uint32_t wait_tries) {
   pdl_enter();
   using D = TcDims<P, MC>;
   extern __shared__ __align__(128) unsigned char sm_raw[];
@@ -284,8 +288,8 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
       bool ok = true;
       for (int it = i0; it < i1; ++it) {
         const int li = it - i0, s = li % kStages, b = li % kAcc;
-        ok = mbar_wait(&bar_full[s], (li / kStages) & 1, kWaitTries);
-        if (ok && li >= kAcc) ok = mbar_wait(&bar_acce[b], ((li / kAcc) - 1) & 1, kWaitTries);
+        ok = mbar_wait(&bar_full[s], (li / kStages) & 1, wait_tries);
+        if (ok && li >= kAcc) ok = mbar_wait(&bar_acce[b], ((li / kAcc) - 1) & 1, wait_tries);
         if (!ok) break;
         tc_fence_after();
         const int tsl = s_tsl[s], ncol = s_icol[s], last = s_last[s];
@@ -317,13 +321,16 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
       if (!ok) {
         atomicExch(err, 1);
         // let MMAs already issued finish before the CTA leaves
-        if (issued > 0) mbar_wait(&bar_bfree[(issued - 1) % kStages], ((issued - 1) / kStages) & 1, kWaitTries);
+        if (issued > 0) mbar_wait(&bar_bfree[(issued - 1) % kStages], ((issued - 1) / kStages) & 1, kDrainTries);
       }
     }
     __syncwarp();
   } else if (tid >= kEpilogue) {
     const int pt = tid - kEpilogue;  // producer thread = gathered row
     int last_tab = -1, ntab_loaded = 0;
+    int armed[kStages];  // item (local index) whose loads were last started on each stage, -1: none
+#pragma unroll
+    for (int q = 0; q < kStages; ++q) armed[q] = -1;
     bool ok = true;
     // metadata of the current item (c_) and of the next one (n_), loaded two items ahead;
     // an item's first pair (nn_b0) is loaded one iteration before its rows are, so no load
@@ -347,9 +354,9 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
       const int li = it - i0, s = li % kStages, b = li % kAcc;
       const bool load_tab = c_tab != last_tab;
       const int tsl = load_tab ? (ntab_loaded % NS) : ((ntab_loaded - 1) % NS);
-      if (ok && li >= kStages) ok = mbar_wait(&bar_bfree[s], ((li / kStages) - 1) & 1, kWaitTries);
-      if (ok && li >= kAcc) ok = mbar_wait(&bar_acce[b], ((li / kAcc) - 1) & 1, kWaitTries);
-      if (ok && load_tab && ntab_loaded >= NS) ok = mbar_wait(&bar_tfree[tsl], ((ntab_loaded / NS) - 1) & 1, kWaitTries);
+      if (ok && li >= kStages) ok = mbar_wait(&bar_bfree[s], ((li / kStages) - 1) & 1, wait_tries);
+      if (ok && li >= kAcc) ok = mbar_wait(&bar_acce[b], ((li / kAcc) - 1) & 1, wait_tries);
+      if (ok && load_tab && ntab_loaded >= NS) ok = mbar_wait(&bar_tfree[tsl], ((ntab_loaded / NS) - 1) & 1, wait_tries);
       if (named_bar_or(1, kProducers, ok ? 0 : 1)) {
         ok = false;
         break;
@@ -370,6 +377,7 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
         mbar_arrive_expect_tx(&bar_full[s], bytes);
       }
       named_bar_sync(1, kProducers);
+      armed[s] = li;
       if (pt == 0) {
         mbar_arrive(&bar_meta[b]);
         if (load_tab)
@@ -396,14 +404,22 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
         if (it + 3 < i1) nn_b0 = item_begin[it + 3];
       }
     }
-    if (!ok) atomicExch(err, 1);
+    if (!ok) {
+      atomicExch(err, 1);
+      // the loads already started land in this CTA's shared memory: wait for each stage's last
+      // armed item (its transaction bytes complete on full[s]) before the CTA may leave
+      if (pt == 0)
+#pragma unroll
+        for (int q = 0; q < kStages; ++q)
+          if (armed[q] >= 0) mbar_wait(&bar_full[q], (armed[q] / kStages) & 1, kDrainTries);
+    }
   } else {
     const int quad = warp & 3, half = warp >> 2;  // TMEM lane quad * 32 + lane: output row of the tile
     const uint32_t lane_base = tbase + ((uint32_t)(quad * 32) << 16);
     for (int it = i0; it < i1; ++it) {
       const int li = it - i0, b = li % kAcc;
-      bool ok = mbar_wait(&bar_meta[b], (li / kAcc) & 1, kWaitTries);
-      if (ok) ok = mbar_wait(&bar_accf[b], (li / kAcc) & 1, kWaitTries);
+      bool ok = mbar_wait(&bar_meta[b], (li / kAcc) & 1, wait_tries);
+      if (ok) ok = mbar_wait(&bar_accf[b], (li / kAcc) & 1, wait_tries);
       if (!__all_sync(0xffffffffu, ok ? 1 : 0)) {
         if (lane == 0) atomicExch(err, 1);
         break;
@@ -563,11 +579,11 @@ int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts, int nd) {
       if constexpr (P <= 10)
         launch_pdl(k_m2l_tc<P, kMaxPairsWide>, grid, kEpilogue + kProducers + kIssuer, TcDims<P, kMaxPairsWide>::SMEM, st, map, a.n_tc_items,
                    a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt, a.n_tc_pairs, a.tc_src, static_cast<const __half*>(a.tc_tab),
-                   static_cast<const __half*>(a.tc_Mt), a.tc_Y, a.tc_err);
+                   static_cast<const __half*>(a.tc_Mt), a.tc_Y, a.tc_err, a.tc_wait_tries);
     } else {
       launch_pdl(k_m2l_tc<P, kMaxPairs>, grid, kEpilogue + kProducers + kIssuer, D::SMEM, st, map, a.n_tc_items, a.tc_item_tab,
                  a.tc_item_begin, a.tc_item_cnt, a.n_tc_pairs, a.tc_src, static_cast<const __half*>(a.tc_tab),
-                 static_cast<const __half*>(a.tc_Mt), a.tc_Y, a.tc_err);
+                 static_cast<const __half*>(a.tc_Mt), a.tc_Y, a.tc_err, a.tc_wait_tries);
     }
     ++launches;
   }
@@ -591,6 +607,7 @@ void tc_tables_launch(int ntab, const double* tab, const double* alpha, __half* 
 }  // namespace
 
 int tc_supported(int p) { return p >= 1 && p <= 12; }
+uint32_t tc_default_wait_tries() { return kWaitTries; }
 int tc_kp(int p) { return ((p + 1) * (p + 1) + 63) / 64 * 64; }
 
 size_t tc_rows_map_bytes() { return sizeof(CUtensorMap); }

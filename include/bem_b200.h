@@ -294,6 +294,13 @@ int bem_gpu_mel_stage(bem_gpu_mel* mel, const bem_mel_surface* s, int32_t stage,
 int bem_gpu_matvec_device_mixed(bem_gpu_ctx* ctx, const double* d_x, double* d_y);
 int bem_gpu_profile_matvec_mixed(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[9]*/);
 int bem_gpu_check_device_status(bem_gpu_ctx* ctx);
+/* Iteration limit of the tensor-core M2L's device-side pipeline waits (a kernel argument;
+ * default 2^22 tries, a fraction of a second).  For testing failure detection: with a small
+ * limit the waits give up, the kernel drains its own copies and MMAs in flight (with the
+ * default limit), records the failure and returns, so bem_gpu_check_device_status reports
+ * BEM_ERR_DEVICE while the context stays usable.  tries < 0 restores the default; the call
+ * clears the recorded failure and recaptures the operator graphs. */
+int bem_gpu_set_wait_limit(bem_gpu_ctx* ctx, int64_t tries);
 
 /* Near-field polynomial preconditioner (opts.preconditioner = 2).
  * bem_gpu_poly_roots: the roots formed by the last set-up, in the order they are applied (a
