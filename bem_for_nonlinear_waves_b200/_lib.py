@@ -19,7 +19,10 @@ P_i64 = ctypes.POINTER(ctypes.c_int64)
 
 BEM_OK = 0
 BEM_ERR_INVALID_ARGUMENT = -1
+BEM_ERR_OUT_OF_MEMORY = -2
 BEM_ERR_NOT_CONVERGED = -3
+BEM_ERR_NAN = -4
+BEM_ERR_DEVICE = -5
 BEM_ERR_NOT_READY = -6
 BEM_ERR_UNSUPPORTED = -7
 STATUS = {0: "ok", -1: "invalid argument", -2: "out of memory", -3: "not converged", -4: "non-finite value",
@@ -30,7 +33,8 @@ class Opts(ctypes.Structure):
     _fields_ = [("expansion_order", c_int), ("mac_theta", c_dbl), ("leaf_max_elements", c_int), ("max_level", c_int),
                 ("tol", c_dbl), ("max_iter", c_int), ("device", c_int), ("tol_relative", c_int), ("preconditioner", c_int),
                 ("precision", c_int), ("poly_degree", c_int), ("tree_on_host", c_int),
-                ("tc_item_pairs", c_int), ("overlap_near", c_int)]
+                ("tc_item_pairs", c_int), ("overlap_near", c_int), ("refine_rtol", c_dbl),
+                ("tc_deterministic", c_int)]
 
 
 class MelSurface(ctypes.Structure):
@@ -97,6 +101,12 @@ EXPORTS = {
                                      ctypes.POINTER(ctypes.c_int64)]),
     "bem_gpu_batch_poll": (c_int, [ctypes.c_void_p, ctypes.c_int64, c_int]),
     "bem_gpu_batch_release": (c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    "bem_gpu_batch_set_budget": (c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    "bem_gpu_batch_submit_chain": (c_int, [ctypes.c_void_p, ctypes.POINTER(Desc), P_u8, P_dbl, c_int, c_dbl, c_dbl, P_dbl, P_dbl,
+                                           ctypes.POINTER(Stats), ctypes.POINTER(ctypes.c_int64)]),
+    "bem_gpu_batch_stats": (c_int, [ctypes.c_void_p, P_i64]),
+    "bem_gpu_device_bytes": (ctypes.c_int64, [ctypes.c_void_p]),
+    "bem_gpu_estimate_bytes": (ctypes.c_int64, [ctypes.POINTER(Opts), ctypes.POINTER(Desc)]),
     "bem_gpu_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "bem_gpu_batch_destroy": (None, [ctypes.c_void_p]),
 }

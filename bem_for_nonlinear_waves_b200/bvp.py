@@ -40,7 +40,8 @@ def build_dofs(X, tri, face_dirichlet):
 
 
 def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter, device,
-               tol_relative, preconditioner, precision, poly_degree=8, tree_on_device=True, tc_item_pairs=0, overlap_near=False):
+               tol_relative, preconditioner, precision, poly_degree=8, tree_on_device=True, tc_item_pairs=0, overlap_near=False,
+               refine_rtol=0.0, tc_deterministic=False):
     o = L.Opts()
     lib.bem_gpu_default_opts(ctypes.byref(o))
     o.expansion_order = int(expansion_order)
@@ -57,6 +58,8 @@ def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_l
     o.tc_item_pairs = int(tc_item_pairs)
     o.overlap_near = 1 if overlap_near else 0
     o.precision = {"fp64": 0, "mixed": 1}[precision]
+    o.refine_rtol = float(refine_rtol)
+    o.tc_deterministic = 1 if tc_deterministic else 0
     return o
 
 
@@ -65,7 +68,8 @@ class BEM_BVP:
 
     def __init__(self, X, tri, face_dirichlet, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30,
                  fmm_max_level=7, solver_tol=1e-9, solver_max_iter=500, device=0, dofs=None, tol_relative=False, preconditioner="none",
-                 precision="fp64", poly_degree=8, tree_on_device=True, tc_item_pairs=0, overlap_near=False):
+                 precision="fp64", poly_degree=8, tree_on_device=True, tc_item_pairs=0, overlap_near=False, refine_rtol=0.0,
+                 tc_deterministic=False):
         self.lib = L.load()
         if not self.lib.bem_gpu_is_available():
             raise RuntimeError("no sm_100 CUDA device visible: the GMRES-FMM solver runs only on the GPU")
@@ -74,7 +78,7 @@ class BEM_BVP:
         self.face_dirichlet = np.ascontiguousarray(face_dirichlet, np.uint8)
         o = _make_opts(self.lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter,
                        device, tol_relative, preconditioner, precision, poly_degree, tree_on_device, tc_item_pairs,
-                       overlap_near)
+                       overlap_near, refine_rtol, tc_deterministic)
         self.opts = o
         self.ctx = self.lib.bem_gpu_create(ctypes.byref(o))
         if not self.ctx:
@@ -253,6 +257,10 @@ class BEM_BVP:
         return {"weights_fp64": 8 * int(out[0]), "weights_fp32": 4 * int(out[1]), "x_gather": 8 * int(out[2]),
                 "rows": 8 * int(out[5]), "blocks": int(out[3]), "targets": int(out[4])}
 
+    def device_bytes(self):
+        """Device bytes the context's buffers hold."""
+        return int(self.lib.bem_gpu_device_bytes(self.ctx))
+
     def matvec_time_ms(self, repeats=10):
         return self.profile_matvec(repeats)["total"]
 
@@ -309,12 +317,12 @@ class BatchSolver:
 
     def __init__(self, n_workers=2, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30, fmm_max_level=7,
                  solver_tol=1e-9, solver_max_iter=500, device=0, tol_relative=False, preconditioner="none", precision="fp64",
-                 poly_degree=8):
+                 poly_degree=8, tc_deterministic=False):
         self.lib = L.load()
         if not self.lib.bem_gpu_is_available():
             raise RuntimeError("no sm_100 CUDA device visible: the GMRES-FMM solver runs only on the GPU")
         o = _make_opts(self.lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter,
-                       device, tol_relative, preconditioner, precision, poly_degree)
+                       device, tol_relative, preconditioner, precision, poly_degree, tc_deterministic=tc_deterministic)
         self.handle = self.lib.bem_gpu_batch_create(ctypes.byref(o), int(n_workers))
         if not self.handle:
             raise RuntimeError("bem_gpu_batch_create failed")
@@ -341,6 +349,53 @@ class BatchSolver:
             raise RuntimeError(f"batch submit: {L.STATUS.get(rc, rc)}")
         self._pending[t.value] = (X, tri, fd, keep, known, phi, phin, st)
         return t.value
+
+    def submit_chain(self, X, tri, face_dirichlet, known, n_steps, dt, dofs=None, gravity=9.81):
+        """A whole RK4 time-stepping chain (n_steps x 4 stages of set-up, solve and MEL update) as one
+        request; `result_chain(ticket)` returns (positions [n, 3], point phi, stats) at the end."""
+        X = np.ascontiguousarray(X, np.float64)
+        tri = np.ascontiguousarray(tri, np.int32)
+        fd = np.ascontiguousarray(face_dirichlet, np.uint8)
+        if dofs is None:
+            dofs = build_dofs(X, tri, fd)
+        keep = [np.ascontiguousarray(dofs[k], np.int32).reshape(-1) for k in ("dof_point", "dof_face", "dof_kind", "face_dof")]
+        flags = np.ascontiguousarray(dofs["point_flags"], np.uint8)
+        n = keep[0].shape[0]
+        known = np.ascontiguousarray(known, np.float64)
+        if known.shape[0] != n:
+            raise ValueError("known values must have one entry per DOF")
+        Xo, po, st = np.zeros(3 * X.shape[0]), np.zeros(X.shape[0]), L.Stats()
+        desc = L.Desc(X.shape[0], L.ptr(X, L.P_dbl), tri.shape[0], L.ptr(tri, L.P_int), L.ptr(fd, L.P_u8), n,
+                      L.ptr(keep[0], L.P_int), L.ptr(keep[1], L.P_int), L.ptr(keep[2], L.P_int), L.ptr(keep[3], L.P_int))
+        t = ctypes.c_int64(0)
+        rc = self.lib.bem_gpu_batch_submit_chain(self.handle, ctypes.byref(desc), L.ptr(flags, L.P_u8), L.ptr(known, L.P_dbl),
+                                                 int(n_steps), float(dt), float(gravity), L.ptr(Xo, L.P_dbl), L.ptr(po, L.P_dbl),
+                                                 ctypes.byref(st), ctypes.byref(t))
+        if rc != L.BEM_OK:
+            raise RuntimeError(f"batch submit_chain: {L.STATUS.get(rc, rc)}")
+        self._pending[t.value] = (X, tri, fd, keep, flags, known, Xo, po, st)
+        return t.value
+
+    def result_chain(self, ticket):
+        rc = self.lib.bem_gpu_batch_poll(self.handle, int(ticket), 1)
+        item = self._pending.pop(int(ticket))
+        msg = self.lib.bem_gpu_batch_last_error(self.handle) if rc not in (L.BEM_OK, L.BEM_ERR_NOT_CONVERGED) else None
+        self.lib.bem_gpu_batch_release(self.handle, int(ticket))
+        if msg is not None:
+            raise RuntimeError(f"batch chain {ticket}: {L.STATUS.get(rc, rc)}: {msg.decode() if msg else ''}")
+        return item[6].reshape(-1, 3), item[7], item[8]
+
+    def set_budget(self, nbytes):
+        """Admission by device memory (bytes held by the worker contexts); 0 = no limit."""
+        rc = self.lib.bem_gpu_batch_set_budget(self.handle, int(nbytes))
+        if rc != L.BEM_OK:
+            raise RuntimeError(f"batch set_budget: {L.STATUS.get(rc, rc)}")
+
+    def stats(self):
+        out = np.zeros(6, np.int64)
+        self.lib.bem_gpu_batch_stats(self.handle, L.ptr(out, L.P_i64))
+        keys = ["admitted", "waited_for_memory", "contexts_recycled", "device_bytes_held", "budget", "queued"]
+        return {k: int(v) for k, v in zip(keys, out)}
 
     def done(self, ticket):
         return self.lib.bem_gpu_batch_poll(self.handle, int(ticket), 0) != L.BEM_ERR_NOT_READY

@@ -31,12 +31,15 @@ template <typename T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0, cap = 0;
+  int64_t* acct = nullptr;  // the owner's running total of allocated device bytes
   DBuf() = default;
+  explicit DBuf(int64_t* a) : acct(a) {}
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
   ~DBuf() { release(); }
   void release() {
     if (p) cudaFree(p);
+    if (acct) *acct -= (int64_t)(sizeof(T) * cap);
     p = nullptr;
     n = cap = 0;
   }
@@ -46,7 +49,10 @@ struct DBuf {
     release();
     n = count;
     const cudaError_t e = cudaMalloc((void**)&p, sizeof(T) * count);
-    if (e == cudaSuccess) cap = count;
+    if (e == cudaSuccess) {
+      cap = count;
+      if (acct) *acct += (int64_t)(sizeof(T) * cap);
+    }
     return e;
   }
 };
@@ -132,44 +138,48 @@ struct bem_gpu_ctx {
   uint32_t tc_wait_tries = tc_default_wait_tries();  // bem_gpu_set_wait_limit
 
   // geometry / tree
-  DBuf<double> Xs, e_q, e_W, e_n, e_near, node_X, WG, WGn, Wc, diag;
-  DBuf<float> Wc32;  // combined near weights of A.x in FP32 (mixed precision, polynomial preconditioner)
-  DBuf<int> leaf_dof_off, leaf_dof, e_slot, slot_block;  // P2M operator of A.x: DOFs per leaf
-  DBuf<double2> p2m_C;                       // [(leaf, DOF)][NC]
-  DBuf<double2> near_scratch;                // element values of the near-weight kernel
-  DBuf<int> e_dof, e_vtx, node_fb, node_fe, leaves, level_parents, child_begin, child_end, node_children;
-  DBuf<int> node_parent, node_level, m2m_nsig, m2m_cnt, m2m_ready;
+  int64_t dev_bytes = 0;  // device bytes held by the DBuf members below (declared first: destroyed last)
+  DBuf<double> Xs{&dev_bytes}, e_q{&dev_bytes}, e_W{&dev_bytes}, e_n{&dev_bytes}, e_near{&dev_bytes}, node_X{&dev_bytes}, WG{&dev_bytes}, WGn{&dev_bytes}, Wc{&dev_bytes}, diag{&dev_bytes};
+  DBuf<float> Wc32{&dev_bytes};  // combined near weights of A.x in FP32 (mixed precision, polynomial preconditioner)
+  DBuf<int> leaf_dof_off{&dev_bytes}, leaf_dof{&dev_bytes}, e_slot{&dev_bytes}, slot_block{&dev_bytes};  // P2M operator of A.x: DOFs per leaf
+  DBuf<double2> p2m_C{&dev_bytes};                       // [(leaf, DOF)][NC]
+  DBuf<double2> near_scratch{&dev_bytes};                // element values of the near-weight kernel
+  DBuf<int> e_dof{&dev_bytes}, e_vtx{&dev_bytes}, node_fb{&dev_bytes}, node_fe{&dev_bytes}, leaves{&dev_bytes}, level_parents{&dev_bytes}, child_begin{&dev_bytes}, child_end{&dev_bytes}, node_children{&dev_bytes};
+  DBuf<int> node_parent{&dev_bytes}, node_level{&dev_bytes}, m2m_nsig{&dev_bytes}, m2m_cnt{&dev_bytes}, m2m_ready{&dev_bytes};
   int n_m2m_ready = 0;
-  DBuf<int> m2l_targets, m2l_off, m2l_src, nb_dofs, nb_targets, nb_ranges, dof_inc_off, dof_inc;
-  DBuf<int> block_of_point, row_of_point, self_col;  // right-Jacobi inputs
-  DBuf<int> point_dof_off, point_dof, dof_kind, dof_point;
-  DBuf<NearBlockDev> blocks;
-  DBuf<int> chunk_grp, chunk_begin, chunk_cnt, grp_pair;
-  DBuf<double> grp_vec;
-  DBuf<double2> Sg, Y, Ftab;
-  DBuf<double> ftab_vec;
-  DBuf<double2> M, L;
+  DBuf<int> m2l_targets{&dev_bytes}, m2l_off{&dev_bytes}, m2l_src{&dev_bytes}, nb_dofs{&dev_bytes}, nb_targets{&dev_bytes}, nb_ranges{&dev_bytes}, dof_inc_off{&dev_bytes}, dof_inc{&dev_bytes};
+  DBuf<int> block_of_point{&dev_bytes}, row_of_point{&dev_bytes}, self_col{&dev_bytes};  // right-Jacobi inputs
+  DBuf<int> point_dof_off{&dev_bytes}, point_dof{&dev_bytes}, dof_kind{&dev_bytes}, dof_point{&dev_bytes};
+  DBuf<NearBlockDev> blocks{&dev_bytes};
+  DBuf<int> chunk_grp{&dev_bytes}, chunk_begin{&dev_bytes}, chunk_cnt{&dev_bytes}, grp_pair{&dev_bytes};
+  DBuf<double> grp_vec{&dev_bytes};
+  DBuf<double2> Sg{&dev_bytes}, Y{&dev_bytes}, Ftab{&dev_bytes};
+  DBuf<double> ftab_vec{&dev_bytes};
+  DBuf<double2> M{&dev_bytes}, L{&dev_bytes};
   std::vector<int> level_parent_off;
-  int n_m2l_targets = 0, max_ntgt = 0, chunk = 0, chunk_ax = 0;
+  int n_m2l_targets = 0, max_ntgt = 0, chunk = 0;
   int64_t w4_total = 0;  // size of the row-padded FP32 near weights
   int n_tc_items = 0;    // tensor-core work items (every table-row-tile image's pair chunks)
   // state
-  DBuf<double> phi, phin, known_s, rows, GPhin, GnPhi;
+  DBuf<double> phi{&dev_bytes}, phin{&dev_bytes}, known_s{&dev_bytes}, rows{&dev_bytes}, GPhin{&dev_bytes}, GnPhi{&dev_bytes};
   // graph-captured A.x : mv_in -> mv_out
-  DBuf<double> mv_in, mv_out;
+  DBuf<double> mv_in{&dev_bytes}, mv_out{&dev_bytes};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   // Krylov
-  DBuf<double> V, w, hdev, partial, xdev, bdev, rdev, ydev, tmp, dinv;
+  DBuf<double> V{&dev_bytes}, w{&dev_bytes}, hdev{&dev_bytes}, partial{&dev_bytes}, xdev{&dev_bytes}, bdev{&dev_bytes}, rdev{&dev_bytes}, ydev{&dev_bytes}, tmp{&dev_bytes}, dinv{&dev_bytes};
   int V_cols = 0;
   int graph_kernels = 0;
   // mixed precision: tensor-core M2L tables and buffers; graph of the low-precision A.x
   bool mixed = false;
-  DBuf<int> tc_item_tab, tc_item_begin, tc_item_cnt, tc_pos, tc_src, tc_err;
-  DBuf<double> tc_tabvec, tc_alpha, node_dL;
-  DBuf<uint16_t> tc_T, tc_Mt;
-  DBuf<float> tc_escale;
-  DBuf<unsigned int> tc_max;
+  DBuf<int> tc_item_tab{&dev_bytes}, tc_item_begin{&dev_bytes}, tc_item_cnt{&dev_bytes}, tc_pos{&dev_bytes}, tc_src{&dev_bytes}, tc_err{&dev_bytes};
+  DBuf<int> near_err{&dev_bytes};  // k_targets_ax: a bounded wait gave up
+  DBuf<double> tc_tabvec{&dev_bytes}, tc_alpha{&dev_bytes}, node_dL{&dev_bytes};
+  DBuf<uint16_t> tc_T{&dev_bytes}, tc_Mt{&dev_bytes};
+  DBuf<float> tc_escale{&dev_bytes};
+  DBuf<int> tc_tgt{&dev_bytes};    // [pairs] compact target index of each work-item-ordered pair
+  DBuf<float> tc_acc{&dev_bytes};  // [n_m2l_targets][KPO] FP32 accumulators of the fused reduction (zero between launches)
+  DBuf<unsigned int> tc_max{&dev_bytes};
   int tc_grid = 148;
   int tc_tune = 0;                 // pairs per tensor-core work item in use
   bool tc_tuned_here = false;      // this set-up ran the tuning
@@ -180,8 +190,8 @@ struct bem_gpu_ctx {
   int graph_kernels_lo = 0;
   // device-resident Arnoldi: state, rotations, g, R; one graph per step; pinned ring of
   // residual estimates with an event per slot
-  DBuf<ArnoldiState> arn_state;
-  DBuf<double> arn_g, arn_cs, arn_sn, arn_R, xbase;
+  DBuf<ArnoldiState> arn_state{&dev_bytes};
+  DBuf<double> arn_g{&dev_bytes}, arn_cs{&dev_bytes}, arn_sn{&dev_bytes}, arn_R{&dev_bytes}, xbase{&dev_bytes};
   cudaGraph_t arn_graph = nullptr;
   cudaGraphExec_t arn_exec = nullptr;
   int arn_kernels = 0;
@@ -190,7 +200,7 @@ struct bem_gpu_ctx {
   // polynomial preconditioner: roots (from the set-up), Arnoldi basis of the root run,
   // apply scratch, and Z = M V (the iterate is updated from Z)
   PolyRoots poly;
-  DBuf<double> poly_V, poly_h, poly_part, poly_prod, poly_y, Z;
+  DBuf<double> poly_V{&dev_bytes}, poly_h{&dev_bytes}, poly_part{&dev_bytes}, poly_prod{&dev_bytes}, poly_y{&dev_bytes}, Z{&dev_bytes};
   double* arn_err_host = nullptr;
   cudaEvent_t arn_ev[kErrRing] = {};
   // accounting of the current setup + solve
@@ -263,7 +273,7 @@ struct bem_gpu_ctx {
     a.L = L.p;
     a.n_blocks = (int)plan.blocks.size();
     a.chunk = chunk;
-    a.chunk_ax = chunk_ax;
+    a.near_err = near_err.p;
     a.max_ntgt = max_ntgt;
     a.blocks = blocks.p;
     a.nb_dofs = nb_dofs.p;
@@ -318,6 +328,8 @@ struct bem_gpu_ctx {
     a.tc_Mt = tc_Mt.p;
     a.tc_escale = tc_escale.p;
     a.tc_Y = reinterpret_cast<float*>(Y.p);
+    a.tc_tgt = tc_tgt.p;
+    a.tc_acc = opts.tc_deterministic ? nullptr : tc_acc.p;
     a.tc_err = tc_err.p;
     a.tc_wait_tries = tc_wait_tries;
     a.node_dL = node_dL.p;
@@ -539,7 +551,7 @@ void bem_gpu_default_opts(bem_gpu_opts* o) {
 
 bem_gpu_ctx* bem_gpu_create(const bem_gpu_opts* opts) {
   if (!opts || opts->expansion_order < 1 || opts->expansion_order > 12 || !(opts->mac_theta > 0) || opts->leaf_max_elements < 1 ||
-      opts->max_level < 1 || opts->max_level > 20 || opts->max_iter < 1)
+      opts->max_level < 1 || opts->max_level > 20 || opts->max_iter < 1 || !(opts->refine_rtol >= 0.0 && opts->refine_rtol < 1.0))
     return nullptr;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || opts->device < 0 || opts->device >= ndev) return nullptr;
@@ -748,6 +760,8 @@ static int tune_tc_items(bem_gpu_ctx* ctx) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  // the timed contractions added into the fused accumulators without a finalize: clear them
+  CK(cudaMemsetAsync(ctx->tc_acc.p, 0, sizeof(float) * ctx->tc_acc.n, s));
   retile_tc_items(ctx->plan, t.best);
   CK(upload_tc_items(ctx, false));
   {
@@ -905,10 +919,11 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   }
   // a multiple of 4 columns (the FP32 rows are read 4 columns at a time)
   ctx->chunk = std::min((max_ndof + 3) & ~3, ((smem_cap - ctx->max_ntgt * 16) / 16) & ~3);
-  // k_targets_ax stages at most 4,096 x values at a time (32 KB, so several CTAs share an SM)
-  ctx->chunk_ax = std::min((max_ndof + 3) & ~3, 4096);
-  const int ax_bytes = 8 * (ctx->chunk_ax + ctx->max_ntgt * 8);
-  configure_targets_smem(P.opt.p, std::max((ctx->chunk + ctx->max_ntgt) * 16, ax_bytes));
+  configure_targets_smem(P.opt.p, (ctx->chunk + ctx->max_ntgt) * 16);
+  if (configure_targets_ax_smem(ctx->max_ntgt) != 0) {
+    ctx->err = "too many targets in one bucket for the near-field kernel";
+    return BEM_ERR_UNSUPPORTED;
+  }
   configure_m2l_smem(P.opt.p);
 
 
@@ -961,6 +976,9 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   CK(ups(ctx->m2l_targets, mt));
   CK(ups(ctx->m2l_off, P.m2l_off));
   CK(ups(ctx->m2l_src, P.m2l_src));
+  // 4 spare elements: k_targets_ax copies 16-byte aligned windows of nb_dofs, which may reach
+  // up to 3 elements past the last block's DOFs
+  CK(ctx->nb_dofs.alloc(P.nb_dofs.size() + 4));
   CK(upn(ctx->nb_dofs, P.nb_dofs));
   CK(upn(ctx->nb_targets, P.nb_targets));
   CK(upn(ctx->nb_ranges, P.nb_ranges));
@@ -1009,15 +1027,23 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     for (int i = 0; i < nb; ++i) dl[i] = P.nodes[i].dL;
     tc_alpha_host(p, al.data());
     CK(upload_tc_items(ctx, reuse));
-    {  // work-item order j -> source bucket; pair slot k -> its position j (the row of its partial)
-      std::vector<int> src(P.tc_pair.size()), pos(P.tc_pair.size());
+    {  // work-item order j -> source bucket and compact target index; pair slot k -> its position j
+       // (the row of its partial)
+      std::vector<int> src(P.tc_pair.size()), pos(P.tc_pair.size()), tgt(P.tc_pair.size()), tgt_of_slot((size_t)P.m2l_pairs);
+      for (size_t ti = 0; ti < P.m2l_targets.size(); ++ti) {
+        const int t = P.m2l_targets[ti];
+        for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) tgt_of_slot[k] = (int)ti;
+      }
       for (size_t j = 0; j < src.size(); ++j) {
         src[j] = P.m2l_src[P.tc_pair[j]];
         pos[P.tc_pair[j]] = (int)j;
+        tgt[j] = tgt_of_slot[P.tc_pair[j]];
       }
       CK(ups(ctx->tc_src, src));
       CK(ups(ctx->tc_pos, pos));
+      CK(ups(ctx->tc_tgt, tgt));
     }
+    CK(ctx->tc_acc.alloc((size_t)std::max<size_t>(P.m2l_targets.size(), 1) * tc_kpo(p)));
     CK(ups(ctx->tc_tabvec, P.tc_tab));
     CK(ups(ctx->tc_alpha, al));
     CK(ups(ctx->node_dL, dl));
@@ -1061,7 +1087,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   CK(ctx->L.alloc((size_t)nb * 2 * NC));
   CK(ctx->WG.alloc(std::max<int64_t>(P.nnz, 1)));
   CK(ctx->WGn.alloc(std::max<int64_t>(P.nnz, 1)));
-  CK(ctx->Wc.alloc(std::max<int64_t>(P.nnz, 1)));
+  CK(ctx->Wc.alloc(std::max<int64_t>(ctx->w4_total, 1)));  // rows padded to 4 columns, as the FP32 copy
   const bool want_w32 = ctx->opts.precision == 1 || ctx->opts.preconditioner == 2;
   if (want_w32) CK(ctx->Wc32.alloc(std::max<int64_t>(ctx->w4_total, 1)));
   const int N = P.ndof;
@@ -1141,8 +1167,11 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     launch_s_tables(P.opt.p, (int)P.grp_off.size() - 1, ctx->grp_vec.p, ctx->Sg.p, s);
     ctx->launches += 1;
   }
+  CK(ctx->near_err.alloc(1));
+  CK(cudaMemsetAsync(ctx->near_err.p, 0, sizeof(int), s));
   if (ctx->mixed) {
     CK(cudaMemsetAsync(ctx->tc_Mt.p, 0, sizeof(uint16_t) * ctx->tc_Mt.n, s));
+    CK(cudaMemsetAsync(ctx->tc_acc.p, 0, sizeof(float) * ctx->tc_acc.n, s));
     CK(cudaMemsetAsync(ctx->tc_err.p, 0, sizeof(int), s));
     if (!reuse) {
       CK(cudaMemsetAsync(ctx->tc_max.p, 0, sizeof(unsigned int), s));
@@ -1335,6 +1364,28 @@ int bem_gpu_near_stats(bem_gpu_ctx* ctx, int64_t* out) {
   out[4] = tg;
   out[5] = P.ndof;
   return BEM_OK;
+}
+
+int64_t bem_gpu_device_bytes(const bem_gpu_ctx* ctx) { return ctx ? ctx->dev_bytes : 0; }
+
+// Device memory of one BVP from its sizes alone (no plan is built): near-field weights (two FP64
+// arrays, the combined FP64 copy and, mixed, the FP32 copy; about 52 nonzeros per point per
+// element of the leaf size on these meshes, at most one per DOF), the M2L pair slots (about 11
+// pairs per element), the P2M operator, the Krylov basis (twice with the polynomial
+// preconditioner's flexible vectors) and the per-element arrays, plus 64 MB for the rest.
+int64_t bem_gpu_estimate_bytes(const bem_gpu_opts* o, const bem_bvp_desc* d) {
+  if (!o || !d || d->n_points <= 0 || d->n_faces <= 0) return 0;
+  const int64_t np = d->n_points, nf = d->n_faces, ndof = std::max(d->n_dof, 1);
+  const int p = std::max(1, std::min(o->expansion_order, 12));
+  const int64_t nc = (int64_t)(p + 1) * (p + 2) / 2, kp = ((int64_t)(p + 1) * (p + 1) + 63) / 64 * 64;
+  const int64_t nnz = std::min<int64_t>(np * 52 * std::max(o->leaf_max_elements, 1), np * ndof);
+  const int64_t pairs = 11 * nf;
+  int64_t b = nnz * (8 + 8 + 8 + (o->precision == 1 ? 4 : 0));
+  b += pairs * 2 * nc * 16 + (o->precision == 1 ? pairs * (kp * 4 / 8 + 8) : 0);
+  b += nf * 2 * nc * 16;  // P2M operator columns
+  b += (int64_t)(std::max(o->max_iter, 1) + 2) * ndof * 8 * (o->preconditioner == 2 ? 2 : 1);
+  b += nf * (18 + 6 + 3 + 8) * 8 + nf * 3 * 4 * 4 + np * 64 + ndof * 160;
+  return b + ((int64_t)64 << 20);
 }
 
 int bem_gpu_tree_stats(bem_gpu_ctx* ctx, int64_t* out) {
@@ -1577,7 +1628,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   // Mixed precision is iterative refinement: each GMRES cycle solves A_lo d = r to
   // max(tol, kInnerRtol |r|) and the cycle ends with the FP64 true residual, from which the
   // next cycle starts (that residual is reused, not recomputed).
-  constexpr double kInnerRtol = 1e-5;
+  const double kInnerRtol = ctx->opts.refine_rtol > 0.0 ? ctx->opts.refine_rtol : 1e-5;
   bool have_res = false;
   auto norm_of = [&](const double* v, double* out) -> int {
     launch_mdot(v, N, 1, v, N, ctx->partial.p, ctx->hdev.p, s);
@@ -1711,7 +1762,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     }
   }
   CK(cudaEventRecord(ctx->ev[3], s));
-  if (mixed && (rc = bem_gpu_check_device_status(ctx)) != BEM_OK) return rc;
+  if ((rc = bem_gpu_check_device_status(ctx)) != BEM_OK) return rc;
   std::vector<double> x(N);
   CK(cudaMemcpyAsync(x.data(), ctx->xdev.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
   ctx->d2h += 8LL * N;
@@ -1857,12 +1908,17 @@ int bem_gpu_set_wait_limit(bem_gpu_ctx* ctx, int64_t tries) {
 
 int bem_gpu_check_device_status(bem_gpu_ctx* ctx) {
   if (!ctx) return BEM_ERR_INVALID_ARGUMENT;
-  if (!ctx->mixed) return BEM_OK;
-  int flag = 0;
-  CK(cudaMemcpyAsync(&flag, ctx->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  if (!ctx->ready) return BEM_OK;
+  int flag[2] = {0, 0};
+  CK(cudaMemcpyAsync(&flag[0], ctx->near_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  if (ctx->mixed) CK(cudaMemcpyAsync(&flag[1], ctx->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  if (flag) {
+  if (flag[1]) {
     ctx->err = "tensor-core M2L: a bounded wait on the MMA completion gave up";
+    return BEM_ERR_DEVICE;
+  }
+  if (flag[0]) {
+    ctx->err = "near-field kernel: a bounded wait on its copy pipeline gave up";
     return BEM_ERR_DEVICE;
   }
   return BEM_OK;

@@ -110,6 +110,11 @@ struct MatvecArgs {
   void* tc_Mt = nullptr;         // FP16 hi/lo rows of M[0] - M[1] [n_nodes+1][2][KP]
   float* tc_escale = nullptr;    // [n_nodes] power-of-two column scales
   float* tc_Y = nullptr;         // per-pair partial locals [pairs][KPO], in work-item order
+  // fused reduction (tc_acc set): the contraction adds each pair into its target's FP32
+  // accumulator [n_m2l_targets][KPO] in L2 instead of writing partials; a finalize kernel
+  // converts and clears them (summation order varies between runs)
+  const int* tc_tgt = nullptr;   // [pairs] compact target index (into m2l_targets), in work-item order
+  float* tc_acc = nullptr;
   int* tc_err = nullptr;         // set when a bounded wait gave up
   uint32_t tc_wait_tries = 0;    // iteration limit of the contraction's pipeline waits
   const double* node_dL = nullptr;
@@ -117,7 +122,7 @@ struct MatvecArgs {
   const void* tc_rows_map = nullptr; // host copy of the TMA tensor map over tc_Mt
   // targets
   int n_blocks = 0, chunk = 0, max_ntgt = 0;
-  int chunk_ax = 0;  // x values staged at a time by k_targets_ax (a multiple of 4)
+  int* near_err = nullptr;  // set when a bounded wait of k_targets_ax gave up
   const NearBlockDev* blocks = nullptr;
   const int* nb_dofs = nullptr;
   const int* nb_targets = nullptr;
@@ -185,6 +190,9 @@ int launch_near_only(int p, const MatvecArgs& a, cudaStream_t st);  // a.rows = 
 // tensor-core M2L (m2l_tc.cu)
 int tc_supported(int p);            // 1 for 1 <= p <= 12
 uint32_t tc_default_wait_tries();   // iteration limit of the contraction's pipeline waits
+// k_targets_ax: sets its dynamic shared-memory permission for the largest near block of a problem
+// (max_ntgt targets) on the current device; -1 when that does not fit an SM
+int configure_targets_ax_smem(int max_ntgt);
 int tc_kp(int p);                   // real coefficients per row, padded to 64
 size_t tc_rows_map_bytes();         // size of the TMA tensor map over the multipole rows
 int tc_make_rows_map(void* map_out, void* Mt, int nrows, int p);

@@ -244,11 +244,12 @@ constexpr int kAccCols = 128;
 static_assert(kMaxPairsWide <= kAccCols, "one accumulator holds an item");
 static_assert(kMaxPairsWide <= kProducers, "one producer thread per gathered row");
 
-template <int P, int MC>
+template <int P, int MC, bool FUSED>
 __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
     k_m2l_tc(const __grid_constant__ CUtensorMap rows_map, int nitems, const int* __restrict__ item_tab, const int* __restrict__ item_begin,
              const int* __restrict__ item_cnt, int npairs, const int* __restrict__ tc_src, const __half* __restrict__ Ttab,
-             const __half* __restrict__ Mt, float* __restrict__ Y, int* __restrict__ err, uint32_t wait_tries) {
+             const __half* __restrict__ Mt, float* __restrict__ Y, int* __restrict__ err, uint32_t wait_tries,
+             const int* __restrict__ tc_tgt, const float* __restrict__ escale, float* __restrict__ acc) {
   pdl_enter();
   using D = TcDims<P, MC>;
   extern __shared__ __align__(128) unsigned char sm_raw[];
@@ -258,6 +259,9 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
   unsigned char* sB = sm_tc + NS * D::TAB_BYTES;  // kStages stages of regions (part, atom): MC rows x 128 B
   __shared__ int s_row[MC];
   __shared__ int s_ncol[kAcc], s_b0[kAcc], s_rt[kAcc];
+  // FUSED: per accumulator, the target (compact index) and source column scale of each pair
+  __shared__ int s_tgt[FUSED ? kAcc : 1][FUSED ? MC : 1];
+  __shared__ float s_sc[FUSED ? kAcc : 1][FUSED ? MC : 1];
   __shared__ int s_tsl[kStages], s_icol[kStages], s_last[kStages];
   __shared__ uint64_t bar_full[kStages], bar_bfree[kStages], bar_tfree[2], bar_accf[kAcc], bar_acce[kAcc], bar_meta[kAcc];
   __shared__ uint32_t tslot;
@@ -336,18 +340,22 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
     // an item's first pair (nn_b0) is loaded one iteration before its rows are, so no load
     // waits on another inside the loop
     int c_tab = 0, c_b0 = 0, c_n = 0, c_src = 0, n_tab = 0, n_b0 = 0, n_n = 0, n_src = 0, nn_b0 = 0;
-    auto load_item = [&](int it, int b0, int& tb, int& n, int& src) {
+    int c_tgt = 0, n_tgt = 0;  // FUSED: target of this thread's pair, and its source's column scale
+    float c_sc = 0.f;
+    auto load_item = [&](int it, int b0, int& tb, int& n, int& src, int& tgt) {
       tb = item_tab[it];
       n = item_cnt[it];
       src = tc_src[min(b0 + pt, npairs - 1)];
+      if constexpr (FUSED) tgt = tc_tgt[min(b0 + pt, npairs - 1)];
     };
     if (i0 < i1) {
       c_b0 = item_begin[i0];
-      load_item(i0, c_b0, c_tab, c_n, c_src);
+      load_item(i0, c_b0, c_tab, c_n, c_src, c_tgt);
+      if constexpr (FUSED) c_sc = escale[c_src];
     }
     if (i0 + 1 < i1) {
       n_b0 = item_begin[i0 + 1];
-      load_item(i0 + 1, n_b0, n_tab, n_n, n_src);
+      load_item(i0 + 1, n_b0, n_tab, n_n, n_src, n_tgt);
     }
     if (i0 + 2 < i1) nn_b0 = item_begin[i0 + 2];
     for (int it = i0; it < i1; ++it) {
@@ -361,7 +369,13 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
         ok = false;
         break;
       }
-      if (pt < c_n) s_row[pt] = c_src;
+      if (pt < c_n) {
+        s_row[pt] = c_src;
+        if constexpr (FUSED) {
+          s_tgt[b][pt] = c_tgt;
+          s_sc[b][pt] = c_sc;
+        }
+      }
       const int cur_tab = c_tab, cur_ncol = c_n;
       const int nquad = (cur_ncol + 3) >> 2;
       if (load_tab) ++ntab_loaded;
@@ -394,13 +408,15 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
         for (int i = 0; i < 4; ++i) y[i] = s_row[min(4 * q + i, cur_ncol - 1)] * 2 + part;
         tma_gather4(sBs + (part * D::KA + a) * D::REGION + q * 4 * 128, &rows_map, a * 64, y[0], y[1], y[2], y[3], &bar_full[s]);
       }
+      if constexpr (FUSED) c_sc = (it + 1 < i1) ? escale[n_src] : 0.f;  // the next item's scale, one iteration ahead
       c_tab = n_tab;
       c_b0 = n_b0;
       c_n = n_n;
       c_src = n_src;
+      c_tgt = n_tgt;
       if (it + 2 < i1) {
         n_b0 = nn_b0;
-        load_item(it + 2, n_b0, n_tab, n_n, n_src);
+        load_item(it + 2, n_b0, n_tab, n_n, n_src, n_tgt);
         if (it + 3 < i1) nn_b0 = item_begin[it + 3];
       }
     }
@@ -437,10 +453,24 @@ __global__ void __launch_bounds__(kEpilogue + kProducers + kIssuer, 1)
           tmem_ld32_wait(ra);
         }
         auto store = [&](const uint32_t* r, int cbase) {
+          if constexpr (FUSED) {
+            // the pair's coefficients, its source's column scale undone, added into the
+            // target's FP32 accumulator in L2 (one coalesced 128-byte reduction per warp)
+            const bool live = row0 + lane < D::NR;
 #pragma unroll
-          for (int q = 0; q < 32; ++q) {
-            const int j = cbase + q;
-            if (j < ncol) Yb[(size_t)j * D::KPO] = __uint_as_float(r[q]);
+            for (int q = 0; q < 32; ++q) {
+              const int j = cbase + q;
+              if (j < ncol && live) {
+                float* dst = acc + (size_t)s_tgt[b][j] * D::KPO + row0 + lane;
+                asm volatile("red.global.add.f32 [%0], %1;" ::"l"(dst), "f"(__uint_as_float(r[q]) * s_sc[b][j]) : "memory");
+              }
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+              const int j = cbase + q;
+              if (j < ncol) Yb[(size_t)j * D::KPO] = __uint_as_float(r[q]);
+            }
           }
         };
         while (c0 < ncol) {
@@ -553,6 +583,42 @@ __global__ void k_m2l_tc_reduce(int ntargets, const int* __restrict__ targets, c
   }
 }
 
+// FUSED path: per target, the FP32 accumulator the contraction reduced into, back to the FP64
+// complex layout [node][density][NC] with the normalisation and a_t^{n+1} undone (L[1] stays
+// zero), and the accumulator cleared for the next launch.  One warp per target.
+template <int P>
+__global__ void k_m2l_tc_finalize(int ntargets, const int* __restrict__ targets, const double* __restrict__ node_dL,
+                                  const double* __restrict__ alpha, float* __restrict__ acc, double2* __restrict__ L) {
+  pdl_enter();
+  using D = TcDims<P>;
+  constexpr int NC = ncoef(P), V = D::KPO / 32;
+  const int lane = threadIdx.x & 31;
+  const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int ti = w0; ti < ntargets; ti += nw) {
+    const int tgt = targets[ti];
+    float* row = acc + (size_t)ti * D::KPO + lane * V;
+    float v[V];
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      v[q] = row[q];
+      row[q] = 0.f;
+    }
+    const double a = node_dL[tgt];
+    double* Lr = reinterpret_cast<double*>(L + (size_t)tgt * 2 * NC);
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      const int i = lane * V + q;
+      if (i < D::NR) {
+        int n, m, part;
+        decode_real(i, n, m, part);
+        double ap = a;
+        for (int t = 0; t < n; ++t) ap *= a;
+        Lr[2 * cidx(n, m) + part] = (double)v[q] * alpha[i] / ap;
+      }
+    }
+  }
+}
+
 template <int P>
 int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts, int nd) {
   using D = TcDims<P>;
@@ -575,19 +641,32 @@ int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts, int nd) {
     std::memcpy(&map, a.tc_rows_map, sizeof(map));
     bool wide = false;
     if constexpr (P <= 10) wide = a.tc_item_pairs > kMaxPairs;
+    const bool fused = a.tc_acc != nullptr;
+    auto go = [&](auto kern, int smem) {
+      launch_pdl(kern, grid, kEpilogue + kProducers + kIssuer, smem, st, map, a.n_tc_items, a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt,
+                 a.n_tc_pairs, a.tc_src, static_cast<const __half*>(a.tc_tab), static_cast<const __half*>(a.tc_Mt), a.tc_Y, a.tc_err,
+                 a.tc_wait_tries, a.tc_tgt, static_cast<const float*>(a.tc_escale), a.tc_acc);
+    };
     if (wide) {
-      if constexpr (P <= 10)
-        launch_pdl(k_m2l_tc<P, kMaxPairsWide>, grid, kEpilogue + kProducers + kIssuer, TcDims<P, kMaxPairsWide>::SMEM, st, map, a.n_tc_items,
-                   a.tc_item_tab, a.tc_item_begin, a.tc_item_cnt, a.n_tc_pairs, a.tc_src, static_cast<const __half*>(a.tc_tab),
-                   static_cast<const __half*>(a.tc_Mt), a.tc_Y, a.tc_err, a.tc_wait_tries);
+      if constexpr (P <= 10) {
+        if (fused)
+          go(k_m2l_tc<P, kMaxPairsWide, true>, TcDims<P, kMaxPairsWide>::SMEM);
+        else
+          go(k_m2l_tc<P, kMaxPairsWide, false>, TcDims<P, kMaxPairsWide>::SMEM);
+      }
     } else {
-      launch_pdl(k_m2l_tc<P, kMaxPairs>, grid, kEpilogue + kProducers + kIssuer, D::SMEM, st, map, a.n_tc_items, a.tc_item_tab,
-                 a.tc_item_begin, a.tc_item_cnt, a.n_tc_pairs, a.tc_src, static_cast<const __half*>(a.tc_tab),
-                 static_cast<const __half*>(a.tc_Mt), a.tc_Y, a.tc_err, a.tc_wait_tries);
+      if (fused)
+        go(k_m2l_tc<P, kMaxPairs, true>, D::SMEM);
+      else
+        go(k_m2l_tc<P, kMaxPairs, false>, D::SMEM);
     }
     ++launches;
   }
-  if (parts & TC_REDUCE) {
+  if ((parts & TC_REDUCE) && a.tc_acc) {
+    const int gr = (int)std::min<int64_t>(((int64_t)a.n_m2l_targets * 32 + 255) / 256, 148 * 16);
+    launch_pdl(k_m2l_tc_finalize<P>, gr, 256, 0, st, a.n_m2l_targets, a.m2l_targets, a.node_dL, a.tc_alpha, a.tc_acc, a.L);
+    ++launches;
+  } else if (parts & TC_REDUCE) {
     const int gr = (int)std::min<int64_t>(((int64_t)a.n_m2l_targets * 32 + 255) / 256, 148 * 16);
     launch_pdl(k_m2l_tc_reduce<P>, gr, 256, 0, st, a.n_m2l_targets, a.m2l_targets, a.m2l_off, a.m2l_src, a.tc_pos, a.tc_escale, a.node_dL,
                                            a.tc_alpha, a.tc_Y, a.L);
@@ -598,9 +677,12 @@ int m2l_tc_launch(const MatvecArgs& a, cudaStream_t st, int parts, int nd) {
 
 template <int P>
 void tc_tables_launch(int ntab, const double* tab, const double* alpha, __half* T, unsigned int* maxbits, cudaStream_t st) {
-  cudaFuncSetAttribute(k_m2l_tc<P, kMaxPairs>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcDims<P>::SMEM);
-  if constexpr (P <= 10)
-    cudaFuncSetAttribute(k_m2l_tc<P, kMaxPairsWide>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcDims<P, kMaxPairsWide>::SMEM);
+  cudaFuncSetAttribute(k_m2l_tc<P, kMaxPairs, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcDims<P>::SMEM);
+  cudaFuncSetAttribute(k_m2l_tc<P, kMaxPairs, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcDims<P>::SMEM);
+  if constexpr (P <= 10) {
+    cudaFuncSetAttribute(k_m2l_tc<P, kMaxPairsWide, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcDims<P, kMaxPairsWide>::SMEM);
+    cudaFuncSetAttribute(k_m2l_tc<P, kMaxPairsWide, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcDims<P, kMaxPairsWide>::SMEM);
+  }
   if (ntab > 0) k_tc_tables<P><<<ntab * TcDims<P>::RT, 128, 0, st>>>(ntab, tab, alpha, T, maxbits);
 }
 

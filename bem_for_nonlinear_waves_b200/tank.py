@@ -57,11 +57,18 @@ class Tank:
 
 def make_tank(length: float = 2.0, width: float = 1.0, depth: float = 0.5, h: float = 0.05,
               amplitude: float = 0.01, wavelength: float = 1.0, noise_sigma: float = 0.0,
-              seed: int = 0) -> Tank:
+              seed: int = 0, floating_box=None) -> Tank:
     """Closed box [0,L]x[0,W]x[-D,0] meshed as structured right-triangle grids.
 
     `noise_sigma` perturbs the z of every free-surface node with seeded Gaussian
-    noise (the points stay on the vertical wall planes)."""
+    noise (the points stay on the vertical wall planes).
+
+    `floating_box` = (xc, yc, a, b, draft, U, Omega) cuts an a x b hole (snapped to the grid)
+    centred at (xc, yc) into the free surface and closes it with the walls and bottom of a box of
+    the given draft: a floating body piercing the free surface, its faces Neumann with the rigid
+    velocity phin = (U + Omega x (x - c)) . n (bem/BEM_setBoundaryTypes.hpp:753-847), its
+    normals pointing into the box (out of the fluid).  The waterline points are shared by the free
+    surface and the body walls (CORNER points of the reference's classification)."""
     nx = max(1, int(round(length / h)))
     ny = max(1, int(round(width / h)))
     nz = max(1, int(round(depth / h)))
@@ -97,41 +104,103 @@ def make_tank(length: float = 2.0, width: float = 1.0, depth: float = 0.5, h: fl
                     tris.append(t)
                     fdir.append(dirichlet)
 
-    quad_grid(2, nz, +1, 1)   # free surface z = 0
+    hole = None
+    if floating_box is not None:
+        xc, yc, a, b, draft = (float(v) for v in floating_box[:5])
+        i0 = int(round((xc - a / 2) / (length / nx)))
+        i1 = i0 + max(1, int(round(a / (length / nx))))
+        j0 = int(round((yc - b / 2) / (width / ny)))
+        j1 = j0 + max(1, int(round(b / (width / ny))))
+        k0 = nz - max(1, int(round(draft / (depth / nz))))
+        if not (0 < i0 < i1 < nx and 0 < j0 < j1 < ny and 0 < k0 < nz):
+            raise ValueError("floating box does not fit inside the tank on this grid")
+        hole = (i0, i1, j0, j1, k0)
+
+    def box_faces(i0, i1, j0, j1, k0, k1):
+        """The walls and bottom of the box [i0,i1]x[j0,j1]x[k0,k1] (lattice indices)."""
+        def rect(fixed_axis, fixed_index, r0, r1):
+            axes = [a for a in range(3) if a != fixed_axis]
+            for u in range(r0[0], r1[0]):
+                for v in range(r0[1], r1[1]):
+                    def ijk(du, dv):
+                        idx = [0, 0, 0]
+                        idx[fixed_axis] = fixed_index
+                        idx[axes[0]] = u + du
+                        idx[axes[1]] = v + dv
+                        return point(*idx)
+                    a_, b_, c_, d_ = ijk(0, 0), ijk(1, 0), ijk(1, 1), ijk(0, 1)
+                    for t in ((a_, b_, c_), (a_, c_, d_)):
+                        tris.append(t)
+                        fdir.append(0)
+        rect(0, i0, (j0, k0), (j1, k1))
+        rect(0, i1, (j0, k0), (j1, k1))
+        rect(1, j0, (i0, k0), (i1, k1))
+        rect(1, j1, (i0, k0), (i1, k1))
+        rect(2, k0, (i0, j0), (i1, j1))
+
+    if hole is None:
+        quad_grid(2, nz, +1, 1)   # free surface z = 0
+    else:  # free surface without the box's waterplane
+        i0, i1, j0, j1, k0 = hole
+        for u in range(nx):
+            for v in range(ny):
+                if i0 <= u < i1 and j0 <= v < j1:
+                    continue
+                a_, b_, c_, d_ = point(u, v, nz), point(u + 1, v, nz), point(u + 1, v + 1, nz), point(u, v + 1, nz)
+                for t in ((a_, b_, c_), (a_, c_, d_)):
+                    tris.append(t)
+                    fdir.append(1)
     quad_grid(2, 0, -1, 0)    # bottom
     quad_grid(0, 0, -1, 0)    # x = 0
     quad_grid(0, nx, +1, 0)   # x = L
     quad_grid(1, 0, -1, 0)    # y = 0
     quad_grid(1, ny, +1, 0)   # y = W
+    n_tank_faces = len(tris)
+    if hole is not None:
+        i0, i1, j0, j1, k0 = hole
+        box_faces(i0, i1, j0, j1, k0, nz)
 
     X = np.asarray(coords, dtype=np.float64)
     tri = np.asarray(tris, dtype=np.int32)
     fdir = np.asarray(fdir, dtype=np.uint8)
 
-    # orient every triangle outward: normal . (centroid - box centre) > 0 on a box
+    # orient every tank triangle outward: normal . (centroid - box centre) > 0 on a box; the
+    # floating box's triangles point into the box (out of the fluid)
     centre = np.array([length / 2, width / 2, -depth / 2])
     n = np.cross(X[tri[:, 1]] - X[tri[:, 0]], X[tri[:, 2]] - X[tri[:, 0]])
     cen = X[tri].mean(axis=1)
     flip = np.einsum("ij,ij->i", n, cen - centre) < 0
+    body = None
+    if hole is not None:
+        i0, i1, j0, j1, k0 = hole
+        bc = np.array([(xs[i0] + xs[i1]) / 2, (ys[j0] + ys[j1]) / 2, zs[k0] / 2])
+        fb = np.arange(tri.shape[0]) >= n_tank_faces
+        flip[fb] = np.einsum("ij,ij->i", n[fb], cen[fb] - bc) > 0
+        U = np.asarray(floating_box[5] if len(floating_box) > 5 else (0.0, 0.0, 0.0), np.float64)
+        Om = np.asarray(floating_box[6] if len(floating_box) > 6 else (0.0, 0.0, 0.0), np.float64)
+        body = Body(point_begin=-1, face_begin=n_tank_faces, center=bc, U=U, Omega=Om, face_mask=fb)
     tri[flip] = tri[flip][:, [0, 2, 1]]
 
     if noise_sigma > 0.0:
         rng = np.random.default_rng(seed)
         top = np.isclose(X[:, 2], 0.0)
+        if body is not None:  # the waterline stays on the body walls
+            top &= ~np.isin(np.arange(X.shape[0]), tri[body.face_mask].reshape(-1))
         X[top, 2] += rng.normal(0.0, noise_sigma, size=int(top.sum()))
 
     return Tank(X=X, tri=tri, face_dirichlet=fdir, length=length, width=width, depth=depth,
-                amplitude=amplitude, wavenumber=2.0 * math.pi / wavelength)
+                amplitude=amplitude, wavenumber=2.0 * math.pi / wavelength, body=body)
 
 
 @dataclasses.dataclass
 class Body:
-    """A rigid box inside the fluid: its faces are Neumann with phin = (U + Omega x (x - c)) . n."""
-    point_begin: int            # first point of the body surface in the tank's point array
+    """A rigid box in the fluid: its faces are Neumann with phin = (U + Omega x (x - c)) . n."""
+    point_begin: int            # first point of the body surface in the tank's point array (-1: shared points)
     face_begin: int             # first face of the body surface
     center: np.ndarray
     U: np.ndarray
     Omega: np.ndarray
+    face_mask: "np.ndarray | None" = None  # [n_faces] True on the body's faces (None: faces >= face_begin)
 
 
 def add_box_body(tank: Tank, center, size, h: float, U=(0.0, 0.0, 0.0), Omega=(0.0, 0.0, 0.0)) -> Tank:
@@ -178,7 +247,12 @@ def known_values(tank: Tank, dof_point: np.ndarray, dof_face: np.ndarray, dof_ki
     kv[nd] = np.einsum("ij,ij->i", g, nrm)
     b = getattr(tank, "body", None)
     if b is not None:  # rigid-body Neumann data on the body surface
-        on = nd & (dof_point >= b.point_begin)
+        fmask = b.face_mask if b.face_mask is not None else (np.arange(tank.tri.shape[0]) >= b.face_begin)
+        # a point's DOF without a face belongs to the body if every face of the point does
+        pt_all_body = np.ones(X.shape[0], bool)
+        np.logical_and.at(pt_all_body, tank.tri[~fmask].reshape(-1), False)
+        on_face = (dof_face >= 0) & fmask[np.maximum(dof_face, 0)]
+        on = nd & (on_face | ((dof_face < 0) & pt_all_body[dof_point]))
         xb = X[dof_point[on]]
         vel = b.U[None, :] + np.cross(b.Omega[None, :], xb - b.center[None, :])
         kv[on] = np.einsum("ij,ij->i", vel, nrm[on[nd]])

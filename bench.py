@@ -349,11 +349,12 @@ def load_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def mixed_problems(n, seed):
-    """Tanks of mixed sizes drawn from one seed (the batch size class of the reference's
-    hot-path table, without its floating box): length U[1, 4], width 1, depth U[0.3, 1.0], h
-    chosen so the point count is log-uniform in [2k, 80k], amplitude U[0.005, 0.05],
-    wavelength U[0.5, 2]."""
+def mixed_problems(n, seed, floating_box=True):
+    """The batch workload: tanks of mixed sizes drawn from one seed -- length U[1, 4], width 1,
+    depth U[0.3, 1.0], h chosen so the point count is log-uniform in [2k, 80k], amplitude
+    U[0.005, 0.05], wavelength U[0.5, 2] -- each with a floating box 0.3 x 0.3 m, draft 0.2 m, at a
+    random x (centred in y, snapped to the grid), its faces Neumann with the rigid-body velocity of
+    seeded 6-DOF velocities U, Omega in U[-0.1, 0.1]^3."""
     from bem_for_nonlinear_waves_b200 import build_dofs, known_values, make_tank, point_normals
     rng = np.random.default_rng(seed)
     out = []
@@ -361,80 +362,193 @@ def mixed_problems(n, seed):
         L, W, D = rng.uniform(1, 4), 1.0, rng.uniform(0.3, 1.0)
         pts = math.exp(rng.uniform(math.log(2e3), math.log(8e4)))
         h = math.sqrt(2 * (L * W + L * D + W * D) / pts)
-        t = make_tank(L, W, D, h, amplitude=rng.uniform(0.005, 0.05), wavelength=rng.uniform(0.5, 2.0))
+        amp, wl = rng.uniform(0.005, 0.05), rng.uniform(0.5, 2.0)
+        xb = rng.uniform(0.3, L - 0.3)
+        U, Om = rng.uniform(-0.1, 0.1, 3), rng.uniform(-0.1, 0.1, 3)
+        fb = (xb, W / 2, 0.3, 0.3, 0.2, U, Om) if floating_box else None
+        t = make_tank(L, W, D, h, amplitude=amp, wavelength=wl, floating_box=fb)
         d = build_dofs(t.X, t.tri, t.face_dirichlet)
         out.append((t, d, known_values(t, d["dof_point"], d["dof_face"], d["dof_kind"], point_normals(t))))
     return out
 
 
 def run_batch(args, cfg, local):
-    """Serving mode: `--batch P` seeded tanks of the workload's size (different free
-    surfaces) go to a BatchSolver with `--workers W` contexts at once; reports whole-batch
-    solves/s and per-problem latency from submission to result (p50 / p99), next to the same
-    problems solved one after another on one context."""
+    """Batch mode.  `--mixed-sizes`: the 96-tank batch workload (mixed_problems: 2k-80k points,
+    floating box, p = 8).  Every problem is first solved by the FP64 GPU path at relative residual
+    1e-12 (its oracle, not timed); then, at the accuracy gate's tolerance, (a) the batch through a
+    BatchSolver of `--workers W` mixed-precision contexts, all submitted at once or with seeded
+    Poisson arrivals (`--arrival-rate`), with per-problem latency from submission to result, and
+    (b) the same problems one after another through the plain FP64 GPU path; both solutions are
+    checked against the oracle.  Without `--mixed-sizes`: `--batch P` seeded tanks of the
+    workload's size."""
     from bem_for_nonlinear_waves_b200 import BEM_BVP, BatchSolver
-    rank = 0
     if args.mixed_sizes:
         probs = mixed_problems(args.batch, 2024)
-        cfg = dict(cfg, p=8, rel_tol=1e-8)
+        cfg = dict(cfg, p=8)
+        workload = "mixed_2k_80k_floating_box_p8"
     else:
-        probs = [make_problem(cfg, rank + 1000 + i) for i in range(args.batch)]
-    kw = dict(expansion_order=cfg["p"], solver_tol=cfg["rel_tol"], tol_relative=True, solver_max_iter=args.max_iter,
-              preconditioner=args.precond, poly_degree=args.poly_degree, device=local, precision=args.precision)
-    one = BEM_BVP(probs[0][0].X, probs[0][0].tri, probs[0][0].face_dirichlet, dofs=probs[0][1], **kw)
-    for _ in range(args.warmup):
-        one.setup()
-        one.solve(probs[0][2])
-    w0 = time.perf_counter()
-    seq_lat = []
+        probs = [make_problem(cfg, 1000 + i) for i in range(args.batch)]
+        workload = args.config
+    tol = args.tol or 1e-11
+    base = dict(expansion_order=cfg["p"], tol_relative=True, solver_max_iter=args.max_iter, preconditioner=args.precond,
+                poly_degree=args.poly_degree, device=local)
+    # oracles: the FP64 GPU solve of each problem at relative residual 1e-12
+    refs = []
     for t, d, kv in probs:
-        b = BEM_BVP(t.X, t.tri, t.face_dirichlet, dofs=d, **kw)
+        b = BEM_BVP(t.X, t.tri, t.face_dirichlet, dofs=d, solver_tol=ORACLE_REL_TOL, precision="fp64", **dict(base, solver_max_iter=4000))
+        b.solve(kv)
+        refs.append(b.ans.copy())
+        del b
+
+    def err(ans, ref):
+        return float(np.abs(ans - ref).max() / np.abs(ref).max())
+
+    # (b) plain FP64 GPU path, one after another (one warm solve first)
+    b = BEM_BVP(probs[0][0].X, probs[0][0].tri, probs[0][0].face_dirichlet, dofs=probs[0][1], solver_tol=tol, precision="fp64", **base)
+    b.solve(probs[0][2])
+    del b
+    seq_lat, seq_err = [], []
+    w0 = time.perf_counter()
+    for (t, d, kv), ref in zip(probs, refs):
+        b = BEM_BVP(t.X, t.tri, t.face_dirichlet, dofs=d, solver_tol=tol, precision="fp64", **base)
         s0 = time.perf_counter()
         b.solve(kv)
         seq_lat.append(time.perf_counter() - s0)
+        seq_err.append(err(b.ans, ref))
         del b
     seq_s = time.perf_counter() - w0
-    bs = BatchSolver(args.workers, **kw)
-    for _ in range(args.warmup):  # every worker context warm
-        for tk in [bs.submit(t.X, t.tri, t.face_dirichlet, kv, dofs=d) for t, d, kv in probs[:args.workers]]:
-            bs.result(tk)
+    # (a) the batched mixed-precision solver
+    bs = BatchSolver(args.workers, solver_tol=tol, precision=args.precision, tc_deterministic=bool(args.tc_deterministic), **base)
+    for tk in [bs.submit(t.X, t.tri, t.face_dirichlet, kv, dofs=d) for t, d, kv in probs[:args.workers]]:
+        bs.result(tk)  # every worker context warm
     with ClockSampler(local) as clk:
         w0 = time.perf_counter()
-        sub = {}
-        lat = {}
+        sub, lat = {}, {}
 
         def reap():
             for tk in sub:
                 if tk not in lat and bs.done(tk):
                     lat[tk] = time.perf_counter() - sub[tk]
 
-        # all at once, or Poisson arrivals at --arrival-rate requests/s (seeded)
         gaps = np.random.default_rng(77).exponential(1.0 / args.arrival_rate, len(probs)) if args.arrival_rate > 0 else None
         t_next = w0
+        order = []
         for i, (t, d, kv) in enumerate(probs):
             if gaps is not None:
                 t_next += gaps[i]
                 while time.perf_counter() < t_next:
                     reap()
                     time.sleep(0.0002)
-            sub[bs.submit(t.X, t.tri, t.face_dirichlet, kv, dofs=d)] = time.perf_counter()
+            tk = bs.submit(t.X, t.tri, t.face_dirichlet, kv, dofs=d)
+            sub[tk] = time.perf_counter()
+            order.append(tk)
         while len(lat) < len(sub):
             reap()
             time.sleep(0.0005)
         batch_s = time.perf_counter() - w0
-    conv = all(bs.result(tk)[2].converged for tk in sub)
+    b_err, conv = [], True
+    for tk, (t, d, kv), ref in zip(order, probs, refs):
+        phi, phin, st = bs.result(tk)
+        conv = conv and bool(st.converged)
+        b_err.append(err(np.where(d["dof_kind"] == 0, phin, phi), ref))
     bs.close()
     lats = sorted(lat.values())
     pct = lambda v, q: float(np.percentile(np.asarray(v), q))  # noqa: E731
-    line = {"metric": "bvp_solves_per_s", "value": len(probs) / batch_s, "unit": "solves/s", "n_gpus": 1, "mode": "batch",
+    value = len(probs) / batch_s
+    seq_v = len(probs) / seq_s
+    line = {"metric": "bvp_solves_per_s", "value": value, "unit": "solves/s", "n_gpus": 1, "mode": "batch",
             "higher_is_better": True, "dtype": "f64/f16x3-tc" if args.precision == "mixed" else "f64", "data": "synthetic",
-            "config": {"workload": "mixed_2k_80k_p8" if args.mixed_sizes else args.config, "problems": len(probs),
-                       "points": [int(p[0].n_points) for p in probs], "workers": args.workers, "precision": args.precision,
-                       "preconditioner": args.precond, "converged": bool(conv),
+            "config": {"workload": workload, "problems": len(probs), "points": [int(p[0].n_points) for p in probs],
+                       "workers": args.workers, "precision": args.precision, "preconditioner": args.precond, "rel_tol": tol,
                        "arrivals": f"poisson {args.arrival_rate}/s" if args.arrival_rate > 0 else "all at once"},
             "latency_s": {"p50": pct(lats, 50), "p99": pct(lats, 99), "max": lats[-1]},
-            "sequential": {"solves_per_s": len(probs) / seq_s, "latency_p50_s": pct(seq_lat, 50)},
+            "accuracy": {"gate": GATE, "max_rel_err_batch": max(b_err), "max_rel_err_fp64": max(seq_err),
+                         "within_gate": bool(max(b_err) <= GATE and max(seq_err) <= GATE), "converged": conv},
+            "fp64_gpu_sequential": {"solves_per_s": seq_v, "latency_p50_s": pct(seq_lat, 50), "latency_p99_s": pct(seq_lat, 99)},
+            "speedup_vs_fp64_gpu": value / seq_v,
             "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def chain_problems(n, seed, median=15000, sigma=0.75, lo=3000, hi=200000):
+    """The serving workload's tanks: as mixed_problems (floating box), with point counts
+    lognormal around `median` (sigma in log space), clipped to [lo, hi]."""
+    from bem_for_nonlinear_waves_b200 import build_dofs, known_values, make_tank, point_normals
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        L, W, D = rng.uniform(1, 4), 1.0, rng.uniform(0.3, 1.0)
+        pts = float(np.clip(median * math.exp(rng.normal(0.0, sigma)), lo, hi))
+        h = math.sqrt(2 * (L * W + L * D + W * D) / pts)
+        amp, wl = rng.uniform(0.005, 0.05), rng.uniform(0.5, 2.0)
+        xb = rng.uniform(0.3, L - 0.3)
+        U, Om = rng.uniform(-0.1, 0.1, 3), rng.uniform(-0.1, 0.1, 3)
+        t = make_tank(L, W, D, h, amplitude=amp, wavelength=wl, floating_box=(xb, W / 2, 0.3, 0.3, 0.2, U, Om))
+        d = build_dofs(t.X, t.tri, t.face_dirichlet)
+        out.append((t, d, known_values(t, d["dof_point"], d["dof_face"], d["dof_kind"], point_normals(t))))
+    return out
+
+
+def run_serve(args, local):
+    """Serving mode: `--serve-chains R` requests, each a whole RK4 time-stepping chain of
+    `--chain-steps` steps (4 BVPs per step, the MEL update between them) on a tank of the serving
+    workload (chain_problems), arriving as a seeded Poisson stream of `--arrival-rate` requests/s,
+    served by a BatchSolver of `--workers` contexts with admission by device memory (150 GB, or
+    90 % of the free memory if less).  Run for the mixed-precision and the plain FP64 solver;
+    reports request latency p50/p99 (arrival to result) and BVP solves/s."""
+    import torch
+    from bem_for_nonlinear_waves_b200 import BatchSolver
+    probs = chain_problems(args.serve_chains, 4242)
+    free = torch.cuda.mem_get_info(local)[0]
+    budget = int(min(150e9, 0.9 * free))
+    tol = args.tol or 1e-11
+    out = {}
+    for prec in ("mixed", "fp64"):
+        bs = BatchSolver(args.workers, expansion_order=8, solver_tol=tol, tol_relative=True, solver_max_iter=args.max_iter,
+                         preconditioner=args.precond, device=local, precision=prec)
+        bs.set_budget(budget)
+        t0, d0, k0 = probs[0]  # every worker context warm
+        for tk in [bs.submit(t0.X, t0.tri, t0.face_dirichlet, k0, dofs=d0) for _ in range(args.workers)]:
+            bs.result(tk)
+        gaps = np.random.default_rng(99).exponential(1.0 / args.arrival_rate, len(probs))
+        sub, lat, order = {}, {}, []
+        with ClockSampler(local) as clk:
+            w0 = time.perf_counter()
+            t_next = w0
+            for i, (t, d, kv) in enumerate(probs):
+                t_next += gaps[i]
+                while time.perf_counter() < t_next:
+                    time.sleep(0.0002)
+                tk = bs.submit_chain(t.X, t.tri, t.face_dirichlet, kv, n_steps=args.chain_steps, dt=1e-3, dofs=d)
+                sub[tk] = time.perf_counter()
+                order.append(tk)
+            while len(lat) < len(sub):
+                for tk in order:
+                    if tk not in lat and bs.done(tk):
+                        lat[tk] = time.perf_counter() - sub[tk]
+                time.sleep(0.001)
+            wall = time.perf_counter() - w0
+        iters, conv = 0, True
+        for tk in order:
+            _, _, st = bs.result_chain(tk)
+            iters += st.iterations
+            conv = conv and bool(st.converged)
+        stats = bs.stats()
+        bs.close()
+        solves = len(probs) * args.chain_steps * 4
+        lats = sorted(lat.values())
+        out[prec] = {"solves_per_s": solves / wall, "requests_per_s": len(probs) / wall,
+                     "latency_s": {"p50": float(np.percentile(lats, 50)), "p99": float(np.percentile(lats, 99)), "max": lats[-1]},
+                     "gmres_iterations_per_solve": iters / solves, "converged": conv, "admission": stats, "clocks": clk.summary()}
+    line = {"metric": "bvp_solves_per_s", "value": out["mixed"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "mode": "serve",
+            "higher_is_better": True, "dtype": "f64/f16x3-tc", "data": "synthetic",
+            "config": {"workload": "rk4_chains_lognormal_15k_floating_box_p8", "requests": len(probs), "chain_steps": args.chain_steps,
+                       "bvps_per_request": 4 * args.chain_steps, "points": [int(p[0].n_points) for p in probs],
+                       "arrivals": f"poisson {args.arrival_rate}/s", "workers": args.workers, "hbm_budget_bytes": budget,
+                       "rel_tol": tol},
+            "mixed": out["mixed"], "fp64": out["fp64"],
+            "speedup_vs_fp64_gpu": out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"]}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -485,6 +599,9 @@ def main():
     ap.add_argument("--poly-degree", type=int, default=8, help="degree of the near_poly preconditioner")
     ap.add_argument("--overlap-near", type=int, default=0, help="1: near field of the mixed A.x on a second stream")
     ap.add_argument("--max-iter", type=int, default=1500)
+    ap.add_argument("--refine-rtol", type=float, default=0.0, help="mixed: inner-cycle relative tolerance (0: library default)")
+    ap.add_argument("--tc-deterministic", type=int, default=0,
+                    help="mixed: 1 = tensor-core M2L partials summed in a fixed order (bit-reproducible), 0 = fused L2 reduction")
     ap.add_argument("--tol", type=float, default=0.0,
                     help="relative tolerance of the timed solves (0: the loosest of 1e-9..1e-12 within half the accuracy gate)")
     ap.add_argument("--ref-iters", type=int, default=1000)
@@ -496,10 +613,16 @@ def main():
     ap.add_argument("--workers", type=int, default=2)
     ap.add_argument("--mixed-sizes", action="store_true", help="serving mode over tanks of 2k-80k points (p = 8)")
     ap.add_argument("--arrival-rate", type=float, default=0.0, help="serving mode: Poisson arrivals per second (0: all at once)")
+    ap.add_argument("--serve-chains", type=int, default=0, help="serving mode: number of RK4-chain requests (one GPU)")
+    ap.add_argument("--chain-steps", type=int, default=20, help="serving mode: RK4 steps per chain request")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference(args, cfg)
+    if args.serve_chains > 0:
+        if args.arrival_rate <= 0:
+            args.arrival_rate = 200.0
+        return run_serve(args, int(os.environ.get("LOCAL_RANK", "0")))
     if args.batch > 0:
         return run_batch(args, cfg, int(os.environ.get("LOCAL_RANK", "0")))
 
@@ -512,7 +635,8 @@ def main():
     def make(prec, tol, precond=None, max_iter=None):
         return BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=cfg["p"], solver_tol=tol, tol_relative=True,
                        solver_max_iter=max_iter or args.max_iter, preconditioner=precond or args.precond, poly_degree=args.poly_degree,
-                       overlap_near=args.overlap_near, dofs=d, device=local, precision=prec)
+                       overlap_near=args.overlap_near, dofs=d, device=local, precision=prec, refine_rtol=args.refine_rtol,
+                       tc_deterministic=bool(args.tc_deterministic))
 
     if args.count_reference_iterations:
         tol = args.tol or cfg["rel_tol"]

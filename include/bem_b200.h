@@ -71,6 +71,12 @@ typedef struct {
                                 depend on it) */
   int32_t overlap_near;      /* mixed: 1 = the near field of A.x runs on a second stream while the FMM
                                 passes run, its far part added after; 0 = one fused kernel after them */
+  double refine_rtol;        /* mixed: each inner GMRES cycle on the low-precision operator stops at
+                                max(tol, refine_rtol * |r|) before the FP64 residual update (0: 1e-5) */
+  int32_t tc_deterministic;  /* mixed: 0 = the tensor-core M2L adds each pair's translated expansion into
+                                its target's FP32 accumulator in L2 (fast; the summation order, and so the
+                                last bits, vary between runs); 1 = per-pair partials summed in a fixed
+                                order (bit-reproducible, one more pass over HBM) */
 } bem_gpu_opts;
 
 /* One boundary-value problem.  The DOF table is what the reference's setNodeFaceIndices()
@@ -191,6 +197,12 @@ int bem_gpu_matvec_device(bem_gpu_ctx* ctx, const double* d_x, double* d_y);
  * BEM_solveBVP_GMRES_FMM.hpp:2124-2155). */
 int bem_gpu_matvec_device_noalloc(bem_gpu_ctx* ctx, const double* d_x, double* d_y);
 
+/* Device bytes a context's buffers hold now (they keep their size across set-ups), and an
+ * estimate of a BVP's device bytes from its sizes alone (no GPU needed), for admission control.
+ * No counterpart in the reference. */
+int64_t bem_gpu_device_bytes(const bem_gpu_ctx* ctx);
+int64_t bem_gpu_estimate_bytes(const bem_gpu_opts* opts, const bem_bvp_desc* desc);
+
 /* Introspection for parity tests. */
 int bem_gpu_get_diag(bem_gpu_ctx* ctx, double* diag);                 /* [n_dof] */
 double bem_gpu_scale_factor(const bem_gpu_ctx* ctx);                  /* L */
@@ -241,6 +253,27 @@ int bem_gpu_batch_submit(bem_gpu_batch* batch, const bem_bvp_desc* desc, const d
                          bem_gpu_stats* stats, int64_t* ticket);
 int bem_gpu_batch_poll(bem_gpu_batch* batch, int64_t ticket, int32_t wait);
 int bem_gpu_batch_release(bem_gpu_batch* batch, int64_t ticket);   /* forget a finished ticket; NOT_READY if unknown or pending */
+/* Admission by device memory: the queue's head request starts only while the bytes the worker
+ * contexts hold (each replaced, for the worker taking the request, by the larger of its own and
+ * the request's bem_gpu_estimate_bytes) stay within `bytes`; an idle worker whose buffers keep
+ * the head out gives them back.  A request above the budget alone ends with
+ * BEM_ERR_OUT_OF_MEMORY.  0 = no limit (the default). */
+int bem_gpu_batch_set_budget(bem_gpu_batch* batch, int64_t bytes);
+/* A whole Runge-Kutta time-stepping chain of a BEM-MEL simulation as one request: n_steps steps
+ * of 4 stages, each a set-up at the stage positions (bem_gpu_setup first, then
+ * bem_gpu_setup_refresh), a solve warm-started from the previous stage's solution, and the MEL
+ * stage update (bem_gpu_mel_stage, dt, gravity) whose positions and point phi give the next
+ * stage's geometry and Dirichlet values (bem/main_time_domain.cpp:1071-2600); Neumann values stay
+ * as given.  point_flags as bem_gpu_build_dofs.  Outputs the positions [3*n_points] and point phi
+ * [n_points] at the end; stats sums the chain's solves (iterations, times, operator
+ * applications; converged = every solve converged). */
+int bem_gpu_batch_submit_chain(bem_gpu_batch* batch, const bem_bvp_desc* desc, const uint8_t* point_flags, const double* known,
+                               int32_t n_steps, double dt, double gravity, double* out_X, double* out_phi_point,
+                               bem_gpu_stats* stats, int64_t* ticket);
+/* out[6]: requests admitted, admissions that had to wait for device memory, worker contexts
+ * recreated to give memory back, device bytes held (or reserved) by the workers now, the
+ * budget, requests queued. */
+int bem_gpu_batch_stats(bem_gpu_batch* batch, int64_t* out);
 const char* bem_gpu_batch_last_error(const bem_gpu_batch* batch);  /* message of this thread's last polled failure */
 void bem_gpu_batch_destroy(bem_gpu_batch* batch);                  /* finishes queued problems first */
 

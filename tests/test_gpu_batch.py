@@ -1,8 +1,9 @@
 """Batch / asynchronous solving (bem_gpu_batch_*): several tanks of different sizes queued on
-two or three workers give exactly the solutions of one-at-a-time solves (every reduction on
-the device has a fixed order, so the results are bit-identical), tickets poll NOT_READY
-before they finish, and a problem that fails set-up reports its error without stopping the
-others."""
+two or three workers give exactly the solutions of one-at-a-time solves when every device
+reduction has a fixed order (FP64, and mixed precision with tc_deterministic: bit-identical),
+and the same solutions within the solve's tolerance with the tensor-core M2L's fused L2
+reduction (whose FP32 summation order varies); tickets poll NOT_READY before they finish, and a
+problem that fails set-up reports its error without stopping the others."""
 import numpy as np
 import pytest
 
@@ -21,7 +22,7 @@ def _problem(h, seed):
 @pytest.mark.parametrize("precision,workers", [("fp64", 2), ("mixed", 3)])
 def test_batch_matches_sequential(product_lib, precision, workers):
     kw = dict(expansion_order=8, solver_tol=1e-9, tol_relative=True, solver_max_iter=800, preconditioner="jacobi",
-              precision=precision)
+              precision=precision, tc_deterministic=True)
     probs = [_problem(h, s) for h, s in [(0.05, 1), (0.04, 2), (0.06, 3), (0.045, 4), (0.05, 5)]]
     ref = []
     for t, d, known in probs:
@@ -38,6 +39,26 @@ def test_batch_matches_sequential(product_lib, precision, workers):
         assert st.iterations == it0
         assert np.array_equal(phi, phi0)
         assert np.array_equal(phin, phin0)
+    bs.close()
+
+
+def test_batch_matches_sequential_fused_reduction(product_lib):
+    kw = dict(expansion_order=8, solver_tol=1e-10, tol_relative=True, solver_max_iter=800, preconditioner="jacobi",
+              precision="mixed")
+    probs = [_problem(h, s) for h, s in [(0.05, 1), (0.04, 2), (0.06, 3)]]
+    ref = []
+    for t, d, known in probs:
+        b = BEM_BVP(t.X, t.tri, t.face_dirichlet, dofs=d, **kw)
+        b.solve(known)
+        assert b.last_gmres_converged
+        ref.append(b.ans.copy())
+    bs = BatchSolver(3, **kw)
+    tickets = [bs.submit(t.X, t.tri, t.face_dirichlet, known, dofs=d) for t, d, known in probs]
+    for a0, tk, (t, d, known) in zip(ref, tickets, probs):
+        phi, phin, st = bs.result(tk)
+        assert st.converged == 1
+        ans = np.where(d["dof_kind"] == 0, phin, phi)
+        assert np.abs(ans - a0).max() <= 1e-7 * np.abs(a0).max()
     bs.close()
 
 

@@ -64,3 +64,32 @@ def test_mixed_solve_matches_fp64(product_lib, precond, tol, agree):
     assert np.abs(a - b).max() <= agree * np.abs(b).max()
     assert sols["mixed"][2] > 0 and sols["fp64"][2] == 0
     assert sols["mixed"][1] < sols["mixed"][2]  # most operator applications are low precision
+
+
+@pytest.mark.parametrize("p", [10, 12])
+def test_fused_reduction_matches_fixed_order(product_lib, p):
+    """The tensor-core M2L's two reductions: each pair added into its target's FP32 accumulator in
+    L2 (default; the summation order varies), or per-pair partials summed in a fixed order in FP64
+    (tc_deterministic; repeated applications are bit-identical).  Both apply the same operator to
+    FP32 rounding of the M2L sums: within 1e-6 of each other relative to the vector maximum."""
+    import torch
+
+    t = _tank()
+    fused = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=p, precision="mixed")
+    fixed = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=p, precision="mixed", tc_deterministic=True)
+    fused.setup()
+    fixed.setup()
+    n = fused.matrix_size
+    x = torch.randn(n, dtype=torch.float64, generator=torch.Generator().manual_seed(9)).cuda()
+    ys = [torch.empty_like(x) for _ in range(4)]
+    torch.cuda.synchronize()
+    fused.matvec_device(x.data_ptr(), ys[0].data_ptr(), mixed=True)
+    fused.matvec_device(x.data_ptr(), ys[1].data_ptr(), mixed=True)
+    fixed.matvec_device(x.data_ptr(), ys[2].data_ptr(), mixed=True)
+    fixed.matvec_device(x.data_ptr(), ys[3].data_ptr(), mixed=True)
+    torch.cuda.synchronize()
+    a, a2, b, b2 = (y.cpu().numpy() for y in ys)
+    scale = np.abs(b).max()
+    assert np.array_equal(b, b2)
+    assert np.abs(a - b).max() <= 1e-6 * scale
+    assert np.abs(a2 - b).max() <= 1e-6 * scale

@@ -1,8 +1,8 @@
 """The low-precision A.x with its near field on a second stream (concurrent with the FMM
 passes, far field added afterwards; opts.overlap_near = 1) against the single-stream fused
 form: the same operator up to the association of one sum per row (near + far - diag x), so
-one application agrees to 1e-13 relative, and both solves converge to the same solution within
-the tolerance."""
+one application agrees to 1e-13 relative (with the fixed-order M2L reduction, tc_deterministic),
+and both solves converge to the same solution within the tolerance."""
 import numpy as np
 import pytest
 
@@ -17,8 +17,8 @@ def test_overlapped_operator_equals_fused(product_lib, p):
 
     t = make_tank(1.0, 0.5, 0.4, 0.04, amplitude=0.02, wavelength=0.7, noise_sigma=0.1, seed=61)
     d = build_dofs(t.X, t.tri, t.face_dirichlet)
-    a = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=p, precision="mixed", dofs=d, overlap_near=True)
-    b = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=p, precision="mixed", dofs=d, overlap_near=False)
+    a = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=p, precision="mixed", dofs=d, overlap_near=True, tc_deterministic=True)
+    b = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=p, precision="mixed", dofs=d, overlap_near=False, tc_deterministic=True)
     a.setup()
     b.setup()
     n = a.matrix_size
@@ -38,7 +38,8 @@ def test_overlapped_solve(product_lib):
     t = make_tank(1.0, 0.5, 0.4, 0.04, amplitude=0.02, wavelength=0.7, noise_sigma=0.1, seed=62)
     d = build_dofs(t.X, t.tri, t.face_dirichlet)
     k = known_values(t, d["dof_point"], d["dof_face"], d["dof_kind"], point_normals(t))
-    kw = dict(expansion_order=10, solver_tol=1e-11, tol_relative=True, preconditioner="jacobi", precision="mixed", dofs=d)
+    kw = dict(expansion_order=10, solver_tol=1e-11, tol_relative=True, preconditioner="jacobi", precision="mixed", dofs=d,
+              tc_deterministic=True)
     a = BEM_BVP(t.X, t.tri, t.face_dirichlet, overlap_near=True, **kw)
     b = BEM_BVP(t.X, t.tri, t.face_dirichlet, overlap_near=False, **kw)
     a.solve(k)

@@ -2,7 +2,7 @@
 the octree root (the reference's rebin path, bem/BEM_solveBVP_GMRES_FMM.hpp:3125-3346) and,
 when the structure is unchanged, the device's structural arrays.  Where the bounding box (hence
 the scaling and the root) does not change, the refreshed operator must be the operator of a
-fresh set-up bit for bit."""
+fresh set-up bit for bit (mixed precision with its fixed-order M2L reduction, tc_deterministic)."""
 import dataclasses
 
 import numpy as np
@@ -45,7 +45,7 @@ def test_refresh_same_coordinates_bit_exact(product_lib, precision):
     t, d = _tank(41)
     k = _known(t, d, t.X)
     b = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=8, solver_tol=1e-10, tol_relative=True, preconditioner="jacobi",
-                precision=precision, dofs=d)
+                precision=precision, dofs=d, tc_deterministic=True)
     b.solve(k)
     a0 = b.ans.copy()
     assert b.refresh(np.array(t.X)) == 2
@@ -59,7 +59,8 @@ def test_refresh_equals_fresh_setup_in_the_same_root(product_lib, precision, eps
     t, d = _tank(42)
     X1 = _interior_shift(t, eps, seed=5)
     k1 = _known(t, d, X1)
-    kw = dict(expansion_order=8, solver_tol=1e-10, tol_relative=True, preconditioner="jacobi", precision=precision, dofs=d)
+    kw = dict(expansion_order=8, solver_tol=1e-10, tol_relative=True, preconditioner="jacobi", precision=precision, dofs=d,
+              tc_deterministic=True)
     b = BEM_BVP(t.X, t.tri, t.face_dirichlet, **kw)
     b.setup()
     kept = b.refresh(X1)

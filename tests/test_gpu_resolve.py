@@ -1,7 +1,8 @@
 """Several right-hand sides on one set-up (the phi_t BVP of a floating-body step, or the next
 Runge-Kutta stage with unchanged geometry, reuses the operator: BEM_solveBVP.hpp:922-1040).
 A second solve on a set-up context must equal a fresh set-up + solve bit for bit (the set-up
-is deterministic and nothing of the first solve leaks into the second), and the solution is
+is deterministic -- for mixed precision with the fixed-order M2L reduction -- and nothing of
+the first solve leaks into the second), and the solution is
 linear in the known boundary values (to the solve tolerance)."""
 import numpy as np
 import pytest
@@ -19,7 +20,7 @@ def test_resolve_on_one_setup(product_lib, precision):
     rng = np.random.default_rng(4)
     k2 = -0.7 * k1 + 0.01 * rng.standard_normal(k1.shape)
     kw = dict(expansion_order=8, solver_tol=1e-11, tol_relative=True, solver_max_iter=1500, preconditioner="jacobi",
-              precision=precision, dofs=d)
+              precision=precision, dofs=d, tc_deterministic=True)
     b = BEM_BVP(t.X, t.tri, t.face_dirichlet, **kw)
     b.solve(k1)
     a1 = b.ans.copy()

@@ -5,7 +5,7 @@ to 0 through bem_gpu_set_wait_limit, the first pipeline wait of every CTA gives 
 CTA records the failure, waits (with the default limit) for its own copies and MMAs already in
 flight, frees its tensor memory and returns.  The host then reads BEM_ERR_DEVICE from
 bem_gpu_check_device_status, and after restoring the limit the same context computes the same
-mixed-precision mat-vec as before, bit for bit."""
+mixed-precision mat-vec as before, bit for bit (fixed-order M2L reduction)."""
 import numpy as np
 import pytest
 
@@ -19,7 +19,7 @@ def test_tc_wait_timeout_is_reported_and_context_recovers(product_lib):
     import torch
 
     t = make_tank(1.0, 0.5, 0.4, 0.04, amplitude=0.02, wavelength=0.7, noise_sigma=0.1, seed=3)
-    bvp = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=10, precision="mixed")
+    bvp = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=10, precision="mixed", tc_deterministic=True)
     bvp.setup()
     assert bvp.tree_stats()["m2l_pairs"] > 0
     lib = L.load()
