@@ -250,12 +250,14 @@ class BEM_BVP:
 
     def near_bytes(self):
         """Algorithmic bytes of one near-field SpMV of A.x: stored weight blocks in FP64 and in FP32
-        (rows padded to 4 columns), the gathered unknowns (8 B per block column) and the rows
+        (rows padded to 4 columns), the gathered unknowns (8 B per block column) and their DOF
+        indices (4 B per block column), the per-target near sums (8 B per target) and the rows
         written (8 B per DOF)."""
         out = np.zeros(6, np.int64)
         self._check(self.lib.bem_gpu_near_stats(self.ctx, L.ptr(out, L.P_i64)), "near_stats")
         return {"weights_fp64": 8 * int(out[0]), "weights_fp32": 4 * int(out[1]), "x_gather": 8 * int(out[2]),
-                "rows": 8 * int(out[5]), "blocks": int(out[3]), "targets": int(out[4])}
+                "dof_index": 4 * int(out[2]), "near_sums": 8 * int(out[4]), "rows": 8 * int(out[5]), "blocks": int(out[3]),
+                "targets": int(out[4])}
 
     def device_bytes(self):
         """Device bytes the context's buffers hold."""
@@ -267,10 +269,10 @@ class BEM_BVP:
     def profile_matvec(self, repeats=10, mixed=False):
         """Per-stage mat-vec time in ms (CUDA events on the solver stream); mixed=True profiles
         the tensor-core operator of a precision="mixed" context."""
-        st = np.zeros(9)
+        st = np.zeros(10)
         fn = self.lib.bem_gpu_profile_matvec_mixed if mixed else self.lib.bem_gpu_profile_matvec
         self._check(fn(self.ctx, int(repeats), L.ptr(st, L.P_dbl)), "profile")
-        keys = ["p2m", "m2m", "m2l", "l2l", "targets", "total"] + (["m2l_expand", "m2l_contract", "m2l_reduce"] if mixed else [])
+        keys = ["p2m", "m2m", "m2l", "l2l", "targets", "total"] + (["m2l_expand", "m2l_contract", "m2l_reduce", "near_sums"] if mixed else [])
         return dict(zip(keys, map(float, st)))
 
     def matvec_device(self, d_x, d_y, mixed=False):

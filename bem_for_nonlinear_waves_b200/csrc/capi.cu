@@ -173,7 +173,7 @@ struct bem_gpu_ctx {
   // mixed precision: tensor-core M2L tables and buffers; graph of the low-precision A.x
   bool mixed = false;
   DBuf<int> tc_item_tab{&dev_bytes}, tc_item_begin{&dev_bytes}, tc_item_cnt{&dev_bytes}, tc_pos{&dev_bytes}, tc_src{&dev_bytes}, tc_err{&dev_bytes};
-  DBuf<int> near_err{&dev_bytes};  // k_targets_ax: a bounded wait gave up
+  DBuf<double> near_sum{&dev_bytes};  // near sums of A.x by target slot
   DBuf<double> tc_tabvec{&dev_bytes}, tc_alpha{&dev_bytes}, node_dL{&dev_bytes};
   DBuf<uint16_t> tc_T{&dev_bytes}, tc_Mt{&dev_bytes};
   DBuf<float> tc_escale{&dev_bytes};
@@ -273,7 +273,7 @@ struct bem_gpu_ctx {
     a.L = L.p;
     a.n_blocks = (int)plan.blocks.size();
     a.chunk = chunk;
-    a.near_err = near_err.p;
+    a.near_sum = near_sum.p;
     a.max_ntgt = max_ntgt;
     a.blocks = blocks.p;
     a.nb_dofs = nb_dofs.p;
@@ -976,9 +976,6 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   CK(ups(ctx->m2l_targets, mt));
   CK(ups(ctx->m2l_off, P.m2l_off));
   CK(ups(ctx->m2l_src, P.m2l_src));
-  // 4 spare elements: k_targets_ax copies 16-byte aligned windows of nb_dofs, which may reach
-  // up to 3 elements past the last block's DOFs
-  CK(ctx->nb_dofs.alloc(P.nb_dofs.size() + 4));
   CK(upn(ctx->nb_dofs, P.nb_dofs));
   CK(upn(ctx->nb_targets, P.nb_targets));
   CK(upn(ctx->nb_ranges, P.nb_ranges));
@@ -1167,8 +1164,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     launch_s_tables(P.opt.p, (int)P.grp_off.size() - 1, ctx->grp_vec.p, ctx->Sg.p, s);
     ctx->launches += 1;
   }
-  CK(ctx->near_err.alloc(1));
-  CK(cudaMemsetAsync(ctx->near_err.p, 0, sizeof(int), s));
+  CK(ctx->near_sum.alloc(std::max<size_t>(P.nb_targets.size(), 1)));
   if (ctx->mixed) {
     CK(cudaMemsetAsync(ctx->tc_Mt.p, 0, sizeof(uint16_t) * ctx->tc_Mt.n, s));
     CK(cudaMemsetAsync(ctx->tc_acc.p, 0, sizeof(float) * ctx->tc_acc.n, s));
@@ -1862,6 +1858,13 @@ int profile_matvec(bem_gpu_ctx* ctx, int repeats, bool tc, double* stage_ms) {
       CK(cudaEventElapsedTime(&ms, e0, e1));
       stage_ms[6 + k] = ms / repeats;
     }
+    CK(cudaEventRecord(e0, s));
+    for (int r = 0; r < repeats; ++r) launch_near_sums(a, s);
+    CK(cudaEventRecord(e1, s));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    stage_ms[9] = ms / repeats;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1909,16 +1912,12 @@ int bem_gpu_set_wait_limit(bem_gpu_ctx* ctx, int64_t tries) {
 int bem_gpu_check_device_status(bem_gpu_ctx* ctx) {
   if (!ctx) return BEM_ERR_INVALID_ARGUMENT;
   if (!ctx->ready) return BEM_OK;
-  int flag[2] = {0, 0};
-  CK(cudaMemcpyAsync(&flag[0], ctx->near_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  if (ctx->mixed) CK(cudaMemcpyAsync(&flag[1], ctx->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  if (!ctx->mixed) return BEM_OK;  // only the tensor-core M2L waits on the device
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, ctx->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  if (flag[1]) {
+  if (flag) {
     ctx->err = "tensor-core M2L: a bounded wait on the MMA completion gave up";
-    return BEM_ERR_DEVICE;
-  }
-  if (flag[0]) {
-    ctx->err = "near-field kernel: a bounded wait on its copy pipeline gave up";
     return BEM_ERR_DEVICE;
   }
   return BEM_OK;

@@ -718,289 +718,130 @@ __global__ void __launch_bounds__(128) k_targets(const NearBlockDev* __restrict_
 // straight from the unknown vector x; a CORNER row is its own unknown (phi_i = x_i).
 //
 // HBM-bound: every weight is read once per application (369 MB in FP32 at tank_60k: 5,476
-// blocks of ~12 rows x ~1,570 columns).  Persistent CTAs (one per SM) take the near blocks
-// round robin, warp-specialised so that the weight stream never waits on the latency-bound
-// steps:
-//   warp 8 (producer, one thread)  per chunk of a block's columns (at most kAxXCap), a bulk copy
-//       of the chunk's DOF indices; then the chunk's weights through a ring of kAxStages x
-//       kAxStageBytes of shared memory in pieces of whole rows (row segments when a row is
-//       longer than a stage), up to kAxStages pieces ahead of the consumers;
-//   warps 9-10 (gather)  the chunk's x values through those indices into one of two x buffers,
-//       one chunk ahead of the dot-product warps;
-//   warps 0-7 (dot products)  each piece's column groups (4 FP32 or 2 FP64 columns per 16 bytes)
-//       across the 256 threads, every row of the piece per x value read; each row summed by a
-//       warp reduction into per-(row, warp) slots, added in warp order (fixed order: the result
-//       does not depend on timing); after a block's pieces one warp per target writes its rows
-//       (near sum - diag x, or x on a CORNER row).
-// The far field (L2P of the bucket's local expansion) is added by k_l2p_add afterwards, where
-// many small CTAs hide its serial recurrence.  Weight rows are padded with zeros to 4 columns in
-// both precisions (16-byte aligned pieces).  Every wait is bounded; a timeout records *err, the
-// producer waits (with a fixed limit) for its copies in flight, and the CTA returns.
-constexpr int kAxDot = 256;                // dot-product threads
-constexpr int kAxDotWarps = kAxDot / 32;
-constexpr int kAxGather = 64;              // gather threads
-constexpr int kAxThreads = kAxDot + 32 + kAxGather;
-constexpr int kAxWarps = kAxDotWarps;      // partial-sum slots per row
-constexpr int kAxStages = 4;
-constexpr int kAxStageBytes = 24 * 1024;
-constexpr int kAxXCap = 4096;              // x values per chunk buffer
-constexpr int kAxIdxCap = kAxXCap + 8;     // index window of a chunk (rounded out to 16 bytes)
-constexpr int kAxRowsMax = 8;              // rows per piece (dot-product accumulators)
-constexpr uint32_t kAxWaitTries = 1u << 22;
-constexpr uint32_t kAxDrainTries = 1u << 22;
+// blocks of ~12 rows x ~1,570 columns).  One small CTA per near block, many resident per SM,
+// so that one CTA's gather of x (a dependent load through the block's DOF list) overlaps the
+// weight streams of the others: the block's x values go to shared memory in chunks of kNsXCap
+// columns, then warp tl % kNsWarps streams row tl, every lane kNsUnroll 16-byte loads ahead
+// of its FMAs, and reduces it by a warp shuffle in a fixed order (the result does not depend
+// on timing).  Weight rows are padded with zeros to a multiple of 4 columns in both precisions
+// (16-byte aligned loads); x past the block's last column is 0.  FP32: x in four planes, column
+// c at xs[(c % 4) * q + c / 4] (q = chunk / 4), so lanes reading consecutive column groups hit
+// consecutive words.  The near sum of each target goes to its target slot; the rows (near sum
+// + the far field of the bucket's local expansion - diag x, or x on a CORNER row) are written
+// by k_target_rows afterwards.
+constexpr int kNsThreads = 128;
+constexpr int kNsWarps = kNsThreads / 32;
+constexpr int kNsXCap = 2048;  // x values per chunk (a multiple of 4)
+constexpr int kNsUnroll = 4;   // 16-byte weight loads in flight per lane
 
-// dynamic shared memory of k_targets_ax: the ring, two x buffers, two index windows and the
-// per-(row, warp) partial sums (1 KB of alignment slack)
-inline size_t ax_smem_bytes(const MatvecArgs& a) {
-  return (size_t)kAxStages * kAxStageBytes + 2 * sizeof(double) * kAxXCap + 2 * sizeof(int) * kAxIdxCap +
-         sizeof(double) * (size_t)a.max_ntgt * kAxWarps + 1024;
-}
-
-// The piece schedule of one CTA, walked identically by every role: on_begin(b, B) starts block b;
-// on_chunk(B, c, cc0, cc1) starts chunk c (columns [cc0, cc1) of the padded rows; none for a block
-// without targets or columns); on_piece(B, c, cc0, r0, nr, c0, nc) is one ring stage (rows
-// [r0, r0 + nr), columns [c0, c0 + nc)); on_end(b, B) follows the block's last piece.  A callback
-// returning false ends the walk.
-template <typename WT, typename FBegin, typename FChunk, typename FPiece, typename FEnd>
-__device__ __forceinline__ void ax_walk(const NearBlockDev* __restrict__ blocks, int nblocks, FBegin on_begin, FChunk on_chunk,
-                                        FPiece on_piece, FEnd on_end) {
-  int chunk = 0;
-  for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
-    const NearBlockDev B = blocks[b];
-    if (!on_begin(b, B)) return;
-    const int stride = B.ntgt > 0 ? (B.ndof + 3) & ~3 : 0;
-    const int row_bytes = stride * (int)sizeof(WT);
-    for (int cc0 = 0; cc0 < stride; cc0 += kAxXCap) {
-      const int cc1 = min(stride, cc0 + kAxXCap);
-      if (!on_chunk(B, chunk, cc0, cc1)) return;
-      if (cc0 == 0 && cc1 == stride && row_bytes <= kAxStageBytes) {
-        const int rpp = min(kAxRowsMax, kAxStageBytes / row_bytes);
-        for (int r0 = 0; r0 < B.ntgt; r0 += rpp)
-          if (!on_piece(B, chunk, cc0, r0, min(rpp, B.ntgt - r0), 0, stride)) return;
-      } else {
-        constexpr int cpp = kAxStageBytes / (int)sizeof(WT);  // a multiple of 4 columns
-        for (int r = 0; r < B.ntgt; ++r)
-          for (int c = cc0; c < cc1; c += cpp)
-            if (!on_piece(B, chunk, cc0, r, 1, c, min(cpp, cc1 - c))) return;
-      }
-      ++chunk;
-    }
-    if (!on_end(b, B)) return;
-  }
-}
-
-// the 16-byte aligned window of nb_dofs holding a chunk's real columns [cc0, min(cc1, ndof))
-struct AxIdxWindow {
-  int first;  // first element copied (a multiple of 4)
-  int n;      // elements copied (a multiple of 4)
-  int skip;   // position of column cc0 in the window
-  int ncols;  // real columns of the chunk
-};
-__device__ __forceinline__ AxIdxWindow ax_idx_window(const NearBlockDev& B, int cc0, int cc1) {
-  AxIdxWindow w;
-  const int s = B.dof_off + cc0;
-  w.ncols = max(0, min(cc1, B.ndof) - cc0);
-  w.first = s & ~3;
-  w.n = ((s + w.ncols + 3) & ~3) - w.first;
-  w.skip = s - w.first;
-  return w;
-}
+// dynamic shared memory of k_near_sums: one x chunk and a running sum per target
+inline size_t ns_smem_bytes(int max_ntgt) { return sizeof(double) * (kNsXCap + (size_t)std::max(max_ntgt, 1)); }
 
 template <typename WT>
-__global__ void __launch_bounds__(kAxThreads, 1) k_targets_ax(const NearBlockDev* __restrict__ blocks, int nblocks,
-                                                              const int* __restrict__ nb_dofs, const int* __restrict__ nb_targets,
-                                                              const WT* __restrict__ Wc, const double* __restrict__ x,
-                                                              const int* __restrict__ point_dof_off, const int* __restrict__ point_dof,
-                                                              const int* __restrict__ dof_kind, const double* __restrict__ diag,
-                                                              double* __restrict__ rows, int* __restrict__ err) {
+__global__ void __launch_bounds__(kNsThreads) k_near_sums(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs,
+                                                          const WT* __restrict__ Wc, const double* __restrict__ x,
+                                                          double* __restrict__ near_sum) {
   pdl_enter();
   constexpr int VC = 16 / (int)sizeof(WT);  // columns per 16-byte load
-  extern __shared__ __align__(16) unsigned char ax_raw[];
-  unsigned char* ring = ax_raw + ((1024u - (smem_u32(ax_raw) & 1023u)) & 1023u);
-  double* xs = reinterpret_cast<double*>(ring + kAxStages * kAxStageBytes);  // [2][kAxXCap]
-  int* idxw = reinterpret_cast<int*>(xs + 2 * kAxXCap);                      // [2][kAxIdxCap]
-  double* part = reinterpret_cast<double*>(idxw + 2 * kAxIdxCap);            // [ntgt][kAxWarps]
-  __shared__ uint64_t full[kAxStages], empty[kAxStages], ifull[2], iempty[2], xfull[2], xempty[2];
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (tid == 0) {
-    for (int q = 0; q < kAxStages; ++q) {
-      mbar_init(&full[q], 1);
-      mbar_init(&empty[q], kAxDotWarps);
-    }
-    for (int q = 0; q < 2; ++q) {
-      mbar_init(&ifull[q], 1);
-      mbar_init(&iempty[q], kAxGather / 32);
-      mbar_init(&xfull[q], kAxGather / 32);
-      mbar_init(&xempty[q], kAxDotWarps);
-    }
+  extern __shared__ __align__(16) double ns_smem[];
+  double* xs = ns_smem;          // [kNsXCap]
+  double* run = xs + kNsXCap;    // [ntgt] sums over the previous chunks
+  const NearBlockDev B = blocks[blockIdx.x];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int stride = (B.ndof + 3) & ~3;
+  if (B.ntgt <= 0) return;
+  if (stride == 0) {
+    for (int tl = threadIdx.x; tl < B.ntgt; tl += kNsThreads) near_sum[B.tgt_off + tl] = 0.0;
+    return;
   }
-  __syncthreads();
-  auto yes = [](int, const NearBlockDev&) { return true; };
-  if (warp == kAxDotWarps) {
-    // producer: one thread issues the index windows and the weight pieces
-    if (lane == 0) {
-      int piece = 0;
-      int armed[kAxStages], iarmed[2] = {-1, -1};
+  for (int c0 = 0; c0 < stride; c0 += kNsXCap) {
+    const int cn = min(kNsXCap, stride - c0);  // a multiple of 4
+    const int real = min(cn, B.ndof - c0);
+    const bool last = c0 + cn >= stride;
+    if (c0 > 0) __syncthreads();  // every warp is done with the previous chunk
+    const int* idx = nb_dofs + B.dof_off + c0;
+    if constexpr (VC == 4) {
+      const int q = cn >> 2;
+      for (int i = threadIdx.x; i < cn; i += kNsThreads) xs[(i & 3) * q + (i >> 2)] = i < real ? x[idx[i]] : 0.0;
+    } else {
+      for (int i = threadIdx.x; i < cn; i += kNsThreads) xs[i] = i < real ? x[idx[i]] : 0.0;
+    }
+    __syncthreads();
+    const int ng = cn / VC;  // 16-byte groups of a row in this chunk
+    for (int tl = warp; tl < B.ntgt; tl += kNsWarps) {
+      const WT* wrow = Wc + B.w4_off + (int64_t)tl * stride + c0;
+      double s0 = 0.0, s1 = 0.0;
+      if constexpr (VC == 4) {
+        const float4* w4 = reinterpret_cast<const float4*>(wrow);
+        const int q = ng;
+        int g = lane;
+        for (; g + 32 * (kNsUnroll - 1) < ng; g += 32 * kNsUnroll) {
+          float4 v[kNsUnroll];
 #pragma unroll
-      for (int q = 0; q < kAxStages; ++q) armed[q] = -1;
-      bool ok = true;
-      ax_walk<WT>(
-          blocks, nblocks, yes,
-          [&](const NearBlockDev& B, int c, int cc0, int cc1) {
-            const int ib = c & 1;
-            if (c >= 2) ok = mbar_wait(&iempty[ib], ((c >> 1) - 1) & 1, kAxWaitTries);
-            if (!ok) return false;
-            const AxIdxWindow w = ax_idx_window(B, cc0, cc1);
-            mbar_arrive_expect_tx(&ifull[ib], (uint32_t)(4 * w.n));
-            if (w.n > 0) bulk_copy_g2s(idxw + ib * kAxIdxCap, nb_dofs + w.first, (uint32_t)(4 * w.n), &ifull[ib]);
-            iarmed[ib] = c >> 1;
-            return true;
-          },
-          [&](const NearBlockDev& B, int, int, int r0, int nr, int c0, int nc) {
-            const int st = piece % kAxStages, use = piece / kAxStages;
-            if (use > 0) ok = mbar_wait(&empty[st], (use - 1) & 1, kAxWaitTries);
-            if (!ok) return false;
-            const int stride = (B.ndof + 3) & ~3;
-            const uint32_t bytes = (uint32_t)(nr * nc) * (uint32_t)sizeof(WT);
-            mbar_arrive_expect_tx(&full[st], bytes);
-            bulk_copy_g2s(ring + st * kAxStageBytes, Wc + B.w4_off + (int64_t)r0 * stride + c0, bytes, &full[st]);
-            armed[st] = use;
-            ++piece;
-            return true;
-          },
-          yes);
-      if (!ok) {
-        atomicExch(err, 1);
-        // bulk copies already started land in this CTA's shared memory: wait for them
-        for (int q = 0; q < kAxStages; ++q)
-          if (armed[q] >= 0) mbar_wait(&full[q], armed[q] & 1, kAxDrainTries);
-        for (int q = 0; q < 2; ++q)
-          if (iarmed[q] >= 0) mbar_wait(&ifull[q], iarmed[q] & 1, kAxDrainTries);
+          for (int u = 0; u < kNsUnroll; ++u) v[u] = __ldcs(w4 + g + 32 * u);
+#pragma unroll
+          for (int u = 0; u < kNsUnroll; ++u) {
+            const int gg = g + 32 * u;
+            s0 = fma((double)v[u].x, xs[gg], s0);
+            s1 = fma((double)v[u].y, xs[q + gg], s1);
+            s0 = fma((double)v[u].z, xs[2 * q + gg], s0);
+            s1 = fma((double)v[u].w, xs[3 * q + gg], s1);
+          }
+        }
+        for (; g < ng; g += 32) {
+          const float4 v = __ldcs(w4 + g);
+          s0 = fma((double)v.x, xs[g], s0);
+          s1 = fma((double)v.y, xs[q + g], s1);
+          s0 = fma((double)v.z, xs[2 * q + g], s0);
+          s1 = fma((double)v.w, xs[3 * q + g], s1);
+        }
+      } else {
+        const double2* w2 = reinterpret_cast<const double2*>(wrow);
+        const double2* x2 = reinterpret_cast<const double2*>(xs);
+        int g = lane;
+        for (; g + 32 * (kNsUnroll - 1) < ng; g += 32 * kNsUnroll) {
+          double2 v[kNsUnroll];
+#pragma unroll
+          for (int u = 0; u < kNsUnroll; ++u) v[u] = __ldcs(w2 + g + 32 * u);
+#pragma unroll
+          for (int u = 0; u < kNsUnroll; ++u) {
+            const double2 xv = x2[g + 32 * u];
+            s0 = fma(v[u].x, xv.x, s0);
+            s1 = fma(v[u].y, xv.y, s1);
+          }
+        }
+        for (; g < ng; g += 32) {
+          const double2 v = __ldcs(w2 + g), xv = x2[g];
+          s0 = fma(v.x, xv.x, s0);
+          s1 = fma(v.y, xv.y, s1);
+        }
+      }
+      double s = s0 + s1;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) {
+        // row tl stays on this warp in every chunk: its running sum needs no synchronisation
+        const double tot = (c0 > 0 ? run[tl] : 0.0) + s;
+        if (last)
+          near_sum[B.tgt_off + tl] = tot;
+        else
+          run[tl] = tot;
       }
     }
-    __syncwarp();
-  } else if (warp > kAxDotWarps) {
-    // gather warps: x values of each chunk through its index window, one chunk ahead
-    const int gt = tid - (kAxDot + 32);
-    bool ok = true;
-    ax_walk<WT>(
-        blocks, nblocks, yes,
-        [&](const NearBlockDev& B, int c, int cc0, int cc1) {
-          const int ib = c & 1;
-          ok = mbar_wait(&ifull[ib], (c >> 1) & 1, kAxWaitTries);
-          if (ok && c >= 2) ok = mbar_wait(&xempty[ib], ((c >> 1) - 1) & 1, kAxWaitTries);
-          if (!__all_sync(0xffffffffu, ok ? 1 : 0)) return ok = false;
-          const AxIdxWindow w = ax_idx_window(B, cc0, cc1);
-          const int* iw = idxw + ib * kAxIdxCap + w.skip;
-          double* xb = xs + ib * kAxXCap;
-          for (int i = gt; i < cc1 - cc0; i += kAxGather) xb[i] = i < w.ncols ? x[iw[i]] : 0.0;
-          __syncwarp();
-          if (lane == 0) {
-            mbar_arrive(&iempty[ib]);  // the index window may be overwritten
-            mbar_arrive(&xfull[ib]);   // the x values are in place
-          }
-          return true;
-        },
-        [&](const NearBlockDev&, int, int, int, int, int, int) { return true; }, yes);
-    if (!ok && lane == 0) atomicExch(err, 1);
-  } else {
-    // dot-product warps
-    int piece = 0;
-    bool ok = true;
-    ax_walk<WT>(
-        blocks, nblocks,
-        [&](int, const NearBlockDev& B) {
-          // a new block: its partial sums start at zero
-          named_bar_sync(2, kAxDot);  // the previous block's rows are written
-          for (int i = tid; i < B.ntgt * kAxWarps; i += kAxDot) part[i] = 0.0;
-          named_bar_sync(2, kAxDot);
-          return true;
-        },
-        [&](const NearBlockDev&, int c, int, int) {
-          if (ok) ok = mbar_wait(&xfull[c & 1], (c >> 1) & 1, kAxWaitTries);
-          return true;
-        },
-        [&](const NearBlockDev& B, int c, int cc0, int r0, int nr, int c0, int nc) {
-          const int st = piece % kAxStages, use = piece / kAxStages;
-          ++piece;
-          if (ok) ok = mbar_wait(&full[st], use & 1, kAxWaitTries);
-          if (!ok) return true;  // skip to the block's end, where the dot warps agree to stop
-          const WT* w = reinterpret_cast<const WT*>(ring + st * kAxStageBytes);
-          const double* xc = xs + (c & 1) * kAxXCap + (c0 - cc0);
-          const int ng = nc / VC;
-          double acc[kAxRowsMax];
-#pragma unroll
-          for (int r = 0; r < kAxRowsMax; ++r) acc[r] = 0.0;
-          for (int g = tid; g < ng; g += kAxDot) {
-            const double2 xa = *reinterpret_cast<const double2*>(xc + VC * g);
-            if constexpr (VC == 4) {
-              const double2 xb = *reinterpret_cast<const double2*>(xc + VC * g + 2);
-#pragma unroll
-              for (int r = 0; r < kAxRowsMax; ++r)
-                if (r < nr) {
-                  const float4 q = reinterpret_cast<const float4*>(w + (size_t)r * nc)[g];
-                  acc[r] = fma((double)q.x, xa.x, acc[r]);
-                  acc[r] = fma((double)q.y, xa.y, acc[r]);
-                  acc[r] = fma((double)q.z, xb.x, acc[r]);
-                  acc[r] = fma((double)q.w, xb.y, acc[r]);
-                }
-            } else {
-#pragma unroll
-              for (int r = 0; r < kAxRowsMax; ++r)
-                if (r < nr) {
-                  const double2 q = reinterpret_cast<const double2*>(w + (size_t)r * nc)[g];
-                  acc[r] = fma(q.x, xa.x, acc[r]);
-                  acc[r] = fma(q.y, xa.y, acc[r]);
-                }
-            }
-          }
-#pragma unroll
-          for (int r = 0; r < kAxRowsMax; ++r) {
-            if (r >= nr) break;
-            double v = acc[r];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) part[(r0 + r) * kAxWarps + warp] += v;
-          }
-          __syncwarp();
-          if (lane == 0) {
-            mbar_arrive(&empty[st]);
-            if (c0 + nc >= min((B.ndof + 3) & ~3, cc0 + kAxXCap) && r0 + nr >= B.ntgt)
-              mbar_arrive(&xempty[c & 1]);  // the chunk's last piece: its x buffer is free
-          }
-          return true;
-        },
-        [&](int, const NearBlockDev& B) {
-          // every dot warp learns whether any wait gave up; if so all stop here together
-          if (named_bar_or(2, kAxDot, ok ? 0 : 1)) return ok = false;
-          for (int tl = warp; tl < B.ntgt; tl += kAxDotWarps) {
-            const int p = nb_targets[B.tgt_off + tl];
-            double near = 0.0;
-#pragma unroll
-            for (int q = 0; q < kAxWarps; ++q) near += part[tl * kAxWarps + q];
-            for (int k = point_dof_off[p] + lane; k < point_dof_off[p + 1]; k += 32) {
-              const int i = point_dof[k];
-              const int kd = dof_kind[i];
-              rows[i] = (kd == 2) ? x[i] : near - (kd == 0 ? 0.0 : diag[i] * x[i]);
-            }
-          }
-          return true;
-        });
-    if (!ok && tid == 0) atomicExch(err, 1);
   }
-  __syncthreads();
 }
 
-// Far-field part of A.x rows when the near part ran on its own (k_targets_ax with L = null, on
-// a second stream while the FMM passes run): rows[i] += L2P of the target's bucket at its point
-// for every row that is not a corner row.  One CTA per near block (= target bucket), one warp per
-// target, the L2P recurrence of k_targets_ax.
+// Rows of A.x from the near sums k_near_sums left per target slot: rows[i] = near + far -
+// diag_i x_i (a CORNER row: x_i), far = the L2P of the target bucket's local expansion L[0] at the
+// point (no far field when L is null: the near-field operator alone).  One CTA per near block
+// (= target bucket), one warp per target, lane m owning column m of the solid harmonics.
 template <int P>
-__global__ void __launch_bounds__(128) k_l2p_add(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_targets,
-                                                 const double* __restrict__ Xs, const double* __restrict__ node_X,
-                                                 const double2* __restrict__ L, const int* __restrict__ point_dof_off,
-                                                 const int* __restrict__ point_dof, const int* __restrict__ dof_kind,
-                                                 double* __restrict__ rows) {
+__global__ void __launch_bounds__(128) k_target_rows(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_targets,
+                                                     const double* __restrict__ Xs, const double* __restrict__ node_X,
+                                                     const double2* __restrict__ L, const double* __restrict__ near_sum,
+                                                     const double* __restrict__ x, const int* __restrict__ point_dof_off,
+                                                     const int* __restrict__ point_dof, const int* __restrict__ dof_kind,
+                                                     const double* __restrict__ diag, double* __restrict__ rows) {
   pdl_enter();
   constexpr int NC = ncoef(P);
   __shared__ double2 sL[NC];
@@ -1012,7 +853,8 @@ __global__ void __launch_bounds__(128) k_l2p_add(const NearBlockDev* __restrict_
   }
   const NearBlockDev B = blocks[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
-  for (int i = threadIdx.x; i < NC; i += blockDim.x) sL[i] = L[(size_t)B.node * 2 * NC + i];
+  if (L)
+    for (int i = threadIdx.x; i < NC; i += blockDim.x) sL[i] = L[(size_t)B.node * 2 * NC + i];
   __syncthreads();
   const double cx = node_X[3 * B.node], cy = node_X[3 * B.node + 1], cz = node_X[3 * B.node + 2];
   for (int tl = warp; tl < B.ntgt; tl += nwarp) {
@@ -1020,7 +862,7 @@ __global__ void __launch_bounds__(128) k_l2p_add(const NearBlockDev* __restrict_
     const double px = Xs[3 * p] - cx, py = Xs[3 * p + 1] - cy, pz = Xs[3 * p + 2] - cz;
     double f0 = 0.0;
     const int m = lane;
-    if (m <= P) {
+    if (m <= P && L) {
       const double r2 = px * px + py * py + pz * pz;
       double2 cur = make_double2(1.0, 0.0);
       for (int k = 1; k <= m; ++k) cur = cscale(cmul(cur, make_double2(px, py)), sHalf[k]);
@@ -1039,9 +881,11 @@ __global__ void __launch_bounds__(128) k_l2p_add(const NearBlockDev* __restrict_
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) f0 += __shfl_xor_sync(0xffffffffu, f0, o);
+    const double g = near_sum[B.tgt_off + tl] + f0;
     for (int k = point_dof_off[p] + lane; k < point_dof_off[p + 1]; k += 32) {
       const int i = point_dof[k];
-      if (dof_kind[i] != 2) rows[i] += f0;
+      const int kd = dof_kind[i];
+      rows[i] = (kd == 2) ? x[i] : g - (kd == 0 ? 0.0 : diag[i] * x[i]);
     }
   }
 }
@@ -1050,8 +894,8 @@ __global__ void __launch_bounds__(128) k_l2p_add(const NearBlockDev* __restrict_
 template <typename WT>
 __global__ void k_combine_weights(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs, const int* __restrict__ dof_kind,
                                   const double* __restrict__ WG, const double* __restrict__ WGn, WT* __restrict__ Wc) {
-  // each row padded with zeros to a multiple of 4 columns (16-byte aligned rows for the bulk
-  // copies of k_targets_ax), from the block's own offset w4_off, in both precisions
+  // each row padded with zeros to a multiple of 4 columns (16-byte aligned rows for the vector
+  // loads of k_near_sums), from the block's own offset w4_off, in both precisions
   const NearBlockDev B = blocks[blockIdx.x];
   const int stride = (B.ndof + 3) & ~3;
   const int64_t base = B.w4_off;
@@ -1366,25 +1210,27 @@ __global__ void k_fp64_probe(int iters, double seed, double* __restrict__ sink) 
 
 // ---------------------------------------------------------------------------
 // launchers
-template <int P>
-int launch_near_only_t(const MatvecArgs& a, cudaStream_t st);
+// the near-field SpMV of A.x: per-target near sums (one CTA per near block)
+int launch_near_sums(const MatvecArgs& a, cudaStream_t st) {
+  const size_t shm = ns_smem_bytes(a.max_ntgt);
+  if (a.Wc32)
+    launch_pdl(k_near_sums<float>, a.n_blocks, kNsThreads, shm, st, a.blocks, a.nb_dofs, a.Wc32, a.ax, a.near_sum);
+  else
+    launch_pdl(k_near_sums<double>, a.n_blocks, kNsThreads, shm, st, a.blocks, a.nb_dofs, a.Wc, a.ax, a.near_sum);
+  return 1;
+}
 
-// the near-field SpMV of A.x (one persistent CTA per SM), then, when L is given, the far field
-// added by k_l2p_add
+// the rows of A.x from the near sums, with the far field of L (none when L is null)
+template <int P>
+int launch_target_rows(const MatvecArgs& a, cudaStream_t st, const double2* L) {
+  launch_pdl(k_target_rows<P>, a.n_blocks, 128, 0, st, a.blocks, a.nb_targets, a.Xs, a.node_X, L, a.near_sum, a.ax, a.point_dof_off,
+             a.point_dof, a.dof_kind, a.diag, a.rows);
+  return 1;
+}
+
 template <int P>
 int launch_targets_ax(const MatvecArgs& a, cudaStream_t st, const double2* L) {
-  const size_t shm = ax_smem_bytes(a);
-  const int grid = std::min(a.n_blocks, 148);
-  if (a.Wc32)
-    launch_pdl(k_targets_ax<float>, grid, kAxThreads, shm, st, a.blocks, a.n_blocks, a.nb_dofs, a.nb_targets, a.Wc32, a.ax,
-               a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.near_err);
-  else
-    launch_pdl(k_targets_ax<double>, grid, kAxThreads, shm, st, a.blocks, a.n_blocks, a.nb_dofs, a.nb_targets, a.Wc, a.ax,
-               a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows, a.near_err);
-  if (!L) return 1;
-  launch_pdl(k_l2p_add<P>, a.n_blocks, 128, 0, st, a.blocks, a.nb_targets, a.Xs, a.node_X, L, a.point_dof_off, a.point_dof, a.dof_kind,
-             a.rows);
-  return 2;
+  return launch_near_sums(a, st) + launch_target_rows<P>(a, st, L);
 }
 
 template <int P, int ND>
@@ -1398,7 +1244,7 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
   if (overlap) {
     cudaEventRecord(a.ev_fork, st);
     cudaStreamWaitEvent(a.side, a.ev_fork, 0);
-    launches += launch_near_only_t<P>(a, a.side);
+    launches += launch_near_sums(a, a.side);
     cudaEventRecord(a.ev_join, a.side);
     stages &= ~STAGE_TARGETS;
   }
@@ -1448,8 +1294,7 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
   }
   if (overlap) {
     cudaStreamWaitEvent(st, a.ev_join, 0);
-    k_l2p_add<P><<<a.n_blocks, 128, 0, st>>>(a.blocks, a.nb_targets, a.Xs, a.node_X, a.L, a.point_dof_off, a.point_dof, a.dof_kind, a.rows);
-    ++launches;
+    launches += launch_target_rows<P>(a, st, a.L);
   }
   return launches;
 }
@@ -1471,13 +1316,11 @@ void set_target_smem(int bytes) {
   cudaFuncSetAttribute(k_targets<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-// k_targets_ax's dynamic shared memory (ring, x buffers, index windows, per-target partials):
-// the permission only grows, per device, as for the other targets kernels
+// k_near_sums's dynamic shared memory (an x chunk and a running sum per target): the permission
+// only grows, per device, as for the other targets kernels
 int configure_targets_ax_smem(int max_ntgt) {
-  MatvecArgs a;
-  a.max_ntgt = max_ntgt;
-  const size_t bytes = ax_smem_bytes(a);
-  if (bytes > 220 * 1024) return -1;  // the kernel's static shared memory comes on top
+  const size_t bytes = ns_smem_bytes(max_ntgt);
+  if (bytes > 200 * 1024) return -1;
   static std::mutex mu;
   static int granted[kMaxDevices] = {};
   int dev = -1;
@@ -1486,8 +1329,8 @@ int configure_targets_ax_smem(int max_ntgt) {
   std::lock_guard<std::mutex> lk(mu);
   if (tracked && (int)bytes <= granted[dev]) return 0;
   if (tracked) granted[dev] = (int)bytes;
-  cudaFuncSetAttribute(k_targets_ax<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  cudaFuncSetAttribute(k_targets_ax<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_near_sums<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_near_sums<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   return 0;
 }
 
@@ -1505,7 +1348,7 @@ int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages) {
 }
 
 // y = A_near x: the near-field rows of the A.x operator (combined weights, diagonal and
-// constraint rows as k_targets_ax, no far field); a.ax -> a.rows, FP32 weights when present
+// constraint rows as k_near_sums + k_target_rows, no far field); a.ax -> a.rows, FP32 weights when present
 template <int P>
 int launch_near_only_t(const MatvecArgs& a, cudaStream_t st) {
   if (a.n_blocks <= 0 || !a.ax || !(a.Wc || a.Wc32)) return 0;

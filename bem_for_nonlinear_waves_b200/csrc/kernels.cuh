@@ -122,7 +122,7 @@ struct MatvecArgs {
   const void* tc_rows_map = nullptr; // host copy of the TMA tensor map over tc_Mt
   // targets
   int n_blocks = 0, chunk = 0, max_ntgt = 0;
-  int* near_err = nullptr;  // set when a bounded wait of k_targets_ax gave up
+  double* near_sum = nullptr;  // [targets] near sums of A.x by target slot (blocks' tgt_off order)
   const NearBlockDev* blocks = nullptr;
   const int* nb_dofs = nullptr;
   const int* nb_targets = nullptr;
@@ -186,11 +186,12 @@ enum { STAGE_P2M = 1, STAGE_M2M = 2, STAGE_M2L = 4, STAGE_L2L = 8, STAGE_TARGETS
 // phin = 0 (the rigid-mode diagonal).
 int launch_matvec(int p, const MatvecArgs& a, cudaStream_t st, int stages = STAGE_ALL);
 int launch_near_only(int p, const MatvecArgs& a, cudaStream_t st);  // a.rows = A_near a.ax (no far field)
+int launch_near_sums(const MatvecArgs& a, cudaStream_t st);          // a.near_sum = per-target near sums of a.ax
 
 // tensor-core M2L (m2l_tc.cu)
 int tc_supported(int p);            // 1 for 1 <= p <= 12
 uint32_t tc_default_wait_tries();   // iteration limit of the contraction's pipeline waits
-// k_targets_ax: sets its dynamic shared-memory permission for the largest near block of a problem
+// k_near_sums: sets its dynamic shared-memory permission for the largest near block of a problem
 // (max_ntgt targets) on the current device; -1 when that does not fit an SM
 int configure_targets_ax_smem(int max_ntgt);
 int tc_kp(int p);                   // real coefficients per row, padded to 64

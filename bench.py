@@ -54,7 +54,9 @@ TOL_LADDER = (1e-9, 1e-10, 1e-11, 1e-12)
 # preconditioner NONE) on each workload, by relative tolerance: the same Krylov iteration on the
 # same operator, counted by the FP64 GPU path with `bench.py --count-reference-iterations`.
 # They turn the CPU baseline's measured set-up and mat-vec into a (modeled) solve time.
-REFERENCE_ITERATIONS = {"tank_60k": {1e-8: 1324}, "tank_2800": {1e-10: 384}}
+# tank_60k at 1e-11: 713 iterations (`bench.py --count-reference-iterations --tol 1e-11`, B200);
+# tank_2800 at 1e-10: 384.
+REFERENCE_ITERATIONS = {"tank_60k": {1e-11: 713}, "tank_2800": {1e-10: 384}}
 
 
 def reference_iterations(config, tol):
@@ -794,18 +796,23 @@ def main():
 
 
 def near_roofline(bvp, tree, prof, peaks, peaks_kind, mixed, workload):
-    """The near-field SpMV + L2P kernel of A.x against HBM: algorithmic bytes = the stored weight
-    blocks (FP32 in the mixed operator, FP64 otherwise) + the gathered unknowns + the rows
-    written, over the targets stage's CUDA-event time."""
+    """The near-field SpMV of A.x against HBM.  Mixed operator: k_near_sums<float> timed alone,
+    algorithmic bytes = the stored FP32 weight blocks + the gathered unknowns and their DOF
+    indices + the per-target sums written.  FP64 operator: the whole targets stage (near sums,
+    then the L2P and rows), with the rows written on top."""
     nb = bvp.near_bytes()
-    wbytes = nb["weights_fp32"] if mixed else nb["weights_fp64"]
-    alg = wbytes + nb["x_gather"] + nb["rows"]
-    t_k = prof["targets"] * 1e-3
-    achieved = alg / t_k / 1e9
-    return {"kernel": "k_targets_ax<float>" if mixed else "k_targets_ax<double>", "bound": "hbm", "achieved": achieved,
+    if mixed:
+        alg = nb["weights_fp32"] + nb["x_gather"] + nb["dof_index"] + nb["near_sums"]
+        ms, name = prof["near_sums"], "k_near_sums<float>"
+    else:
+        alg = nb["weights_fp64"] + nb["x_gather"] + nb["dof_index"] + nb["near_sums"] + nb["rows"]
+        ms, name = prof["targets"], "k_near_sums<double> + k_target_rows"
+    achieved = alg / (ms * 1e-3) / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": achieved,
             "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-            "traffic": load_traffic("k_targets_ax", workload), "algorithmic_bytes_per_launch": alg,
-            "peak_source": f"{peaks_kind} HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)", "kernel_ms": prof["targets"]}
+            "traffic": load_traffic("k_near_sums", workload), "algorithmic_bytes_per_launch": alg,
+            "peak_source": f"{peaks_kind} HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)", "kernel_ms": ms,
+            "targets_stage_ms": prof["targets"]}
 
 
 def measure_extras(args, cfg, t, d, kv, bvp, tol, local):

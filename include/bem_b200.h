@@ -321,11 +321,12 @@ int bem_gpu_mel_stage(bem_gpu_mel* mel, const bem_mel_surface* s, int32_t stage,
  * bem_gpu_matvec_device_mixed: y = A_lo x on device buffers (tensor-core M2L, everything
  *   else FP64), on the context's stream — the correction operator of the mixed solve.
  * bem_gpu_profile_matvec_mixed: stage times of that operator, the layout above followed by
- *   the three kernels of its M2L alone: [6] expand, [7] tensor-core contraction, [8] reduce.
+ *   the three kernels of its M2L alone: [6] expand, [7] tensor-core contraction, [8] reduce,
+ *   and [9] the near-field sums alone (the FP32 near-weight stream of stage [4], no rows).
  * bem_gpu_check_device_status: BEM_ERR_DEVICE if a bounded device-side wait of the
  *   tensor-core M2L gave up since set-up (the results of that launch are invalid). */
 int bem_gpu_matvec_device_mixed(bem_gpu_ctx* ctx, const double* d_x, double* d_y);
-int bem_gpu_profile_matvec_mixed(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[9]*/);
+int bem_gpu_profile_matvec_mixed(bem_gpu_ctx* ctx, int repeats, double* stage_ms /*[10]*/);
 int bem_gpu_check_device_status(bem_gpu_ctx* ctx);
 /* Iteration limit of the tensor-core M2L's device-side pipeline waits (a kernel argument;
  * default 2^22 tries, a fraction of a second).  For testing failure detection: with a small
