@@ -833,56 +833,59 @@ __global__ void __launch_bounds__(kNsThreads) k_near_sums(const NearBlockDev* __
 
 // Rows of A.x from the near sums k_near_sums left per target slot: rows[i] = near + far -
 // diag_i x_i (a CORNER row: x_i), far = the L2P of the target bucket's local expansion L[0] at the
-// point (no far field when L is null: the near-field operator alone).  One CTA per near block
-// (= target bucket), one warp per target, lane m owning column m of the solid harmonics.
+// point (no far field when L is null: the near-field operator alone).  One warp-sized CTA per
+// near block (= target bucket), one thread per target: the L2P sums the bucket's expansion
+// against the regular solid harmonics of the point, column m by column from
+// R_m^m = (x + iy)^m / (2^m m!) with (n - m)(n + m) R_n^m = (2n - 1) z R_{n-1}^m - r^2 R_{n-2}^m,
+// fully unrolled so that the recurrence constants fold at compile time; the expansion is read
+// from shared memory at the same address by every thread (a broadcast).
 template <int P>
-__global__ void __launch_bounds__(128) k_target_rows(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_targets,
-                                                     const double* __restrict__ Xs, const double* __restrict__ node_X,
-                                                     const double2* __restrict__ L, const double* __restrict__ near_sum,
-                                                     const double* __restrict__ x, const int* __restrict__ point_dof_off,
-                                                     const int* __restrict__ point_dof, const int* __restrict__ dof_kind,
-                                                     const double* __restrict__ diag, double* __restrict__ rows) {
+__global__ void __launch_bounds__(32) k_target_rows(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_targets,
+                                                    const double* __restrict__ Xs, const double* __restrict__ node_X,
+                                                    const double2* __restrict__ L, const double* __restrict__ near_sum,
+                                                    const double* __restrict__ x, const int* __restrict__ point_dof_off,
+                                                    const int* __restrict__ point_dof, const int* __restrict__ dof_kind,
+                                                    const double* __restrict__ diag, double* __restrict__ rows) {
   pdl_enter();
   constexpr int NC = ncoef(P);
   __shared__ double2 sL[NC];
-  __shared__ double sHalf[P + 1], sRec[(P + 1) * (P + 1)];
-  for (int i = threadIdx.x; i < (P + 1) * (P + 1); i += blockDim.x) {
-    const int n = i / (P + 1), m = i - n * (P + 1);
-    sRec[i] = n > m ? 1.0 / double(n * n - m * m) : 0.0;
-    if (i <= P) sHalf[i] = i > 0 ? 1.0 / (2.0 * i) : 0.0;
-  }
   const NearBlockDev B = blocks[blockIdx.x];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  const int lane = threadIdx.x;
   if (L)
-    for (int i = threadIdx.x; i < NC; i += blockDim.x) sL[i] = L[(size_t)B.node * 2 * NC + i];
-  __syncthreads();
+    for (int i = lane; i < NC; i += 32) sL[i] = L[(size_t)B.node * 2 * NC + i];
+  __syncwarp();
   const double cx = node_X[3 * B.node], cy = node_X[3 * B.node + 1], cz = node_X[3 * B.node + 2];
-  for (int tl = warp; tl < B.ntgt; tl += nwarp) {
+  for (int tl = lane; tl < B.ntgt; tl += 32) {
     const int p = nb_targets[B.tgt_off + tl];
-    const double px = Xs[3 * p] - cx, py = Xs[3 * p + 1] - cy, pz = Xs[3 * p + 2] - cz;
-    double f0 = 0.0;
-    const int m = lane;
-    if (m <= P && L) {
+    double far = 0.0;
+    if (L) {
+      const double px = Xs[3 * p] - cx, py = Xs[3 * p + 1] - cy, pz = Xs[3 * p + 2] - cz;
       const double r2 = px * px + py * py + pz * pz;
-      double2 cur = make_double2(1.0, 0.0);
-      for (int k = 1; k <= m; ++k) cur = cscale(cmul(cur, make_double2(px, py)), sHalf[k]);
-      double2 prev = make_double2(0.0, 0.0);
-      const double w = (m == 0) ? 1.0 : 2.0;
-      for (int n = m; n <= P; ++n) {
-        if (n > m) {
-          const double inv = sRec[n * (P + 1) + m];
-          double2 nx = make_double2(((2 * n - 1) * pz * cur.x - r2 * prev.x) * inv, ((2 * n - 1) * pz * cur.y - r2 * prev.y) * inv);
-          prev = cur;
-          cur = nx;
+      double2 rmm = make_double2(1.0, 0.0);  // R_m^m
+#pragma unroll
+      for (int m = 0; m <= P; ++m) {
+        if (m > 0) rmm = cscale(cmul(rmm, make_double2(px, py)), 1.0 / (2.0 * m));
+        double2 prev = make_double2(0.0, 0.0), cur = rmm;
+        double fm = 0.0;
+#pragma unroll
+        for (int n = m; n <= P; ++n) {
+          if (n > m) {
+            const double inv = 1.0 / double(n * n - m * m);
+            const double2 nx = make_double2(((2 * n - 1) * pz * cur.x - r2 * prev.x) * inv, ((2 * n - 1) * pz * cur.y - r2 * prev.y) * inv);
+            prev = cur;
+            cur = nx;
+          }
+          const double2 l0 = sL[cidx(n, m)];
+          fm += l0.x * cur.x + l0.y * cur.y;
         }
-        const double2 l0 = sL[cidx(n, m)];
-        f0 += w * (l0.x * cur.x + l0.y * cur.y);
+        far += (m == 0 ? 1.0 : 2.0) * fm;
+        // keep the next column's expansion loads below this column (bounded register use)
+        asm volatile("" ::: "memory");
       }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) f0 += __shfl_xor_sync(0xffffffffu, f0, o);
-    const double g = near_sum[B.tgt_off + tl] + f0;
-    for (int k = point_dof_off[p] + lane; k < point_dof_off[p + 1]; k += 32) {
+    const double g = near_sum[B.tgt_off + tl] + far;
+    const int k1 = point_dof_off[p + 1];
+    for (int k = point_dof_off[p]; k < k1; ++k) {
       const int i = point_dof[k];
       const int kd = dof_kind[i];
       rows[i] = (kd == 2) ? x[i] : g - (kd == 0 ? 0.0 : diag[i] * x[i]);
@@ -1223,7 +1226,7 @@ int launch_near_sums(const MatvecArgs& a, cudaStream_t st) {
 // the rows of A.x from the near sums, with the far field of L (none when L is null)
 template <int P>
 int launch_target_rows(const MatvecArgs& a, cudaStream_t st, const double2* L) {
-  launch_pdl(k_target_rows<P>, a.n_blocks, 128, 0, st, a.blocks, a.nb_targets, a.Xs, a.node_X, L, a.near_sum, a.ax, a.point_dof_off,
+  launch_pdl(k_target_rows<P>, a.n_blocks, 32, 0, st, a.blocks, a.nb_targets, a.Xs, a.node_X, L, a.near_sum, a.ax, a.point_dof_off,
              a.point_dof, a.dof_kind, a.diag, a.rows);
   return 1;
 }
