@@ -856,20 +856,44 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     ce[i] = P.nodes[i].child_end;
   }
   // parents per level (non-empty nodes with children)
-  std::vector<int> lp;
-  ctx->level_parent_off.assign(1, 0);
+  std::vector<int> lp, lp_all, lp_all_off(1, 0);
   for (int l = 0; l < (int)P.level_nodes.size(); ++l) {
     for (int i : P.level_nodes[l])
-      if (P.nodes[i].child_end > P.nodes[i].child_begin) lp.push_back(i);
+      if (P.nodes[i].child_end > P.nodes[i].child_begin) lp_all.push_back(i);
+    lp_all_off.push_back((int)lp_all.size());
+  }
+  // Passes that cannot change a result are left out (exactly: the values they skip are zero or
+  // never read).  node_up[i]: the parent, or -1 at the root.  M of a node is needed when the
+  // node is an M2L source or its parent's M is needed (M2M builds a parent from its children);
+  // the local expansion of a node is non-zero only when the node or an ancestor is an M2L
+  // target, so the downward pass starts below the levels without targets.
+  std::vector<int> node_up(nb, -1);
+  std::vector<char> m_needed(nb, 0), l_nonzero(nb, 0);
+  for (int i = 0; i < nb; ++i)
+    for (int ci = P.nodes[i].child_begin; ci < P.nodes[i].child_end; ++ci) node_up[P.node_children[ci]] = i;
+  {
+    std::vector<char> is_src(nb, 0);
+    for (int32_t s2 : P.m2l_src) is_src[s2] = 1;
+    for (int l = 0; l < (int)P.level_nodes.size(); ++l)
+      for (int i : P.level_nodes[l]) {
+        const int up = node_up[i];
+        m_needed[i] = is_src[i] || (up >= 0 && m_needed[up]);
+        l_nonzero[i] = (P.m2l_off[i + 1] > P.m2l_off[i]) || (up >= 0 && l_nonzero[up]);
+      }
+  }
+  ctx->level_parent_off.assign(1, 0);
+  for (int l = 0; l + 1 < (int)lp_all_off.size(); ++l) {
+    for (int q = lp_all_off[l]; q < lp_all_off[l + 1]; ++q)
+      if (l_nonzero[lp_all[q]]) lp.push_back(lp_all[q]);
     ctx->level_parent_off.push_back((int)lp.size());
   }
   {  // parent-to-child F tables per (level, octant), from the first pair met of each
-    const int nlev = (int)ctx->level_parent_off.size() - 1;
+    const int nlev = (int)lp_all_off.size() - 1;
     std::vector<double> fv((size_t)std::max(nlev, 1) * 8 * 3, 0.0);
     std::vector<char> seen((size_t)std::max(nlev, 1) * 8, 0);
     for (int l = 0; l < nlev; ++l)
-      for (int q = ctx->level_parent_off[l]; q < ctx->level_parent_off[l + 1]; ++q) {
-        const int par = lp[q];
+      for (int q = lp_all_off[l]; q < lp_all_off[l + 1]; ++q) {
+        const int par = lp_all[q];
         for (int ci = P.nodes[par].child_begin; ci < P.nodes[par].child_end; ++ci) {
           const int c = P.node_children[ci];
           double d[3];
@@ -947,15 +971,15 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     for (int l : P.leaves) leaf[l] = 1;
     for (int l = 0; l < (int)P.level_nodes.size(); ++l)
       for (int i : P.level_nodes[l]) lev[i] = l;
-    for (int i = 0; i < nb; ++i)
-      for (int ci = P.nodes[i].child_begin; ci < P.nodes[i].child_end; ++ci) par[P.node_children[ci]] = i;
-    // a node has a multipole if it is a leaf (from the P2M) or one of its children has one;
-    // a parent waits for its children with multipoles that are not leaves (nsig), and the
-    // parents that wait for none start the pass; deepest levels first
+    // the pass climbs only into parents whose multipole is needed
+    for (int i = 0; i < nb; ++i) par[i] = (node_up[i] >= 0 && m_needed[node_up[i]]) ? node_up[i] : -1;
+    // a node has a multipole if it is a leaf (from the P2M) or it is needed and one of its
+    // children has one; a parent waits for its children with multipoles that are not leaves
+    // (nsig), and the parents that wait for none start the pass; deepest levels first
     std::vector<int> nch(nb, 0), ready;
     for (int l = (int)P.level_nodes.size() - 1; l >= 0; --l)
       for (int i : P.level_nodes[l]) {
-        sig[i] = leaf[i] || nch[i] > 0;
+        sig[i] = leaf[i] || (m_needed[i] && nch[i] > 0);
         if (sig[i] && par[i] >= 0) {
           ++nch[par[i]];
           if (!leaf[i]) ++nsig[par[i]];
@@ -963,7 +987,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
       }
     for (int l = (int)P.level_nodes.size() - 1; l >= 0; --l)
       for (int i : P.level_nodes[l])
-        if (!leaf[i] && nch[i] > 0 && nsig[i] == 0) ready.push_back(i);
+        if (!leaf[i] && m_needed[i] && nch[i] > 0 && nsig[i] == 0) ready.push_back(i);
     ctx->n_m2m_ready = (int)ready.size();
     if (ready.empty()) ready.push_back(0);
     CK(ups(ctx->m2m_ready, ready));

@@ -684,8 +684,13 @@ def main():
     fp64_peak = _lib.load().bem_gpu_fp64_peak_tflops(local)
 
     barrier(world)
+    import torch
+    # the timed steps are the profiled range of a profiler run with --profile-from-start off
+    # (no effect otherwise)
+    torch.cuda.profiler.start()
     with ClockSampler(local) as clk:
         r = time_solves(bvp, kv, args.steps)
+    torch.cuda.profiler.stop()
     barrier(world)
     dev_max, e2e_max = allreduce_max([r["dev_s"], r["e2e_s"]], world)
     ans = bvp.ans.copy()
