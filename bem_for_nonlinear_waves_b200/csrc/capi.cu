@@ -144,9 +144,14 @@ struct bem_gpu_ctx {
   DBuf<int> leaf_dof_off{&dev_bytes}, leaf_dof{&dev_bytes}, e_slot{&dev_bytes}, slot_block{&dev_bytes};  // P2M operator of A.x: DOFs per leaf
   DBuf<double2> p2m_C{&dev_bytes};                       // [(leaf, DOF)][NC]
   DBuf<double2> near_scratch{&dev_bytes};                // element values of the near-weight kernel
-  DBuf<int> e_dof{&dev_bytes}, e_vtx{&dev_bytes}, node_fb{&dev_bytes}, node_fe{&dev_bytes}, leaves{&dev_bytes}, level_parents{&dev_bytes}, child_begin{&dev_bytes}, child_end{&dev_bytes}, node_children{&dev_bytes};
-  DBuf<int> node_parent{&dev_bytes}, node_level{&dev_bytes}, m2m_nsig{&dev_bytes}, m2m_cnt{&dev_bytes}, m2m_ready{&dev_bytes};
-  int n_m2m_ready = 0;
+  DBuf<int> e_dof{&dev_bytes}, e_vtx{&dev_bytes}, node_fb{&dev_bytes}, node_fe{&dev_bytes}, leaves{&dev_bytes}, child_begin{&dev_bytes}, child_end{&dev_bytes}, node_children{&dev_bytes};
+  // tree passes, one launch per level: upward-pass nodes and the parent each hands its multipole
+  // to, the multipoles shifted to the parent, downward-pass (parent, child) pairs
+  DBuf<int> m2m_nodes{&dev_bytes}, node_up{&dev_bytes};
+  DBuf<double2> Yup{&dev_bytes};
+  DBuf<int2> l2l_pairs{&dev_bytes};
+  std::vector<int> m2m_level_off, l2l_level_off;
+  int n_tree_levels = 0;
   DBuf<int> m2l_targets{&dev_bytes}, m2l_off{&dev_bytes}, m2l_src{&dev_bytes}, nb_dofs{&dev_bytes}, nb_targets{&dev_bytes}, nb_ranges{&dev_bytes}, dof_inc_off{&dev_bytes}, dof_inc{&dev_bytes};
   DBuf<int> block_of_point{&dev_bytes}, row_of_point{&dev_bytes}, self_col{&dev_bytes};  // right-Jacobi inputs
   DBuf<int> point_dof_off{&dev_bytes}, point_dof{&dev_bytes}, dof_kind{&dev_bytes}, dof_point{&dev_bytes};
@@ -156,7 +161,6 @@ struct bem_gpu_ctx {
   DBuf<double2> Sg{&dev_bytes}, Y{&dev_bytes}, Ftab{&dev_bytes};
   DBuf<double> ftab_vec{&dev_bytes};
   DBuf<double2> M{&dev_bytes}, L{&dev_bytes};
-  std::vector<int> level_parent_off;
   int n_m2l_targets = 0, max_ntgt = 0, chunk = 0;
   int64_t w4_total = 0;  // size of the row-padded FP32 near weights
   int n_tc_items = 0;    // tensor-core work items (every table-row-tile image's pair chunks)
@@ -235,7 +239,7 @@ struct bem_gpu_ctx {
   MatvecArgs args(const double* d_phi, const double* d_phin, double* d_rows, double* d_gphin, double* d_gnphi) const {
     MatvecArgs a;
     a.n_nodes = (int)plan.nodes.size();
-    a.n_levels = (int)level_parent_off.size() - 1;
+    a.n_levels = n_tree_levels;
     a.n_leaves = (int)plan.leaves.size();
     a.leaves = leaves.p;
     a.node_fb = node_fb.p;
@@ -245,18 +249,16 @@ struct bem_gpu_ctx {
     a.e_W = e_W.p;
     a.e_n = e_n.p;
     a.e_dof = e_dof.p;
-    a.level_parent_off = level_parent_off.data();
-    a.level_parents = level_parents.p;
     a.child_begin = child_begin.p;
     a.child_end = child_end.p;
     a.node_children = node_children.p;
     a.Ftab = Ftab.p;
-    a.node_parent = node_parent.p;
-    a.node_level = node_level.p;
-    a.m2m_nsig = m2m_nsig.p;
-    a.m2m_cnt = m2m_cnt.p;
-    a.n_m2m_ready = n_m2m_ready;
-    a.m2m_ready = m2m_ready.p;
+    a.m2m_level_off = m2m_level_off.empty() ? nullptr : m2m_level_off.data();
+    a.m2m_nodes = m2m_nodes.p;
+    a.node_up = node_up.p;
+    a.Yup = Yup.p;
+    a.l2l_level_off = l2l_level_off.empty() ? nullptr : l2l_level_off.data();
+    a.l2l_pairs = l2l_pairs.p;
 
     a.n_m2l_targets = n_m2l_targets;
     a.m2l_targets = m2l_targets.p;
@@ -856,7 +858,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     ce[i] = P.nodes[i].child_end;
   }
   // parents per level (non-empty nodes with children)
-  std::vector<int> lp, lp_all, lp_all_off(1, 0);
+  std::vector<int> lp_all, lp_all_off(1, 0);
   for (int l = 0; l < (int)P.level_nodes.size(); ++l) {
     for (int i : P.level_nodes[l])
       if (P.nodes[i].child_end > P.nodes[i].child_begin) lp_all.push_back(i);
@@ -881,11 +883,33 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
         l_nonzero[i] = (P.m2l_off[i + 1] > P.m2l_off[i]) || (up >= 0 && l_nonzero[up]);
       }
   }
-  ctx->level_parent_off.assign(1, 0);
-  for (int l = 0; l + 1 < (int)lp_all_off.size(); ++l) {
-    for (int q = lp_all_off[l]; q < lp_all_off[l + 1]; ++q)
-      if (l_nonzero[lp_all[q]]) lp.push_back(lp_all[q]);
-    ctx->level_parent_off.push_back((int)lp.size());
+  {  // per-level lists of the tree passes
+    const int nlev = (int)P.level_nodes.size();
+    ctx->n_tree_levels = nlev;
+    std::vector<int> up_needed(nb, -1), mnodes;
+    for (int i = 0; i < nb; ++i) up_needed[i] = (node_up[i] >= 0 && m_needed[node_up[i]]) ? node_up[i] : -1;
+    // upward: nodes that build a needed multipole from their children or hand theirs up
+    ctx->m2m_level_off.assign(1, 0);
+    for (int l = 0; l < nlev; ++l) {
+      for (int i : P.level_nodes[l])
+        if ((P.nodes[i].child_end > P.nodes[i].child_begin && m_needed[i]) || up_needed[i] >= 0) mnodes.push_back(i);
+      ctx->m2m_level_off.push_back((int)mnodes.size());
+    }
+    // downward: (parent, child) pairs of the parents with a non-zero local expansion
+    std::vector<int2> pairs;
+    ctx->l2l_level_off.assign(1, 0);
+    for (int l = 0; l < nlev; ++l) {
+      for (int i : P.level_nodes[l])
+        if (l_nonzero[i])
+          for (int ci = P.nodes[i].child_begin; ci < P.nodes[i].child_end; ++ci) pairs.push_back(make_int2(i, P.node_children[ci]));
+      ctx->l2l_level_off.push_back((int)pairs.size());
+    }
+    if (mnodes.empty()) mnodes.push_back(0);  // keep the device arrays non-empty
+    if (pairs.empty()) pairs.push_back(make_int2(0, 0));
+    CK(ups(ctx->m2m_nodes, mnodes));
+    CK(ups(ctx->node_up, up_needed));
+    CK(ups(ctx->l2l_pairs, pairs));
+    CK(ctx->Yup.alloc((size_t)std::max(nb, 1) * 2 * ncoef(P.opt.p)));
   }
   {  // parent-to-child F tables per (level, octant), from the first pair met of each
     const int nlev = (int)lp_all_off.size() - 1;
@@ -965,38 +989,6 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   CK(ups(ctx->child_end, ce));
   CK(ups(ctx->node_children, P.node_children));
   CK(ups(ctx->leaves, P.leaves));
-  {  // upward pass: parent, Ftab row and the number of children whose multipole completes
-    std::vector<int> par(nb, -1), lev(nb, 0), nsig(nb, 0);
-    std::vector<char> sig(nb, 0), leaf(nb, 0);
-    for (int l : P.leaves) leaf[l] = 1;
-    for (int l = 0; l < (int)P.level_nodes.size(); ++l)
-      for (int i : P.level_nodes[l]) lev[i] = l;
-    // the pass climbs only into parents whose multipole is needed
-    for (int i = 0; i < nb; ++i) par[i] = (node_up[i] >= 0 && m_needed[node_up[i]]) ? node_up[i] : -1;
-    // a node has a multipole if it is a leaf (from the P2M) or it is needed and one of its
-    // children has one; a parent waits for its children with multipoles that are not leaves
-    // (nsig), and the parents that wait for none start the pass; deepest levels first
-    std::vector<int> nch(nb, 0), ready;
-    for (int l = (int)P.level_nodes.size() - 1; l >= 0; --l)
-      for (int i : P.level_nodes[l]) {
-        sig[i] = leaf[i] || (m_needed[i] && nch[i] > 0);
-        if (sig[i] && par[i] >= 0) {
-          ++nch[par[i]];
-          if (!leaf[i]) ++nsig[par[i]];
-        }
-      }
-    for (int l = (int)P.level_nodes.size() - 1; l >= 0; --l)
-      for (int i : P.level_nodes[l])
-        if (!leaf[i] && m_needed[i] && nch[i] > 0 && nsig[i] == 0) ready.push_back(i);
-    ctx->n_m2m_ready = (int)ready.size();
-    if (ready.empty()) ready.push_back(0);
-    CK(ups(ctx->m2m_ready, ready));
-    CK(ups(ctx->node_parent, par));
-    CK(ups(ctx->node_level, lev));
-    CK(ups(ctx->m2m_nsig, nsig));
-    CK(ctx->m2m_cnt.alloc(std::max(nb, 1)));
-  }
-  CK(ups(ctx->level_parents, lp));
   CK(ups(ctx->m2l_targets, mt));
   CK(ups(ctx->m2l_off, P.m2l_off));
   CK(ups(ctx->m2l_src, P.m2l_src));
@@ -1182,7 +1174,6 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   CK(cudaMemsetAsync(ctx->GPhin.p, 0, sizeof(double) * P.np, s));
   CK(cudaMemsetAsync(ctx->GnPhi.p, 0, sizeof(double) * P.np, s));
   CK(cudaMemsetAsync(ctx->M.p, 0, sizeof(double2) * ctx->M.n, s));
-  CK(cudaMemsetAsync(ctx->m2m_cnt.p, 0, sizeof(int) * ctx->m2m_cnt.n, s));
   CK(cudaMemsetAsync(ctx->p2m_C.p, 0, sizeof(double2) * ctx->p2m_C.n, s));
   if (!reuse) {  // translation tables depend on the bucket geometry alone
     launch_s_tables(P.opt.p, (int)P.grp_off.size() - 1, ctx->grp_vec.p, ctx->Sg.p, s);

@@ -3,10 +3,10 @@
 // Per mat-vec (return_A_dot_v, bem/BEM_solveBVP_GMRES_FMM.hpp:2124-2155):
 //   k_densities   per-DOF phi/phin from the unknown vector (setUnknowns/setKnowns, :1142-1176)
 //   k_p2m         leaf multipoles from the 6 Dunavant points of every element (moments.hpp:307-368)
-//   k_m2m_up      the whole upward pass in one launch, parents completed by arrival counts
-//                 (moments.hpp:419-436, 912-915)
+//   k_m2m_level   one launch per level from the deepest: multipoles summed from the children's
+//                 shifted ones, then shifted to the parent (moments.hpp:419-436, 912-915)
 //   k_m2l         every M2L pair of every level in one launch (moments.hpp:732-764)
-//   k_l2l         one launch per level, top-down (moments.hpp:869-884, 925-929)
+//   k_l2l_pairs   one launch per level, top-down, a CTA per (parent, child) (moments.hpp:869-884, 925-929)
 //   k_targets     near-field block SpMV + L2P + BIE rows (compute_Ax_minus_b, :34-158)
 // Set-up:
 //   k_near_weights  near-field quadrature into per-block dense rows (target4FMM::setDirectIntegration,
@@ -281,99 +281,6 @@ __device__ __forceinline__ int child_octant(const double* __restrict__ node_X, i
          (node_X[3 * c + 2] > node_X[3 * par + 2] ? 4 : 0);
 }
 
-// Tree translations with a thread per output coefficient.  A translation of order P has
-// (P+1)(P+2)/2 output coefficients of up to ~(P+1)^2/2 terms each; a block runs kTreeGroups
-// translations side by side, each by a group of coefficient threads, and every thread sums
-// its terms in two interleaved chains so that consecutive multiply-adds do not wait on one
-// another.
-constexpr int kTreeGroups = 4;
-template <int P>
-constexpr int tree_group_threads() { return (ncoef(P) + 31) / 32 * 32; }
-
-// one output coefficient (n, m) of an M2M shift: sum conj(F_{n1}^{m1}) M_{n-n1}^{m-m1}
-template <int P, int ND>
-__device__ __forceinline__ void m2m_coef(int n, int m, const double2* __restrict__ sF, const double2* __restrict__ sM, double2& o0,
-                                         double2& o1) {
-  constexpr int NF = (P + 1) * (P + 1);
-  double2 a0 = make_double2(0.0, 0.0), a1 = a0, b0 = a0, b1 = a0;
-  for (int n1 = 0; n1 <= n; ++n1) {
-    const int n2 = n - n1;
-    const int lo = max(-n1, m - n2), hi = min(n1, m + n2);
-    const double2* f = sF + n1 * (n1 + 1);
-    const double2* x = sM + n2 * (n2 + 1) + m;
-    int m1 = lo;
-    for (; m1 < hi; m1 += 2) {
-      const double2 f0 = f[m1], f1 = f[m1 + 1];
-      const double2 x0 = x[-m1], y0 = x[-m1 - 1];
-      a0.x += f0.x * x0.x + f0.y * x0.y;
-      a0.y += f0.x * x0.y - f0.y * x0.x;
-      b0.x += f1.x * y0.x + f1.y * y0.y;
-      b0.y += f1.x * y0.y - f1.y * y0.x;
-      if (ND == 2) {
-        const double2 x1 = x[NF - m1], y1 = x[NF - m1 - 1];
-        a1.x += f0.x * x1.x + f0.y * x1.y;
-        a1.y += f0.x * x1.y - f0.y * x1.x;
-        b1.x += f1.x * y1.x + f1.y * y1.y;
-        b1.y += f1.x * y1.y - f1.y * y1.x;
-      }
-    }
-    if (m1 == hi) {
-      const double2 f0 = f[m1], x0 = x[-m1];
-      a0.x += f0.x * x0.x + f0.y * x0.y;
-      a0.y += f0.x * x0.y - f0.y * x0.x;
-      if (ND == 2) {
-        const double2 x1 = x[NF - m1];
-        a1.x += f0.x * x1.x + f0.y * x1.y;
-        a1.y += f0.x * x1.y - f0.y * x1.x;
-      }
-    }
-  }
-  o0 = cadd(o0, cadd(a0, b0));
-  if (ND == 2) o1 = cadd(o1, cadd(a1, b1));
-}
-
-// one output coefficient (k, j) of an L2L shift: sum_{n>=k} L_n^m conj(F_{n-k}^{m-j})
-template <int P, int ND>
-__device__ __forceinline__ void l2l_coef(int k, int j, const double2* __restrict__ sF, const double2* __restrict__ sL, double2& o0,
-                                         double2& o1) {
-  constexpr int NF = (P + 1) * (P + 1);
-  double2 a0 = make_double2(0.0, 0.0), a1 = a0, b0 = a0, b1 = a0;
-  for (int n = k; n <= P; ++n) {
-    const int dn = n - k;
-    const int lo = max(-n, j - dn), hi = min(n, j + dn);
-    const double2* f = sF + dn * (dn + 1) - j;
-    const double2* x = sL + n * (n + 1);
-    int m = lo;
-    for (; m < hi; m += 2) {
-      const double2 f0 = f[m], f1 = f[m + 1];
-      const double2 x0 = x[m], y0 = x[m + 1];
-      a0.x += x0.x * f0.x + x0.y * f0.y;
-      a0.y += x0.y * f0.x - x0.x * f0.y;
-      b0.x += y0.x * f1.x + y0.y * f1.y;
-      b0.y += y0.y * f1.x - y0.x * f1.y;
-      if (ND == 2) {
-        const double2 x1 = x[NF + m], y1 = x[NF + m + 1];
-        a1.x += x1.x * f0.x + x1.y * f0.y;
-        a1.y += x1.y * f0.x - x1.x * f0.y;
-        b1.x += y1.x * f1.x + y1.y * f1.y;
-        b1.y += y1.y * f1.x - y1.x * f1.y;
-      }
-    }
-    if (m == hi) {
-      const double2 f0 = f[m], x0 = x[m];
-      a0.x += x0.x * f0.x + x0.y * f0.y;
-      a0.y += x0.y * f0.x - x0.x * f0.y;
-      if (ND == 2) {
-        const double2 x1 = x[NF + m];
-        a1.x += x1.x * f0.x + x1.y * f0.y;
-        a1.y += x1.y * f0.x - x1.x * f0.y;
-      }
-    }
-  }
-  o0 = cadd(o0, cadd(a0, b0));
-  if (ND == 2) o1 = cadd(o1, cadd(a1, b1));
-}
-
 // half-stored [ND][NC] -> full [ND][(P+1)^2] by the threads [0, nthr) of a group
 template <int P, int ND, bool kThroughL2>
 __device__ __forceinline__ void expand_full_group(const double2* __restrict__ src, double2* dst, int tid, int nthr) {
@@ -390,70 +297,137 @@ __device__ __forceinline__ void expand_full_group(const double2* __restrict__ sr
   }
 }
 
-// M2M: the upward pass in one launch.  A block starts at a parent whose children with
-// multipoles are all leaves (ready from the P2M), computes its multipole (group g translating
-// children g, g + 4, ...; partial multipoles summed in group order, so the result does not
-// depend on which block computes it) and climbs: it counts the node in at the parent (a
-// counter per node over the parent's non-leaf children), and the block whose count completes
-// the parent computes the parent next.  Nothing waits: a block that does not complete its
-// parent stops.  The last arrival resets the parent's counter, so every launch starts from
-// zero.  Children's multipoles written by other blocks of the launch are read through L2.
+// Tree translations with kTreeLanes lanes per output coefficient: lane q sums the rows
+// (source degree) q, q + kTreeLanes, ... of the coefficient's terms in two interleaved chains,
+// and the lanes' partial sums are added by warp shuffles in a fixed order (every lane ends with
+// the same sum).  The longest coefficient (121 terms at p = 10) then takes about a third of the
+// dependent adds, and the row bookkeeping is not repeated across lanes.  One CTA per
+// translation (a child and its parent).
+constexpr int kTreeLanes = 4;
+template <int P>
+constexpr int tree_threads() { return (kTreeLanes * ncoef(P) + 31) / 32 * 32; }
+
+__device__ __forceinline__ double2 tree_lanes_sum(double2 v) {
+#pragma unroll
+  for (int o = 1; o < kTreeLanes; o <<= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+
+// conj(f) * x added to a
+__device__ __forceinline__ void cmac_conj(double2& a, const double2 f, const double2 x) {
+  a.x += f.x * x.x + f.y * x.y;
+  a.y += f.x * x.y - f.y * x.x;
+}
+
+// lane q's rows of the M2M output (n, m): sum conj(F_{n1}^{m1}) M_{n-n1}^{m-m1}, n1 = q, q + 4, ...
 template <int P, int ND>
-__global__ void __launch_bounds__(kTreeGroups * tree_group_threads<P>()) k_m2m_up(
-    const int* __restrict__ ready, const int* __restrict__ node_parent, const int* __restrict__ node_level,
-    const int* __restrict__ nsig, int* __restrict__ cnt, const int* __restrict__ child_begin, const int* __restrict__ child_end,
-    const int* __restrict__ node_children, const double* __restrict__ node_X, const double2* __restrict__ Ftab, double2* __restrict__ M) {
+__device__ __forceinline__ void m2m_terms(int n, int m, int q, const double2* __restrict__ sF, const double2* __restrict__ sM, double2& o0,
+                                          double2& o1) {
+  constexpr int NF = (P + 1) * (P + 1);
+  double2 a0 = make_double2(0.0, 0.0), b0 = a0, a1 = a0, b1 = a0;
+  for (int n1 = q; n1 <= n; n1 += kTreeLanes) {
+    const int n2 = n - n1;
+    const int lo = max(-n1, m - n2), hi = min(n1, m + n2);
+    const double2* f = sF + n1 * (n1 + 1);
+    const double2* x = sM + n2 * (n2 + 1) + m;
+    int m1 = lo;
+    for (; m1 < hi; m1 += 2) {
+      cmac_conj(a0, f[m1], x[-m1]);
+      cmac_conj(b0, f[m1 + 1], x[-m1 - 1]);
+      if (ND == 2) {
+        cmac_conj(a1, f[m1], x[NF - m1]);
+        cmac_conj(b1, f[m1 + 1], x[NF - m1 - 1]);
+      }
+    }
+    if (m1 == hi) {
+      cmac_conj(a0, f[m1], x[-m1]);
+      if (ND == 2) cmac_conj(a1, f[m1], x[NF - m1]);
+    }
+  }
+  o0 = cadd(a0, b0);
+  if (ND == 2) o1 = cadd(a1, b1);
+}
+
+// lane q's rows of the L2L output (k, j): sum_{n>=k} L_n^m conj(F_{n-k}^{m-j}), n = k + q, k + q + 4, ...
+template <int P, int ND>
+__device__ __forceinline__ void l2l_terms(int k, int j, int q, const double2* __restrict__ sF, const double2* __restrict__ sL, double2& o0,
+                                          double2& o1) {
+  constexpr int NF = (P + 1) * (P + 1);
+  double2 a0 = make_double2(0.0, 0.0), b0 = a0, a1 = a0, b1 = a0;
+  for (int n = k + q; n <= P; n += kTreeLanes) {
+    const int dn = n - k;
+    const int lo = max(-n, j - dn), hi = min(n, j + dn);
+    const double2* f = sF + dn * (dn + 1) - j;
+    const double2* x = sL + n * (n + 1);
+    int m = lo;
+    for (; m < hi; m += 2) {
+      cmac_conj(a0, f[m], x[m]);
+      cmac_conj(b0, f[m + 1], x[m + 1]);
+      if (ND == 2) {
+        cmac_conj(a1, f[m], x[NF + m]);
+        cmac_conj(b1, f[m + 1], x[NF + m + 1]);
+      }
+    }
+    if (m == hi) {
+      cmac_conj(a0, f[m], x[m]);
+      if (ND == 2) cmac_conj(a1, f[m], x[NF + m]);
+    }
+  }
+  o0 = cadd(a0, b0);
+  if (ND == 2) o1 = cadd(a1, b1);
+}
+
+// M2M, one launch per level from the deepest (moments.hpp:419-436): a CTA per node c of the
+// level that either builds a multipole (a non-leaf whose multipole is needed: the sum of its
+// children's translated multipoles Yup, in child order) or hands its multipole up (its parent's
+// multipole is needed: Yup[c] = the multipole shifted to the parent's centre).  A leaf's
+// multipole comes from the P2M.  Fup: the F tables of the parent level [8 octants][(P+1)^2].
+template <int P, int ND>
+__global__ void __launch_bounds__(tree_threads<P>(), 5) k_m2m_level(const int* __restrict__ nodes, const int* __restrict__ node_up,
+                                                                 const int* __restrict__ child_begin, const int* __restrict__ child_end,
+                                                                 const int* __restrict__ node_children, const double* __restrict__ node_X,
+                                                                 const double2* __restrict__ Fup, double2* __restrict__ M,
+                                                                 double2* __restrict__ Yup) {
   pdl_enter();
-  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), G = kTreeGroups, GT = tree_group_threads<P>();
-  __shared__ double2 sF[G][NF];
-  __shared__ double2 sM[G][ND * NF];
-  __shared__ double2 part[G][ND * NC];
-  __shared__ int s_go;
-  const int g = threadIdx.x / GT, t = threadIdx.x - g * GT;
-  int n = 0, m = 0;
-  if (t < NC) decode_nm(t, n, m);
-  int node = ready[blockIdx.x];
-  for (;;) {
-    const double2* Fl = Ftab + (size_t)node_level[node] * 8 * NF;
-    const int cb = child_begin[node], ce = child_end[node];
-    double2 o0 = make_double2(0.0, 0.0), o1 = o0;
-    for (int c0 = cb; c0 < ce; c0 += G) {
-      const int ci = c0 + g;
-      if (ci < ce) {
-        const int c = node_children[ci];
-        const double2* Ft = Fl + (size_t)child_octant(node_X, c, node) * NF;
-        for (int i = t; i < NF; i += GT) sF[g][i] = Ft[i];
-        expand_full_group<P, ND, true>(M + (size_t)c * 2 * NC, sM[g], t, GT);
-      }
-      __syncthreads();
-      if (ci < ce && t < NC) m2m_coef<P, ND>(n, m, sF[g], sM[g], o0, o1);
-      __syncthreads();
-    }
-    if (t < NC) {
-      part[g][t] = o0;
-      if (ND == 2) part[g][NC + t] = o1;
-    }
-    __syncthreads();
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
+  __shared__ double2 sF[NF];
+  __shared__ double2 sHalf[ND * NC];
+  __shared__ double2 sM[ND * NF];
+  const int c = nodes[blockIdx.x];
+  const int cb = child_begin[c], ce = child_end[c], up = node_up[c];
+  double2* Mc = M + (size_t)c * 2 * NC;
+  if (ce > cb) {
     for (int i = threadIdx.x; i < ND * NC; i += blockDim.x) {
-      double2 v = part[0][i];
-      for (int w = 1; w < G; ++w) v = cadd(v, part[w][i]);
-      M[(size_t)node * 2 * NC + i] = v;
+      double2 s = make_double2(0.0, 0.0);
+      for (int ci = cb; ci < ce; ++ci) s = cadd(s, Yup[(size_t)node_children[ci] * 2 * NC + i]);
+      Mc[i] = s;
+      sHalf[i] = s;
     }
-    const int par = node_parent[node];
-    if (par < 0) return;
-    __threadfence();  // this node's multipole before the count
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int go = atomicAdd(&cnt[par], 1) == nsig[par] - 1;
-      if (go) {
-        cnt[par] = 0;
-        __threadfence();
-      }
-      s_go = go;
-    }
-    __syncthreads();
-    if (!s_go) return;
-    node = par;
+  } else {
+    for (int i = threadIdx.x; i < ND * NC; i += blockDim.x) sHalf[i] = Mc[i];
+  }
+  if (up < 0) return;  // uniform over the CTA
+  const double2* Ft = Fup + (size_t)child_octant(node_X, c, up) * NF;
+  for (int i = threadIdx.x; i < NF; i += blockDim.x) sF[i] = Ft[i];
+  __syncthreads();
+  expand_full_group<P, ND, false>(sHalf, sM, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int o = threadIdx.x / kTreeLanes, q = threadIdx.x % kTreeLanes;
+  double2 a0 = make_double2(0.0, 0.0), a1 = a0;
+  if (o < NC) {
+    int n = 0, m = 0;
+    decode_nm(o, n, m);
+    m2m_terms<P, ND>(n, m, q, sF, sM, a0, a1);
+  }
+  a0 = tree_lanes_sum(a0);
+  if (ND == 2) a1 = tree_lanes_sum(a1);
+  if (o < NC && q == 0) {
+    double2* y = Yup + (size_t)c * 2 * NC;
+    y[o] = a0;
+    if (ND == 2) y[NC + o] = a1;
   }
 }
 
@@ -562,40 +536,35 @@ __global__ void k_m2l_reduce(int ntargets, const int* __restrict__ targets, cons
 }
 
 // ---------------------------------------------------------------------------
-// L2L: one launch per level, top-down; block per parent, its expanded local expansion shared
-// by the groups, group g shifting it to children g, g + 4, ... (thread per output
-// coefficient): L'_k^j += sum_{n>=k} L_n^m conj(F_{n-k}^{m-j}).
+// L2L: one launch per level, top-down (moments.hpp:869-884), a CTA per (parent, child) pair of
+// the level: L'_k^j += sum_{n>=k} L_n^m conj(F_{n-k}^{m-j}), kTreeLanes lanes per output.  Only
+// the child's CTA writes the child in this launch, and parents are only read.
 template <int P, int ND>
-__global__ void __launch_bounds__(kTreeGroups * tree_group_threads<P>()) k_l2l(
-    const int* __restrict__ parents, const int* __restrict__ child_begin, const int* __restrict__ child_end,
-    const int* __restrict__ node_children, const double* __restrict__ node_X, const double2* __restrict__ Ftab,
-    double2* __restrict__ L) {
+__global__ void __launch_bounds__(tree_threads<P>(), 5) k_l2l_pairs(const int2* __restrict__ pairs, const double* __restrict__ node_X,
+                                                                 const double2* __restrict__ Fl, double2* __restrict__ L) {
   pdl_enter();
-  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1), G = kTreeGroups, GT = tree_group_threads<P>();
-  __shared__ double2 sF[G][NF];
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
+  __shared__ double2 sF[NF];
   __shared__ double2 sL[ND * NF];
-  const int par = parents[blockIdx.x];
-  const int g = threadIdx.x / GT, t = threadIdx.x - g * GT;
-  int k = 0, j = 0;
-  if (t < NC) decode_nm(t, k, j);
+  const int2 pc = pairs[blockIdx.x];
+  const int par = pc.x, c = pc.y;
+  const double2* Ft = Fl + (size_t)child_octant(node_X, c, par) * NF;
+  for (int i = threadIdx.x; i < NF; i += blockDim.x) sF[i] = Ft[i];
   expand_full_group<P, ND, false>(L + (size_t)par * 2 * NC, sL, threadIdx.x, blockDim.x);
-  const int cb = child_begin[par], ce = child_end[par];
-  for (int c0 = cb; c0 < ce; c0 += G) {
-    const int ci = c0 + g;
-    const int c = ci < ce ? node_children[ci] : 0;
-    if (ci < ce) {
-      const double2* Ft = Ftab + (size_t)child_octant(node_X, c, par) * NF;
-      for (int i = t; i < NF; i += GT) sF[g][i] = Ft[i];
-    }
-    __syncthreads();
-    if (ci < ce && t < NC) {
-      double2 o0 = make_double2(0.0, 0.0), o1 = o0;
-      l2l_coef<P, ND>(k, j, sF[g], sL, o0, o1);
-      double2* dst = L + (size_t)c * 2 * NC;
-      dst[t] = cadd(dst[t], o0);
-      if (ND == 2) dst[NC + t] = cadd(dst[NC + t], o1);
-    }
-    __syncthreads();
+  __syncthreads();
+  const int o = threadIdx.x / kTreeLanes, q = threadIdx.x % kTreeLanes;
+  double2 a0 = make_double2(0.0, 0.0), a1 = a0;
+  if (o < NC) {
+    int k = 0, j = 0;
+    decode_nm(o, k, j);
+    l2l_terms<P, ND>(k, j, q, sF, sL, a0, a1);
+  }
+  a0 = tree_lanes_sum(a0);
+  if (ND == 2) a1 = tree_lanes_sum(a1);
+  if (o < NC && q == 0) {
+    double2* dst = L + (size_t)c * 2 * NC;
+    dst[o] = cadd(dst[o], a0);
+    if (ND == 2) dst[NC + o] = cadd(dst[NC + o], a1);
   }
 }
 
@@ -1258,11 +1227,16 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     k_p2m<P, ND><<<a.n_leaves, 128, 0, st>>>(a.leaves, a.node_fb, a.node_fe, a.node_X, a.e_q, a.e_W, a.e_n, a.e_dof, a.phi, a.phin, a.M);
     ++launches;
   }
-  if ((stages & STAGE_M2M) && a.n_m2m_ready > 0) {
-    launch_pdl(k_m2m_up<P, ND>, a.n_m2m_ready, kTreeGroups * tree_group_threads<P>(), 0, st, a.m2m_ready, a.node_parent, a.node_level,
-               a.m2m_nsig, a.m2m_cnt, a.child_begin, a.child_end, a.node_children, a.node_X, a.Ftab, a.M);
-    ++launches;
-  }
+  constexpr int NF = (P + 1) * (P + 1);
+  if ((stages & STAGE_M2M) && a.m2m_level_off)
+    for (int l = a.n_levels - 1; l >= 0; --l) {
+      const int cnt = a.m2m_level_off[l + 1] - a.m2m_level_off[l];
+      if (cnt <= 0) continue;
+      const double2* Fup = a.Ftab + (size_t)std::max(l - 1, 0) * 8 * NF;  // tables of the parent level
+      launch_pdl(k_m2m_level<P, ND>, cnt, tree_threads<P>(), 0, st, a.m2m_nodes + a.m2m_level_off[l], a.node_up, a.child_begin, a.child_end,
+                 a.node_children, a.node_X, Fup, a.M, a.Yup);
+      ++launches;
+    }
   if (stages & STAGE_M2L) {
     cudaMemsetAsync(a.L, 0, sizeof(double2) * 2 * NC * (size_t)a.n_nodes, st);
     if (a.use_tc) {
@@ -1277,15 +1251,13 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
       launches += 2;
     }
   }
-  if (stages & STAGE_L2L)
+  if ((stages & STAGE_L2L) && a.l2l_level_off)
     for (int l = 0; l < a.n_levels; ++l) {
-      const int cnt = a.level_parent_off[l + 1] - a.level_parent_off[l];
-      if (cnt > 0) {
-        launch_pdl(k_l2l<P, ND>, cnt, kTreeGroups * tree_group_threads<P>(), 0, st, a.level_parents + a.level_parent_off[l], a.child_begin,
-                                                                            a.child_end, a.node_children, a.node_X,
-                                                                            a.Ftab + (size_t)l * 8 * (P + 1) * (P + 1), a.L);
-        ++launches;
-      }
+      const int cnt = a.l2l_level_off[l + 1] - a.l2l_level_off[l];
+      if (cnt <= 0) continue;
+      launch_pdl(k_l2l_pairs<P, ND>, cnt, tree_threads<P>(), 0, st, a.l2l_pairs + a.l2l_level_off[l], a.node_X, a.Ftab + (size_t)l * 8 * NF,
+                 a.L);
+      ++launches;
     }
   if ((stages & STAGE_TARGETS) && a.n_blocks > 0 && ND == 1 && a.ax && (a.Wc || a.Wc32)) {
     launches += launch_targets_ax<P>(a, st, a.L);

@@ -54,7 +54,7 @@ struct NearBlockDev {
 };
 
 struct MatvecArgs {
-  int n_nodes = 0, n_levels = 0;
+  int n_nodes = 0, n_levels = 0;  // n_levels: tree levels (rows of the per-level lists below)
   // P2M
   int n_leaves = 0;
   const int* leaves = nullptr;
@@ -66,18 +66,18 @@ struct MatvecArgs {
   const double* e_n = nullptr;
   const int* e_dof = nullptr;
   // tree passes
-  const int* level_parent_off = nullptr;  // host array [n_levels+1]
-  const int* level_parents = nullptr;     // device
   const int* child_begin = nullptr;
   const int* child_end = nullptr;
   const int* node_children = nullptr;
   const double2* Ftab = nullptr;           // [level][octant][(P+1)^2] parent-to-child F tables
-  const int* node_parent = nullptr;        // [n_nodes] parent bucket, -1 at the root
-  const int* node_level = nullptr;         // [n_nodes] level (row block of Ftab)
-  const int* m2m_nsig = nullptr;           // [n_nodes] non-leaf children whose multipole completes in the upward pass
-  int n_m2m_ready = 0;                     // parents whose children with multipoles are all leaves
-  const int* m2m_ready = nullptr;
-  int* m2m_cnt = nullptr;                  // [n_nodes] upward-pass arrival counters (zero between launches)
+  // upward pass, one launch per level: the level's nodes that build or hand up a multipole
+  const int* m2m_level_off = nullptr;      // host [n_levels+1] into m2m_nodes
+  const int* m2m_nodes = nullptr;          // device
+  const int* node_up = nullptr;            // [n_nodes] parent whose multipole is needed, else -1
+  double2* Yup = nullptr;                  // [n_nodes][2][NC] multipoles shifted to the parent's centre
+  // downward pass, one launch per parent level: (parent, child) pairs of parents with a local expansion
+  const int* l2l_level_off = nullptr;      // host [n_levels+1] into l2l_pairs
+  const int2* l2l_pairs = nullptr;         // device
 
   int n_m2l_targets = 0;
   const int* m2l_targets = nullptr;
