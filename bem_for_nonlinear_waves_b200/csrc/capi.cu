@@ -150,6 +150,7 @@ struct bem_gpu_ctx {
   DBuf<int> m2m_nodes{&dev_bytes}, node_up{&dev_bytes};
   DBuf<double2> Yup{&dev_bytes};
   DBuf<int2> l2l_pairs{&dev_bytes};
+  DBuf<int> blk_path_off{&dev_bytes}, blk_path{&dev_bytes};  // near block -> its bucket's M2L-target path
   std::vector<int> m2m_level_off, l2l_level_off;
   int n_tree_levels = 0;
   DBuf<int> m2l_targets{&dev_bytes}, m2l_off{&dev_bytes}, m2l_src{&dev_bytes}, nb_dofs{&dev_bytes}, nb_targets{&dev_bytes}, nb_ranges{&dev_bytes}, dof_inc_off{&dev_bytes}, dof_inc{&dev_bytes};
@@ -259,6 +260,8 @@ struct bem_gpu_ctx {
     a.Yup = Yup.p;
     a.l2l_level_off = l2l_level_off.empty() ? nullptr : l2l_level_off.data();
     a.l2l_pairs = l2l_pairs.p;
+    a.blk_path_off = blk_path_off.p;
+    a.blk_path = blk_path.p;
 
     a.n_m2l_targets = n_m2l_targets;
     a.m2l_targets = m2l_targets.p;
@@ -959,6 +962,17 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     max_ndof = std::max(max_ndof, b.ndof);
   }
   ctx->w4_total = w4_total;
+  {  // per near block: its bucket and the bucket's ancestors that are M2L targets, deepest first
+    std::vector<int> off(1, 0), path;
+    for (const auto& b : P.blocks) {
+      for (int a = b.node; a >= 0; a = node_up[a])
+        if (P.m2l_off[a + 1] > P.m2l_off[a]) path.push_back(a);
+      off.push_back((int)path.size());
+    }
+    if (path.empty()) path.push_back(0);
+    CK(up(ctx, ctx->blk_path_off, off));
+    CK(up(ctx, ctx->blk_path, path));
+  }
   // shared memory budget of k_targets: chunk of (phi, phin) + per-target sums
   const int smem_cap = 160 * 1024;
   if (ctx->max_ntgt * 16 > smem_cap / 2) {

@@ -800,18 +800,52 @@ __global__ void __launch_bounds__(kNsThreads) k_near_sums(const NearBlockDev* __
   }
 }
 
+// L2P of one local expansion (shared memory, read at the same address by every thread: a
+// broadcast) at the point d from its centre: the expansion against the regular solid harmonics
+// of d, column m by column from R_m^m = (x + iy)^m / (2^m m!) with
+// (n - m)(n + m) R_n^m = (2n - 1) z R_{n-1}^m - r^2 R_{n-2}^m, fully unrolled so that the
+// recurrence constants fold at compile time.
+template <int P>
+__device__ __forceinline__ double l2p_point(const double2* __restrict__ sL, double px, double py, double pz) {
+  const double r2 = px * px + py * py + pz * pz;
+  double far = 0.0;
+  double2 rmm = make_double2(1.0, 0.0);  // R_m^m
+#pragma unroll
+  for (int m = 0; m <= P; ++m) {
+    if (m > 0) rmm = cscale(cmul(rmm, make_double2(px, py)), 1.0 / (2.0 * m));
+    double2 prev = make_double2(0.0, 0.0), cur = rmm;
+    double fm = 0.0;
+#pragma unroll
+    for (int n = m; n <= P; ++n) {
+      if (n > m) {
+        const double inv = 1.0 / double(n * n - m * m);
+        const double2 nx = make_double2(((2 * n - 1) * pz * cur.x - r2 * prev.x) * inv, ((2 * n - 1) * pz * cur.y - r2 * prev.y) * inv);
+        prev = cur;
+        cur = nx;
+      }
+      const double2 l0 = sL[cidx(n, m)];
+      fm += l0.x * cur.x + l0.y * cur.y;
+    }
+    far += (m == 0 ? 1.0 : 2.0) * fm;
+    // keep the next column's expansion loads below this column (bounded register use)
+    asm volatile("" ::: "memory");
+  }
+  return far;
+}
+
 // Rows of A.x from the near sums k_near_sums left per target slot: rows[i] = near + far -
-// diag_i x_i (a CORNER row: x_i), far = the L2P of the target bucket's local expansion L[0] at the
-// point (no far field when L is null: the near-field operator alone).  One warp-sized CTA per
-// near block (= target bucket), one thread per target: the L2P sums the bucket's expansion
-// against the regular solid harmonics of the point, column m by column from
-// R_m^m = (x + iy)^m / (2^m m!) with (n - m)(n + m) R_n^m = (2n - 1) z R_{n-1}^m - r^2 R_{n-2}^m,
-// fully unrolled so that the recurrence constants fold at compile time; the expansion is read
-// from shared memory at the same address by every thread (a broadcast).
+// diag_i x_i (a CORNER row: x_i).  One warp-sized CTA per near block (= target bucket), one
+// thread per target.  far = the L2P at the point of the local expansion its bucket would hold
+// after the downward pass.  L2L is exact for a truncated local expansion (it re-expands the
+// same degree-P harmonic polynomial about another centre), so that equals the sum of the L2Ps of
+// the M2L locals of the bucket and of its ancestors, each about its own centre: with the block's
+// path (the bucket and its ancestors that are M2L targets, deepest first) the downward pass is
+// not needed.  L null: no far field (the near-field operator alone).
 template <int P>
 __global__ void __launch_bounds__(32) k_target_rows(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_targets,
                                                     const double* __restrict__ Xs, const double* __restrict__ node_X,
-                                                    const double2* __restrict__ L, const double* __restrict__ near_sum,
+                                                    const double2* __restrict__ L, const int* __restrict__ path_off,
+                                                    const int* __restrict__ path, const double* __restrict__ near_sum,
                                                     const double* __restrict__ x, const int* __restrict__ point_dof_off,
                                                     const int* __restrict__ point_dof, const int* __restrict__ dof_kind,
                                                     const double* __restrict__ diag, double* __restrict__ rows) {
@@ -820,42 +854,25 @@ __global__ void __launch_bounds__(32) k_target_rows(const NearBlockDev* __restri
   __shared__ double2 sL[NC];
   const NearBlockDev B = blocks[blockIdx.x];
   const int lane = threadIdx.x;
-  if (L)
-    for (int i = lane; i < NC; i += 32) sL[i] = L[(size_t)B.node * 2 * NC + i];
-  __syncwarp();
-  const double cx = node_X[3 * B.node], cy = node_X[3 * B.node + 1], cz = node_X[3 * B.node + 2];
-  for (int tl = lane; tl < B.ntgt; tl += 32) {
-    const int p = nb_targets[B.tgt_off + tl];
+  const int k0 = L ? path_off[blockIdx.x] : 0, k1 = L ? path_off[blockIdx.x + 1] : 0;
+  for (int t0 = 0; t0 < B.ntgt; t0 += 32) {
+    const int tl = t0 + lane;
+    const bool act = tl < B.ntgt;
+    const int p = act ? nb_targets[B.tgt_off + tl] : 0;
+    const double X0 = Xs[3 * p], X1 = Xs[3 * p + 1], X2 = Xs[3 * p + 2];
     double far = 0.0;
-    if (L) {
-      const double px = Xs[3 * p] - cx, py = Xs[3 * p + 1] - cy, pz = Xs[3 * p + 2] - cz;
-      const double r2 = px * px + py * py + pz * pz;
-      double2 rmm = make_double2(1.0, 0.0);  // R_m^m
-#pragma unroll
-      for (int m = 0; m <= P; ++m) {
-        if (m > 0) rmm = cscale(cmul(rmm, make_double2(px, py)), 1.0 / (2.0 * m));
-        double2 prev = make_double2(0.0, 0.0), cur = rmm;
-        double fm = 0.0;
-#pragma unroll
-        for (int n = m; n <= P; ++n) {
-          if (n > m) {
-            const double inv = 1.0 / double(n * n - m * m);
-            const double2 nx = make_double2(((2 * n - 1) * pz * cur.x - r2 * prev.x) * inv, ((2 * n - 1) * pz * cur.y - r2 * prev.y) * inv);
-            prev = cur;
-            cur = nx;
-          }
-          const double2 l0 = sL[cidx(n, m)];
-          fm += l0.x * cur.x + l0.y * cur.y;
-        }
-        far += (m == 0 ? 1.0 : 2.0) * fm;
-        // keep the next column's expansion loads below this column (bounded register use)
-        asm volatile("" ::: "memory");
-      }
+    for (int k = k0; k < k1; ++k) {
+      const int a = path[k];
+      __syncwarp();
+      for (int i = lane; i < NC; i += 32) sL[i] = L[(size_t)a * 2 * NC + i];
+      __syncwarp();
+      far += l2p_point<P>(sL, X0 - node_X[3 * a], X1 - node_X[3 * a + 1], X2 - node_X[3 * a + 2]);
     }
+    if (!act) continue;
     const double g = near_sum[B.tgt_off + tl] + far;
-    const int k1 = point_dof_off[p + 1];
-    for (int k = point_dof_off[p]; k < k1; ++k) {
-      const int i = point_dof[k];
+    const int d1 = point_dof_off[p + 1];
+    for (int d = point_dof_off[p]; d < d1; ++d) {
+      const int i = point_dof[d];
       const int kd = dof_kind[i];
       rows[i] = (kd == 2) ? x[i] : g - (kd == 0 ? 0.0 : diag[i] * x[i]);
     }
@@ -1195,8 +1212,8 @@ int launch_near_sums(const MatvecArgs& a, cudaStream_t st) {
 // the rows of A.x from the near sums, with the far field of L (none when L is null)
 template <int P>
 int launch_target_rows(const MatvecArgs& a, cudaStream_t st, const double2* L) {
-  launch_pdl(k_target_rows<P>, a.n_blocks, 32, 0, st, a.blocks, a.nb_targets, a.Xs, a.node_X, L, a.near_sum, a.ax, a.point_dof_off,
-             a.point_dof, a.dof_kind, a.diag, a.rows);
+  launch_pdl(k_target_rows<P>, a.n_blocks, 32, 0, st, a.blocks, a.nb_targets, a.Xs, a.node_X, a.blk_path ? L : nullptr, a.blk_path_off,
+             a.blk_path, a.near_sum, a.ax, a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows);
   return 1;
 }
 
@@ -1251,7 +1268,9 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
       launches += 2;
     }
   }
-  if ((stages & STAGE_L2L) && a.l2l_level_off)
+  // the A.x rows sum the L2Ps along each target bucket's path instead (k_target_rows)
+  const bool ax_rows = ND == 1 && a.ax && (a.Wc || a.Wc32) && a.blk_path;
+  if ((stages & STAGE_L2L) && a.l2l_level_off && !ax_rows)
     for (int l = 0; l < a.n_levels; ++l) {
       const int cnt = a.l2l_level_off[l + 1] - a.l2l_level_off[l];
       if (cnt <= 0) continue;

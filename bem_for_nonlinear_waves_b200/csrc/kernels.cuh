@@ -123,6 +123,10 @@ struct MatvecArgs {
   // targets
   int n_blocks = 0, chunk = 0, max_ntgt = 0;
   double* near_sum = nullptr;  // [targets] near sums of A.x by target slot (blocks' tgt_off order)
+  // per near block, its bucket and the bucket's ancestors that are M2L targets, deepest first
+  // (the A.x rows sum their L2Ps instead of a downward pass)
+  const int* blk_path_off = nullptr;  // [n_blocks + 1]
+  const int* blk_path = nullptr;
   const NearBlockDev* blocks = nullptr;
   const int* nb_dofs = nullptr;
   const int* nb_targets = nullptr;
