@@ -151,6 +151,7 @@ struct bem_gpu_ctx {
   DBuf<double2> Yup{&dev_bytes};
   DBuf<int2> l2l_pairs{&dev_bytes};
   DBuf<int> blk_path_off{&dev_bytes}, blk_path{&dev_bytes};  // near block -> its bucket's M2L-target path
+  int max_path = 0;
   std::vector<int> m2m_level_off, l2l_level_off;
   int n_tree_levels = 0;
   DBuf<int> m2l_targets{&dev_bytes}, m2l_off{&dev_bytes}, m2l_src{&dev_bytes}, nb_dofs{&dev_bytes}, nb_targets{&dev_bytes}, nb_ranges{&dev_bytes}, dof_inc_off{&dev_bytes}, dof_inc{&dev_bytes};
@@ -261,6 +262,7 @@ struct bem_gpu_ctx {
     a.l2l_level_off = l2l_level_off.empty() ? nullptr : l2l_level_off.data();
     a.l2l_pairs = l2l_pairs.p;
     a.blk_path_off = blk_path_off.p;
+    a.max_path = max_path;
     a.blk_path = blk_path.p;
 
     a.n_m2l_targets = n_m2l_targets;
@@ -968,6 +970,12 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
       for (int a = b.node; a >= 0; a = node_up[a])
         if (P.m2l_off[a + 1] > P.m2l_off[a]) path.push_back(a);
       off.push_back((int)path.size());
+    }
+    ctx->max_path = 0;
+    for (size_t b = 0; b + 1 < off.size(); ++b) ctx->max_path = std::max(ctx->max_path, off[b + 1] - off[b]);
+    if (configure_target_rows_smem(P.opt.p, ctx->max_path, ctx->max_ntgt) != 0) {
+      ctx->err = "too many targets in one bucket for the rows kernel";
+      return BEM_ERR_UNSUPPORTED;
     }
     if (path.empty()) path.push_back(0);
     CK(up(ctx, ctx->blk_path_off, off));

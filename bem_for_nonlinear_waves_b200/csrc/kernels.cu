@@ -834,41 +834,52 @@ __device__ __forceinline__ double l2p_point(const double2* __restrict__ sL, doub
 }
 
 // Rows of A.x from the near sums k_near_sums left per target slot: rows[i] = near + far -
-// diag_i x_i (a CORNER row: x_i).  One warp-sized CTA per near block (= target bucket), one
-// thread per target.  far = the L2P at the point of the local expansion its bucket would hold
-// after the downward pass.  L2L is exact for a truncated local expansion (it re-expands the
-// same degree-P harmonic polynomial about another centre), so that equals the sum of the L2Ps of
-// the M2L locals of the bucket and of its ancestors, each about its own centre: with the block's
-// path (the bucket and its ancestors that are M2L targets, deepest first) the downward pass is
-// not needed.  L null: no far field (the near-field operator alone).
+// diag_i x_i (a CORNER row: x_i).  far = the L2P at the point of the local expansion its bucket
+// would hold after the downward pass.  L2L is exact for a truncated local expansion (it
+// re-expands the same degree-P harmonic polynomial about another centre), so that equals the sum
+// of the L2Ps of the M2L locals of the bucket and of its ancestors, each about its own centre:
+// with the block's path (the bucket and its ancestors that are M2L targets, deepest first) the
+// downward pass is not needed.  One CTA per near block (= target bucket): the path's locals go
+// to shared memory, a thread per (path node, target) pair evaluates one L2P (pairs node-major,
+// so a warp reads few distinct expansions), and thread t adds its target's L2Ps in path order.
+// L null: no far field (the near-field operator alone).  Dynamic shared memory:
+// target_rows_smem_bytes(P, max_path, max_ntgt).
+constexpr int kRowsThreads = 64;
+inline size_t target_rows_smem_bytes(int p, int max_path, int max_ntgt) {
+  return sizeof(double2) * (size_t)ncoef(p) * std::max(max_path, 1) + sizeof(double) * (size_t)std::max(max_path, 1) * std::max(max_ntgt, 1);
+}
+
 template <int P>
-__global__ void __launch_bounds__(32) k_target_rows(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_targets,
-                                                    const double* __restrict__ Xs, const double* __restrict__ node_X,
-                                                    const double2* __restrict__ L, const int* __restrict__ path_off,
-                                                    const int* __restrict__ path, const double* __restrict__ near_sum,
-                                                    const double* __restrict__ x, const int* __restrict__ point_dof_off,
-                                                    const int* __restrict__ point_dof, const int* __restrict__ dof_kind,
-                                                    const double* __restrict__ diag, double* __restrict__ rows) {
+__global__ void __launch_bounds__(kRowsThreads) k_target_rows(const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_targets,
+                                                              const double* __restrict__ Xs, const double* __restrict__ node_X,
+                                                              const double2* __restrict__ L, const int* __restrict__ path_off,
+                                                              const int* __restrict__ path, const double* __restrict__ near_sum,
+                                                              const double* __restrict__ x, const int* __restrict__ point_dof_off,
+                                                              const int* __restrict__ point_dof, const int* __restrict__ dof_kind,
+                                                              const double* __restrict__ diag, double* __restrict__ rows) {
   pdl_enter();
   constexpr int NC = ncoef(P);
-  __shared__ double2 sL[NC];
+  extern __shared__ __align__(16) double2 rows_smem[];
   const NearBlockDev B = blocks[blockIdx.x];
-  const int lane = threadIdx.x;
-  const int k0 = L ? path_off[blockIdx.x] : 0, k1 = L ? path_off[blockIdx.x + 1] : 0;
-  for (int t0 = 0; t0 < B.ntgt; t0 += 32) {
-    const int tl = t0 + lane;
-    const bool act = tl < B.ntgt;
-    const int p = act ? nb_targets[B.tgt_off + tl] : 0;
-    const double X0 = Xs[3 * p], X1 = Xs[3 * p + 1], X2 = Xs[3 * p + 2];
+  const int k0 = L ? path_off[blockIdx.x] : 0, np = L ? path_off[blockIdx.x + 1] - k0 : 0;
+  double2* sL = rows_smem;                                            // [np][NC]
+  double* part = reinterpret_cast<double*>(rows_smem + (size_t)np * NC);  // [ntgt][np]
+  for (int i = threadIdx.x; i < np * NC; i += kRowsThreads) {
+    const int k = i / NC;
+    sL[i] = L[(size_t)path[k0 + k] * 2 * NC + (i - k * NC)];
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < np * B.ntgt; j += kRowsThreads) {
+    const int k = j / B.ntgt, tl = j - k * B.ntgt;
+    const int a = path[k0 + k], p = nb_targets[B.tgt_off + tl];
+    part[tl * np + k] = l2p_point<P>(sL + (size_t)k * NC, Xs[3 * p] - node_X[3 * a], Xs[3 * p + 1] - node_X[3 * a + 1],
+                                     Xs[3 * p + 2] - node_X[3 * a + 2]);
+  }
+  __syncthreads();
+  for (int tl = threadIdx.x; tl < B.ntgt; tl += kRowsThreads) {
+    const int p = nb_targets[B.tgt_off + tl];
     double far = 0.0;
-    for (int k = k0; k < k1; ++k) {
-      const int a = path[k];
-      __syncwarp();
-      for (int i = lane; i < NC; i += 32) sL[i] = L[(size_t)a * 2 * NC + i];
-      __syncwarp();
-      far += l2p_point<P>(sL, X0 - node_X[3 * a], X1 - node_X[3 * a + 1], X2 - node_X[3 * a + 2]);
-    }
-    if (!act) continue;
+    for (int k = 0; k < np; ++k) far += part[tl * np + k];
     const double g = near_sum[B.tgt_off + tl] + far;
     const int d1 = point_dof_off[p + 1];
     for (int d = point_dof_off[p]; d < d1; ++d) {
@@ -1212,7 +1223,7 @@ int launch_near_sums(const MatvecArgs& a, cudaStream_t st) {
 // the rows of A.x from the near sums, with the far field of L (none when L is null)
 template <int P>
 int launch_target_rows(const MatvecArgs& a, cudaStream_t st, const double2* L) {
-  launch_pdl(k_target_rows<P>, a.n_blocks, 32, 0, st, a.blocks, a.nb_targets, a.Xs, a.node_X, a.blk_path ? L : nullptr, a.blk_path_off,
+  launch_pdl(k_target_rows<P>, a.n_blocks, kRowsThreads, target_rows_smem_bytes(P, a.max_path, a.max_ntgt), st, a.blocks, a.nb_targets, a.Xs, a.node_X, a.blk_path ? L : nullptr, a.blk_path_off,
              a.blk_path, a.near_sum, a.ax, a.point_dof_off, a.point_dof, a.dof_kind, a.diag, a.rows);
   return 1;
 }
@@ -1424,6 +1435,36 @@ void configure_targets_smem(int p, int bytes) {
 #undef BEMB200_CASE
     default: break;
   }
+}
+
+template <int P>
+void set_rows_smem(int bytes) {
+  static std::mutex mu;
+  static int granted[kMaxDevices] = {};
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+  const bool tracked = dev >= 0 && dev < kMaxDevices;
+  std::lock_guard<std::mutex> lk(mu);
+  if (tracked && bytes <= granted[dev]) return;
+  if (tracked) granted[dev] = bytes;
+  cudaFuncSetAttribute(k_target_rows<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+// k_target_rows's dynamic shared memory (the path's locals and the per-(target, node) L2Ps);
+// -1 when it does not fit an SM
+int configure_target_rows_smem(int p, int max_path, int max_ntgt) {
+  const size_t bytes = target_rows_smem_bytes(p, max_path, max_ntgt);
+  if (bytes > 200 * 1024) return -1;
+  switch (p) {
+#define BEMB200_CASE(PP) \
+  case PP:               \
+    set_rows_smem<PP>((int)bytes); break;
+    BEMB200_CASE(1) BEMB200_CASE(2) BEMB200_CASE(3) BEMB200_CASE(4) BEMB200_CASE(5) BEMB200_CASE(6)
+    BEMB200_CASE(7) BEMB200_CASE(8) BEMB200_CASE(9) BEMB200_CASE(10) BEMB200_CASE(11) BEMB200_CASE(12)
+#undef BEMB200_CASE
+    default: break;
+  }
+  return 0;
 }
 
 template <int P>

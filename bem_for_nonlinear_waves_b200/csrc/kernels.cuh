@@ -125,6 +125,7 @@ struct MatvecArgs {
   double* near_sum = nullptr;  // [targets] near sums of A.x by target slot (blocks' tgt_off order)
   // per near block, its bucket and the bucket's ancestors that are M2L targets, deepest first
   // (the A.x rows sum their L2Ps instead of a downward pass)
+  int max_path = 0;                   // longest path
   const int* blk_path_off = nullptr;  // [n_blocks + 1]
   const int* blk_path = nullptr;
   const NearBlockDev* blocks = nullptr;
@@ -178,6 +179,7 @@ struct NearArgs {
 int near_weights_grid();  // CTAs of the near-weight kernel (one scratch row each)
 void upload_quadrature(const double dv[6][4], const double gw[25][3], cudaStream_t s);
 void configure_targets_smem(int p, int bytes);
+int configure_target_rows_smem(int p, int max_path, int max_ntgt);  // -1: does not fit an SM
 void configure_m2l_smem(int p);
 void launch_s_tables(int p, int ngroups, const double* gvec, double2* Sg, cudaStream_t st);
 // F(child - parent) per (level, octant) from one representative offset each: vec [ntab][3]
