@@ -198,12 +198,14 @@ class BEM_BVP:
 
     def setup_phases(self):
         """Seconds spent in each part of the last set-up (host plan phases, uploads, device part)."""
-        out = np.zeros(10)
+        out = np.zeros(16)
         self._check(self.lib.bem_gpu_setup_phases(self.ctx, L.ptr(out, L.P_dbl)), "bem_gpu_setup_phases")
         keys = ["sources", "octree", "lists", "order_nodes", "m2l_groups", "near_blocks", "dof_incidence", "upload", "device"]
         d = {k: float(v) for k, v in zip(keys, out)}
         d["tree_on_device"] = bool(int(out[9]) & 1)
         d["lists_on_device"] = bool(int(out[9]) & 2)
+        up = ["upload_nodes", "upload_blocks", "upload_tc_items", "upload_p2m_lists", "upload_rest", "upload_wait"]
+        d.update({k: float(v) for k, v in zip(up, out[10:16])})
         return d
 
     def poly_roots(self):

@@ -215,6 +215,10 @@ struct bem_gpu_ctx {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // setup device start/end, solve start/end
   float setup_dev_ms = 0.f;
   double time_plan = 0.0, time_upload = 0.0;
+  // the upload part of the set-up by step: [0] node and level arrays, [1] near blocks and
+  // element/tree arrays, [2] tensor-core items, [3] P2M operator lists, [4] remaining arrays,
+  // [5] waiting for the copies
+  double upload_part_s[6] = {0, 0, 0, 0, 0, 0};
 
   DeviceTree* dtree = nullptr;  // octree growth on the device (set-up)
   PinnedStage stage;  // set-up uploads
@@ -674,6 +678,7 @@ int bem_gpu_setup_phases(bem_gpu_ctx* ctx, double* out) {
   out[7] = ctx->time_upload;
   out[8] = 1e-3 * ctx->setup_dev_ms;
   out[9] = (ctx->plan.tree_on_device ? 1 : 0) + (ctx->plan.lists_on_device ? 2 : 0);
+  for (int k = 0; k < 6; ++k) out[10 + k] = ctx->upload_part_s[k];
   return BEM_OK;
 }
 
@@ -833,6 +838,12 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   }
   std::swap(ctx->plan, ctx->plan_spare);
   ctx->time_plan = now_s() - t0;
+  double t_part = now_s();
+  auto part_done = [&](int k) {
+    const double t = now_s();
+    ctx->upload_part_s[k] = t - t_part;
+    t_part = t;
+  };
   Plan& P = ctx->plan;
   ctx->launches += P.device_launches;  // octree and list kernels of the plan
   // a refresh that kept the tree and lists (reuse) and the L2P targets (reuse_near) skips the
@@ -997,6 +1008,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   configure_m2l_smem(P.opt.p);
 
 
+  part_done(0);
   CK(up(ctx, ctx->Xs, P.Xs));
   CK(up(ctx, ctx->e_q, P.e_q));
   CK(up(ctx, ctx->e_W, P.e_W));
@@ -1039,6 +1051,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     CK(ctx->Y.alloc(ctx->opts.precision == 1 ? std::max(y64, ytc) : y64));
   }
   ctx->mixed = ctx->opts.precision == 1;
+  part_done(1);
   if (ctx->mixed) {  // tensor-core M2L: translation tables, multipole rows, work items
     const int p = P.opt.p, kp = tc_kp(p);
     if (!reuse) {  // item size: forced, tuned earlier for this class, or the kernel's maximum until tuned
@@ -1064,16 +1077,8 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     CK(upload_tc_items(ctx, reuse));
     {  // work-item order j -> source bucket and compact target index; pair slot k -> its position j
        // (the row of its partial)
-      std::vector<int> src(P.tc_pair.size()), pos(P.tc_pair.size()), tgt(P.tc_pair.size()), tgt_of_slot((size_t)P.m2l_pairs);
-      for (size_t ti = 0; ti < P.m2l_targets.size(); ++ti) {
-        const int t = P.m2l_targets[ti];
-        for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) tgt_of_slot[k] = (int)ti;
-      }
-      for (size_t j = 0; j < src.size(); ++j) {
-        src[j] = P.m2l_src[P.tc_pair[j]];
-        pos[P.tc_pair[j]] = (int)j;
-        tgt[j] = tgt_of_slot[P.tc_pair[j]];
-      }
+      std::vector<int> src, pos, tgt;
+      tc_item_arrays(P, src, pos, tgt);
       CK(ups(ctx->tc_src, src));
       CK(ups(ctx->tc_pos, pos));
       CK(ups(ctx->tc_tgt, tgt));
@@ -1096,6 +1101,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->opts.device));
     ctx->tc_grid = sms;
   }
+  part_done(2);
   {  // P2M operator of A.x: the DOFs of each leaf's elements, and the slot of every vertex
     const int nl = (int)P.leaves.size();
     std::vector<int> ldo(nl + 1, 0), ld, es(3 * (size_t)P.nf, 0);
@@ -1118,6 +1124,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     CK(ups(ctx->e_slot, es));
     CK(ctx->p2m_C.alloc(std::max<size_t>(ld.size(), 1) * NC));
   }
+  part_done(3);
   CK(ctx->M.alloc((size_t)nb * 2 * NC));
   CK(ctx->L.alloc((size_t)nb * 2 * NC));
   CK(ctx->WG.alloc(std::max<int64_t>(P.nnz, 1)));
@@ -1187,7 +1194,9 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     CK(upn(ctx->self_col, P.self_col));
     CK(ctx->dinv.alloc(N));
   }
+  part_done(4);
   CK(cudaStreamSynchronize(s));
+  part_done(5);
   ctx->time_upload = now_s() - t0 - ctx->time_plan;
   ctx->stage_bytes = std::max(ctx->stage_bytes, ctx->stage.used);
   // device part of the set-up starts here (inputs resident): every kernel that derives the

@@ -39,10 +39,67 @@ inline V3 bary(const double w0, const double w1, const double w2, const V3& a, c
   for (int j = 0; j < 3; ++j) r[j] = std::fma(w2, c[j], r[j]);
   return r;
 }
-// Cross() in binary128, rounded once (basic_arithmetic_array_operations.hpp:906-920)
-inline V3 cross128(const V3& A, const V3& B) {
-  __float128 ax = A[0], ay = A[1], az = A[2], bx = B[0], by = B[1], bz = B[2];
-  return {(double)(ay * bz - az * by), (double)(az * bx - ax * bz), (double)(ax * by - ay * bx)};
+// Double-double arithmetic (Dekker's and Knuth's error-free transformations, ~106 significant
+// bits) in place of the reference's binary128 for the element normals and Jacobians: each
+// result is rounded to double once, as the reference's is, and agrees with it except where the
+// exact value lies within ~2^-104 of a rounding boundary.
+struct DD {
+  double hi, lo;
+};
+inline DD two_sum(double a, double b) {
+  const double s = a + b, bb = s - a;
+  return {s, (a - (s - bb)) + (b - bb)};
+}
+inline DD quick_two_sum(double a, double b) {
+  const double s = a + b;
+  return {s, b - (s - a)};
+}
+inline DD two_prod(double a, double b) {
+  const double p = a * b;
+  return {p, std::fma(a, b, -p)};
+}
+inline DD dd_add(DD x, DD y) {
+  DD s = two_sum(x.hi, y.hi);
+  const DD t = two_sum(x.lo, y.lo);
+  s.lo += t.hi;
+  s = quick_two_sum(s.hi, s.lo);
+  s.lo += t.lo;
+  return quick_two_sum(s.hi, s.lo);
+}
+inline DD dd_neg(DD x) { return {-x.hi, -x.lo}; }
+inline DD dd_mul(DD x, DD y) {
+  DD p = two_prod(x.hi, y.hi);
+  p.lo += x.hi * y.lo + x.lo * y.hi;
+  return quick_two_sum(p.hi, p.lo);
+}
+inline DD dd_mul_d(DD x, double y) {
+  DD p = two_prod(x.hi, y);
+  p.lo += x.lo * y;
+  return quick_two_sum(p.hi, p.lo);
+}
+// 1 / s for a double s: q + (1 - q s) / s
+inline DD dd_recip(double s) {
+  const double q = 1.0 / s;
+  return quick_two_sum(q, std::fma(-q, s, 1.0) / s);
+}
+// Cross(), products exact and differences to ~106 bits, rounded once
+// (basic_arithmetic_array_operations.hpp:906-920)
+inline V3 cross_dd(const V3& A, const V3& B) {
+  return {dd_add(two_prod(A[1], B[2]), dd_neg(two_prod(A[2], B[1]))).hi, dd_add(two_prod(A[2], B[0]), dd_neg(two_prod(A[0], B[2]))).hi,
+          dd_add(two_prod(A[0], B[1]), dd_neg(two_prod(A[1], B[0]))).hi};
+}
+// TriangleNormalHP (…:961-986) in double-double: edge vectors exact, the cross product and its
+// squared norm to ~106 bits, 1/sqrt of the norm rounded to double as the reference does
+inline V3 normal_dd(const V3& a, const V3& b, const V3& c) {
+  const DD bax = two_sum(b[0], -a[0]), bay = two_sum(b[1], -a[1]), baz = two_sum(b[2], -a[2]);
+  const DD cax = two_sum(c[0], -a[0]), cay = two_sum(c[1], -a[1]), caz = two_sum(c[2], -a[2]);
+  const DD nx = dd_add(dd_mul(bay, caz), dd_neg(dd_mul(baz, cay)));
+  const DD ny = dd_add(dd_mul(baz, cax), dd_neg(dd_mul(bax, caz)));
+  const DD nz = dd_add(dd_mul(bax, cay), dd_neg(dd_mul(bay, cax)));
+  const DD n2 = dd_add(dd_add(dd_mul(nx, nx), dd_mul(ny, ny)), dd_mul(nz, nz));
+  if (n2.hi == 0.0) return {0, 0, 0};
+  const DD inv = dd_recip(std::sqrt(n2.hi));
+  return {dd_mul(nx, inv).hi, dd_mul(ny, inv).hi, dd_mul(nz, inv).hi};
 }
 inline V3 unit(V3 a) {  // Normalize (basic_arithmetic_array_operations.hpp:837-850)
   double n = 0.;
@@ -51,16 +108,6 @@ inline V3 unit(V3 a) {  // Normalize (basic_arithmetic_array_operations.hpp:837-
   n = std::sqrt(n);
   for (auto& v : a) v /= n;
   return a;
-}
-inline V3 normal128(const V3& a, const V3& b, const V3& c) {  // TriangleNormalHP (…:961-986)
-  __float128 ax = a[0], ay = a[1], az = a[2];
-  __float128 bax = (__float128)b[0] - ax, bay = (__float128)b[1] - ay, baz = (__float128)b[2] - az;
-  __float128 cax = (__float128)c[0] - ax, cay = (__float128)c[1] - ay, caz = (__float128)c[2] - az;
-  __float128 nx = bay * caz - baz * cay, ny = baz * cax - bax * caz, nz = bax * cay - bay * cax;
-  __float128 n2 = nx * nx + ny * ny + nz * nz;
-  if (n2 == 0) return {0, 0, 0};
-  __float128 inv = (__float128)1 / (__float128)std::sqrt((double)n2);
-  return {(double)(nx * inv), (double)(ny * inv), (double)(nz * inv)};
 }
 inline double dotfma(const V3& a, const V3& b) { return std::fma(a[0], b[0], std::fma(a[1], b[1], a[2] * b[2])); }
 
@@ -292,6 +339,40 @@ bool grow_on_device(TreeBuilder& T, DeviceTree* dt, int nf, const std::vector<V3
 // a stable sort by the part above the slot: a counting sort over a dense table of lattice
 // offsets |r| <= 31 and levels, with the off-lattice pairs last.  Falls back to a comparison
 // sort for larger offsets.
+// The positions i in [0, n) where head(i) holds, in increasing order, found in parallel
+// (per-thread counts, an exclusive scan, then per-thread writes).
+template <typename F>
+static void parallel_heads(int64_t n, F head, std::vector<int64_t>& out) {
+  const int nt = std::max(1, omp_get_max_threads());
+  std::vector<int64_t> cnt(nt + 1, 0);
+#pragma omp parallel num_threads(nt)
+  {
+    const int t = omp_get_thread_num(), T = omp_get_num_threads();
+    const int64_t lo = n * t / T, hi = n * (t + 1) / T;
+    int64_t c = 0;
+    for (int64_t i = lo; i < hi; ++i) c += head(i) ? 1 : 0;
+    cnt[t + 1] = c;
+#pragma omp barrier
+#pragma omp single
+    {
+      for (int k = 0; k < T; ++k) cnt[k + 1] += cnt[k];
+      out.resize(cnt[T]);
+    }
+    int64_t w = cnt[t];
+    for (int64_t i = lo; i < hi; ++i)
+      if (head(i)) out[w++] = i;
+  }
+}
+
+// target bucket of every M2L pair slot (the target-major CSR m2l_off / m2l_src)
+static void pair_targets(const Plan& P, std::vector<int>& pair_tgt) {
+  const int nb = (int)P.nodes.size();
+  pair_tgt.resize(P.m2l_off.empty() ? 0 : P.m2l_off[nb]);
+#pragma omp parallel for schedule(static)
+  for (int t = 0; t < nb; ++t)
+    for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) pair_tgt[k] = t;
+}
+
 void sort_pair_keys(std::vector<uint64_t>& keyed) {
   constexpr int R = 31, W = 2 * R + 1;
   constexpr int64_t kOff = (int64_t)W * W * W * 16;  // dense bucket index; kOff = off the lattice
@@ -425,8 +506,8 @@ int build_dofs(int np, const double* X, int nf, const int32_t* tri, const uint8_
   auto P = [&](int i) { return V3{X[3 * i], X[3 * i + 1], X[3 * i + 2]}; };
   for (int f = 0; f < nf; ++f) {
     V3 a = P(tri[3 * f]), b = P(tri[3 * f + 1]), c = P(tri[3 * f + 2]);
-    fn[f] = normal128(a, b, c);
-    fa[f] = 0.5 * nrm(cross128(sub(b, a), sub(c, a)));
+    fn[f] = normal_dd(a, b, c);
+    fa[f] = 0.5 * nrm(cross_dd(sub(b, a), sub(c, a)));
   }
   std::vector<uint8_t> neu(np, 0), dir(np, 0), cor(np, 0), mult(np, 0);
   const double lim = 20. * M_PI / 180.;  // setIsMultipleNode (BEM_setBoundaryTypes.hpp:434-441)
@@ -614,7 +695,7 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
 #pragma omp parallel for schedule(static)
   for (int f = 0; f < nf; ++f) {
     const V3 a = XP(tri[3 * f]), b = XP(tri[3 * f + 1]), c = XP(tri[3 * f + 2]);
-    const V3 cr = cross128(sub(b, a), sub(c, a));
+    const V3 cr = cross_dd(sub(b, a), sub(c, a));
     const V3 n = unit(cr);
     const double J = nrm(cr);
     pole[f] = bary(1. / 3., 1. / 3., 1. / 3., a, b, c);
@@ -628,7 +709,7 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     offs[f] = off;
     for (int d = 0; d < 3; ++d) en[3 * f + d] = n[d];
     const double area = 0.5 * nrm(cr);
-    const V3 nh = normal128(a, b, c);
+    const V3 nh = normal_dd(a, b, c);
     enear[8 * f + 0] = 2. * area;
     for (int d = 0; d < 3; ++d) {
       enear[8 * f + 1 + d] = 2. * area * nh[d];
@@ -856,6 +937,7 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   P.m2l_pairs = P.m2l_off[nb];
   // targets (target4FMM::setL2P / setDirectIntegration: getBucketAtDeepest)
   P.target_box.assign(np, -1);
+#pragma omp parallel for schedule(static)
   for (int p = 0; p < np; ++p) {
     if (P.point_dof_off[p] == P.point_dof_off[p + 1]) continue;
     const double* x = &P.Xs[3 * p];
@@ -894,10 +976,8 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
       P.error = "too many M2L pairs";
       return false;
     }
-    std::vector<int> pair_tgt(npair);
-#pragma omp parallel for schedule(static)
-    for (int t = 0; t < nb; ++t)
-      for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) pair_tgt[k] = t;
+    std::vector<int> pair_tgt;
+    pair_targets(P, pair_tgt);
     std::vector<uint64_t>& keyed = P.m2l_key_sorted;
     keyed.resize(npair);
     std::vector<double> bx(4 * (size_t)nb);  // bucket centre and size, packed (the pair loop reads them at random)
@@ -921,32 +1001,39 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
       keyed[k] = lattice ? ((((rkey << 4) | (uint64_t)P.nodes[t].level) << 29) | (uint64_t)k) : ((uint64_t(1) << 63) | (uint64_t)k);
     }
     sort_pair_keys(keyed);
-    P.grp_vec.clear();
-    P.grp_off.assign(1, 0);
+    // groups: runs of one (offset, level) key; a pair off the lattice is a group of its own
+    const uint64_t kmask = (uint64_t(1) << 29) - 1;
+    std::vector<int64_t> gs;
+    parallel_heads(
+        npair, [&](int64_t i) { return i == 0 || (keyed[i] >> 63) || (keyed[i - 1] >> 63) || (keyed[i] >> 29) != (keyed[i - 1] >> 29); },
+        gs);
+    const int ng = (int)gs.size();
+    P.grp_off.resize(ng + 1);
+    P.grp_vec.resize(3 * (size_t)ng);
     P.grp_pair.resize(npair);
-    for (int64_t i = 0; i < npair;) {
-      int64_t j = i;
-      const int k0 = (int)(keyed[i] & ((uint64_t(1) << 29) - 1));
+    std::vector<int> nch(ng + 1, 0);  // chunks of <= 8 pairs per group, then their offsets
+#pragma omp parallel for schedule(static)
+    for (int g = 0; g < ng; ++g) {
+      const int64_t b = gs[g], e = g + 1 < ng ? gs[g + 1] : npair;
+      P.grp_off[g] = (int)b;
+      const int k0 = (int)(keyed[b] & kmask);
       const int t0 = pair_tgt[k0], s0 = P.m2l_src[k0];
-      for (int a = 0; a < 3; ++a) P.grp_vec.push_back(B[t0].X[a] - B[s0].X[a]);
-      const bool lattice = (keyed[i] >> 63) == 0;
-      const uint64_t g = keyed[i] >> 29;
-      do {
-        P.grp_pair[j] = (int)(keyed[j] & ((uint64_t(1) << 29) - 1));
-        ++j;
-      } while (lattice && j < npair && (keyed[j] >> 29) == g);
-      P.grp_off.push_back((int)j);
-      i = j;
+      for (int a = 0; a < 3; ++a) P.grp_vec[3 * (size_t)g + a] = B[t0].X[a] - B[s0].X[a];
+      nch[g + 1] = (int)((e - b + 7) / 8);
     }
-    P.chunk_grp.clear();
-    P.chunk_begin.clear();
-    P.chunk_cnt.clear();
-    const int ng = (int)P.grp_off.size() - 1;
+    P.grp_off[ng] = (int)npair;
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < npair; ++j) P.grp_pair[j] = (int)(keyed[j] & kmask);
+    for (int g = 0; g < ng; ++g) nch[g + 1] += nch[g];
+    P.chunk_grp.resize(nch[ng]);
+    P.chunk_begin.resize(nch[ng]);
+    P.chunk_cnt.resize(nch[ng]);
+#pragma omp parallel for schedule(static)
     for (int g = 0; g < ng; ++g)
-      for (int b = P.grp_off[g]; b < P.grp_off[g + 1]; b += 8) {
-        P.chunk_grp.push_back(g);
-        P.chunk_begin.push_back(b);
-        P.chunk_cnt.push_back(std::min(8, P.grp_off[g + 1] - b));
+      for (int c = nch[g], b = P.grp_off[g]; c < nch[g + 1]; ++c, b += 8) {
+        P.chunk_grp[c] = g;
+        P.chunk_begin[c] = b;
+        P.chunk_cnt[c] = std::min(8, P.grp_off[g + 1] - b);
       }
     P.m2l_targets.clear();
     for (int t = 0; t < nb; ++t)
@@ -1109,40 +1196,68 @@ void retile_tc_items(Plan& P, int max_pairs) {
 void build_tc_groups(Plan& P, int max_pairs) {
   // tables = runs of one lattice offset over all levels in the sorted pair order of the FP64
   // groups (the pairs of one offset are contiguous there); pairs off the lattice get one each
-  const int nb = (int)P.nodes.size();
   const int64_t npair = (int64_t)P.m2l_key_sorted.size();
+  const std::vector<uint64_t>& keyed = P.m2l_key_sorted;
   const uint64_t kmask = (uint64_t(1) << 29) - 1;
-  std::vector<int> pair_tgt(npair);
-  for (int t = 0; t < nb; ++t)
-    for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) pair_tgt[k] = t;
-  P.tc_tab.clear();
+  std::vector<int> pair_tgt;
+  pair_targets(P, pair_tgt);
+  std::vector<int64_t> rs;
+  parallel_heads(
+      npair, [&](int64_t i) { return i == 0 || (keyed[i] >> 63) || (keyed[i - 1] >> 63) || (keyed[i] >> 33) != (keyed[i - 1] >> 33); }, rs);
+  const int nt = (int)rs.size();
+  P.tc_tab.resize(4 * (size_t)nt);
   P.tc_pair.resize(npair);
-  P.tc_item_tab.clear();
-  P.tc_item_begin.clear();
-  P.tc_item_cnt.clear();
-  for (int64_t i = 0; i < npair;) {
-    const uint64_t v0 = P.m2l_key_sorted[i];
-    const bool lattice = (v0 >> 63) == 0;
-    const int k0 = (int)(v0 & kmask);
+  std::vector<int> nit(nt + 1, 0);  // items per table, then their offsets
+#pragma omp parallel for schedule(static)
+  for (int t = 0; t < nt; ++t) {
+    const int64_t b = rs[t], e = t + 1 < nt ? rs[t + 1] : npair;
+    const bool lattice = (keyed[b] >> 63) == 0;
+    const int k0 = (int)(keyed[b] & kmask);
     const auto& T = P.nodes[pair_tgt[k0]];
     const auto& S = P.nodes[P.m2l_src[k0]];
     for (int a = 0; a < 3; ++a) {
       const double q = (T.X[a] - S.X[a]) / T.dL;
-      P.tc_tab.push_back(lattice ? (double)std::llround(q) : q);
+      P.tc_tab[4 * (size_t)t + a] = lattice ? (double)std::llround(q) : q;
     }
-    P.tc_tab.push_back(lattice ? 1.0 : S.dL / T.dL);
-    const int tab = (int)(P.tc_tab.size() / 4) - 1;
-    int64_t j = i;
-    do {
-      P.tc_pair[j] = (int)(P.m2l_key_sorted[j] & kmask);
-      ++j;
-    } while (lattice && j < npair && (P.m2l_key_sorted[j] >> 33) == (v0 >> 33));
-    for (int64_t b = i; b < j; b += max_pairs) {
-      P.tc_item_tab.push_back(tab);
-      P.tc_item_begin.push_back((int)b);
-      P.tc_item_cnt.push_back((int)std::min<int64_t>(max_pairs, j - b));
+    P.tc_tab[4 * (size_t)t + 3] = lattice ? 1.0 : S.dL / T.dL;
+    nit[t + 1] = (int)((e - b + max_pairs - 1) / max_pairs);
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < npair; ++j) P.tc_pair[j] = (int)(keyed[j] & kmask);
+  for (int t = 0; t < nt; ++t) nit[t + 1] += nit[t];
+  P.tc_item_tab.resize(nit[nt]);
+  P.tc_item_begin.resize(nit[nt]);
+  P.tc_item_cnt.resize(nit[nt]);
+#pragma omp parallel for schedule(static)
+  for (int t = 0; t < nt; ++t) {
+    const int64_t e = t + 1 < nt ? rs[t + 1] : npair;
+    int64_t b = rs[t];
+    for (int i = nit[t]; i < nit[t + 1]; ++i, b += max_pairs) {
+      P.tc_item_tab[i] = t;
+      P.tc_item_begin[i] = (int)b;
+      P.tc_item_cnt[i] = (int)std::min<int64_t>(max_pairs, e - b);
     }
-    i = j;
+  }
+}
+
+void tc_item_arrays(const Plan& P, std::vector<int>& src, std::vector<int>& pos, std::vector<int>& tgt) {
+  const size_t n = P.tc_pair.size();
+  src.resize(n);
+  pos.resize(n);
+  tgt.resize(n);
+  std::vector<int> tgt_of_slot((size_t)P.m2l_pairs);
+  const int nt = (int)P.m2l_targets.size();
+#pragma omp parallel for schedule(static)
+  for (int ti = 0; ti < nt; ++ti) {
+    const int t = P.m2l_targets[ti];
+    for (int k = P.m2l_off[t]; k < P.m2l_off[t + 1]; ++k) tgt_of_slot[k] = ti;
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < (int64_t)n; ++j) {
+    const int k = P.tc_pair[j];
+    src[j] = P.m2l_src[k];
+    pos[k] = (int)j;
+    tgt[j] = tgt_of_slot[k];
   }
 }
 

@@ -155,6 +155,9 @@ void parallel_copy(void* dst, const void* src, size_t bytes);
 
 // Groups the M2L pairs for the tensor-core path (tc_* fields); items hold <= max_pairs pairs.
 void build_tc_groups(Plan& plan, int max_pairs);
+// per tensor-core pair (work-item order j): its source bucket and compact target index (into
+// m2l_targets); per pair slot k: its position j
+void tc_item_arrays(const Plan& plan, std::vector<int>& src, std::vector<int>& pos, std::vector<int>& tgt);
 // Re-splits the tensor-core work items of build_tc_groups into items of <= max_pairs pairs
 // (tables and pair order unchanged).
 void retile_tc_items(Plan& plan, int max_pairs);
