@@ -129,7 +129,7 @@ struct Bucket {
   std::vector<int> data;                  // data1D
   std::vector<int> kid_of_cell;
   double off = 0.0;
-  std::vector<int> near, m2l, l2m;
+  std::vector<int> near, m2l;
 };
 
 void bucket_init(Bucket& b, const double lo[3], const double hi[3], double dL) {
@@ -832,9 +832,45 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     for (int g = 0; g < (int)starts.size() - 1; ++g)
       for (int i = starts[g]; i < starts[g + 1]; ++i) lists(opt, B, tasks[torder[i]].first, tasks[torder[i]].second);
   }
-  for (auto& lv : lvl)
-    for (int a : lv)
-      for (int b : B[a].m2l) B[b].l2m.push_back(a);
+  // the M2L sources of every target b, in the order the traversal (level by level) meets them:
+  // the inverse of the m2l lists as a CSR, built by a parallel counting sort over the sources
+  // taken in that order (per-thread counts per target, then a scan over (target, thread))
+  std::vector<int> l2m_off(nb + 1, 0), l2m_src;
+  {
+    std::vector<int> order;
+    for (auto& lv : lvl) order.insert(order.end(), lv.begin(), lv.end());
+    const int na = (int)order.size();
+    const int nt = std::max(1, omp_get_max_threads());
+    std::vector<int> cnt((size_t)nt * nb, 0);
+    int T = 1;
+#pragma omp parallel num_threads(nt)
+    {
+      const int t = omp_get_thread_num();
+#pragma omp single
+      T = omp_get_num_threads();
+      const int lo = (int)((int64_t)na * t / T), hi = (int)((int64_t)na * (t + 1) / T);
+      int* c = &cnt[(size_t)t * nb];
+      for (int i = lo; i < hi; ++i)
+        for (int b : B[order[i]].m2l) ++c[b];
+#pragma omp barrier
+#pragma omp single
+      {
+        int run = 0;
+        for (int b = 0; b < nb; ++b) {
+          l2m_off[b] = run;
+          for (int u = 0; u < T; ++u) {
+            const int k = cnt[(size_t)u * nb + b];
+            cnt[(size_t)u * nb + b] = run;
+            run += k;
+          }
+        }
+        l2m_off[nb] = run;
+        l2m_src.resize(run);
+      }
+      for (int i = lo; i < hi; ++i)
+        for (int b : B[order[i]].m2l) l2m_src[c[b]++] = order[i];
+    }
+  }
 
   lap(2);
   // element order: DFS pre-order of the deepest bucket holding each element
@@ -925,13 +961,13 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   P.m2l_off.assign(nb + 1, 0);
   P.near_off.assign(nb + 1, 0);
   for (int i = 0; i < nb; ++i) {
-    P.m2l_off[i + 1] = P.m2l_off[i] + (B[i].data.empty() ? 0 : (int)B[i].l2m.size());
+    P.m2l_off[i + 1] = P.m2l_off[i] + (B[i].data.empty() ? 0 : l2m_off[i + 1] - l2m_off[i]);
     P.near_off[i + 1] = P.near_off[i] + (int)B[i].near.size();
   }
   P.m2l_src.resize(P.m2l_off[nb]);
   P.near_nodes.resize(P.near_off[nb]);
   for (int i = 0; i < nb; ++i) {
-    if (!B[i].data.empty()) std::copy(B[i].l2m.begin(), B[i].l2m.end(), P.m2l_src.begin() + P.m2l_off[i]);
+    if (!B[i].data.empty()) std::copy(l2m_src.begin() + l2m_off[i], l2m_src.begin() + l2m_off[i + 1], P.m2l_src.begin() + P.m2l_off[i]);
     std::copy(B[i].near.begin(), B[i].near.end(), P.near_nodes.begin() + P.near_off[i]);
   }
   P.m2l_pairs = P.m2l_off[nb];
