@@ -147,12 +147,12 @@ struct bem_gpu_ctx {
   DBuf<int> e_dof{&dev_bytes}, e_vtx{&dev_bytes}, node_fb{&dev_bytes}, node_fe{&dev_bytes}, leaves{&dev_bytes}, child_begin{&dev_bytes}, child_end{&dev_bytes}, node_children{&dev_bytes};
   // tree passes, one launch per level: upward-pass nodes and the parent each hands its multipole
   // to, the multipoles shifted to the parent, downward-pass (parent, child) pairs
-  DBuf<int> m2m_nodes{&dev_bytes}, node_up{&dev_bytes};
+  DBuf<int> m2m_nodes{&dev_bytes}, node_up{&dev_bytes}, m2m_nodes_nl{&dev_bytes}, leaf_level{&dev_bytes};
   DBuf<double2> Yup{&dev_bytes};
   DBuf<int2> l2l_pairs{&dev_bytes};
   DBuf<int> blk_path_off{&dev_bytes}, blk_path{&dev_bytes};  // near block -> its bucket's M2L-target path
   int max_path = 0;
-  std::vector<int> m2m_level_off, l2l_level_off;
+  std::vector<int> m2m_level_off, m2m_level_off_nl, l2l_level_off;
   int n_tree_levels = 0;
   DBuf<int> m2l_targets{&dev_bytes}, m2l_off{&dev_bytes}, m2l_src{&dev_bytes}, nb_dofs{&dev_bytes}, nb_targets{&dev_bytes}, nb_ranges{&dev_bytes}, dof_inc_off{&dev_bytes}, dof_inc{&dev_bytes};
   DBuf<int> block_of_point{&dev_bytes}, row_of_point{&dev_bytes}, self_col{&dev_bytes};  // right-Jacobi inputs
@@ -263,6 +263,9 @@ struct bem_gpu_ctx {
     a.m2m_nodes = m2m_nodes.p;
     a.node_up = node_up.p;
     a.Yup = Yup.p;
+    a.m2m_level_off_nl = m2m_level_off_nl.empty() ? nullptr : m2m_level_off_nl.data();
+    a.m2m_nodes_nl = m2m_nodes_nl.p;
+    a.leaf_level = leaf_level.p;
     a.l2l_level_off = l2l_level_off.empty() ? nullptr : l2l_level_off.data();
     a.l2l_pairs = l2l_pairs.p;
     a.blk_path_off = blk_path_off.p;
@@ -904,13 +907,21 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     ctx->n_tree_levels = nlev;
     std::vector<int> up_needed(nb, -1), mnodes;
     for (int i = 0; i < nb; ++i) up_needed[i] = (node_up[i] >= 0 && m_needed[node_up[i]]) ? node_up[i] : -1;
-    // upward: nodes that build a needed multipole from their children or hand theirs up
+    // upward: nodes that build a needed multipole from their children or hand theirs up; the
+    // same without the leaves (the A.x P2M kernel shifts the leaves' multipoles itself)
+    std::vector<int> mnodes_nl, llev(std::max<size_t>(P.leaves.size(), 1), 0);
     ctx->m2m_level_off.assign(1, 0);
+    ctx->m2m_level_off_nl.assign(1, 0);
     for (int l = 0; l < nlev; ++l) {
-      for (int i : P.level_nodes[l])
-        if ((P.nodes[i].child_end > P.nodes[i].child_begin && m_needed[i]) || up_needed[i] >= 0) mnodes.push_back(i);
+      for (int i : P.level_nodes[l]) {
+        const bool parent = P.nodes[i].child_end > P.nodes[i].child_begin;
+        if ((parent && m_needed[i]) || up_needed[i] >= 0) mnodes.push_back(i);
+        if (parent && (m_needed[i] || up_needed[i] >= 0)) mnodes_nl.push_back(i);
+      }
       ctx->m2m_level_off.push_back((int)mnodes.size());
+      ctx->m2m_level_off_nl.push_back((int)mnodes_nl.size());
     }
+    for (size_t li = 0; li < P.leaves.size(); ++li) llev[li] = P.nodes[P.leaves[li]].level;
     // downward: (parent, child) pairs of the parents with a non-zero local expansion
     std::vector<int2> pairs;
     ctx->l2l_level_off.assign(1, 0);
@@ -921,9 +932,12 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
       ctx->l2l_level_off.push_back((int)pairs.size());
     }
     if (mnodes.empty()) mnodes.push_back(0);  // keep the device arrays non-empty
+    if (mnodes_nl.empty()) mnodes_nl.push_back(0);
     if (pairs.empty()) pairs.push_back(make_int2(0, 0));
     CK(ups(ctx->m2m_nodes, mnodes));
     CK(ups(ctx->node_up, up_needed));
+    CK(ups(ctx->m2m_nodes_nl, mnodes_nl));
+    CK(ups(ctx->leaf_level, llev));
     CK(ups(ctx->l2l_pairs, pairs));
     CK(ctx->Yup.alloc((size_t)std::max(nb, 1) * 2 * ncoef(P.opt.p)));
   }

@@ -431,6 +431,58 @@ __global__ void __launch_bounds__(tree_threads<P>(), 5) k_m2m_level(const int* _
   }
 }
 
+// P2M of A.x fused with the leaf's first M2M shift: a CTA per leaf computes
+// M_leaf = sum_d x_d C_{leaf,d} (kTreeLanes lanes per coefficient over interleaved DOFs, lane
+// sums added by shuffles in a fixed order) and, when its parent's multipole is needed, shifts
+// it to the parent's centre into Yup (the same shift as k_m2m_level), so the upward pass
+// starts at the leaves' parents.  Fl: the F tables of every level, leaf_level: each leaf's level.
+template <int P>
+__global__ void __launch_bounds__(tree_threads<P>(), 5) k_p2m_leaf(const int* __restrict__ leaves, const int* __restrict__ leaf_dof_off,
+                                                                   const int* __restrict__ leaf_dof, const double2* __restrict__ C,
+                                                                   const double* __restrict__ x, const int* __restrict__ node_up,
+                                                                   const int* __restrict__ leaf_level, const double* __restrict__ node_X,
+                                                                   const double2* __restrict__ Ftab, double2* __restrict__ M,
+                                                                   double2* __restrict__ Yup) {
+  pdl_enter();
+  constexpr int NC = ncoef(P), NF = (P + 1) * (P + 1);
+  __shared__ double2 sF[NF];
+  __shared__ double2 sHalf[NC];
+  __shared__ double2 sM[NF];
+  const int li = blockIdx.x, leaf = leaves[li];
+  const int o = threadIdx.x / kTreeLanes, q = threadIdx.x % kTreeLanes;
+  const int up = node_up[leaf];
+  if (up >= 0) {  // the shift's table, loaded while the multipole is summed
+    const double2* Ft = Ftab + ((size_t)(leaf_level[li] - 1) * 8 + child_octant(node_X, leaf, up)) * NF;
+    for (int i = threadIdx.x; i < NF; i += blockDim.x) sF[i] = Ft[i];
+  }
+  const int d0 = leaf_dof_off[li], d1 = leaf_dof_off[li + 1];
+  double2 acc = make_double2(0.0, 0.0);
+  if (o < NC)
+    for (int j = d0 + q; j < d1; j += kTreeLanes) {
+      const double xv = x[leaf_dof[j]];
+      const double2 c = C[(size_t)j * NC + o];
+      acc.x = fma(xv, c.x, acc.x);
+      acc.y = fma(xv, c.y, acc.y);
+    }
+  acc = tree_lanes_sum(acc);
+  if (o < NC && q == 0) {
+    M[(size_t)leaf * 2 * NC + o] = acc;
+    sHalf[o] = acc;
+  }
+  if (up < 0) return;  // uniform over the CTA
+  __syncthreads();
+  expand_full_group<P, 1, false>(sHalf, sM, threadIdx.x, blockDim.x);
+  __syncthreads();
+  double2 a0 = make_double2(0.0, 0.0), a1 = a0;
+  if (o < NC) {
+    int n = 0, m = 0;
+    decode_nm(o, n, m);
+    m2m_terms<P, 1>(n, m, q, sF, sM, a0, a1);
+  }
+  a0 = tree_lanes_sum(a0);
+  if (o < NC && q == 0) Yup[(size_t)leaf * 2 * NC + o] = a0;
+}
+
 // ---------------------------------------------------------------------------
 // M2L grouped by translation vector.
 //   k_s_tables    (set-up) one irregular-harmonic table S(d_g) per group, all orders
@@ -1248,7 +1300,14 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     cudaEventRecord(a.ev_join, a.side);
     stages &= ~STAGE_TARGETS;
   }
-  if ((stages & STAGE_P2M) && a.n_leaves > 0 && ND == 1 && a.ax && a.p2m_C) {
+  // A.x: the P2M operator, each leaf's multipole shifted to its parent in the same kernel, and
+  // an upward pass over the non-leaf nodes only
+  const bool ax_p2m = ND == 1 && a.ax && a.p2m_C && a.leaf_level && a.m2m_level_off_nl;
+  if ((stages & STAGE_P2M) && a.n_leaves > 0 && ax_p2m) {
+    launch_pdl(k_p2m_leaf<P>, a.n_leaves, tree_threads<P>(), 0, st, a.leaves, a.leaf_dof_off, a.leaf_dof, a.p2m_C, a.ax, a.node_up,
+               a.leaf_level, a.node_X, a.Ftab, a.M, a.Yup);
+    ++launches;
+  } else if ((stages & STAGE_P2M) && a.n_leaves > 0 && ND == 1 && a.ax && a.p2m_C) {
     launch_pdl(k_p2m_apply<P>, a.n_leaves, tpb_coef, 0, st, a.leaves, a.leaf_dof_off, a.leaf_dof, a.p2m_C, a.ax, a.M);
     ++launches;
   } else if ((stages & STAGE_P2M) && a.n_leaves > 0) {
@@ -1256,15 +1315,18 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     ++launches;
   }
   constexpr int NF = (P + 1) * (P + 1);
-  if ((stages & STAGE_M2M) && a.m2m_level_off)
+  if ((stages & STAGE_M2M) && a.m2m_level_off) {
+    const int* off = ax_p2m ? a.m2m_level_off_nl : a.m2m_level_off;  // without the leaves when k_p2m_leaf shifted them
+    const int* nodes = ax_p2m ? a.m2m_nodes_nl : a.m2m_nodes;
     for (int l = a.n_levels - 1; l >= 0; --l) {
-      const int cnt = a.m2m_level_off[l + 1] - a.m2m_level_off[l];
+      const int cnt = off[l + 1] - off[l];
       if (cnt <= 0) continue;
       const double2* Fup = a.Ftab + (size_t)std::max(l - 1, 0) * 8 * NF;  // tables of the parent level
-      launch_pdl(k_m2m_level<P, ND>, cnt, tree_threads<P>(), 0, st, a.m2m_nodes + a.m2m_level_off[l], a.node_up, a.child_begin, a.child_end,
-                 a.node_children, a.node_X, Fup, a.M, a.Yup);
+      launch_pdl(k_m2m_level<P, ND>, cnt, tree_threads<P>(), 0, st, nodes + off[l], a.node_up, a.child_begin, a.child_end, a.node_children,
+                 a.node_X, Fup, a.M, a.Yup);
       ++launches;
     }
+  }
   if (stages & STAGE_M2L) {
     cudaMemsetAsync(a.L, 0, sizeof(double2) * 2 * NC * (size_t)a.n_nodes, st);
     if (a.use_tc) {

@@ -75,6 +75,9 @@ struct MatvecArgs {
   const int* m2m_nodes = nullptr;          // device
   const int* node_up = nullptr;            // [n_nodes] parent whose multipole is needed, else -1
   double2* Yup = nullptr;                  // [n_nodes][2][NC] multipoles shifted to the parent's centre
+  const int* m2m_level_off_nl = nullptr;   // host [n_levels+1]: the same lists without the leaves
+  const int* m2m_nodes_nl = nullptr;       // device
+  const int* leaf_level = nullptr;         // [n_leaves] level of each leaf (A.x: k_p2m_leaf shifts the leaves)
   // downward pass, one launch per parent level: (parent, child) pairs of parents with a local expansion
   const int* l2l_level_off = nullptr;      // host [n_levels+1] into l2l_pairs
   const int2* l2l_pairs = nullptr;         // device
