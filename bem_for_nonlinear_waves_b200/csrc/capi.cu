@@ -212,7 +212,8 @@ struct bem_gpu_ctx {
   // accounting of the current setup + solve
   int64_t h2d = 0, d2h = 0, launches = 0;
   int64_t setup_h2d = 0, setup_launches = 0;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // setup device start/end, solve start/end
+  // set-up device window start/end, solve start/end, near-field quadrature start/end
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   float setup_dev_ms = 0.f;
   double time_plan = 0.0, time_upload = 0.0;
   // the upload part of the set-up by step: [0] node and level arrays, [1] near blocks and
@@ -835,7 +836,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   // built into the spare plan (the one before the current: its arrays' memory is reused), then
   // swapped in; the current plan is the refresh's previous plan
   if (!build_plan(ctx->plan_spare, po, d->n_points, d->X, d->n_faces, d->tri, d->face_dirichlet, d->n_dof, d->dof_point, d->dof_face,
-                  d->dof_kind, d->face_dof, refresh && had_plan ? &ctx->plan : nullptr)) {
+                  d->dof_kind, d->face_dof, refresh && had_plan ? &ctx->plan : nullptr, /*defer_m2l_groups=*/true)) {
     ctx->err = ctx->plan_spare.error;
     return BEM_ERR_INVALID_ARGUMENT;
   }
@@ -856,7 +857,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
      // plan's array sizes for the first one (pinning a larger area later is slow)
     const size_t ne = (size_t)P.nf, pairs = (size_t)P.m2l_pairs;
     const size_t est = ne * (18 + 6 + 3 + 8) * 8 + ne * 3 * 4 * 4 + (size_t)P.np * 3 * 8 + P.nb_dofs.size() * 4 +
-                       pairs * 4 * (ctx->opts.precision == 1 ? 4 : 2) + P.chunk_grp.size() * 12 + P.dof_inc.size() * 4 +
+                       pairs * 4 * (ctx->opts.precision == 1 ? 4 : 2) + pairs * 2 + P.dof_inc.size() * 4 +
                        P.blocks.size() * sizeof(NearBlockDev) + P.nb_targets.size() * 8 + P.nb_ranges.size() * 4 +
                        (size_t)P.ndof * 16 + (size_t)P.np * 12 + P.nodes.size() * 64 + (size_t)(4 << 20);
     CK(ctx->stage.begin(std::max(ctx->stage_bytes, reuse ? 0 : est), ctx->stream));
@@ -967,8 +968,6 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
       ctx->launches += 1;
     }
   }
-  const std::vector<int>& mt = P.m2l_targets;
-  ctx->n_m2l_targets = (int)mt.size();
   std::vector<NearBlockDev> bd(P.blocks.size());
   ctx->max_ntgt = 1;
   int max_ndof = 1;
@@ -1023,13 +1022,75 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
 
 
   part_done(0);
+  // The near-field quadrature needs only the near blocks and the element geometry: those go up
+  // first and the quadrature runs on the device while the host groups the M2L pairs.  Its
+  // device time is counted into the set-up's (a window of its own: the uploads around it are
+  // not device work).
   CK(up(ctx, ctx->Xs, P.Xs));
+  CK(up(ctx, ctx->e_near, P.e_near));
+  CK(ups(ctx->e_vtx, P.e_vtx));
+  CK(upn(ctx->nb_dofs, P.nb_dofs));
+  CK(upn(ctx->nb_targets, P.nb_targets));
+  CK(upn(ctx->nb_ranges, P.nb_ranges));
+  CK(ups(ctx->dof_inc_off, P.dof_inc_off));
+  CK(ups(ctx->dof_inc, P.dof_inc));
+  CK(upn(ctx->blocks, bd));
+  CK(ctx->WG.alloc(std::max<int64_t>(P.nnz, 1)));
+  CK(ctx->WGn.alloc(std::max<int64_t>(P.nnz, 1)));
+  NearArgs na;
+  na.n_blocks = (int)P.blocks.size();
+  na.blocks = ctx->blocks.p;
+  na.nb_dofs = ctx->nb_dofs.p;
+  na.nb_targets = ctx->nb_targets.p;
+  na.nb_ranges = ctx->nb_ranges.p;
+  na.dof_inc_off = ctx->dof_inc_off.p;
+  na.dof_inc = ctx->dof_inc.p;
+  na.Xs = ctx->Xs.p;
+  na.e_vtx = ctx->e_vtx.p;
+  na.e_near = ctx->e_near.p;
+  na.near_region = P.near_region;
+  na.WG = ctx->WG.p;
+  na.WGn = ctx->WGn.p;
+  {
+    std::vector<int> sb(P.nb_targets.size());
+    int mr = 0;
+    int64_t mel = 1;
+    for (int bi = 0; bi < (int)P.blocks.size(); ++bi) {
+      const auto& nbk = P.blocks[bi];
+      for (int tl = 0; tl < nbk.ntgt; ++tl) sb[nbk.tgt_off + tl] = bi;
+      mr = std::max(mr, nbk.nrng);
+      int64_t ne = 0;
+      for (int r = 0; r < nbk.nrng; ++r) ne += P.nb_ranges[2 * (nbk.rng_off + r) + 1] - P.nb_ranges[2 * (nbk.rng_off + r)];
+      mel = std::max(mel, ne);
+    }
+    CK(upn(ctx->slot_block, sb));
+    na.n_slots = (int)sb.size();
+    na.slot_block = ctx->slot_block.p;
+    na.max_nrng = mr;
+    na.scratch_stride = 3 * mel;
+    CK(ctx->near_scratch.alloc((size_t)near_weights_grid() * na.scratch_stride));
+    na.scratch = ctx->near_scratch.p;
+  }
+  CK(cudaEventRecord(ctx->ev[4], s));
+  launch_near_weights(na, s);
+  CK(cudaEventRecord(ctx->ev[5], s));
+  CK(cudaGetLastError());
+  if (!P.reused_m2l) {  // M2L grouping on the host meanwhile
+    const double tg = now_s();
+    if (!build_m2l_groups(P)) {
+      ctx->err = P.error;
+      return BEM_ERR_INVALID_ARGUMENT;
+    }
+    P.phase_s[4] += now_s() - tg;
+    ctx->time_plan += now_s() - tg;  // host plan work, not upload
+  }
+  t_part = now_s();
+  const std::vector<int>& mt = P.m2l_targets;
+  ctx->n_m2l_targets = (int)mt.size();
   CK(up(ctx, ctx->e_q, P.e_q));
   CK(up(ctx, ctx->e_W, P.e_W));
   CK(up(ctx, ctx->e_n, P.e_n));
-  CK(up(ctx, ctx->e_near, P.e_near));
   CK(ups(ctx->e_dof, P.e_dof));
-  CK(ups(ctx->e_vtx, P.e_vtx));
   CK(ups(ctx->node_X, nX));
   CK(ups(ctx->node_fb, nfb));
   CK(ups(ctx->node_fe, nfe));
@@ -1040,16 +1101,10 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   CK(ups(ctx->m2l_targets, mt));
   CK(ups(ctx->m2l_off, P.m2l_off));
   CK(ups(ctx->m2l_src, P.m2l_src));
-  CK(upn(ctx->nb_dofs, P.nb_dofs));
-  CK(upn(ctx->nb_targets, P.nb_targets));
-  CK(upn(ctx->nb_ranges, P.nb_ranges));
-  CK(ups(ctx->dof_inc_off, P.dof_inc_off));
-  CK(ups(ctx->dof_inc, P.dof_inc));
   CK(ups(ctx->point_dof_off, P.point_dof_off));
   CK(ups(ctx->point_dof, P.point_dof));
   CK(ups(ctx->dof_kind, P.dof_kind));
   CK(ups(ctx->dof_point, P.dof_point));
-  CK(upn(ctx->blocks, bd));
   CK(ups(ctx->chunk_grp, P.chunk_grp));
   CK(ups(ctx->chunk_begin, P.chunk_begin));
   CK(ups(ctx->chunk_cnt, P.chunk_cnt));
@@ -1141,8 +1196,6 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   part_done(3);
   CK(ctx->M.alloc((size_t)nb * 2 * NC));
   CK(ctx->L.alloc((size_t)nb * 2 * NC));
-  CK(ctx->WG.alloc(std::max<int64_t>(P.nnz, 1)));
-  CK(ctx->WGn.alloc(std::max<int64_t>(P.nnz, 1)));
   CK(ctx->Wc.alloc(std::max<int64_t>(ctx->w4_total, 1)));  // rows padded to 4 columns, as the FP32 copy
   const bool want_w32 = ctx->opts.precision == 1 || ctx->opts.preconditioner == 2;
   if (want_w32) CK(ctx->Wc32.alloc(std::max<int64_t>(ctx->w4_total, 1)));
@@ -1162,41 +1215,6 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   CK(ctx->GnPhi.alloc(P.np));
   CK(ctx->mv_in.alloc(N));
   CK(ctx->mv_out.alloc(N));
-  // near-field weights: work partition and scratch
-  NearArgs na;
-  na.n_blocks = (int)P.blocks.size();
-  na.blocks = ctx->blocks.p;
-  na.nb_dofs = ctx->nb_dofs.p;
-  na.nb_targets = ctx->nb_targets.p;
-  na.nb_ranges = ctx->nb_ranges.p;
-  na.dof_inc_off = ctx->dof_inc_off.p;
-  na.dof_inc = ctx->dof_inc.p;
-  na.Xs = ctx->Xs.p;
-  na.e_vtx = ctx->e_vtx.p;
-  na.e_near = ctx->e_near.p;
-  na.near_region = P.near_region;
-  na.WG = ctx->WG.p;
-  na.WGn = ctx->WGn.p;
-  {
-    std::vector<int> sb(P.nb_targets.size());
-    int mr = 0;
-    int64_t mel = 1;
-    for (int bi = 0; bi < (int)P.blocks.size(); ++bi) {
-      const auto& nbk = P.blocks[bi];
-      for (int tl = 0; tl < nbk.ntgt; ++tl) sb[nbk.tgt_off + tl] = bi;
-      mr = std::max(mr, nbk.nrng);
-      int64_t ne = 0;
-      for (int r = 0; r < nbk.nrng; ++r) ne += P.nb_ranges[2 * (nbk.rng_off + r) + 1] - P.nb_ranges[2 * (nbk.rng_off + r)];
-      mel = std::max(mel, ne);
-    }
-    CK(upn(ctx->slot_block, sb));
-    na.n_slots = (int)sb.size();
-    na.slot_block = ctx->slot_block.p;
-    na.max_nrng = mr;
-    na.scratch_stride = 3 * mel;
-    CK(ctx->near_scratch.alloc((size_t)near_weights_grid() * na.scratch_stride));
-    na.scratch = ctx->near_scratch.p;
-  }
   {  // right-Jacobi scaling inputs: each point's near-field block row
     std::vector<int> bop(P.np), rop(P.np);
     for (int p = 0; p < P.np; ++p) {
@@ -1241,7 +1259,6 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     launch_p2m_op(P.opt.p, pa, ctx->e_slot.p, s);
     ctx->launches += 1;
   }
-  launch_near_weights(na, s);
   launch_combine_weights((int)P.blocks.size(), ctx->blocks.p, ctx->nb_dofs.p, ctx->dof_kind.p, ctx->WG.p, ctx->WGn.p, ctx->Wc.p,
                          want_w32 ? ctx->Wc32.p : nullptr, s);
   ctx->launches += want_w32 ? 2 : 1;
@@ -1289,6 +1306,11 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   if (rc != BEM_OK) return rc;
   CK(cudaStreamSynchronize(s));
   CK(cudaEventElapsedTime(&ctx->setup_dev_ms, ctx->ev[0], ctx->ev[1]));
+  {
+    float nw_ms = 0.f;
+    CK(cudaEventElapsedTime(&nw_ms, ctx->ev[4], ctx->ev[5]));
+    ctx->setup_dev_ms += nw_ms;
+  }
   ctx->setup_h2d = ctx->h2d;
   ctx->setup_launches = ctx->launches;
   ctx->time_setup = now_s() - t0;

@@ -593,8 +593,87 @@ static bool same_tree(const Plan& a, const Plan& b) {
          a.leaves == b.leaves && a.level_nodes == b.level_nodes;
 }
 
+// M2L grouped by lattice offset r = (X_t - X_s) / dL_t and level; groups ordered by key,
+// pairs within a group in slot order.  One parallel sort of packed 64-bit values
+// (offset key | level | slot; a pair off the lattice gets a value of its own, sorted last)
+// serves both the FP64 groups (level, r) and the tensor-core tables (r on every level).  Fills
+// the groups, their chunks of <= 8 pairs and the targets with at least one pair.
+bool build_m2l_groups(Plan& P) {
+  const int nb = (int)P.nodes.size();
+  const int64_t npair = P.m2l_pairs;
+  if (npair >= (int64_t(1) << 29)) {
+    P.error = "too many M2L pairs";
+    return false;
+  }
+  std::vector<int> pair_tgt;
+  pair_targets(P, pair_tgt);
+  std::vector<uint64_t>& keyed = P.m2l_key_sorted;
+  keyed.resize(npair);
+  std::vector<double> bx(4 * (size_t)nb);  // bucket centre and size, packed (the pair loop reads them at random)
+  for (int i = 0; i < nb; ++i) {
+    for (int a = 0; a < 3; ++a) bx[4 * (size_t)i + a] = P.nodes[i].X[a];
+    bx[4 * (size_t)i + 3] = P.nodes[i].dL;
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < npair; ++k) {
+    const int t = pair_tgt[k], s = P.m2l_src[k];
+    const double* xt = &bx[4 * (size_t)t];
+    const double* xs = &bx[4 * (size_t)s];
+    bool lattice = std::abs(xs[3] - xt[3]) <= 1e-12 * xt[3];
+    long long r[3];
+    for (int a = 0; a < 3; ++a) {
+      const double q = (xt[a] - xs[a]) / xt[3];
+      r[a] = std::llround(q);
+      if (std::abs(q - (double)r[a]) > 1e-9 || std::abs(r[a]) > 500) lattice = false;
+    }
+    const uint64_t rkey = (uint64_t)(((r[0] + 512) << 20) | ((r[1] + 512) << 10) | (r[2] + 512));
+    keyed[k] = lattice ? ((((rkey << 4) | (uint64_t)P.nodes[t].level) << 29) | (uint64_t)k) : ((uint64_t(1) << 63) | (uint64_t)k);
+  }
+  sort_pair_keys(keyed);
+  // groups: runs of one (offset, level) key; a pair off the lattice is a group of its own
+  const uint64_t kmask = (uint64_t(1) << 29) - 1;
+  std::vector<int64_t> gs;
+  parallel_heads(
+      npair, [&](int64_t i) { return i == 0 || (keyed[i] >> 63) || (keyed[i - 1] >> 63) || (keyed[i] >> 29) != (keyed[i - 1] >> 29); },
+      gs);
+  const int ng = (int)gs.size();
+  P.grp_off.resize(ng + 1);
+  P.grp_vec.resize(3 * (size_t)ng);
+  P.grp_pair.resize(npair);
+  std::vector<int> nch(ng + 1, 0);  // chunks of <= 8 pairs per group, then their offsets
+#pragma omp parallel for schedule(static)
+  for (int g = 0; g < ng; ++g) {
+    const int64_t b = gs[g], e = g + 1 < ng ? gs[g + 1] : npair;
+    P.grp_off[g] = (int)b;
+    const int k0 = (int)(keyed[b] & kmask);
+    const int t0 = pair_tgt[k0], s0 = P.m2l_src[k0];
+    for (int a = 0; a < 3; ++a) P.grp_vec[3 * (size_t)g + a] = P.nodes[t0].X[a] - P.nodes[s0].X[a];
+    nch[g + 1] = (int)((e - b + 7) / 8);
+  }
+  P.grp_off[ng] = (int)npair;
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < npair; ++j) P.grp_pair[j] = (int)(keyed[j] & kmask);
+  for (int g = 0; g < ng; ++g) nch[g + 1] += nch[g];
+  P.chunk_grp.resize(nch[ng]);
+  P.chunk_begin.resize(nch[ng]);
+  P.chunk_cnt.resize(nch[ng]);
+#pragma omp parallel for schedule(static)
+  for (int g = 0; g < ng; ++g)
+    for (int c = nch[g], b = P.grp_off[g]; c < nch[g + 1]; ++c, b += 8) {
+      P.chunk_grp[c] = g;
+      P.chunk_begin[c] = b;
+      P.chunk_cnt[c] = std::min(8, P.grp_off[g + 1] - b);
+    }
+  P.m2l_targets.clear();
+  for (int t = 0; t < nb; ++t)
+    if (P.m2l_off[t + 1] > P.m2l_off[t]) P.m2l_targets.push_back(t);
+
+  return true;
+}
+
 bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int ndof,
-                const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof, Plan* prev) {
+                const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof, Plan* prev,
+                bool defer_m2l_groups) {
   {  // start from an empty plan that keeps the capacity of P's arrays: a plan of similar size
      // then reuses memory whose pages are already mapped
     Plan fresh;
@@ -1002,79 +1081,7 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     P.tc_item_begin = std::move(prev->tc_item_begin);
     P.tc_item_cnt = std::move(prev->tc_item_cnt);
   }
-  // M2L grouped by lattice offset r = (X_t - X_s) / dL_t and level; groups ordered by key,
-  // pairs within a group in slot order.  One parallel sort of packed 64-bit values
-  // (offset key | level | slot; a pair off the lattice gets a value of its own, sorted last)
-  // serves both the FP64 groups (level, r) and the tensor-core tables (r on every level).
-  if (!P.reused_m2l) {
-    const int64_t npair = P.m2l_pairs;
-    if (npair >= (int64_t(1) << 29)) {
-      P.error = "too many M2L pairs";
-      return false;
-    }
-    std::vector<int> pair_tgt;
-    pair_targets(P, pair_tgt);
-    std::vector<uint64_t>& keyed = P.m2l_key_sorted;
-    keyed.resize(npair);
-    std::vector<double> bx(4 * (size_t)nb);  // bucket centre and size, packed (the pair loop reads them at random)
-    for (int i = 0; i < nb; ++i) {
-      for (int a = 0; a < 3; ++a) bx[4 * (size_t)i + a] = B[i].X[a];
-      bx[4 * (size_t)i + 3] = B[i].dL;
-    }
-#pragma omp parallel for schedule(static)
-    for (int64_t k = 0; k < npair; ++k) {
-      const int t = pair_tgt[k], s = P.m2l_src[k];
-      const double* xt = &bx[4 * (size_t)t];
-      const double* xs = &bx[4 * (size_t)s];
-      bool lattice = std::abs(xs[3] - xt[3]) <= 1e-12 * xt[3];
-      long long r[3];
-      for (int a = 0; a < 3; ++a) {
-        const double q = (xt[a] - xs[a]) / xt[3];
-        r[a] = std::llround(q);
-        if (std::abs(q - (double)r[a]) > 1e-9 || std::abs(r[a]) > 500) lattice = false;
-      }
-      const uint64_t rkey = (uint64_t)(((r[0] + 512) << 20) | ((r[1] + 512) << 10) | (r[2] + 512));
-      keyed[k] = lattice ? ((((rkey << 4) | (uint64_t)P.nodes[t].level) << 29) | (uint64_t)k) : ((uint64_t(1) << 63) | (uint64_t)k);
-    }
-    sort_pair_keys(keyed);
-    // groups: runs of one (offset, level) key; a pair off the lattice is a group of its own
-    const uint64_t kmask = (uint64_t(1) << 29) - 1;
-    std::vector<int64_t> gs;
-    parallel_heads(
-        npair, [&](int64_t i) { return i == 0 || (keyed[i] >> 63) || (keyed[i - 1] >> 63) || (keyed[i] >> 29) != (keyed[i - 1] >> 29); },
-        gs);
-    const int ng = (int)gs.size();
-    P.grp_off.resize(ng + 1);
-    P.grp_vec.resize(3 * (size_t)ng);
-    P.grp_pair.resize(npair);
-    std::vector<int> nch(ng + 1, 0);  // chunks of <= 8 pairs per group, then their offsets
-#pragma omp parallel for schedule(static)
-    for (int g = 0; g < ng; ++g) {
-      const int64_t b = gs[g], e = g + 1 < ng ? gs[g + 1] : npair;
-      P.grp_off[g] = (int)b;
-      const int k0 = (int)(keyed[b] & kmask);
-      const int t0 = pair_tgt[k0], s0 = P.m2l_src[k0];
-      for (int a = 0; a < 3; ++a) P.grp_vec[3 * (size_t)g + a] = B[t0].X[a] - B[s0].X[a];
-      nch[g + 1] = (int)((e - b + 7) / 8);
-    }
-    P.grp_off[ng] = (int)npair;
-#pragma omp parallel for schedule(static)
-    for (int64_t j = 0; j < npair; ++j) P.grp_pair[j] = (int)(keyed[j] & kmask);
-    for (int g = 0; g < ng; ++g) nch[g + 1] += nch[g];
-    P.chunk_grp.resize(nch[ng]);
-    P.chunk_begin.resize(nch[ng]);
-    P.chunk_cnt.resize(nch[ng]);
-#pragma omp parallel for schedule(static)
-    for (int g = 0; g < ng; ++g)
-      for (int c = nch[g], b = P.grp_off[g]; c < nch[g + 1]; ++c, b += 8) {
-        P.chunk_grp[c] = g;
-        P.chunk_begin[c] = b;
-        P.chunk_cnt[c] = std::min(8, P.grp_off[g + 1] - b);
-      }
-    P.m2l_targets.clear();
-    for (int t = 0; t < nb; ++t)
-      if (P.m2l_off[t + 1] > P.m2l_off[t]) P.m2l_targets.push_back(t);
-  }
+  if (!P.reused_m2l && !defer_m2l_groups && !build_m2l_groups(P)) return false;
   P.near_pairs = P.near_off[nb];
   for (int i = 0; i < nb; ++i)
     if (B[i].data.empty()) P.near_pairs -= (int)B[i].near.size();

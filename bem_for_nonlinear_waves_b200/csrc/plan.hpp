@@ -146,9 +146,13 @@ int build_dofs(int np, const double* X, int nf, const int32_t* tri, const uint8_
 // tree and lists come out identical to prev's, the M2L structure is moved out of prev (prev is
 // left partly empty; plan.reused_m2l), and with identical L2P targets the near-field blocks too
 // (plan.reused_near).
+// defer_m2l_groups: leave the M2L grouping (build_m2l_groups) to the caller, who can run it while
+// the device works on what the plan already holds (it is skipped anyway when reused_m2l).
 bool build_plan(Plan& plan, const PlanOptions& opt, int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int ndof,
                 const int32_t* dof_point, const int32_t* dof_face, const int32_t* dof_kind, const int32_t* face_dof,
-                Plan* prev = nullptr);
+                Plan* prev = nullptr, bool defer_m2l_groups = false);
+// the M2L grouping of build_plan (FP64 groups, chunks, targets with pairs)
+bool build_m2l_groups(Plan& plan);
 
 // memcpy in 1 MiB pieces over the OpenMP threads (staging of the set-up uploads)
 void parallel_copy(void* dst, const void* src, size_t bytes);
