@@ -29,6 +29,8 @@
 #include <unordered_set>
 #include <vector>
 
+#include <omp.h>
+
 #include "../../include/bem_b200.h"
 
 struct bem_gpu_batch {
@@ -248,7 +250,13 @@ bem_gpu_batch* bem_gpu_batch_create(const bem_gpu_opts* opts, int32_t n_workers)
   b->mel.assign(n_workers, nullptr);
   b->held.assign(n_workers, 0);
   b->reserved.assign(n_workers, 0);
-  for (int w = 0; w < n_workers; ++w) b->workers.emplace_back([b, w] { b->run(w); });
+  // the host plan of each worker runs OpenMP regions: the workers share the host's cores
+  const int threads = std::max(1, omp_get_num_procs() / std::max(1, n_workers));
+  for (int w = 0; w < n_workers; ++w)
+    b->workers.emplace_back([b, w, threads] {
+      omp_set_num_threads(threads);
+      b->run(w);
+    });
   return b;
 }
 
