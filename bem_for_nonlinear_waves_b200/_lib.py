@@ -96,6 +96,8 @@ EXPORTS = {
     "bem_gpu_mel_velocity": (c_int, [ctypes.c_void_p, ctypes.POINTER(MelSurface), P_dbl, P_dbl]),
     "bem_gpu_mel_stage": (c_int, [ctypes.c_void_p, ctypes.POINTER(MelSurface), c_int, c_dbl, c_dbl, P_dbl, P_dbl, P_dbl, P_dbl,
                                   P_dbl, P_dbl, P_dbl, P_dbl, P_dbl, P_dbl]),
+    "bem_gpu_mel_phit_known": (c_int, [ctypes.c_void_p, ctypes.POINTER(MelSurface), P_int, P_int, P_int, P_int, c_int, P_dbl, c_dbl,
+                                       P_dbl, P_dbl]),
     "bem_gpu_batch_create": (ctypes.c_void_p, [ctypes.POINTER(Opts), c_int]),
     "bem_gpu_batch_submit": (c_int, [ctypes.c_void_p, ctypes.POINTER(Desc), P_dbl, P_dbl, P_dbl, ctypes.POINTER(Stats),
                                      ctypes.POINTER(ctypes.c_int64)]),

@@ -491,3 +491,26 @@ class MELStage:
                                         L.ptr(dp, L.P_dbl))
         self._check(rc, "mel stage")
         return Xo.reshape(-1, 3), po, u.reshape(-1, 3), dp
+
+    def phit_known(self, X, phi, phin, face_body=None, bodies=None, u=None):
+        """Known values of the phi_t BVP (setPhiPhin_t, bem/BEM_setBoundaryTypes.hpp:858-935) for
+        the solution (phi, phin per DOF) at positions X: phi_t = -|u|^2/2 - g z on Dirichlet DOFs,
+        phin_t on Neumann DOFs (0 on faces of no body; on faces of rigid body b, face_body[f] = b,
+        phint_Neumann with bodies[b] = (centre, velocity, angular velocity, acceleration, angular
+        acceleration), 15 values).  u: point velocities, None to compute them from the solution.
+        Solve with BEM_BVP.solve(known) on the same set-up: ans is phin_t on Dirichlet DOFs and
+        phi_t on the others."""
+        s = self._surface(X, phi, phin)
+        d = self.dofs
+        dp, df, dk = (np.ascontiguousarray(d[k], np.int32) for k in ("dof_point", "dof_face", "dof_kind"))
+        nf = self.tri.shape[0]
+        fb = np.full(nf, -1, np.int32) if face_body is None else np.ascontiguousarray(face_body, np.int32)
+        bd = np.zeros((0, 15)) if bodies is None else np.ascontiguousarray(bodies, np.float64).reshape(-1, 15)
+        bdf = np.ascontiguousarray(bd.reshape(-1)) if bd.size else np.zeros(15)
+        uu = None if u is None else np.ascontiguousarray(u, np.float64).reshape(-1)
+        out = np.zeros(dp.shape[0])
+        rc = self.lib.bem_gpu_mel_phit_known(self.handle, ctypes.byref(s), L.ptr(dp, L.P_int), L.ptr(df, L.P_int), L.ptr(dk, L.P_int),
+                                             L.ptr(fb, L.P_int), int(bd.shape[0]), L.ptr(bdf, L.P_dbl), self.gravity,
+                                             None if uu is None else L.ptr(uu, L.P_dbl), L.ptr(out, L.P_dbl))
+        self._check(rc, "phi_t known values")
+        return out

@@ -266,12 +266,123 @@ __global__ void k_mel_push(int np, int stage, double dt, double gravity, const u
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Known values of the phi_t boundary-value problem (setPhiPhin_t,
+// bem/BEM_setBoundaryTypes.hpp:858-935).
+
+// gradient, within the triangle's plane, of the linear function taking v[k] at x[k] (the three
+// vertices): with e = x1 - x0, f = x2 - x0 and the in-plane frame ex = e/|e|,
+// ey = (ez x ex), ez the unit normal of e x f, the function is v0 + a (p . ex) + b (p . ey) with
+// a = (v1 - v0)/|e| and b fixed by the third vertex (gradP1, lib/include/basic_vectors.hpp:2112-2128)
+__device__ void grad_linear_tri(const double x[3][3], const double v[3], double g[3]) {
+  double e[3] = {x[1][0] - x[0][0], x[1][1] - x[0][1], x[1][2] - x[0][2]};
+  double f[3] = {x[2][0] - x[0][0], x[2][1] - x[0][1], x[2][2] - x[0][2]};
+  double ex[3] = {e[0], e[1], e[2]}, ez[3], ey[3];
+  v3unit(ex);
+  v3cross(e, f, ez);
+  v3unit(ez);
+  v3cross(ez, ex, ey);
+  v3unit(ey);
+  const double x1 = sqrt(v3dot(e, e)), x2 = v3dot(f, ex), y2 = v3dot(f, ey);
+  const double a = (v[1] - v[0]) / x1;
+  const double b = (v[2] * x1 - v[1] * x2 + v[0] * (x2 - x1)) / (x1 * y2);
+  for (int k = 0; k < 3; ++k) g[k] = a * ex[k] + b * ey[k];
+}
+
+// phin_t at point p on the Neumann face F (phint_Neumann(p, F), bem/BEM_BoundaryValues.hpp:701-728):
+// 0 on a face of no body; on a face of rigid body b (bodies[15 b ..]: centre c, velocity U,
+// angular velocity W, acceleration A, angular acceleration Al; RigidBodyDynamics.hpp:84-89)
+//   v = U + W x r, a = A + Al x r + W x (W x r), r = x_p - c,
+//   phin_t = n.a + (W x n).(v - u_p) - (B v).H0,
+// B = {n, s0, s1} (OrthogonalBasis, :307-315) and H0 the first row of HessianOfPhi (:653-672):
+// with the vertices and their velocities in that basis and g_ij = component j of the in-plane
+// gradient of component i of the velocity, H0 = (-g11 - g22, (g01 + g10)/2, (g02 + g20)/2).
+__device__ double phint_face(int p, int F, const int32_t* __restrict__ tri, const double* __restrict__ X, const double* __restrict__ normal,
+                             const double* __restrict__ u, const int32_t* __restrict__ face_body, const double* __restrict__ bodies) {
+  const int b = face_body[F];
+  if (b < 0) return 0.0;
+  const double* B = bodies + 15 * b;
+  const double n[3] = {normal[3 * F], normal[3 * F + 1], normal[3 * F + 2]};
+  const double r[3] = {X[3 * p] - B[0], X[3 * p + 1] - B[1], X[3 * p + 2] - B[2]};
+  double wr[3], wwr[3], alr[3], wn[3];
+  v3cross(B + 6, r, wr);
+  v3cross(B + 6, wr, wwr);
+  v3cross(B + 12, r, alr);
+  v3cross(B + 6, n, wn);
+  double v[3], a[3];
+  for (int k = 0; k < 3; ++k) {
+    v[k] = B[3 + k] + wr[k];
+    a[k] = B[9 + k] + alr[k] + wwr[k];
+  }
+  // basis {n, s0, s1}: s0 = the part of ex (or ey, when ex is almost normal) off n
+  double s0[3] = {1.0 - n[0] * n[0], -n[0] * n[1], -n[0] * n[2]};
+  if (sqrt(v3dot(s0, s0)) < 1e-3) {
+    s0[0] = -n[1] * n[0];
+    s0[1] = 1.0 - n[1] * n[1];
+    s0[2] = -n[1] * n[2];
+  }
+  v3unit(s0);
+  double s1[3];
+  v3cross(n, s0, s1);
+  v3unit(s1);
+  const double* basis[3] = {n, s0, s1};
+  double xr[3][3], ur[3][3];  // [vertex][basis component]
+  for (int k = 0; k < 3; ++k) {
+    const int q = tri[3 * F + k];
+    for (int i = 0; i < 3; ++i) {
+      xr[k][i] = v3dot(basis[i], X + 3 * q);
+      ur[k][i] = v3dot(basis[i], u + 3 * q);
+    }
+  }
+  double g[3][3];  // g[i][j]: in-plane gradient (component j) of velocity component i
+  for (int i = 0; i < 3; ++i) {
+    const double vi[3] = {ur[0][i], ur[1][i], ur[2][i]};
+    grad_linear_tri(xr, vi, g[i]);
+  }
+  const double H0[3] = {-g[1][1] - g[2][2], 0.5 * (g[0][1] + g[1][0]), 0.5 * (g[0][2] + g[2][0])};
+  const double tmp[3] = {v3dot(n, v), v3dot(s0, v), v3dot(s1, v)};
+  const double du[3] = {v[0] - u[3 * p], v[1] - u[3 * p + 1], v[2] - u[3 * p + 2]};
+  return v3dot(n, a) + v3dot(wn, du) - v3dot(tmp, H0);
+}
+
+// per DOF: Dirichlet (kind 0) phi_t = -|u|^2/2 - gravity z (aphiat(0), lib/include/Network.hpp:971-976);
+// Neumann (kinds 1, 2) phin_t of its face, or for a point DOF the area-weighted mean over the
+// point's Neumann faces (phint_Neumann(p), bem/BEM_BoundaryValues.hpp:751-779)
+__global__ void k_phit_known(int ndof, const int32_t* __restrict__ dof_point, const int32_t* __restrict__ dof_face,
+                             const int32_t* __restrict__ dof_kind, const int32_t* __restrict__ pf_off, const int32_t* __restrict__ pf_face,
+                             const int32_t* __restrict__ tri, const uint8_t* __restrict__ face_dir, const double* __restrict__ X,
+                             const double* __restrict__ normal, const double* __restrict__ area, const double* __restrict__ u,
+                             const int32_t* __restrict__ face_body, const double* __restrict__ bodies, double gravity,
+                             double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ndof) return;
+  const int p = dof_point[i];
+  if (dof_kind[i] == 0) {
+    const double* up = u + 3 * p;
+    out[i] = -0.5 * v3dot(up, up) - gravity * X[3 * p + 2];
+    return;
+  }
+  const int F = dof_face[i];
+  if (F >= 0) {
+    out[i] = phint_face(p, F, tri, X, normal, u, face_body, bodies);
+    return;
+  }
+  double s = 0.0, w = 0.0;
+  for (int k = pf_off[p]; k < pf_off[p + 1]; ++k) {
+    const int f = pf_face[k];
+    if (face_dir[f]) continue;
+    s += phint_face(p, f, tri, X, normal, u, face_body, bodies) * area[f];
+    w += area[f];
+  }
+  out[i] = w > 0.0 ? s / w : 0.0;
+}
+
 struct bem_gpu_mel {
   int device = 0;
   cudaStream_t stream = nullptr;
   std::string err;
-  MBuf<double> X, normal, area, phi_dof, phin_dof, phi_pt, u, u_node, damping, X0, phi0, accX, accphi, Xout, phiout, dphidt;
-  MBuf<int32_t> tri, face_dof, pf_off, pf_face;
+  MBuf<double> X, normal, area, phi_dof, phin_dof, phi_pt, u, u_node, damping, X0, phi0, accX, accphi, Xout, phiout, dphidt, bodies, known_t;
+  MBuf<int32_t> tri, face_dof, pf_off, pf_face, dof_point, dof_face, dof_kind, face_body;
   MBuf<int8_t> pf_slot;
   MBuf<uint8_t> flags, face_dir;
   ~bem_gpu_mel() {
@@ -416,6 +527,42 @@ int bem_gpu_mel_stage(bem_gpu_mel* m, const bem_mel_surface* s, int32_t stage, d
   MK(cudaMemcpyAsync(out_phi, m->phiout.p, sizeof(double) * np, cudaMemcpyDeviceToHost, m->stream));
   if (out_u) MK(cudaMemcpyAsync(out_u, m->u.p, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost, m->stream));
   if (out_dphidt) MK(cudaMemcpyAsync(out_dphidt, m->dphidt.p, sizeof(double) * np, cudaMemcpyDeviceToHost, m->stream));
+  MK(cudaStreamSynchronize(m->stream));
+  return BEM_OK;
+}
+
+int bem_gpu_mel_phit_known(bem_gpu_mel* m, const bem_mel_surface* s, const int32_t* dof_point, const int32_t* dof_face,
+                           const int32_t* dof_kind, const int32_t* face_body, int32_t n_bodies, const double* bodies, double gravity,
+                           const double* u, double* out_known) {
+  if (!m || !s || !dof_point || !dof_face || !dof_kind || !face_body || n_bodies < 0 || (n_bodies > 0 && !bodies) ||
+      !std::isfinite(gravity) || !out_known)
+    return BEM_ERR_INVALID_ARGUMENT;
+  const int nd = s->n_dof, nf = s->n_faces;
+  for (int i = 0; i < nd; ++i)
+    if (dof_point[i] < 0 || dof_point[i] >= s->n_points || dof_kind[i] < 0 || dof_kind[i] > 2 || dof_face[i] < -1 || dof_face[i] >= nf) {
+      m->err = "invalid DOF table";
+      return BEM_ERR_INVALID_ARGUMENT;
+    }
+  for (int f = 0; f < nf; ++f)
+    if (face_body[f] < -1 || face_body[f] >= n_bodies) {
+      m->err = "face_body out of range";
+      return BEM_ERR_INVALID_ARGUMENT;
+    }
+  int rc = mel_prepare(m, s);
+  if (rc != BEM_OK) return rc;
+  if (u) MK(put(m, m->u, u, 3 * (size_t)s->n_points));  // the caller's velocities replace the computed ones
+  MK(put(m, m->dof_point, dof_point, (size_t)nd));
+  MK(put(m, m->dof_face, dof_face, (size_t)nd));
+  MK(put(m, m->dof_kind, dof_kind, (size_t)nd));
+  MK(put(m, m->face_body, face_body, (size_t)nf));
+  MK(m->bodies.reserve(15 * (size_t)std::max(n_bodies, 1)));
+  if (n_bodies > 0) MK(cudaMemcpyAsync(m->bodies.p, bodies, sizeof(double) * 15 * n_bodies, cudaMemcpyHostToDevice, m->stream));
+  MK(m->known_t.reserve((size_t)nd));
+  k_phit_known<<<(nd + 255) / 256, 256, 0, m->stream>>>(nd, m->dof_point.p, m->dof_face.p, m->dof_kind.p, m->pf_off.p, m->pf_face.p, m->tri.p,
+                                                         m->face_dir.p, m->X.p, m->normal.p, m->area.p, m->u.p, m->face_body.p,
+                                                         m->bodies.p, gravity, m->known_t.p);
+  MK(cudaGetLastError());
+  MK(cudaMemcpyAsync(out_known, m->known_t.p, sizeof(double) * nd, cudaMemcpyDeviceToHost, m->stream));
   MK(cudaStreamSynchronize(m->stream));
   return BEM_OK;
 }

@@ -315,6 +315,25 @@ int bem_gpu_mel_velocity(bem_gpu_mel* mel, const bem_mel_surface* s, double* out
 int bem_gpu_mel_stage(bem_gpu_mel* mel, const bem_mel_surface* s, int32_t stage, double dt, double gravity, const double* u_node,
                       const double* damping, double* rk_X0, double* rk_phi0, double* rk_accX, double* rk_accphi, double* out_X,
                       double* out_phi, double* out_u, double* out_dphidt);
+/* Known values of the phi_t boundary-value problem that a floating-body step solves with the
+ * same operator (setPhiPhin_t, bem/BEM_setBoundaryTypes.hpp:858-935), per DOF of the table
+ * (dof_point / dof_face / dof_kind as bem_gpu_build_dofs):
+ *   Dirichlet DOF: phi_t = -|u|^2/2 - gravity z (aphiat(0), lib/include/Network.hpp:971-976);
+ *   Neumann DOF on face F: phin_t = 0 on a face of no body (face_body[F] = -1), else, for the
+ *     rigid body b = face_body[F] with bodies[15 b ..] = centre (3), velocity (3), angular
+ *     velocity (3), acceleration (3), angular acceleration (3) (RigidBodyDynamics.hpp:84-89),
+ *     phint_Neumann(p, F) (bem/BEM_BoundaryValues.hpp:701-728): n.a + (Omega x n).(v - u)
+ *     - (B v).H0 with the body's velocity v and acceleration a at the point, the face basis
+ *     B = {n, s0, s1} (OrthogonalBasis, :307-315) and H0 the first row of HessianOfPhi (:653-672);
+ *   Neumann point DOF (dof_face -1): the area-weighted mean over the point's Neumann faces
+ *     (phint_Neumann(p), :751-779).
+ * u: point velocities [3 n_points], NULL to compute them from the surface's solution as
+ * bem_gpu_mel_velocity does.  Physical units; out_known [n_dof] is the `known` argument of the
+ * phi_t solve (bem_gpu_solve on the same set-up): its result is phin_t on Dirichlet DOFs and
+ * phi_t on the others. */
+int bem_gpu_mel_phit_known(bem_gpu_mel* mel, const bem_mel_surface* s, const int32_t* dof_point, const int32_t* dof_face,
+                           const int32_t* dof_kind, const int32_t* face_body, int32_t n_bodies, const double* bodies, double gravity,
+                           const double* u, double* out_known);
 
 /* Mixed precision (context set up with opts.precision = 1).  No reference counterpart: the
  * reference's M2L is FP64 only (lib/include/moments.hpp:732-764).
