@@ -1706,7 +1706,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
   // Mixed precision is iterative refinement: each GMRES cycle solves A_lo d = r to
   // max(tol, kInnerRtol |r|) and the cycle ends with the FP64 true residual, from which the
   // next cycle starts (that residual is reused, not recomputed).
-  const double kInnerRtol = ctx->opts.refine_rtol > 0.0 ? ctx->opts.refine_rtol : 1e-5;
+  const double kInnerRtol = ctx->opts.refine_rtol > 0.0 ? ctx->opts.refine_rtol : 1e-6;
   bool have_res = false;
   auto norm_of = [&](const double* v, double* out) -> int {
     launch_mdot(v, N, 1, v, N, ctx->partial.p, ctx->hdev.p, s);

@@ -72,7 +72,7 @@ typedef struct {
   int32_t overlap_near;      /* mixed: 1 = the near field of A.x runs on a second stream while the FMM
                                 passes run, its far part added after; 0 = one fused kernel after them */
   double refine_rtol;        /* mixed: each inner GMRES cycle on the low-precision operator stops at
-                                max(tol, refine_rtol * |r|) before the FP64 residual update (0: 1e-5) */
+                                max(tol, refine_rtol * |r|) before the FP64 residual update (0: 1e-6) */
   int32_t tc_deterministic;  /* mixed: 0 = the tensor-core M2L adds each pair's translated expansion into
                                 its target's FP32 accumulator in L2 (fast; the summation order, and so the
                                 last bits, vary between runs); 1 = per-pair partials summed in a fixed
