@@ -180,7 +180,8 @@ __device__ __forceinline__ void decode_nm(int t, int& n, int& m) {
 //                W_k N_a(k) conj(F(y_k - c))      (Dirichlet DOF: phin = x_d)
 //             or -W_k N_a(k) conj(nu . grad F)    (otherwise: phi = x_d)
 // so each A.x computes M_leaf = sum_d x_d C_{leaf,d}: one pass over C (a few bytes per
-// source point) instead of the harmonics of every P2M point.  k_p2m_op builds C at set-up:
+// source point) instead of the harmonics of every P2M point (k_p2m_leaf, with the leaf's first
+// M2M shift).  k_p2m_op builds C at set-up:
 // block per leaf, four points at a time (a warp fills the F table of one point), thread per
 // coefficient adding the points in order into its own entries of C (deterministic).
 template <int P>
@@ -246,24 +247,6 @@ __global__ void __launch_bounds__(128) k_p2m_op(const int* __restrict__ leaves, 
 }
 
 // M_leaf[0] = sum_d x_d C_{leaf,d} (block per leaf, thread per coefficient)
-template <int P>
-__global__ void k_p2m_apply(const int* __restrict__ leaves, const int* __restrict__ leaf_dof_off, const int* __restrict__ leaf_dof,
-                            const double2* __restrict__ C, const double* __restrict__ x, double2* __restrict__ M) {
-  pdl_enter();
-  constexpr int NC = ncoef(P);
-  const int li = blockIdx.x, leaf = leaves[li];
-  const int t = threadIdx.x;
-  if (t >= NC) return;
-  const int d0 = leaf_dof_off[li], d1 = leaf_dof_off[li + 1];
-  double2 acc = make_double2(0.0, 0.0);
-  for (int j = d0; j < d1; ++j) {
-    const double xv = x[leaf_dof[j]];
-    const double2 c = C[(size_t)j * NC + t];
-    acc.x = fma(xv, c.x, acc.x);
-    acc.y = fma(xv, c.y, acc.y);
-  }
-  M[(size_t)leaf * 2 * NC + t] = acc;
-}
 
 // ---------------------------------------------------------------------------
 // Parent-to-child translation tables.  A child bucket sits at one of eight offsets from its
@@ -1288,7 +1271,6 @@ int launch_targets_ax(const MatvecArgs& a, cudaStream_t st, const double2* L) {
 template <int P, int ND>
 int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
   constexpr int NC = ncoef(P);
-  constexpr int tpb_coef = ((NC + 31) / 32) * 32;
   int launches = 0;
   // overlap: the near-field part of the rows (HBM-bound) runs on the side stream while the FMM
   // passes run here; the far-field part is added once both are done
@@ -1307,9 +1289,7 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
     launch_pdl(k_p2m_leaf<P>, a.n_leaves, tree_threads<P>(), 0, st, a.leaves, a.leaf_dof_off, a.leaf_dof, a.p2m_C, a.ax, a.node_up,
                a.leaf_level, a.node_X, a.Ftab, a.M, a.Yup);
     ++launches;
-  } else if ((stages & STAGE_P2M) && a.n_leaves > 0 && ND == 1 && a.ax && a.p2m_C) {
-    launch_pdl(k_p2m_apply<P>, a.n_leaves, tpb_coef, 0, st, a.leaves, a.leaf_dof_off, a.leaf_dof, a.p2m_C, a.ax, a.M);
-    ++launches;
+
   } else if ((stages & STAGE_P2M) && a.n_leaves > 0) {
     k_p2m<P, ND><<<a.n_leaves, 128, 0, st>>>(a.leaves, a.node_fb, a.node_fe, a.node_X, a.e_q, a.e_W, a.e_n, a.e_dof, a.phi, a.phin, a.M);
     ++launches;
