@@ -980,11 +980,12 @@ __device__ void elem_weights3(int s, int t, const double* __restrict__ Xs, const
       const double nr_inv = rsqrt(Rx * Rx + Ry * Ry + Rz * Rz);
       const double base = ww * (1. - t0) * nr_inv;
       const double dn = -((Rx * crx + Ry * cry + Rz * crz) * nr_inv);
+      const double bn = dn * base * nr_inv;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        const double tmp = base * N[(a - o + 3) % 3];
-        G[a] += J * tmp;
-        Gn[a] += dn * tmp * nr_inv;
+        const double Na = N[(a - o + 3) % 3];
+        G[a] += base * Na;  // times J after the loop
+        Gn[a] += bn * Na;
       }
     }
     Gn[0] = 0.0;  // the element's first vertex: dropped (rigid-mode diagonal)
@@ -1001,13 +1002,13 @@ __device__ void elem_weights3(int s, int t, const double* __restrict__ Xs, const
         const double Ry = N[0] * X0[1] + N[1] * X1[1] + N[2] * X2[1] - yt;
         const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
         const double nr_inv = rsqrt(Rx * Rx + Ry * Ry + Rz * Rz);
-        const double wt = ww * (1. - t0);
+        const double sw = ww * (1. - t0) * nr_inv;
         const double dn = (Rx * crx + Ry * cry + Rz * crz) * nr_inv;
+        const double tw = dn * sw * nr_inv;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          const double tmp = wt * N[a] * nr_inv;
-          G[a] += J * tmp;
-          Gn[a] -= dn * (tmp * nr_inv);
+          G[a] += sw * N[a];  // times J after the loop
+          Gn[a] -= tw * N[a];
         }
       }
     } else {
@@ -1018,18 +1019,18 @@ __device__ void elem_weights3(int s, int t, const double* __restrict__ Xs, const
         const double Rz = N[0] * X0[2] + N[1] * X1[2] + N[2] * X2[2] - zt;
         const double nr_inv = rsqrt(Rx * Rx + Ry * Ry + Rz * Rz);
         const double dn = (Rx * crx + Ry * cry + Rz * crz) * nr_inv;
+        const double sw = c_dv[q][3] * nr_inv, tw = dn * sw * nr_inv;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          const double tmp = c_dv[q][3] * N[a] * nr_inv;
-          G[a] += J * tmp;
-          Gn[a] -= dn * (tmp * nr_inv);
+          G[a] += sw * N[a];  // times J after the loop
+          Gn[a] -= tw * N[a];
         }
       }
     }
   }
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    wG[a] = G[a];
+    wG[a] = J * G[a];  // every rule's single-layer sum carries the factor J once
     wGn[a] = Gn[a];
   }
 }
@@ -1042,7 +1043,7 @@ __device__ void elem_weights3(int s, int t, const double* __restrict__ Xs, const
 // (target, element) instead of one per (target, DOF, element).
 constexpr int kNearThreads = 256;
 
-__global__ void __launch_bounds__(kNearThreads) k_near_weights(int nslots, const NearBlockDev* __restrict__ blocks,
+__global__ void __launch_bounds__(kNearThreads, 3) k_near_weights(int nslots, const NearBlockDev* __restrict__ blocks,
                                                               const int* __restrict__ slot_block, const int* __restrict__ nb_dofs,
                                                               const int* __restrict__ nb_targets, const int* __restrict__ nb_ranges,
                                                               const int* __restrict__ dof_inc_off, const int* __restrict__ dof_inc,
