@@ -40,7 +40,7 @@ def build_dofs(X, tri, face_dirichlet):
 
 
 def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_level, solver_tol, solver_max_iter, device,
-               tol_relative, preconditioner, precision, poly_degree=8, tree_on_device=True, tc_item_pairs=0, overlap_near=False,
+               tol_relative, preconditioner, precision, poly_degree=8, tree_on_device=True, tc_item_pairs=0, overlap_near=True,
                refine_rtol=0.0, tc_deterministic=False):
     o = L.Opts()
     lib.bem_gpu_default_opts(ctypes.byref(o))
@@ -68,7 +68,7 @@ class BEM_BVP:
 
     def __init__(self, X, tri, face_dirichlet, *, expansion_order=10, mac_theta=0.25, fmm_bucket_max_points=30,
                  fmm_max_level=7, solver_tol=1e-9, solver_max_iter=500, device=0, dofs=None, tol_relative=False, preconditioner="none",
-                 precision="fp64", poly_degree=8, tree_on_device=True, tc_item_pairs=0, overlap_near=False, refine_rtol=0.0,
+                 precision="fp64", poly_degree=8, tree_on_device=True, tc_item_pairs=0, overlap_near=True, refine_rtol=0.0,
                  tc_deterministic=False):
         self.lib = L.load()
         if not self.lib.bem_gpu_is_available():

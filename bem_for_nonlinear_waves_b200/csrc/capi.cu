@@ -562,6 +562,7 @@ void bem_gpu_default_opts(bem_gpu_opts* o) {
   o->tol = 1e-9;
   o->max_iter = 500;
   o->device = 0;
+  o->overlap_near = 1;
 }
 
 bem_gpu_ctx* bem_gpu_create(const bem_gpu_opts* opts) {

@@ -599,7 +599,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "none", "near_poly"])
     ap.add_argument("--poly-degree", type=int, default=8, help="degree of the near_poly preconditioner")
-    ap.add_argument("--overlap-near", type=int, default=0, help="1: near field of the mixed A.x on a second stream")
+    ap.add_argument("--overlap-near", type=int, default=1, help="1: near field of the mixed A.x on a second stream (0: after the FMM passes)")
     ap.add_argument("--max-iter", type=int, default=1500)
     ap.add_argument("--refine-rtol", type=float, default=0.0, help="mixed: inner-cycle relative tolerance (0: library default)")
     ap.add_argument("--tc-deterministic", type=int, default=0,
