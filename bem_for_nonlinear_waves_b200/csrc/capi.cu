@@ -315,6 +315,11 @@ struct bem_gpu_ctx {
     a.p2m_C = p2m_C.p;
     a.Wc = lowp ? nullptr : Wc.p;
     a.Wc32 = lowp ? Wc32.p : nullptr;
+    if (opts.overlap_near == 1) {  // near-field sums on the side stream, concurrent with the FMM passes
+      a.side = side;
+      a.ev_fork = ev_fork;
+      a.ev_join = ev_join;
+    }
   }
   // the near-field part of A.x (FP32 weights where built): mv_in -> mv_out
   MatvecArgs near_args() const {
@@ -333,11 +338,6 @@ struct bem_gpu_ctx {
     a.tc_pos = tc_pos.p;
     a.n_tc_pairs = (int)plan.tc_pair.size();
     a.tc_item_pairs = tc_tune > 0 ? tc_tune : 80;
-    if (opts.overlap_near == 1) {  // near field on the side stream, concurrent with the FMM passes
-      a.side = side;
-      a.ev_fork = ev_fork;
-      a.ev_join = ev_join;
-    }
     a.tc_src = tc_src.p;
     a.tc_tab = tc_T.p;
     a.tc_Mt = tc_Mt.p;

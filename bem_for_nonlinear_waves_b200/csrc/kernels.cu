@@ -1275,7 +1275,7 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
   int launches = 0;
   // overlap: the near-field part of the rows (HBM-bound) runs on the side stream while the FMM
   // passes run here; the far-field part is added once both are done
-  const bool overlap = stages == STAGE_ALL && ND == 1 && a.side && a.ev_fork && a.ev_join && a.Wc32 && a.ax && a.n_blocks > 0;
+  const bool overlap = stages == STAGE_ALL && ND == 1 && a.side && a.ev_fork && a.ev_join && (a.Wc32 || a.Wc) && a.ax && a.n_blocks > 0;
   if (overlap) {
     cudaEventRecord(a.ev_fork, st);
     cudaStreamWaitEvent(a.side, a.ev_fork, 0);

@@ -69,7 +69,7 @@ typedef struct {
   int32_t tc_item_pairs;     /* mixed: pairs per tensor-core M2L work item, 1..128 (p <= 10) or 1..80;
                                 0: autotuned (once per process and problem class; the result does not
                                 depend on it) */
-  int32_t overlap_near;      /* mixed: 1 (bem_gpu_default_opts) = the near-field sums of A.x run on a
+  int32_t overlap_near;      /* 1 (bem_gpu_default_opts) = the near-field sums of A.x run on a
                                 second stream while the FMM passes run, the rows after both; 0 = the
                                 near sums after the FMM passes on one stream */
   double refine_rtol;        /* mixed: each inner GMRES cycle on the low-precision operator stops at
