@@ -204,8 +204,8 @@ class BEM_BVP:
         d = {k: float(v) for k, v in zip(keys, out)}
         d["tree_on_device"] = bool(int(out[9]) & 1)
         d["lists_on_device"] = bool(int(out[9]) & 2)
-        up = ["upload_nodes", "upload_blocks", "upload_tc_items", "upload_p2m_lists", "upload_rest", "upload_wait"]
-        d.update({k: float(v) for k, v in zip(up, out[10:16])})
+        up = ["upload_nodes", "upload_blocks", "upload_tc_items", "upload_p2m_lists", "upload_rest"]
+        d.update({k: float(v) for k, v in zip(up, out[10:15])})
         return d
 
     def poly_roots(self):

@@ -152,6 +152,7 @@ struct bem_gpu_ctx {
   DBuf<int2> l2l_pairs{&dev_bytes};
   DBuf<int> blk_path_off{&dev_bytes}, blk_path{&dev_bytes};  // near block -> its bucket's M2L-target path
   int max_path = 0;
+  std::vector<int> h_tc_src, h_tc_pos, h_tc_tgt;  // host staging of the tensor-core work-item arrays
   std::vector<int> m2m_level_off, m2m_level_off_nl, l2l_level_off;
   int n_tree_levels = 0;
   DBuf<int> m2l_targets{&dev_bytes}, m2l_off{&dev_bytes}, m2l_src{&dev_bytes}, nb_dofs{&dev_bytes}, nb_targets{&dev_bytes}, nb_ranges{&dev_bytes}, dof_inc_off{&dev_bytes}, dof_inc{&dev_bytes};
@@ -216,9 +217,9 @@ struct bem_gpu_ctx {
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   float setup_dev_ms = 0.f;
   double time_plan = 0.0, time_upload = 0.0;
-  // the upload part of the set-up by step: [0] node and level arrays, [1] near blocks and
-  // element/tree arrays, [2] tensor-core items, [3] P2M operator lists, [4] remaining arrays,
-  // [5] waiting for the copies
+  // the upload part of the set-up by step (host time; the copies are asynchronous): [0] node and
+  // level arrays, [1] near blocks and element/tree arrays, [2] tensor-core items, [3] P2M operator
+  // lists, [4] remaining arrays, [5] unused (0)
   double upload_part_s[6] = {0, 0, 0, 0, 0, 0};
 
   DeviceTree* dtree = nullptr;  // octree growth on the device (set-up)
@@ -1147,7 +1148,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     CK(upload_tc_items(ctx, reuse));
     {  // work-item order j -> source bucket and compact target index; pair slot k -> its position j
        // (the row of its partial)
-      std::vector<int> src, pos, tgt;
+      std::vector<int>&src = ctx->h_tc_src, &pos = ctx->h_tc_pos, &tgt = ctx->h_tc_tgt;  // kept across set-ups
       tc_item_arrays(P, src, pos, tgt);
       CK(ups(ctx->tc_src, src));
       CK(ups(ctx->tc_pos, pos));
@@ -1228,8 +1229,8 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     CK(ctx->dinv.alloc(N));
   }
   part_done(4);
-  CK(cudaStreamSynchronize(s));
-  part_done(5);
+  // no wait here: the device part follows the copies (and the near-field quadrature) in stream
+  // order, and its events time only device work
   ctx->time_upload = now_s() - t0 - ctx->time_plan;
   ctx->stage_bytes = std::max(ctx->stage_bytes, ctx->stage.used);
   // device part of the set-up starts here (inputs resident): every kernel that derives the

@@ -605,7 +605,7 @@ bool build_m2l_groups(Plan& P) {
     P.error = "too many M2L pairs";
     return false;
   }
-  std::vector<int> pair_tgt;
+  std::vector<int>& pair_tgt = P.scratch_pair_tgt;
   pair_targets(P, pair_tgt);
   std::vector<uint64_t>& keyed = P.m2l_key_sorted;
   keyed.resize(npair);
@@ -682,6 +682,9 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   fresh.v.clear();
     BEMB200_PLAN_ARRAYS(BEMB200_KEEP)
 #undef BEMB200_KEEP
+    fresh.src_scratch = std::move(P.src_scratch);  // kept with their sizes
+    fresh.scratch_pair_tgt = std::move(P.scratch_pair_tgt);
+    fresh.scratch_slot_tgt = std::move(P.scratch_slot_tgt);
     P = std::move(fresh);
   }
   P.opt = opt;
@@ -769,8 +772,15 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
 
   // element sources (BEM_solveBVP_GMRES_FMM.hpp:1799-1937)
   auto XP = [&](int i) { return V3{P.Xs[3 * i], P.Xs[3 * i + 1], P.Xs[3 * i + 2]}; };
-  std::vector<V3> pole(nf);
-  std::vector<double> q(nf * 18), W(nf * 6), en(nf * 3), enear(nf * 8), offs(nf);
+  Plan::SourceScratch& S = P.src_scratch;
+  S.pole.resize(nf);
+  S.q.resize(nf * 18);
+  S.W.resize(nf * 6);
+  S.en.resize(nf * 3);
+  S.enear.resize(nf * 8);
+  S.offs.resize(nf);
+  std::vector<V3>& pole = S.pole;
+  std::vector<double>&q = S.q, &W = S.W, &en = S.en, &enear = S.enear, &offs = S.offs;
 #pragma omp parallel for schedule(static)
   for (int f = 0; f < nf; ++f) {
     const V3 a = XP(tri[3 * f]), b = XP(tri[3 * f + 1]), c = XP(tri[3 * f + 2]);
@@ -1242,7 +1252,7 @@ void build_tc_groups(Plan& P, int max_pairs) {
   const int64_t npair = (int64_t)P.m2l_key_sorted.size();
   const std::vector<uint64_t>& keyed = P.m2l_key_sorted;
   const uint64_t kmask = (uint64_t(1) << 29) - 1;
-  std::vector<int> pair_tgt;
+  std::vector<int>& pair_tgt = P.scratch_pair_tgt;
   pair_targets(P, pair_tgt);
   std::vector<int64_t> rs;
   parallel_heads(
@@ -1283,12 +1293,13 @@ void build_tc_groups(Plan& P, int max_pairs) {
   }
 }
 
-void tc_item_arrays(const Plan& P, std::vector<int>& src, std::vector<int>& pos, std::vector<int>& tgt) {
+void tc_item_arrays(Plan& P, std::vector<int>& src, std::vector<int>& pos, std::vector<int>& tgt) {
   const size_t n = P.tc_pair.size();
   src.resize(n);
   pos.resize(n);
   tgt.resize(n);
-  std::vector<int> tgt_of_slot((size_t)P.m2l_pairs);
+  std::vector<int32_t>& tgt_of_slot = P.scratch_slot_tgt;
+  tgt_of_slot.resize((size_t)P.m2l_pairs);
   const int nt = (int)P.m2l_targets.size();
 #pragma omp parallel for schedule(static)
   for (int ti = 0; ti < nt; ++ti) {

@@ -115,6 +115,14 @@ struct Plan {
   std::vector<int32_t> dof_inc_off, dof_inc;  // dof_inc = pos*3 + slot
 
   double phase_s[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // host set-up phase timings
+  // per-face source data by face id before the element order is known (scratch kept across
+  // set-ups with its size: a set-up of the same mesh writes it without new pages or clearing)
+  struct SourceScratch {
+    std::vector<std::array<double, 3>> pole;
+    std::vector<double> q, W, en, enear, offs;
+  } src_scratch;
+  // scratch of the M2L grouping and of the tensor-core item arrays, kept the same way
+  std::vector<int32_t> scratch_pair_tgt, scratch_slot_tgt;
 
   // root bucket (centre, half-width) the tree was grown in; a refresh keeps it
   double root_C[3] = {0, 0, 0}, root_R = 0.0;
@@ -161,7 +169,7 @@ void parallel_copy(void* dst, const void* src, size_t bytes);
 void build_tc_groups(Plan& plan, int max_pairs);
 // per tensor-core pair (work-item order j): its source bucket and compact target index (into
 // m2l_targets); per pair slot k: its position j
-void tc_item_arrays(const Plan& plan, std::vector<int>& src, std::vector<int>& pos, std::vector<int>& tgt);
+void tc_item_arrays(Plan& plan, std::vector<int>& src, std::vector<int>& pos, std::vector<int>& tgt);
 // Re-splits the tensor-core work items of build_tc_groups into items of <= max_pairs pairs
 // (tables and pair order unchanged).
 void retile_tc_items(Plan& plan, int max_pairs);
