@@ -683,6 +683,11 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     BEMB200_PLAN_ARRAYS(BEMB200_KEEP)
 #undef BEMB200_KEEP
     fresh.src_scratch = std::move(P.src_scratch);  // kept with their sizes
+    // per-element source arrays: resized and overwritten in full, so kept with their sizes too
+    fresh.e_q.swap(P.e_q);
+    fresh.e_W.swap(P.e_W);
+    fresh.e_n.swap(P.e_n);
+    fresh.e_near.swap(P.e_near);
     fresh.scratch_pair_tgt = std::move(P.scratch_pair_tgt);
     fresh.scratch_slot_tgt = std::move(P.scratch_slot_tgt);
     P = std::move(fresh);

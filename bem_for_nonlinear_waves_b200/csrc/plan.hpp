@@ -138,7 +138,7 @@ struct Plan {
 };
 
 // every array member of Plan (build_plan reuses their capacity from the plan it overwrites)
-#define BEMB200_PLAN_ARRAYS(X) X(Xs) X(dof_point) X(dof_face) X(dof_kind) X(face_dof) X(point_dof_off) X(point_dof) X(corner_src_dof) X(face_of_pos) X(pos_of_face) X(owner_of_pos) X(e_q) X(e_W) X(e_n) X(e_dof) X(e_vtx) X(e_near) X(nodes) X(node_children) X(level_nodes) X(leaves) X(m2l_off) X(m2l_src) X(near_off) X(near_nodes) X(grp_vec) X(grp_off) X(grp_pair) X(chunk_grp) X(chunk_begin) X(chunk_cnt) X(m2l_targets) X(m2l_key_sorted) X(tc_tab) X(tc_pair) X(tc_item_tab) X(tc_item_begin) X(tc_item_cnt) X(target_box) X(blocks) X(nb_dofs) X(nb_targets) X(nb_ranges) X(block_of_point) X(row_of_point) X(self_col) X(dof_inc_off) X(dof_inc)
+#define BEMB200_PLAN_ARRAYS(X) X(Xs) X(dof_point) X(dof_face) X(dof_kind) X(face_dof) X(point_dof_off) X(point_dof) X(corner_src_dof) X(face_of_pos) X(pos_of_face) X(owner_of_pos) X(e_dof) X(e_vtx) X(nodes) X(node_children) X(level_nodes) X(leaves) X(m2l_off) X(m2l_src) X(near_off) X(near_nodes) X(grp_vec) X(grp_off) X(grp_pair) X(chunk_grp) X(chunk_begin) X(chunk_cnt) X(m2l_targets) X(m2l_key_sorted) X(tc_tab) X(tc_pair) X(tc_item_tab) X(tc_item_begin) X(tc_item_cnt) X(target_box) X(blocks) X(nb_dofs) X(nb_targets) X(nb_ranges) X(block_of_point) X(row_of_point) X(self_col) X(dof_inc_off) X(dof_inc)
 
 // Fills dof tables from face flags with the reference's key rules; returns n_dof or -1.
 int build_dofs(int np, const double* X, int nf, const int32_t* tri, const uint8_t* fdir, int32_t* dof_point, int32_t* dof_face,
