@@ -688,6 +688,8 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
     fresh.e_W.swap(P.e_W);
     fresh.e_n.swap(P.e_n);
     fresh.e_near.swap(P.e_near);
+    fresh.scratch_blk_dofs.swap(P.scratch_blk_dofs);
+    fresh.scratch_blk_rng.swap(P.scratch_blk_rng);
     fresh.scratch_pair_tgt = std::move(P.scratch_pair_tgt);
     fresh.scratch_slot_tgt = std::move(P.scratch_slot_tgt);
     P = std::move(fresh);
@@ -1140,14 +1142,34 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
   P.nb_targets.clear();
   P.nb_ranges.clear();
   const int nblk = (int)P.blocks.size();
-  std::vector<std::vector<int>> blk_rng(nblk), blk_dofs(nblk);
-#pragma omp parallel
+  // each thread appends its blocks' merged element ranges and DOF lists to buffers of its own
+  // (kept across set-ups), then every block is copied to its place
+  struct BlkRec {
+    int th;
+    int nd, nr;
+    int64_t d0, r0;
+  };
+  std::vector<BlkRec> rec(nblk);
+  const int nthr = std::max(1, omp_get_max_threads());
+  if ((int)P.scratch_blk_dofs.size() < nthr) {
+    P.scratch_blk_dofs.resize(nthr);
+    P.scratch_blk_rng.resize(nthr);
+  }
+#pragma omp parallel num_threads(nthr)
   {
+    const int th = omp_get_thread_num();
+    // the buffers on this thread's stack while it appends (their headers would otherwise share
+    // cache lines between threads), back in the plan afterwards
+    std::vector<int32_t> bd = std::move(P.scratch_blk_dofs[th]), br = std::move(P.scratch_blk_rng[th]);
+    bd.clear();
+    br.clear();
     std::vector<int> mark(ndof, -1);
+    std::vector<std::pair<int, int>> rng, merged;
 #pragma omp for schedule(dynamic, 8)
     for (int bi = 0; bi < nblk; ++bi) {
       const int t = P.blocks[bi].node;
-      std::vector<std::pair<int, int>> rng;
+      rng.clear();
+      merged.clear();
       auto addr = [&](int n) {
         if (P.nodes[n].fe > P.nodes[n].fb) rng.push_back({P.nodes[n].fb, P.nodes[n].fe});
       };
@@ -1157,37 +1179,43 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
         for (int n : B[a].near)
           if (B[n].kids.empty()) addr(n);
       std::sort(rng.begin(), rng.end());
-      std::vector<std::pair<int, int>> merged;
       for (auto& r : rng) {
         if (!merged.empty() && r.first <= merged.back().second)
           merged.back().second = std::max(merged.back().second, r.second);
         else
           merged.push_back(r);
       }
-      std::vector<int>& dl = blk_dofs[bi];
+      BlkRec& R = rec[bi];
+      R.th = th;
+      R.d0 = (int64_t)bd.size();
+      R.r0 = (int64_t)br.size();
       for (auto& r : merged) {
-        blk_rng[bi].push_back(r.first);
-        blk_rng[bi].push_back(r.second);
+        br.push_back(r.first);
+        br.push_back(r.second);
         for (int s = r.first; s < r.second; ++s)
           for (int a = 0; a < 3; ++a) {
             const int d = P.e_dof[s * 3 + a];
             if (mark[d] != bi) {
               mark[d] = bi;
-              dl.push_back(d);
+              bd.push_back(d);
             }
           }
       }
+      R.nd = (int)((int64_t)bd.size() - R.d0);
+      R.nr = (int)(((int64_t)br.size() - R.r0) / 2);
     }
+    P.scratch_blk_dofs[th] = std::move(bd);
+    P.scratch_blk_rng[th] = std::move(br);
   }
   // offsets first, then one parallel copy into arrays sized once
   int64_t woff = 0, roff = 0, doff = 0, toff = 0;
   for (int bi = 0; bi < nblk; ++bi) {
     Plan::NearBlock& nbk = P.blocks[bi];
     nbk.rng_off = (int)(roff / 2);
-    nbk.nrng = (int)blk_rng[bi].size() / 2;
-    roff += (int64_t)blk_rng[bi].size();
+    nbk.nrng = rec[bi].nr;
+    roff += 2 * (int64_t)rec[bi].nr;
     nbk.dof_off = (int)doff;
-    nbk.ndof = (int)blk_dofs[bi].size();
+    nbk.ndof = rec[bi].nd;
     doff += nbk.ndof;
     nbk.tgt_off = (int)toff;
     nbk.ntgt = (int)btargets[bi].size();
@@ -1201,8 +1229,11 @@ bool build_plan(Plan& P, const PlanOptions& opt, int np, const double* X, int nf
 #pragma omp parallel for schedule(dynamic, 16)
   for (int bi = 0; bi < nblk; ++bi) {
     const Plan::NearBlock& nbk = P.blocks[bi];
-    std::copy(blk_rng[bi].begin(), blk_rng[bi].end(), P.nb_ranges.begin() + 2 * (int64_t)nbk.rng_off);
-    std::copy(blk_dofs[bi].begin(), blk_dofs[bi].end(), P.nb_dofs.begin() + nbk.dof_off);
+    const BlkRec& R = rec[bi];
+    const std::vector<int32_t>& bd = P.scratch_blk_dofs[R.th];
+    const std::vector<int32_t>& br = P.scratch_blk_rng[R.th];
+    std::copy(br.begin() + R.r0, br.begin() + R.r0 + 2 * (int64_t)R.nr, P.nb_ranges.begin() + 2 * (int64_t)nbk.rng_off);
+    std::copy(bd.begin() + R.d0, bd.begin() + R.d0 + R.nd, P.nb_dofs.begin() + nbk.dof_off);
     std::copy(btargets[bi].begin(), btargets[bi].end(), P.nb_targets.begin() + nbk.tgt_off);
   }
   P.nnz = woff;

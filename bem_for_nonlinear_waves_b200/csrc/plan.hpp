@@ -123,6 +123,7 @@ struct Plan {
   } src_scratch;
   // scratch of the M2L grouping and of the tensor-core item arrays, kept the same way
   std::vector<int32_t> scratch_pair_tgt, scratch_slot_tgt;
+  std::vector<std::vector<int32_t>> scratch_blk_dofs, scratch_blk_rng;  // per-thread near-block buffers
 
   // root bucket (centre, half-width) the tree was grown in; a refresh keeps it
   double root_C[3] = {0, 0, 0}, root_R = 0.0;
