@@ -246,6 +246,19 @@ int main(int argc, char** argv) {
     for (size_t i = 0; i < Av.size(); ++i) std::fprintf(out, "%.17g\n", Av[i]);
   }
   std::fprintf(out, "L %.17g\n", water->getScaleFactor());
+  // the MEL stage quantities of the solution: point phi (storePhiPhin), the velocity gradPhi
+  // (BEM_BoundaryValues.hpp:565, set as set_u_potential_BEM does, BEM_calculateVelocities.hpp:
+  // 1027-1031) and Dphi/Dt with the node moving with the fluid and zero pressure
+  // (Network.hpp:224-235); physical units
+  {
+    for (auto* p : water->getPoints()) p->u_potential_BEM = gradPhi(p);  // the point loop of set_u_potential_BEM
+    std::vector<std::tuple<int, double, Tddd, double>> mel;
+    for (auto* p : water->getPoints())
+      mel.emplace_back(pid[p], std::get<0>(p->phiphin), p->u_potential_BEM, p->DphiDt(p->u_potential_BEM, 0.));
+    std::sort(mel.begin(), mel.end(), [](const auto& a, const auto& b) { return std::get<0>(a) < std::get<0>(b); });
+    std::fprintf(out, "mel %zu\n", mel.size());
+    for (auto& [pp, ph, u, dd] : mel) std::fprintf(out, "%d %.17g %.17g %.17g %.17g %.17g\n", pp, ph, u[0], u[1], u[2], dd);
+  }
   std::fclose(out);
   return 0;
 }

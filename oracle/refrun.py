@@ -92,6 +92,13 @@ def parse(path, log=""):
                 a = np.array([list(map(float, nxt().split())) for _ in range(m)]) if m else np.zeros((0, 3))
                 rows[t] = (a[:, 0].astype(np.int64), a[:, 1], a[:, 2])
             res["near_rows"] = rows
+        elif key == "mel":
+            n = int(rest[0])
+            a = np.array([list(map(float, nxt().split())) for _ in range(n)]) if n else np.zeros((0, 6))
+            res["mel_point"] = a[:, 0].astype(np.int64)
+            res["mel_phi"] = a[:, 1]
+            res["mel_u"] = a[:, 2:5]
+            res["mel_dphidt"] = a[:, 5]
         elif key == "matvec":
             n = int(rest[0])
             res["matvec"] = np.array([float(nxt()) for _ in range(n)])

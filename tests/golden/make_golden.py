@@ -1,6 +1,8 @@
 """Generates golden fixtures by running the compiled, unmodified reference GMRES-FMM path
 (oracle/_ref/bem_ref_pP, built by oracle/ref/build_ref.sh from the reference sources) on
-small seeded tanks.  Writes tests/golden/<name>.npz.  Needs the reference checkout at
+small seeded tanks: the solve, its intermediates, and the MEL quantities of the solution
+(point phi, the velocity gradPhi and Dphi/Dt of a node moving with the fluid).  Writes
+tests/golden/<name>.npz.  Needs the reference checkout at
 build time only; the fixtures themselves are self-contained.
 
     python tests/golden/make_golden.py
@@ -62,6 +64,7 @@ def make(name, spec):
         sample_points=sample, sample_off=np.array(rows_off), sample_idx=np.concatenate(rows_idx),
         sample_g=np.concatenate(rows_g), sample_gn=np.concatenate(rows_gn),
         time_setup=R["time_setup"], time_solve=R["time_solve"],
+        mel_point=R["mel_point"], mel_phi=R["mel_phi"], mel_u=R["mel_u"], mel_dphidt=R["mel_dphidt"],
     )
     print(name, "ref iters", R["gmres_iter"], "setup", R["time_setup"], "solve", R["time_solve"])
 

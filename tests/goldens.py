@@ -59,3 +59,21 @@ class Golden:
         d = np.zeros(len(perm))
         d[perm] = self.z["diag"]
         return d
+
+    def surface_values(self, dofs):
+        """Per-DOF (phi, phin) of the reference's solution: the known values (the analytic
+        linear Stokes potential the reference run was given) with the solved unknowns."""
+        from bem_for_nonlinear_waves_b200 import known_values, point_normals
+
+        kv = known_values(self.tank, dofs["dof_point"], dofs["dof_face"], dofs["dof_kind"], point_normals(self.tank))
+        sol = self.solution(dofs)
+        dirichlet = dofs["dof_kind"] == 0
+        return np.where(dirichlet, kv, sol), np.where(dirichlet, sol, kv)
+
+    def mel(self):
+        """The reference's MEL quantities of its solution, per point: phi, gradPhi (u) and
+        Dphi/Dt of a node moving with the fluid (0.5 |u|^2 - g z at zero pressure)."""
+        z = self.z
+        n = self.tank.X.shape[0]
+        assert np.array_equal(z["mel_point"], np.arange(n))
+        return z["mel_phi"], z["mel_u"], z["mel_dphidt"]

@@ -3,7 +3,8 @@
 phin, and four RK4 stages chained through moving positions, within 1e-12 relative (the fit's
 3 x 3 solve differs: adjugate on the GPU, pivoted elimination in the oracle).  The linear
 potential's velocity is exact on the GPU too.  Then one RK4 step of the BEM-MEL loop: BVP
-solve, stage update, at the stage positions."""
+solve, stage update, at the stage positions.  Pinned to the compiled reference's gradPhi and
+DphiDt on the golden cases."""
 import os
 import sys
 
@@ -12,6 +13,7 @@ import pytest
 
 sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "oracle"))
 import oracle as O  # noqa: E402
+import goldens  # noqa: E402
 
 from bem_for_nonlinear_waves_b200 import BEM_BVP, MELStage, build_dofs, known_values, make_tank, point_normals  # noqa: E402
 from test_mel_oracle import A, linear_field_surface  # noqa: E402
@@ -88,3 +90,29 @@ def test_mel_rk4_step_with_bvp(product_lib):
     assert np.isfinite(X).all() and np.isfinite(pnext).all()
     top = (d["point_flags"] & 2) != 0
     assert np.abs(X[top] - t.X[top]).max() > 0
+
+
+@pytest.mark.parametrize("name", goldens.names())
+def test_mel_matches_reference(product_lib, name):
+    """The device MEL update against the compiled reference's gradPhi / DphiDt of its own
+    solution (golden fixtures): from the reference's per-DOF solution within 1e-11 of the largest
+    value; and end to end, the device's own FP64 solve of the same problem followed by the device
+    velocity fit, within 1e-8 (the solve agrees to 1e-10, the surface gradient divides by h)."""
+    g = goldens.Golden(name)
+    t = g.tank
+    d = build_dofs(t.X, t.tri, t.face_dirichlet)
+    phi, phin = g.surface_values(d)
+    rphi, ru, rdp = g.mel()
+    m = MELStage(t.X, t.tri, t.face_dirichlet, dofs=d, gravity=t.g)
+    pp, u = m.velocity(t.X, phi, phin)
+    assert np.abs(pp - rphi).max() <= 1e-12 * np.abs(rphi).max()
+    assert np.abs(u - ru).max() <= 1e-11 * np.abs(ru).max()
+    _, _, _, dp = m.stage(0, 1e-3, t.X, phi, phin)
+    pushed = (d["point_flags"] & 1) == 0
+    assert np.abs(dp[pushed] - rdp[pushed]).max() <= 1e-11 * np.abs(rdp).max()
+    kv = known_values(t, d["dof_point"], d["dof_face"], d["dof_kind"], point_normals(t))
+    b = BEM_BVP(t.X, t.tri, t.face_dirichlet, dofs=d, expansion_order=g.p, solver_tol=g.tol, solver_max_iter=1000)
+    b.solve(kv)
+    pp, u = m.velocity(t.X, b.phi, b.phin)
+    assert np.abs(pp - rphi).max() <= 1e-8 * np.abs(rphi).max()
+    assert np.abs(u - ru).max() <= 1e-8 * np.abs(ru).max()
