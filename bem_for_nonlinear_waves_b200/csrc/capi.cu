@@ -1779,9 +1779,10 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     x_zero = false;
     launch_axpby(N, 1.0 / beta, ctx->rdev.p, 0.0, ctx->V.p, s);
     launch_arnoldi_init(ctx->arn_state.p, ctx->arn_g.p, beta, s);
+    launch_arnoldi_prep(N, ctx->V.p, prec != 0 ? ctx->dinv.p : nullptr, ctx->arn_state.p, ctx->mv_in.p, s);
     // x_base: the iterate this cycle's corrections start from
     CK(cudaMemcpyAsync(ctx->xbase.p, ctx->xdev.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
-    ctx->launches += 2;
+    ctx->launches += 3;
     const int cycle_cap = std::min(cols - 2, max_iter - iters);  // steps this cycle may take
     const double check_at = mixed ? std::max(tol, kInnerRtol * beta) : tol * 10.;
     int launched = 0, done = 0, sat = 0;
@@ -1828,6 +1829,9 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
         }
         if (sat++ >= 5) break;
         if (launched >= cycle_cap) break;
+        // the check's operator application overwrote the next step's input: write it again
+        launch_arnoldi_prep(N, ctx->V.p, prec != 0 ? ctx->dinv.p : nullptr, ctx->arn_state.p, ctx->mv_in.p, s);
+        ctx->launches += 1;
         continue;
       }
       if (done >= cycle_cap) {  // basis full or iteration cap: finish the cycle at this iterate

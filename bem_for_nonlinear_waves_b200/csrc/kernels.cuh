@@ -250,8 +250,8 @@ struct ArnoldiArgs {
   double* x = nullptr;            // operator input (the mat-vec's ax)
   double* w = nullptr;            // operator output (the mat-vec's rows)
   MatvecArgs mv;                  // the operator
-  double* h = nullptr;            // [3][cols]: the two Gram-Schmidt passes and |w|^2
-  double* partial = nullptr;      // [arnoldi_dot_blocks(nrow)][cols]
+  double* h = nullptr;            // [3][cols]: the two Gram-Schmidt passes (third column unused)
+  double* partial = nullptr;      // [cols][arnoldi_dot_blocks(nrow)] per-slice partial dots
   double* cs = nullptr;           // [cols] rotations
   double* sn = nullptr;
   double* g = nullptr;            // [cols + 1] rotated right-hand side
@@ -265,9 +265,11 @@ struct ArnoldiArgs {
   double* Z = nullptr;              // [cols][nrow]
 };
 int arnoldi_dot_blocks(int nrow);
-int configure_arnoldi(int cols);  // before capture: shared memory of the Givens step; -1 if cols is too large
+int configure_arnoldi(int cols);  // before capture: shared memory of the orthogonalisation kernels; -1 if cols is too large
 int launch_arnoldi_step(const ArnoldiArgs& a, cudaStream_t st);  // returns kernel launches
 void launch_arnoldi_init(ArnoldiState* state, double* g, double beta, cudaStream_t st);
+// the first operator input of a cycle, x = (dinv .*) V[:, 0] (each step writes the next one's)
+void launch_arnoldi_prep(int nrow, const double* V, const double* dinv, const ArnoldiState* state, double* x, cudaStream_t st);
 void launch_arnoldi_solve_y(const ArnoldiState* state, const double* R, int ldr, const double* g, double* y, cudaStream_t st);
 void launch_arnoldi_update(const double* V, int nrow, int cols, const ArnoldiState* state, const double* y, double* w, cudaStream_t st);
 
