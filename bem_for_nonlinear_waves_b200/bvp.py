@@ -206,6 +206,7 @@ class BEM_BVP:
         d["lists_on_device"] = bool(int(out[9]) & 2)
         up = ["upload_nodes", "upload_blocks", "upload_tc_items", "upload_p2m_lists", "upload_rest"]
         d.update({k: float(v) for k, v in zip(up, out[10:15])})
+        d["device_near_weights"] = float(out[15])
         return d
 
     def poly_roots(self):

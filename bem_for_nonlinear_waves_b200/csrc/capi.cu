@@ -216,6 +216,7 @@ struct bem_gpu_ctx {
   // set-up device window start/end, solve start/end, near-field quadrature start/end
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   float setup_dev_ms = 0.f;
+  float near_weights_ms = 0.f;  // the near-field quadrature's part of setup_dev_ms
   double time_plan = 0.0, time_upload = 0.0;
   // the upload part of the set-up by step (host time; the copies are asynchronous): [0] node and
   // level arrays, [1] near blocks and element/tree arrays, [2] tensor-core items, [3] P2M operator
@@ -684,7 +685,8 @@ int bem_gpu_setup_phases(bem_gpu_ctx* ctx, double* out) {
   out[7] = ctx->time_upload;
   out[8] = 1e-3 * ctx->setup_dev_ms;
   out[9] = (ctx->plan.tree_on_device ? 1 : 0) + (ctx->plan.lists_on_device ? 2 : 0);
-  for (int k = 0; k < 6; ++k) out[10 + k] = ctx->upload_part_s[k];
+  for (int k = 0; k < 5; ++k) out[10 + k] = ctx->upload_part_s[k];
+  out[15] = 1e-3 * ctx->near_weights_ms;
   return BEM_OK;
 }
 
@@ -1312,6 +1314,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     float nw_ms = 0.f;
     CK(cudaEventElapsedTime(&nw_ms, ctx->ev[4], ctx->ev[5]));
     ctx->setup_dev_ms += nw_ms;
+    ctx->near_weights_ms = nw_ms;
   }
   ctx->setup_h2d = ctx->h2d;
   ctx->setup_launches = ctx->launches;

@@ -374,8 +374,8 @@ int bem_gpu_tc_tuning(bem_gpu_ctx* ctx, int32_t* pairs_in_use, int32_t* candidat
  * (host plan), [7] uploads, [8] device set-up; [9] = 1 if the octree was grown on the device
  * + 2 if the lists were built there; [10..15] the host time of the uploads by step: node and
  * level arrays, near blocks and element/tree arrays, tensor-core work items, P2M operator
- * lists, remaining arrays, 0 (the copies are asynchronous; the device part follows them in
- * stream order). */
+ * lists, remaining arrays (the copies are asynchronous; the device part follows them in
+ * stream order); [15] the near-field quadrature's part of [8]. */
 int bem_gpu_setup_phases(bem_gpu_ctx* ctx, double* out /*[16]*/);
 int bem_harmonic_ritz_values(int32_t k, const double* H, int32_t ldh, double* re, double* im);
 
