@@ -143,6 +143,7 @@ struct bem_gpu_ctx {
   DBuf<float> Wc32{&dev_bytes};  // combined near weights of A.x in FP32 (mixed precision, polynomial preconditioner)
   DBuf<int> leaf_dof_off{&dev_bytes}, leaf_dof{&dev_bytes}, e_slot{&dev_bytes}, slot_block{&dev_bytes};  // P2M operator of A.x: DOFs per leaf
   DBuf<double2> p2m_C{&dev_bytes};                       // [(leaf, DOF)][NC]
+  DBuf<float2> p2m_C32{&dev_bytes};                      // its FP32 copy (mixed precision)
   DBuf<double2> near_scratch{&dev_bytes};                // element values of the near-weight kernel
   DBuf<int> e_dof{&dev_bytes}, e_vtx{&dev_bytes}, node_fb{&dev_bytes}, node_fe{&dev_bytes}, leaves{&dev_bytes}, child_begin{&dev_bytes}, child_end{&dev_bytes}, node_children{&dev_bytes};
   // tree passes, one launch per level: upward-pass nodes and the parent each hands its multipole
@@ -315,6 +316,7 @@ struct bem_gpu_ctx {
     a.leaf_dof_off = leaf_dof_off.p;
     a.leaf_dof = leaf_dof.p;
     a.p2m_C = p2m_C.p;
+    a.p2m_C32 = lowp ? p2m_C32.p : nullptr;
     a.Wc = lowp ? nullptr : Wc.p;
     a.Wc32 = lowp ? Wc32.p : nullptr;
     if (opts.overlap_near == 1) {  // near-field sums on the side stream, concurrent with the FMM passes
@@ -1196,6 +1198,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     CK(ups(ctx->leaf_dof, ld));
     CK(ups(ctx->e_slot, es));
     CK(ctx->p2m_C.alloc(std::max<size_t>(ld.size(), 1) * NC));
+    if (ctx->mixed) CK(ctx->p2m_C32.alloc(std::max<size_t>(ld.size(), 1) * NC));
   }
   part_done(3);
   CK(ctx->M.alloc((size_t)nb * 2 * NC));
@@ -1262,6 +1265,10 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     ctx->set_ax(pa, false);
     launch_p2m_op(P.opt.p, pa, ctx->e_slot.p, s);
     ctx->launches += 1;
+    if (ctx->mixed) {
+      launch_to_float2(ctx->p2m_C.n, ctx->p2m_C.p, ctx->p2m_C32.p, s);
+      ctx->launches += 1;
+    }
   }
   launch_combine_weights((int)P.blocks.size(), ctx->blocks.p, ctx->nb_dofs.p, ctx->dof_kind.p, ctx->WG.p, ctx->WGn.p, ctx->Wc.p,
                          want_w32 ? ctx->Wc32.p : nullptr, s);

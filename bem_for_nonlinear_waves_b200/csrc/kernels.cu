@@ -419,9 +419,15 @@ __global__ void __launch_bounds__(tree_threads<P>(), 5) k_m2m_level(const int* _
 // sums added by shuffles in a fixed order) and, when its parent's multipole is needed, shifts
 // it to the parent's centre into Yup (the same shift as k_m2m_level), so the upward pass
 // starts at the leaves' parents.  Fl: the F tables of every level, leaf_level: each leaf's level.
-template <int P>
+template <typename CT>
+__device__ __forceinline__ double2 load_c2(const CT* c) {
+  const CT v = *c;
+  return make_double2((double)v.x, (double)v.y);
+}
+
+template <int P, typename CT>
 __global__ void __launch_bounds__(tree_threads<P>(), 5) k_p2m_leaf(const int* __restrict__ leaves, const int* __restrict__ leaf_dof_off,
-                                                                   const int* __restrict__ leaf_dof, const double2* __restrict__ C,
+                                                                   const int* __restrict__ leaf_dof, const CT* __restrict__ C,
                                                                    const double* __restrict__ x, const int* __restrict__ node_up,
                                                                    const int* __restrict__ leaf_level, const double* __restrict__ node_X,
                                                                    const double2* __restrict__ Ftab, double2* __restrict__ M,
@@ -443,7 +449,7 @@ __global__ void __launch_bounds__(tree_threads<P>(), 5) k_p2m_leaf(const int* __
   if (o < NC)
     for (int j = d0 + q; j < d1; j += kTreeLanes) {
       const double xv = x[leaf_dof[j]];
-      const double2 c = C[(size_t)j * NC + o];
+      const double2 c = load_c2(C + (size_t)j * NC + o);
       acc.x = fma(xv, c.x, acc.x);
       acc.y = fma(xv, c.y, acc.y);
     }
@@ -1287,8 +1293,12 @@ int launch_matvec_fmm(const MatvecArgs& a, cudaStream_t st, int stages) {
   // an upward pass over the non-leaf nodes only
   const bool ax_p2m = ND == 1 && a.ax && a.p2m_C && a.leaf_level && a.m2m_level_off_nl;
   if ((stages & STAGE_P2M) && a.n_leaves > 0 && ax_p2m) {
-    launch_pdl(k_p2m_leaf<P>, a.n_leaves, tree_threads<P>(), 0, st, a.leaves, a.leaf_dof_off, a.leaf_dof, a.p2m_C, a.ax, a.node_up,
-               a.leaf_level, a.node_X, a.Ftab, a.M, a.Yup);
+    if (a.p2m_C32)  // low-precision operator: the FP32 copy (half the bytes of the kernel's dominant read)
+      launch_pdl(k_p2m_leaf<P, float2>, a.n_leaves, tree_threads<P>(), 0, st, a.leaves, a.leaf_dof_off, a.leaf_dof, a.p2m_C32, a.ax,
+                 a.node_up, a.leaf_level, a.node_X, a.Ftab, a.M, a.Yup);
+    else
+      launch_pdl(k_p2m_leaf<P, double2>, a.n_leaves, tree_threads<P>(), 0, st, a.leaves, a.leaf_dof_off, a.leaf_dof,
+                 (const double2*)a.p2m_C, a.ax, a.node_up, a.leaf_level, a.node_X, a.Ftab, a.M, a.Yup);
     ++launches;
 
   } else if ((stages & STAGE_P2M) && a.n_leaves > 0) {
@@ -1527,6 +1537,17 @@ void launch_p2m_op(int p, const MatvecArgs& a, const int* e_slot, cudaStream_t s
 #undef BEMB200_CASE
     default: break;
   }
+}
+
+__global__ void k_to_float2(size_t n, const double2* __restrict__ src, float2* __restrict__ dst) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = make_float2((float)src[i].x, (float)src[i].y);
+}
+
+void launch_to_float2(size_t n, const double2* src, float2* dst, cudaStream_t st) {
+  if (n == 0) return;
+  const size_t g = std::min<size_t>((n + 255) / 256, 148 * 16);
+  k_to_float2<<<(int)g, 256, 0, st>>>(n, src, dst);
 }
 
 void launch_combine_weights(int nblocks, const NearBlockDev* blocks, const int* nb_dofs, const int* dof_kind, const double* WG,

@@ -156,6 +156,7 @@ struct MatvecArgs {
   const int* leaf_dof_off = nullptr;
   const int* leaf_dof = nullptr;
   double2* p2m_C = nullptr;
+  const float2* p2m_C32 = nullptr;  // FP32 copy of the P2M operator (low-precision A.x), or null
 };
 
 struct NearArgs {
@@ -218,6 +219,8 @@ int launch_m2l_tc(int p, const MatvecArgs& a, cudaStream_t st, int parts = TC_AL
 // builds the P2M operator (a.p2m_C zeroed beforehand); e_slot[3 s + a]: slot of the DOF of
 // vertex a of element s within its leaf's DOF list
 void launch_p2m_op(int p, const MatvecArgs& a, const int* e_slot, cudaStream_t st);
+// FP32 copy of a complex FP64 array (the low-precision operator's P2M operator)
+void launch_to_float2(size_t n, const double2* src, float2* dst, cudaStream_t st);
 void launch_combine_weights(int nblocks, const NearBlockDev* blocks, const int* nb_dofs, const int* dof_kind, const double* WG,
                             const double* WGn, double* Wc, float* Wc32, cudaStream_t st);
 void launch_densities(int n, int mode, const double* x, const double* known, const int* kind, double* phi, double* phin, cudaStream_t st);
