@@ -141,7 +141,8 @@ struct bem_gpu_ctx {
   int64_t dev_bytes = 0;  // device bytes held by the DBuf members below (declared first: destroyed last)
   DBuf<double> Xs{&dev_bytes}, e_q{&dev_bytes}, e_W{&dev_bytes}, e_n{&dev_bytes}, e_near{&dev_bytes}, node_X{&dev_bytes}, WG{&dev_bytes}, WGn{&dev_bytes}, Wc{&dev_bytes}, diag{&dev_bytes};
   DBuf<float> Wc32{&dev_bytes};  // combined near weights of A.x in FP32 (mixed precision, polynomial preconditioner)
-  DBuf<int> leaf_dof_off{&dev_bytes}, leaf_dof{&dev_bytes}, e_slot{&dev_bytes}, slot_block{&dev_bytes};  // P2M operator of A.x: DOFs per leaf
+  DBuf<int> leaf_dof_off{&dev_bytes}, leaf_dof{&dev_bytes}, e_slot{&dev_bytes};  // P2M operator of A.x: DOFs per leaf
+  DBuf<int> near_counter{&dev_bytes};  // next near block of the near-field quadrature
   DBuf<double2> p2m_C{&dev_bytes};                       // [(leaf, DOF)][NC]
   DBuf<float2> p2m_C32{&dev_bytes};                      // its FP32 copy (mixed precision)
   DBuf<double2> near_scratch{&dev_bytes};                // element values of the near-weight kernel
@@ -1058,27 +1059,28 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
   na.WG = ctx->WG.p;
   na.WGn = ctx->WGn.p;
   {
-    std::vector<int> sb(P.nb_targets.size());
     int mr = 0;
     int64_t mel = 1;
     for (int bi = 0; bi < (int)P.blocks.size(); ++bi) {
       const auto& nbk = P.blocks[bi];
-      for (int tl = 0; tl < nbk.ntgt; ++tl) sb[nbk.tgt_off + tl] = bi;
       mr = std::max(mr, nbk.nrng);
       int64_t ne = 0;
       for (int r = 0; r < nbk.nrng; ++r) ne += P.nb_ranges[2 * (nbk.rng_off + r) + 1] - P.nb_ranges[2 * (nbk.rng_off + r)];
       mel = std::max(mel, ne);
     }
-    CK(upn(ctx->slot_block, sb));
-    na.n_slots = (int)sb.size();
-    na.slot_block = ctx->slot_block.p;
+    na.n_slots = (int)P.nb_targets.size();
+    CK(ctx->near_counter.alloc(1));
+    na.next_block = ctx->near_counter.p;
     na.max_nrng = mr;
     na.scratch_stride = 3 * mel;
     CK(ctx->near_scratch.alloc((size_t)near_weights_grid() * na.scratch_stride));
     na.scratch = ctx->near_scratch.p;
   }
   CK(cudaEventRecord(ctx->ev[4], s));
-  launch_near_weights(na, s);
+  if (launch_near_weights(na, s) != 0) {
+    ctx->err = "near-field quadrature: block element ranges exceed the kernel's shared memory";
+    return BEM_ERR_UNSUPPORTED;
+  }
   CK(cudaEventRecord(ctx->ev[5], s));
   CK(cudaGetLastError());
   if (!P.reused_m2l) {  // M2L grouping on the host meanwhile

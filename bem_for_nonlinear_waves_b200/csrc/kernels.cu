@@ -1041,90 +1041,178 @@ __device__ void elem_weights3(int s, int t, const double* __restrict__ Xs, const
   }
 }
 
-// Near-field weights.  Persistent CTAs walk the targets; for each target the CTA integrates
-// every near element of its block once for its three vertices into a per-CTA scratch row in
-// global memory (L2-resident), then each thread sums, for the DOF columns it owns, the
-// vertices of the DOF's incident elements in incidence order.  The block's element ranges
-// and their prefix sums sit in shared memory.  The quadrature work is one evaluation per
-// (target, element) instead of one per (target, DOF, element).
+// Near-field weights.  Persistent CTAs take whole near blocks from a counter; for a block the
+// CTA stages its element ranges and, where it fits in shared memory, the block's element list
+// and the map from each DOF column's incidences (in incidence order) to the element-vertex
+// slot they read (or "not near").  Then for each target of the block it integrates every near
+// element once for its three vertices into a per-CTA scratch row in global memory
+// (L2-resident), and each thread sums, for the DOF columns it owns, its incidences' slots in
+// incidence order.  The searches of an element in the block's ranges are done once per block
+// instead of once per target; a block whose map does not fit searches per target.  The
+// quadrature work is one evaluation per (target, element) instead of one per (target, DOF,
+// element).
 constexpr int kNearThreads = 256;
+constexpr int kNearMapBytes = 70 * 1024;  // element list, column offsets and incidence map of one block
+constexpr unsigned short kNotNear = 0xFFFFu;
 
-__global__ void __launch_bounds__(kNearThreads, 3) k_near_weights(int nslots, const NearBlockDev* __restrict__ blocks,
-                                                              const int* __restrict__ slot_block, const int* __restrict__ nb_dofs,
+// the range r of the sorted half-open ranges holding element s, or -1
+__device__ __forceinline__ int find_range(const int* sRng, int nrng, int s) {
+  int lo = 0, hi = nrng - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    if (s < sRng[2 * mid])
+      hi = mid - 1;
+    else if (s >= sRng[2 * mid + 1])
+      lo = mid + 1;
+    else
+      return mid;
+  }
+  return -1;
+}
+
+// the range r with sR[r] <= li < sR[r + 1]
+__device__ __forceinline__ int range_of_local(const int* sR, int nrng, int li) {
+  int lo = 0, hi = nrng - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sR[mid] <= li)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kNearThreads, 3) k_near_weights(int nblocks, int* __restrict__ next_block, int max_nrng,
+                                                              const NearBlockDev* __restrict__ blocks, const int* __restrict__ nb_dofs,
                                                               const int* __restrict__ nb_targets, const int* __restrict__ nb_ranges,
                                                               const int* __restrict__ dof_inc_off, const int* __restrict__ dof_inc,
                                                               const double* __restrict__ Xs, const int* __restrict__ e_vtx,
                                                               const double* __restrict__ e_near, double near_region, double2* __restrict__ scratch,
                                                               int64_t scratch_stride, double* __restrict__ WG, double* __restrict__ WGn) {
-  extern __shared__ int sm_near[];  // ranges [2 nrng], prefix [nrng + 1]
+  // shared: ranges [2 max_nrng], prefix [max_nrng + 1], then (map mode) element list [nel],
+  // column offsets [ndof + 1] and the incidence map [total incidences] (16-bit slots)
+  extern __shared__ int sm_near[];
+  __shared__ int s_bi, s_total;
+  __shared__ int s_warp[kNearThreads / 32];
   double2* E = scratch + (int64_t)blockIdx.x * scratch_stride;  // [3 * near elements] (G, Gn)
-  int cur_block = -1, nrng = 0, nel = 0;
   int* sRng = sm_near;
-  int* sR = nullptr;
-  for (int slot = blockIdx.x; slot < nslots; slot += gridDim.x) {
-    const int bi = slot_block[slot];
+  int* sR = sm_near + 2 * max_nrng;
+  int* sMap0 = sR + max_nrng + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  while (true) {
+    __syncthreads();  // the previous block's shared data are no longer read
+    if (threadIdx.x == 0) s_bi = atomicAdd(next_block, 1);
+    __syncthreads();
+    const int bi = s_bi;
+    if (bi >= nblocks) return;
     const NearBlockDev B = blocks[bi];
-    if (bi != cur_block) {  // stage the block's ranges
-      __syncthreads();
-      nrng = B.nrng;
-      sR = sm_near + 2 * nrng;
-      const int* rng = nb_ranges + 2 * B.rng_off;
-      for (int i = threadIdx.x; i < 2 * nrng; i += blockDim.x) sRng[i] = rng[i];
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int r = 0; r < nrng; ++r) {
-          sR[r] = acc;
-          acc += sRng[2 * r + 1] - sRng[2 * r];
-        }
-        sR[nrng] = acc;
+    const int nrng = B.nrng, ndof = B.ndof;
+    const int* rng = nb_ranges + 2 * B.rng_off;
+    for (int i = threadIdx.x; i < 2 * nrng; i += blockDim.x) sRng[i] = rng[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int r = 0; r < nrng; ++r) {
+        sR[r] = acc;
+        acc += sRng[2 * r + 1] - sRng[2 * r];
       }
-      __syncthreads();
-      nel = sR[nrng];
-      cur_block = bi;
+      sR[nrng] = acc;
     }
-    const int tl = slot - B.tgt_off;
-    const int t = nb_targets[slot];
-    for (int li = threadIdx.x; li < nel; li += blockDim.x) {
-      int lo = 0, hi = nrng - 1;  // the range r with sR[r] <= li < sR[r + 1]
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (sR[mid] <= li)
-          lo = mid;
-        else
-          hi = mid - 1;
+    // incidences of the block's columns: a contiguous run of columns per thread, block scan
+    const int per = (ndof + blockDim.x - 1) / blockDim.x;
+    const int j0 = min(ndof, (int)threadIdx.x * per), j1 = min(ndof, j0 + per);
+    int local = 0;
+    for (int j = j0; j < j1; ++j) {
+      const int d = nb_dofs[B.dof_off + j];
+      local += dof_inc_off[d + 1] - dof_inc_off[d];
+    }
+    int incl = local;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        const int v = s_warp[w];
+        s_warp[w] = acc;
+        acc += v;
       }
-      const int s = sRng[2 * lo] + (li - sR[lo]);
-      double g[3], gn[3];
-      elem_weights3(s, t, Xs, e_vtx, e_near, near_region, g, gn);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) E[3 * li + a] = make_double2(g[a], gn[a]);
+      s_total = acc;
     }
     __syncthreads();
-    for (int j = threadIdx.x; j < B.ndof; j += blockDim.x) {
-      const int dof = nb_dofs[B.dof_off + j];
-      double G = 0.0, Gn = 0.0;
-      for (int k = dof_inc_off[dof]; k < dof_inc_off[dof + 1]; ++k) {
-        const int s = dof_inc[k] / 3, a = dof_inc[k] % 3;
-        int lo = 0, hi = nrng - 1;  // s in one of the sorted half-open ranges?
-        while (lo <= hi) {
-          const int mid = (lo + hi) >> 1;
-          if (s < sRng[2 * mid])
-            hi = mid - 1;
-          else if (s >= sRng[2 * mid + 1])
-            lo = mid + 1;
-          else {
-            const double2 w = E[3 * (sR[mid] + (s - sRng[2 * mid])) + a];
-            G += w.x;
-            Gn += w.y;
-            break;
-          }
+    const int nel = sR[nrng], total = s_total;
+    // map mode when the element list, the column offsets and the map fit
+    const int map_words = nel + (ndof + 1) + (total + 1) / 2;
+    const bool use_map = map_words * 4 <= kNearMapBytes;
+    int* sElem = sMap0;                                                  // [nel] element of local index li
+    int* sCol = sElem + nel;                                             // [ndof + 1]
+    unsigned short* sMap = reinterpret_cast<unsigned short*>(sCol + ndof + 1);  // [total]
+    if (use_map) {
+      for (int li = threadIdx.x; li < nel; li += blockDim.x) {
+        const int r = range_of_local(sR, nrng, li);
+        sElem[li] = sRng[2 * r] + (li - sR[r]);
+      }
+      int off = s_warp[warp] + incl - local;  // exclusive prefix of this thread's run
+      for (int j = j0; j < j1; ++j) {
+        sCol[j] = off;
+        const int d = nb_dofs[B.dof_off + j];
+        for (int k = dof_inc_off[d]; k < dof_inc_off[d + 1]; ++k) {
+          const int s = dof_inc[k] / 3, a = dof_inc[k] % 3;
+          const int r = find_range(sRng, nrng, s);
+          sMap[off++] = r < 0 ? kNotNear : (unsigned short)(3 * (sR[r] + (s - sRng[2 * r])) + a);
         }
       }
-      WG[B.w_off + (int64_t)tl * B.ndof + j] = G;
-      WGn[B.w_off + (int64_t)tl * B.ndof + j] = Gn;
+      if (threadIdx.x == 0) sCol[ndof] = total;
     }
-    __syncthreads();  // E is rewritten by the next target
+    __syncthreads();
+    for (int tl = 0; tl < B.ntgt; ++tl) {
+      const int t = nb_targets[B.tgt_off + tl];
+      for (int li = threadIdx.x; li < nel; li += blockDim.x) {
+        int s;
+        if (use_map) {
+          s = sElem[li];
+        } else {
+          const int r = range_of_local(sR, nrng, li);
+          s = sRng[2 * r] + (li - sR[r]);
+        }
+        double g[3], gn[3];
+        elem_weights3(s, t, Xs, e_vtx, e_near, near_region, g, gn);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) E[3 * li + a] = make_double2(g[a], gn[a]);
+      }
+      __syncthreads();
+      for (int j = threadIdx.x; j < ndof; j += blockDim.x) {
+        double G = 0.0, Gn = 0.0;
+        if (use_map) {
+          for (int q = sCol[j]; q < sCol[j + 1]; ++q) {
+            const unsigned short m = sMap[q];
+            if (m != kNotNear) {
+              const double2 w = E[m];
+              G += w.x;
+              Gn += w.y;
+            }
+          }
+        } else {
+          const int d = nb_dofs[B.dof_off + j];
+          for (int k = dof_inc_off[d]; k < dof_inc_off[d + 1]; ++k) {
+            const int s = dof_inc[k] / 3, a = dof_inc[k] % 3;
+            const int r = find_range(sRng, nrng, s);
+            if (r >= 0) {
+              const double2 w = E[3 * (sR[r] + (s - sRng[2 * r])) + a];
+              G += w.x;
+              Gn += w.y;
+            }
+          }
+        }
+        WG[B.w_off + (int64_t)tl * ndof + j] = G;
+        WGn[B.w_off + (int64_t)tl * ndof + j] = Gn;
+      }
+      __syncthreads();  // E is rewritten by the next target
+    }
   }
 }
 
@@ -1564,12 +1652,27 @@ void launch_densities(int n, int mode, const double* x, const double* known, con
 
 int near_weights_grid() { return 148 * 3; }  // three 256-thread CTAs per SM (80 registers a thread)
 
-void launch_near_weights(const NearArgs& a, cudaStream_t st) {
-  const size_t shm = sizeof(int) * (size_t)(3 * a.max_nrng + 1);
-  if (a.n_slots > 0)
-    k_near_weights<<<std::min(a.n_slots, near_weights_grid()), kNearThreads, shm, st>>>(
-        a.n_slots, a.blocks, a.slot_block, a.nb_dofs, a.nb_targets, a.nb_ranges, a.dof_inc_off, a.dof_inc, a.Xs, a.e_vtx, a.e_near,
-        a.near_region, a.scratch, a.scratch_stride, a.WG, a.WGn);
+int launch_near_weights(const NearArgs& a, cudaStream_t st) {
+  if (a.n_blocks <= 0 || a.n_slots <= 0) return 0;
+  const size_t shm = sizeof(int) * (size_t)(3 * a.max_nrng + 1) + kNearMapBytes;
+  if (shm > 200 * 1024) return -1;
+  {  // the permission only grows, per device (contexts of other threads launch it too)
+    static std::mutex mu;
+    static size_t granted[kMaxDevices] = {};
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+    const bool tracked = dev >= 0 && dev < kMaxDevices;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!tracked || shm > granted[dev]) {
+      if (cudaFuncSetAttribute(k_near_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) != cudaSuccess) return -1;
+      if (tracked) granted[dev] = shm;
+    }
+  }
+  if (cudaMemsetAsync(a.next_block, 0, sizeof(int), st) != cudaSuccess) return -1;
+  k_near_weights<<<std::min(a.n_blocks, near_weights_grid()), kNearThreads, shm, st>>>(
+      a.n_blocks, a.next_block, a.max_nrng, a.blocks, a.nb_dofs, a.nb_targets, a.nb_ranges, a.dof_inc_off, a.dof_inc, a.Xs, a.e_vtx,
+      a.e_near, a.near_region, a.scratch, a.scratch_stride, a.WG, a.WGn);
+  return 0;
 }
 
 void launch_diag(int n, const int* dof_point, const double* GnPhi, double* diag, cudaStream_t st) {

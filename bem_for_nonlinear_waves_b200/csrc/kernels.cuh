@@ -162,7 +162,7 @@ struct MatvecArgs {
 struct NearArgs {
   int n_blocks = 0;
   int n_slots = 0;                  // targets over all blocks (rows of the weight arrays)
-  const int* slot_block = nullptr;  // [n_slots] block of each target slot
+  int* next_block = nullptr;        // device counter of the blocks taken (zeroed at launch)
   int max_nrng = 0;                 // most element ranges of one block
   double2* scratch = nullptr;       // near_weights_grid() rows of 3 x scratch_stride/3 element values
   int64_t scratch_stride = 0;       // >= 3 x most near elements of one block
@@ -224,7 +224,7 @@ void launch_to_float2(size_t n, const double2* src, float2* dst, cudaStream_t st
 void launch_combine_weights(int nblocks, const NearBlockDev* blocks, const int* nb_dofs, const int* dof_kind, const double* WG,
                             const double* WGn, double* Wc, float* Wc32, cudaStream_t st);
 void launch_densities(int n, int mode, const double* x, const double* known, const int* kind, double* phi, double* phin, cudaStream_t st);
-void launch_near_weights(const NearArgs& a, cudaStream_t st);
+int launch_near_weights(const NearArgs& a, cudaStream_t st);  // -1 if the block ranges exceed shared memory
 void launch_diag(int n, const int* dof_point, const double* GnPhi, double* diag, cudaStream_t st);
 int mdot_blocks(int n);
 void launch_mdot(const double* V, int ldv, int k, const double* w, int n, double* partial, double* out, cudaStream_t st);
