@@ -120,6 +120,26 @@ def test_gpu_single_bucket_mesh(product_lib, oracle_mod):
     assert np.abs(bvp.ans - ref).max() <= 1e-9 * np.abs(ref).max()
 
 
+def test_gpu_near_quadrature_block_beyond_shared_memory(product_lib, oracle_mod):
+    """The whole surface in one bucket, so one near block holds every element: its element
+    list, column offsets and incidence map (nf + ndof + 1.5 nf words) exceed the near-quadrature
+    kernel's 70 KB of shared memory, and the kernel searches the block's element ranges per
+    target instead.  Diagonal and operator against the oracle."""
+    t = make_tank(h=0.04)
+    d = build_dofs(t.X, t.tri, t.face_dirichlet)
+    nf, ndof = t.tri.shape[0], d["dof_point"].shape[0]
+    assert (nf + ndof + 1.5 * nf) * 4 > 70 * 1024
+    bvp = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=4, dofs=d, fmm_bucket_max_points=100000)
+    bvp.setup()
+    assert bvp.tree_stats()["m2l_pairs"] == 0
+    o = oracle_mod.Oracle(t.X, t.tri, t.face_dirichlet, d, p=4, max_points=100000)
+    np.testing.assert_allclose(bvp.diag(), o.compute_diag(), rtol=1e-11, atol=1e-11)
+    rng = np.random.default_rng(4)
+    phi, phin = rng.normal(size=bvp.matrix_size), rng.normal(size=bvp.matrix_size)
+    got, exp = bvp.apply(phi, phin), o.apply(phi, phin)
+    assert np.abs(got - exp).max() <= 1e-10 * np.abs(exp).max()
+
+
 def test_gpu_rejects_nonfinite_boundary_values(product_lib):
     t = make_tank(h=0.25)
     bvp = BEM_BVP(t.X, t.tri, t.face_dirichlet, expansion_order=4)
