@@ -52,7 +52,7 @@ def _make_opts(lib, expansion_order, mac_theta, fmm_bucket_max_points, fmm_max_l
     o.max_iter = int(solver_max_iter)
     o.device = int(device)
     o.tol_relative = 1 if tol_relative else 0
-    o.preconditioner = {"none": 0, "jacobi": 1, "near_poly": 2}[preconditioner]
+    o.preconditioner = {"none": 0, "jacobi": 1, "near_poly": 2, "near_block": 3}[preconditioner]
     o.poly_degree = int(poly_degree)
     o.tree_on_host = 0 if tree_on_device else 1
     o.tc_item_pairs = int(tc_item_pairs)

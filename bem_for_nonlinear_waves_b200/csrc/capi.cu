@@ -143,6 +143,10 @@ struct bem_gpu_ctx {
   DBuf<float> Wc32{&dev_bytes};  // combined near weights of A.x in FP32 (mixed precision, polynomial preconditioner)
   DBuf<int> leaf_dof_off{&dev_bytes}, leaf_dof{&dev_bytes}, e_slot{&dev_bytes};  // P2M operator of A.x: DOFs per leaf
   DBuf<int> near_counter{&dev_bytes};  // next near block of the near-field quadrature
+  // near-block preconditioner (preconditioner = 3): core DOFs per near block and the inverses
+  DBuf<int> bj_doff{&dev_bytes}, bj_dofs{&dev_bytes};
+  DBuf<int64_t> bj_ioff{&dev_bytes};
+  DBuf<double> bj_inv{&dev_bytes}, bj_tmp{&dev_bytes};
   DBuf<double2> p2m_C{&dev_bytes};                       // [(leaf, DOF)][NC]
   DBuf<float2> p2m_C32{&dev_bytes};                      // its FP32 copy (mixed precision)
   DBuf<double2> near_scratch{&dev_bytes};                // element values of the near-weight kernel
@@ -309,6 +313,17 @@ struct bem_gpu_ctx {
     a.rows = d_rows;
     a.GPhin = d_gphin;
     a.GnPhi = d_gnphi;
+    return a;
+  }
+  NearBjArgs bj_args() const {
+    NearBjArgs a;
+    if (opts.preconditioner != 3) return a;
+    a.nblocks = (int)plan.blocks.size();
+    a.blocks = blocks.p;
+    a.doff = bj_doff.p;
+    a.dofs = bj_dofs.p;
+    a.ioff = bj_ioff.p;
+    a.inv = bj_inv.p;
     return a;
   }
   // marks an argument set as A.x of mv_in (combined near weights, FP32 ones when lowp)
@@ -488,7 +503,8 @@ int ensure_arnoldi_graph(bem_gpu_ctx* ctx, int prec, bool lowp, int cols) {
   a.cols = cols;
   a.p = ctx->plan.opt.p;
   a.V = ctx->V.p;
-  a.dinv = prec != 0 ? ctx->dinv.p : nullptr;
+  a.dinv = (prec == 1 || prec == 2) ? ctx->dinv.p : nullptr;
+  if (prec == 3) a.bj = ctx->bj_args();
   a.state = ctx->arn_state.p;
   a.x = ctx->mv_in.p;
   a.w = ctx->mv_out.p;
@@ -826,9 +842,9 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
     ctx->err = "tc_item_pairs must be 0 (autotuned) or 1..128 (p <= 10), 1..80 (p 11, 12)";
     return BEM_ERR_INVALID_ARGUMENT;
   }
-  if (ctx->opts.preconditioner < 0 || ctx->opts.preconditioner > 2 || ctx->opts.poly_degree < 0 ||
+  if (ctx->opts.preconditioner < 0 || ctx->opts.preconditioner > 3 || ctx->opts.poly_degree < 0 ||
       ctx->opts.poly_degree > kMaxPolyDegree) {
-    ctx->err = "preconditioner must be 0 (none), 1 (Jacobi) or 2 (near-field polynomial, degree 0..24; 0: 8)";
+    ctx->err = "preconditioner must be 0 (none), 1 (Jacobi), 2 (near-field polynomial, degree 0..24; 0: 8) or 3 (near blocks)";
     return BEM_ERR_INVALID_ARGUMENT;
   }
   PlanOptions po;
@@ -1287,6 +1303,39 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
                 ctx->self_col.p, ctx->WG.p, ctx->WGn.p, ctx->dinv.p, s);
   ctx->launches += 1;
   CK(cudaGetLastError());
+  if (ctx->opts.preconditioner == 3) {  // near-block preconditioner: cores = the DOFs of each block's targets
+    const int nb = (int)P.blocks.size();
+    std::vector<int> doff(nb + 1, 0), cdofs;
+    std::vector<int64_t> ioff(nb + 1, 0);
+    cdofs.reserve(N);
+    for (int b = 0; b < nb; ++b) {
+      const auto& B = P.blocks[b];
+      for (int tl = 0; tl < B.ntgt; ++tl) {
+        const int p = P.nb_targets[B.tgt_off + tl];
+        for (int k = P.point_dof_off[p]; k < P.point_dof_off[p + 1]; ++k) cdofs.push_back(P.point_dof[k]);
+      }
+      doff[b + 1] = (int)cdofs.size();
+      const int64_t m = doff[b + 1] - doff[b];
+      ioff[b + 1] = ioff[b] + m * m;
+    }
+    if ((int)cdofs.size() != N) {
+      ctx->err = "near-block preconditioner: the blocks' targets do not cover every DOF once";
+      return BEM_ERR_INVALID_ARGUMENT;
+    }
+    CK(ctx->bj_doff.alloc(nb + 1));
+    CK(ctx->bj_dofs.alloc(std::max(N, 1)));
+    CK(ctx->bj_ioff.alloc(nb + 1));
+    CK(ctx->bj_inv.alloc(std::max<int64_t>(ioff[nb], 1)));
+    CK(ctx->bj_tmp.alloc(std::max(N, 1)));
+    CK(cudaMemcpyAsync(ctx->bj_doff.p, doff.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->bj_dofs.p, cdofs.data(), sizeof(int) * N, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->bj_ioff.p, ioff.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));  // the host vectors go out of scope
+    launch_bj_setup(ctx->bj_args(), ctx->nb_dofs.p, ctx->dof_point.p, ctx->row_of_point.p, ctx->dof_kind.p, ctx->diag.p, ctx->Wc.p,
+                    ctx->dinv.p, s);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+  }
   ctx->poly.n = 0;
   if (ctx->opts.preconditioner == 2) {
     const int rc = build_poly(ctx);
@@ -1744,6 +1793,12 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     if (prec == 2) {
       launch_arnoldi_update(ctx->Z.p, N, cols, ctx->arn_state.p, ctx->ydev.p, ctx->xdev.p, s);
       ctx->launches += 2;
+    } else if (prec == 3) {  // x += M^{-1} (V R^{-1} g)
+      CK(cudaMemsetAsync(ctx->tmp.p, 0, sizeof(double) * N, s));
+      launch_arnoldi_update(ctx->V.p, N, cols, ctx->arn_state.p, ctx->ydev.p, ctx->tmp.p, s);
+      launch_bj_apply(ctx->bj_args(), ctx->tmp.p, N, nullptr, ctx->bj_tmp.p, s);
+      launch_axpby(N, 1.0, ctx->bj_tmp.p, 1.0, ctx->xdev.p, s);
+      ctx->launches += 4;
     } else if (!jacobi) {
       launch_arnoldi_update(ctx->V.p, N, cols, ctx->arn_state.p, ctx->ydev.p, ctx->xdev.p, s);
       ctx->launches += 2;
@@ -1791,7 +1846,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
     x_zero = false;
     launch_axpby(N, 1.0 / beta, ctx->rdev.p, 0.0, ctx->V.p, s);
     launch_arnoldi_init(ctx->arn_state.p, ctx->arn_g.p, beta, s);
-    launch_arnoldi_prep(N, ctx->V.p, prec != 0 ? ctx->dinv.p : nullptr, ctx->arn_state.p, ctx->mv_in.p, s);
+    launch_arnoldi_prep(N, ctx->V.p, (prec == 1 || prec == 2) ? ctx->dinv.p : nullptr, ctx->arn_state.p, ctx->mv_in.p, s);
     // x_base: the iterate this cycle's corrections start from
     CK(cudaMemcpyAsync(ctx->xbase.p, ctx->xdev.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
     ctx->launches += 3;
@@ -1842,7 +1897,7 @@ int bem_gpu_solve(bem_gpu_ctx* ctx, const double* known, const double* x0, doubl
         if (sat++ >= 5) break;
         if (launched >= cycle_cap) break;
         // the check's operator application overwrote the next step's input: write it again
-        launch_arnoldi_prep(N, ctx->V.p, prec != 0 ? ctx->dinv.p : nullptr, ctx->arn_state.p, ctx->mv_in.p, s);
+        launch_arnoldi_prep(N, ctx->V.p, (prec == 1 || prec == 2) ? ctx->dinv.p : nullptr, ctx->arn_state.p, ctx->mv_in.p, s);
         ctx->launches += 1;
         continue;
       }

@@ -360,7 +360,12 @@ int launch_arnoldi_step(const ArnoldiArgs& a, cudaStream_t st) {
   const int rows = arnoldi_rows(a.nrow);
   const int nb = arnoldi_dot_blocks(a.nrow);
   int launches = 0;
-  if (a.poly && a.poly->n > 0) launches = launch_poly_apply(a, st);  // else x was written by the previous step's k_arn_next
+  if (a.poly && a.poly->n > 0) {
+    launches = launch_poly_apply(a, st);
+  } else if (a.bj.nblocks > 0) {  // x = M^{-1} V[:, n] (block Jacobi)
+    launch_bj_apply(a.bj, a.V, a.nrow, a.state, a.x, st);
+    launches = 1;
+  }  // else x was written by the previous step's k_arn_next
   launches += launch_matvec(a.p, a.mv, st);
   double* h1 = a.h;
   double* h2 = a.h + a.cols;

@@ -1320,6 +1320,145 @@ __global__ void k_jacobi(int n, const int* __restrict__ dof_point, const int* __
   }
 }
 
+// Near-block preconditioner: block Jacobi (non-overlapping additive Schwarz) whose cores are
+// the DOFs of each near block's targets (the points of one deepest bucket), the counterpart of
+// the reference's additive Schwarz on the near-field matrix (SchwarzAdditive_CRS built at
+// bem/BEM_solveBVP_GMRES_FMM.hpp:899-1013, cores grown by BFS over the near-field graph; here
+// the cores are the buckets and there is no overlap).  The core matrix holds the operator's
+// near-field entries among the core's DOFs: combined weight Wc of the row's point and the
+// column DOF, minus diag_i on the diagonal of a Neumann row, unit rows for constraint rows.
+// One CTA per block inverts it by Gauss-Jordan elimination with partial pivoting in shared
+// memory and stores the inverse column-major; a core larger than kBjMax, or one whose
+// elimination meets a zero pivot, keeps the point-Jacobi scaling on its diagonal.
+constexpr int kBjMax = 64;
+constexpr int kBjThreads = 256;
+
+size_t bj_setup_smem() { return sizeof(double) * (2 * (size_t)kBjMax * kBjMax + kBjMax); }
+
+__global__ void __launch_bounds__(kBjThreads) k_bj_setup(const NearBlockDev* __restrict__ blocks, const int* __restrict__ bj_doff,
+                                                        const int* __restrict__ bj_dofs, const int64_t* __restrict__ bj_ioff,
+                                                        const int* __restrict__ nb_dofs, const int* __restrict__ dof_point,
+                                                        const int* __restrict__ row_of_point, const int* __restrict__ dof_kind,
+                                                        const double* __restrict__ diag, const double* __restrict__ Wc,
+                                                        const double* __restrict__ dinv, double* __restrict__ inv) {
+  extern __shared__ double bj_sm[];
+  __shared__ int s_piv, s_ok;
+  __shared__ int s_col[kBjMax];  // column of each core DOF in the block's DOF set
+  const int b = blockIdx.x;
+  const NearBlockDev B = blocks[b];
+  const int d0 = bj_doff[b], m = bj_doff[b + 1] - d0;
+  const int* core = bj_dofs + d0;
+  double* out = inv + bj_ioff[b];  // column-major m x m
+  bool ok = m <= kBjMax;
+  if (ok) {
+    double* A = bj_sm;                         // [m][m] row-major
+    double* X = bj_sm + kBjMax * kBjMax;        // [m][m] inverse being formed
+    double* f = bj_sm + 2 * kBjMax * kBjMax;    // [m] elimination factors
+    const int stride = (B.ndof + 3) & ~3;
+    for (int c = threadIdx.x; c < m; c += blockDim.x) s_col[c] = -1;
+    __syncthreads();
+    {  // the block's DOF set is in first-appearance order: scan it once for the core's DOFs
+      const int* cols = nb_dofs + B.dof_off;
+      for (int k = threadIdx.x; k < B.ndof; k += blockDim.x) {
+        const int d = cols[k];
+        for (int c = 0; c < m; ++c)
+          if (core[c] == d) s_col[c] = k;
+      }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int a = e / m, c = e - a * m;
+      const int i = core[a];
+      const int k = dof_kind[i];
+      double v;
+      if (k == 2) {
+        v = (a == c) ? 1.0 : 0.0;
+      } else {
+        const int col = s_col[c];
+        v = col < 0 ? 0.0 : Wc[B.w4_off + (int64_t)row_of_point[dof_point[i]] * stride + col];
+        if (k == 1 && a == c) v -= diag[i];
+      }
+      A[e] = v;
+      X[e] = (a == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int kk = 0; kk < m; ++kk) {
+      if (threadIdx.x == 0) {
+        int p = kk;
+        double best = fabs(A[kk * m + kk]);
+        for (int r = kk + 1; r < m; ++r)
+          if (fabs(A[r * m + kk]) > best) {
+            best = fabs(A[r * m + kk]);
+            p = r;
+          }
+        s_piv = p;
+        s_ok = best > 1e-300;
+      }
+      __syncthreads();
+      if (!s_ok) {
+        ok = false;
+        break;
+      }
+      const int p = s_piv;
+      if (p != kk)
+        for (int c = threadIdx.x; c < m; c += blockDim.x) {
+          double t = A[kk * m + c];
+          A[kk * m + c] = A[p * m + c];
+          A[p * m + c] = t;
+          t = X[kk * m + c];
+          X[kk * m + c] = X[p * m + c];
+          X[p * m + c] = t;
+        }
+      __syncthreads();
+      const double ip = 1.0 / A[kk * m + kk];
+      __syncthreads();
+      for (int c = threadIdx.x; c < m; c += blockDim.x) {
+        A[kk * m + c] *= ip;
+        X[kk * m + c] *= ip;
+      }
+      for (int r = threadIdx.x; r < m; r += blockDim.x) f[r] = (r == kk) ? 0.0 : A[r * m + kk];
+      __syncthreads();
+      for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+        const int r = e / m, c = e - r * m;
+        if (r != kk) {
+          A[e] = fma(-f[r], A[kk * m + c], A[e]);
+          X[e] = fma(-f[r], X[kk * m + c], X[e]);
+        }
+      }
+      __syncthreads();
+    }
+    if (ok)
+      for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+        const int a = e / m, c = e - a * m;
+        out[(int64_t)c * m + a] = X[e];
+      }
+  }
+  if (!ok)  // point-Jacobi scaling on the diagonal
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int a = e / m, c = e - a * m;
+      out[(int64_t)c * m + a] = (a == c) ? dinv[core[a]] : 0.0;
+    }
+}
+
+// z = M^{-1} y: a warp per block, lane per core row (the inverse column-major: the lanes read
+// consecutive entries); with st, y is the basis column V[:, st->n]
+__global__ void k_bj_apply(int nblocks, const int* __restrict__ bj_doff, const int* __restrict__ bj_dofs, const int64_t* __restrict__ bj_ioff,
+                           const double* __restrict__ inv, const double* __restrict__ y, int ldy, const ArnoldiState* __restrict__ st,
+                           double* __restrict__ z) {
+  pdl_enter();
+  const int b = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (b >= nblocks) return;
+  const double* yc = st ? y + (size_t)st->n * ldy : y;
+  const int d0 = bj_doff[b], m = bj_doff[b + 1] - d0;
+  const int* core = bj_dofs + d0;
+  const double* M = inv + bj_ioff[b];
+  for (int a = lane; a < m; a += 32) {
+    double s = 0.0;
+    for (int c = 0; c < m; ++c) s = fma(M[(int64_t)c * m + a], yc[core[c]], s);
+    z[core[a]] = s;
+  }
+}
+
 // FP64 FMA throughput probe: 8 independent FMA chains per thread.
 __global__ void k_fp64_probe(int iters, double seed, double* __restrict__ sink) {
   double a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6, a7 = a0 + 7;
@@ -1738,6 +1877,31 @@ void launch_add_mul(int n, const double* xb, const double* a, const double* u, d
   int g = (n + 255) / 256;
   if (g > 1184) g = 1184;
   k_add_mul<<<g > 0 ? g : 1, 256, 0, st>>>(n, xb, a, u, y);
+}
+
+void launch_bj_setup(const NearBjArgs& a, const int* nb_dofs, const int* dof_point, const int* row_of_point, const int* dof_kind,
+                     const double* diag, const double* Wc, const double* dinv, cudaStream_t st) {
+  if (a.nblocks <= 0) return;
+  static std::mutex mu;
+  static bool granted[kMaxDevices] = {};
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 0 || dev >= kMaxDevices || !granted[dev]) {
+      cudaFuncSetAttribute(k_bj_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bj_setup_smem());
+      if (dev >= 0 && dev < kMaxDevices) granted[dev] = true;
+    }
+  }
+  k_bj_setup<<<a.nblocks, kBjThreads, bj_setup_smem(), st>>>(a.blocks, a.doff, a.dofs, a.ioff, nb_dofs, dof_point, row_of_point, dof_kind,
+                                                               diag, Wc, dinv, a.inv);
+}
+
+void launch_bj_apply(const NearBjArgs& a, const double* y, int ldy, const ArnoldiState* st, double* z, cudaStream_t s) {
+  if (a.nblocks <= 0) return;
+  const int warps_per_cta = 8;
+  launch_pdl(k_bj_apply, (a.nblocks + warps_per_cta - 1) / warps_per_cta, 32 * warps_per_cta, 0, s, a.nblocks, (const int*)a.doff,
+             (const int*)a.dofs, (const int64_t*)a.ioff, (const double*)a.inv, y, ldy, st, z);
 }
 
 void launch_jacobi(int n, const int* dof_point, const int* dof_kind, const double* diag, const int* block_of_point, const int* row_of_point,

@@ -234,6 +234,20 @@ void launch_scale_inv(int n, const double* x, const double* s, double* y, cudaSt
 void launch_mul(int n, const double* a, const double* x, double* y, cudaStream_t st);
 void launch_hash_fill(int n, unsigned long long seed, double* y, cudaStream_t st);  // fixed pseudo-random [-0.5, 0.5)
 void launch_add_mul(int n, const double* xb, const double* a, const double* u, double* y, cudaStream_t st);
+struct ArnoldiState;
+// near-block (block-Jacobi) preconditioner: per near block the DOFs of its targets (the core)
+// and the column-major inverse of the core's near-field matrix
+struct NearBjArgs {
+  int nblocks = 0;
+  const NearBlockDev* blocks = nullptr;
+  const int* doff = nullptr;      // [nblocks + 1] into dofs
+  const int* dofs = nullptr;      // core DOFs, block by block
+  const int64_t* ioff = nullptr;  // [nblocks + 1] into inv (m^2 per block)
+  double* inv = nullptr;
+};
+void launch_bj_setup(const NearBjArgs& a, const int* nb_dofs, const int* dof_point, const int* row_of_point, const int* dof_kind,
+                     const double* diag, const double* Wc, const double* dinv, cudaStream_t st);
+void launch_bj_apply(const NearBjArgs& a, const double* y, int ldy, const ArnoldiState* st, double* z, cudaStream_t s);
 void launch_jacobi(int n, const int* dof_point, const int* dof_kind, const double* diag, const int* block_of_point, const int* row_of_point,
                    const NearBlockDev* blocks, const int* self_col, const double* WG, const double* WGn, double* dinv, cudaStream_t st);
 double fp64_probe_tflops(cudaStream_t st, double* sink);
@@ -262,6 +276,7 @@ struct ArnoldiArgs {
   // polynomial preconditioner: x = D^{-1} p(B) V[:, n] with B = A_near D^{-1}, written to the
   // operator input and to Z[:, n] (flexible storage: the iterate is updated from Z)
   const PolyRoots* poly = nullptr;  // null: x = (D^{-1}) V[:, n]
+  NearBjArgs bj;                    // nblocks > 0: x = M^{-1} V[:, n] with the near-block preconditioner
   MatvecArgs near;                  // B: a.x (with D^{-1} applied) -> a.w, near field only
   double* prod = nullptr;           // [nrow] running product of the root factors
   double* y = nullptr;              // [nrow] polynomial accumulator

@@ -597,7 +597,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="tank_60k", choices=list(CONFIGS))
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--precond", default="jacobi", choices=["jacobi", "none", "near_poly"])
+    ap.add_argument("--precond", default="near_block", choices=["near_block", "jacobi", "none", "near_poly"])
     ap.add_argument("--poly-degree", type=int, default=8, help="degree of the near_poly preconditioner")
     ap.add_argument("--overlap-near", type=int, default=1, help="1: near field of the mixed A.x on a second stream (0: after the FMM passes)")
     ap.add_argument("--max-iter", type=int, default=1500)

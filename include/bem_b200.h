@@ -60,7 +60,10 @@ typedef struct {
                                 2: right near-field polynomial -- D^-1 p(A_near D^-1), p the GMRES
                                 polynomial (harmonic Ritz roots) of a poly_degree-step Arnoldi run on
                                 A_near D^-1; the device counterpart of the reference's near-field
-                                ILU/Schwarz preconditioners (bem/BEM_solveBVP_GMRES_FMM.hpp:215-1050) */
+                                ILU/Schwarz preconditioners (bem/BEM_solveBVP_GMRES_FMM.hpp:215-1050);
+                                3: right near-block -- block Jacobi over the DOFs of each near block's
+                                targets (the reference's additive Schwarz, :899-1013, with bucket
+                                cores and no overlap), inverses formed at set-up */
   int32_t precision;         /* 0: FP64 throughout; 1: mixed -- GMRES corrections use the tensor-core
                                 M2L (FP16 split operands, FP32 accumulate), FP64 outer refinement on the
                                 true residual, same stopping test; needs p <= 12 */
