@@ -1441,7 +1441,9 @@ __global__ void __launch_bounds__(kBjThreads) k_bj_setup(const NearBlockDev* __r
 }
 
 // z = M^{-1} y: a warp per block, lane per core row (the inverse column-major: the lanes read
-// consecutive entries); with st, y is the basis column V[:, st->n]
+// consecutive entries); the core's y values are gathered 32 at a time, one per lane, and
+// broadcast by shuffles, so the gathers are not chained through the sum.  With st, y is the
+// basis column V[:, st->n].
 __global__ void k_bj_apply(int nblocks, const int* __restrict__ bj_doff, const int* __restrict__ bj_dofs, const int64_t* __restrict__ bj_ioff,
                            const double* __restrict__ inv, const double* __restrict__ y, int ldy, const ArnoldiState* __restrict__ st,
                            double* __restrict__ z) {
@@ -1452,10 +1454,18 @@ __global__ void k_bj_apply(int nblocks, const int* __restrict__ bj_doff, const i
   const int d0 = bj_doff[b], m = bj_doff[b + 1] - d0;
   const int* core = bj_dofs + d0;
   const double* M = inv + bj_ioff[b];
-  for (int a = lane; a < m; a += 32) {
+  for (int a0 = 0; a0 < m; a0 += 32) {  // rows a0 .. a0 + 31
+    const int a = a0 + lane;
     double s = 0.0;
-    for (int c = 0; c < m; ++c) s = fma(M[(int64_t)c * m + a], yc[core[c]], s);
-    z[core[a]] = s;
+    for (int c0 = 0; c0 < m; c0 += 32) {  // columns c0 .. c0 + 31, in order
+      const double yv = (c0 + lane < m) ? yc[core[c0 + lane]] : 0.0;
+      const int cn = min(32, m - c0);
+      for (int k = 0; k < cn; ++k) {
+        const double yk = __shfl_sync(0xffffffffu, yv, k);
+        if (a < m) s = fma(M[(int64_t)(c0 + k) * m + a], yk, s);
+      }
+    }
+    if (a < m) z[core[a]] = s;
   }
 }
 
