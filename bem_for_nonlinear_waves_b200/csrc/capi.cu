@@ -1523,9 +1523,10 @@ int64_t bem_gpu_estimate_bytes(const bem_gpu_opts* o, const bem_bvp_desc* d) {
   const int64_t pairs = 11 * nf;
   int64_t b = nnz * (8 + 8 + 8 + (o->precision == 1 ? 4 : 0));
   b += pairs * 2 * nc * 16 + (o->precision == 1 ? pairs * (kp * 4 / 8 + 8) : 0);
-  b += nf * 2 * nc * 16;  // P2M operator columns
+  b += nf * 2 * nc * 16 + (o->precision == 1 ? nf * 2 * nc * 8 : 0);  // P2M operator columns (and their FP32 copy)
   b += (int64_t)(std::max(o->max_iter, 1) + 2) * ndof * 8 * (o->preconditioner == 2 ? 2 : 1);
   b += nf * (18 + 6 + 3 + 8) * 8 + nf * 3 * 4 * 4 + np * 64 + ndof * 160;
+  if (o->preconditioner == 3) b += ndof * (64 * 8 + 16);  // near-block inverses (cores of <= 64 DOFs) and core lists
   return b + ((int64_t)64 << 20);
 }
 
