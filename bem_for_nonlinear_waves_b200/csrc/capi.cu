@@ -1316,7 +1316,7 @@ static int setup_impl(bem_gpu_ctx* ctx, const bem_bvp_desc* d, bool refresh) {
       }
       doff[b + 1] = (int)cdofs.size();
       const int64_t m = doff[b + 1] - doff[b];
-      ioff[b + 1] = ioff[b] + m * m;
+      ioff[b + 1] = ioff[b] + (m <= kBjMaxCore ? m * m : m);
     }
     if ((int)cdofs.size() != N) {
       ctx->err = "near-block preconditioner: the blocks' targets do not cover every DOF once";

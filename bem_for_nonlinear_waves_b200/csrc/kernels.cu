@@ -1328,9 +1328,10 @@ __global__ void k_jacobi(int n, const int* __restrict__ dof_point, const int* __
 // near-field entries among the core's DOFs: combined weight Wc of the row's point and the
 // column DOF, minus diag_i on the diagonal of a Neumann row, unit rows for constraint rows.
 // One CTA per block inverts it by Gauss-Jordan elimination with partial pivoting in shared
-// memory and stores the inverse column-major; a core larger than kBjMax, or one whose
-// elimination meets a zero pivot, keeps the point-Jacobi scaling on its diagonal.
-constexpr int kBjMax = 64;
+// memory and stores the inverse column-major; a core whose elimination meets a zero pivot
+// keeps the point-Jacobi scaling on the diagonal of its m x m slot, and a core larger than
+// kBjMax keeps it as m diagonal entries only (its slot holds m values, not m^2).
+constexpr int kBjMax = kBjMaxCore;
 constexpr int kBjThreads = 256;
 
 size_t bj_setup_smem() { return sizeof(double) * (2 * (size_t)kBjMax * kBjMax + kBjMax); }
@@ -1349,8 +1350,12 @@ __global__ void __launch_bounds__(kBjThreads) k_bj_setup(const NearBlockDev* __r
   const int d0 = bj_doff[b], m = bj_doff[b + 1] - d0;
   const int* core = bj_dofs + d0;
   double* out = inv + bj_ioff[b];  // column-major m x m
-  bool ok = m <= kBjMax;
-  if (ok) {
+  if (m > kBjMax) {  // diagonal slot
+    for (int a = threadIdx.x; a < m; a += blockDim.x) out[a] = dinv[core[a]];
+    return;
+  }
+  bool ok = true;
+  {
     double* A = bj_sm;                         // [m][m] row-major
     double* X = bj_sm + kBjMax * kBjMax;        // [m][m] inverse being formed
     double* f = bj_sm + 2 * kBjMax * kBjMax;    // [m] elimination factors
@@ -1454,6 +1459,10 @@ __global__ void k_bj_apply(int nblocks, const int* __restrict__ bj_doff, const i
   const int d0 = bj_doff[b], m = bj_doff[b + 1] - d0;
   const int* core = bj_dofs + d0;
   const double* M = inv + bj_ioff[b];
+  if (m > kBjMax) {  // a core kept diagonal: m entries
+    for (int a = lane; a < m; a += 32) z[core[a]] = M[a] * yc[core[a]];
+    return;
+  }
   for (int a0 = 0; a0 < m; a0 += 32) {  // rows a0 .. a0 + 31
     const int a = a0 + lane;
     double s = 0.0;

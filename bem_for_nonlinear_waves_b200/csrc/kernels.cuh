@@ -236,13 +236,15 @@ void launch_hash_fill(int n, unsigned long long seed, double* y, cudaStream_t st
 void launch_add_mul(int n, const double* xb, const double* a, const double* u, double* y, cudaStream_t st);
 struct ArnoldiState;
 // near-block (block-Jacobi) preconditioner: per near block the DOFs of its targets (the core)
-// and the column-major inverse of the core's near-field matrix
+// and the column-major inverse of the core's near-field matrix (m^2 values); a core of more
+// than kBjMaxCore DOFs keeps the point-Jacobi scaling as m diagonal values
+constexpr int kBjMaxCore = 64;
 struct NearBjArgs {
   int nblocks = 0;
   const NearBlockDev* blocks = nullptr;
   const int* doff = nullptr;      // [nblocks + 1] into dofs
   const int* dofs = nullptr;      // core DOFs, block by block
-  const int64_t* ioff = nullptr;  // [nblocks + 1] into inv (m^2 per block)
+  const int64_t* ioff = nullptr;  // [nblocks + 1] into inv (m^2 per block, m above kBjMaxCore)
   double* inv = nullptr;
 };
 void launch_bj_setup(const NearBjArgs& a, const int* nb_dofs, const int* dof_point, const int* row_of_point, const int* dof_kind,
