@@ -69,3 +69,34 @@ def test_plan_rejects_nonfinite_coordinates(product_lib):
     X[3, 1] = np.nan
     with pytest.raises(ValueError):
         inspect_plan(X, t.tri, t.face_dirichlet, d)
+
+
+def test_device_memory_estimate_counts_precision_and_preconditioner_buffers(product_lib):
+    """bem_gpu_estimate_bytes (host arithmetic only): the mixed context adds the FP32 weights and
+    the FP32 copy of the P2M operator, the near-block preconditioner its inverses (at most 64^2
+    values per core of <= 64 DOFs) and core lists, the polynomial preconditioner its flexible
+    basis."""
+    import ctypes
+
+    from bem_for_nonlinear_waves_b200 import _lib as L
+    from bem_for_nonlinear_waves_b200.bvp import _make_opts
+
+    t = make_tank(h=0.05)
+    d = build_dofs(t.X, t.tri, t.face_dirichlet)
+    X = np.ascontiguousarray(t.X, np.float64)
+    tri = np.ascontiguousarray(t.tri, np.int32)
+    fd = np.ascontiguousarray(t.face_dirichlet, np.uint8)
+    arrs = [np.ascontiguousarray(d[k], np.int32).reshape(-1) for k in ("dof_point", "dof_face", "dof_kind", "face_dof")]
+    desc = L.Desc(X.shape[0], L.ptr(X, L.P_dbl), tri.shape[0], L.ptr(tri, L.P_int), L.ptr(fd, L.P_u8), arrs[0].shape[0],
+                  L.ptr(arrs[0], L.P_int), L.ptr(arrs[1], L.P_int), L.ptr(arrs[2], L.P_int), L.ptr(arrs[3], L.P_int))
+
+    def est(precond, precision):
+        o = _make_opts(product_lib, 8, 0.25, 30, 7, 1e-9, 500, 0, True, precond, precision)
+        return product_lib.bem_gpu_estimate_bytes(ctypes.byref(o), ctypes.byref(desc))
+
+    ndof = arrs[0].shape[0]
+    base = est("jacobi", "fp64")
+    assert base > 0
+    assert est("jacobi", "mixed") > base
+    assert est("near_block", "fp64") - base == ndof * (64 * 8 + 16)
+    assert est("near_poly", "fp64") - base == (500 + 2) * ndof * 8  # the flexible basis: max_iter + 2 more columns
